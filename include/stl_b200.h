@@ -1,0 +1,164 @@
+/* C ABI of the B200 ScatCov engine (libstl_b200.so).
+ *
+ * Drop-in for the reference's stl-bridge C ABI (jmdelouis/STL-Dev-MPI,
+ * crates/stl-bridge/src/lib.rs), bound by its Python module
+ * python/stl_ensemble/stl_port/native.py (signature table at
+ * native.py:56-110) when STL_NATIVE_LIBRARY points at this library.
+ *
+ * Conventions (as the reference): maps are f64 NESTED [batch, 12 nside^2];
+ * values and cotangents complex128 interleaved (re, im) [batch, ncoeff];
+ * the gradient is that of Re sum(conj(cotangent) * values); every forward
+ * state has an identity (handle, generation, member, objective) that
+ * stlp_vjp / stlp_restore check.  Failures return -1 (int), NULL
+ * (pointers) and set stlp_last_error().  One caller thread per handle.
+ */
+#ifndef STL_B200_H
+#define STL_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct StlpHandle StlpHandle;
+typedef struct StlpSnapshot StlpSnapshot;
+typedef struct StlpPatchHandle StlpPatchHandle;
+
+/* Message of the last failure on the calling thread; library-owned, valid
+ * until the next failure on that thread.  (stl-bridge lib.rs:260-263) */
+const char* stlp_last_error(void);
+
+/* Frees a string returned by stlp_info / stlp_patch_info.  (lib.rs:266-271) */
+void stlp_string_free(char* p);
+
+/* New handle from a JSON config: nside (128), j (7), batch (1), kernel (5),
+ * orientations (4), backend ("gpu"; "cpu" is refused: no CPU fallback),
+ * device (0), dtype ("float64" | "float32": field precision; sums stay
+ * FP64).  Unknown keys are ignored.  The device operators are built on
+ * first use (or by stlp_prepare).  NULL on failure.  (lib.rs:280-351) */
+StlpHandle* stlp_new(const char* config);
+
+/* Frees a handle (NULL ignored).  (lib.rs:354-359) */
+void stlp_free(StlpHandle* h);
+
+/* JSON: version, sizes, dtype, the plan [{index, family, native_dg, c1, c2,
+ * j1, j2, j3, l1, l2, l3}], device memory, timers.  Free with
+ * stlp_string_free.  (lib.rs:364-391) */
+char* stlp_info(StlpHandle* h);
+
+/* Masked averages: k masks [k, 12 nside^2] (k = 0: whole sky).
+ * (lib.rs:396-422) */
+int stlp_set_masks(StlpHandle* h, const double* weights, size_t k);
+
+/* Pixels each coefficient averages, [K, ncoeff].  (lib.rs:459-472) */
+int stlp_native_pixels(StlpHandle* h, size_t* out);
+
+/* Forward sweep of host maps x (n = batch * 12 nside^2): values to out
+ * (2 batch ncoeff), with moments the spatial variances to var (batch
+ * ncoeff).  (lib.rs:478-530) */
+int stlp_forward(StlpHandle* h, const double* x, size_t n, uint64_t generation, uint64_t member, uint64_t objective,
+                 bool moments, double* out, double* var);
+
+/* Map cotangent out (batch * 12 nside^2) of the cotangents cot (n = batch
+ * ncoeff complex) after the forward of the same identity.  (lib.rs:535-581) */
+int stlp_vjp(StlpHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t member, uint64_t objective,
+             double* out);
+
+/* Forward on maps already on the device (x: device pointer to f32 if f32,
+ * else f64; same layout as stlp_forward).  Values go to host memory.
+ * Runs on the handle's stream (stlp_set_stream) and returns once done.
+ * No reference counterpart for full-sky maps; the pattern of
+ * stlp_patch_forward_device (lib.rs:1153). */
+int stlp_forward_device(StlpHandle* h, uint64_t x, size_t n, int f32, uint64_t generation, uint64_t member,
+                        uint64_t objective, bool moments, double* out, double* var);
+
+/* Map cotangent written to device memory out (f32 if f32, else f64) after
+ * the forward of the same identity; cotangents on the host.  Returns once
+ * the stream has finished.  (pattern of stlp_patch_vjp_device, lib.rs:1171) */
+int stlp_vjp_device(StlpHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t member,
+                    uint64_t objective, uint64_t out, int f32);
+
+/* CUDA stream (cudaStream_t as an integer, 0: default stream) the handle
+ * launches on.  No reference counterpart. */
+int stlp_set_stream(StlpHandle* h, uint64_t stream);
+
+/* Builds the device operators now instead of at the first forward.  No
+ * reference counterpart (the reference builds in stlp_new). */
+int stlp_prepare(StlpHandle* h);
+
+/* Copy of the current forward state (the loaded maps; the fields are
+ * recomputed by stlp_restore); NULL on failure.  (lib.rs:647-659) */
+StlpSnapshot* stlp_checkpoint(StlpHandle* h);
+void stlp_checkpoint_free(StlpSnapshot* s);                /* (lib.rs:662-667) */
+size_t stlp_checkpoint_bytes(const StlpSnapshot* s);       /* (lib.rs:670-680) */
+/* Makes a checkpoint of this handle the current state.  (lib.rs:684-709) */
+int stlp_restore(StlpHandle* h, const StlpSnapshot* s, uint64_t generation, uint64_t member, uint64_t objective);
+
+/* Statistics of maps given at every level (validation).  (lib.rs:588-623) */
+int stlp_forward_levels(StlpHandle* h, const double* x, size_t n, double* out);
+
+/* L-BFGS with strong Wolfe line search of the callback from x (updated in
+ * place); options JSON: lr (1), max_iter (20), max_eval, tolerance_grad
+ * (1e-12), tolerance_change (1e-15), history_size (10).  Returns the number
+ * of evaluations, -1 on failure (non-finite loss or gradient included).
+ * (lib.rs:711-741) */
+typedef double (*stlp_callback)(const double* x, size_t n, double* grad, void* ctx);
+int64_t stlp_lbfgs(double* x, size_t n, const char* options, stlp_callback callback, void* ctx);
+
+/* Disc patches (lib.rs:743-1176). */
+StlpPatchHandle* stlp_patch_new(const char* config);
+void stlp_patch_free(StlpPatchHandle* h);
+char* stlp_patch_info(StlpPatchHandle* h);
+int stlp_pixel_vectors(size_t nside, const int64_t* ids, size_t n, double* out);
+int stlp_patch_select(StlpPatchHandle* h, const double* centres, size_t b, double radius, double core, size_t* counts);
+int stlp_patch_ids(StlpPatchHandle* h, size_t patch, int64_t* out);
+int stlp_patch_core_pixels(StlpPatchHandle* h, size_t* out);
+int stlp_patch_forward(StlpPatchHandle* h, const double* x, size_t n, uint64_t generation, bool moments, double* out,
+                       double* var);
+int stlp_patch_vjp(StlpPatchHandle* h, const double* cot, size_t n, uint64_t generation, double* out);
+int stlp_patch_forward_device(StlpPatchHandle* h, uint64_t x, size_t n, uint64_t generation, bool moments,
+                              double* out, double* var);
+int stlp_patch_vjp_device(StlpPatchHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t out);
+
+/* Entry points of subsystems outside this engine (spin-2 front end,
+ * spectrum, U-Net training).  They exist so that native.py's signature
+ * table binds; each returns failure with stlp_last_error() naming the
+ * subsystem as not built.  (lib.rs:628-643, 1178-1492; unet.rs) */
+int stlp_spin_fields(StlpHandle* h, const double* x, size_t n, size_t level, double* qu, double* chi);
+void* stlp_spec_new(const char* config);
+void stlp_spec_free(void* h);
+char* stlp_spec_info(void* h);
+int stlp_spec_set_masks(void* h, const double* w, size_t k);
+int stlp_spec_forward(void* h, const double* x, size_t n, uint64_t g, uint64_t m, uint64_t o, double* out);
+int stlp_spec_vjp(void* h, const double* cot, size_t n, uint64_t g, uint64_t m, uint64_t o, double* out);
+void* stlp_unet_new(const char* config);
+void stlp_unet_free(void* h);
+char* stlp_unet_info(void* h);
+int stlp_unet_get_params(void* h, float* out);
+int stlp_unet_set_params(void* h, const float* p, size_t n);
+int stlp_unet_get_grads(void* h, float* out);
+int stlp_unet_zero_grad(void* h);
+int stlp_unet_adam(void* h, double lr);
+int stlp_unet_set_cond(void* h, const float* c, size_t n);
+int stlp_unet_apply(void* h, const double* x, size_t n, double* a, double* b, double* c);
+int stlp_train_set_masks(void* h, const double* w, size_t k);
+int stlp_train_set_common(void* h, const double* w);
+int stlp_train_set_field(void* h, uint32_t f, const double* a, const double* b, const double* c, const double* d,
+                         const double* e, const double* g, size_t n, double s);
+int stlp_train_bias(void* h, uint32_t f, const uint64_t* a, const double* b, size_t n);
+int stlp_train_loss(void* h, uint32_t f, bool a, double* out);
+int stlp_train_step(void* h, uint32_t f, double lr, double* out);
+int stlp_train_live(void* h, uint32_t f, const uint64_t* a, const double* b, size_t n, const uint64_t* c,
+                    const double* d, size_t m, bool e, double s, double* out);
+void* stlp_train_lbfgs(void* h, const uint32_t* f, size_t n, const char* opts);
+int stlp_train_set_joint(void* h, const double* a, const double* b, uint32_t c, uint32_t d, const char* e, double s);
+int stlp_train_front(void* h, const double* x, size_t n, bool a, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STL_B200_H */

@@ -150,6 +150,21 @@ void or_down_get(void* hv, i64* coarse, i64* indptr, i64* indices, double* value
 }
 void or_down_free(void* h) { delete (DownH*)h; }
 
+// plan rows (family, native, c1, c2, j1, j2, j3, l1, l2, l3) of dg(j) = j;
+// returns the count (rows written only when it fits in cap)
+i64 or_build_plan(int J, int L, int C, int cross_only, int* out, i64 cap) {
+  std::vector<int> dg(J);
+  for (int j = 0; j < J; ++j) dg[j] = j;
+  auto plan = build_plan(J, L, dg, C, cross_only != 0);
+  if ((i64)plan.size() <= cap)
+    for (size_t i = 0; i < plan.size(); ++i) {
+      const Coef& c = plan[i];
+      int v[10] = {c.family, c.native, c.c1, c.c2, c.j1, c.j2, c.j3, c.l1, c.l2, c.l3};
+      std::memcpy(out + 10 * i, v, sizeof(v));
+    }
+  return (i64)plan.size();
+}
+
 // -- engine ----------------------------------------------------------------
 struct EngineH {
   Engine e;

@@ -61,6 +61,7 @@ def lib():
             "or_down_nnz": ([C.c_void_p], C.c_int64),
             "or_down_get": ([C.c_void_p, _I64, _I64, _I64, _D], None),
             "or_down_free": ([C.c_void_p], None),
+            "or_build_plan": ([C.c_int, C.c_int, C.c_int, C.c_int, _I32, C.c_int64], C.c_int64),
             "or_engine_new": ([C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I32, C.c_int, C.c_double], C.c_void_p),
             "or_engine_free": ([C.c_void_p], None),
             "or_engine_ncoeff": ([C.c_void_p], C.c_int64),
@@ -239,6 +240,14 @@ def plan_dicts(plan_rows):
         out.append({"index": i, "family": FAMILIES[r[0]], "native_dg": int(r[1]), "c1": int(r[2]), "c2": int(r[3]),
                     "j1": f(r[4]), "j2": f(r[5]), "j3": f(r[6]), "l1": f(r[7]), "l2": f(r[8]), "l3": f(r[9])})
     return out
+
+
+def build_plan(J, L=4, channels=1, cross_only=False):
+    """Plan dicts of dg(j) = j (plan.rs:80-158), as the bridge's stlp_info lists them."""
+    n = lib().or_build_plan(J, L, channels, int(cross_only), None, 0)
+    rows = np.empty((n, 10), np.int32)
+    lib().or_build_plan(J, L, channels, int(cross_only), _p(rows, _I32), n)
+    return plan_dicts(rows)
 
 
 class OracleEngine:

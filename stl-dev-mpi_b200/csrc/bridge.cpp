@@ -1,0 +1,312 @@
+// C ABI of the B200 ScatCov engine: the `stlp_*` entry points of the
+// reference's stl-bridge (crates/stl-bridge/src/lib.rs), same names, types
+// and conventions, so that its Python binding (python/stl_ensemble/
+// stl_port/native.py) loads this library through STL_NATIVE_LIBRARY.
+//
+// Conventions kept from the reference: maps are f64 NESTED [batch, 12
+// nside^2]; complex values and cotangents are interleaved (re, im); the
+// gradient is that of Re sum(conj(cotangent) * values); every forward
+// state carries an identity (handle, generation, member, objective) that
+// stlp_vjp and stlp_restore check; failures return -1 / NULL and
+// stlp_last_error() holds the message (thread-local, owned by the
+// library).  Additions: device-pointer forward/VJP (f32 or f64 maps),
+// the caller's CUDA stream, and an explicit prepare.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <string>
+
+#include "engine.cuh"
+#include "json.hpp"
+#include "scatcov.hpp"
+#include "../../include/stl_b200.h"
+
+using namespace stl;
+
+namespace {
+
+const char* kVersion = "stl-b200-0.1 (abi 2026-11-09-v12)";
+thread_local std::string g_error;
+std::atomic<uint64_t> g_next_id{1};
+
+struct Identity {
+  uint64_t owner = 0, generation = 0, member = 0, objective = 0;
+  bool operator==(const Identity& o) const {
+    return owner == o.owner && generation == o.generation && member == o.member && objective == o.objective;
+  }
+};
+
+template <typename R, typename F>
+R guard(R fail, F&& f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    g_error = e.what();
+  } catch (...) {
+    g_error = "unknown native failure";
+  }
+  return fail;
+}
+
+void require(bool ok, const std::string& msg) {
+  if (!ok) throw std::runtime_error(msg);
+}
+
+std::string jstr(const std::string& s) {
+  std::string o = "\"";
+  for (char c : s) {
+    if (c == '"' || c == '\\') { o += '\\'; o += c; }
+    else if (c == '\n') o += "\\n";
+    else o += c;
+  }
+  return o + "\"";
+}
+
+}  // namespace
+
+namespace stl {
+void set_error(const std::string& msg) { g_error = msg; }
+}  // namespace stl
+
+struct StlpHandle {
+  std::unique_ptr<Engine> engine;
+  uint64_t id = 0;
+  bool has_current = false;
+  Identity current;
+  int device = 0;
+  size_t input_len() const { return (size_t)engine->options().B * (size_t)engine->npix(0); }
+  size_t values_len() const { return (size_t)engine->options().B * engine->plan().size(); }
+  void activate() { STL_CUDA(cudaSetDevice(device)); }
+};
+
+struct StlpSnapshot {
+  Identity identity;
+  uint64_t owner = 0;
+  std::vector<double> maps;
+};
+
+extern "C" {
+
+const char* stlp_last_error(void) { return g_error.c_str(); }
+
+void stlp_string_free(char* p) { free(p); }
+
+StlpHandle* stlp_new(const char* config) {
+  return guard<StlpHandle*>(nullptr, [&]() -> StlpHandle* {
+    Json v = Json::parse(config);
+    require(v.kind == Json::Object, "config must be a JSON object");
+    Options o;
+    o.nside = v.integer("nside", 128);
+    o.J = (int)v.integer("j", 7);
+    o.B = (int)v.integer("batch", 1);
+    o.ksz = (int)v.integer("kernel", 5);
+    o.L = (int)v.integer("orientations", 4);
+    o.device = (int)v.integer("device", 0);
+    std::string backend = v.string("backend", "gpu");
+    require(backend == "gpu",
+            "backend '" + backend + "' is not built in this library: it is the B200 engine (use backend \"gpu\")");
+    std::string dtype = v.string("dtype", "float64");
+    require(dtype == "float64" || dtype == "float32", "dtype must be float64 or float32");
+    o.fp32 = dtype == "float32";
+    require(!v.boolean("cross", false), "cross statistics (two channels) are not built in this library");
+    require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
+    require(o.nside > 0 && (o.nside & (o.nside - 1)) == 0, "nside must be a power of two");
+    auto h = std::make_unique<StlpHandle>();
+    h->engine = Engine::create(o);
+    h->device = o.device;
+    h->id = g_next_id.fetch_add(1);
+    return h.release();
+  });
+}
+
+void stlp_free(StlpHandle* h) {
+  if (!h) return;
+  try {
+    h->activate();
+  } catch (...) {
+  }
+  delete h;
+}
+
+int stlp_prepare(StlpHandle* h) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr, "null handle");
+    h->activate();
+    h->engine->prepare();
+    return 0;
+  });
+}
+
+int stlp_set_stream(StlpHandle* h, uint64_t stream) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr, "null handle");
+    h->engine->set_stream(reinterpret_cast<cudaStream_t>(stream));
+    return 0;
+  });
+}
+
+char* stlp_info(StlpHandle* h) {
+  return guard<char*>(nullptr, [&]() -> char* {
+    require(h != nullptr, "null handle");
+    const Engine& e = *h->engine;
+    const Options& o = e.options();
+    std::ostringstream js;
+    js.precision(17);
+    js << "{\"version\": " << jstr(kVersion) << ", \"engine\": \"b200\", \"nside\": " << o.nside
+       << ", \"j\": " << o.J << ", \"batch\": " << o.B << ", \"channels\": 1, \"cross\": false"
+       << ", \"dtype\": " << jstr(o.fp32 ? "float32 fields, float64 sums/complex128" : "float64/complex128")
+       << ", \"fewer\": false, \"orientations\": " << o.L << ", \"kernel\": " << o.ksz
+       << ", \"levels\": " << e.levels() << ", \"masks\": 0, \"spin\": 0, \"device\": " << o.device
+       << ", \"conv\": \"folded-stencil\", \"fields\": \"keep\"";
+    js << ", \"device_memory\": {\"operator_bytes\": " << e.operator_bytes() << ", \"field_bytes\": " << e.field_bytes()
+       << ", \"live_bytes\": " << device_bytes_live() << ", \"peak_bytes\": " << device_bytes_peak() << "}";
+    js << ", \"timers\": {\"build_s\": " << e.timers.build_s << ", \"forward_ms\": " << e.timers.forward_ms
+       << ", \"reverse_ms\": " << e.timers.reverse_ms << ", \"forwards\": " << e.timers.forwards
+       << ", \"reverses\": " << e.timers.reverses << "}";
+    js << ", \"plan\": [";
+    const auto& plan = e.plan();
+    auto opt = [](int v) { return v < 0 ? std::string("null") : std::to_string(v); };
+    for (size_t i = 0; i < plan.size(); ++i) {
+      const Coef& c = plan[i];
+      if (i) js << ", ";
+      js << "{\"index\": " << i << ", \"family\": \"" << family_name(c.family) << "\", \"native_dg\": " << c.native
+         << ", \"c1\": " << c.c1 << ", \"c2\": " << c.c2 << ", \"j1\": " << opt(c.j1) << ", \"j2\": " << opt(c.j2)
+         << ", \"j3\": " << opt(c.j3) << ", \"l1\": " << opt(c.l1) << ", \"l2\": " << opt(c.l2)
+         << ", \"l3\": " << opt(c.l3) << "}";
+    }
+    js << "]}";
+    std::string s = js.str();
+    char* out = (char*)malloc(s.size() + 1);
+    std::memcpy(out, s.c_str(), s.size() + 1);
+    return out;
+  });
+}
+
+int stlp_native_pixels(StlpHandle* h, size_t* out) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && out != nullptr, "null argument");
+    const auto& plan = h->engine->plan();
+    for (size_t i = 0; i < plan.size(); ++i) out[i] = (size_t)h->engine->npix(plan[i].native);
+    return 0;
+  });
+}
+
+int stlp_set_masks(StlpHandle* h, const double* weights, size_t k) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr, "null handle");
+    (void)weights;
+    h->has_current = false;
+    require(k == 0, "masked averages are not built in this library yet");
+    return 0;
+  });
+}
+
+static int forward_common(StlpHandle* h, uint64_t generation, uint64_t member, uint64_t objective, bool moments,
+                          double* out, double* var) {
+  h->engine->forward(moments, out, var);
+  h->current = Identity{h->id, generation, member, objective};
+  h->has_current = true;
+  return 0;
+}
+
+int stlp_forward(StlpHandle* h, const double* x, size_t n, uint64_t generation, uint64_t member, uint64_t objective,
+                 bool moments, double* out, double* var) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && x != nullptr && out != nullptr, "null argument");
+    require(n == h->input_len(), "input shape mismatch");
+    require(!moments || var != nullptr, "moments need a variance buffer");
+    h->activate();
+    h->has_current = false;
+    h->engine->load_host(x);
+    return forward_common(h, generation, member, objective, moments, out, var);
+  });
+}
+
+int stlp_forward_device(StlpHandle* h, uint64_t x, size_t n, int f32, uint64_t generation, uint64_t member,
+                        uint64_t objective, bool moments, double* out, double* var) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && x != 0 && out != nullptr, "null argument");
+    require(n == h->input_len(), "input shape mismatch");
+    require(!moments || var != nullptr, "moments need a variance buffer");
+    h->activate();
+    h->has_current = false;
+    h->engine->load_device(reinterpret_cast<const void*>(x), f32 != 0);
+    return forward_common(h, generation, member, objective, moments, out, var);
+  });
+}
+
+static void check_identity(StlpHandle* h, uint64_t generation, uint64_t member, uint64_t objective, size_t n) {
+  require(h->has_current && h->current == Identity{h->id, generation, member, objective},
+          "stale, wrong-member or wrong-objective forward state");
+  require(n == h->values_len(), "cotangent shape mismatch");
+}
+
+int stlp_vjp(StlpHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t member, uint64_t objective,
+             double* out) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && cot != nullptr && out != nullptr, "null argument");
+    check_identity(h, generation, member, objective, n);
+    h->activate();
+    h->engine->reverse_host(cot, out);
+    return 0;
+  });
+}
+
+int stlp_vjp_device(StlpHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t member,
+                    uint64_t objective, uint64_t out, int f32) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && cot != nullptr && out != 0, "null argument");
+    check_identity(h, generation, member, objective, n);
+    h->activate();
+    h->engine->reverse_device(cot, reinterpret_cast<void*>(out), f32 != 0);
+    return 0;
+  });
+}
+
+StlpSnapshot* stlp_checkpoint(StlpHandle* h) {
+  return guard<StlpSnapshot*>(nullptr, [&]() -> StlpSnapshot* {
+    require(h != nullptr, "null handle");
+    require(h->has_current, "checkpoint requires a forward state");
+    h->activate();
+    auto s = std::make_unique<StlpSnapshot>();
+    s->identity = h->current;
+    s->owner = h->id;
+    h->engine->save_input(s->maps);
+    return s.release();
+  });
+}
+
+void stlp_checkpoint_free(StlpSnapshot* s) { delete s; }
+
+size_t stlp_checkpoint_bytes(const StlpSnapshot* s) { return s ? s->maps.size() * sizeof(double) : 0; }
+
+int stlp_restore(StlpHandle* h, const StlpSnapshot* s, uint64_t generation, uint64_t member, uint64_t objective) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && s != nullptr, "null argument");
+    require(s->owner == h->id && s->identity == Identity{h->id, generation, member, objective},
+            "stale, wrong-member, wrong-objective or foreign checkpoint");
+    h->activate();
+    h->has_current = false;
+    // The forward state is recomputed from the saved maps: the sweeps are
+    // deterministic, so the restored fields equal the checkpointed ones.
+    h->engine->load_host(s->maps.data());
+    std::vector<double> values(2 * h->values_len());
+    h->engine->forward(false, values.data(), nullptr);
+    h->current = s->identity;
+    h->has_current = true;
+    return 0;
+  });
+}
+
+int stlp_forward_levels(StlpHandle* h, const double* x, size_t n, double* out) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr, "null handle");
+    (void)x; (void)n; (void)out;
+    throw std::runtime_error("stlp_forward_levels is not built in this library yet");
+    return -1;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,433 @@
+// Level sweeps of the B200 ScatCov engine (forward and exact VJP).
+//
+// Forward, levels ascending (crates/stl-core/src/engine.rs:485-602 in
+// full-sky form): z_n = psi * maps[n] with |z_n| into the stored-moduli
+// field Mod[n] (slot n); the stored moduli of the finer levels pushed one
+// decimation down, Mod[n][d] = D Mod[n-1][d] (m[d][n] = D^(n-d) |z_d|); the
+// second wavelets Br[n] = psi * Mod[n] (all (d, l1) rows in one launch);
+// then the FP64 coefficient sums of the level.
+//
+// Reverse, levels descending (engine.rs:610-724, 1117-1174): the
+// cotangents of the stored moduli of level n start as D^T of those of
+// level n + 1 (a Horner form of the reference's per-block decimation
+// chains); the coefficient cotangents give (gz, gBr) per pixel; the
+// adjoint of the second wavelet adds into gMod[n]; its own slot n goes
+// through the modulus VJP into gz; the wavelet adjoint of gz plus D^T of
+// the next level's map cotangent is the map cotangent of level n
+// (map_cotangent, engine.rs:757-779).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <mutex>
+
+#include "engine.cuh"
+#include "scatcov.hpp"
+
+namespace stl {
+
+// ---- device memory accounting ----------------------------------------------
+static std::mutex g_mem_mu;
+static size_t g_live = 0, g_peak = 0;
+void DevMem::alloc(size_t n) {
+  release();
+  if (n == 0) return;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    throw std::runtime_error("device allocation of " + std::to_string(n) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes = n;
+  std::lock_guard<std::mutex> g(g_mem_mu);
+  g_live += n;
+  g_peak = std::max(g_peak, g_live);
+}
+void DevMem::release() {
+  if (p) {
+    cudaFree(p);
+    std::lock_guard<std::mutex> g(g_mem_mu);
+    g_live -= bytes;
+  }
+  p = nullptr;
+  bytes = 0;
+}
+size_t device_bytes_live() { std::lock_guard<std::mutex> g(g_mem_mu); return g_live; }
+size_t device_bytes_peak() { std::lock_guard<std::mutex> g(g_mem_mu); return g_peak; }
+void device_bytes_reset_peak() { std::lock_guard<std::mutex> g(g_mem_mu); g_peak = g_live; }
+
+// ---- plan (crates/stl-core/src/plan.rs:80-158, one channel) ---------------
+const char* family_name(int f) {
+  static const char* n[] = {"mean", "var", "S1", "S2", "S3", "S4"};
+  return (f >= 0 && f < 6) ? n[f] : "?";
+}
+
+std::vector<Coef> build_plan(int J, int L) {
+  std::vector<Coef> plan;
+  auto mk = [](int fam, int nat) { return Coef{fam, nat, 0, 0, -1, -1, -1, -1, -1, -1}; };
+  plan.push_back(mk(MEAN, 0));
+  plan.push_back(mk(VAR, 0));
+  for (int j3 = 0; j3 < J; ++j3) {
+    for (int fam : {S1, S2})
+      for (int l = 0; l < L; ++l) {
+        Coef c = mk(fam, j3);
+        c.j1 = j3; c.l1 = l;
+        plan.push_back(c);
+      }
+    for (int j2 = 0; j2 <= j3; ++j2) {
+      for (int l2 = 0; l2 < L; ++l2)
+        for (int l3 = 0; l3 < L; ++l3) {
+          Coef c = mk(S3, j3);
+          c.j1 = j2; c.j3 = j3; c.l1 = l2; c.l3 = l3;
+          plan.push_back(c);
+        }
+      for (int j1 = 0; j1 <= j2; ++j1)
+        for (int l1 = 0; l1 < L; ++l1)
+          for (int l2 = 0; l2 < L; ++l2)
+            for (int l3 = 0; l3 < L; ++l3) {
+              Coef c = mk(S4, j3);
+              c.j1 = j1; c.j2 = j2; c.j3 = j3; c.l1 = l1; c.l2 = l2; c.l3 = l3;
+              plan.push_back(c);
+            }
+    }
+  }
+  // already in native-level order (dg(j) = j, the stable sort of plan.rs:156)
+  return plan;
+}
+
+// f32-rounded wavelet kernel [G][2][P] (wavelet.rs:11-35, conv.rs:167-172)
+static std::vector<double> wavelet_kernel(int ksz, int G) {
+  int P = ksz * ksz;
+  std::vector<double> re, im;
+  for (int i = 0; i < ksz; ++i)
+    for (int j = 0; j < ksz; ++j) {
+      double x = (double)j - ((double)ksz - 1.0) / 2.0, y = (double)i - ((double)ksz - 1.0) / 2.0;
+      double mother = std::exp(-(x * x + y * y) / (2.0 * 1.0 * 1.0));
+      double angle = 0.5 * 3.141592653589793115997963468544185161590576171875 * x;
+      re.push_back(std::cos(angle) * mother);
+      im.push_back(std::sin(angle) * mother);
+    }
+  double sr = 0.0, si = 0.0;
+  for (int t = 0; t < P; ++t) { sr += re[t]; si += im[t]; }
+  double mr = sr / P, mi = si / P;
+  double l1 = 0.0;
+  for (int t = 0; t < P; ++t) {
+    re[t] -= mr; im[t] -= mi;
+    l1 += std::hypot(re[t], im[t]);
+  }
+  std::vector<double> out;
+  for (int g = 0; g < G; ++g) {
+    for (int t = 0; t < P; ++t) out.push_back((double)(float)(re[t] / l1));
+    for (int t = 0; t < P; ++t) out.push_back((double)(float)(im[t] / l1));
+  }
+  return out;
+}
+
+Engine::Engine(const Options& o) : opt_(o) {
+  if (o.nside < 1 || (o.nside & (o.nside - 1)) != 0) throw std::runtime_error("nside must be a power of two");
+  int order = 0;
+  while ((i64(1) << order) < o.nside) ++order;
+  if (o.J < 1 || o.J > order + 1) throw std::runtime_error("invalid number of scales");
+  if (o.B < 1) throw std::runtime_error("batch must be positive");
+  if (o.L != 4) throw std::runtime_error("the B200 engine is built for orientations = 4");
+  if (o.ksz != 5 && o.ksz != 3) throw std::runtime_error("kernel must be 3 or 5");
+  plan_ = build_plan(o.J, o.L);
+  levels_ = o.J;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+template <typename T>
+class EngineImpl final : public Engine {
+ public:
+  explicit EngineImpl(const Options& o) : Engine(o) {
+    int K0 = 0;
+    (void)K0;
+    // plan -> slot map of the product sums
+    map_.resize(plan_.size());
+    for (size_t i = 0; i < plan_.size(); ++i) map_[i] = locate(plan_[i]);
+  }
+
+  void prepare() override {
+    if (ready_) return;
+    auto t0 = std::chrono::steady_clock::now();
+    STL_CUDA(cudaSetDevice(opt_.device));
+    const int L = opt_.L, B = opt_.B;
+    DType dt = sizeof(T) == 8 ? DType::F64 : DType::F32;
+    std::vector<double> ker = wavelet_kernel(opt_.ksz, L);
+    conv_.resize(levels_);
+    dec_.resize(levels_ > 1 ? levels_ - 1 : 0);
+    for (int n = 0; n < levels_; ++n) {
+      ConvSpec cs;
+      cs.nside = opt_.nside >> n; cs.ksz = opt_.ksz; cs.G = L; cs.gauge = 0;
+      build_conv(cs, ker, dt, conv_[n], stream_);
+      operator_bytes_ += conv_[n].bytes();
+    }
+    for (int d = 0; d + 1 < levels_; ++d) {
+      DecSpec ds;
+      ds.nside = opt_.nside >> d;
+      build_dec(ds, dt, dec_[d], stream_);
+      operator_bytes_ += dec_[d].bytes();
+    }
+    // fields
+    X_.resize(levels_); Z_.resize(levels_); Mod_.resize(levels_); Br_.resize(levels_);
+    gMod_.resize(levels_); gX_.resize(levels_);
+    shapes_.resize(levels_);
+    size_t max_part = 0, max_gz = 0, max_gbr = 0;
+    for (int n = 0; n < levels_; ++n) {
+      i64 N = npix(n);
+      X_[n].alloc(sizeof(T) * B * N);
+      Z_[n].alloc(sizeof(T) * 2 * B * L * N);
+      Mod_[n].alloc(sizeof(T) * B * (n + 1) * L * N);
+      Br_[n].alloc(sizeof(T) * 2 * B * (n + 1) * L * L * N);
+      gMod_[n].alloc(sizeof(T) * B * (n + 1) * L * N);
+      gX_[n].alloc(sizeof(T) * B * N);
+      shapes_[n] = product_shape(n, L, B, N);
+      max_part = std::max(max_part, (size_t)B * L * shapes_[n].blocks * shapes_[n].slots);
+      max_gz = std::max(max_gz, (size_t)2 * B * L * N);
+      max_gbr = std::max(max_gbr, (size_t)2 * B * (n + 1) * L * L * N);
+      field_bytes_ += X_[n].bytes + Z_[n].bytes + Mod_[n].bytes + Br_[n].bytes + gMod_[n].bytes + gX_[n].bytes;
+    }
+    partials_.alloc(sizeof(double) * max_part);
+    size_t total_sums = 0;
+    sum_off_.resize(levels_);
+    for (int n = 0; n < levels_; ++n) {
+      sum_off_[n] = total_sums;
+      total_sums += (size_t)B * L * shapes_[n].slots;
+    }
+    sums_.alloc(sizeof(double) * total_sums);
+    h_sums_.resize(total_sums);
+    gZ_.alloc(sizeof(T) * max_gz);
+    gBr_.alloc(sizeof(T) * max_gbr);
+    size_t max_m = 0;
+    for (int n = 0; n < levels_; ++n) max_m = std::max(max_m, (size_t)2 * B * L * shapes_[n].K * shapes_[n].K);
+    M_.alloc(sizeof(T) * max_m);
+    s1c_.alloc(sizeof(T) * B * L);
+    mv_.alloc(sizeof(double) * 2 * B);
+    in_f64_.alloc(sizeof(double) * B * npix(0));
+    field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + M_.bytes + in_f64_.bytes;
+    STL_CUDA(cudaStreamSynchronize(stream_));
+    ready_ = true;
+    timers.build_s += ms_since(t0) / 1000.0;
+  }
+
+  void load_host(const double* x) override {
+    prepare();
+    size_t n = (size_t)opt_.B * npix(0);
+    STL_CUDA(cudaMemcpyAsync(in_f64_.p, x, n * 8, cudaMemcpyHostToDevice, stream_));
+    convert<double, T>(in_f64_.as<double>(), X_[0].as<T>(), (i64)n, stream_);
+    loaded_ = true;
+  }
+
+  void load_device(const void* x, bool f32) override {
+    prepare();
+    i64 n = (i64)opt_.B * npix(0);
+    if (f32) convert<float, T>(static_cast<const float*>(x), X_[0].as<T>(), n, stream_);
+    else convert<double, T>(static_cast<const double*>(x), X_[0].as<T>(), n, stream_);
+    loaded_ = true;
+  }
+
+  void save_input(std::vector<double>& x) override {
+    i64 n = (i64)opt_.B * npix(0);
+    convert<T, double>(X_[0].as<T>(), in_f64_.as<double>(), n, stream_);
+    x.resize(n);
+    STL_CUDA(cudaMemcpyAsync(x.data(), in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  void forward(bool moments, double* values, double* var) override {
+    if (!loaded_) throw std::runtime_error("forward before the maps were loaded");
+    auto t0 = std::chrono::steady_clock::now();
+    const int L = opt_.L, B = opt_.B;
+    cudaStream_t s = stream_;
+    for (int d = 0; d + 1 < levels_; ++d)
+      dec_apply<T>(dec_[d], false, X_[d].as<T>(), npix(d), X_[d + 1].as<T>(), npix(d + 1), B, 1, false, s);
+    for (int n = 0; n < levels_; ++n) {
+      i64 N = npix(n);
+      T* mod = Mod_[n].as<T>();
+      conv_forward<T>(conv_[n], X_[n].as<T>(), B, Z_[n].as<T>(), 2 * L * N, mod + (i64)n * L * N,
+                      (i64)(n + 1) * L * N, s);
+      if (n > 0)
+        dec_apply<T>(dec_[n - 1], false, Mod_[n - 1].as<T>(), (i64)n * L * npix(n - 1), mod, (i64)(n + 1) * L * N, B,
+                     n * L, false, s);
+      conv_forward<T>(conv_[n], mod, B * (n + 1) * L, Br_[n].as<T>(), 2 * L * N, nullptr, 0, s);
+      products_forward<T>(shapes_[n], Z_[n].as<T>(), Br_[n].as<T>(), X_[0].as<T>(), partials_.as<double>(),
+                          sums_.as<double>() + sum_off_[n], s);
+    }
+    STL_CUDA(cudaMemcpyAsync(h_sums_.data(), sums_.p, h_sums_.size() * 8, cudaMemcpyDeviceToHost, s));
+    STL_CUDA(cudaStreamSynchronize(s));
+    assemble(values, moments ? var : nullptr);
+    forward_done_ = true;
+    timers.forward_ms += ms_since(t0);
+    timers.forwards += 1;
+  }
+
+  void reverse_host(const double* cot, double* out) override {
+    reverse_impl(cot);
+    i64 n = (i64)opt_.B * npix(0);
+    convert<T, double>(gX_[0].as<T>(), in_f64_.as<double>(), n, stream_);
+    STL_CUDA(cudaMemcpyAsync(out, in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  void reverse_device(const double* cot, void* out, bool f32) override {
+    reverse_impl(cot);
+    i64 n = (i64)opt_.B * npix(0);
+    if (f32) convert<T, float>(gX_[0].as<T>(), static_cast<float*>(out), n, stream_);
+    else convert<T, double>(gX_[0].as<T>(), static_cast<double*>(out), n, stream_);
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+ private:
+  // where a plan coefficient's sums live: level, l3 row, slot; conj flag;
+  // kind 0 Gram entry, 1 S1 (sum |z|), 2 mean, 3 var
+  struct Loc {
+    int level, l3, kind, entry, conj;
+    double second_slot;  // unused
+  };
+  static int entry_of(int K, int i, int j) { return i * K - i * (i - 1) / 2 + (j - i); }
+
+  Loc locate(const Coef& c) const {
+    const int L = opt_.L;
+    int n = c.native;
+    int K = (n + 1) * L + 1, z = K - 1;
+    Loc l{n, 0, 0, 0, 0, 0};
+    switch (c.family) {
+      case MEAN: l.kind = 2; break;
+      case VAR: l.kind = 3; break;
+      case S1: l.kind = 1; l.l3 = c.l1; break;
+      case S2: l.l3 = c.l1; l.entry = entry_of(K, z, z); break;
+      case S3: l.l3 = c.l3; l.entry = entry_of(K, c.j1 * L + c.l1, z); break;
+      case S4: {
+        int i = c.j1 * L + c.l1, j = c.j2 * L + c.l2;
+        l.l3 = c.l3;
+        if (i <= j) l.entry = entry_of(K, i, j);
+        else { l.entry = entry_of(K, j, i); l.conj = 1; }
+        break;
+      }
+    }
+    return l;
+  }
+
+  void assemble(double* values, double* var) const {
+    const int L = opt_.L, B = opt_.B;
+    const i64 np = (i64)plan_.size();
+    for (int b = 0; b < B; ++b)
+      for (i64 i = 0; i < np; ++i) {
+        const Coef& c = plan_[i];
+        const Loc& l = map_[i];
+        const ProductShape& sh = shapes_[l.level];
+        int K = sh.K, E = K * (K + 1) / 2;
+        const double* row = h_sums_.data() + sum_off_[l.level] + ((size_t)b * L + l.l3) * sh.slots;
+        double N = (double)npix(l.level);
+        double re = 0, im = 0, second = 0;
+        switch (l.kind) {
+          case 0:
+            re = row[2 * l.entry]; im = row[2 * l.entry + 1];
+            if (l.conj) im = -im;
+            second = row[2 * E + l.entry];
+            if (c.family == S2) { im = 0.0; second = row[3 * E + 1]; }
+            break;
+          case 1: re = row[3 * E]; second = row[2 * entry_of(K, K - 1, K - 1)]; break;
+          case 2: re = row[3 * E + 2]; second = row[3 * E + 3]; break;
+          case 3: re = row[3 * E + 3]; second = row[3 * E + 4]; break;
+        }
+        double vr = re / N, vi = im / N;
+        values[2 * (b * np + i)] = vr;
+        values[2 * (b * np + i) + 1] = vi;
+        if (var) var[b * np + i] = std::max(second / N - (vr * vr + vi * vi), 0.0);
+      }
+  }
+
+  void reverse_impl(const double* cot) {
+    if (!forward_done_) throw std::runtime_error("vjp before forward");
+    auto t0 = std::chrono::steady_clock::now();
+    const int L = opt_.L, B = opt_.B;
+    const i64 np = (i64)plan_.size();
+    cudaStream_t s = stream_;
+    // host: per-level cotangent matrices, auto-S1 scales, mean/var scales
+    std::vector<std::vector<std::complex<double>>> M(levels_);
+    std::vector<std::vector<double>> s1(levels_, std::vector<double>((size_t)B * L, 0.0));
+    std::vector<double> mv((size_t)2 * B, 0.0);
+    for (int n = 0; n < levels_; ++n) M[n].assign((size_t)B * L * shapes_[n].K * shapes_[n].K, 0.0);
+    for (int b = 0; b < B; ++b)
+      for (i64 i = 0; i < np; ++i) {
+        std::complex<double> g(cot[2 * (b * np + i)], cot[2 * (b * np + i) + 1]);
+        if (g == std::complex<double>(0.0, 0.0)) continue;
+        const Coef& c = plan_[i];
+        int n = c.native, K = shapes_[n].K, z = K - 1;
+        double N = (double)npix(n);
+        auto at = [&](int l3, int r, int q) -> std::complex<double>& {
+          return M[n][(((size_t)b * L + l3) * K + r) * K + q];
+        };
+        switch (c.family) {
+          case MEAN: mv[2 * b] += g.real() / N; break;
+          case VAR: mv[2 * b + 1] += 2.0 * g.real() / N; break;
+          case S1: s1[n][(size_t)b * L + c.l1] += g.real() / N; break;
+          case S2: at(c.l1, z, z) += 2.0 * g.real() / N; break;
+          case S3: {
+            int r = c.j1 * L + c.l1;
+            at(c.l3, r, z) += g / N;
+            at(c.l3, z, r) += std::conj(g) / N;
+            break;
+          }
+          case S4: {
+            int r = c.j1 * L + c.l1, q = c.j2 * L + c.l2;
+            at(c.l3, r, q) += g / N;
+            at(c.l3, q, r) += std::conj(g) / N;
+            break;
+          }
+        }
+      }
+    for (int n = levels_ - 1; n >= 0; --n) {
+      i64 N = npix(n);
+      const ProductShape& sh = shapes_[n];
+      T* gmod = gMod_[n].as<T>();
+      if (n + 1 < levels_)
+        dec_apply<T>(dec_[n], true, gMod_[n + 1].as<T>(), (i64)(n + 2) * L * npix(n + 1), gmod, (i64)(n + 1) * L * N, B,
+                     (n + 1) * L, false, s);
+      else
+        STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
+      // cotangent matrices in the field precision
+      h_M_.resize(2 * M[n].size());
+      for (size_t q = 0; q < M[n].size(); ++q) { h_M_[2 * q] = (T)M[n][q].real(); h_M_[2 * q + 1] = (T)M[n][q].imag(); }
+      h_s1_.resize(s1[n].size());
+      for (size_t q = 0; q < s1[n].size(); ++q) h_s1_[q] = (T)s1[n][q];
+      STL_CUDA(cudaMemcpyAsync(M_.p, h_M_.data(), h_M_.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+      STL_CUDA(cudaMemcpyAsync(s1c_.p, h_s1_.data(), h_s1_.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+      products_reverse<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), M_.as<T>(), s1c_.as<T>(), gZ_.as<T>(), gBr_.as<T>(), s);
+      conv_adjoint<T>(conv_[n], gBr_.as<T>(), 2 * L * N, B * (n + 1) * L, gmod, true, s);
+      modulus_vjp_add<T>(Z_[n].as<T>(), gmod + (i64)n * L * N, (i64)(n + 1) * L * N, gZ_.as<T>(), B, (i64)L * N, s);
+      conv_adjoint<T>(conv_[n], gZ_.as<T>(), 2 * L * N, B, gX_[n].as<T>(), false, s);
+      if (n + 1 < levels_)
+        dec_apply<T>(dec_[n], true, gX_[n + 1].as<T>(), npix(n + 1), gX_[n].as<T>(), N, B, 1, true, s);
+      // the host staging buffers are reused next level: wait for the copies
+      STL_CUDA(cudaStreamSynchronize(s));
+    }
+    STL_CUDA(cudaMemcpyAsync(mv_.p, mv.data(), mv.size() * 8, cudaMemcpyHostToDevice, s));
+    mean_var_grad<T>(X_[0].as<T>(), mv_.as<double>(), B, npix(0), gX_[0].as<T>(), s);
+    STL_CUDA(cudaStreamSynchronize(s));
+    timers.reverse_ms += ms_since(t0);
+    timers.reverses += 1;
+  }
+
+  bool ready_ = false, loaded_ = false, forward_done_ = false;
+  std::vector<ConvOp> conv_;
+  std::vector<DecOp> dec_;
+  std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;
+  std::vector<ProductShape> shapes_;
+  std::vector<size_t> sum_off_;
+  DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_;
+  std::vector<double> h_sums_;
+  std::vector<T> h_M_, h_s1_;
+  std::vector<Loc> map_;
+};
+
+std::unique_ptr<Engine> Engine::create(const Options& o) {
+  if (o.fp32) return std::unique_ptr<Engine>(new EngineImpl<float>(o));
+  return std::unique_ptr<Engine>(new EngineImpl<double>(o));
+}
+
+}  // namespace stl

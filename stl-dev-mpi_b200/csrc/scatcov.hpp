@@ -1,0 +1,89 @@
+// Host interface of the B200 ScatCov engine (one GPU, one handle).
+//
+// The engine mirrors the reference's `Evaluator` contract
+// (crates/stl-core/src/engine.rs:254-271): forward(x) -> statistics of a
+// batch of maps (optionally with the spatial variance of every
+// coefficient's terms), then gradient(cotangent) -> the level-0 map
+// cotangent of Re sum(conj(cotangent) * values).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace stl {
+
+typedef int64_t i64;
+enum class DType;
+
+// crates/stl-core/src/plan.rs:4-68; unused indices are -1
+enum Family { MEAN = 0, VAR = 1, S1 = 2, S2 = 3, S3 = 4, S4 = 5 };
+struct Coef {
+  int family, native, c1, c2, j1, j2, j3, l1, l2, l3;
+};
+const char* family_name(int f);
+// build_plan of one channel, dg(j) = j, all families (plan.rs:80-158)
+std::vector<Coef> build_plan(int J, int L);
+
+struct Options {
+  i64 nside = 128;
+  int J = 7;
+  int B = 1;
+  int L = 4;
+  int ksz = 5;
+  bool fp32 = false;  // compute precision of the fields (sums are FP64 in both)
+  int device = 0;
+};
+
+struct Timers {
+  double build_s = 0, forward_ms = 0, reverse_ms = 0;
+  int forwards = 0, reverses = 0;
+};
+
+class Engine {
+ public:
+  static std::unique_ptr<Engine> create(const Options& o);
+  virtual ~Engine() = default;
+
+  const Options& options() const { return opt_; }
+  const std::vector<Coef>& plan() const { return plan_; }
+  int levels() const { return levels_; }
+  i64 npix(int d) const { return 12 * (opt_.nside >> d) * (opt_.nside >> d); }
+  bool fp32() const { return opt_.fp32; }
+
+  void set_stream(cudaStream_t s) { stream_ = s; }
+  cudaStream_t stream() const { return stream_; }
+
+  // Builds the device operators of every level (first use does it too).
+  virtual void prepare() = 0;
+  // Loads maps [B][N_0] from host (f64) or device memory (f64 or f32).
+  virtual void load_host(const double* x) = 0;
+  virtual void load_device(const void* x, bool f32) = 0;
+  // Forward sweep on the loaded maps: values [B][np] complex (interleaved),
+  // var [B][np] when moments.  Host outputs; the call synchronises.
+  virtual void forward(bool moments, double* values, double* var) = 0;
+  // After forward: map cotangent of Re sum(conj(cot) * values), cot [B][np]
+  // complex interleaved (host).  Output to host f64 or device f64/f32.
+  virtual void reverse_host(const double* cot, double* out) = 0;
+  virtual void reverse_device(const double* cot, void* out, bool f32) = 0;
+  // Device level-0 maps of the last load (T), for checkpoints.
+  virtual void save_input(std::vector<double>& x) = 0;
+
+  size_t operator_bytes() const { return operator_bytes_; }
+  size_t field_bytes() const { return field_bytes_; }
+  Timers timers;
+
+ protected:
+  explicit Engine(const Options& o);
+  Options opt_;
+  std::vector<Coef> plan_;
+  int levels_ = 1;
+  cudaStream_t stream_ = nullptr;
+  size_t operator_bytes_ = 0, field_bytes_ = 0;
+};
+
+}  // namespace stl

@@ -1,0 +1,352 @@
+"""Python host side of the B200 ScatCov engine (libstl_b200.so).
+
+``NativeEngine`` mirrors the reference's binding of the same name
+(jmdelouis/STL-Dev-MPI, python/stl_ensemble/stl_port/native.py:153-490):
+same constructor keywords, the plan from ``info()["plan"]``, ``forward``
+returning ``(values, variances)``, ``vjp`` of ``Re sum(conj(cot) values)``,
+the (generation, member, objective) identity of a forward state,
+``checkpoint`` / ``restore`` and ``native_pixels``.  ``backend`` must be
+"gpu": this library has no CPU engine, and fails loudly when the library
+or the device is missing.
+
+Additions for PyTorch: ``forward_tensor`` / ``vjp_tensor`` on CUDA tensors
+(float32 or float64, no host copy of the maps) and ``scattering(engine, x)``,
+a ``torch.autograd.Function`` over them; torch hands the backward of a
+complex output the cotangent dL/dRe + i dL/dIm, the engine's convention.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import itertools
+import json
+import os
+import threading
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "libstl_b200.so"
+
+_D = C.POINTER(C.c_double)
+_SIZE = C.POINTER(C.c_size_t)
+_VOID = C.c_void_p
+_CALLBACK = C.CFUNCTYPE(C.c_double, _D, C.c_size_t, _D, _VOID)
+_lib = None
+_lock = threading.Lock()
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("STL_B200_LIBRARY", LIBRARY))
+
+
+def lib():
+    """The engine library with its C signatures (include/stl_b200.h)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = library_path()
+        if not path.is_file():
+            raise RuntimeError(f"the B200 engine library is missing: {path} (build it with "
+                               f"`make -C {HERE}` or __graft_entry__.build()); there is no fallback engine")
+        l = C.CDLL(str(path))
+        u64, sz, b = C.c_uint64, C.c_size_t, C.c_bool
+        sig = {
+            "stlp_last_error": ([], C.c_char_p),
+            "stlp_string_free": ([_VOID], None),
+            "stlp_new": ([C.c_char_p], _VOID),
+            "stlp_free": ([_VOID], None),
+            "stlp_info": ([_VOID], _VOID),
+            "stlp_prepare": ([_VOID], C.c_int),
+            "stlp_set_stream": ([_VOID, u64], C.c_int),
+            "stlp_set_masks": ([_VOID, _D, sz], C.c_int),
+            "stlp_native_pixels": ([_VOID, _SIZE], C.c_int),
+            "stlp_forward": ([_VOID, _D, sz, u64, u64, u64, b, _D, _D], C.c_int),
+            "stlp_vjp": ([_VOID, _D, sz, u64, u64, u64, _D], C.c_int),
+            "stlp_forward_device": ([_VOID, u64, sz, C.c_int, u64, u64, u64, b, _D, _D], C.c_int),
+            "stlp_vjp_device": ([_VOID, _D, sz, u64, u64, u64, u64, C.c_int], C.c_int),
+            "stlp_checkpoint": ([_VOID], _VOID),
+            "stlp_checkpoint_free": ([_VOID], None),
+            "stlp_checkpoint_bytes": ([_VOID], sz),
+            "stlp_restore": ([_VOID, _VOID, u64, u64, u64], C.c_int),
+            "stlp_forward_levels": ([_VOID, _D, sz, _D], C.c_int),
+            "stlp_lbfgs": ([_D, sz, C.c_char_p, _CALLBACK, _VOID], C.c_int64),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(l, name)
+            f.argtypes, f.restype = args, res
+        _lib = l
+        return l
+
+
+def _error():
+    return RuntimeError(lib().stlp_last_error().decode("utf-8", errors="replace"))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_D)
+
+
+def _key(generation, member, objective):
+    """Identity of a forward state, as native.py:122-129."""
+    for name, v in (("generation", generation), ("member", member)):
+        if isinstance(v, bool) or not isinstance(v, (int, np.integer)) or v < 0 or v >= 2 ** 64:
+            raise ValueError(f"{name} must be an unsigned 64-bit integer")
+    if not isinstance(objective, str) or not objective:
+        raise ValueError("objective must be a nonempty name")
+    return (int(generation), int(member), int.from_bytes(hashlib.sha256(objective.encode()).digest()[:8], "little"))
+
+
+class Snapshot:
+    """Saved forward state (the maps of the forward); ``close()`` frees it."""
+
+    def __init__(self, handle, key, owner):
+        self._handle, self.key, self.owner = handle, key, owner
+
+    def close(self):
+        if self._handle:
+            lib().stlp_checkpoint_free(self._handle)
+            self._handle = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *_):
+        self.close()
+
+
+class NativeEngine:
+    """One persistent B200 workspace with an immutable plan, resolution and batch.
+
+    ``dtype`` is the precision of the fields ("float64": everything FP64;
+    "float32": convolutions, moduli and products in FP32, the pixel sums in
+    FP64).  Values are complex128 ``[batch, ncoeff]`` in the order of
+    ``plan``.
+    """
+
+    def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
+                 prepare=False, **unused):
+        if backend != "gpu":
+            raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
+        for v in (nside, j, batch, kernel, orientations):
+            if isinstance(v, bool) or int(v) != v or int(v) <= 0:
+                raise ValueError("engine sizes must be positive integers")
+        self.nside, self.j, self.batch = int(nside), int(j), int(batch)
+        self.npix = 12 * self.nside ** 2
+        self.dtype = dtype
+        self.device = int(device)
+        self.config = dict(nside=self.nside, j=self.j, batch=self.batch, backend="gpu", kernel=int(kernel),
+                           orientations=int(orientations), device=self.device, dtype=dtype)
+        self._lib = lib()
+        self._handle = self._lib.stlp_new(json.dumps(self.config).encode())
+        if not self._handle:
+            raise _error()
+        self._mutex = threading.RLock()
+        info = self.info()
+        self.plan = info["plan"]
+        self.levels = info["levels"]
+        self.ncoeff = len(self.plan)
+        self._current_key = None
+        self._stream = None
+        if prepare:
+            self.prepare()
+
+    # -- handle plumbing ----------------------------------------------------
+    def _open(self):
+        if not self._handle:
+            raise RuntimeError("engine is closed")
+
+    def prepare(self):
+        """Builds the device operators now (otherwise at the first forward)."""
+        with self._mutex:
+            self._open()
+            if self._lib.stlp_prepare(self._handle):
+                raise _error()
+
+    def info(self):
+        with self._mutex:
+            self._open()
+            p = self._lib.stlp_info(self._handle)
+            if not p:
+                raise _error()
+            try:
+                return json.loads(C.string_at(p))
+            finally:
+                self._lib.stlp_string_free(p)
+
+    def native_pixels(self):
+        with self._mutex:
+            self._open()
+            out = np.empty(self.ncoeff, dtype=np.uintp)
+            if self._lib.stlp_native_pixels(self._handle, out.ctypes.data_as(_SIZE)):
+                raise _error()
+            return out.astype(np.int64)
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.stlp_free(self._handle)
+            self._handle = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *_):
+        self.close()
+
+    # -- host arrays (the reference's interface) ------------------------------
+    def forward(self, maps, generation=0, member=0, objective="gaussian", moments=False):
+        """Statistics of maps ``[batch, npix]`` (``[npix]`` when batch = 1), f64 NESTED."""
+        with self._mutex:
+            self._open()
+            key = _key(generation, member, objective)
+            x = np.ascontiguousarray(maps, dtype=np.float64)
+            if x.shape == (self.npix,) and self.batch == 1:
+                x = x[None]
+            if x.shape != (self.batch, self.npix):
+                raise ValueError(f"expected maps {(self.batch, self.npix)}, got {x.shape}")
+            if not np.isfinite(x).all():
+                raise ValueError("input map contains non-finite values")
+            values = np.empty((self.batch, self.ncoeff), dtype=np.complex128)
+            var = np.empty((self.batch, self.ncoeff) if moments else (self.batch, 0))
+            self._current_key = None
+            if self._lib.stlp_forward(self._handle, _ptr(x), x.size, *key, bool(moments),
+                                      _ptr(values.view(np.float64)), _ptr(var)):
+                raise _error()
+            self._current_key = key
+            return values, var
+
+    def _cotangent(self, cotangents):
+        c = np.ascontiguousarray(cotangents, dtype=np.complex128)
+        if c.shape == (self.ncoeff,) and self.batch == 1:
+            c = c[None]
+        if c.shape != (self.batch, self.ncoeff):
+            raise ValueError(f"expected cotangents {(self.batch, self.ncoeff)}, got {c.shape}")
+        if not np.isfinite(c).all():
+            raise ValueError("non-finite coefficient cotangent")
+        return c
+
+    def vjp(self, cotangents, generation=0, member=0, objective="gaussian"):
+        """Gradient ``[batch, npix]`` of ``Re sum(conj(cotangents) * values)``."""
+        with self._mutex:
+            self._open()
+            key = _key(generation, member, objective)
+            if key != self._current_key:
+                raise RuntimeError("stale/wrong-member/objective forward state")
+            c = self._cotangent(cotangents)
+            grad = np.empty((self.batch, self.npix))
+            if self._lib.stlp_vjp(self._handle, _ptr(c.view(np.float64)), c.size, *key, _ptr(grad)):
+                raise _error()
+            return grad
+
+    def checkpoint(self):
+        with self._mutex:
+            self._open()
+            p = self._lib.stlp_checkpoint(self._handle)
+            if not p:
+                raise _error()
+            return Snapshot(p, self._current_key, self._handle)
+
+    def restore(self, snapshot, generation=0, member=0, objective="gaussian"):
+        with self._mutex:
+            self._open()
+            key = _key(generation, member, objective)
+            if not isinstance(snapshot, Snapshot) or not snapshot._handle:
+                raise ValueError("checkpoint is closed or invalid")
+            if snapshot.key != key:
+                raise RuntimeError("stale/wrong-member/objective checkpoint state")
+            if snapshot.owner != self._handle:
+                raise ValueError("checkpoint engine/plan owner mismatch")
+            if self._lib.stlp_restore(self._handle, snapshot._handle, *key):
+                raise _error()
+            self._current_key = key
+
+    # -- CUDA tensors -----------------------------------------------------------
+    def _bind_stream(self, torch):
+        s = torch.cuda.current_stream(torch.device("cuda", self.device)).cuda_stream
+        if s != self._stream:
+            if self._lib.stlp_set_stream(self._handle, s):
+                raise _error()
+            self._stream = s
+
+    def forward_tensor(self, x, generation=0, member=0, objective="gaussian", moments=False):
+        """Statistics of a CUDA tensor ``[batch, npix]`` (float32 or float64), no host copy
+        of the maps; runs on torch's current stream.  Returns numpy (values, var)."""
+        import torch
+        with self._mutex:
+            self._open()
+            key = _key(generation, member, objective)
+            if not x.is_cuda or x.dtype not in (torch.float32, torch.float64):
+                raise ValueError("forward_tensor needs a float32/float64 CUDA tensor")
+            x = x.detach().reshape(self.batch, self.npix).contiguous()
+            self._bind_stream(torch)
+            values = np.empty((self.batch, self.ncoeff), dtype=np.complex128)
+            var = np.empty((self.batch, self.ncoeff) if moments else (self.batch, 0))
+            self._current_key = None
+            if self._lib.stlp_forward_device(self._handle, x.data_ptr(), x.numel(), int(x.dtype == torch.float32),
+                                             *key, bool(moments), _ptr(values.view(np.float64)), _ptr(var)):
+                raise _error()
+            self._current_key = key
+            return values, var
+
+    def vjp_tensor(self, cotangents, out, generation=0, member=0, objective="gaussian"):
+        """Writes the gradient into the CUDA tensor ``out`` ``[batch, npix]`` (float32/64)."""
+        import torch
+        with self._mutex:
+            self._open()
+            key = _key(generation, member, objective)
+            if key != self._current_key:
+                raise RuntimeError("stale/wrong-member/objective forward state")
+            if not (out.is_cuda and out.is_contiguous() and out.numel() == self.batch * self.npix
+                    and out.dtype in (torch.float32, torch.float64)):
+                raise ValueError("out must be a contiguous float32/float64 CUDA tensor [batch, npix]")
+            c = self._cotangent(cotangents)
+            self._bind_stream(torch)
+            if self._lib.stlp_vjp_device(self._handle, _ptr(c.view(np.float64)), c.size, *key, out.data_ptr(),
+                                         int(out.dtype == torch.float32)):
+                raise _error()
+            return out
+
+
+_generation = itertools.count(1)
+
+
+def _function():
+    import torch
+
+    class ScatCov(torch.autograd.Function):
+        """Statistics of a CUDA batch of maps as a differentiable torch op:
+        x [batch, npix] -> complex128 [batch, ncoeff] on x's device."""
+
+        @staticmethod
+        def forward(ctx, x, engine):
+            g = next(_generation)
+            values, _ = engine.forward_tensor(x, generation=g)
+            ctx.engine, ctx.generation = engine, g
+            ctx.shape, ctx.dtype = x.shape, x.dtype
+            return torch.from_numpy(values).to(x.device)
+
+        @staticmethod
+        def backward(ctx, gy):
+            out = torch.empty(ctx.shape, dtype=ctx.dtype, device=gy.device)
+            ctx.engine.vjp_tensor(gy.detach().resolve_conj().cpu().numpy(), out, generation=ctx.generation)
+            return out, None
+
+    return ScatCov
+
+
+_ScatCov = None
+
+
+def scattering(engine, x):
+    """Differentiable statistics of the CUDA tensor x [batch, npix] (one forward state
+    per engine: run backward before the next forward of the same engine)."""
+    global _ScatCov
+    if _ScatCov is None:
+        _ScatCov = _function()
+    return _ScatCov.apply(x, engine)

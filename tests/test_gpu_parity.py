@@ -1,0 +1,146 @@
+"""Parity of the CUDA engine with the FP64 oracle and the reference's fixtures.
+
+FP64 mode must match the reference to its own tolerances
+(crates/stl-core/tests/stats.rs:175-190: values 1e-11 abs + 1e-10 rel, map
+cotangents 1e-10 abs + 1e-9 rel).  FP32 mode (FP32 fields, FP64 sums) is
+checked against the FP64 oracle with |a - b| <= atol + rtol |b|, rtol 1e-6
+and atol 1e-6 times the largest |S| of the coefficient's family and level
+(near-zero S3/S4 cross terms are judged on the scale of their family).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import cases, close_ratio
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def stl():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a CUDA device is required")
+    import stl_b200
+    return stl_b200
+
+
+def lognormal(rng, shape, sigma=1.0):
+    g = rng.standard_normal(shape)
+    return np.exp(sigma * g - 0.5 * sigma * sigma)
+
+
+def family_scale(plan, values):
+    """max |S| per (family, native level, batch) broadcast to every coefficient."""
+    fam = np.array([c["family"] for c in plan])
+    lev = np.array([c["native_dg"] for c in plan])
+    scale = np.zeros(values.shape)
+    for f in set(fam):
+        for n in set(lev):
+            sel = (fam == f) & (lev == n)
+            if sel.any():
+                scale[..., sel] = np.max(np.abs(values[..., sel]), axis=-1, keepdims=True)
+    return scale
+
+
+def test_config1_fixture_fp64(stl):
+    """nside 16, J 3, L 4: the reference's golden statistics and gradient."""
+    case = next(c for c in cases("stats", "stats") if c.name == "stats_n16_J3_L4_k5_C1_B1_full_b256")
+    e = stl.NativeEngine(16, 3, dtype="float64")
+    x = case.npy("map0").reshape(1, -1)
+    values, _ = e.forward(x)
+    ref = case.complex("values").reshape(values.shape)
+    assert close_ratio(values.real, ref.real, 1e-11, 1e-10) <= 1.0
+    assert close_ratio(values.imag, ref.imag, 1e-11, 1e-10) <= 1.0
+    cot = case.complex("gradient").reshape(values.shape)
+    grad = e.vjp(cot)
+    assert close_ratio(grad, case.npy("band_gradient0"), 1e-10, 1e-9) <= 1.0
+
+
+@pytest.mark.parametrize("nside,J,B", [(16, 3, 2), (32, 4, 1), (64, 5, 2), (8, 4, 1)])
+def test_fp64_matches_oracle(stl, nside, J, B):
+    rng = np.random.default_rng(nside + J)
+    x = lognormal(rng, (B, 12 * nside * nside))
+    o = O.OracleEngine(nside, J, batch=B)
+    ref, ref_var = o.forward(x, moments=True)
+    e = stl.NativeEngine(nside, J, batch=B, dtype="float64")
+    values, var = e.forward(x, moments=True)
+    assert close_ratio(values.real, ref.real, 1e-11, 1e-10) <= 1.0
+    assert close_ratio(values.imag, ref.imag, 1e-11, 1e-10) <= 1.0
+    assert close_ratio(var, ref_var, 1e-11, 1e-9) <= 1.0
+    cot = rng.standard_normal(values.shape) + 1j * rng.standard_normal(values.shape)
+    g_ref = o.vjp(cot)
+    grad = e.vjp(cot)
+    assert close_ratio(grad, g_ref, 1e-10 * np.max(np.abs(g_ref)), 1e-9) <= 1.0
+
+
+def test_fp32_within_1e6_of_fp64_oracle(stl):
+    nside, J, B = 64, 5, 2
+    rng = np.random.default_rng(7)
+    x = lognormal(rng, (B, 12 * nside * nside))
+    o = O.OracleEngine(nside, J, batch=B)
+    ref = o.forward(x)
+    e = stl.NativeEngine(nside, J, batch=B, dtype="float32")
+    values, _ = e.forward(x.astype(np.float32).astype(np.float64))
+    scale = family_scale(e.plan, ref)
+    for part in (np.real, np.imag):
+        err = np.abs(part(values) - part(ref))
+        ratio = np.max(err / (1e-6 * scale + 1e-6 * np.abs(part(ref))))
+        rel = np.max(err / np.maximum(np.abs(part(ref)), 1e-300)[...])
+        print(f"fp32 vs oracle: worst ratio to tolerance {ratio:.3f}, plain max relative error {rel:.2e}")
+        assert ratio <= 1.0
+    cot = rng.standard_normal(values.shape) + 1j * rng.standard_normal(values.shape)
+    g_ref = o.vjp(cot)
+    grad = e.vjp(cot)
+    assert np.max(np.abs(grad - g_ref)) <= 1e-5 * np.max(np.abs(g_ref))
+
+
+def test_deterministic_and_restorable(stl):
+    nside, J = 32, 4
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((1, 12 * nside * nside))
+    e = stl.NativeEngine(nside, J, dtype="float32")
+    v1, _ = e.forward(x, generation=1)
+    cot = rng.standard_normal(v1.shape) + 1j * rng.standard_normal(v1.shape)
+    g1 = e.vjp(cot, generation=1)
+    snap = e.checkpoint()
+    v2, _ = e.forward(x * 2.0, generation=2)
+    e.restore(snap, generation=1)
+    g2 = e.vjp(cot, generation=1)
+    assert np.array_equal(g1, g2)
+    v3, _ = e.forward(x, generation=3)
+    assert np.array_equal(v1, v3)
+    with pytest.raises(RuntimeError, match="stale"):
+        e.vjp(cot, generation=1)
+
+
+def test_torch_function_gradient(stl):
+    import torch
+    nside, J, B = 32, 4, 2
+    e = stl.NativeEngine(nside, J, batch=B, dtype="float64")
+    rng = np.random.default_rng(11)
+    x_np = lognormal(rng, (B, 12 * nside * nside))
+    target = rng.standard_normal((B, e.ncoeff)) + 1j * rng.standard_normal((B, e.ncoeff))
+    x = torch.tensor(x_np, device="cuda", requires_grad=True)
+    s = stl.scattering(e, x)
+    loss = (s - torch.tensor(target, device="cuda")).abs().pow(2).sum()
+    loss.backward()
+    o = O.OracleEngine(nside, J, batch=B)
+    vals = o.forward(x_np)
+    g_ref = o.vjp(2.0 * (vals - target))
+    assert close_ratio(x.grad.cpu().numpy(), g_ref, 1e-10 * np.max(np.abs(g_ref)), 1e-9) <= 1.0
+
+
+def test_float32_tensor_path(stl):
+    import torch
+    nside, J = 32, 4
+    e = stl.NativeEngine(nside, J, dtype="float32")
+    rng = np.random.default_rng(12)
+    x = torch.tensor(rng.standard_normal((1, 12 * nside * nside)), device="cuda", dtype=torch.float32)
+    v_dev, _ = e.forward_tensor(x, generation=5)
+    v_host, _ = e.forward(x.cpu().double().numpy(), generation=6)
+    assert np.array_equal(v_dev, v_host)
+    cot = np.ones_like(v_host)
+    out = torch.empty_like(x)
+    e.vjp_tensor(cot, out, generation=6)
+    assert np.array_equal(out.cpu().double().numpy(), e.vjp(cot, generation=6).astype(np.float32))
