@@ -1,0 +1,309 @@
+"""Benchmark of the B200 ScatCov engine: S1-S4 forward + VJP evaluations per second.
+
+Workload (one step): forward + exact VJP of the full ScatCov statistics
+(mean, var, S1..S4; L = 4, J = 9, 11 354 coefficients) of a batch of B = 4
+synthetic lognormal HEALPix maps at nside 1024 (12 582 912 NESTED pixels,
+x = exp(g - 1/2), g ~ N(0, 1), seeds 0..3), in FP32 fields with FP64 sums;
+the cotangent is that of the loss sum |S - S_t|^2 (S_t: the map of seed 100),
+computed on the host from the step's values.  One evaluation = one map.
+The same step is timed for one FP64 map (the plain FP64 path) and through
+the reference-facing host-buffer API (stlp_forward / stlp_vjp: f64 maps in
+and gradients out over PCIe).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) every rank evaluates its own batch (independent
+replicas, no collective in the path); the time is the max over ranks.
+``--impl reference`` times the CPU oracle (the FP64 restatement of the
+reference's CPU engine) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "stl-dev-mpi_b200"))
+
+METRIC = "S1–S4 fwd+VJP evals/s, nside 1024 J=9: FP32-batched vs FP64 plain, err≤1e-6"
+UNIT = "evals/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--nside", type=int, default=1024)
+    p.add_argument("--J", type=int, default=9)
+    p.add_argument("--batch", type=int, default=4)
+    p.add_argument("--skip-fp64", action="store_true")
+    p.add_argument("--skip-cpu", action="store_true")
+    return p.parse_args()
+
+
+def lognormal(seed, npix, sigma=1.0):
+    g = np.random.default_rng(seed).standard_normal(npix)
+    return np.exp(sigma * g - 0.5 * sigma * sigma)
+
+
+def sum_pixels(nside, J):
+    return sum(12 * (nside >> n) ** 2 for n in range(J))
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during a timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *_):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "samples": len(rows),
+                "reasons": reasons}
+
+
+def time_steps(torch, step, steps, warmup, dist):
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def cpu_baseline(nside=256, J=7):
+    """The FP64 CPU oracle (the restatement of the reference's CPU engine) on all
+    host cores: one forward + VJP of one lognormal map at (nside, J), scaled to
+    nside 1024, J = 9 by the pixel count of the pyramid."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    e = oracle.OracleEngine(nside, J, batch=1, cache_gb=0.0)
+    x = lognormal(0, 12 * nside * nside)
+    t0 = time.perf_counter()
+    v = e.forward(x)
+    e.vjp(2.0 * v)
+    dt = time.perf_counter() - t0
+    scale = sum_pixels(1024, 9) / sum_pixels(nside, J)
+    return {"value": 1.0 / (dt * scale), "unit": UNIT, "cores": oracle.threads(), "kind": "port",
+            "sample": f"one FP64 forward+VJP of one lognormal map at nside {nside}, J={J} ({dt:.2f} s), "
+                      f"scaled x{scale:.2f} by the pyramid pixel count to nside 1024, J=9"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    samples = []
+    warm = min(args.warmup, 1)
+    for i in range(warm + args.steps):
+        b = cpu_baseline(128, 6)
+        if i >= warm:
+            samples.append(1.0 / b["value"])
+    mean_s = sum(samples) / len(samples)
+    value = 1.0 / mean_s
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "scatcov fwd+vjp nside1024 J9 L4, 1 FP64 map per step (CPU oracle sample)",
+                       "nside": 1024, "J": 9, "L": 4, "batch": 1},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.threads(), "kind": "port",
+                             "sample": b["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    import stl_b200
+
+    nside, J, B = args.nside, args.J, args.batch
+    npix = 12 * nside * nside
+    dev = torch.device("cuda", local if world > 1 else 0)
+
+    # -- FP32 batched: the headline -------------------------------------------
+    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True)
+    seeds = [rank * B + s for s in range(B)]
+    x_host = np.stack([lognormal(s, npix) for s in seeds])
+    x = torch.tensor(x_host, dtype=torch.float32, device=dev)
+    # target statistics S_t: the FP32 engine on the map of seed 100 (replicated over the batch)
+    xt = torch.tensor(np.stack([lognormal(100, npix)] * B), dtype=torch.float32, device=dev)
+    target, _ = eng.forward_tensor(xt, generation=1)
+    grad = torch.empty_like(x)
+    gen = iter(range(10, 10 ** 9))
+
+    def step32():
+        g = next(gen)
+        values, _ = eng.forward_tensor(x, generation=g)
+        eng.vjp_tensor(2.0 * (values - target), grad, generation=g)
+
+    for _ in range(args.warmup):
+        step32()
+    eng.profile(on=True, reset=True)
+    with Clocks(dev.index) as clk:
+        ms32 = time_steps(torch, step32, args.steps, 0, dist)
+    clocks = clk.summary()
+    stats = eng.kernel_stats()
+    eng.profile(on=False, reset=False)
+    value = world * B * args.steps / (ms32 / 1e3)
+    launches = sum(s["launches"] for s in stats.values())
+
+    # roofline of the dominant kernel class, timed live with CUDA events
+    peaks = load_peaks()
+    dom = max(stats.values(), key=lambda s: s["ms"])
+    achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9 if dom["ms"] > 0 else 0.0
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        t = json.loads(tp.read_text()).get(dom["name"])
+        if t:
+            traffic = t.get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom["name"],
+                "launches_per_step": dom["launches"] / args.steps, "ms_per_step": dom["ms"] / args.steps,
+                "peak_source": peaks["source"],
+                "fp32_tflops": dom["flops"] / (dom["ms"] / 1e3) / 1e12 if dom["ms"] > 0 else 0.0,
+                "all_kernels_ms_per_step": {k: s["ms"] / args.steps for k, s in stats.items()}}
+
+    # -- end to end through the reference-facing host API ---------------------
+    def step_e2e():
+        g = next(gen)
+        values, _ = eng.forward(x_host, generation=g)
+        eng.vjp(2.0 * (values - target), generation=g)
+
+    ms_e2e = time_steps(torch, step_e2e, max(2, args.steps // 2), 1, dist)
+    e2e_steps = max(2, args.steps // 2)
+    ncoeff = eng.ncoeff
+    e2e = {"value": world * B * e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": B * npix * 8 + B * ncoeff * 16, "d2h_bytes_per_step": B * ncoeff * 16 + B * npix * 8,
+           "api": "stlp_forward + stlp_vjp (host f64 buffers)"}
+    eng.close()
+    del x, xt, grad
+    torch.cuda.empty_cache()
+
+    # -- FP64 plain single map --------------------------------------------------
+    fp64 = None
+    if not args.skip_fp64:
+        e64 = stl_b200.NativeEngine(nside, J, batch=1, dtype="float64", device=dev.index, prepare=True)
+        x64 = torch.tensor(x_host[:1], dtype=torch.float64, device=dev)
+        t64, _ = e64.forward_tensor(torch.tensor(lognormal(100, npix)[None], dtype=torch.float64, device=dev),
+                                    generation=1)
+        g64 = torch.empty_like(x64)
+
+        def step64():
+            g = next(gen)
+            values, _ = e64.forward_tensor(x64, generation=g)
+            e64.vjp_tensor(2.0 * (values - t64), g64, generation=g)
+
+        ms64 = time_steps(torch, step64, args.steps, args.warmup, dist)
+        fp64 = world * args.steps / (ms64 / 1e3)
+        e64.close()
+        del x64, g64
+        torch.cuda.empty_cache()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"scatcov fwd+vjp nside{nside} J{J} L4 batch{B} fp32 (sums fp64)",
+                           "nside": nside, "J": J, "L": 4, "batch_per_gpu": B, "ncoeff": ncoeff,
+                           "maps": "lognormal exp(g-1/2), numpy default_rng seeds rank*B..rank*B+B-1",
+                           "l2": "inputs larger than L2 (fields and operators of tens of GB per step)",
+                           "parallelism": f"replicas x{world}",
+                           "fp64_plain_evals_per_s": fp64,
+                           "fp32_batched_over_fp64_plain": (value / world) / (fp64 / world) if fp64 else None},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -89,6 +89,13 @@ int stlp_set_stream(StlpHandle* h, uint64_t stream);
  * reference counterpart (the reference builds in stlp_new). */
 int stlp_prepare(StlpHandle* h);
 
+/* Kernel statistics: reset != 0 clears the per-class launch counts, device
+ * times and algorithmic bytes/flops reported by stlp_info ("kernels");
+ * on != 0 times every launch with CUDA events on the handle's stream.  The
+ * reference's counterpart is its per-phase wall timers (crates/stl-gpu/src/
+ * engine.rs:811-818, reported by stlp_info). */
+int stlp_profile(StlpHandle* h, int on, int reset);
+
 /* Copy of the current forward state (the loaded maps; the fields are
  * recomputed by stlp_restore); NULL on failure.  (lib.rs:647-659) */
 StlpSnapshot* stlp_checkpoint(StlpHandle* h);

@@ -139,6 +139,16 @@ int stlp_prepare(StlpHandle* h) {
   });
 }
 
+int stlp_profile(StlpHandle* h, int on, int reset) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr, "null handle");
+    h->activate();
+    if (reset) h->engine->reset_kernel_stats();
+    h->engine->set_profiling(on != 0);
+    return 0;
+  });
+}
+
 int stlp_set_stream(StlpHandle* h, uint64_t stream) {
   return guard<int>(-1, [&] {
     require(h != nullptr, "null handle");
@@ -165,6 +175,15 @@ char* stlp_info(StlpHandle* h) {
     js << ", \"timers\": {\"build_s\": " << e.timers.build_s << ", \"forward_ms\": " << e.timers.forward_ms
        << ", \"reverse_ms\": " << e.timers.reverse_ms << ", \"forwards\": " << e.timers.forwards
        << ", \"reverses\": " << e.timers.reverses << "}";
+    js << ", \"kernels\": [";
+    auto ks = e.kernel_stats();
+    for (size_t i = 0; i < ks.size(); ++i)
+      js << (i ? ", " : "") << "{\"name\": " << jstr(ks[i].name) << ", \"launches\": " << ks[i].launches
+         << ", \"ms\": " << ks[i].ms << ", \"bytes\": " << ks[i].bytes << ", \"flops\": " << ks[i].flops << "}";
+    js << "], \"mean_cells_per_row\": [";
+    auto ms = e.mean_slots();
+    for (size_t i = 0; i < ms.size(); ++i) js << (i ? ", " : "") << ms[i];
+    js << "]";
     js << ", \"plan\": [";
     const auto& plan = e.plan();
     auto opt = [](int v) { return v < 0 ? std::string("null") : std::to_string(v); };

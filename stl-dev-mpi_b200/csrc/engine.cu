@@ -139,6 +139,62 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Launch accounting of the sweeps: counts and algorithmic bytes / flops
+// always, device time from CUDA events on the launching stream when on.
+class Profiler {
+ public:
+  enum Cat { CONV_FWD, CONV_ADJ, DEC, PROD_FWD, PROD_REV, ELEM, NCAT };
+  bool on = false;
+  KernelStat stat[NCAT];
+  Profiler() {
+    const char* names[NCAT] = {"conv_forward", "conv_adjoint", "decimation", "products_forward", "products_reverse",
+                               "elementwise"};
+    for (int c = 0; c < NCAT; ++c) stat[c].name = names[c];
+  }
+  ~Profiler() {
+    for (auto& r : pending_) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : pool_) cudaEventDestroy(e);
+  }
+  template <typename F>
+  void launch(Cat c, int kernels, double bytes, double flops, cudaStream_t s, F&& f) {
+    stat[c].launches += kernels;
+    stat[c].bytes += bytes;
+    stat[c].flops += flops;
+    if (!on) { f(); return; }
+    cudaEvent_t a = get(), b = get();
+    STL_CUDA(cudaEventRecord(a, s));
+    f();
+    STL_CUDA(cudaEventRecord(b, s));
+    pending_.push_back({c, a, b});
+  }
+  // after the stream has been synchronised
+  void collect() {
+    for (auto& r : pending_) {
+      float ms = 0.f;
+      STL_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+      stat[r.c].ms += ms;
+      pool_.push_back(r.a);
+      pool_.push_back(r.b);
+    }
+    pending_.clear();
+  }
+  void reset() {
+    collect();
+    for (auto& s : stat) { s.launches = 0; s.ms = s.bytes = s.flops = 0.0; }
+  }
+
+ private:
+  struct Rec { Cat c; cudaEvent_t a, b; };
+  std::vector<Rec> pending_;
+  std::vector<cudaEvent_t> pool_;
+  cudaEvent_t get() {
+    if (!pool_.empty()) { cudaEvent_t e = pool_.back(); pool_.pop_back(); return e; }
+    cudaEvent_t e;
+    STL_CUDA(cudaEventCreate(&e));
+    return e;
+  }
+};
+
 template <typename T>
 class EngineImpl final : public Engine {
  public:
@@ -217,21 +273,24 @@ class EngineImpl final : public Engine {
     prepare();
     size_t n = (size_t)opt_.B * npix(0);
     STL_CUDA(cudaMemcpyAsync(in_f64_.p, x, n * 8, cudaMemcpyHostToDevice, stream_));
-    convert<double, T>(in_f64_.as<double>(), X_[0].as<T>(), (i64)n, stream_);
+    prof_.launch(Profiler::ELEM, 1, n * (8.0 + sizeof(T)), 0.0, stream_,
+                 [&] { to_pixel_major<double, T>(in_f64_.as<double>(), X_[0].as<T>(), npix(0), opt_.B, stream_); });
     loaded_ = true;
   }
 
   void load_device(const void* x, bool f32) override {
     prepare();
     i64 n = (i64)opt_.B * npix(0);
-    if (f32) convert<float, T>(static_cast<const float*>(x), X_[0].as<T>(), n, stream_);
-    else convert<double, T>(static_cast<const double*>(x), X_[0].as<T>(), n, stream_);
+    prof_.launch(Profiler::ELEM, 1, n * ((f32 ? 4.0 : 8.0) + sizeof(T)), 0.0, stream_, [&] {
+      if (f32) to_pixel_major<float, T>(static_cast<const float*>(x), X_[0].as<T>(), npix(0), opt_.B, stream_);
+      else to_pixel_major<double, T>(static_cast<const double*>(x), X_[0].as<T>(), npix(0), opt_.B, stream_);
+    });
     loaded_ = true;
   }
 
   void save_input(std::vector<double>& x) override {
     i64 n = (i64)opt_.B * npix(0);
-    convert<T, double>(X_[0].as<T>(), in_f64_.as<double>(), n, stream_);
+    to_map_major<T, double>(X_[0].as<T>(), in_f64_.as<double>(), npix(0), opt_.B, stream_);
     x.resize(n);
     STL_CUDA(cudaMemcpyAsync(x.data(), in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
     STL_CUDA(cudaStreamSynchronize(stream_));
@@ -243,21 +302,37 @@ class EngineImpl final : public Engine {
     const int L = opt_.L, B = opt_.B;
     cudaStream_t s = stream_;
     for (int d = 0; d + 1 < levels_; ++d)
-      dec_apply<T>(dec_[d], false, X_[d].as<T>(), npix(d), X_[d + 1].as<T>(), npix(d + 1), B, 1, false, s);
+      prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[d], B, false), dec_flops(dec_[d], B, false), s, [&] {
+        dec_apply<T>(dec_[d], false, X_[d].as<T>(), B, 0, X_[d + 1].as<T>(), B, 0, 1, B, false, s);
+      });
     for (int n = 0; n < levels_; ++n) {
       i64 N = npix(n);
       T* mod = Mod_[n].as<T>();
-      conv_forward<T>(conv_[n], X_[n].as<T>(), B, Z_[n].as<T>(), 2 * L * N, mod + (i64)n * L * N,
-                      (i64)(n + 1) * L * N, s);
+      const ConvOp& op = conv_[n];
+      prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, true), conv_flops(op, B), s, [&] {
+        conv_forward<T>(op, X_[n].as<T>(), B, Z_[n].as<T>(), mod, B * (n + 1) * L, (n + 1) * L, n * L, s);
+      });
       if (n > 0)
-        dec_apply<T>(dec_[n - 1], false, Mod_[n - 1].as<T>(), (i64)n * L * npix(n - 1), mod, (i64)(n + 1) * L * N, B,
-                     n * L, false, s);
-      conv_forward<T>(conv_[n], mod, B * (n + 1) * L, Br_[n].as<T>(), 2 * L * N, nullptr, 0, s);
-      products_forward<T>(shapes_[n], Z_[n].as<T>(), Br_[n].as<T>(), X_[0].as<T>(), partials_.as<double>(),
-                          sums_.as<double>() + sum_off_[n], s);
+        prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n - 1], B * n * L, false), dec_flops(dec_[n - 1], B * n * L, false),
+                     s, [&] {
+                       dec_apply<T>(dec_[n - 1], false, Mod_[n - 1].as<T>(), B * n * L, n * L, mod, B * (n + 1) * L,
+                                    (n + 1) * L, B, n * L, false, s);
+                     });
+      const int R = B * (n + 1) * L;
+      prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
+        conv_forward<T>(op, mod, R, Br_[n].as<T>(), nullptr, 0, 0, 0, s);
+      });
+      const ProductShape& sh = shapes_[n];
+      double E = sh.K * (sh.K + 1) / 2.0;
+      prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(T), (double)B * L * N * E * 10.0, s,
+                   [&] {
+                     products_forward<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), X_[0].as<T>(), partials_.as<double>(),
+                                         sums_.as<double>() + sum_off_[n], s);
+                   });
     }
     STL_CUDA(cudaMemcpyAsync(h_sums_.data(), sums_.p, h_sums_.size() * 8, cudaMemcpyDeviceToHost, s));
     STL_CUDA(cudaStreamSynchronize(s));
+    prof_.collect();
     assemble(values, moments ? var : nullptr);
     forward_done_ = true;
     timers.forward_ms += ms_since(t0);
@@ -267,7 +342,8 @@ class EngineImpl final : public Engine {
   void reverse_host(const double* cot, double* out) override {
     reverse_impl(cot);
     i64 n = (i64)opt_.B * npix(0);
-    convert<T, double>(gX_[0].as<T>(), in_f64_.as<double>(), n, stream_);
+    prof_.launch(Profiler::ELEM, 1, n * (8.0 + sizeof(T)), 0.0, stream_,
+                 [&] { to_map_major<T, double>(gX_[0].as<T>(), in_f64_.as<double>(), npix(0), opt_.B, stream_); });
     STL_CUDA(cudaMemcpyAsync(out, in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
     STL_CUDA(cudaStreamSynchronize(stream_));
   }
@@ -275,39 +351,78 @@ class EngineImpl final : public Engine {
   void reverse_device(const double* cot, void* out, bool f32) override {
     reverse_impl(cot);
     i64 n = (i64)opt_.B * npix(0);
-    if (f32) convert<T, float>(gX_[0].as<T>(), static_cast<float*>(out), n, stream_);
-    else convert<T, double>(gX_[0].as<T>(), static_cast<double*>(out), n, stream_);
+    prof_.launch(Profiler::ELEM, 1, n * ((f32 ? 4.0 : 8.0) + sizeof(T)), 0.0, stream_, [&] {
+      if (f32) to_map_major<T, float>(gX_[0].as<T>(), static_cast<float*>(out), npix(0), opt_.B, stream_);
+      else to_map_major<T, double>(gX_[0].as<T>(), static_cast<double*>(out), npix(0), opt_.B, stream_);
+    });
     STL_CUDA(cudaStreamSynchronize(stream_));
   }
 
- private:
-  // where a plan coefficient's sums live: level, l3 row, slot; conj flag;
-  // kind 0 Gram entry, 1 S1 (sum |z|), 2 mean, 3 var
-  struct Loc {
-    int level, l3, kind, entry, conj;
-    double second_slot;  // unused
-  };
-  static int entry_of(int K, int i, int j) { return i * K - i * (i - 1) / 2 + (j - i); }
+  std::vector<KernelStat> kernel_stats() const override {
+    return std::vector<KernelStat>(prof_.stat, prof_.stat + Profiler::NCAT);
+  }
+  void reset_kernel_stats() override { prof_.reset(); }
+  void set_profiling(bool on) override { prof_.on = on; }
+  std::vector<double> mean_slots() const override {
+    std::vector<double> v;
+    for (const auto& c : conv_) v.push_back(c.mean_slots);
+    return v;
+  }
 
+ private:
+  // Algorithmic traffic of one wavelet launch over R rows: the used
+  // coefficients of the stored rows (2L values and a 4-byte cell index per
+  // cell read; a quarter of the rows on the full sky), the input rows read
+  // once, the complex outputs written once (plus |z|, or the
+  // read-modify-write of an accumulated adjoint).
+  double conv_bytes(const ConvOp& op, int R, bool fwd, bool extra) const {
+    const double s = sizeof(T), N = (double)op.n_rows, D = op.mean_slots;
+    double coef = (double)op.n_rep * D * (8.0 * s + 4.0);
+    double field = fwd ? R * N * s + R * N * 8.0 * s : R * N * 8.0 * s + R * N * s;
+    if (extra) field += fwd ? R * N * 4.0 * s : R * N * s;
+    return coef + field;
+  }
+  double conv_flops(const ConvOp& op, int R) const { return 2.0 * 8.0 * R * (double)op.n_rows * op.mean_slots; }
+  double dec_bytes(const DecOp& op, int R, bool transpose) const {
+    const double s = sizeof(T);
+    double nnz = op.mean_w * (double)op.n_out;
+    return nnz * (s + 4.0) + R * (double)(op.n_in + op.n_out) * s;
+    (void)transpose;
+  }
+  double dec_flops(const DecOp& op, int R, bool) const { return 2.0 * R * op.mean_w * (double)op.n_out; }
+
+  // where a plan coefficient's sums live: level, l3 row, and the slots of
+  // its real part, imaginary part (-1: exactly zero) and second moment
+  struct Loc {
+    int level, l3, re, im, second;
+  };
+
+  // Sums of the products kernel per (b, l3) (kernels.cu): 4 x 4 Gram blocks
+  // (d1 <= d2) of the branches, 4 x 1 blocks (d, z), then the per-pixel sums.
   Loc locate(const Coef& c) const {
     const int L = opt_.L;
-    int n = c.native;
-    int K = (n + 1) * L + 1, z = K - 1;
-    Loc l{n, 0, 0, 0, 0, 0};
+    const int n = c.native, nd = n + 1;
+    const int nBB = nd * (nd + 1) / 2, zb = nBB * 48 + nd * 12;
+    auto tblock = [&](int d1, int d2) { return d1 * nd - d1 * (d1 - 1) / 2 + (d2 - d1); };
+    Loc l{n, 0, 0, 0, 0};
     switch (c.family) {
-      case MEAN: l.kind = 2; break;
-      case VAR: l.kind = 3; break;
-      case S1: l.kind = 1; l.l3 = c.l1; break;
-      case S2: l.l3 = c.l1; l.entry = entry_of(K, z, z); break;
-      case S3: l.l3 = c.l3; l.entry = entry_of(K, c.j1 * L + c.l1, z); break;
+      case MEAN: l.re = zb + 3; l.second = zb + 4; l.im = -1; break;
+      case VAR: l.re = zb + 4; l.second = zb + 5; l.im = -1; break;
+      case S1: l.l3 = c.l1; l.re = zb; l.second = zb + 1; l.im = -1; break;
+      case S2: l.l3 = c.l1; l.re = zb + 1; l.second = zb + 2; l.im = -1; break;
+      case S3: {
+        const int base = nBB * 48 + 12 * c.j1;
+        l.l3 = c.l3; l.re = base + 2 * c.l1; l.im = l.re + 1; l.second = base + 8 + c.l1;
+        break;
+      }
       case S4: {
-        int i = c.j1 * L + c.l1, j = c.j2 * L + c.l2;
-        l.l3 = c.l3;
-        if (i <= j) l.entry = entry_of(K, i, j);
-        else { l.entry = entry_of(K, j, i); l.conj = 1; }
+        const int t = tblock(c.j1, c.j2), e = c.l1 * 4 + c.l2;
+        l.l3 = c.l3; l.re = t * 48 + 2 * e; l.im = l.re + 1; l.second = t * 48 + 32 + e;
+        if (c.j1 == c.j2 && c.l1 == c.l2) l.im = -1;  // v conj(v): an exactly real term
         break;
       }
     }
+    (void)L;
     return l;
   }
 
@@ -316,25 +431,12 @@ class EngineImpl final : public Engine {
     const i64 np = (i64)plan_.size();
     for (int b = 0; b < B; ++b)
       for (i64 i = 0; i < np; ++i) {
-        const Coef& c = plan_[i];
         const Loc& l = map_[i];
         const ProductShape& sh = shapes_[l.level];
-        int K = sh.K, E = K * (K + 1) / 2;
         const double* row = h_sums_.data() + sum_off_[l.level] + ((size_t)b * L + l.l3) * sh.slots;
-        double N = (double)npix(l.level);
-        double re = 0, im = 0, second = 0;
-        switch (l.kind) {
-          case 0:
-            re = row[2 * l.entry]; im = row[2 * l.entry + 1];
-            if (l.conj) im = -im;
-            second = row[2 * E + l.entry];
-            if (c.family == S2) { im = 0.0; second = row[3 * E + 1]; }
-            break;
-          case 1: re = row[3 * E]; second = row[2 * entry_of(K, K - 1, K - 1)]; break;
-          case 2: re = row[3 * E + 2]; second = row[3 * E + 3]; break;
-          case 3: re = row[3 * E + 3]; second = row[3 * E + 4]; break;
-        }
-        double vr = re / N, vi = im / N;
+        const double N = (double)npix(l.level);
+        const double re = row[l.re], im = l.im >= 0 ? row[l.im] : 0.0, second = row[l.second];
+        const double vr = re / N, vi = im / N;
         values[2 * (b * np + i)] = vr;
         values[2 * (b * np + i) + 1] = vi;
         if (var) var[b * np + i] = std::max(second / N - (vr * vr + vi * vi), 0.0);
@@ -384,10 +486,14 @@ class EngineImpl final : public Engine {
     for (int n = levels_ - 1; n >= 0; --n) {
       i64 N = npix(n);
       const ProductShape& sh = shapes_[n];
+      const ConvOp& op = conv_[n];
       T* gmod = gMod_[n].as<T>();
       if (n + 1 < levels_)
-        dec_apply<T>(dec_[n], true, gMod_[n + 1].as<T>(), (i64)(n + 2) * L * npix(n + 1), gmod, (i64)(n + 1) * L * N, B,
-                     (n + 1) * L, false, s);
+        prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B * (n + 1) * L, true), dec_flops(dec_[n], B * (n + 1) * L, true),
+                     s, [&] {
+                       dec_apply<T>(dec_[n], true, gMod_[n + 1].as<T>(), B * (n + 2) * L, (n + 2) * L, gmod,
+                                    B * (n + 1) * L, (n + 1) * L, B, (n + 1) * L, false, s);
+                     });
       else
         STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
       // cotangent matrices in the field precision
@@ -397,22 +503,36 @@ class EngineImpl final : public Engine {
       for (size_t q = 0; q < s1[n].size(); ++q) h_s1_[q] = (T)s1[n][q];
       STL_CUDA(cudaMemcpyAsync(M_.p, h_M_.data(), h_M_.size() * sizeof(T), cudaMemcpyHostToDevice, s));
       STL_CUDA(cudaMemcpyAsync(s1c_.p, h_s1_.data(), h_s1_.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-      products_reverse<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), M_.as<T>(), s1c_.as<T>(), gZ_.as<T>(), gBr_.as<T>(), s);
-      conv_adjoint<T>(conv_[n], gBr_.as<T>(), 2 * L * N, B * (n + 1) * L, gmod, true, s);
-      modulus_vjp_add<T>(Z_[n].as<T>(), gmod + (i64)n * L * N, (i64)(n + 1) * L * N, gZ_.as<T>(), B, (i64)L * N, s);
-      conv_adjoint<T>(conv_[n], gZ_.as<T>(), 2 * L * N, B, gX_[n].as<T>(), false, s);
+      const double sz = sizeof(T);
+      prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0, s,
+                   [&] {
+                     products_reverse<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), M_.as<T>(), s1c_.as<T>(), gZ_.as<T>(),
+                                         gBr_.as<T>(), s);
+                   });
+      const int R = B * (n + 1) * L;
+      prof_.launch(Profiler::CONV_ADJ, 1, conv_bytes(op, R, false, true), conv_flops(op, R), s,
+                   [&] { conv_adjoint<T>(op, gBr_.as<T>(), R, gmod, true, s); });
+      prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
+        modulus_vjp_add<T>(Z_[n].as<T>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<T>(), N, B, L, s);
+      });
+      prof_.launch(Profiler::CONV_ADJ, 1, conv_bytes(op, B, false, false), conv_flops(op, B), s,
+                   [&] { conv_adjoint<T>(op, gZ_.as<T>(), B, gX_[n].as<T>(), false, s); });
       if (n + 1 < levels_)
-        dec_apply<T>(dec_[n], true, gX_[n + 1].as<T>(), npix(n + 1), gX_[n].as<T>(), N, B, 1, true, s);
+        prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
+                     [&] { dec_apply<T>(dec_[n], true, gX_[n + 1].as<T>(), B, 0, gX_[n].as<T>(), B, 0, 1, B, true, s); });
       // the host staging buffers are reused next level: wait for the copies
       STL_CUDA(cudaStreamSynchronize(s));
     }
     STL_CUDA(cudaMemcpyAsync(mv_.p, mv.data(), mv.size() * 8, cudaMemcpyHostToDevice, s));
-    mean_var_grad<T>(X_[0].as<T>(), mv_.as<double>(), B, npix(0), gX_[0].as<T>(), s);
+    prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * sizeof(T), (double)B * npix(0) * 2.0, s,
+                 [&] { mean_var_grad<T>(X_[0].as<T>(), mv_.as<double>(), B, npix(0), gX_[0].as<T>(), s); });
     STL_CUDA(cudaStreamSynchronize(s));
+    prof_.collect();
     timers.reverse_ms += ms_since(t0);
     timers.reverses += 1;
   }
 
+  Profiler prof_;
   bool ready_ = false, loaded_ = false, forward_done_ = false;
   std::vector<ConvOp> conv_;
   std::vector<DecOp> dec_;

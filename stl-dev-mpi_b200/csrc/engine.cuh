@@ -74,19 +74,33 @@ struct ConvSpec {
   i64 n_in = 0;
   const i64* d_rows = nullptr;  // NESTED ids of the output rows (device), nullptr: rows == grid
   i64 n_rows = 0;
+  bool symmetric = true;        // full sky: store the rows of faces 0, 4, 8 only
 };
 
+// Full sky: HEALPix's 4-fold azimuthal symmetry (faces 4m + k, k = 0..3,
+// are rotations by k pi / 2 of face 4m) makes the folded stencil of
+// pixel (4m + k, x, y) the one of (4m, x, y) with every cell read rotated
+// to face 4m + k, the gauges permuted (g <- (g + 2k) mod 4) and the
+// imaginary part negated when the rotated gauge angle wraps by pi.  Only
+// the rows of faces 0, 4 and 8 ("representative rows", nk = 4) are
+// stored; kernels evaluate the 4 rotations from one coefficient load.
+// Partial grids (disc patches) store every row (nk = 1).
 struct ConvOp {
-  i64 n_rows = 0, n_in = 0;
-  int S = 0;        // slots per row
-  int ST = 0;       // transposed entries per input cell
-  int shift = 0;    // transposed entry = row << shift | slot
+  i64 n_rows = 0, n_in = 0;  // output rows, input cells (full level or grid)
+  i64 n_rep = 0;             // stored rows (n_rows / nk)
+  int nk = 1;                // 4: full-sky rotations, 1: every row stored
+  int o2 = 0;                // 2 log2(nside): pixel = face << o2 | local
+  int S = 0;                 // slots per stored row
+  int ST = 0;                // transposed entries per stored cell
+  int tshift = 0;            // transposed entry = u << tshift | s << 2 | j
   DType dtype = DType::F32;
-  DevMem cell;      // int32 [S][n_rows]
-  DevMem coef;      // T [S][n_rows][8] (G = 4) or [S][n_rows][2G]
-  DevMem tent;      // uint32 [ST][n_in], 0xFFFFFFFF past the end of a cell's list
+  DevMem cell;               // int32 [S][n_rep]: cell read (full-sky id, or grid position)
+  DevMem coef;               // T [S][n_rep][8]: (gauge, re/im) coefficients
+  DevMem tent;               // uint32 [ST][n_rep]: entries (u, s, j) reading rotation j of a stored cell
+  DevMem coefT;              // T [ST][n_rep][8]: coef of each transposed entry
   int G = 4;
-  size_t bytes() const { return cell.bytes + coef.bytes + tent.bytes; }
+  double mean_slots = 0.0;   // cells read per row, averaged over the rows
+  size_t bytes() const { return cell.bytes + coef.bytes + tent.bytes + coefT.bytes; }
 };
 
 struct DecSpec {
@@ -95,14 +109,21 @@ struct DecSpec {
   i64 n_in = 0;
   const i64* d_out = nullptr;  // sorted coarse ids = parents of the grid (device), nullptr: whole sky
   i64 n_out = 0;
+  bool symmetric = true;       // full sky: store the rows of faces 0, 4, 8 only
 };
 
+// Decimation rows, stored for the coarse pixels of faces 0, 4, 8 on the
+// full sky (nk = 4: rows of the other faces are the rotated ones, as for
+// ConvOp), and the transposed rows for the fine pixels of faces 0, 4, 8.
 struct DecOp {
-  i64 n_out = 0, n_in = 0;
+  i64 n_out = 0, n_in = 0;         // coarse rows, fine cells (full level or grid)
+  i64 n_rep_out = 0, n_rep_in = 0; // stored coarse rows, stored fine cells
+  int nk = 1, o2 = 0, co2 = 0;     // rotations; 2 log2 nside of the fine and coarse levels
   int W = 0, WT = 0;
   DType dtype = DType::F32;
-  DevMem col, w;    // int32 / T [W][n_out]
-  DevMem tcol, tw;  // int32 / T [WT][n_in]
+  DevMem col, w;    // int32 / T [W][n_rep_out]: fine column (full-sky id or grid position)
+  DevMem tcol, tw;  // int32 / T [WT][n_rep_in]: coarse row (full-sky id or position)
+  double mean_w = 0.0;  // weights per coarse row, averaged
   size_t bytes() const { return col.bytes + w.bytes + tcol.bytes + tw.bytes; }
 };
 
@@ -111,40 +132,55 @@ void build_conv(const ConvSpec& spec, const std::vector<double>& kernel, DType d
                 cudaStream_t stream);
 void build_dec(const DecSpec& spec, DType dtype, DecOp& out, cudaStream_t stream);
 
-// Kernel launchers (kernels.cu).  Rows of every field are planes of
-// `plane` elements; complex fields interleave (re, im).
+// Kernel launchers (kernels.cu).  Fields are pixel-major (a vector of
+// rows per pixel); complex values interleave (re, im).
+//  conv_forward: x [n_in][R] -> out [n_rows][R][4] complex; with mod, |out|
+//    of row r, gauge g at mod[p mod_pix + r mod_row + mod_off + g].
+//  conv_adjoint: gy [n_rows][R][4] complex -> gx [n_in][R] (or += gx).
+//  dec_apply: y[c][ro][ri] = (D or D^T) x, row (ro, ri) of pixel c at
+//    c pix + ro outer + ri.
 template <typename T>
-void conv_forward(const ConvOp& op, const T* x, int R, T* out, i64 out_row_stride, T* mod_out, i64 mod_row_stride,
+void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
                   cudaStream_t s);
 template <typename T>
-void conv_adjoint(const ConvOp& op, const T* gy, i64 gy_row_stride, int R, T* gx, bool accumulate, cudaStream_t s);
-// y[ro][ri] = D x[ro][ri] with row (ro, ri) at base + ro * outer + ri * plane
+void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s);
 template <typename T>
-void dec_apply(const DecOp& op, bool transpose, const T* x, i64 x_outer, T* y, i64 y_outer, int R_outer,
-               int R_inner, bool accumulate, cudaStream_t s);
+void dec_apply(const DecOp& op, bool transpose, const T* x, int x_pix, int x_outer, T* y, int y_pix, int y_outer,
+               int R_outer, int R_inner, bool accumulate, cudaStream_t s);
+// gz[p][b][l] += g z / |z|, z and gz [N][B][L] complex, g at p g_pix + b g_row + l
 template <typename T>
-void modulus_vjp_add(const T* z, const T* g, i64 g_outer, T* gz, int B, i64 plane_elems, cudaStream_t s);
+void modulus_vjp_add(const T* z, const T* g, int g_pix, int g_row, T* gz, i64 N, int B, int L, cudaStream_t s);
 
 // Coefficient products of one level (see kernels.cu for the slot layout).
 struct ProductShape {
+  int nd = 1;        // levels of the branches: n + 1
   int K = 0;         // operand vector length: (n + 1) L branches + z
   int L = 4;
   int B = 1;
   i64 N = 0;         // pixels of the level
   bool level0 = false;
-  int blocks = 0;    // partial sums per (b, l3)
-  int slots = 0;     // doubles per partial
+  int blocks = 0;    // partial sums per map
+  int slots = 0;     // doubles per (b, l3) partial
 };
 ProductShape product_shape(int n, int L, int B, i64 N);
+// z [N][B][L], br [N][B][(n+1) L][L] complex, x0 [N][B] (level 0) ->
+// sums [B][L][slots] (FP64)
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials,
                       double* sums, cudaStream_t s);
+// M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
                       cudaStream_t s);
+// gx[p][b] += coefs[b][0] + coefs[b][1] x0[p][b]
 template <typename T>
 void mean_var_grad(const T* x0, const double* coefs, int B, i64 N, T* gx, cudaStream_t s);
 template <typename Tin, typename Tout>
 void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s);
+// [B][N] map-major <-> [N][B] pixel-major
+template <typename Tin, typename Tout>
+void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s);
+template <typename Tin, typename Tout>
+void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s);
 
 }  // namespace stl

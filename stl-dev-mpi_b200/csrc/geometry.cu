@@ -45,7 +45,9 @@ struct FoldArgs {
   const i64* grid;
   i64 n_in;
   const i64* rows;
-  i64 n_rows;
+  i64 n_rows;             // rows built (the stored rows)
+  int sym;                // stored row u is pixel (4 (u >> sym_o2)) << sym_o2 | local
+  int sym_o2;
   const double* stencil;  // [P][3]
   const double* kernel;   // [G][2][P]
 };
@@ -56,7 +58,13 @@ template <typename T>
 __global__ void k_fold(FoldArgs a, int* counts, int S, int32_t* cell, T* coef, int* overflow) {
   i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.n_rows) return;
-  i64 id = a.rows ? a.rows[k] : (a.grid ? a.grid[k] : k);
+  i64 id;
+  if (a.sym) {
+    i64 mask = (i64(1) << a.sym_o2) - 1;
+    id = ((4 * (k >> a.sym_o2)) << a.sym_o2) | (k & mask);
+  } else {
+    id = a.rows ? a.rows[k] : (a.grid ? a.grid[k] : k);
+  }
   double theta, phi;
   pix2ang_nest(id, a.nside, theta, phi);
   theta = deg2rad(90.0 - rad2deg(kPi / 2.0 - theta));
@@ -144,23 +152,60 @@ __global__ void k_max_int(const int* v, i64 n, int* out) {
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-// transposed table of a slot-major ELL: entries (row << shift | slot) per column
-__global__ void k_tcount(const int32_t* cell, const int* counts, i64 n_rows, int S, int* tcount) {
-  i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_rows) return;
-  int n = counts ? counts[k] : S;
-  for (int s = 0; s < n; ++s) atomicAdd(&tcount[cell[(i64)s * n_rows + k]], 1);
+// transposed entries of the wavelet: stored row u reads cell c at slot s;
+// c is rotation j of the stored cell v (full sky), or v = c, j = 0.
+__device__ __forceinline__ void split_cell(i64 c, int sym, int sym_o2, i64& v, int& j) {
+  if (sym) {
+    i64 f = c >> sym_o2;
+    v = ((f >> 2) << sym_o2) | (c & ((i64(1) << sym_o2) - 1));
+    j = (int)(f & 3);
+  } else {
+    v = c;
+    j = 0;
+  }
 }
 
-__global__ void k_tfill(const int32_t* cell, const int* counts, i64 n_rows, int S, int shift, i64 n_in, int* tfill,
-                        uint32_t* tent) {
-  i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_rows) return;
-  int n = counts ? counts[k] : S;
-  for (int s = 0; s < n; ++s) {
-    int32_t c = cell[(i64)s * n_rows + k];
-    int pos = atomicAdd(&tfill[c], 1);
-    tent[(i64)pos * n_in + c] = (uint32_t)(((uint64_t)k << shift) | (uint64_t)s);
+__global__ void k_conv_tcount(const int32_t* cell, const int* counts, i64 n_rep, int sym, int sym_o2, int* tcount) {
+  i64 u = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n_rep) return;
+  for (int s = 0; s < counts[u]; ++s) {
+    i64 v;
+    int j;
+    split_cell(cell[(i64)s * n_rep + u], sym, sym_o2, v, j);
+    atomicAdd(&tcount[v], 1);
+  }
+}
+
+__global__ void k_conv_tfill(const int32_t* cell, const int* counts, i64 n_rep, int sym, int sym_o2, int tshift,
+                             int* tfill, uint32_t* tent) {
+  i64 u = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n_rep) return;
+  for (int s = 0; s < counts[u]; ++s) {
+    i64 v;
+    int j;
+    split_cell(cell[(i64)s * n_rep + u], sym, sym_o2, v, j);
+    int pos = atomicAdd(&tfill[v], 1);
+    tent[(i64)pos * n_rep + v] = (uint32_t)(((uint64_t)u << tshift) | ((uint64_t)s << 2) | (uint64_t)j);
+  }
+}
+
+// coefficients of the (sorted) transposed entries, zeros past the end
+template <typename T>
+__global__ void k_conv_coefT(const uint32_t* tent, const T* coef, i64 n_rep, int ST, int tshift, T* coefT) {
+  i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_rep) return;
+  const uint32_t smask = (1u << (tshift - 2)) - 1u;
+  for (int e = 0; e < ST; ++e) {
+    uint32_t ent = tent[(i64)e * n_rep + v];
+    T* dst = coefT + ((i64)e * n_rep + v) * 8;
+    if (ent == kSentinel) {
+      for (int o = 0; o < 8; ++o) dst[o] = (T)0;
+      continue;
+    }
+    i64 u = (i64)(ent >> tshift);
+    int s = (int)((ent >> 2) & smask);
+    const T* src = coef + ((i64)s * n_rep + u) * 8;
+    for (int o = 0; o < 8; ++o) dst[o] = src[o];
   }
 }
 
@@ -187,7 +232,9 @@ struct DecArgs {
   const i64* ids;  // fine grid (nullptr: whole sky)
   i64 n_in;
   const i64* out;  // coarse rows (nullptr: whole sky)
-  i64 n_out;
+  i64 n_out;       // rows built (the stored rows)
+  int sym;         // stored row u is coarse pixel (4 (u >> sym_co2)) << sym_co2 | local
+  int sym_co2;
   double radius, sigma;
 };
 
@@ -204,7 +251,9 @@ template <typename T>
 __global__ void k_dec_rows(DecArgs a, int* counts, int W, int32_t* col, T* wout, int* overflow) {
   i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= a.n_out) return;
-  i64 c = a.out ? a.out[r] : r;
+  i64 c;
+  if (a.sym) c = ((4 * (r >> a.sym_co2)) << a.sym_co2) | (r & ((i64(1) << a.sym_co2) - 1));
+  else c = a.out ? a.out[r] : r;
   i64 cn = a.nside / 2;
   i64 cand[kDecCap];
   int n = 0;
@@ -275,18 +324,39 @@ __global__ void k_dec_rows(DecArgs a, int* counts, int W, int32_t* col, T* wout,
     }
 }
 
-// transpose of an ELL (col, w) [W][n_out] -> (tcol, tw) [WT][n_in], entries of a
-// fine column in increasing coarse row (decimation.rs:70-91)
-template <typename T>
-__global__ void k_dec_tfill(const int32_t* col, const T* w, const int* counts, i64 n_out, i64 n_in, int* tfill,
-                            int32_t* tcol, T* tw) {
+// transpose of the stored decimation rows: for every stored fine cell v, the
+// coarse rows (full-sky ids, or positions) reading it and their weights,
+// sorted by coarse row (decimation.rs:70-91).  On the full sky a stored
+// coarse row u reads rotation j of v when its column is rotation j of v;
+// rotation (4 - j) mod 4 of u then reads v itself.
+__device__ __forceinline__ i64 sym_pixel(i64 u, int k, int o2) {
+  return ((4 * (u >> o2) + k) << o2) | (u & ((i64(1) << o2) - 1));
+}
+
+__global__ void k_dec_tcount(const int32_t* col, const int* counts, i64 n_rows, int sym, int fine_o2, int* tcount) {
   i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n_out) return;
+  if (r >= n_rows) return;
   for (int k = 0; k < counts[r]; ++k) {
-    int32_t c = col[(i64)k * n_out + r];
-    int pos = atomicAdd(&tfill[c], 1);
-    tcol[(i64)pos * n_in + c] = (int32_t)r;
-    tw[(i64)pos * n_in + c] = w[(i64)k * n_out + r];
+    i64 v;
+    int j;
+    split_cell(col[(i64)k * n_rows + r], sym, fine_o2, v, j);
+    atomicAdd(&tcount[v], 1);
+  }
+}
+
+template <typename T>
+__global__ void k_dec_tfill(const int32_t* col, const T* w, const int* counts, i64 n_rows, i64 n_cells, int sym,
+                            int fine_o2, int coarse_o2, int* tfill, int32_t* tcol, T* tw) {
+  i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_rows) return;
+  for (int k = 0; k < counts[r]; ++k) {
+    i64 v;
+    int j;
+    split_cell(col[(i64)k * n_rows + r], sym, fine_o2, v, j);
+    i64 coarse = sym ? sym_pixel(r, (4 - j) & 3, coarse_o2) : r;
+    int pos = atomicAdd(&tfill[v], 1);
+    tcol[(i64)pos * n_cells + v] = (int32_t)coarse;
+    tw[(i64)pos * n_cells + v] = w[(i64)k * n_rows + r];
   }
 }
 
@@ -323,6 +393,15 @@ int device_max(const int* d, i64 n, cudaStream_t s) {
   STL_CUDA(cudaMemcpyAsync(&h, m.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   STL_CUDA(cudaStreamSynchronize(s));
   return h;
+}
+
+double device_mean(const int* d, i64 n, cudaStream_t s) {
+  std::vector<int> h(n);
+  STL_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  STL_CUDA(cudaStreamSynchronize(s));
+  double t = 0.0;
+  for (int v : h) t += v;
+  return n > 0 ? t / (double)n : 0.0;
 }
 
 int read_flag(const DevMem& f, cudaStream_t s) {
@@ -362,13 +441,20 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   DevMem d_st(st.size() * 8), d_ker(kernel.size() * 8);
   STL_CUDA(cudaMemcpyAsync(d_st.p, st.data(), st.size() * 8, cudaMemcpyHostToDevice, s));
   STL_CUDA(cudaMemcpyAsync(d_ker.p, kernel.data(), kernel.size() * 8, cudaMemcpyHostToDevice, s));
+  const bool sym = sp.symmetric && sp.d_grid == nullptr && sp.d_rows == nullptr;
   FoldArgs a;
   a.nside = sp.nside; a.order = order_of(sp.nside); a.ksz = sp.ksz; a.P = P; a.G = sp.G; a.gauge = sp.gauge;
   a.p_ref = (sp.ksz / 2) * (sp.ksz + 1); a.eps = sp.eps;
   a.grid = sp.d_grid; a.n_in = sp.d_grid ? sp.n_in : npix_of(sp.nside);
-  a.rows = sp.d_rows; a.n_rows = sp.d_rows ? sp.n_rows : a.n_in;
+  a.rows = sp.d_rows;
+  i64 n_rows = sp.d_rows ? sp.n_rows : a.n_in;
+  a.n_rows = sym ? n_rows / 4 : n_rows;
+  a.sym = sym ? 1 : 0;
+  a.sym_o2 = 2 * a.order;
   a.stencil = d_st.as<double>(); a.kernel = d_ker.as<double>();
-  op.n_rows = a.n_rows; op.n_in = a.n_in; op.G = sp.G;
+  op.n_rows = n_rows; op.n_in = a.n_in; op.n_rep = a.n_rows; op.G = sp.G;
+  op.nk = sym ? 4 : 1;
+  op.o2 = 2 * a.order;
   op.dtype = sizeof(T) == 8 ? DType::F64 : DType::F32;
   DevMem counts(sizeof(int) * std::max<i64>(a.n_rows, 1)), flag(sizeof(int));
   STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
@@ -377,28 +463,40 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   STL_CUDA(cudaGetLastError());
   if (read_flag(flag, s)) throw std::runtime_error("a wavelet stencil reads more cells than the builder holds");
   op.S = std::max(1, device_max(counts.as<int>(), a.n_rows, s));
+  op.mean_slots = device_mean(counts.as<int>(), a.n_rows, s);
   op.cell.alloc(sizeof(int32_t) * op.S * a.n_rows);
   op.coef.alloc(sizeof(T) * 2 * sp.G * op.S * a.n_rows);
   k_fold<T><<<nblocks(a.n_rows, TB), TB, 0, s>>>(a, counts.as<int>(), op.S, op.cell.as<int32_t>(), op.coef.as<T>(),
                                                 flag.as<int>());
   STL_CUDA(cudaGetLastError());
-  // transposed gather table
-  op.shift = 1;
-  while ((1 << op.shift) < op.S) ++op.shift;
-  if ((uint64_t)(a.n_rows - 1) >= ((uint64_t)1 << (32 - op.shift)) - 1)
+  // transposed gather table over the stored cells: entries (u, s, j)
+  int sbits = 1;
+  while ((1 << sbits) < op.S) ++sbits;
+  op.tshift = sbits + 2;
+  if ((uint64_t)std::max<i64>(a.n_rows - 1, 0) >= ((uint64_t)1 << (32 - op.tshift)) - 1)
     throw std::runtime_error("level too large for the 32-bit transposed table");
-  DevMem tcount(sizeof(int) * a.n_in), tfill(sizeof(int) * a.n_in);
+  const i64 n_cells = sym ? a.n_in / 4 : a.n_in;  // stored cells == stored rows on the full sky
+  if (sym && n_cells != a.n_rows) throw std::runtime_error("symmetric operator needs rows == cells");
+  DevMem tcount(sizeof(int) * n_cells), tfill(sizeof(int) * n_cells);
   STL_CUDA(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
   STL_CUDA(cudaMemsetAsync(tfill.p, 0, tfill.bytes, s));
-  k_tcount<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, op.S,
-                                                   tcount.as<int>());
+  k_conv_tcount<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, a.sym,
+                                                       a.sym_o2, tcount.as<int>());
   STL_CUDA(cudaGetLastError());
-  op.ST = std::max(1, device_max(tcount.as<int>(), a.n_in, s));
-  op.tent.alloc(sizeof(uint32_t) * op.ST * a.n_in);
-  k_tfill<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, op.S, op.shift,
-                                                  a.n_in, tfill.as<int>(), op.tent.as<uint32_t>());
+  op.ST = std::max(1, device_max(tcount.as<int>(), n_cells, s));
+  if (!sym && n_cells != a.n_rows) {
+    // partial grids keep the transposed table over the grid cells
+    throw std::runtime_error("rows and grid must coincide");
+  }
+  op.tent.alloc(sizeof(uint32_t) * op.ST * n_cells);
+  k_conv_tfill<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, a.sym,
+                                                      a.sym_o2, op.tshift, tfill.as<int>(), op.tent.as<uint32_t>());
   STL_CUDA(cudaGetLastError());
-  k_tsort<<<nblocks(a.n_in, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), tcount.as<int>(), a.n_in, op.ST);
+  k_tsort<<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), tcount.as<int>(), n_cells, op.ST);
+  STL_CUDA(cudaGetLastError());
+  op.coefT.alloc(sizeof(T) * 8 * op.ST * n_cells);
+  k_conv_coefT<T><<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), op.coef.as<T>(), n_cells, op.ST,
+                                                        op.tshift, op.coefT.as<T>());
   STL_CUDA(cudaGetLastError());
   STL_CUDA(cudaStreamSynchronize(s));
 }
@@ -410,14 +508,23 @@ void build_conv(const ConvSpec& spec, const std::vector<double>& kernel, DType d
 
 template <typename T>
 static void build_dec_t(const DecSpec& sp, DecOp& op, cudaStream_t s) {
+  const bool sym = sp.symmetric && sp.d_ids == nullptr && sp.d_out == nullptr && sp.nside >= 2;
   DecArgs a;
   a.nside = sp.nside; a.order = order_of(sp.nside); a.corder = order_of(sp.nside / 2);
   a.ids = sp.d_ids; a.n_in = sp.d_ids ? sp.n_in : npix_of(sp.nside);
-  a.out = sp.d_out; a.n_out = sp.d_out ? sp.n_out : npix_of(sp.nside / 2);
+  a.out = sp.d_out;
+  i64 n_out = sp.d_out ? sp.n_out : npix_of(sp.nside / 2);
+  a.n_out = sym ? n_out / 4 : n_out;
+  a.sym = sym ? 1 : 0;
+  a.sym_co2 = 2 * a.corder;
   double pix_deg = std::sqrt(4.0 * kPi / (double)npix_of(sp.nside)) * (180.0 / kPi);
   a.radius = (3.0 * pix_deg) * (kPi / 180.0);
   a.sigma = a.radius / 2.0;
-  op.n_out = a.n_out; op.n_in = a.n_in;
+  op.n_out = n_out; op.n_in = a.n_in;
+  op.nk = sym ? 4 : 1;
+  op.o2 = 2 * a.order; op.co2 = 2 * a.corder;
+  op.n_rep_out = a.n_out;
+  op.n_rep_in = sym ? a.n_in / 4 : a.n_in;
   op.dtype = sizeof(T) == 8 ? DType::F64 : DType::F32;
   DevMem counts(sizeof(int) * std::max<i64>(a.n_out, 1)), flag(sizeof(int));
   STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
@@ -426,25 +533,29 @@ static void build_dec_t(const DecSpec& sp, DecOp& op, cudaStream_t s) {
   STL_CUDA(cudaGetLastError());
   if (read_flag(flag, s)) throw std::runtime_error("a decimation row has more candidates than the builder holds");
   op.W = std::max(1, device_max(counts.as<int>(), a.n_out, s));
+  op.mean_w = device_mean(counts.as<int>(), a.n_out, s);
   op.col.alloc(sizeof(int32_t) * op.W * a.n_out);
   op.w.alloc(sizeof(T) * op.W * a.n_out);
   k_dec_rows<T><<<nblocks(a.n_out, TB), TB, 0, s>>>(a, counts.as<int>(), op.W, op.col.as<int32_t>(), op.w.as<T>(),
                                                    flag.as<int>());
   STL_CUDA(cudaGetLastError());
-  DevMem tcount(sizeof(int) * a.n_in), tfill(sizeof(int) * a.n_in);
+  const i64 n_cells = op.n_rep_in;
+  const int fine_o2 = op.o2, symi = sym ? 1 : 0;
+  DevMem tcount(sizeof(int) * n_cells), tfill(sizeof(int) * n_cells);
   STL_CUDA(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
   STL_CUDA(cudaMemsetAsync(tfill.p, 0, tfill.bytes, s));
-  k_tcount<<<nblocks(a.n_out, 256), 256, 0, s>>>(op.col.as<int32_t>(), counts.as<int>(), a.n_out, op.W,
-                                                  tcount.as<int>());
+  k_dec_tcount<<<nblocks(a.n_out, 256), 256, 0, s>>>(op.col.as<int32_t>(), counts.as<int>(), a.n_out, symi, fine_o2,
+                                                      tcount.as<int>());
   STL_CUDA(cudaGetLastError());
-  op.WT = std::max(1, device_max(tcount.as<int>(), a.n_in, s));
-  op.tcol.alloc(sizeof(int32_t) * op.WT * a.n_in);
-  op.tw.alloc(sizeof(T) * op.WT * a.n_in);
+  op.WT = std::max(1, device_max(tcount.as<int>(), n_cells, s));
+  op.tcol.alloc(sizeof(int32_t) * op.WT * n_cells);
+  op.tw.alloc(sizeof(T) * op.WT * n_cells);
   k_dec_tfill<T><<<nblocks(a.n_out, 256), 256, 0, s>>>(op.col.as<int32_t>(), op.w.as<T>(), counts.as<int>(), a.n_out,
-                                                       a.n_in, tfill.as<int>(), op.tcol.as<int32_t>(), op.tw.as<T>());
+                                                       n_cells, symi, fine_o2, op.co2, tfill.as<int>(),
+                                                       op.tcol.as<int32_t>(), op.tw.as<T>());
   STL_CUDA(cudaGetLastError());
-  k_dec_tsort<T><<<nblocks(a.n_in, 256), 256, 0, s>>>(op.tcol.as<int32_t>(), op.tw.as<T>(), tcount.as<int>(), a.n_in,
-                                                      op.WT);
+  k_dec_tsort<T><<<nblocks(n_cells, 256), 256, 0, s>>>(op.tcol.as<int32_t>(), op.tw.as<T>(), tcount.as<int>(),
+                                                       n_cells, op.WT);
   STL_CUDA(cudaGetLastError());
   STL_CUDA(cudaStreamSynchronize(s));
 }

@@ -1,12 +1,20 @@
 // Compute kernels of the engine's level sweeps (sm_100a).
 //
-//  conv_forward  y[r, g, :] = sum_s coef[s, p, g] x[r, cell[s, p]]   (+ |y|)
-//  conv_adjoint  gx[r, c]   = sum over the (p, s) reading c of coef[s, p] . gy[r, :, p]
+// Fields are pixel-major: a level's field holds, per pixel, a contiguous
+// vector of rows (maps [N][B]; moduli [N][B][n+1][L]; complex wavelet
+// outputs [N][R][4 gauges] interleaved (re, im)), so the gathers of the
+// stencils read whole row vectors of a cell.
+//
+//  conv_forward  out[p][r][g] = sum_s coef[s][p][g] x[cell(p, s)][r]   (+ |out|)
+//  conv_adjoint  gx[c][r]     = sum over the (p, s) reading c of coef[s][p] . gy[p][r]
 //  dec_apply     y = D x or D^T x over ELL rows
 //  products      the coefficient sums of one level (FP64) and their VJP
 //
-// Every reduction has a fixed order (no floating-point atomics): results
-// are bit-reproducible run to run.
+// On the full sky the operators are stored for faces 0, 4, 8 and every
+// thread evaluates the 4 rotated pixels (ConvOp in engine.cuh).  Every
+// reduction has a fixed order (no floating-point atomics): results are
+// bit-reproducible run to run.
+#include <algorithm>
 #include <cstdio>
 
 #include "engine.cuh"
@@ -21,7 +29,19 @@ template <typename T> struct V2;
 template <> struct V2<float> { typedef float2 type; };
 template <> struct V2<double> { typedef double2 type; };
 
-// 8 coefficients of one (slot, row): float4 x 2 or double2 x 4
+constexpr uint32_t kSentinel = 0xFFFFFFFFu;
+
+// pixel of rotation k of stored index u (full sky: faces 4 (u >> o2) + k)
+__device__ __forceinline__ i64 rot_pixel(i64 u, int k, int o2) {
+  return ((4 * (u >> o2) + k) << o2) | (u & ((i64(1) << o2) - 1));
+}
+// cell c rotated by k within its ring of faces
+__device__ __forceinline__ i64 rot_cell(i64 c, int k, int o2) {
+  i64 f = c >> o2;
+  return (((f & ~i64(3)) | ((f + k) & 3)) << o2) | (c & ((i64(1) << o2) - 1));
+}
+
+// 8 values of one (slot, row): float4 x 2 or double2 x 4
 __device__ __forceinline__ void load8(const float* p, float w[8]) {
   float4 a = __ldg(reinterpret_cast<const float4*>(p));
   float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
@@ -34,419 +54,623 @@ __device__ __forceinline__ void load8(const double* p, double w[8]) {
     w[2 * k] = a.x; w[2 * k + 1] = a.y;
   }
 }
+__device__ __forceinline__ void store8(float* p, const float w[8]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(w[0], w[1], w[2], w[3]);
+  reinterpret_cast<float4*>(p)[1] = make_float4(w[4], w[5], w[6], w[7]);
+}
+__device__ __forceinline__ void store8(double* p, const double w[8]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) reinterpret_cast<double2*>(p)[k] = make_double2(w[2 * k], w[2 * k + 1]);
+}
 
-// One thread per (output row, RB input rows).  out row r, gauge g, pixel p
-// at out + r * out_row_stride + (g * n_rows + p) * 2 (complex, interleaved).
-template <typename T, int RB>
+// RB consecutive values of a row vector (RB in 1, 2, 4)
+template <int RB>
+__device__ __forceinline__ void loadR(const float* p, float v[RB]) {
+  if (RB == 4) {
+    float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  } else if (RB == 2) {
+    float2 a = __ldg(reinterpret_cast<const float2*>(p));
+    v[0] = a.x; v[1] = a.y;
+  } else {
+    v[0] = __ldg(p);
+  }
+}
+template <int RB>
+__device__ __forceinline__ void loadR(const double* p, double v[RB]) {
+  if (RB >= 2) {
+#pragma unroll
+    for (int k = 0; k < RB / 2; ++k) {
+      double2 a = __ldg(reinterpret_cast<const double2*>(p) + k);
+      v[2 * k] = a.x; v[2 * k + 1] = a.y;
+    }
+  } else {
+    v[0] = __ldg(p);
+  }
+}
+
+// gauge map of rotation k: output gauge g of pixel (4m + k) takes the
+// stored gauge (g + 2k) mod 4, conjugated when ((2k - g + 3) >> 2) is odd
+__host__ __device__ constexpr int rot_src(int k, int g) { return (g + 2 * k) & 3; }
+__host__ __device__ constexpr int rot_conj(int k, int g) { return ((2 * k - g + 3) >> 2) & 1; }
+
+// ---- forward ----------------------------------------------------------------
+// One thread per (stored row u, chunk of RB input rows); NK rotations per
+// thread.  threadIdx.x runs over the chunks of a row vector, threadIdx.y over
+// stored rows, so a warp reads whole row vectors of the cells it gathers.
+template <typename T, int NK, int RB>
 __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ cell, const T* __restrict__ coef, int S,
-                                                  i64 n_rows, const T* __restrict__ x, i64 n_in, int R,
-                                                  T* __restrict__ out, i64 out_row_stride, T* __restrict__ mod_out,
-                                                  i64 mod_row_stride) {
-  i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_rows) return;
-  int r0 = blockIdx.y * RB;
-  T acc[RB][8];
+                                                  i64 n_rep, int o2, const T* __restrict__ x, int R,
+                                                  T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row,
+                                                  int mod_off) {
+  const i64 u = (i64)blockIdx.x * blockDim.y + threadIdx.y;
+  const int chunk = blockIdx.y * blockDim.x + threadIdx.x;
+  if (u >= n_rep || chunk * RB >= R) return;
+  const int r0 = chunk * RB;
+  T acc[NK][RB][8];
 #pragma unroll
-  for (int rb = 0; rb < RB; ++rb)
+  for (int k = 0; k < NK; ++k)
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc[rb][k] = (T)0;
-  const T* xr[RB];
+    for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
-  for (int rb = 0; rb < RB; ++rb) xr[rb] = x + (i64)min(r0 + rb, R - 1) * n_in;
+      for (int j = 0; j < 8; ++j) acc[k][rb][j] = (T)0;
   for (int s = 0; s < S; ++s) {
-    i64 e = (i64)s * n_rows + p;
-    int c = __ldg(cell + e);
+    const i64 e = (i64)s * n_rep + u;
+    const i64 c = __ldg(cell + e);
     T w[8];
     load8(coef + e * 8, w);
 #pragma unroll
-    for (int rb = 0; rb < RB; ++rb) {
-      T xv = __ldg(xr[rb] + c);
+    for (int k = 0; k < NK; ++k) {
+      const i64 ck = NK == 1 ? c : rot_cell(c, k, o2);
+      T xv[RB];
+      loadR<RB>(x + ck * R + r0, xv);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) acc[rb][k] = fma(w[k], xv, acc[rb][k]);
+      for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[k][rb][j] = fma(w[j], xv[rb], acc[k][rb][j]);
     }
   }
 #pragma unroll
-  for (int rb = 0; rb < RB; ++rb) {
-    int r = r0 + rb;
-    if (r >= R) break;
-    typedef typename V2<T>::type T2;
-    T2* o = reinterpret_cast<T2*>(out + (i64)r * out_row_stride);
-#pragma unroll
-    for (int g = 0; g < 4; ++g) {
-      T2 v;
-      v.x = acc[rb][2 * g];
-      v.y = acc[rb][2 * g + 1];
-      o[(i64)g * n_rows + p] = v;
-      if (mod_out) mod_out[(i64)r * mod_row_stride + (i64)g * n_rows + p] = hypot(v.x, v.y);
-    }
-  }
-}
-
-// One thread per (input cell, RB cotangent rows); gy row r, gauge g, row p
-// at gy + r * gy_row_stride + (g * n_rows + p) * 2.
-template <typename T, int RB>
-__global__ void __launch_bounds__(128) k_conv_adj(const uint32_t* __restrict__ tent, int ST, int shift, i64 n_in,
-                                                  const T* __restrict__ coef, i64 n_rows, const T* __restrict__ gy,
-                                                  i64 gy_row_stride, int R, T* __restrict__ gx, int accumulate) {
-  i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n_in) return;
-  int r0 = blockIdx.y * RB;
-  const uint32_t mask = (1u << shift) - 1u;
-  T acc[RB];
-#pragma unroll
-  for (int rb = 0; rb < RB; ++rb) acc[rb] = (T)0;
-  typedef typename V2<T>::type T2;
-  const T2* gr[RB];
-#pragma unroll
-  for (int rb = 0; rb < RB; ++rb) gr[rb] = reinterpret_cast<const T2*>(gy + (i64)min(r0 + rb, R - 1) * gy_row_stride);
-  for (int q = 0; q < ST; ++q) {
-    uint32_t v = __ldg(tent + (i64)q * n_in + c);
-    if (v == 0xFFFFFFFFu) break;
-    i64 row = (i64)(v >> shift);
-    int s = (int)(v & mask);
-    T w[8];
-    load8(coef + ((i64)s * n_rows + row) * 8, w);
+  for (int k = 0; k < NK; ++k) {
+    const i64 p = NK == 1 ? u : rot_pixel(u, k, o2);
 #pragma unroll
     for (int rb = 0; rb < RB; ++rb) {
+      const int r = r0 + rb;
+      T o[8];
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
-        T2 gv = gr[rb][(i64)g * n_rows + row];
-        acc[rb] = fma(w[2 * g], gv.x, acc[rb]);
-        acc[rb] = fma(w[2 * g + 1], gv.y, acc[rb]);
+        const int src = NK == 1 ? g : rot_src(k, g);
+        const bool cj = NK == 1 ? false : rot_conj(k, g);
+        o[2 * g] = acc[k][rb][2 * src];
+        o[2 * g + 1] = cj ? -acc[k][rb][2 * src + 1] : acc[k][rb][2 * src + 1];
+      }
+      store8(out + (p * R + r) * 8, o);
+      if (mod) {
+        T* m = mod + p * mod_pix + (i64)r * mod_row + mod_off;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) m[g] = hypot(o[2 * g], o[2 * g + 1]);
+      }
+    }
+  }
+}
+
+// ---- adjoint ----------------------------------------------------------------
+// dot of stored coefficients w (rotation k applied) with a cotangent g8
+template <typename T, int K>
+__device__ __forceinline__ T rot_dot(const T w[8], const T g8[8]) {
+  T a = (T)0;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    const int src = rot_src(K, g);
+    a = fma(w[2 * src], g8[2 * g], a);
+    a = rot_conj(K, g) ? fma(-w[2 * src + 1], g8[2 * g + 1], a) : fma(w[2 * src + 1], g8[2 * g + 1], a);
+  }
+  return a;
+}
+
+// One thread per (stored cell v, RB cotangent rows): for each transposed
+// entry (u, j) -- stored row u reads rotation j of v -- rotation k of row
+// u reads rotation (k + j) mod 4 of v.
+template <typename T, int NK, int RB>
+__global__ void __launch_bounds__(128) k_conv_adj(const uint32_t* __restrict__ tent, const T* __restrict__ coefT,
+                                                  int ST, int tshift, i64 n_rep, int o2, const T* __restrict__ gy,
+                                                  int R, T* __restrict__ gx, int accumulate) {
+  const i64 v = (i64)blockIdx.x * blockDim.y + threadIdx.y;
+  const int chunk = blockIdx.y * blockDim.x + threadIdx.x;
+  if (v >= n_rep || chunk * RB >= R) return;
+  const int r0 = chunk * RB;
+  T acc[NK][RB];
+#pragma unroll
+  for (int k = 0; k < NK; ++k)
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) acc[k][rb] = (T)0;
+  for (int q = 0; q < ST; ++q) {
+    const i64 e = (i64)q * n_rep + v;
+    const uint32_t ent = __ldg(tent + e);
+    if (ent == kSentinel) break;
+    const i64 u = (i64)(ent >> tshift);
+    const int j = (int)(ent & 3u);
+    T w[8];
+    load8(coefT + e * 8, w);
+    T d[NK][RB];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      const i64 p = NK == 1 ? u : rot_pixel(u, k, o2);
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) {
+        T g8[8];
+        load8(gy + (p * R + r0 + rb) * 8, g8);
+        d[k][rb] = k == 0 ? rot_dot<T, 0>(w, g8)
+                          : (k == 1 ? rot_dot<T, 1>(w, g8) : (k == 2 ? rot_dot<T, 2>(w, g8) : rot_dot<T, 3>(w, g8)));
+      }
+    }
+    if (NK == 1) {
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) acc[0][rb] += d[0][rb];
+    } else {
+      // rotation k of u reads rotation (k + j) of v: rotate d by j
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) {
+        T t0 = d[0][rb], t1 = d[NK > 1 ? 1 : 0][rb], t2 = d[NK > 2 ? 2 : 0][rb], t3 = d[NK > 3 ? 3 : 0][rb];
+        if (j & 1) { T t = t3; t3 = t2; t2 = t1; t1 = t0; t0 = t; }
+        if (j & 2) { T a = t0, b = t1; t0 = t2; t1 = t3; t2 = a; t3 = b; }
+        acc[0][rb] += t0;
+        acc[NK > 1 ? 1 : 0][rb] += t1;
+        acc[NK > 2 ? 2 : 0][rb] += t2;
+        acc[NK > 3 ? 3 : 0][rb] += t3;
       }
     }
   }
 #pragma unroll
-  for (int rb = 0; rb < RB; ++rb) {
-    int r = r0 + rb;
-    if (r >= R) break;
-    T* o = gx + (i64)r * n_in + c;
-    *o = accumulate ? *o + acc[rb] : acc[rb];
+  for (int k = 0; k < NK; ++k) {
+    const i64 c = NK == 1 ? v : rot_pixel(v, k, o2);
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+      T* o = gx + c * R + r0 + rb;
+      *o = accumulate ? *o + acc[k][rb] : acc[k][rb];
+    }
   }
 }
 
-// y[ro][ri][c] (+)= sum_k w[k][c] x[ro][ri][col[k][c]]
-template <typename T>
-__global__ void k_ell(const int32_t* __restrict__ col, const T* __restrict__ w, int W, i64 n_out, i64 n_in,
-                      const T* __restrict__ x, i64 x_outer, T* __restrict__ y, i64 y_outer, int accumulate) {
-  i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n_out) return;
-  const T* xr = x + (i64)blockIdx.z * x_outer + (i64)blockIdx.y * n_in;
-  T* yr = y + (i64)blockIdx.z * y_outer + (i64)blockIdx.y * n_out;
-  T s = (T)0;
-  for (int k = 0; k < W; ++k) {
-    i64 e = (i64)k * n_out + c;
-    s = fma(__ldg(w + e), __ldg(xr + __ldg(col + e)), s);
+// ---- decimation ---------------------------------------------------------------
+// y[c][ro][ri] (+)= sum_e w[e][c] x[col[e][c]][ro][ri]; one thread per (stored
+// row u, chunk of RB rows of the R_outer x R_inner rows), NK rotations per
+// thread; threadIdx.x runs over the chunks of a pixel's rows.
+template <typename T, int NK, int RB>
+__global__ void k_ell(const int32_t* __restrict__ col, const T* __restrict__ w, int W, i64 n_rep, int o2_out,
+                      int o2_in, const T* __restrict__ x, int x_pix, int x_outer, T* __restrict__ y, int y_pix,
+                      int y_outer, int R_outer, int R_inner, int accumulate) {
+  const i64 u = (i64)blockIdx.x * blockDim.y + threadIdx.y;
+  const int chunk = blockIdx.y * blockDim.x + threadIdx.x;
+  const int per = R_inner / RB;
+  if (u >= n_rep || chunk >= R_outer * per) return;
+  const int ro = chunk / per, ri = (chunk % per) * RB;
+  T acc[NK][RB];
+#pragma unroll
+  for (int k = 0; k < NK; ++k)
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) acc[k][rb] = (T)0;
+  for (int e = 0; e < W; ++e) {
+    const i64 idx = (i64)e * n_rep + u;
+    const T we = __ldg(w + idx);
+    const i64 c = __ldg(col + idx);
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      const i64 ck = NK == 1 ? c : rot_cell(c, k, o2_in);
+      T xv[RB];
+      loadR<RB>(x + ck * x_pix + (i64)ro * x_outer + ri, xv);
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) acc[k][rb] = fma(we, xv[rb], acc[k][rb]);
+    }
   }
-  yr[c] = accumulate ? yr[c] + s : s;
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const i64 p = NK == 1 ? u : rot_pixel(u, k, o2_out);
+    T* yr = y + p * y_pix + (i64)ro * y_outer + ri;
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) yr[rb] = accumulate ? yr[rb] + acc[k][rb] : acc[k][rb];
+  }
 }
 
-// gz[b][e] += g[b][e] z/|z| (0 at z = 0), e over L * N complex values
+// gz[p][b][l] += g[p][b][l] z/|z| (0 at z = 0); g at g + p g_pix + b g_row + l
 template <typename T>
-__global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, i64 g_outer, T* __restrict__ gz,
-                         i64 plane) {
-  i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= plane) return;
-  i64 b = blockIdx.y;
-  i64 zi = (b * plane + e) * 2;
-  T zr = z[zi], zm = z[zi + 1];
-  T mag = hypot(zr, zm);
-  T gv = g[b * g_outer + e];
-  T d = mag == (T)0 ? (T)1 : mag;
-  gz[zi] += gv * zr / d;
-  gz[zi + 1] += gv * zm / d;
+__global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, int g_pix, int g_row, T* __restrict__ gz,
+                         i64 N, int B, int L) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over N * B * L
+  if (i >= N * B * L) return;
+  const i64 p = i / (B * L);
+  const int b = (int)((i / L) % B), l = (int)(i % L);
+  const T zr = z[2 * i], zm = z[2 * i + 1];
+  const T mag = hypot(zr, zm);
+  const T gv = g[p * g_pix + (i64)b * g_row + l];
+  const T dd = mag == (T)0 ? (T)1 : mag;
+  gz[2 * i] += gv * zr / dd;
+  gz[2 * i + 1] += gv * zm / dd;
 }
 
-// ---- coefficient products --------------------------------------------------
+// ---- coefficient products --------------------------------------------------------
 //
 // Per level n, map b and orientation l3, the operand vector of a pixel is
-// v = (branch[d][l1][l3] for d <= n, l1 < L; z[l3]), K = (n + 1) L + 1
-// complex values.  Every S3/S4 coefficient of the level is an entry of the
-// Hermitian Gram matrix sum_p v v^H (S3: (branch, z); S4: (branch,
-// branch)), S2 its (z, z) entry.  A block owns (b, l3) and a set of
-// 128-pixel sub-chunks; work items are (Gram entry i <= j, pixel subgroup).
-// Sums are FP64 from the FP32 or FP64 operands.  Partial layout per block
-// (doubles): [2 E] complex entries (i-major upper triangle), [E] second
-// moments sum |v_i|^2 |v_j|^2, then sum |z|, sum |z|^4, and at level 0 (l3 =
-// 0 blocks) sum x, sum x^2, sum x^4.
-constexpr int kPC = 128;  // pixels per sub-chunk
-constexpr int kPT = 256;  // threads of a products block
+// v = (branch[d][l1][l3] for d <= n, l1 < L; z[l3]).  Every S3/S4
+// coefficient of the level is an entry of the Hermitian Gram matrix
+// sum_p v v^H: S4 in the 4 x 4 blocks (d1, d2), d1 <= d2, of the branches,
+// S3 in the blocks (d, z), S2 its (z, z) entry.  Work items, for every l3:
+// the (d1, d2) blocks, the (d, z) blocks and one item for the per-pixel sums
+// (|z|, |z|^2, |z|^4 and, at level 0, x, x^2, x^4).  One warp per item,
+// one lane per pixel of a 32-pixel tile staged in shared memory; sums in
+// FP64 (products of the FP32 or FP64 operands), reduced across lanes and
+// then across blocks in a fixed order.  Partial layout per (block, b, l3), in
+// doubles:
+//   BB block t (d1 <= d2, d1-major): [t 48 .. +32) 16 complex (l1, l2)
+//                                    [t 48 + 32 .. +16) 16 sums |a|^2 |b|^2
+//   Bz block d: [nBB 48 + 12 d .. +8) 4 complex (l1, z), then 4 second sums
+//   z item:     [nBB 48 + 12 (n + 1) .. +6) |z|, |z|^2, |z|^4, x, x^2, x^4
+constexpr int kTile = 32;        // pixels per tile
+constexpr int kTileP = kTile + 1;  // padded tile stride in shared memory
 
+// stage v[l][i][px] (i < K1: branch i; i == K1: z) of the tile at p0
 template <typename T>
-__global__ void __launch_bounds__(kPT) k_products(int K, int L, i64 N, int nsub, const T* __restrict__ z,
-                                                  const T* __restrict__ br, const T* __restrict__ x0, int Q,
-                                                  double* __restrict__ partials, int slots) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void stage_tile(typename V2<T>::type* v, int stride, int K1, int L, int B, int b, i64 p0,
+                                           i64 N, int np, const T* br, const T* z) {
   typedef typename V2<T>::type T2;
-  T2* v = reinterpret_cast<T2*>(smem);                                   // [K][kPC]
-  double* u = reinterpret_cast<double*>(v + (size_t)K * kPC);           // [K][kPC] |v|^2
-  double* red = u + (size_t)K * kPC;                                     // [kPT] scratch
-  const int b = blockIdx.z, l3 = blockIdx.y, tid = threadIdx.x;
-  const int E = K * (K + 1) / 2;
-  const int items = E * Q;
-  const int per = kPC / Q;
-  const int nb = K - 1;  // branches
-  const T2* zr = reinterpret_cast<const T2*>(z) + ((i64)b * L + l3) * N;
-  const T2* brb = reinterpret_cast<const T2*>(br) + (i64)b * nb * L * N;
-  constexpr int MAXI = 4;
-  double acc[MAXI][3];
-  int it_i[MAXI], it_j[MAXI], it_q[MAXI];
-  int nit = 0;
-  for (int it = tid; it < items && nit < MAXI; it += kPT, ++nit) {
-    int e = it % E, q = it / E;
-    int i = 0, rem = e;
-    while (rem >= K - i) { rem -= K - i; ++i; }
-    it_i[nit] = i; it_j[nit] = i + rem; it_q[nit] = q;
-    acc[nit][0] = acc[nit][1] = acc[nit][2] = 0.0;
-  }
-  double s_abs = 0.0, s_z4 = 0.0, s_x = 0.0, s_x2 = 0.0, s_x4 = 0.0;
-  const bool extra_x = x0 != nullptr && l3 == 0;
-  for (int sc = blockIdx.x; sc < nsub; sc += gridDim.x) {
-    i64 p0 = (i64)sc * kPC;
-    __syncthreads();
-    for (int idx = tid; idx < K * kPC; idx += kPT) {
-      int i = idx / kPC, px = idx % kPC;
-      i64 p = p0 + px;
-      T2 a;
-      a.x = (T)0; a.y = (T)0;
-      if (p < N) a = (i == nb) ? zr[p] : brb[((i64)i * L + l3) * N + p];
-      v[idx] = a;
-      u[idx] = (double)a.x * (double)a.x + (double)a.y * (double)a.y;
-    }
-    __syncthreads();
-    for (int k = 0; k < nit; ++k) {
-      const T2* vi = v + it_i[k] * kPC + it_q[k] * per;
-      const T2* vj = v + it_j[k] * kPC + it_q[k] * per;
-      const double* ui = u + it_i[k] * kPC + it_q[k] * per;
-      const double* uj = u + it_j[k] * kPC + it_q[k] * per;
-      double ar = 0.0, ai = 0.0, am = 0.0;
-      for (int px = 0; px < per; ++px) {
-        double xr = vi[px].x, xi = vi[px].y, yr = vj[px].x, yi = vj[px].y;
-        ar = fma(xr, yr, fma(xi, yi, ar));
-        ai = fma(xi, yr, fma(-xr, yi, ai));
-        am = fma(ui[px], uj[px], am);
-      }
-      acc[k][0] += ar; acc[k][1] += ai; acc[k][2] += am;
-    }
-    if (tid < kPC && p0 + tid < N) {
-      T2 zz = v[nb * kPC + tid];
-      double m = hypot((double)zz.x, (double)zz.y);
-      double m2 = m * m;
-      s_abs += m;
-      s_z4 += m2 * m2;
-      if (extra_x) {
-        double xv = (double)x0[(i64)b * N + p0 + tid];
-        double x2 = xv * xv;
-        s_x += xv; s_x2 += x2; s_x4 += x2 * x2;
-      }
-    }
-  }
-  __syncthreads();
-  double* out = partials + (((i64)b * L + l3) * gridDim.x + blockIdx.x) * slots;
-  // Gram entries: subgroup partials through shared memory, summed in q order
-  double* gs = reinterpret_cast<double*>(smem);  // reuse: [Q][E][3]
-  for (int k = 0; k < nit; ++k) {
-    int e = 0;
-    for (int r = 0; r < it_i[k]; ++r) e += K - r;
-    e += it_j[k] - it_i[k];
-    double* d = gs + ((size_t)it_q[k] * E + e) * 3;
-    d[0] = acc[k][0]; d[1] = acc[k][1]; d[2] = acc[k][2];
-  }
-  __syncthreads();
-  for (int e = tid; e < E; e += kPT) {
-    double r = 0.0, im = 0.0, m = 0.0;
-    for (int q = 0; q < Q; ++q) {
-      const double* d = gs + ((size_t)q * E + e) * 3;
-      r += d[0]; im += d[1]; m += d[2];
-    }
-    out[2 * e] = r; out[2 * e + 1] = im; out[2 * E + e] = m;
-  }
-  // per-pixel extras: fixed tree over the block
-  double ext[5] = {s_abs, s_z4, s_x, s_x2, s_x4};
-  for (int k = 0; k < 5; ++k) {
-    __syncthreads();
-    red[tid] = ext[k];
-    __syncthreads();
-    for (int w = kPT / 2; w > 0; w >>= 1) {
-      if (tid < w) red[tid] += red[tid + w];
-      __syncthreads();
-    }
-    if (tid == 0) out[3 * E + k] = red[0];
-  }
-}
-
-// sums[row][slot] = sum over blocks of partials[row][blk][slot] in block order
-__global__ void k_reduce_partials(const double* __restrict__ partials, int nblk, int slots, double* __restrict__ sums) {
-  i64 row = blockIdx.y;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
-    double a = 0.0;
-    const double* p = partials + row * (i64)nblk * slots + s;
-    for (int k = 0; k < nblk; ++k) a += p[(i64)k * slots];
-    sums[row * slots + s] = a;
-  }
-}
-
-// gv = M v per pixel (M: K x K complex of the coefficient cotangents of one
-// (b, l3)); gz additionally gets s1c z / |z| (auto S1).
-template <typename T>
-__global__ void __launch_bounds__(kPC) k_products_rev(int K, int L, i64 N, const T* __restrict__ z,
-                                                      const T* __restrict__ br, const T* __restrict__ M,
-                                                      const T* __restrict__ s1c, T* __restrict__ gz,
-                                                      T* __restrict__ gbr) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  typedef typename V2<T>::type T2;
-  T2* m = reinterpret_cast<T2*>(smem);  // [K][K]
-  T2* v = m + (size_t)K * K;            // [K][kPC]
-  const int b = blockIdx.z, l3 = blockIdx.y, tid = threadIdx.x;
-  const int nb = K - 1;
-  const T2* Mb = reinterpret_cast<const T2*>(M) + ((i64)b * L + l3) * K * K;
-  for (int i = tid; i < K * K; i += kPC) m[i] = Mb[i];
-  i64 p0 = (i64)blockIdx.x * kPC;
-  const T2* zr = reinterpret_cast<const T2*>(z) + ((i64)b * L + l3) * N;
-  const T2* brb = reinterpret_cast<const T2*>(br) + (i64)b * nb * L * N;
-  for (int idx = tid; idx < K * kPC; idx += kPC) {
-    int i = idx / kPC, px = idx % kPC;
-    i64 p = p0 + px;
+  const int K = K1 + 1;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  for (int idx = tid; idx < np * K * L; idx += nt) {
+    const int px = idx / (K * L), rem = idx % (K * L);
+    const int i = rem / L, l = rem % L;
+    const i64 p = p0 + px;
     T2 a;
     a.x = (T)0; a.y = (T)0;
-    if (p < N) a = (i == nb) ? zr[p] : brb[((i64)i * L + l3) * N + p];
-    v[idx] = a;
+    if (p < N) {
+      const T* src = i < K1 ? br + (((p * B + b) * K1 + i) * L + l) * 2 : z + ((p * B + b) * L + l) * 2;
+      a.x = src[0]; a.y = src[1];
+    }
+    v[(l * K + i) * stride + px] = a;
   }
+}
+
+__device__ __forceinline__ double warp_sum(double a) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+  return a;
+}
+
+// One block per (tile range, map b, item w): blockDim (32, L), warp y = l3,
+// lane = pixel of a 32-pixel tile.  The L warps read the same sectors of the
+// pixel-major fields (their l3 values interleave), which L1 shares.
+template <typename T>
+__global__ void __launch_bounds__(128) k_products(int nd, int L, i64 N, int B, const T* __restrict__ z,
+                                                  const T* __restrict__ br, const T* __restrict__ x0, int slots,
+                                                  int ntiles, double* __restrict__ partials) {
+  typedef typename V2<T>::type T2;
+  const int K1 = nd * L;
+  const int b = blockIdx.y, w = blockIdx.z, lane = threadIdx.x, l3 = threadIdx.y;
+  const int nBB = nd * (nd + 1) / 2;
+  int kind = 2, d1 = 0, d2 = 0;
+  if (w < nBB) {
+    kind = 0;
+    int t = w;
+    while (t >= nd - d1) { t -= nd - d1; ++d1; }
+    d2 = d1 + t;
+  } else if (w < nBB + nd) {
+    kind = 1;
+    d1 = w - nBB;
+  }
+  const T2* brv = reinterpret_cast<const T2*>(br);
+  const T2* zv = reinterpret_cast<const T2*>(z);
+  double acc[48];
+#pragma unroll
+  for (int i = 0; i < 48; ++i) acc[i] = 0.0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const i64 p = (i64)tile * kTile + lane;
+    if (p >= N) break;
+    const i64 row = (p * B + b) * K1;  // branch (d, l1) of (p, b) at row + d L + l1, gauge l3
+    if (kind == 0) {
+      double ar[4], ai[4], bR[4], bI[4], am[4], bm[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const T2 x = brv[(row + d1 * 4 + l) * L + l3], y = brv[(row + d2 * 4 + l) * L + l3];
+        ar[l] = x.x; ai[l] = x.y; bR[l] = y.x; bI[l] = y.y;
+        am[l] = ar[l] * ar[l] + ai[l] * ai[l];
+        bm[l] = bR[l] * bR[l] + bI[l] * bI[l];
+      }
+#pragma unroll
+      for (int l1 = 0; l1 < 4; ++l1)
+#pragma unroll
+        for (int l2 = 0; l2 < 4; ++l2) {
+          const int e = l1 * 4 + l2;
+          acc[2 * e] = fma(ar[l1], bR[l2], fma(ai[l1], bI[l2], acc[2 * e]));
+          acc[2 * e + 1] = fma(ai[l1], bR[l2], fma(-ar[l1], bI[l2], acc[2 * e + 1]));
+          acc[32 + e] = fma(am[l1], bm[l2], acc[32 + e]);
+        }
+    } else if (kind == 1) {
+      const T2 zz = zv[(p * B + b) * L + l3];
+      const double zr = zz.x, zi = zz.y, zm = zr * zr + zi * zi;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const T2 x = brv[(row + d1 * 4 + l) * L + l3];
+        const double xr = x.x, xi = x.y;
+        acc[2 * l] = fma(xr, zr, fma(xi, zi, acc[2 * l]));
+        acc[2 * l + 1] = fma(xi, zr, fma(-xr, zi, acc[2 * l + 1]));
+        acc[8 + l] = fma(xr * xr + xi * xi, zm, acc[8 + l]);
+      }
+    } else {
+      const T2 zz = zv[(p * B + b) * L + l3];
+      const double m = hypot((double)zz.x, (double)zz.y);
+      const double m2 = m * m;
+      acc[0] += m;
+      acc[1] += m2;
+      acc[2] += m2 * m2;
+      if (x0 && l3 == 0) {
+        const double xv = (double)x0[p * B + b];
+        const double x2 = xv * xv;
+        acc[3] += xv;
+        acc[4] += x2;
+        acc[5] += x2 * x2;
+      }
+    }
+  }
+  const int n_i = kind == 0 ? 48 : (kind == 1 ? 12 : 6);
+  const int base = kind == 0 ? w * 48 : (kind == 1 ? nBB * 48 + (w - nBB) * 12 : nBB * 48 + nd * 12);
+  double* out = partials + (((i64)blockIdx.x * B + b) * L + l3) * slots + base;
+#pragma unroll
+  for (int i = 0; i < 48; ++i) {
+    if (i >= n_i) break;
+    const double t = warp_sum(acc[i]);
+    if (lane == 0) out[i] = t;
+  }
+}
+
+// sums[row][slot] = sum over blocks of partials[blk][row][slot] in block order
+__global__ void k_reduce_partials(const double* __restrict__ partials, int nblk, int rows, int slots,
+                                  double* __restrict__ sums) {
+  const i64 total = (i64)rows * slots;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (i64)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int k = 0; k < nblk; ++k) a += partials[(i64)k * total + i];
+    sums[i] = a;
+  }
+}
+
+// gv = M v per pixel and l3 (M: K x K complex of the coefficient cotangents
+// of one (b, l3)); gz additionally gets s1c z / |z| (auto S1).  Block: TP
+// pixels (threadIdx.x) x L orientations (threadIdx.y); the tile is staged in
+// shared memory both ways so global accesses stay coalesced.
+template <typename T>
+__global__ void k_products_rev(int nd, int L, i64 N, int B, int TP, const T* __restrict__ z, const T* __restrict__ br,
+                               const T* __restrict__ M, const T* __restrict__ s1c, T* __restrict__ gz,
+                               T* __restrict__ gbr) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  typedef typename V2<T>::type T2;
+  const int K1 = nd * L, K = K1 + 1;
+  const int st = TP + 1;                    // padded tile stride
+  T2* m = reinterpret_cast<T2*>(smem);      // [L][K][K]
+  T2* v = m + (size_t)L * K * K;            // [L][K][st]
+  T2* gv = v + (size_t)L * K * st;          // [L][K][st]
+  const int b = blockIdx.y, px = threadIdx.x, l3 = threadIdx.y;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  const T2* Mb = reinterpret_cast<const T2*>(M) + (i64)b * L * K * K;
+  for (int i = tid; i < L * K * K; i += nt) m[i] = Mb[i];
+  const i64 p0 = (i64)blockIdx.x * TP;
+  stage_tile<T>(v, st, K1, L, B, b, p0, N, TP, br, z);
   __syncthreads();
-  i64 p = p0 + tid;
-  if (p >= N) return;
-  T2* gzr = reinterpret_cast<T2*>(gz) + ((i64)b * L + l3) * N;
-  T2* gbb = reinterpret_cast<T2*>(gbr) + (i64)b * nb * L * N;
+  const T2* ml = m + (size_t)l3 * K * K;
+  const T2* vl = v + (size_t)l3 * K * st;
   for (int i = 0; i < K; ++i) {
     T ar = (T)0, ai = (T)0;
     for (int j = 0; j < K; ++j) {
-      T2 mm = m[i * K + j], vv = v[j * kPC + tid];
+      const T2 mm = ml[i * K + j], vv = vl[j * st + px];
       ar = fma(mm.x, vv.x, fma(-mm.y, vv.y, ar));
       ai = fma(mm.x, vv.y, fma(mm.y, vv.x, ai));
     }
-    T2 o;
-    if (i < nb) {
-      o.x = ar; o.y = ai;
-      gbb[((i64)i * L + l3) * N + p] = o;
-    } else {
-      T2 zz = v[nb * kPC + tid];
-      T mag = hypot(zz.x, zz.y);
-      T c = s1c[(i64)b * L + l3] / (mag == (T)0 ? (T)1 : mag);
-      o.x = ar + c * zz.x;
-      o.y = ai + c * zz.y;
-      gzr[p] = o;
+    if (i == K1) {
+      const T2 zz = vl[K1 * st + px];
+      const T mag = hypot(zz.x, zz.y);
+      const T c = s1c[(i64)b * L + l3] / (mag == (T)0 ? (T)1 : mag);
+      ar += c * zz.x;
+      ai += c * zz.y;
     }
+    T2 o;
+    o.x = ar; o.y = ai;
+    gv[((size_t)l3 * K + i) * st + px] = o;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < TP * K * L; idx += nt) {
+    const int q = idx / (K * L), rem = idx % (K * L);
+    const int i = rem / L, l = rem % L;
+    const i64 p = p0 + q;
+    if (p >= N) continue;
+    const T2 o = gv[((size_t)l * K + i) * st + q];
+    T* dst = i < K1 ? gbr + (((p * B + b) * K1 + i) * L + l) * 2 : gz + ((p * B + b) * L + l) * 2;
+    dst[0] = o.x;
+    dst[1] = o.y;
   }
 }
 
 template <typename T>
-__global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ coefs, i64 N, T* __restrict__ gx) {
-  i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
-  i64 b = blockIdx.y;
-  double c0 = coefs[2 * b], c1 = coefs[2 * b + 1];
-  gx[b * N + p] += (T)(c0 + c1 * (double)x0[b * N + p]);
+__global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ coefs, i64 N, int B,
+                                T* __restrict__ gx) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * B) return;
+  const int b = (int)(i % B);
+  gx[i] += (T)(coefs[2 * b] + coefs[2 * b + 1] * (double)x0[i]);
 }
 
 template <typename Tin, typename Tout>
 __global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, i64 n) {
-  i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (Tout)in[i];
+}
+
+// [B][N] <-> [N][B] transposes of the level-0 maps at the boundary
+template <typename Tin, typename Tout>
+__global__ void k_to_pixel_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over N * B, output order
+  if (i >= N * B) return;
+  const i64 p = i / B;
+  const int b = (int)(i % B);
+  out[i] = (Tout)in[(i64)b * N + p];
+}
+template <typename Tin, typename Tout>
+__global__ void k_to_map_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over B * N, output order
+  if (i >= N * B) return;
+  const int b = (int)(i / N);
+  const i64 p = i % N;
+  out[i] = (Tout)in[p * B + b];
+}
+
+// CTA of 128 threads: blockDim.x = chunks of a row vector handled together
+// (all of them up to 32), blockDim.y = stored rows.
+inline dim3 cta_shape(int chunks) {
+  int c = 1;
+  while (c < chunks && c < 32) c *= 2;
+  return dim3(c, 128 / c);
+}
+
+template <typename T, int NK, int RB>
+void conv_forward_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
+                     cudaStream_t s) {
+  const int chunks = R / RB;
+  dim3 b = cta_shape(chunks);
+  dim3 grid(nblocks(op.n_rep, b.y), (chunks + b.x - 1) / b.x);
+  k_conv_fwd<T, NK, RB><<<grid, b, 0, s>>>(op.cell.as<int32_t>(), op.coef.as<T>(), op.S, op.n_rep, op.o2, x, R, out,
+                                           mod, mod_pix, mod_row, mod_off);
+}
+
+template <typename T, int NK>
+void conv_forward_nk(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
+                     cudaStream_t s) {
+  if (NK == 1 && R % 4 == 0) conv_forward_rb<T, NK, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+  else if (R % 2 == 0) conv_forward_rb<T, NK, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+  else conv_forward_rb<T, NK, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+}
+
+template <typename T, int NK, int RB>
+void conv_adjoint_rb(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s) {
+  const int chunks = R / RB;
+  dim3 b = cta_shape(chunks);
+  dim3 grid(nblocks(op.n_rep, b.y), (chunks + b.x - 1) / b.x);
+  k_conv_adj<T, NK, RB><<<grid, b, 0, s>>>(op.tent.as<uint32_t>(), op.coefT.as<T>(), op.ST, op.tshift, op.n_rep,
+                                           op.o2, gy, R, gx, accumulate ? 1 : 0);
+}
+
+template <typename T, int NK>
+void conv_adjoint_nk(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s) {
+  if (R % 2 == 0) conv_adjoint_rb<T, NK, 2>(op, gy, R, gx, accumulate, s);
+  else conv_adjoint_rb<T, NK, 1>(op, gy, R, gx, accumulate, s);
+}
+
+template <typename T, int NK, int RB>
+void ell_rb(const int32_t* col, const T* w, int W, i64 n_rep, int o2_out, int o2_in, const T* x, int x_pix,
+            int x_outer, T* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
+  const int chunks = R_outer * (R_inner / RB);
+  dim3 b = cta_shape(chunks);
+  dim3 grid(nblocks(n_rep, b.y), (chunks + b.x - 1) / b.x);
+  k_ell<T, NK, RB><<<grid, b, 0, s>>>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
+                                      R_inner, acc ? 1 : 0);
+}
+
+template <typename T, int NK>
+void ell_nk(const int32_t* col, const T* w, int W, i64 n_rep, int o2_out, int o2_in, const T* x, int x_pix,
+            int x_outer, T* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
+  if (R_inner % 2 == 0)
+    ell_rb<T, NK, 2>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, acc, s);
+  else
+    ell_rb<T, NK, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, acc, s);
 }
 
 }  // namespace
 
 template <typename T>
-void conv_forward(const ConvOp& op, const T* x, int R, T* out, i64 out_row_stride, T* mod_out, i64 mod_row_stride,
+void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
                   cudaStream_t s) {
-  constexpr int RB = sizeof(T) == 4 ? 4 : 2;
-  dim3 grid(nblocks(op.n_rows, 128), (R + RB - 1) / RB);
-  k_conv_fwd<T, RB><<<grid, 128, 0, s>>>(op.cell.as<int32_t>(), op.coef.as<T>(), op.S, op.n_rows, x, op.n_in, R, out,
-                                         out_row_stride, mod_out, mod_row_stride);
+  if (op.nk == 4) conv_forward_nk<T, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+  else conv_forward_nk<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename T>
-void conv_adjoint(const ConvOp& op, const T* gy, i64 gy_row_stride, int R, T* gx, bool accumulate, cudaStream_t s) {
-  constexpr int RB = sizeof(T) == 4 ? 4 : 2;
-  dim3 grid(nblocks(op.n_in, 128), (R + RB - 1) / RB);
-  k_conv_adj<T, RB><<<grid, 128, 0, s>>>(op.tent.as<uint32_t>(), op.ST, op.shift, op.n_in, op.coef.as<T>(), op.n_rows,
-                                         gy, gy_row_stride, R, gx, accumulate ? 1 : 0);
+void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s) {
+  if (op.nk == 4) conv_adjoint_nk<T, 4>(op, gy, R, gx, accumulate, s);
+  else conv_adjoint_nk<T, 1>(op, gy, R, gx, accumulate, s);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename T>
-void dec_apply(const DecOp& op, bool transpose, const T* x, i64 x_outer, T* y, i64 y_outer, int R_outer, int R_inner,
-               bool accumulate, cudaStream_t s) {
+void dec_apply(const DecOp& op, bool transpose, const T* x, int x_pix, int x_outer, T* y, int y_pix, int y_outer,
+               int R_outer, int R_inner, bool accumulate, cudaStream_t s) {
   if (R_outer <= 0 || R_inner <= 0) return;
-  i64 n_out = transpose ? op.n_in : op.n_out;
-  i64 n_in = transpose ? op.n_out : op.n_in;
-  dim3 grid(nblocks(n_out, 256), R_inner, R_outer);
-  if (transpose)
-    k_ell<T><<<grid, 256, 0, s>>>(op.tcol.as<int32_t>(), op.tw.as<T>(), op.WT, n_out, n_in, x, x_outer, y, y_outer,
-                                  accumulate ? 1 : 0);
+  const int32_t* col = transpose ? op.tcol.as<int32_t>() : op.col.as<int32_t>();
+  const T* w = transpose ? op.tw.as<T>() : op.w.as<T>();
+  const int W = transpose ? op.WT : op.W;
+  const i64 n_rep = transpose ? op.n_rep_in : op.n_rep_out;
+  const int o2_out = transpose ? op.o2 : op.co2, o2_in = transpose ? op.co2 : op.o2;
+  if (op.nk == 4)
+    ell_nk<T, 4>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
+                 s);
   else
-    k_ell<T><<<grid, 256, 0, s>>>(op.col.as<int32_t>(), op.w.as<T>(), op.W, n_out, n_in, x, x_outer, y, y_outer,
-                                  accumulate ? 1 : 0);
+    ell_nk<T, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
+                 s);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename T>
-void modulus_vjp_add(const T* z, const T* g, i64 g_outer, T* gz, int B, i64 plane, cudaStream_t s) {
-  dim3 grid(nblocks(plane, 256), B);
-  k_modvjp<T><<<grid, 256, 0, s>>>(z, g, g_outer, gz, plane);
+void modulus_vjp_add(const T* z, const T* g, int g_pix, int g_row, T* gz, i64 N, int B, int L, cudaStream_t s) {
+  const i64 n = N * B * L;
+  k_modvjp<T><<<nblocks(n, 256), 256, 0, s>>>(z, g, g_pix, g_row, gz, N, B, L);
   STL_CUDA(cudaGetLastError());
 }
 
 ProductShape product_shape(int n, int L, int B, i64 N) {
   ProductShape sh;
-  sh.K = (n + 1) * L + 1;
+  sh.nd = n + 1;
+  sh.K = sh.nd * L + 1;
   sh.L = L; sh.B = B; sh.N = N; sh.level0 = n == 0;
-  int E = sh.K * (sh.K + 1) / 2;
-  sh.slots = 3 * E + 5;
-  i64 nsub = (N + kPC - 1) / kPC;
-  sh.blocks = (int)std::min<i64>(nsub, 256);
+  const int nBB = sh.nd * (sh.nd + 1) / 2;
+  sh.slots = nBB * 48 + sh.nd * 12 + 6;
+  const int items = nBB + sh.nd + 1;  // blocks of the Gram matrix per (b, l3)
+  const i64 ntiles = (N + kTile - 1) / kTile;
+  // about 16 blocks of 4 warps per SM over (tile ranges, b, items)
+  sh.blocks = (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)148 * 16 / std::max(1, B * items)));
   return sh;
 }
 
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials, double* sums,
                       cudaStream_t s) {
-  const int K = sh.K, E = K * (K + 1) / 2;
-  int Q = 1;
-  while (Q < 16 && E * Q * 2 <= kPT) Q *= 2;
-  if ((E * Q + kPT - 1) / kPT > 4) throw std::runtime_error("too many coefficient products per level");
-  size_t sm_fields = (size_t)K * kPC * (2 * sizeof(T) + sizeof(double));
-  size_t sm_gram = (size_t)Q * E * 3 * sizeof(double);
-  size_t smem = std::max(sm_fields, sm_gram) + kPT * sizeof(double);
-  if (smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  i64 nsub = (sh.N + kPC - 1) / kPC;
-  dim3 grid(sh.blocks, sh.L, sh.B);
-  k_products<T><<<grid, kPT, smem, s>>>(K, sh.L, sh.N, (int)nsub, z, br, sh.level0 ? x0 : nullptr, Q, partials,
-                                        sh.slots);
+  const int L = sh.L, nd = sh.nd;
+  const int items = nd * (nd + 1) / 2 + nd + 1;
+  const int ntiles = (int)((sh.N + kTile - 1) / kTile);
+  dim3 grid(sh.blocks, sh.B, items), block(32, L);
+  k_products<T><<<grid, block, 0, s>>>(nd, L, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots, ntiles,
+                                       partials);
   STL_CUDA(cudaGetLastError());
-  dim3 rg((sh.slots + 255) / 256, sh.B * sh.L);
-  k_reduce_partials<<<rg, 256, 0, s>>>(partials, sh.blocks, sh.slots, sums);
+  const i64 total = (i64)sh.B * L * sh.slots;
+  k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
+                                                                                        sh.B * L, sh.slots, sums);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
                       cudaStream_t s) {
-  const int K = sh.K;
-  size_t smem = (size_t)K * K * 2 * sizeof(T) + (size_t)K * kPC * 2 * sizeof(T);
+  const int K = sh.K, L = sh.L;
+  auto bytes = [&](int tp) { return ((size_t)L * K * K + 2 * (size_t)L * K * (tp + 1)) * 2 * sizeof(T); };
+  int TP = 32;
+  while (TP > 4 && bytes(TP) > 200 * 1024) TP /= 2;
+  const size_t smem = bytes(TP);
+  if (smem > 227 * 1024) throw std::runtime_error("coefficient cotangents exceed shared memory");
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products_rev<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(nblocks(sh.N, kPC), sh.L, sh.B);
-  k_products_rev<T><<<grid, kPC, smem, s>>>(K, sh.L, sh.N, z, br, M, s1c, gz, gbr);
+  dim3 grid(nblocks(sh.N, TP), sh.B), block(TP, L);
+  k_products_rev<T><<<grid, block, smem, s>>>(sh.nd, L, sh.N, sh.B, TP, z, br, M, s1c, gz, gbr);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename T>
 void mean_var_grad(const T* x0, const double* coefs, int B, i64 N, T* gx, cudaStream_t s) {
-  dim3 grid(nblocks(N, 256), B);
-  k_mean_var_grad<T><<<grid, 256, 0, s>>>(x0, coefs, N, gx);
+  k_mean_var_grad<T><<<nblocks(N * B, 256), 256, 0, s>>>(x0, coefs, N, B, gx);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -457,11 +681,23 @@ void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s) {
   STL_CUDA(cudaGetLastError());
 }
 
+template <typename Tin, typename Tout>
+void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
+  k_to_pixel_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B);
+  STL_CUDA(cudaGetLastError());
+}
+
+template <typename Tin, typename Tout>
+void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
+  k_to_map_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B);
+  STL_CUDA(cudaGetLastError());
+}
+
 #define INST(T)                                                                                                   \
-  template void conv_forward<T>(const ConvOp&, const T*, int, T*, i64, T*, i64, cudaStream_t);                    \
-  template void conv_adjoint<T>(const ConvOp&, const T*, i64, int, T*, bool, cudaStream_t);                       \
-  template void dec_apply<T>(const DecOp&, bool, const T*, i64, T*, i64, int, int, bool, cudaStream_t);           \
-  template void modulus_vjp_add<T>(const T*, const T*, i64, T*, int, i64, cudaStream_t);                          \
+  template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t);               \
+  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t);                            \
+  template void dec_apply<T>(const DecOp&, bool, const T*, int, int, T*, int, int, int, int, bool, cudaStream_t); \
+  template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, double*, double*,          \
                                     cudaStream_t);                                                                \
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, T*, T*,          \
@@ -473,5 +709,13 @@ template void convert<double, float>(const double*, float*, i64, cudaStream_t);
 template void convert<float, double>(const float*, double*, i64, cudaStream_t);
 template void convert<double, double>(const double*, double*, i64, cudaStream_t);
 template void convert<float, float>(const float*, float*, i64, cudaStream_t);
+template void to_pixel_major<double, float>(const double*, float*, i64, int, cudaStream_t);
+template void to_pixel_major<double, double>(const double*, double*, i64, int, cudaStream_t);
+template void to_pixel_major<float, float>(const float*, float*, i64, int, cudaStream_t);
+template void to_pixel_major<float, double>(const float*, double*, i64, int, cudaStream_t);
+template void to_map_major<float, double>(const float*, double*, i64, int, cudaStream_t);
+template void to_map_major<double, double>(const double*, double*, i64, int, cudaStream_t);
+template void to_map_major<float, float>(const float*, float*, i64, int, cudaStream_t);
+template void to_map_major<double, float>(const double*, float*, i64, int, cudaStream_t);
 
 }  // namespace stl

@@ -44,6 +44,16 @@ struct Timers {
   int forwards = 0, reverses = 0;
 };
 
+// Per kernel class: launches, device time (CUDA events on the engine's
+// stream, only while profiling is on) and algorithmic bytes / flops of the
+// launches (the minimal traffic and work of the operation, not the
+// kernel's actual traffic).
+struct KernelStat {
+  const char* name;
+  long launches = 0;
+  double ms = 0.0, bytes = 0.0, flops = 0.0;
+};
+
 class Engine {
  public:
   static std::unique_ptr<Engine> create(const Options& o);
@@ -76,6 +86,14 @@ class Engine {
   size_t operator_bytes() const { return operator_bytes_; }
   size_t field_bytes() const { return field_bytes_; }
   Timers timers;
+
+  // Kernel statistics since the last reset; profiling adds a pair of CUDA
+  // events around every launch.
+  virtual std::vector<KernelStat> kernel_stats() const = 0;
+  virtual void reset_kernel_stats() = 0;
+  virtual void set_profiling(bool on) = 0;
+  // Mean cells read per row of each level's wavelet operator.
+  virtual std::vector<double> mean_slots() const = 0;
 
  protected:
   explicit Engine(const Options& o);

@@ -61,6 +61,7 @@ def lib():
             "stlp_info": ([_VOID], _VOID),
             "stlp_prepare": ([_VOID], C.c_int),
             "stlp_set_stream": ([_VOID, u64], C.c_int),
+            "stlp_profile": ([_VOID, C.c_int, C.c_int], C.c_int),
             "stlp_set_masks": ([_VOID, _D, sz], C.c_int),
             "stlp_native_pixels": ([_VOID, _SIZE], C.c_int),
             "stlp_forward": ([_VOID, _D, sz, u64, u64, u64, b, _D, _D], C.c_int),
@@ -177,6 +178,17 @@ class NativeEngine:
                 return json.loads(C.string_at(p))
             finally:
                 self._lib.stlp_string_free(p)
+
+    def profile(self, on=True, reset=True):
+        """Kernel statistics: reset the counters, and time every launch with CUDA events when on."""
+        with self._mutex:
+            self._open()
+            if self._lib.stlp_profile(self._handle, int(bool(on)), int(bool(reset))):
+                raise _error()
+
+    def kernel_stats(self):
+        """Per kernel class since the last reset: launches, ms, algorithmic bytes and flops."""
+        return {k["name"]: k for k in self.info()["kernels"]}
 
     def native_pixels(self):
         with self._mutex:
