@@ -264,6 +264,16 @@ class EngineImpl final : public Engine {
     mv_.alloc(sizeof(double) * 2 * B);
     in_f64_.alloc(sizeof(double) * B * npix(0));
     field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + M_.bytes + in_f64_.bytes;
+    // partial sums of the row-centric adjoint
+    {
+      size_t cap = 0;
+      for (int n = 0; n < levels_; ++n)
+        cap = std::max(cap, adjoint_part_bytes(conv_[n], sizeof(T), B * (n + 1) * L));
+      if (cap) adj_part_.alloc(cap);
+      adj_.part = adj_part_.p;
+      adj_.capacity = cap;
+      field_bytes_ += adj_part_.bytes;
+    }
     STL_CUDA(cudaStreamSynchronize(stream_));
     ready_ = true;
     timers.build_s += ms_since(t0) / 1000.0;
@@ -511,12 +521,12 @@ class EngineImpl final : public Engine {
                    });
       const int R = B * (n + 1) * L;
       prof_.launch(Profiler::CONV_ADJ, 1, conv_bytes(op, R, false, true), conv_flops(op, R), s,
-                   [&] { conv_adjoint<T>(op, gBr_.as<T>(), R, gmod, true, s); });
+                   [&] { conv_adjoint<T>(op, gBr_.as<T>(), R, gmod, true, s, adj_ptr()); });
       prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
         modulus_vjp_add<T>(Z_[n].as<T>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<T>(), N, B, L, s);
       });
       prof_.launch(Profiler::CONV_ADJ, 1, conv_bytes(op, B, false, false), conv_flops(op, B), s,
-                   [&] { conv_adjoint<T>(op, gZ_.as<T>(), B, gX_[n].as<T>(), false, s); });
+                   [&] { conv_adjoint<T>(op, gZ_.as<T>(), B, gX_[n].as<T>(), false, s, adj_ptr()); });
       if (n + 1 < levels_)
         prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
                      [&] { dec_apply<T>(dec_[n], true, gX_[n + 1].as<T>(), B, 0, gX_[n].as<T>(), B, 0, 1, B, true, s); });
@@ -540,6 +550,9 @@ class EngineImpl final : public Engine {
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
   DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_;
+  DevMem adj_part_;
+  AdjScratch adj_;
+  const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }
   std::vector<double> h_sums_;
   std::vector<T> h_M_, h_s1_;
   std::vector<Loc> map_;

@@ -98,10 +98,42 @@ struct ConvOp {
   DevMem coef;               // T [S][n_rep][8]: (gauge, re/im) coefficients
   DevMem tent;               // uint32 [ST][n_rep]: entries (u, s, j) reading rotation j of a stored cell
   DevMem coefT;              // T [ST][n_rep][8]: coef of each transposed entry
+  // Row-centric adjoint: stored rows in tiles of kAdjTile.  Per tile the
+  // sorted distinct cells its rows read; per (tile, chunk of kAdjSC slots)
+  // the (slot, row) entries of every tile cell in (slot, row) order; per
+  // stored input cell the (tile, tile cell, rotation) entries that hold its
+  // partial sums, sorted.  Every sum of the adjoint has a fixed order.
+  i64 n_tiles = 0;
+  int nch = 0;               // slot chunks: ceil(S / kAdjSC)
+  int ncs = 0;               // stride of the tile cell lists: most cells of a tile + 1
+  int max_tile_cells = 0;
+  bool adj_tiles = false;    // tables built (every tile within kAdjCells cells)
+  DevMem tile_cells;         // int32 [n_tiles][kAdjCells]
+  DevMem tile_ncells;        // int32 [n_tiles]
+  DevMem lcell;              // uint16 [S][n_rep]: tile cell of every (slot, row) (build only)
+  DevMem tile_ent;           // uint16 [n_tiles][S kAdjTile]: slot % kAdjSC << 8 | row
+  DevMem tile_off;           // uint16 [n_tiles][nch][ncs]: first entry of (chunk, tile cell)
+  DevMem coff;               // int64 [stored cells + 1]
+  DevMem clist;              // uint32 tile << 12 | tile cell << 2 | rotation
   int G = 4;
   double mean_slots = 0.0;   // cells read per row, averaged over the rows
-  size_t bytes() const { return cell.bytes + coef.bytes + tent.bytes + coefT.bytes; }
+  size_t bytes() const {
+    return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + tile_cells.bytes + tile_ncells.bytes + lcell.bytes +
+           tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
+  }
 };
+constexpr int kAdjTile = 256;    // stored rows per adjoint tile
+constexpr int kAdjCells = 1024;  // cells a tile may read
+constexpr int kAdjSC = 8;        // slots per chunk of the two-phase adjoint
+
+// Scratch of the row-centric adjoint: the tile partial sums
+// [n_tiles][4][ncs][R] (capacity bytes).
+struct AdjScratch {
+  void* part = nullptr;
+  size_t capacity = 0;
+};
+size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R);
+bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch* scr);
 
 struct DecSpec {
   i64 nside = 0;           // fine level
@@ -142,8 +174,11 @@ void build_dec(const DecSpec& spec, DType dtype, DecOp& out, cudaStream_t stream
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
                   cudaStream_t s);
+//  With scratch, operators with tile tables use the row-centric two-phase
+//  adjoint; otherwise the transposed gather.
 template <typename T>
-void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s);
+void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
+                  const AdjScratch* scr = nullptr);
 template <typename T>
 void dec_apply(const DecOp& op, bool transpose, const T* x, int x_pix, int x_outer, T* y, int y_pix, int y_outer,
                int R_outer, int R_inner, bool accumulate, cudaStream_t s);

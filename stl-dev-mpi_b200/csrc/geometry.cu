@@ -209,6 +209,180 @@ __global__ void k_conv_coefT(const uint32_t* tent, const T* coef, i64 n_rep, int
   }
 }
 
+// Adjoint tiles: one block per tile of kAdjTile stored rows.  The cells the
+// tile's rows read (all slots) are sorted in shared memory (bitonic), made
+// unique, written to the tile's list, and every (slot, row) gets the index
+// of its cell in that list.
+__global__ void k_adj_tiles(const int32_t* cell, int S, i64 n_rep, int P2, int32_t* tile_cells, int32_t* tile_nc,
+                            uint16_t* lcell, int* overflow) {
+  extern __shared__ int32_t buf[];  // [P2] sorted cells, then [kAdjCells] unique, then [256] counts
+  int32_t* uniq = buf + P2;
+  int32_t* cnt = uniq + kAdjCells;
+  const int tid = threadIdx.x;
+  const i64 u0 = (i64)blockIdx.x * kAdjTile;
+  const int n = S * kAdjTile;
+  for (int i = tid; i < P2; i += blockDim.x) {
+    int32_t v = 0x7fffffff;
+    if (i < n) {
+      const int s = i / kAdjTile, ul = i % kAdjTile;
+      if (u0 + ul < n_rep) v = cell[(i64)s * n_rep + u0 + ul];
+    }
+    buf[i] = v;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < P2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const int32_t a = buf[i], c = buf[l];
+          if (((i & k) == 0) ? (a > c) : (a < c)) { buf[i] = c; buf[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  const int per = P2 / blockDim.x;
+  int mine = 0;
+  for (int i = tid * per; i < (tid + 1) * per; ++i)
+    if (buf[i] != 0x7fffffff && (i == 0 || buf[i - 1] != buf[i])) ++mine;
+  cnt[tid] = mine;
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) { const int c = cnt[t]; cnt[t] = acc; acc += c; }
+    tile_nc[blockIdx.x] = acc;
+    if (acc > kAdjCells) atomicExch(overflow, 1);
+  }
+  __syncthreads();
+  int pos = cnt[tid];
+  for (int i = tid * per; i < (tid + 1) * per; ++i)
+    if (buf[i] != 0x7fffffff && (i == 0 || buf[i - 1] != buf[i])) {
+      if (pos < kAdjCells) {
+        uniq[pos] = buf[i];
+        tile_cells[(i64)blockIdx.x * kAdjCells + pos] = buf[i];
+      }
+      ++pos;
+    }
+  __syncthreads();
+  const int nc = min(tile_nc[blockIdx.x], kAdjCells);
+  for (int i = tid; i < n; i += blockDim.x) {
+    const int s = i / kAdjTile, ul = i % kAdjTile;
+    if (u0 + ul >= n_rep) continue;
+    const int32_t v = cell[(i64)s * n_rep + u0 + ul];
+    int lo = 0, hi = nc;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (uniq[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    lcell[(i64)s * n_rep + u0 + ul] = (uint16_t)lo;
+  }
+}
+
+// Per tile and slot chunk, the entries (slot, row) of every tile cell in
+// the order (slot, row): keys chunk << 22 | cell << 11 | slot % kAdjSC << 8
+// | row, sorted (bitonic); the low 11 bits are the entry, and off[chunk][lc]
+// the position of the first key of (chunk, lc).  Slots past a row's cell
+// count repeat its first cell: they are left out.
+__global__ void k_adj_csr(const int32_t* cell, const uint16_t* lcell, int S, i64 n_rep, int P2, int nch, int ncs,
+                          const int32_t* tile_nc, uint16_t* tile_ent, uint16_t* tile_off) {
+  extern __shared__ uint32_t key[];
+  const int tid = threadIdx.x;
+  const i64 u0 = (i64)blockIdx.x * kAdjTile;
+  const int n = S * kAdjTile;
+  for (int i = tid; i < P2; i += blockDim.x) {
+    uint32_t v = 0xFFFFFFFFu;
+    if (i < n) {
+      const int sl = i / kAdjTile, ul = i % kAdjTile;
+      const i64 u = u0 + ul;
+      if (u < n_rep) {
+        const i64 e = (i64)sl * n_rep + u;
+        if (sl == 0 || cell[e] != cell[u])
+          v = ((uint32_t)(sl / kAdjSC) << 22) | ((uint32_t)lcell[e] << 11) | ((uint32_t)(sl % kAdjSC) << 8) | (uint32_t)ul;
+      }
+    }
+    key[i] = v;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < P2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const uint32_t a = key[i], c = key[l];
+          if (((i & k) == 0) ? (a > c) : (a < c)) { key[i] = c; key[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  uint16_t* ent = tile_ent + (i64)blockIdx.x * n;
+  for (int i = tid; i < n; i += blockDim.x)
+    if (key[i] != 0xFFFFFFFFu) ent[i] = (uint16_t)(key[i] & 0x7FFu);
+  const int nc = tile_nc[blockIdx.x];
+  uint16_t* off = tile_off + (i64)blockIdx.x * nch * ncs;
+  for (int q = tid; q < nch * (nc + 1); q += blockDim.x) {
+    const int ch = q / (nc + 1), lc = q % (nc + 1);
+    const uint32_t t = ((uint32_t)ch << 22) | ((uint32_t)lc << 11);
+    int lo = 0, hi = P2;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (key[mid] < t) lo = mid + 1; else hi = mid;
+    }
+    off[ch * ncs + lc] = (uint16_t)lo;
+  }
+}
+
+// Tile cells -> stored input cells: cell c of a tile is rotation j of
+// stored cell v (nk = 4: c in face 4m + j; nk = 1: v = c, j = 0).
+__device__ __forceinline__ void tile_cell_owner(int32_t c, int nk, int o2, i64& v, int& j) {
+  if (nk == 4) {
+    const i64 f = (i64)c >> o2;
+    j = (int)(f & 3);
+    v = ((f >> 2) << o2) | ((i64)c & ((i64(1) << o2) - 1));
+  } else {
+    v = c;
+    j = 0;
+  }
+}
+
+__global__ void k_adj_ccount(const int32_t* tile_cells, const int32_t* tile_nc, i64 n_tiles, int nk, int o2,
+                             int* ccount) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_tiles * kAdjCells) return;
+  const i64 tile = i / kAdjCells;
+  const int lc = (int)(i % kAdjCells);
+  if (lc >= tile_nc[tile]) return;
+  i64 v; int j;
+  tile_cell_owner(tile_cells[i], nk, o2, v, j);
+  atomicAdd(ccount + v, 1);
+}
+
+__global__ void k_adj_cfill(const int32_t* tile_cells, const int32_t* tile_nc, i64 n_tiles, int nk, int o2,
+                            const i64* coff, int* cursor, uint32_t* clist) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_tiles * kAdjCells) return;
+  const i64 tile = i / kAdjCells;
+  const int lc = (int)(i % kAdjCells);
+  if (lc >= tile_nc[tile]) return;
+  i64 v; int j;
+  tile_cell_owner(tile_cells[i], nk, o2, v, j);
+  const int pos = atomicAdd(cursor + v, 1);
+  clist[coff[v] + pos] = ((uint32_t)tile << 12) | ((uint32_t)lc << 2) | (uint32_t)j;
+}
+
+// fixed order of every stored cell's list (insertion sort; lists are short)
+__global__ void k_adj_csort(const i64* coff, i64 n, uint32_t* clist) {
+  const i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  uint32_t* l = clist + coff[v];
+  const int m = (int)(coff[v + 1] - coff[v]);
+  for (int a = 1; a < m; ++a) {
+    const uint32_t x = l[a];
+    int b = a - 1;
+    while (b >= 0 && l[b] > x) { l[b + 1] = l[b]; --b; }
+    l[b + 1] = x;
+  }
+}
+
 __global__ void k_tsort(uint32_t* tent, const int* tcount, i64 n_in, int ST) {
   i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_in) return;
@@ -498,6 +672,78 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   k_conv_coefT<T><<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), op.coef.as<T>(), n_cells, op.ST,
                                                         op.tshift, op.coefT.as<T>());
   STL_CUDA(cudaGetLastError());
+  // row-centric adjoint tiles
+  op.adj_tiles = false;
+  if (op.S > 128) return;  // the tile sort holds 128 slots per row
+  op.n_tiles = (a.n_rows + kAdjTile - 1) / kAdjTile;
+  op.tile_cells.alloc(sizeof(int32_t) * kAdjCells * op.n_tiles);
+  op.tile_ncells.alloc(sizeof(int32_t) * op.n_tiles);
+  op.lcell.alloc(sizeof(uint16_t) * op.S * a.n_rows);
+  {
+    int P2 = 1;
+    while (P2 < op.S * kAdjTile) P2 <<= 1;
+    const size_t smem = sizeof(int32_t) * ((size_t)P2 + kAdjCells + 256);
+    if (smem > 48 * 1024)
+      STL_CUDA(cudaFuncSetAttribute(k_adj_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+    k_adj_tiles<<<(unsigned)op.n_tiles, 256, smem, s>>>(op.cell.as<int32_t>(), op.S, a.n_rows, P2,
+                                                          op.tile_cells.as<int32_t>(), op.tile_ncells.as<int32_t>(),
+                                                          op.lcell.as<uint16_t>(), flag.as<int>());
+    STL_CUDA(cudaGetLastError());
+    op.adj_tiles = !read_flag(flag, s);
+    std::vector<int32_t> nc(op.n_tiles);
+    STL_CUDA(cudaMemcpyAsync(nc.data(), op.tile_ncells.p, sizeof(int32_t) * op.n_tiles, cudaMemcpyDeviceToHost, s));
+    STL_CUDA(cudaStreamSynchronize(s));
+    op.max_tile_cells = 0;
+    for (int32_t v : nc) op.max_tile_cells = std::max(op.max_tile_cells, (int)v);
+  }
+  if (!op.adj_tiles || (uint64_t)op.n_tiles >= (1ull << 20)) {
+    op.adj_tiles = false;
+    return;
+  }
+  // per tile and slot chunk: the entries of every tile cell
+  op.nch = (op.S + kAdjSC - 1) / kAdjSC;
+  op.ncs = op.max_tile_cells + 1;
+  op.tile_ent.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * op.S * kAdjTile);
+  op.tile_off.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * op.nch * op.ncs);
+  {
+    int P2 = 1;
+    while (P2 < op.S * kAdjTile) P2 <<= 1;
+    const size_t smem = sizeof(uint32_t) * (size_t)P2;
+    if (smem > 48 * 1024)
+      STL_CUDA(cudaFuncSetAttribute(k_adj_csr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_adj_csr<<<(unsigned)op.n_tiles, 256, smem, s>>>(op.cell.as<int32_t>(), op.lcell.as<uint16_t>(), op.S,
+                                                        a.n_rows, P2, op.nch, op.ncs, op.tile_ncells.as<int32_t>(),
+                                                        op.tile_ent.as<uint16_t>(), op.tile_off.as<uint16_t>());
+    STL_CUDA(cudaGetLastError());
+  }
+  op.lcell.release();
+  // per stored input cell: the (tile, cell, rotation) entries holding its sums
+  {
+    const i64 n_in_rep = n_cells;
+    const i64 nt = op.n_tiles * kAdjCells;
+    DevMem cnt(sizeof(int) * n_in_rep);
+    STL_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+    k_adj_ccount<<<nblocks(nt, 256), 256, 0, s>>>(op.tile_cells.as<int32_t>(), op.tile_ncells.as<int32_t>(),
+                                                  op.n_tiles, op.nk, op.o2, cnt.as<int>());
+    STL_CUDA(cudaGetLastError());
+    std::vector<int> hc(n_in_rep);
+    STL_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, cnt.bytes, cudaMemcpyDeviceToHost, s));
+    STL_CUDA(cudaStreamSynchronize(s));
+    std::vector<i64> ho(n_in_rep + 1, 0);
+    for (i64 v = 0; v < n_in_rep; ++v) ho[v + 1] = ho[v] + hc[v];
+    op.coff.alloc(sizeof(i64) * (n_in_rep + 1));
+    op.clist.alloc(sizeof(uint32_t) * std::max<i64>(ho[n_in_rep], 1));
+    STL_CUDA(cudaMemcpyAsync(op.coff.p, ho.data(), op.coff.bytes, cudaMemcpyHostToDevice, s));
+    STL_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+    k_adj_cfill<<<nblocks(nt, 256), 256, 0, s>>>(op.tile_cells.as<int32_t>(), op.tile_ncells.as<int32_t>(),
+                                                 op.n_tiles, op.nk, op.o2, op.coff.as<i64>(), cnt.as<int>(),
+                                                 op.clist.as<uint32_t>());
+    STL_CUDA(cudaGetLastError());
+    k_adj_csort<<<nblocks(n_in_rep, 256), 256, 0, s>>>(op.coff.as<i64>(), n_in_rep, op.clist.as<uint32_t>());
+    STL_CUDA(cudaGetLastError());
+    STL_CUDA(cudaStreamSynchronize(s));
+  }
   STL_CUDA(cudaStreamSynchronize(s));
 }
 

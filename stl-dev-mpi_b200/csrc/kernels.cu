@@ -114,21 +114,38 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ ce
     for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[k][rb][j] = (T)0;
-  for (int s = 0; s < S; ++s) {
-    const i64 e = (i64)s * n_rep + u;
-    const i64 c = __ldg(cell + e);
-    T w[8];
-    load8(coef + e * 8, w);
+  // Two-stage software pipeline: the gathers of slot s + 1 and the cell of
+  // slot s + 2 are in flight while slot s is accumulated.
+  T xv[NK][RB], xn[NK][RB], w[8], wn[8];
+  i64 cn = 0;
+  auto gather = [&](i64 c, T (&dst)[NK][RB]) {
 #pragma unroll
-    for (int k = 0; k < NK; ++k) {
-      const i64 ck = NK == 1 ? c : rot_cell(c, k, o2);
-      T xv[RB];
-      loadR<RB>(x + ck * R + r0, xv);
+    for (int k = 0; k < NK; ++k) loadR<RB>(x + (NK == 1 ? c : rot_cell(c, k, o2)) * R + r0, dst[k]);
+  };
+  if (S > 0) {
+    const i64 c0 = __ldg(cell + u);
+    gather(c0, xv);
+    load8(coef + u * 8, w);
+    if (S > 1) cn = __ldg(cell + n_rep + u);
+  }
+  for (int s = 0; s < S; ++s) {
+    if (s + 1 < S) {
+      gather(cn, xn);
+      load8(coef + ((i64)(s + 1) * n_rep + u) * 8, wn);
+      if (s + 2 < S) cn = __ldg(cell + (i64)(s + 2) * n_rep + u);
+    }
+#pragma unroll
+    for (int k = 0; k < NK; ++k)
 #pragma unroll
       for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[k][rb][j] = fma(w[j], xv[rb], acc[k][rb][j]);
-    }
+        for (int j = 0; j < 8; ++j) acc[k][rb][j] = fma(w[j], xv[k][rb], acc[k][rb][j]);
+#pragma unroll
+    for (int k = 0; k < NK; ++k)
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) xv[k][rb] = xn[k][rb];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) w[j] = wn[j];
   }
 #pragma unroll
   for (int k = 0; k < NK; ++k) {
@@ -228,6 +245,148 @@ __global__ void __launch_bounds__(128) k_conv_adj(const uint32_t* __restrict__ t
     for (int rb = 0; rb < RB; ++rb) {
       T* o = gx + c * R + r0 + rb;
       *o = accumulate ? *o + acc[k][rb] : acc[k][rb];
+    }
+  }
+}
+
+// ---- row-centric adjoint (two phases) -----------------------------------------
+// The transposed gather above re-reads every cotangent vector once per entry
+// that reads its row (about 44 times, 32 bytes per rotation and row).  Here
+// a CTA takes a tile of kAdjTile stored rows and RB cotangent rows; each
+// thread keeps its row's 4 rotated cotangent vectors in registers and, per
+// chunk of kAdjSC slots, writes the products of its slots to shared memory
+// (phase 1); then every tile cell adds the products of its entries in
+// (slot, row) order (phase 2).  The tile's sums go to a partial buffer, and
+// k_adj_combine adds the partials of every cell in (tile, cell) order: all
+// sums have a fixed order, so results are bit-reproducible.
+// Thread = stored row, holding its 4 rotated cotangent vectors (the
+// rotation's gauge permutation and conjugation folded in, so every product
+// is a plain 8-term dot with the stored coefficients).  Product planes
+// [rb][k] are kAdjPlane values apart.
+constexpr int kAdjPlane = kAdjSC * kAdjTile;
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(kAdjTile, 2) k_conv_adj_tiles(
+    const T* __restrict__ coef, int S, i64 n_rep, int o2, int nch, int ncs, const int32_t* __restrict__ tile_nc,
+    const uint16_t* __restrict__ tile_ent, const uint16_t* __restrict__ tile_off, const T* __restrict__ gy, int R,
+    T* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* P = reinterpret_cast<T*>(smem_raw);                 // [RB][4][kAdjPlane]
+  T* acc = P + 4 * RB * kAdjPlane;                       // [RB][4][ncs]
+  uint16_t* ent = reinterpret_cast<uint16_t*>(acc + 4 * RB * ncs);  // [kAdjSC kAdjTile]
+  uint16_t* off = ent + kAdjSC * kAdjTile;               // [ncs + 1]
+  const int tile = blockIdx.y, tid = threadIdx.x;
+  const int r0 = blockIdx.x * RB;
+  const int nc = tile_nc[tile];
+  const i64 u = (i64)tile * kAdjTile + tid;
+  const bool valid = u < n_rep;
+  T g[4][RB][8];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+      T t[8];
+      if (valid) load8(gy + (rot_pixel(u, k, o2) * R + r0 + rb) * 8, t);
+      else
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t[q] = (T)0;
+#pragma unroll
+      for (int gg = 0; gg < 4; ++gg) {
+        const int q = rot_src(k, gg);
+        g[k][rb][2 * q] = t[2 * gg];
+        g[k][rb][2 * q + 1] = rot_conj(k, gg) ? -t[2 * gg + 1] : t[2 * gg + 1];
+      }
+    }
+  for (int i = tid; i < 4 * RB * ncs; i += kAdjTile) acc[i] = (T)0;
+  const uint16_t* toff = tile_off + (i64)tile * nch * ncs;
+  const uint16_t* tent = tile_ent + (i64)tile * S * kAdjTile;
+  const T* cu = coef + u * 8;
+  const i64 cstride = n_rep * 8;
+  T wn[8];
+  if (valid) load8(cu, wn);
+  for (int ch = 0; ch < nch; ++ch) {
+    const int s0 = ch * kAdjSC;
+    const int sn = min(kAdjSC, S - s0);
+    if (valid) {
+      for (int sl = 0; sl < sn; ++sl) {
+        T w[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) w[q] = wn[q];
+        if (s0 + sl + 1 < S) load8(cu + (i64)(s0 + sl + 1) * cstride, wn);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (int rb = 0; rb < RB; ++rb) {
+            T a = (T)0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) a = fma(w[q], g[k][rb][q], a);
+            P[(rb * 4 + k) * kAdjPlane + sl * kAdjTile + tid] = a;
+          }
+      }
+    }
+    const int e0 = toff[ch * ncs], e1 = toff[ch * ncs + nc];
+    for (int i = tid; i < e1 - e0; i += kAdjTile) ent[i] = tent[e0 + i];
+    for (int i = tid; i <= nc; i += kAdjTile) off[i] = (uint16_t)(toff[ch * ncs + i] - e0);
+    __syncthreads();
+    for (int lc = tid; lc < nc; lc += kAdjTile) {
+      const int a0 = off[lc], a1 = off[lc + 1];
+      if (a0 == a1) continue;
+      T a[4 * RB];
+#pragma unroll
+      for (int q = 0; q < 4 * RB; ++q) a[q] = acc[q * ncs + lc];
+      for (int e = a0; e < a1; ++e) {
+        const int en = ent[e];
+        const T* p = P + (en >> 8) * kAdjTile + (en & 255);
+#pragma unroll
+        for (int q = 0; q < 4 * RB; ++q) a[q] += p[q * kAdjPlane];
+      }
+#pragma unroll
+      for (int q = 0; q < 4 * RB; ++q) acc[q * ncs + lc] = a[q];
+    }
+    __syncthreads();
+  }
+  // partials [tile][k][ncs][R]
+  for (int i = tid; i < 4 * RB * nc; i += kAdjTile) {
+    const int q = i / nc, lc = i - q * nc;
+    const int rb = q >> 2, kk = q & 3;
+    part[(((i64)tile * 4 + kk) * ncs + lc) * R + r0 + rb] = acc[q * ncs + lc];
+  }
+}
+
+// gx[rotation k' of stored cell v][r] (+)= sum over the entries (tile, lc, j)
+// of v, in order, of part[tile][(k' - j) mod 4][lc][r]
+template <typename T, int NK, int RB>
+__global__ void __launch_bounds__(128) k_adj_combine(const i64* __restrict__ coff, const uint32_t* __restrict__ clist,
+                                                     i64 n_cells, int o2, int ncs, const T* __restrict__ part, int R,
+                                                     T* __restrict__ gx, int accumulate) {
+  const i64 v = (i64)blockIdx.x * blockDim.y + threadIdx.y;
+  const int chunk = blockIdx.y * blockDim.x + threadIdx.x;
+  if (v >= n_cells || chunk * RB >= R) return;
+  const int r0 = chunk * RB;
+  T a[NK][RB];
+#pragma unroll
+  for (int k = 0; k < NK; ++k)
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) a[k][rb] = (T)0;
+  const i64 e1 = coff[v + 1];
+  for (i64 e = coff[v]; e < e1; ++e) {
+    const uint32_t en = __ldg(clist + e);
+    const i64 tile = en >> 12;
+    const int lc = (en >> 2) & 1023, j = en & 3;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      const T* p = part + ((tile * 4 + ((k - j) & 3)) * ncs + lc) * R + r0;
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) a[k][rb] += p[rb];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const i64 c = NK == 1 ? v : rot_pixel(v, k, o2);
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+      T* o = gx + c * R + r0 + rb;
+      *o = accumulate ? *o + a[k][rb] : a[k][rb];
     }
   }
 }
@@ -555,6 +714,35 @@ void conv_adjoint_rb(const ConvOp& op, const T* gy, int R, T* gx, bool accumulat
                                            op.o2, gy, R, gx, accumulate ? 1 : 0);
 }
 
+template <typename T, int RB>
+size_t adj_tiles_smem(const ConvOp& op) {
+  return sizeof(T) * (4 * RB * (size_t)kAdjPlane + 4 * RB * (size_t)op.ncs) +
+         sizeof(uint16_t) * (kAdjSC * kAdjTile + (size_t)op.ncs + 1);
+}
+
+template <typename T, int RB>
+void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, const AdjScratch& scr,
+                           cudaStream_t s) {
+  const size_t smem = adj_tiles_smem<T, RB>(op);
+  if (smem > 48 * 1024)
+    STL_CUDA(cudaFuncSetAttribute(k_conv_adj_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  T* part = static_cast<T*>(scr.part);
+  dim3 grid(R / RB, (unsigned)op.n_tiles);
+  k_conv_adj_tiles<T, RB><<<grid, kAdjTile, smem, s>>>(op.coef.as<T>(), op.S, op.n_rep, op.o2, op.nch, op.ncs,
+                                                       op.tile_ncells.as<int32_t>(), op.tile_ent.as<uint16_t>(),
+                                                       op.tile_off.as<uint16_t>(), gy, R, part);
+  const i64 n_cells = op.n_in / op.nk;
+  const int chunks = R / RB;
+  dim3 b = cta_shape(chunks);
+  dim3 g2(nblocks(n_cells, b.y), (chunks + b.x - 1) / b.x);
+  if (op.nk == 4)
+    k_adj_combine<T, 4, RB><<<g2, b, 0, s>>>(op.coff.as<i64>(), op.clist.as<uint32_t>(), n_cells, op.o2, op.ncs, part,
+                                             R, gx, accumulate ? 1 : 0);
+  else
+    k_adj_combine<T, 1, RB><<<g2, b, 0, s>>>(op.coff.as<i64>(), op.clist.as<uint32_t>(), n_cells, op.o2, op.ncs, part,
+                                             R, gx, accumulate ? 1 : 0);
+}
+
 template <typename T, int NK>
 void conv_adjoint_nk(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s) {
   if (R % 2 == 0) conv_adjoint_rb<T, NK, 2>(op, gy, R, gx, accumulate, s);
@@ -580,6 +768,8 @@ void ell_nk(const int32_t* col, const T* w, int W, i64 n_rep, int o2_out, int o2
     ell_rb<T, NK, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, acc, s);
 }
 
+inline int adj_rb(size_t elem, int R) { return (elem == 4 && R % 2 == 0) ? 2 : 1; }
+
 }  // namespace
 
 template <typename T>
@@ -590,9 +780,26 @@ void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_p
   STL_CUDA(cudaGetLastError());
 }
 
+size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R) {
+  if (!op.adj_tiles) return 0;
+  return elem * (size_t)op.n_tiles * 4 * op.ncs * R;
+}
+
+bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
+  if (!scr || !op.adj_tiles || op.nk != 4 || op.n_tiles > 65535) return false;
+  if (adjoint_part_bytes(op, elem, R) > scr->capacity) return false;
+  const size_t smem = elem == 4 ? (adj_rb(elem, R) == 2 ? adj_tiles_smem<float, 2>(op) : adj_tiles_smem<float, 1>(op))
+                                : adj_tiles_smem<double, 1>(op);
+  return smem <= 200 * 1024;
+}
+
 template <typename T>
-void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s) {
-  if (op.nk == 4) conv_adjoint_nk<T, 4>(op, gy, R, gx, accumulate, s);
+void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
+                  const AdjScratch* scr) {
+  if (adjoint_tiles_usable(op, sizeof(T), R, scr)) {
+    if (adj_rb(sizeof(T), R) == 2) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 2 : 1>(op, gy, R, gx, accumulate, *scr, s);
+    else conv_adjoint_tiles_rb<T, 1>(op, gy, R, gx, accumulate, *scr, s);
+  } else if (op.nk == 4) conv_adjoint_nk<T, 4>(op, gy, R, gx, accumulate, s);
   else conv_adjoint_nk<T, 1>(op, gy, R, gx, accumulate, s);
   STL_CUDA(cudaGetLastError());
 }
@@ -695,7 +902,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
 
 #define INST(T)                                                                                                   \
   template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t);               \
-  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t);                            \
+  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*);                            \
   template void dec_apply<T>(const DecOp&, bool, const T*, int, int, T*, int, int, int, int, bool, cudaStream_t); \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, double*, double*,          \
