@@ -85,6 +85,17 @@ int stlp_vjp_device(StlpHandle* h, const double* cot, size_t n, uint64_t generat
  * launches on.  No reference counterpart. */
 int stlp_set_stream(StlpHandle* h, uint64_t stream);
 
+/* Mean and var coefficients (<x>, <x^2> per map, FP64, as the MEAN and VAR
+ * families of stlp_forward) of batch device maps x [batch][n_pix] (f32 if
+ * f32, else f64) into device memory out [batch][2], launched on stream
+ * (cudaStream_t as an integer); returns after the launches, without waiting.
+ * Allocates nothing: the partial sums sit in a fixed device array of at most
+ * 64 maps (296 KiB); a larger batch is refused.  Calls in flight together on
+ * one device race on that array.  The first call on a device looks up the
+ * array's address (make it before any stream capture).  No reference
+ * counterpart. */
+int stlp_mean_var_noalloc(uint64_t x, size_t n_pix, size_t batch, int f32, uint64_t out, uint64_t stream);
+
 /* Builds the device operators now instead of at the first forward.  No
  * reference counterpart (the reference builds in stlp_new). */
 int stlp_prepare(StlpHandle* h);
