@@ -240,7 +240,7 @@ class EngineImpl final : public Engine {
       Br_[n].alloc(sizeof(T) * 2 * B * (n + 1) * L * L * N);
       gMod_[n].alloc(sizeof(T) * B * (n + 1) * L * N);
       gX_[n].alloc(sizeof(T) * B * N);
-      shapes_[n] = product_shape(n, L, B, N);
+      shapes_[n] = product_shape(n, L, B, N, sizeof(T));
       max_part = std::max(max_part, (size_t)B * L * shapes_[n].blocks * shapes_[n].slots);
       max_gz = std::max(max_gz, (size_t)2 * B * L * N);
       max_gbr = std::max(max_gbr, (size_t)2 * B * (n + 1) * L * L * N);
@@ -262,6 +262,8 @@ class EngineImpl final : public Engine {
     M_.alloc(sizeof(T) * max_m);
     s1c_.alloc(sizeof(T) * B * L);
     mv_.alloc(sizeof(double) * 2 * B);
+    err_.alloc(sizeof(int));
+    STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
     in_f64_.alloc(sizeof(double) * B * npix(0));
     field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + M_.bytes + in_f64_.bytes;
     // partial sums of the row-centric adjoint
@@ -337,12 +339,18 @@ class EngineImpl final : public Engine {
       prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(T), (double)B * L * N * E * 10.0, s,
                    [&] {
                      products_forward<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), X_[0].as<T>(), partials_.as<double>(),
-                                         sums_.as<double>() + sum_off_[n], s);
+                                         sums_.as<double>() + sum_off_[n], err_.as<int>(), s);
                    });
     }
     STL_CUDA(cudaMemcpyAsync(h_sums_.data(), sums_.p, h_sums_.size() * 8, cudaMemcpyDeviceToHost, s));
+    int err = 0;
+    STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     STL_CUDA(cudaStreamSynchronize(s));
     prof_.collect();
+    if (err) {
+      STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
+      throw std::runtime_error("a wait on a staged device copy timed out in the coefficient products");
+    }
     assemble(values, moments ? var : nullptr);
     forward_done_ = true;
     timers.forward_ms += ms_since(t0);
@@ -549,7 +557,7 @@ class EngineImpl final : public Engine {
   std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
-  DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_;
+  DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_;
   DevMem adj_part_;
   AdjScratch adj_;
   const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }

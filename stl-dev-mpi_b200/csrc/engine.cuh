@@ -194,15 +194,21 @@ struct ProductShape {
   int B = 1;
   i64 N = 0;         // pixels of the level
   bool level0 = false;
-  int blocks = 0;    // partial sums per map
+  int blocks = 0;    // partial sums per map (pixel ranges)
   int slots = 0;     // doubles per (b, l3) partial
+  int items = 0;     // Gram items per (b, l3)
+  int item_chunks = 0, items_per_cta = 0, groups = 0;
+  int px_chunk = 0;  // pixels per staged chunk
+  i64 chunk = 0;     // pixels per range
+  size_t smem = 0;   // two stages of staged chunks
 };
-ProductShape product_shape(int n, int L, int B, i64 N);
+ProductShape product_shape(int n, int L, int B, i64 N, size_t elem);
 // z [N][B][L], br [N][B][(n+1) L][L] complex, x0 [N][B] (level 0) ->
 // sums [B][L][slots] (FP64)
+// *err becomes nonzero when a wait on a staged copy timed out.
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials,
-                      double* sums, cudaStream_t s);
+                      double* sums, int* err, cudaStream_t s);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,

@@ -453,130 +453,217 @@ __global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, int g
 // v = (branch[d][l1][l3] for d <= n, l1 < L; z[l3]).  Every S3/S4
 // coefficient of the level is an entry of the Hermitian Gram matrix
 // sum_p v v^H: S4 in the 4 x 4 blocks (d1, d2), d1 <= d2, of the branches,
-// S3 in the blocks (d, z), S2 its (z, z) entry.  Work items, for every l3:
-// the (d1, d2) blocks, the (d, z) blocks and one item for the per-pixel sums
-// (|z|, |z|^2, |z|^4 and, at level 0, x, x^2, x^4).  One warp per item,
-// one lane per pixel of a 32-pixel tile staged in shared memory; sums in
-// FP64 (products of the FP32 or FP64 operands), reduced across lanes and
-// then across blocks in a fixed order.  Partial layout per (block, b, l3), in
-// doubles:
+// S3 in the blocks (d, z), S2 its (z, z) entry.  Items per l3: the (d1, d2)
+// blocks, the (d, z) blocks and one item for the per-pixel sums (|z|,
+// |z|^2, |z|^4 and, at level 0, x, x^2, x^4).  Partial layout per (block,
+// b, l3), in doubles:
 //   BB block t (d1 <= d2, d1-major): [t 48 .. +32) 16 complex (l1, l2)
 //                                    [t 48 + 32 .. +16) 16 sums |a|^2 |b|^2
 //   Bz block d: [nBB 48 + 12 d .. +8) 4 complex (l1, z), then 4 second sums
 //   z item:     [nBB 48 + 12 (n + 1) .. +6) |z|, |z|^2, |z|^4, x, x^2, x^4
-constexpr int kTile = 32;        // pixels per tile
-constexpr int kTileP = kTile + 1;  // padded tile stride in shared memory
+//
+// A CTA takes a contiguous pixel range of all maps and a chunk of the items.
+// Chunks of PC pixels (branch rows and z of every map: contiguous bytes)
+// stream into shared memory by bulk asynchronous copies (cp.async.bulk,
+// completion on an mbarrier), two stages deep, so a chunk is in flight
+// while the previous one is summed.  Thread (group g, map b, item, l3), l3
+// fastest; group g takes the pixels g, g + G, ... of a chunk.  Sums are FP64
+// (products of the FP32 or FP64 operands), reduced over the groups and then
+// over the CTAs in a fixed order.  Every wait on a copy is bounded: on
+// timeout the CTA records the failure in *err and stops.
+constexpr int kProdThreads = 256;
+constexpr int kProdStageBytes = 40 * 1024;
+constexpr int kWaitLimit = 1 << 20;
 
-// stage v[l][i][px] (i < K1: branch i; i == K1: z) of the tile at p0
-template <typename T>
-__device__ __forceinline__ void stage_tile(typename V2<T>::type* v, int stride, int K1, int L, int B, int b, i64 p0,
-                                           i64 N, int np, const T* br, const T* z) {
-  typedef typename V2<T>::type T2;
-  const int K = K1 + 1;
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
-  for (int idx = tid; idx < np * K * L; idx += nt) {
-    const int px = idx / (K * L), rem = idx % (K * L);
-    const int i = rem / L, l = rem % L;
-    const i64 p = p0 + px;
-    T2 a;
-    a.x = (T)0; a.y = (T)0;
-    if (p < N) {
-      const T* src = i < K1 ? br + (((p * B + b) * K1 + i) * L + l) * 2 : z + ((p * B + b) * L + l) * 2;
-      a.x = src[0]; a.y = src[1];
-    }
-    v[(l * K + i) * stride + px] = a;
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+  const uint32_t a = smem_u32(bar);
+  for (int i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
   }
+  return false;
 }
 
-__device__ __forceinline__ double warp_sum(double a) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-  return a;
-}
-
-// One block per (tile range, map b, item w): blockDim (32, L), warp y = l3,
-// lane = pixel of a 32-pixel tile.  The L warps read the same sectors of the
-// pixel-major fields (their l3 values interleave), which L1 shares.
 template <typename T>
-__global__ void __launch_bounds__(128) k_products(int nd, int L, i64 N, int B, const T* __restrict__ z,
-                                                  const T* __restrict__ br, const T* __restrict__ x0, int slots,
-                                                  int ntiles, double* __restrict__ partials) {
+__global__ void __launch_bounds__(kProdThreads, 2) k_products(int nd, i64 N, int B, const T* __restrict__ z,
+                                                              const T* __restrict__ br, const T* __restrict__ x0,
+                                                              int slots, int IB, int G, int PC, i64 chunk,
+                                                              double* __restrict__ partials, int* __restrict__ err) {
   typedef typename V2<T>::type T2;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double red[kProdThreads];
+  __shared__ int fail;
+  constexpr int L = 4;
   const int K1 = nd * L;
-  const int b = blockIdx.y, w = blockIdx.z, lane = threadIdx.x, l3 = threadIdx.y;
-  const int nBB = nd * (nd + 1) / 2;
-  int kind = 2, d1 = 0, d2 = 0;
-  if (w < nBB) {
+  const int nBB = nd * (nd + 1) / 2, I = 2 * nBB + nd + 1;
+  const int t = threadIdx.x;
+  const int l3 = t & 3, q = t >> 2;
+  const int il = q % IB, rest = q / IB;
+  const int b = rest % B, grp = rest / B;
+  const int item = blockIdx.z * IB + il;
+  const bool active = grp < G && item < I;
+  // kind 0: half h (columns l2 = 2h, 2h + 1) of BB block tb = (d1, d2)
+  int kind = 2, d1 = 0, d2 = 0, tb = 0, h = 0;
+  if (item < 2 * nBB) {
     kind = 0;
-    int t = w;
-    while (t >= nd - d1) { t -= nd - d1; ++d1; }
-    d2 = d1 + t;
-  } else if (w < nBB + nd) {
+    tb = item >> 1;
+    h = item & 1;
+    int r = tb;
+    while (r >= nd - d1) { r -= nd - d1; ++d1; }
+    d2 = d1 + r;
+  } else if (item < 2 * nBB + nd) {
     kind = 1;
-    d1 = w - nBB;
+    d1 = item - 2 * nBB;
   }
+  // stage s: branch rows [PC][B][K1][L], then z [PC][B][L]
+  const size_t br_px = (size_t)B * K1 * L, z_px = (size_t)B * L;  // T2 per pixel
+  const size_t stage_t2 = (size_t)PC * (br_px + z_px);
+  T2* stage0 = reinterpret_cast<T2*>(smem);
+  const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
+  const int nchunks = P1 > P0 ? (int)((P1 - P0 + PC - 1) / PC) : 0;
   const T2* brv = reinterpret_cast<const T2*>(br);
   const T2* zv = reinterpret_cast<const T2*>(z);
-  double acc[48];
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int c) {
+    const int st = c & 1;
+    const i64 pc = P0 + (i64)c * PC;
+    const int np = (int)min((i64)PC, P1 - pc);
+    T2* sb = stage0 + st * stage_t2;
+    T2* sz = sb + (size_t)PC * br_px;
+    const unsigned nb = (unsigned)(np * br_px * sizeof(T2)), nz = (unsigned)(np * z_px * sizeof(T2));
+    mbar_expect_tx(&bar[st], nb + nz);
+    bulk_g2s(sb, brv + pc * br_px, nb, &bar[st]);
+    bulk_g2s(sz, zv + pc * z_px, nz, &bar[st]);
+  };
+  if (t == 0) {
+    if (nchunks > 0) issue(0);
+    if (nchunks > 1) issue(1);
+  }
+  double acc[24];
 #pragma unroll
-  for (int i = 0; i < 48; ++i) acc[i] = 0.0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const i64 p = (i64)tile * kTile + lane;
-    if (p >= N) break;
-    const i64 row = (p * B + b) * K1;  // branch (d, l1) of (p, b) at row + d L + l1, gauge l3
-    if (kind == 0) {
-      double ar[4], ai[4], bR[4], bI[4], am[4], bm[4];
+  for (int i = 0; i < 24; ++i) acc[i] = 0.0;
+  int c = 0;
+  for (; c < nchunks; ++c) {
+    const int st = c & 1;
+    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    __syncthreads();
+    if (fail) break;
+    const i64 pc = P0 + (i64)c * PC;
+    const int np = (int)min((i64)PC, P1 - pc);
+    const T2* sb = stage0 + st * stage_t2;
+    const T2* sz = sb + (size_t)PC * br_px;
+    if (active) {
+      for (int j = grp; j < np; j += G) {
+        const T2* rowp = sb + ((size_t)j * B + b) * K1 * L + l3;  // row r at rowp[r L]
+        if (kind == 0) {
+          double ar[4], ai[4], am[4], bR[2], bI[2], bm[2];
 #pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        const T2 x = brv[(row + d1 * 4 + l) * L + l3], y = brv[(row + d2 * 4 + l) * L + l3];
-        ar[l] = x.x; ai[l] = x.y; bR[l] = y.x; bI[l] = y.y;
-        am[l] = ar[l] * ar[l] + ai[l] * ai[l];
-        bm[l] = bR[l] * bR[l] + bI[l] * bI[l];
-      }
+          for (int l = 0; l < 4; ++l) {
+            const T2 x = rowp[(d1 * 4 + l) * L];
+            ar[l] = x.x; ai[l] = x.y;
+            am[l] = ar[l] * ar[l] + ai[l] * ai[l];
+          }
 #pragma unroll
-      for (int l1 = 0; l1 < 4; ++l1)
+          for (int l = 0; l < 2; ++l) {
+            const T2 y = rowp[(d2 * 4 + 2 * h + l) * L];
+            bR[l] = y.x; bI[l] = y.y;
+            bm[l] = bR[l] * bR[l] + bI[l] * bI[l];
+          }
+          // acc: [0, 16) complex (l1, l2 - 2h) at 2 (2 l1 + l2 - 2h); [16, 24) |a|^2 |b|^2
 #pragma unroll
-        for (int l2 = 0; l2 < 4; ++l2) {
-          const int e = l1 * 4 + l2;
-          acc[2 * e] = fma(ar[l1], bR[l2], fma(ai[l1], bI[l2], acc[2 * e]));
-          acc[2 * e + 1] = fma(ai[l1], bR[l2], fma(-ar[l1], bI[l2], acc[2 * e + 1]));
-          acc[32 + e] = fma(am[l1], bm[l2], acc[32 + e]);
+          for (int l1 = 0; l1 < 4; ++l1)
+#pragma unroll
+            for (int l2 = 0; l2 < 2; ++l2) {
+              const int e = l1 * 2 + l2;
+              acc[2 * e] = fma(ar[l1], bR[l2], fma(ai[l1], bI[l2], acc[2 * e]));
+              acc[2 * e + 1] = fma(ai[l1], bR[l2], fma(-ar[l1], bI[l2], acc[2 * e + 1]));
+              acc[16 + e] = fma(am[l1], bm[l2], acc[16 + e]);
+            }
+        } else if (kind == 1) {
+          const T2 zz = sz[((size_t)j * B + b) * L + l3];
+          const double zr = zz.x, zi = zz.y, zm = zr * zr + zi * zi;
+#pragma unroll
+          for (int l = 0; l < 4; ++l) {
+            const T2 x = rowp[(d1 * 4 + l) * L];
+            const double xr = x.x, xi = x.y;
+            acc[2 * l] = fma(xr, zr, fma(xi, zi, acc[2 * l]));
+            acc[2 * l + 1] = fma(xi, zr, fma(-xr, zi, acc[2 * l + 1]));
+            acc[8 + l] = fma(xr * xr + xi * xi, zm, acc[8 + l]);
+          }
+        } else {
+          const T2 zz = sz[((size_t)j * B + b) * L + l3];
+          const double m = hypot((double)zz.x, (double)zz.y);
+          const double m2 = m * m;
+          acc[0] += m;
+          acc[1] += m2;
+          acc[2] += m2 * m2;
+          if (x0 && l3 == 0) {
+            const double xv = (double)x0[(pc + j) * B + b];
+            const double x2 = xv * xv;
+            acc[3] += xv;
+            acc[4] += x2;
+            acc[5] += x2 * x2;
+          }
         }
-    } else if (kind == 1) {
-      const T2 zz = zv[(p * B + b) * L + l3];
-      const double zr = zz.x, zi = zz.y, zm = zr * zr + zi * zi;
-#pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        const T2 x = brv[(row + d1 * 4 + l) * L + l3];
-        const double xr = x.x, xi = x.y;
-        acc[2 * l] = fma(xr, zr, fma(xi, zi, acc[2 * l]));
-        acc[2 * l + 1] = fma(xi, zr, fma(-xr, zi, acc[2 * l + 1]));
-        acc[8 + l] = fma(xr * xr + xi * xi, zm, acc[8 + l]);
-      }
-    } else {
-      const T2 zz = zv[(p * B + b) * L + l3];
-      const double m = hypot((double)zz.x, (double)zz.y);
-      const double m2 = m * m;
-      acc[0] += m;
-      acc[1] += m2;
-      acc[2] += m2 * m2;
-      if (x0 && l3 == 0) {
-        const double xv = (double)x0[p * B + b];
-        const double x2 = xv * xv;
-        acc[3] += xv;
-        acc[4] += x2;
-        acc[5] += x2 * x2;
       }
     }
+    __syncthreads();  // the stage is read: refill it
+    if (t == 0 && c + 2 < nchunks) issue(c + 2);
   }
-  const int n_i = kind == 0 ? 48 : (kind == 1 ? 12 : 6);
-  const int base = kind == 0 ? w * 48 : (kind == 1 ? nBB * 48 + (w - nBB) * 12 : nBB * 48 + nd * 12);
+  if (fail) {
+    // wait (bounded) for the copies still in flight into this CTA's stages
+    for (int k = c; k < min(nchunks, c + 2); ++k) mbar_wait(&bar[k & 1], (k >> 1) & 1);
+    if (t == 0) atomicExch(err, 1);
+  }
+  // sum over the groups in group order; group 0 writes the CTA's partials
+  const int n_i = kind == 0 ? 24 : (kind == 1 ? 12 : 6);
+  const int base = kind == 0 ? tb * 48 : (kind == 1 ? nBB * 48 + (item - 2 * nBB) * 12 : nBB * 48 + nd * 12);
   double* out = partials + (((i64)blockIdx.x * B + b) * L + l3) * slots + base;
+  const int per_group = 4 * IB * B;
 #pragma unroll
-  for (int i = 0; i < 48; ++i) {
-    if (i >= n_i) break;
-    const double t = warp_sum(acc[i]);
-    if (lane == 0) out[i] = t;
+  for (int i = 0; i < 24; ++i) {
+    red[t] = acc[i];
+    __syncthreads();
+    if (active && grp == 0 && i < n_i) {
+      double a = 0.0;
+      for (int g = 0; g < G; ++g) a += red[t + g * per_group];
+      int o = i;
+      if (kind == 0) {  // back to the block layout: e = l1 * 4 + l2
+        const int e2 = i < 16 ? (i >> 1) : i - 16;
+        const int e = (e2 >> 1) * 4 + 2 * h + (e2 & 1);
+        o = i < 16 ? 2 * e + (i & 1) : 32 + e;
+      }
+      out[o] = a;
+    }
+    __syncthreads();
   }
 }
 
@@ -592,57 +679,60 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
 }
 
 // gv = M v per pixel and l3 (M: K x K complex of the coefficient cotangents
-// of one (b, l3)); gz additionally gets s1c z / |z| (auto S1).  Block: TP
-// pixels (threadIdx.x) x L orientations (threadIdx.y); the tile is staged in
-// shared memory both ways so global accesses stay coalesced.
-template <typename T>
-__global__ void k_products_rev(int nd, int L, i64 N, int B, int TP, const T* __restrict__ z, const T* __restrict__ br,
-                               const T* __restrict__ M, const T* __restrict__ s1c, T* __restrict__ gz,
-                               T* __restrict__ gbr) {
+// of one (b, l3), in shared memory); gz additionally gets s1c z / |z| (auto
+// S1).  Thread (pixel, l3), l3 fastest, holds v in registers; CTAs stride
+// over 64-pixel tiles of one map.
+constexpr int kRevThreads = 256;
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, const T* __restrict__ z,
+                                                              const T* __restrict__ br, const T* __restrict__ M,
+                                                              const T* __restrict__ s1c, T* __restrict__ gz,
+                                                              T* __restrict__ gbr) {
   extern __shared__ __align__(16) unsigned char smem[];
   typedef typename V2<T>::type T2;
-  const int K1 = nd * L, K = K1 + 1;
-  const int st = TP + 1;                    // padded tile stride
-  T2* m = reinterpret_cast<T2*>(smem);      // [L][K][K]
-  T2* v = m + (size_t)L * K * K;            // [L][K][st]
-  T2* gv = v + (size_t)L * K * st;          // [L][K][st]
-  const int b = blockIdx.y, px = threadIdx.x, l3 = threadIdx.y;
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  constexpr int L = 4, K1 = K - 1;
+  T2* m = reinterpret_cast<T2*>(smem);  // [L][K][K]
+  const int b = blockIdx.y, t = threadIdx.x;
   const T2* Mb = reinterpret_cast<const T2*>(M) + (i64)b * L * K * K;
-  for (int i = tid; i < L * K * K; i += nt) m[i] = Mb[i];
-  const i64 p0 = (i64)blockIdx.x * TP;
-  stage_tile<T>(v, st, K1, L, B, b, p0, N, TP, br, z);
+  for (int i = t; i < L * K * K; i += kRevThreads) m[i] = Mb[i];
   __syncthreads();
-  const T2* ml = m + (size_t)l3 * K * K;
-  const T2* vl = v + (size_t)l3 * K * st;
-  for (int i = 0; i < K; ++i) {
-    T ar = (T)0, ai = (T)0;
-    for (int j = 0; j < K; ++j) {
-      const T2 mm = ml[i * K + j], vv = vl[j * st + px];
-      ar = fma(mm.x, vv.x, fma(-mm.y, vv.y, ar));
-      ai = fma(mm.x, vv.y, fma(mm.y, vv.x, ai));
+  const int l3 = t & 3, px = t >> 2;
+  const T2* ml = m + l3 * K * K;
+  const T c1 = s1c[(i64)b * L + l3];
+  const T2* brv = reinterpret_cast<const T2*>(br);
+  const T2* zv = reinterpret_cast<const T2*>(z);
+  T2* gbrv = reinterpret_cast<T2*>(gbr);
+  T2* gzv = reinterpret_cast<T2*>(gz);
+  constexpr int TPX = kRevThreads / 4;
+  for (i64 p = (i64)blockIdx.x * TPX + px; p < N; p += (i64)gridDim.x * TPX) {
+    const i64 row = (p * B + b) * K1;
+    T2 v[K];
+#pragma unroll
+    for (int i = 0; i < K1; ++i) v[i] = brv[(row + i) * L + l3];
+    v[K1] = zv[(p * B + b) * L + l3];
+#pragma unroll 1
+    for (int i = 0; i < K; ++i) {
+      T ar = (T)0, ai = (T)0;
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const T2 mm = ml[i * K + j];
+        ar = fma(mm.x, v[j].x, fma(-mm.y, v[j].y, ar));
+        ai = fma(mm.x, v[j].y, fma(mm.y, v[j].x, ai));
+      }
+      T2 o;
+      if (i == K1) {
+        const T mag = hypot(v[K1].x, v[K1].y);
+        const T c = c1 / (mag == (T)0 ? (T)1 : mag);
+        o.x = ar + c * v[K1].x;
+        o.y = ai + c * v[K1].y;
+        gzv[(p * B + b) * L + l3] = o;
+      } else {
+        o.x = ar;
+        o.y = ai;
+        gbrv[(row + i) * L + l3] = o;
+      }
     }
-    if (i == K1) {
-      const T2 zz = vl[K1 * st + px];
-      const T mag = hypot(zz.x, zz.y);
-      const T c = s1c[(i64)b * L + l3] / (mag == (T)0 ? (T)1 : mag);
-      ar += c * zz.x;
-      ai += c * zz.y;
-    }
-    T2 o;
-    o.x = ar; o.y = ai;
-    gv[((size_t)l3 * K + i) * st + px] = o;
-  }
-  __syncthreads();
-  for (int idx = tid; idx < TP * K * L; idx += nt) {
-    const int q = idx / (K * L), rem = idx % (K * L);
-    const int i = rem / L, l = rem % L;
-    const i64 p = p0 + q;
-    if (p >= N) continue;
-    const T2 o = gv[((size_t)l * K + i) * st + q];
-    T* dst = i < K1 ? gbr + (((p * B + b) * K1 + i) * L + l) * 2 : gz + ((p * B + b) * L + l) * 2;
-    dst[0] = o.x;
-    dst[1] = o.y;
   }
 }
 
@@ -829,29 +919,56 @@ void modulus_vjp_add(const T* z, const T* g, int g_pix, int g_row, T* gz, i64 N,
   STL_CUDA(cudaGetLastError());
 }
 
-ProductShape product_shape(int n, int L, int B, i64 N) {
+ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
+  if (L != 4) throw std::runtime_error("the products are built for L = 4");
   ProductShape sh;
   sh.nd = n + 1;
   sh.K = sh.nd * L + 1;
   sh.L = L; sh.B = B; sh.N = N; sh.level0 = n == 0;
   const int nBB = sh.nd * (sh.nd + 1) / 2;
   sh.slots = nBB * 48 + sh.nd * 12 + 6;
-  const int items = nBB + sh.nd + 1;  // blocks of the Gram matrix per (b, l3)
-  const i64 ntiles = (N + kTile - 1) / kTile;
-  // about 16 blocks of 4 warps per SM over (tile ranges, b, items)
-  sh.blocks = (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)148 * 16 / std::max(1, B * items)));
+  sh.items = 2 * nBB + sh.nd + 1;  // half BB blocks, Bz blocks, the per-pixel item
+  if (4 * B > kProdThreads) throw std::runtime_error("batch too large for the products kernel (64 maps)");
+  const int ib_max = std::max(1, kProdThreads / (4 * B));
+  sh.item_chunks = (sh.items + ib_max - 1) / ib_max;
+  sh.items_per_cta = (sh.items + sh.item_chunks - 1) / sh.item_chunks;
+  sh.groups = std::max(1, kProdThreads / (4 * sh.items_per_cta * B));
+  const size_t px_bytes = (size_t)B * sh.K * L * 2 * elem;
+  sh.px_chunk = (int)std::max<size_t>(1, kProdStageBytes / px_bytes);
+  // about 2 CTAs per SM over (pixel ranges, item chunks); ranges of at
+  // least 4 pixel chunks
+  const i64 want = std::max<i64>(1, (i64)148 * 2 / sh.item_chunks);
+  const i64 most = std::max<i64>(1, N / (4 * (i64)sh.px_chunk));
+  sh.blocks = (int)std::max<i64>(1, std::min(want, most));
+  sh.chunk = (N + sh.blocks - 1) / sh.blocks;
+  sh.smem = 2 * (size_t)sh.px_chunk * px_bytes;
   return sh;
 }
 
+namespace {
+template <typename T, int K>
+void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
+                        cudaStream_t s) {
+  const size_t smem = (size_t)4 * K * K * 2 * sizeof(T);
+  if (smem > 48 * 1024)
+    STL_CUDA(cudaFuncSetAttribute(k_products_rev<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const i64 tiles = (sh.N + kRevThreads / 4 - 1) / (kRevThreads / 4);
+  const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 / sh.B));
+  dim3 grid(gx, sh.B);
+  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, z, br, M, s1c, gz, gbr);
+}
+}  // namespace
+
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials, double* sums,
-                      cudaStream_t s) {
+                      int* err, cudaStream_t s) {
   const int L = sh.L, nd = sh.nd;
-  const int items = nd * (nd + 1) / 2 + nd + 1;
-  const int ntiles = (int)((sh.N + kTile - 1) / kTile);
-  dim3 grid(sh.blocks, sh.B, items), block(32, L);
-  k_products<T><<<grid, block, 0, s>>>(nd, L, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots, ntiles,
-                                       partials);
+  if (sh.smem > 48 * 1024)
+    STL_CUDA(cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+  dim3 grid(sh.blocks, 1, sh.item_chunks);
+  const int threads = 4 * sh.items_per_cta * sh.B * sh.groups;
+  k_products<T><<<grid, threads, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots,
+                                                sh.items_per_cta, sh.groups, sh.px_chunk, sh.chunk, partials, err);
   STL_CUDA(cudaGetLastError());
   const i64 total = (i64)sh.B * L * sh.slots;
   k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
@@ -862,16 +979,19 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
                       cudaStream_t s) {
-  const int K = sh.K, L = sh.L;
-  auto bytes = [&](int tp) { return ((size_t)L * K * K + 2 * (size_t)L * K * (tp + 1)) * 2 * sizeof(T); };
-  int TP = 32;
-  while (TP > 4 && bytes(TP) > 200 * 1024) TP /= 2;
-  const size_t smem = bytes(TP);
-  if (smem > 227 * 1024) throw std::runtime_error("coefficient cotangents exceed shared memory");
-  if (smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(k_products_rev<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(nblocks(sh.N, TP), sh.B), block(TP, L);
-  k_products_rev<T><<<grid, block, smem, s>>>(sh.nd, L, sh.N, sh.B, TP, z, br, M, s1c, gz, gbr);
+  switch (sh.nd) {
+    case 1: products_reverse_k<T, 5>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 2: products_reverse_k<T, 9>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 3: products_reverse_k<T, 13>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 4: products_reverse_k<T, 17>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 5: products_reverse_k<T, 21>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 6: products_reverse_k<T, 25>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 7: products_reverse_k<T, 29>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 8: products_reverse_k<T, 33>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 9: products_reverse_k<T, 37>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 10: products_reverse_k<T, 41>(sh, z, br, M, s1c, gz, gbr, s); break;
+    default: throw std::runtime_error("more levels than the products are built for (10)");
+  }
   STL_CUDA(cudaGetLastError());
 }
 
@@ -905,7 +1025,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*);                            \
   template void dec_apply<T>(const DecOp&, bool, const T*, int, int, T*, int, int, int, int, bool, cudaStream_t); \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
-  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, double*, double*,          \
+  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, double*, double*, int*,    \
                                     cudaStream_t);                                                                \
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, T*, T*,          \
                                     cudaStream_t);                                                                \
