@@ -247,6 +247,20 @@ class EngineImpl final : public Engine {
       field_bytes_ += X_[n].bytes + Z_[n].bytes + Mod_[n].bytes + Br_[n].bytes + gMod_[n].bytes + gX_[n].bytes;
     }
     partials_.alloc(sizeof(double) * max_part);
+    {
+      size_t nr = 0;
+      for (int n = 0; n < levels_; ++n) nr += shapes_[n].roles.size();
+      roles_.alloc(sizeof(int32_t) * nr);
+      size_t off = 0;
+      for (int n = 0; n < levels_; ++n) {
+        const auto& r = shapes_[n].roles;
+        STL_CUDA(cudaMemcpyAsync(roles_.as<int32_t>() + off, r.data(), sizeof(int32_t) * r.size(),
+                                 cudaMemcpyHostToDevice, stream_));
+        shapes_[n].d_roles = roles_.as<int32_t>() + off;
+        off += r.size();
+      }
+      STL_CUDA(cudaStreamSynchronize(stream_));
+    }
     size_t total_sums = 0;
     sum_off_.resize(levels_);
     for (int n = 0; n < levels_; ++n) {
@@ -557,7 +571,7 @@ class EngineImpl final : public Engine {
   std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
-  DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_;
+  DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_, roles_;
   DevMem adj_part_;
   AdjScratch adj_;
   const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }

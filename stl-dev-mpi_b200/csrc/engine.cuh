@@ -197,10 +197,13 @@ struct ProductShape {
   int blocks = 0;    // partial sums per map (pixel ranges)
   int slots = 0;     // doubles per (b, l3) partial
   int items = 0;     // Gram items per (b, l3)
-  int item_chunks = 0, items_per_cta = 0, groups = 0;
+  int item_chunks = 0;  // role chunks (grid z)
+  int warps = 0;     // warps per CTA
+  std::vector<int32_t> roles;      // [item_chunks][warps]: role | replica << 16 | replicas << 24, or -1
+  const int32_t* d_roles = nullptr;  // the same on the device
   int px_chunk = 0;  // pixels per staged chunk
   i64 chunk = 0;     // pixels per range
-  size_t smem = 0;   // two stages of staged chunks
+  size_t smem = 0;   // staged chunks
 };
 ProductShape product_shape(int n, int L, int B, i64 N, size_t elem);
 // z [N][B][L], br [N][B][(n+1) L][L] complex, x0 [N][B] (level 0) ->

@@ -462,17 +462,26 @@ __global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, int g
 //   Bz block d: [nBB 48 + 12 d .. +8) 4 complex (l1, z), then 4 second sums
 //   z item:     [nBB 48 + 12 (n + 1) .. +6) |z|, |z|^2, |z|^4, x, x^2, x^4
 //
-// A CTA takes a contiguous pixel range of all maps and a chunk of the items.
-// Chunks of PC pixels (branch rows and z of every map: contiguous bytes)
-// stream into shared memory by bulk asynchronous copies (cp.async.bulk,
-// completion on an mbarrier), two stages deep, so a chunk is in flight
-// while the previous one is summed.  Thread (group g, map b, item, l3), l3
-// fastest; group g takes the pixels g, g + G, ... of a chunk.  Sums are FP64
-// (products of the FP32 or FP64 operands), reduced over the groups and then
-// over the CTAs in a fixed order.  Every wait on a copy is bounded: on
-// timeout the CTA records the failure in *err and stops.
-constexpr int kProdThreads = 256;
-constexpr int kProdStageBytes = 40 * 1024;
+// A CTA takes a contiguous pixel range of all maps.  Chunks of PC pixels
+// (branch rows and z of every map: contiguous bytes) stream into shared
+// memory by bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier), kProdStages deep.  Every warp has one role -- a (map, item)
+// pair -- and a replica index: replica r of P takes every P-th iteration
+// of its role over a chunk.  Lanes of a role:
+//   BB block (d1, d2): (l3, l1, half h); entries (l1, 2h), (l1, 2h + 1);
+//                      one pixel per iteration
+//   Bz block d:        (l3, l1, x); entry (l1, z) of pixel 2 it + x
+//   per-pixel item:    (l3, q); pixel 8 it + q
+// so a warp never diverges on the item kind and its shared-memory reads hit
+// distinct banks.  Roles and replica counts come from a table balanced by
+// cost (product_shape); the CTA's replicas and lanes are summed in a fixed
+// order, then the CTAs in k_reduce_partials.  In FP32 mode the products and
+// the sums over one chunk are FP32 (at most a few dozen pixels per lane),
+// added into FP64 sums after every chunk; FP64 mode sums in FP64.  Every wait
+// on a copy is bounded: on timeout the CTA records the failure in *err.
+constexpr int kProdMaxWarps = 32;
+constexpr int kProdStages = 3;
+constexpr int kProdStageBytes = 48 * 1024;
 constexpr int kWaitLimit = 1 << 20;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -505,37 +514,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kProdThreads, 2) k_products(int nd, i64 N, int B, const T* __restrict__ z,
-                                                              const T* __restrict__ br, const T* __restrict__ x0,
-                                                              int slots, int IB, int G, int PC, i64 chunk,
-                                                              double* __restrict__ partials, int* __restrict__ err) {
+__global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
+    int nd, i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0, int slots,
+    const int32_t* __restrict__ roles, int W, int PC, i64 chunk, double* __restrict__ partials,
+    int* __restrict__ err) {
   typedef typename V2<T>::type T2;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[2];
-  __shared__ double red[kProdThreads];
+  __shared__ __align__(8) uint64_t bar[kProdStages];
   __shared__ int fail;
   constexpr int L = 4;
   const int K1 = nd * L;
-  const int nBB = nd * (nd + 1) / 2, I = 2 * nBB + nd + 1;
-  const int t = threadIdx.x;
-  const int l3 = t & 3, q = t >> 2;
-  const int il = q % IB, rest = q / IB;
-  const int b = rest % B, grp = rest / B;
-  const int item = blockIdx.z * IB + il;
-  const bool active = grp < G && item < I;
-  // kind 0: half h (columns l2 = 2h, 2h + 1) of BB block tb = (d1, d2)
-  int kind = 2, d1 = 0, d2 = 0, tb = 0, h = 0;
-  if (item < 2 * nBB) {
+  const int nBB = nd * (nd + 1) / 2, I = nBB + nd + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t rc = roles[(i64)blockIdx.z * W + warp];
+  const bool active = rc >= 0;
+  const int role = active ? (rc & 0xFFFF) : 0, rep = (rc >> 16) & 0xFF, nrep = active ? (rc >> 24) & 0xFF : 1;
+  const int b = role / I, item = role % I;
+  int kind = 2, d1 = 0, d2 = 0;
+  if (item < nBB) {
     kind = 0;
-    tb = item >> 1;
-    h = item & 1;
-    int r = tb;
+    int r = item;
     while (r >= nd - d1) { r -= nd - d1; ++d1; }
     d2 = d1 + r;
-  } else if (item < 2 * nBB + nd) {
+  } else if (item < nBB + nd) {
     kind = 1;
-    d1 = item - 2 * nBB;
+    d1 = item - nBB;
   }
+  const int l3 = lane & 3, l1 = (lane >> 2) & 3, hx = lane >> 4, q8 = lane >> 2;
   // stage s: branch rows [PC][B][K1][L], then z [PC][B][L]
   const size_t br_px = (size_t)B * K1 * L, z_px = (size_t)B * L;  // T2 per pixel
   const size_t stage_t2 = (size_t)PC * (br_px + z_px);
@@ -544,16 +549,15 @@ __global__ void __launch_bounds__(kProdThreads, 2) k_products(int nd, i64 N, int
   const int nchunks = P1 > P0 ? (int)((P1 - P0 + PC - 1) / PC) : 0;
   const T2* brv = reinterpret_cast<const T2*>(br);
   const T2* zv = reinterpret_cast<const T2*>(z);
-  if (t == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kProdStages; ++st) mbar_init(&bar[st], 1);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int c) {
-    const int st = c & 1;
+    const int st = c % kProdStages;
     const i64 pc = P0 + (i64)c * PC;
     const int np = (int)min((i64)PC, P1 - pc);
     T2* sb = stage0 + st * stage_t2;
@@ -563,17 +567,17 @@ __global__ void __launch_bounds__(kProdThreads, 2) k_products(int nd, i64 N, int
     bulk_g2s(sb, brv + pc * br_px, nb, &bar[st]);
     bulk_g2s(sz, zv + pc * z_px, nz, &bar[st]);
   };
-  if (t == 0) {
-    if (nchunks > 0) issue(0);
-    if (nchunks > 1) issue(1);
-  }
-  double acc[24];
+  if (threadIdx.x == 0)
+    for (int c = 0; c < min(nchunks, kProdStages); ++c) issue(c);
+  constexpr bool kSplit = sizeof(T) == 4;  // FP32: chunk sums in FP32, then FP64
+  double acc[6];
+  T f[6];
 #pragma unroll
-  for (int i = 0; i < 24; ++i) acc[i] = 0.0;
+  for (int i = 0; i < 6; ++i) { acc[i] = 0.0; f[i] = (T)0; }
   int c = 0;
   for (; c < nchunks; ++c) {
-    const int st = c & 1;
-    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    const int st = c % kProdStages;
+    if (!mbar_wait(&bar[st], (c / kProdStages) & 1)) fail = 1;
     __syncthreads();
     if (fail) break;
     const i64 pc = P0 + (i64)c * PC;
@@ -581,89 +585,119 @@ __global__ void __launch_bounds__(kProdThreads, 2) k_products(int nd, i64 N, int
     const T2* sb = stage0 + st * stage_t2;
     const T2* sz = sb + (size_t)PC * br_px;
     if (active) {
-      for (int j = grp; j < np; j += G) {
-        const T2* rowp = sb + ((size_t)j * B + b) * K1 * L + l3;  // row r at rowp[r L]
-        if (kind == 0) {
-          double ar[4], ai[4], am[4], bR[2], bI[2], bm[2];
-#pragma unroll
-          for (int l = 0; l < 4; ++l) {
-            const T2 x = rowp[(d1 * 4 + l) * L];
-            ar[l] = x.x; ai[l] = x.y;
-            am[l] = ar[l] * ar[l] + ai[l] * ai[l];
+      if (kind == 0) {
+        const int ra = (d1 * 4 + l1) * L + l3, rb = (d2 * 4 + 2 * hx) * L + l3;
+        for (int j = rep; j < np; j += nrep) {
+          const T2* rowp = sb + ((size_t)j * B + b) * K1 * L;
+          const T2 a = rowp[ra], y0 = rowp[rb], y1 = rowp[rb + L];
+          const T am = fma(a.x, a.x, a.y * a.y);
+          f[0] = fma(a.x, y0.x, fma(a.y, y0.y, f[0]));
+          f[1] = fma(a.y, y0.x, fma(-a.x, y0.y, f[1]));
+          f[2] = fma(a.x, y1.x, fma(a.y, y1.y, f[2]));
+          f[3] = fma(a.y, y1.x, fma(-a.x, y1.y, f[3]));
+          f[4] = fma(am, fma(y0.x, y0.x, y0.y * y0.y), f[4]);
+          f[5] = fma(am, fma(y1.x, y1.x, y1.y * y1.y), f[5]);
+        }
+      } else if (kind == 1) {
+        const int ra = (d1 * 4 + l1) * L + l3;
+        const int ni = (np + 1) >> 1;
+        for (int it = rep; it < ni; it += nrep) {
+          const int j = 2 * it + hx;
+          if (j < np) {
+            const T2 x = sb[((size_t)j * B + b) * K1 * L + ra];
+            const T2 zz = sz[((size_t)j * B + b) * L + l3];
+            f[0] = fma(x.x, zz.x, fma(x.y, zz.y, f[0]));
+            f[1] = fma(x.y, zz.x, fma(-x.x, zz.y, f[1]));
+            f[2] = fma(fma(x.x, x.x, x.y * x.y), fma(zz.x, zz.x, zz.y * zz.y), f[2]);
           }
-#pragma unroll
-          for (int l = 0; l < 2; ++l) {
-            const T2 y = rowp[(d2 * 4 + 2 * h + l) * L];
-            bR[l] = y.x; bI[l] = y.y;
-            bm[l] = bR[l] * bR[l] + bI[l] * bI[l];
-          }
-          // acc: [0, 16) complex (l1, l2 - 2h) at 2 (2 l1 + l2 - 2h); [16, 24) |a|^2 |b|^2
-#pragma unroll
-          for (int l1 = 0; l1 < 4; ++l1)
-#pragma unroll
-            for (int l2 = 0; l2 < 2; ++l2) {
-              const int e = l1 * 2 + l2;
-              acc[2 * e] = fma(ar[l1], bR[l2], fma(ai[l1], bI[l2], acc[2 * e]));
-              acc[2 * e + 1] = fma(ai[l1], bR[l2], fma(-ar[l1], bI[l2], acc[2 * e + 1]));
-              acc[16 + e] = fma(am[l1], bm[l2], acc[16 + e]);
+        }
+      } else {
+        const int ni = (np + 7) >> 3;
+        for (int it = rep; it < ni; it += nrep) {
+          const int j = 8 * it + q8;
+          if (j < np) {
+            const T2 zz = sz[((size_t)j * B + b) * L + l3];
+            const double m = hypot((double)zz.x, (double)zz.y);
+            const double m2 = m * m;
+            acc[0] += m;
+            acc[1] += m2;
+            acc[2] += m2 * m2;
+            if (x0 && l3 == 0) {
+              const double xv = (double)x0[(pc + j) * B + b];
+              const double x2 = xv * xv;
+              acc[3] += xv;
+              acc[4] += x2;
+              acc[5] += x2 * x2;
             }
-        } else if (kind == 1) {
-          const T2 zz = sz[((size_t)j * B + b) * L + l3];
-          const double zr = zz.x, zi = zz.y, zm = zr * zr + zi * zi;
-#pragma unroll
-          for (int l = 0; l < 4; ++l) {
-            const T2 x = rowp[(d1 * 4 + l) * L];
-            const double xr = x.x, xi = x.y;
-            acc[2 * l] = fma(xr, zr, fma(xi, zi, acc[2 * l]));
-            acc[2 * l + 1] = fma(xi, zr, fma(-xr, zi, acc[2 * l + 1]));
-            acc[8 + l] = fma(xr * xr + xi * xi, zm, acc[8 + l]);
-          }
-        } else {
-          const T2 zz = sz[((size_t)j * B + b) * L + l3];
-          const double m = hypot((double)zz.x, (double)zz.y);
-          const double m2 = m * m;
-          acc[0] += m;
-          acc[1] += m2;
-          acc[2] += m2 * m2;
-          if (x0 && l3 == 0) {
-            const double xv = (double)x0[(pc + j) * B + b];
-            const double x2 = xv * xv;
-            acc[3] += xv;
-            acc[4] += x2;
-            acc[5] += x2 * x2;
           }
         }
       }
     }
+    if (kSplit) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        acc[i] += (double)f[i];
+        f[i] = (T)0;
+      }
+    }
     __syncthreads();  // the stage is read: refill it
-    if (t == 0 && c + 2 < nchunks) issue(c + 2);
+    if (threadIdx.x == 0 && c + kProdStages < nchunks) issue(c + kProdStages);
   }
   if (fail) {
     // wait (bounded) for the copies still in flight into this CTA's stages
-    for (int k = c; k < min(nchunks, c + 2); ++k) mbar_wait(&bar[k & 1], (k >> 1) & 1);
-    if (t == 0) atomicExch(err, 1);
+    for (int k = c; k < min(nchunks, c + kProdStages); ++k) mbar_wait(&bar[k % kProdStages], (k / kProdStages) & 1);
+    if (threadIdx.x == 0) atomicExch(err, 1);
   }
-  // sum over the groups in group order; group 0 writes the CTA's partials
-  const int n_i = kind == 0 ? 24 : (kind == 1 ? 12 : 6);
-  const int base = kind == 0 ? tb * 48 : (kind == 1 ? nBB * 48 + (item - 2 * nBB) * 12 : nBB * 48 + nd * 12);
-  double* out = partials + (((i64)blockIdx.x * B + b) * L + l3) * slots + base;
-  const int per_group = 4 * IB * B;
+  if (!kSplit) {
 #pragma unroll
-  for (int i = 0; i < 24; ++i) {
-    red[t] = acc[i];
-    __syncthreads();
-    if (active && grp == 0 && i < n_i) {
-      double a = 0.0;
-      for (int g = 0; g < G; ++g) a += red[t + g * per_group];
-      int o = i;
-      if (kind == 0) {  // back to the block layout: e = l1 * 4 + l2
-        const int e2 = i < 16 ? (i >> 1) : i - 16;
-        const int e = (e2 >> 1) * 4 + 2 * h + (e2 & 1);
-        o = i < 16 ? 2 * e + (i & 1) : 32 + e;
-      }
-      out[o] = a;
+    for (int i = 0; i < 6; ++i) acc[i] += (double)f[i];
+  }
+  // replicas of a role are consecutive warps, replica 0 first: sum them in
+  // order (through the stage memory, free now), then the lanes
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(smem);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) red[(warp * 32 + lane) * 6 + i] = acc[i];
+  __syncthreads();
+  if (!active || rep != 0) return;
+  double v[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double a = 0.0;
+    for (int r = 0; r < nrep; ++r) a += red[((warp + r) * 32 + lane) * 6 + i];
+    v[i] = a;
+  }
+  double* out = partials + (((i64)blockIdx.x * B + b) * L + l3) * slots;
+  if (kind == 0) {
+    const int e0 = l1 * 4 + 2 * hx, e1 = e0 + 1;
+    double* o = out + item * 48;
+    o[2 * e0] = v[0];
+    o[2 * e0 + 1] = v[1];
+    o[2 * e1] = v[2];
+    o[2 * e1 + 1] = v[3];
+    o[32 + e0] = v[4];
+    o[32 + e1] = v[5];
+  } else if (kind == 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] += __shfl_down_sync(0xffffffffu, v[i], 16);
+    if (hx == 0) {
+      double* o = out + nBB * 48 + (item - nBB) * 12;
+      o[2 * l1] = v[0];
+      o[2 * l1 + 1] = v[1];
+      o[8 + l1] = v[2];
     }
-    __syncthreads();
+  } else {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      v[i] += __shfl_down_sync(0xffffffffu, v[i], 16);
+      v[i] += __shfl_down_sync(0xffffffffu, v[i], 8);
+      v[i] += __shfl_down_sync(0xffffffffu, v[i], 4);
+    }
+    if (q8 == 0) {
+      double* o = out + nBB * 48 + nd * 12;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) o[i] = (i < 3 || l3 == 0) ? v[i] : 0.0;
+    }
   }
 }
 
@@ -921,27 +955,66 @@ void modulus_vjp_add(const T* z, const T* g, int g_pix, int g_row, T* gz, i64 N,
 
 ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
   if (L != 4) throw std::runtime_error("the products are built for L = 4");
+  if (B > 255) throw std::runtime_error("batch too large for the products kernel");
   ProductShape sh;
   sh.nd = n + 1;
   sh.K = sh.nd * L + 1;
   sh.L = L; sh.B = B; sh.N = N; sh.level0 = n == 0;
   const int nBB = sh.nd * (sh.nd + 1) / 2;
   sh.slots = nBB * 48 + sh.nd * 12 + 6;
-  sh.items = 2 * nBB + sh.nd + 1;  // half BB blocks, Bz blocks, the per-pixel item
-  if (4 * B > kProdThreads) throw std::runtime_error("batch too large for the products kernel (64 maps)");
-  const int ib_max = std::max(1, kProdThreads / (4 * B));
-  sh.item_chunks = (sh.items + ib_max - 1) / ib_max;
-  sh.items_per_cta = (sh.items + sh.item_chunks - 1) / sh.item_chunks;
-  sh.groups = std::max(1, kProdThreads / (4 * sh.items_per_cta * B));
+  const int I = nBB + sh.nd + 1, R = B * I;
+  sh.items = I;
+  // roles (map, item) with a per-pixel cost: BB blocks 8, Bz blocks 3, the
+  // per-pixel item 2; spread over chunks of at most kProdMaxWarps roles
+  // (round robin by decreasing cost), replicated within a chunk in
+  // proportion to cost
+  auto cost = [&](int r) { const int it = r % I; return it < nBB ? 8 : (it < nBB + sh.nd ? 3 : 2); };
+  std::vector<int> order(R);
+  for (int r = 0; r < R; ++r) order[r] = r;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return cost(a) > cost(b2); });
+  sh.item_chunks = (R + kProdMaxWarps - 1) / kProdMaxWarps;
+  std::vector<std::vector<int>> chunk_roles(sh.item_chunks);
+  for (int k = 0; k < R; ++k) chunk_roles[k % sh.item_chunks].push_back(order[k]);
+  std::vector<std::vector<int>> reps(sh.item_chunks);
+  int W = 1;
+  for (int zc = 0; zc < sh.item_chunks; ++zc) {
+    auto& cr = chunk_roles[zc];
+    std::sort(cr.begin(), cr.end());
+    double total = 0.0;
+    for (int r : cr) total += cost(r);
+    auto& P = reps[zc];
+    int sum = 0;
+    for (int r : cr) {
+      P.push_back(std::max(1, (int)std::lround(cost(r) * kProdMaxWarps / total)));
+      sum += P.back();
+    }
+    while (sum > kProdMaxWarps) {
+      int m = -1;
+      for (int k = 0; k < (int)P.size(); ++k)
+        if (P[k] > 1 && (m < 0 || P[k] > P[m])) m = k;
+      --P[m];
+      --sum;
+    }
+    W = std::max(W, sum);
+  }
+  sh.warps = W;
+  sh.roles.assign((size_t)sh.item_chunks * W, -1);
+  for (int zc = 0; zc < sh.item_chunks; ++zc) {
+    int w = 0;
+    for (size_t k = 0; k < chunk_roles[zc].size(); ++k)
+      for (int rp = 0; rp < reps[zc][k]; ++rp)
+        sh.roles[(size_t)zc * W + w++] = chunk_roles[zc][k] | (rp << 16) | (reps[zc][k] << 24);
+  }
   const size_t px_bytes = (size_t)B * sh.K * L * 2 * elem;
-  sh.px_chunk = (int)std::max<size_t>(1, kProdStageBytes / px_bytes);
-  // about 2 CTAs per SM over (pixel ranges, item chunks); ranges of at
-  // least 4 pixel chunks
-  const i64 want = std::max<i64>(1, (i64)148 * 2 / sh.item_chunks);
+  if (px_bytes > (size_t)kProdStageBytes) throw std::runtime_error("a pixel's operands exceed a products stage");
+  sh.px_chunk = (int)(kProdStageBytes / px_bytes);
+  // one CTA per SM over (pixel ranges, role chunks); ranges of at least 4
+  // pixel chunks
+  const i64 want = std::max<i64>(1, (i64)148 / sh.item_chunks);
   const i64 most = std::max<i64>(1, N / (4 * (i64)sh.px_chunk));
   sh.blocks = (int)std::max<i64>(1, std::min(want, most));
   sh.chunk = (N + sh.blocks - 1) / sh.blocks;
-  sh.smem = 2 * (size_t)sh.px_chunk * px_bytes;
+  sh.smem = std::max((size_t)kProdStages * sh.px_chunk * px_bytes, (size_t)W * 32 * 6 * sizeof(double));
   return sh;
 }
 
@@ -963,12 +1036,12 @@ template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials, double* sums,
                       int* err, cudaStream_t s) {
   const int L = sh.L, nd = sh.nd;
+  if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
   if (sh.smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
   dim3 grid(sh.blocks, 1, sh.item_chunks);
-  const int threads = 4 * sh.items_per_cta * sh.B * sh.groups;
-  k_products<T><<<grid, threads, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots,
-                                                sh.items_per_cta, sh.groups, sh.px_chunk, sh.chunk, partials, err);
+  k_products<T><<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots,
+                                                      sh.d_roles, sh.warps, sh.px_chunk, sh.chunk, partials, err);
   STL_CUDA(cudaGetLastError());
   const i64 total = (i64)sh.B * L * sh.slots;
   k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
