@@ -336,7 +336,8 @@ class EngineImpl final : public Engine {
       T* mod = Mod_[n].as<T>();
       const ConvOp& op = conv_[n];
       prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, true), conv_flops(op, B), s, [&] {
-        conv_forward<T>(op, X_[n].as<T>(), B, Z_[n].as<T>(), mod, B * (n + 1) * L, (n + 1) * L, n * L, s);
+        conv_forward<T>(op, X_[n].as<T>(), B, Z_[n].as<T>(), mod, B * (n + 1) * L, (n + 1) * L, n * L, s,
+                        err_.as<int>());
       });
       if (n > 0)
         prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n - 1], B * n * L, false), dec_flops(dec_[n - 1], B * n * L, false),
@@ -346,7 +347,7 @@ class EngineImpl final : public Engine {
                      });
       const int R = B * (n + 1) * L;
       prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
-        conv_forward<T>(op, mod, R, Br_[n].as<T>(), nullptr, 0, 0, 0, s);
+        conv_forward<T>(op, mod, R, Br_[n].as<T>(), nullptr, 0, 0, 0, s, err_.as<int>());
       });
       const ProductShape& sh = shapes_[n];
       double E = sh.K * (sh.K + 1) / 2.0;
@@ -363,7 +364,7 @@ class EngineImpl final : public Engine {
     prof_.collect();
     if (err) {
       STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
-      throw std::runtime_error("a wait on a staged device copy timed out in the coefficient products");
+      throw std::runtime_error("a wait on a staged device copy timed out in the forward sweep");
     }
     assemble(values, moments ? var : nullptr);
     forward_done_ = true;

@@ -111,6 +111,7 @@ struct ConvOp {
   DevMem tile_cells;         // int32 [n_tiles][kAdjCells]
   DevMem tile_ncells;        // int32 [n_tiles]
   DevMem lcell;              // uint16 [S][n_rep]: tile cell of every (slot, row) (build only)
+  DevMem lcell_t;            // uint16 [n_tiles][nch 4][kAdjTile]: the same, tile-major, slots padded to 4
   DevMem tile_ent;           // uint16 [n_tiles][S kAdjTile]: slot % kAdjSC << 8 | row
   DevMem tile_off;           // uint16 [n_tiles][nch][ncs]: first entry of (chunk, tile cell)
   DevMem coff;               // int64 [stored cells + 1]
@@ -119,7 +120,7 @@ struct ConvOp {
   double mean_slots = 0.0;   // cells read per row, averaged over the rows
   size_t bytes() const {
     return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + tile_cells.bytes + tile_ncells.bytes + lcell.bytes +
-           tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
+           lcell_t.bytes + tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
   }
 };
 constexpr int kAdjTile = 256;    // stored rows per adjoint tile
@@ -171,9 +172,11 @@ void build_dec(const DecSpec& spec, DType dtype, DecOp& out, cudaStream_t stream
 //  conv_adjoint: gy [n_rows][R][4] complex -> gx [n_in][R] (or += gx).
 //  dec_apply: y[c][ro][ri] = (D or D^T) x, row (ro, ri) of pixel c at
 //    c pix + ro outer + ri.
+//  With err (device int, set on a timed-out copy wait), operators with tile
+//  tables use the tiled forward; otherwise the per-row gather.
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                  cudaStream_t s);
+                  cudaStream_t s, int* err = nullptr);
 //  With scratch, operators with tile tables use the row-centric two-phase
 //  adjoint; otherwise the transposed gather.
 template <typename T>

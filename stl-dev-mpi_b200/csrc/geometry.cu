@@ -331,6 +331,18 @@ __global__ void k_adj_csr(const int32_t* cell, const uint16_t* lcell, int S, i64
   }
 }
 
+// lcell [S][n_rep] -> tile-major [n_tiles][nch * 4][kAdjTile] (slots padded
+// to a multiple of 4 with index 0: their coefficients are never read)
+__global__ void k_lcell_tiles(const uint16_t* lcell, int S, i64 n_rep, int S4, i64 n_tiles, uint16_t* out) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_tiles * S4 * kAdjTile) return;
+  const i64 tile = i / ((i64)S4 * kAdjTile);
+  const int rem = (int)(i % ((i64)S4 * kAdjTile));
+  const int s = rem / kAdjTile, ul = rem % kAdjTile;
+  const i64 u = tile * kAdjTile + ul;
+  out[i] = (s < S && u < n_rep) ? lcell[(i64)s * n_rep + u] : (uint16_t)0;
+}
+
 // Tile cells -> stored input cells: cell c of a tile is rotation j of
 // stored cell v (nk = 4: c in face 4m + j; nk = 1: v = c, j = 0).
 __device__ __forceinline__ void tile_cell_owner(int32_t c, int nk, int o2, i64& v, int& j) {
@@ -717,7 +729,16 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
                                                         op.tile_ent.as<uint16_t>(), op.tile_off.as<uint16_t>());
     STL_CUDA(cudaGetLastError());
   }
-  op.lcell.release();
+  {
+    const int S4 = ((op.S + 3) / 4) * 4;
+    op.lcell_t.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * S4 * kAdjTile);
+    const i64 n = op.n_tiles * S4 * kAdjTile;
+    k_lcell_tiles<<<nblocks(n, 256), 256, 0, s>>>(op.lcell.as<uint16_t>(), op.S, a.n_rows, S4, op.n_tiles,
+                                                  op.lcell_t.as<uint16_t>());
+    STL_CUDA(cudaGetLastError());
+    STL_CUDA(cudaStreamSynchronize(s));
+    op.lcell.release();
+  }
   // per stored input cell: the (tile, cell, rotation) entries holding its sums
   {
     const i64 n_in_rep = n_cells;

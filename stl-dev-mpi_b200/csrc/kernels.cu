@@ -41,6 +41,40 @@ __device__ __forceinline__ i64 rot_cell(i64 c, int k, int o2) {
   return (((f & ~i64(3)) | ((f + k) & 3)) << o2) | (c & ((i64(1) << o2) - 1));
 }
 
+// ---- bulk asynchronous copies ------------------------------------------------
+// Every wait on an mbarrier is bounded (kWaitLimit polls); a kernel that
+// gives up records the failure in an error flag the host reads.
+constexpr int kWaitLimit = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+  const uint32_t a = smem_u32(bar);
+  for (int i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // 8 values of one (slot, row): float4 x 2 or double2 x 4
 __device__ __forceinline__ void load8(const float* p, float w[8]) {
   float4 a = __ldg(reinterpret_cast<const float4*>(p));
@@ -51,6 +85,19 @@ __device__ __forceinline__ void load8(const double* p, double w[8]) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     double2 a = __ldg(reinterpret_cast<const double2*>(p) + k);
+    w[2 * k] = a.x; w[2 * k + 1] = a.y;
+  }
+}
+// the same from shared memory (plain loads: __ldg reads global memory only)
+__device__ __forceinline__ void load8_shared(const float* p, float w[8]) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0];
+  const float4 b = reinterpret_cast<const float4*>(p)[1];
+  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w; w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+}
+__device__ __forceinline__ void load8_shared(const double* p, double w[8]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double2 a = reinterpret_cast<const double2*>(p)[k];
     w[2 * k] = a.x; w[2 * k + 1] = a.y;
   }
 }
@@ -167,6 +214,136 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ ce
 #pragma unroll
         for (int g = 0; g < 4; ++g) m[g] = hypot(o[2 * g], o[2 * g + 1]);
       }
+    }
+  }
+}
+
+// Tiled forward: a CTA takes a tile of kAdjTile stored rows and RB input
+// rows; thread (row, rotation k), k fastest, so the 4 rotations of a row
+// share each coefficient read.  The CTA gathers the tile's cells (4
+// rotations x RB values) into shared memory once; the coefficients and
+// tile-cell indices of the tile stream through shared memory in chunks of
+// SC slots, two stages deep, by bulk asynchronous copies.
+constexpr int kFwdThreads = 4 * kAdjTile;
+
+template <typename T>
+__host__ __device__ constexpr int fwd_sc() { return sizeof(T) == 4 ? 8 : 4; }
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
+    const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2,
+    const int32_t* __restrict__ tile_cells, const int32_t* __restrict__ tile_nc, const T* __restrict__ x, int R,
+    T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err) {
+  constexpr int SC = fwd_sc<T>();
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int fail;
+  // stage: coef [SC][kAdjTile][8] T, then indices [SC][kAdjTile] uint16
+  constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
+  constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
+  T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][nc][RB]
+  const int tile = blockIdx.y, tid = threadIdx.x;
+  const int k = tid & 3, row = tid >> 2;
+  const int r0 = blockIdx.x * RB;
+  const int nc = tile_nc[tile];
+  const i64 u0 = (i64)tile * kAdjTile;
+  const int rows = (int)min((i64)kAdjTile, n_rep - u0);
+  const int S4 = ((S + 3) / 4) * 4;  // slots per tile in the tile-major index table
+  const int nch = (S + SC - 1) / SC;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int c) {
+    const int st = c & 1;
+    unsigned char* base = smem_raw + st * kStage;
+    const int s0 = c * SC, sn = min(SC, S - s0);
+    const int sn4 = min(SC, S4 - s0);  // index rows are padded to 4 slots
+    const unsigned cb = (unsigned)(rows * 8 * sizeof(T));
+    const unsigned lb = (unsigned)(sn4 * kAdjTile * sizeof(uint16_t));
+    mbar_expect_tx(&bar[st], sn * cb + lb);
+    for (int sl = 0; sl < sn; ++sl)
+      bulk_g2s(base + (size_t)sl * kAdjTile * 8 * sizeof(T), coef + ((i64)(s0 + sl) * n_rep + u0) * 8, cb, &bar[st]);
+    bulk_g2s(base + kStageCoef, lcell_t + ((i64)tile * S4 + s0) * kAdjTile, lb, &bar[st]);
+  };
+  if (tid == 0) {
+    issue(0);
+    if (nch > 1) issue(1);
+  }
+  const int32_t* tc = tile_cells + (i64)tile * kAdjCells;
+  for (int i = tid; i < 4 * nc; i += kFwdThreads) {
+    const int kk = i / nc, lc = i - kk * nc;
+    const i64 c = rot_cell(tc[lc], kk, o2);
+    T v[RB];
+    loadR<RB>(x + c * R + r0, v);
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) sx[(size_t)i * RB + rb] = v[rb];
+  }
+  T acc[RB][8];
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[rb][j] = (T)0;
+  const T* sxk = sx + (size_t)k * nc * RB;
+  int c = 0;
+  for (; c < nch; ++c) {
+    const int st = c & 1;
+    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    __syncthreads();  // also orders the cell gather before the first chunk
+    if (fail) break;
+    const unsigned char* base = smem_raw + st * kStage;
+    const T* cs = reinterpret_cast<const T*>(base);
+    const uint16_t* ls = reinterpret_cast<const uint16_t*>(base + kStageCoef);
+    const int sn = min(SC, S - c * SC);
+    if (row < rows) {
+#pragma unroll
+      for (int sl = 0; sl < SC; ++sl) {
+        if (sl < sn) {
+          T w[8];
+          load8_shared(cs + ((size_t)sl * kAdjTile + row) * 8, w);
+          T xv[RB];
+          const T* xs = sxk + (size_t)ls[sl * kAdjTile + row] * RB;
+#pragma unroll
+          for (int rb = 0; rb < RB; ++rb) xv[rb] = xs[rb];
+#pragma unroll
+          for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[rb][j] = fma(w[j], xv[rb], acc[rb][j]);
+        }
+      }
+    }
+    __syncthreads();  // the stage is read: refill it
+    if (tid == 0 && c + 2 < nch) issue(c + 2);
+  }
+  if (fail) {
+    for (int q = c; q < min(nch, c + 2); ++q) mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  if (row >= rows) return;
+  const i64 p = rot_pixel(u0 + row, k, o2);
+  const bool odd = k & 1;
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb) {
+    const int r = r0 + rb;
+    T o[8];
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      // stored gauge of output gauge g under rotation k: g, or g ^ 2 for odd k
+      const T re = odd ? acc[rb][2 * (g ^ 2)] : acc[rb][2 * g];
+      const T im = odd ? acc[rb][2 * (g ^ 2) + 1] : acc[rb][2 * g + 1];
+      o[2 * g] = re;
+      o[2 * g + 1] = rot_conj(k, g) ? -im : im;
+    }
+    store8(out + (p * R + r) * 8, o);
+    if (mod) {
+      T* m = mod + p * mod_pix + (i64)r * mod_row + mod_off;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) m[g] = hypot(o[2 * g], o[2 * g + 1]);
     }
   }
 }
@@ -482,36 +659,6 @@ __global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, int g
 constexpr int kProdMaxWarps = 32;
 constexpr int kProdStages = 3;
 constexpr int kProdStageBytes = 48 * 1024;
-constexpr int kWaitLimit = 1 << 20;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
-  const uint32_t a = smem_u32(bar);
-  for (int i = 0; i < kWaitLimit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(a), "r"(phase)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
 
 template <typename T>
 __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
@@ -896,10 +1043,36 @@ inline int adj_rb(size_t elem, int R) { return (elem == 4 && R % 2 == 0) ? 2 : 1
 
 }  // namespace
 
+template <typename T, int RB>
+size_t fwd_tiles_smem(const ConvOp& op) {
+  const size_t stage = (size_t)fwd_sc<T>() * kAdjTile * (8 * sizeof(T) + sizeof(uint16_t));
+  return 2 * stage + sizeof(T) * 4 * (size_t)op.max_tile_cells * RB;
+}
+
+template <typename T, int RB>
+void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row,
+                           int mod_off, int* err, cudaStream_t s) {
+  const size_t smem = fwd_tiles_smem<T, RB>(op);
+  if (smem > 48 * 1024)
+    STL_CUDA(cudaFuncSetAttribute(k_conv_fwd_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(R / RB, (unsigned)op.n_tiles);
+  k_conv_fwd_tiles<T, RB><<<grid, kFwdThreads, smem, s>>>(op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S,
+                                                          op.n_rep, op.o2, op.tile_cells.as<int32_t>(),
+                                                          op.tile_ncells.as<int32_t>(), x, R, out, mod, mod_pix,
+                                                          mod_row, mod_off, err);
+}
+
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                  cudaStream_t s) {
-  if (op.nk == 4) conv_forward_nk<T, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+                  cudaStream_t s, int* err) {
+  constexpr int RBmax = sizeof(T) == 4 ? 4 : 2;
+  const int RB = R % RBmax == 0 ? RBmax : (R % 2 == 0 ? 2 : 1);
+  const bool fits = (RB == RBmax ? fwd_tiles_smem<T, RBmax>(op) : fwd_tiles_smem<T, 2>(op)) <= 220 * 1024;
+  if (err && op.nk == 4 && op.adj_tiles && op.lcell_t.p && op.n_tiles <= 65535 && fits) {
+    if (RB == RBmax) conv_forward_tiles_rb<T, RBmax>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, s);
+    else if (RB == 2) conv_forward_tiles_rb<T, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, s);
+    else conv_forward_tiles_rb<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, s);
+  } else if (op.nk == 4) conv_forward_nk<T, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
   else conv_forward_nk<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
   STL_CUDA(cudaGetLastError());
 }
@@ -1094,7 +1267,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
 }
 
 #define INST(T)                                                                                                   \
-  template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t);               \
+  template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t, int*);               \
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*);                            \
   template void dec_apply<T>(const DecOp&, bool, const T*, int, int, T*, int, int, int, int, bool, cudaStream_t); \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
