@@ -321,10 +321,16 @@ int stlp_restore(StlpHandle* h, const StlpSnapshot* s, uint64_t generation, uint
 
 int stlp_forward_levels(StlpHandle* h, const double* x, size_t n, double* out) {
   return guard<int>(-1, [&] {
-    require(h != nullptr, "null handle");
-    (void)x; (void)n; (void)out;
-    throw std::runtime_error("stlp_forward_levels is not built in this library yet");
-    return -1;
+    require(h != nullptr && x != nullptr && out != nullptr, "null argument");
+    size_t want = 0;
+    for (int d = 0; d < h->engine->levels(); ++d) want += (size_t)h->engine->options().B * h->engine->npix(d);
+    require(n == want, "input shape mismatch");
+    for (size_t i = 0; i < n; ++i) require(std::isfinite(x[i]), "input map contains non-finite values");
+    h->activate();
+    h->has_current = false;  // a validation sweep: no vjp or checkpoint follows it
+    h->engine->load_levels(x);
+    h->engine->forward(false, out, nullptr);
+    return 0;
   });
 }
 

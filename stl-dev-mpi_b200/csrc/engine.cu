@@ -302,6 +302,21 @@ class EngineImpl final : public Engine {
     prof_.launch(Profiler::ELEM, 1, n * (8.0 + sizeof(T)), 0.0, stream_,
                  [&] { to_pixel_major<double, T>(in_f64_.as<double>(), X_[0].as<T>(), npix(0), opt_.B, stream_); });
     loaded_ = true;
+    levels_given_ = false;
+  }
+
+  void load_levels(const double* x) override {
+    prepare();
+    size_t off = 0;
+    for (int d = 0; d < levels_; ++d) {
+      const size_t n = (size_t)opt_.B * npix(d);
+      STL_CUDA(cudaMemcpyAsync(in_f64_.p, x + off, n * 8, cudaMemcpyHostToDevice, stream_));
+      to_pixel_major<double, T>(in_f64_.as<double>(), X_[d].as<T>(), npix(d), opt_.B, stream_);
+      STL_CUDA(cudaStreamSynchronize(stream_));  // the staging buffer is reused for the next level
+      off += n;
+    }
+    loaded_ = true;
+    levels_given_ = true;
   }
 
   void load_device(const void* x, bool f32) override {
@@ -312,6 +327,7 @@ class EngineImpl final : public Engine {
       else to_pixel_major<double, T>(static_cast<const double*>(x), X_[0].as<T>(), npix(0), opt_.B, stream_);
     });
     loaded_ = true;
+    levels_given_ = false;
   }
 
   void save_input(std::vector<double>& x) override {
@@ -327,7 +343,7 @@ class EngineImpl final : public Engine {
     auto t0 = std::chrono::steady_clock::now();
     const int L = opt_.L, B = opt_.B;
     cudaStream_t s = stream_;
-    for (int d = 0; d + 1 < levels_; ++d)
+    for (int d = 0; d + 1 < levels_ && !levels_given_; ++d)
       prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[d], B, false), dec_flops(dec_[d], B, false), s, [&] {
         dec_apply<T>(dec_[d], false, X_[d].as<T>(), B, 0, X_[d + 1].as<T>(), B, 0, 1, B, false, s);
       });
@@ -567,6 +583,7 @@ class EngineImpl final : public Engine {
 
   Profiler prof_;
   bool ready_ = false, loaded_ = false, forward_done_ = false;
+  bool levels_given_ = false;  // X_[d] for d > 0 were loaded, not decimated
   std::vector<ConvOp> conv_;
   std::vector<DecOp> dec_;
   std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;

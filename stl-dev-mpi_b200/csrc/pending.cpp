@@ -1,4 +1,4 @@
-// Entry points whose engines are added next (L-BFGS driver, disc patches).
+// Entry points whose engine is added next (disc patches).
 #include <string>
 
 #include "../../include/stl_b200.h"
@@ -15,7 +15,6 @@ int fail(const char* what) {
 }  // namespace
 
 extern "C" {
-int64_t stlp_lbfgs(double*, size_t, const char*, stlp_callback, void*) { return fail("stlp_lbfgs"); }
 StlpPatchHandle* stlp_patch_new(const char*) { fail("stlp_patch_new"); return nullptr; }
 void stlp_patch_free(StlpPatchHandle*) {}
 char* stlp_patch_info(StlpPatchHandle*) { fail("stlp_patch_info"); return nullptr; }

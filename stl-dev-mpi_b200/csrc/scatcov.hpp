@@ -73,6 +73,10 @@ class Engine {
   // Loads maps [B][N_0] from host (f64) or device memory (f64 or f32).
   virtual void load_host(const double* x) = 0;
   virtual void load_device(const void* x, bool f32) = 0;
+  // Maps given at every level (host f64, the concatenation over d of
+  // [B][12 (nside / 2^d)^2]): the next forward uses them instead of the
+  // decimation pyramid of level 0.
+  virtual void load_levels(const double* x) = 0;
   // Forward sweep on the loaded maps: values [B][np] complex (interleaved),
   // var [B][np] when moments.  Host outputs; the call synchronises.
   virtual void forward(bool moments, double* values, double* var) = 0;

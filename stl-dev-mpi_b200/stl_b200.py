@@ -190,6 +190,19 @@ class NativeEngine:
         """Per kernel class since the last reset: launches, ms, algorithmic bytes and flops."""
         return {k["name"]: k for k in self.info()["kernels"]}
 
+    def forward_levels(self, levels):
+        """Statistics of maps given at every level (no decimation of level 0; for
+        validation, no vjp follows): levels[d] [batch, 12 (nside/2^d)^2]
+        (native.py:292-303)."""
+        with self._mutex:
+            self._open()
+            x = np.ascontiguousarray(np.concatenate([np.asarray(v, dtype=np.float64).ravel() for v in levels]))
+            values = np.empty((self.batch, self.ncoeff), dtype=np.complex128)
+            self._current_key = None
+            if self._lib.stlp_forward_levels(self._handle, _ptr(x), x.size, _ptr(values.view(np.float64))):
+                raise _error()
+            return values
+
     def native_pixels(self):
         with self._mutex:
             self._open()
@@ -362,3 +375,70 @@ def scattering(engine, x):
     if _ScatCov is None:
         _ScatCov = _function()
     return _ScatCov.apply(x, engine)
+
+
+def native_lbfgs(callback, x, options=None):
+    """L-BFGS with the strong Wolfe line search (stlp_lbfgs) of
+    ``callback(x) -> (loss, gradient)`` from ``x``; a float64 C-contiguous ``x``
+    is updated in place.  Options: lr, max_iter, max_eval, tolerance_grad,
+    tolerance_change, history_size.  Returns (x, report) as native.py:1023-1056."""
+    resolved = dict(lr=1.0, max_iter=20, max_eval=None, tolerance_grad=1e-12, tolerance_change=1e-15,
+                    history_size=10)
+    if options:
+        unknown = set(options) - set(resolved)
+        if unknown:
+            raise ValueError(f"unknown native L-BFGS options: {sorted(unknown)}")
+        resolved.update(options)
+    for k in ("max_iter", "history_size"):
+        if isinstance(resolved[k], bool) or int(resolved[k]) != resolved[k] or resolved[k] < 1:
+            raise ValueError(f"{k} must be a positive integer")
+    if resolved["max_eval"] is not None and (int(resolved["max_eval"]) != resolved["max_eval"]
+                                             or resolved["max_eval"] < 1):
+        raise ValueError("max_eval must be a positive integer or None")
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.size == 0 or not np.isfinite(x).all():
+        raise ValueError("finite nonempty initial point required")
+    shape, history, errors = x.shape, [], []
+
+    @_CALLBACK
+    def evaluate(p, n, gp, _context):
+        try:
+            trial = np.ctypeslib.as_array(p, shape=(n,)).reshape(shape)
+            trial.flags.writeable = False
+            value, grad = callback(trial)
+            grad = np.asarray(grad, dtype=np.float64)
+            if grad.shape != shape:
+                raise ValueError(f"gradient shape {grad.shape} != {shape}")
+            np.ctypeslib.as_array(gp, shape=(n,))[:] = grad.ravel()
+            history.append(float(value))
+            return float(value)
+        except BaseException as exc:  # reported after the native call returns
+            errors.append(exc)
+            return float("nan")
+
+    count = lib().stlp_lbfgs(_ptr(x), x.size, json.dumps(resolved).encode(), evaluate, None)
+    if errors:
+        raise errors[0]
+    if count < 0:
+        raise _error()
+    return x, dict(evaluations=int(count), loss_history=history, options=resolved,
+                   optimizer="native L-BFGS", line_search="strong_wolfe")
+
+
+def synthesis_objective(engine, target, weights=None):
+    """Loss sum_k w_k |S_k(x) - T_k|^2 of maps x [batch, npix] and its gradient
+    (the synthesis objective of crates/stl-mpi/src/synthesis.rs:207-270):
+    a callback for native_lbfgs that evaluates S and the VJP on the engine."""
+    target = np.asarray(target, dtype=np.complex128).reshape(engine.batch, engine.ncoeff)
+    w = np.ones(engine.ncoeff) if weights is None else np.asarray(weights, dtype=np.float64)
+    counter = itertools.count(1)
+
+    def f(x):
+        gen = next(counter)
+        values, _ = engine.forward(np.asarray(x).reshape(engine.batch, -1), generation=gen)
+        r = values - target
+        loss = float(np.sum(w * (r.real ** 2 + r.imag ** 2)))
+        grad = engine.vjp(2.0 * w * r, generation=gen)
+        return loss, grad.reshape(np.shape(x))
+
+    return f

@@ -203,3 +203,13 @@ def test_mask_of_whole_sky_equals_full_sky():
     assert masked.shape == (1, 2, e.ncoeff)
     assert np.max(np.abs(masked[:, 0] - full)) <= 1e-14
     assert np.max(np.abs(masked[:, 1] - full)) <= 1e-14
+
+
+def test_oracle_forward_levels_on_fixture_pyramid():
+    """The oracle's forward_levels on the fixture's level maps gives the golden values."""
+    case = next(c for c in cases("stats", "stats") if c.name == "stats_n16_J3_L4_k5_C1_B1_full_b256")
+    o = O.OracleEngine(16, 3)
+    levels = [case.npy(f"map{d}").reshape(1, -1) for d in range(3)]
+    values = o.forward_levels(levels)
+    ref = case.complex("values").reshape(values.shape)
+    assert close_ratio(values, ref, 1e-11, 1e-10) <= 1.0
