@@ -559,12 +559,14 @@ class EngineImpl final : public Engine {
                                          gBr_.as<T>(), s);
                    });
       const int R = B * (n + 1) * L;
-      prof_.launch(Profiler::CONV_ADJ, 1, conv_bytes(op, R, false, true), conv_flops(op, R), s,
+      prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(T), R, adj_ptr()) ? 2 : 1,
+                   conv_bytes(op, R, false, true), conv_flops(op, R), s,
                    [&] { conv_adjoint<T>(op, gBr_.as<T>(), R, gmod, true, s, adj_ptr()); });
       prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
         modulus_vjp_add<T>(Z_[n].as<T>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<T>(), N, B, L, s);
       });
-      prof_.launch(Profiler::CONV_ADJ, 1, conv_bytes(op, B, false, false), conv_flops(op, B), s,
+      prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(T), B, adj_ptr()) ? 2 : 1,
+                   conv_bytes(op, B, false, false), conv_flops(op, B), s,
                    [&] { conv_adjoint<T>(op, gZ_.as<T>(), B, gX_[n].as<T>(), false, s, adj_ptr()); });
       if (n + 1 < levels_)
         prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
