@@ -292,7 +292,7 @@ StlpSnapshot* stlp_checkpoint(StlpHandle* h) {
     auto s = std::make_unique<StlpSnapshot>();
     s->identity = h->current;
     s->owner = h->id;
-    h->engine->save_input(s->maps);
+    h->engine->save_state(s->maps);
     return s.release();
   });
 }
@@ -310,7 +310,7 @@ int stlp_restore(StlpHandle* h, const StlpSnapshot* s, uint64_t generation, uint
     h->has_current = false;
     // The forward state is recomputed from the saved maps: the sweeps are
     // deterministic, so the restored fields equal the checkpointed ones.
-    h->engine->load_host(s->maps.data());
+    h->engine->load_state(s->maps);
     std::vector<double> values(2 * h->values_len());
     h->engine->forward(false, values.data(), nullptr);
     h->current = s->identity;

@@ -195,6 +195,15 @@ class Profiler {
   }
 };
 
+// Coarse levels of an FP32 engine (nside at most kFp64Nside) run in FP64:
+// there the wavelet answers small fluctuations of smooth fields (the map
+// pyramid, the decimated moduli), and FP32 rounding of those fields and of
+// the wavelet sums would pass the 1e-6 criterion on S1-S3; those levels hold
+// well under 1 % of the work.
+constexpr int kFp64Nside = 32;
+
+template <typename U> struct Tag { typedef U type; };
+
 template <typename T>
 class EngineImpl final : public Engine {
  public:
@@ -206,25 +215,35 @@ class EngineImpl final : public Engine {
     for (size_t i = 0; i < plan_.size(); ++i) map_[i] = locate(plan_[i]);
   }
 
+  // field precision of level n
+  bool hi(int n) const { return sizeof(T) == 8 || (opt_.nside >> n) <= kFp64Nside; }
+  size_t esz(int n) const { return hi(n) ? 8 : sizeof(T); }
+  // f(Tag<U>()) with U the field type of level n
+  template <typename F>
+  void typed(int n, F&& f) {
+    if (hi(n)) f(Tag<double>());
+    else f(Tag<float>());
+  }
+
   void prepare() override {
     if (ready_) return;
     auto t0 = std::chrono::steady_clock::now();
     STL_CUDA(cudaSetDevice(opt_.device));
     const int L = opt_.L, B = opt_.B;
-    DType dt = sizeof(T) == 8 ? DType::F64 : DType::F32;
+    auto dtype_of = [&](int n) { return hi(n) ? DType::F64 : DType::F32; };
     std::vector<double> ker = wavelet_kernel(opt_.ksz, L);
     conv_.resize(levels_);
     dec_.resize(levels_ > 1 ? levels_ - 1 : 0);
     for (int n = 0; n < levels_; ++n) {
       ConvSpec cs;
       cs.nside = opt_.nside >> n; cs.ksz = opt_.ksz; cs.G = L; cs.gauge = 0;
-      build_conv(cs, ker, dt, conv_[n], stream_);
+      build_conv(cs, ker, dtype_of(n), conv_[n], stream_);
       operator_bytes_ += conv_[n].bytes();
     }
     for (int d = 0; d + 1 < levels_; ++d) {
       DecSpec ds;
       ds.nside = opt_.nside >> d;
-      build_dec(ds, dt, dec_[d], stream_);
+      build_dec(ds, dtype_of(d + 1), dec_[d], stream_);  // FP64 weights into an FP64 level
       operator_bytes_ += dec_[d].bytes();
     }
     // fields
@@ -234,16 +253,17 @@ class EngineImpl final : public Engine {
     size_t max_part = 0, max_gz = 0, max_gbr = 0;
     for (int n = 0; n < levels_; ++n) {
       i64 N = npix(n);
-      X_[n].alloc(sizeof(T) * B * N);
-      Z_[n].alloc(sizeof(T) * 2 * B * L * N);
-      Mod_[n].alloc(sizeof(T) * B * (n + 1) * L * N);
-      Br_[n].alloc(sizeof(T) * 2 * B * (n + 1) * L * L * N);
-      gMod_[n].alloc(sizeof(T) * B * (n + 1) * L * N);
-      gX_[n].alloc(sizeof(T) * B * N);
-      shapes_[n] = product_shape(n, L, B, N, sizeof(T));
+      const size_t e = esz(n);
+      X_[n].alloc(e * B * N);
+      Z_[n].alloc(e * 2 * B * L * N);
+      Mod_[n].alloc(e * B * (n + 1) * L * N);
+      Br_[n].alloc(e * 2 * B * (n + 1) * L * L * N);
+      gMod_[n].alloc(e * B * (n + 1) * L * N);
+      gX_[n].alloc(e * B * N);
+      shapes_[n] = product_shape(n, L, B, N, e);
       max_part = std::max(max_part, (size_t)B * L * shapes_[n].blocks * shapes_[n].slots);
-      max_gz = std::max(max_gz, (size_t)2 * B * L * N);
-      max_gbr = std::max(max_gbr, (size_t)2 * B * (n + 1) * L * L * N);
+      max_gz = std::max(max_gz, e * 2 * B * L * N);
+      max_gbr = std::max(max_gbr, e * 2 * B * (n + 1) * L * L * N);
       field_bytes_ += X_[n].bytes + Z_[n].bytes + Mod_[n].bytes + Br_[n].bytes + gMod_[n].bytes + gX_[n].bytes;
     }
     partials_.alloc(sizeof(double) * max_part);
@@ -269,22 +289,29 @@ class EngineImpl final : public Engine {
     }
     sums_.alloc(sizeof(double) * total_sums);
     h_sums_.resize(total_sums);
-    gZ_.alloc(sizeof(T) * max_gz);
-    gBr_.alloc(sizeof(T) * max_gbr);
+    gZ_.alloc(max_gz);
+    gBr_.alloc(max_gbr);
     size_t max_m = 0;
-    for (int n = 0; n < levels_; ++n) max_m = std::max(max_m, (size_t)2 * B * L * shapes_[n].K * shapes_[n].K);
-    M_.alloc(sizeof(T) * max_m);
-    s1c_.alloc(sizeof(T) * B * L);
+    for (int n = 0; n < levels_; ++n)
+      max_m = std::max(max_m, esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K);
+    M_.alloc(max_m);
+    s1c_.alloc(sizeof(double) * B * L);
     mv_.alloc(sizeof(double) * 2 * B);
     err_.alloc(sizeof(int));
     STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
+    // per-row constants of the fields: maps [level][B], moduli [level][B][L],
+    // branch rows of one level, and the partial sums of their means
+    xc_.alloc(sizeof(double) * levels_ * B);
+    zc_.alloc(sizeof(double) * levels_ * B * L);
+    rc_.alloc(sizeof(double) * B * levels_ * L);
+    mpart_.alloc(sizeof(double) * kMeansBlocks * B * L);
     in_f64_.alloc(sizeof(double) * B * npix(0));
     field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + M_.bytes + in_f64_.bytes;
     // partial sums of the row-centric adjoint
     {
       size_t cap = 0;
       for (int n = 0; n < levels_; ++n)
-        cap = std::max(cap, adjoint_part_bytes(conv_[n], sizeof(T), B * (n + 1) * L));
+        cap = std::max(cap, adjoint_part_bytes(conv_[n], esz(n), B * (n + 1) * L));
       if (cap) adj_part_.alloc(cap);
       adj_.part = adj_part_.p;
       adj_.capacity = cap;
@@ -299,8 +326,25 @@ class EngineImpl final : public Engine {
     prepare();
     size_t n = (size_t)opt_.B * npix(0);
     STL_CUDA(cudaMemcpyAsync(in_f64_.p, x, n * 8, cudaMemcpyHostToDevice, stream_));
-    prof_.launch(Profiler::ELEM, 1, n * (8.0 + sizeof(T)), 0.0, stream_,
-                 [&] { to_pixel_major<double, T>(in_f64_.as<double>(), X_[0].as<T>(), npix(0), opt_.B, stream_); });
+    load_maps(in_f64_.as<double>());
+  }
+
+  // level-0 maps (map-major, device) -> constants [B] and pixel-major
+  // deviations; the pyramid levels carry the same constants
+  template <typename Tin>
+  void load_maps(const Tin* x) {
+    const int B = opt_.B;
+    const i64 N = npix(0);
+    prof_.launch(Profiler::ELEM, 3, B * N * (2.0 * sizeof(Tin) + esz(0)), 0.0, stream_, [&] {
+      row_means<Tin>(x, false, false, N, B, mpart_.as<double>(), xc_.as<double>(), stream_);
+      typed(0, [&](auto t) {
+        using U = typename decltype(t)::type;
+        to_pixel_major<Tin, U>(x, X_[0].as<U>(), N, B, stream_, xc_.as<double>());
+      });
+    });
+    for (int d = 1; d < levels_; ++d)
+      STL_CUDA(cudaMemcpyAsync(xc_.as<double>() + d * B, xc_.p, sizeof(double) * B, cudaMemcpyDeviceToDevice,
+                               stream_));
     loaded_ = true;
     levels_given_ = false;
   }
@@ -311,7 +355,12 @@ class EngineImpl final : public Engine {
     for (int d = 0; d < levels_; ++d) {
       const size_t n = (size_t)opt_.B * npix(d);
       STL_CUDA(cudaMemcpyAsync(in_f64_.p, x + off, n * 8, cudaMemcpyHostToDevice, stream_));
-      to_pixel_major<double, T>(in_f64_.as<double>(), X_[d].as<T>(), npix(d), opt_.B, stream_);
+      double* c = xc_.as<double>() + (size_t)d * opt_.B;
+      row_means<double>(in_f64_.as<double>(), false, false, npix(d), opt_.B, mpart_.as<double>(), c, stream_);
+      typed(d, [&](auto t) {
+        using U = typename decltype(t)::type;
+        to_pixel_major<double, U>(in_f64_.as<double>(), X_[d].as<U>(), npix(d), opt_.B, stream_, c);
+      });
       STL_CUDA(cudaStreamSynchronize(stream_));  // the staging buffer is reused for the next level
       off += n;
     }
@@ -321,18 +370,45 @@ class EngineImpl final : public Engine {
 
   void load_device(const void* x, bool f32) override {
     prepare();
-    i64 n = (i64)opt_.B * npix(0);
-    prof_.launch(Profiler::ELEM, 1, n * ((f32 ? 4.0 : 8.0) + sizeof(T)), 0.0, stream_, [&] {
-      if (f32) to_pixel_major<float, T>(static_cast<const float*>(x), X_[0].as<T>(), npix(0), opt_.B, stream_);
-      else to_pixel_major<double, T>(static_cast<const double*>(x), X_[0].as<T>(), npix(0), opt_.B, stream_);
+    if (f32) load_maps(static_cast<const float*>(x));
+    else load_maps(static_cast<const double*>(x));
+  }
+
+  // the level-0 deviations (exact in FP64) and their constants
+  void save_state(std::vector<double>& st) override {
+    const size_t n = (size_t)opt_.B * npix(0);
+    st.resize(n + opt_.B);
+    typed(0, [&](auto t) {
+      using U = typename decltype(t)::type;
+      convert<U, double>(X_[0].as<U>(), in_f64_.as<double>(), (i64)n, stream_);
     });
+    STL_CUDA(cudaMemcpyAsync(st.data(), in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
+    STL_CUDA(cudaMemcpyAsync(st.data() + n, xc_.p, sizeof(double) * opt_.B, cudaMemcpyDeviceToHost, stream_));
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
+  void load_state(const std::vector<double>& st) override {
+    prepare();
+    const size_t n = (size_t)opt_.B * npix(0);
+    if (st.size() != n + (size_t)opt_.B) throw std::runtime_error("checkpoint of another configuration");
+    STL_CUDA(cudaMemcpyAsync(in_f64_.p, st.data(), n * 8, cudaMemcpyHostToDevice, stream_));
+    typed(0, [&](auto t) {
+      using U = typename decltype(t)::type;
+      convert<double, U>(in_f64_.as<double>(), X_[0].as<U>(), (i64)n, stream_);
+    });
+    for (int d = 0; d < levels_; ++d)
+      STL_CUDA(cudaMemcpyAsync(xc_.as<double>() + (size_t)d * opt_.B, st.data() + n, sizeof(double) * opt_.B,
+                               cudaMemcpyHostToDevice, stream_));
+    STL_CUDA(cudaStreamSynchronize(stream_));
     loaded_ = true;
     levels_given_ = false;
   }
 
   void save_input(std::vector<double>& x) override {
     i64 n = (i64)opt_.B * npix(0);
-    to_map_major<T, double>(X_[0].as<T>(), in_f64_.as<double>(), npix(0), opt_.B, stream_);
+    typed(0, [&](auto t) {
+      using U = typename decltype(t)::type;
+      to_map_major<U, double>(X_[0].as<U>(), in_f64_.as<double>(), npix(0), opt_.B, stream_, xc_.as<double>());
+    });
     x.resize(n);
     STL_CUDA(cudaMemcpyAsync(x.data(), in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
     STL_CUDA(cudaStreamSynchronize(stream_));
@@ -345,34 +421,16 @@ class EngineImpl final : public Engine {
     cudaStream_t s = stream_;
     for (int d = 0; d + 1 < levels_ && !levels_given_; ++d)
       prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[d], B, false), dec_flops(dec_[d], B, false), s, [&] {
-        dec_apply<T>(dec_[d], false, X_[d].as<T>(), B, 0, X_[d + 1].as<T>(), B, 0, 1, B, false, s);
+        typed(d, [&](auto ti) {
+          typed(d + 1, [&](auto to) {
+            using Ui = typename decltype(ti)::type;
+            using Uo = typename decltype(to)::type;
+            dec_apply<Ui, Uo>(dec_[d], false, X_[d].as<Ui>(), B, 0, X_[d + 1].as<Uo>(), B, 0, 1, B, false, s);
+          });
+        });
       });
-    for (int n = 0; n < levels_; ++n) {
-      i64 N = npix(n);
-      T* mod = Mod_[n].as<T>();
-      const ConvOp& op = conv_[n];
-      prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, true), conv_flops(op, B), s, [&] {
-        conv_forward<T>(op, X_[n].as<T>(), B, Z_[n].as<T>(), mod, B * (n + 1) * L, (n + 1) * L, n * L, s,
-                        err_.as<int>());
-      });
-      if (n > 0)
-        prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n - 1], B * n * L, false), dec_flops(dec_[n - 1], B * n * L, false),
-                     s, [&] {
-                       dec_apply<T>(dec_[n - 1], false, Mod_[n - 1].as<T>(), B * n * L, n * L, mod, B * (n + 1) * L,
-                                    (n + 1) * L, B, n * L, false, s);
-                     });
-      const int R = B * (n + 1) * L;
-      prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
-        conv_forward<T>(op, mod, R, Br_[n].as<T>(), nullptr, 0, 0, 0, s, err_.as<int>());
-      });
-      const ProductShape& sh = shapes_[n];
-      double E = sh.K * (sh.K + 1) / 2.0;
-      prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(T), (double)B * L * N * E * 10.0, s,
-                   [&] {
-                     products_forward<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), X_[0].as<T>(), partials_.as<double>(),
-                                         sums_.as<double>() + sum_off_[n], err_.as<int>(), s);
-                   });
-    }
+    for (int n = 0; n < levels_; ++n)
+      typed(n, [&](auto t) { forward_level<typename decltype(t)::type>(n); });
     STL_CUDA(cudaMemcpyAsync(h_sums_.data(), sums_.p, h_sums_.size() * 8, cudaMemcpyDeviceToHost, s));
     int err = 0;
     STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -388,11 +446,56 @@ class EngineImpl final : public Engine {
     timers.forwards += 1;
   }
 
+  template <typename U>
+  void forward_level(int n) {
+    const int L = opt_.L, B = opt_.B;
+    cudaStream_t s = stream_;
+    const i64 N = npix(n);
+    U* mod = Mod_[n].as<U>();
+    const ConvOp& op = conv_[n];
+    prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, false), conv_flops(op, B), s, [&] {
+      conv_forward<U>(op, X_[n].as<U>(), B, Z_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(),
+                      xc_.as<double>() + (size_t)n * B);
+    });
+    // |z| as deviations from their means per (map, orientation)
+    double* zc = zc_.as<double>() + (size_t)n * B * L;
+    prof_.launch(Profiler::ELEM, 3, (double)N * B * L * (2 * 2 * sizeof(U) + sizeof(U)), 0.0, s, [&] {
+      row_means<U>(Z_[n].as<U>(), true, true, N, B * L, mpart_.as<double>(), zc, s);
+      moduli_deviations<U>(Z_[n].as<U>(), N, B, L, zc, mod, B * (n + 1) * L, (n + 1) * L, n * L, s);
+    });
+    if (n > 0)
+      prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n - 1], B * n * L, false), dec_flops(dec_[n - 1], B * n * L, false),
+                   s, [&] {
+                     typed(n - 1, [&](auto ti) {
+                       using Ui = typename decltype(ti)::type;
+                       dec_apply<Ui, U>(dec_[n - 1], false, Mod_[n - 1].as<Ui>(), B * n * L, n * L, mod,
+                                        B * (n + 1) * L, (n + 1) * L, B, n * L, false, s);
+                     });
+                   });
+    const int R = B * (n + 1) * L;
+    branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s);
+    prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
+      conv_forward<U>(op, mod, R, Br_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>());
+    });
+    const ProductShape& sh = shapes_[n];
+    const double E = sh.K * (sh.K + 1) / 2.0;
+    prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
+                 [&] {
+                   products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
+                                       xc_.as<double>(), partials_.as<double>(), sums_.as<double>() + sum_off_[n],
+                                       err_.as<int>(), s);
+                 });
+  }
+
   void reverse_host(const double* cot, double* out) override {
     reverse_impl(cot);
     i64 n = (i64)opt_.B * npix(0);
-    prof_.launch(Profiler::ELEM, 1, n * (8.0 + sizeof(T)), 0.0, stream_,
-                 [&] { to_map_major<T, double>(gX_[0].as<T>(), in_f64_.as<double>(), npix(0), opt_.B, stream_); });
+    prof_.launch(Profiler::ELEM, 1, n * (8.0 + esz(0)), 0.0, stream_, [&] {
+      typed(0, [&](auto t) {
+        using U = typename decltype(t)::type;
+        to_map_major<U, double>(gX_[0].as<U>(), in_f64_.as<double>(), npix(0), opt_.B, stream_);
+      });
+    });
     STL_CUDA(cudaMemcpyAsync(out, in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
     STL_CUDA(cudaStreamSynchronize(stream_));
   }
@@ -400,9 +503,12 @@ class EngineImpl final : public Engine {
   void reverse_device(const double* cot, void* out, bool f32) override {
     reverse_impl(cot);
     i64 n = (i64)opt_.B * npix(0);
-    prof_.launch(Profiler::ELEM, 1, n * ((f32 ? 4.0 : 8.0) + sizeof(T)), 0.0, stream_, [&] {
-      if (f32) to_map_major<T, float>(gX_[0].as<T>(), static_cast<float*>(out), npix(0), opt_.B, stream_);
-      else to_map_major<T, double>(gX_[0].as<T>(), static_cast<double*>(out), npix(0), opt_.B, stream_);
+    prof_.launch(Profiler::ELEM, 1, n * ((f32 ? 4.0 : 8.0) + esz(0)), 0.0, stream_, [&] {
+      typed(0, [&](auto t) {
+        using U = typename decltype(t)::type;
+        if (f32) to_map_major<U, float>(gX_[0].as<U>(), static_cast<float*>(out), npix(0), opt_.B, stream_);
+        else to_map_major<U, double>(gX_[0].as<U>(), static_cast<double*>(out), npix(0), opt_.B, stream_);
+      });
     });
     STL_CUDA(cudaStreamSynchronize(stream_));
   }
@@ -425,7 +531,7 @@ class EngineImpl final : public Engine {
   // once, the complex outputs written once (plus |z|, or the
   // read-modify-write of an accumulated adjoint).
   double conv_bytes(const ConvOp& op, int R, bool fwd, bool extra) const {
-    const double s = sizeof(T), N = (double)op.n_rows, D = op.mean_slots;
+    const double s = op.dtype == DType::F64 ? 8.0 : 4.0, N = (double)op.n_rows, D = op.mean_slots;
     double coef = (double)op.n_rep * D * (8.0 * s + 4.0);
     double field = fwd ? R * N * s + R * N * 8.0 * s : R * N * 8.0 * s + R * N * s;
     if (extra) field += fwd ? R * N * 4.0 * s : R * N * s;
@@ -433,7 +539,7 @@ class EngineImpl final : public Engine {
   }
   double conv_flops(const ConvOp& op, int R) const { return 2.0 * 8.0 * R * (double)op.n_rows * op.mean_slots; }
   double dec_bytes(const DecOp& op, int R, bool transpose) const {
-    const double s = sizeof(T);
+    const double s = op.dtype == DType::F64 ? 8.0 : 4.0;
     double nnz = op.mean_w * (double)op.n_out;
     return nnz * (s + 4.0) + R * (double)(op.n_in + op.n_out) * s;
     (void)transpose;
@@ -532,55 +638,75 @@ class EngineImpl final : public Engine {
           }
         }
       }
-    for (int n = levels_ - 1; n >= 0; --n) {
-      i64 N = npix(n);
-      const ProductShape& sh = shapes_[n];
-      const ConvOp& op = conv_[n];
-      T* gmod = gMod_[n].as<T>();
-      if (n + 1 < levels_)
-        prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B * (n + 1) * L, true), dec_flops(dec_[n], B * (n + 1) * L, true),
-                     s, [&] {
-                       dec_apply<T>(dec_[n], true, gMod_[n + 1].as<T>(), B * (n + 2) * L, (n + 2) * L, gmod,
-                                    B * (n + 1) * L, (n + 1) * L, B, (n + 1) * L, false, s);
-                     });
-      else
-        STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
-      // cotangent matrices in the field precision
-      h_M_.resize(2 * M[n].size());
-      for (size_t q = 0; q < M[n].size(); ++q) { h_M_[2 * q] = (T)M[n][q].real(); h_M_[2 * q + 1] = (T)M[n][q].imag(); }
-      h_s1_.resize(s1[n].size());
-      for (size_t q = 0; q < s1[n].size(); ++q) h_s1_[q] = (T)s1[n][q];
-      STL_CUDA(cudaMemcpyAsync(M_.p, h_M_.data(), h_M_.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-      STL_CUDA(cudaMemcpyAsync(s1c_.p, h_s1_.data(), h_s1_.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-      const double sz = sizeof(T);
-      prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0, s,
-                   [&] {
-                     products_reverse<T>(sh, Z_[n].as<T>(), Br_[n].as<T>(), M_.as<T>(), s1c_.as<T>(), gZ_.as<T>(),
-                                         gBr_.as<T>(), s);
-                   });
-      const int R = B * (n + 1) * L;
-      prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(T), R, adj_ptr()) ? 2 : 1,
-                   conv_bytes(op, R, false, true), conv_flops(op, R), s,
-                   [&] { conv_adjoint<T>(op, gBr_.as<T>(), R, gmod, true, s, adj_ptr()); });
-      prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
-        modulus_vjp_add<T>(Z_[n].as<T>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<T>(), N, B, L, s);
-      });
-      prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(T), B, adj_ptr()) ? 2 : 1,
-                   conv_bytes(op, B, false, false), conv_flops(op, B), s,
-                   [&] { conv_adjoint<T>(op, gZ_.as<T>(), B, gX_[n].as<T>(), false, s, adj_ptr()); });
-      if (n + 1 < levels_)
-        prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
-                     [&] { dec_apply<T>(dec_[n], true, gX_[n + 1].as<T>(), B, 0, gX_[n].as<T>(), B, 0, 1, B, true, s); });
-      // the host staging buffers are reused next level: wait for the copies
-      STL_CUDA(cudaStreamSynchronize(s));
-    }
+    for (int n = levels_ - 1; n >= 0; --n)
+      typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n, M[n], s1[n]); });
     STL_CUDA(cudaMemcpyAsync(mv_.p, mv.data(), mv.size() * 8, cudaMemcpyHostToDevice, s));
-    prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * sizeof(T), (double)B * npix(0) * 2.0, s,
-                 [&] { mean_var_grad<T>(X_[0].as<T>(), mv_.as<double>(), B, npix(0), gX_[0].as<T>(), s); });
+    prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
+      typed(0, [&](auto t) {
+        using U = typename decltype(t)::type;
+        mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mv_.as<double>(), B, npix(0), gX_[0].as<U>(), s);
+      });
+    });
     STL_CUDA(cudaStreamSynchronize(s));
     prof_.collect();
     timers.reverse_ms += ms_since(t0);
     timers.reverses += 1;
+  }
+
+  // one level of the reverse sweep (field type U); M: the level's cotangent
+  // matrices [B][L][K][K], s1: the auto-S1 scales [B][L]
+  template <typename U>
+  void reverse_level(int n, const std::vector<std::complex<double>>& M, const std::vector<double>& s1) {
+    const int L = opt_.L, B = opt_.B;
+    cudaStream_t s = stream_;
+    const i64 N = npix(n);
+    const ProductShape& sh = shapes_[n];
+    const ConvOp& op = conv_[n];
+    U* gmod = gMod_[n].as<U>();
+    if (n + 1 < levels_)
+      prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B * (n + 1) * L, true), dec_flops(dec_[n], B * (n + 1) * L, true),
+                   s, [&] {
+                     typed(n + 1, [&](auto ti) {
+                       using Ui = typename decltype(ti)::type;
+                       dec_apply<Ui, U>(dec_[n], true, gMod_[n + 1].as<Ui>(), B * (n + 2) * L, (n + 2) * L, gmod,
+                                        B * (n + 1) * L, (n + 1) * L, B, (n + 1) * L, false, s);
+                     });
+                   });
+    else
+      STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
+    // cotangent matrices in the field precision
+    std::vector<U> hm(2 * M.size()), hs(s1.size());
+    for (size_t q = 0; q < M.size(); ++q) { hm[2 * q] = (U)M[q].real(); hm[2 * q + 1] = (U)M[q].imag(); }
+    for (size_t q = 0; q < s1.size(); ++q) hs[q] = (U)s1[q];
+    STL_CUDA(cudaMemcpyAsync(M_.p, hm.data(), hm.size() * sizeof(U), cudaMemcpyHostToDevice, s));
+    STL_CUDA(cudaMemcpyAsync(s1c_.p, hs.data(), hs.size() * sizeof(U), cudaMemcpyHostToDevice, s));
+    const double sz = sizeof(U);
+    prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0, s,
+                 [&] {
+                   products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), M_.as<U>(), s1c_.as<U>(), gZ_.as<U>(),
+                                       gBr_.as<U>(), s);
+                 });
+    const int R = B * (n + 1) * L;
+    prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), R, adj_ptr()) ? 2 : 1,
+                 conv_bytes(op, R, false, true), conv_flops(op, R), s,
+                 [&] { conv_adjoint<U>(op, gBr_.as<U>(), R, gmod, true, s, adj_ptr()); });
+    prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
+      modulus_vjp_add<U>(Z_[n].as<U>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<U>(), N, B, L, s);
+    });
+    prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), B, adj_ptr()) ? 2 : 1,
+                 conv_bytes(op, B, false, false), conv_flops(op, B), s,
+                 [&] { conv_adjoint<U>(op, gZ_.as<U>(), B, gX_[n].as<U>(), false, s, adj_ptr()); });
+    if (n + 1 < levels_)
+      prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
+                   [&] {
+                     typed(n + 1, [&](auto ti) {
+                       using Ui = typename decltype(ti)::type;
+                       dec_apply<Ui, U>(dec_[n], true, gX_[n + 1].as<Ui>(), B, 0, gX_[n].as<U>(), B, 0, 1, B, true,
+                                        s);
+                     });
+                   });
+    // the host staging vectors are released at return: wait for the copies
+    STL_CUDA(cudaStreamSynchronize(s));
   }
 
   Profiler prof_;
@@ -592,11 +718,11 @@ class EngineImpl final : public Engine {
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
   DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_, roles_;
+  DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
   DevMem adj_part_;
   AdjScratch adj_;
   const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }
   std::vector<double> h_sums_;
-  std::vector<T> h_M_, h_s1_;
   std::vector<Loc> map_;
 };
 

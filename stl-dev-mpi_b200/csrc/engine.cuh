@@ -98,6 +98,7 @@ struct ConvOp {
   DevMem coef;               // T [S][n_rep][8]: (gauge, re/im) coefficients
   DevMem tent;               // uint32 [ST][n_rep]: entries (u, s, j) reading rotation j of a stored cell
   DevMem coefT;              // T [ST][n_rep][8]: coef of each transposed entry
+  DevMem rowsum;             // T [n_rep][8]: sum over the slots of coef (the response to a constant field)
   // Row-centric adjoint: stored rows in tiles of kAdjTile.  Per tile the
   // sorted distinct cells its rows read; per (tile, chunk of kAdjSC slots)
   // the (slot, row) entries of every tile cell in (slot, row) order; per
@@ -119,7 +120,7 @@ struct ConvOp {
   int G = 4;
   double mean_slots = 0.0;   // cells read per row, averaged over the rows
   size_t bytes() const {
-    return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + tile_cells.bytes + tile_ncells.bytes + lcell.bytes +
+    return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + rowsum.bytes + tile_cells.bytes + tile_ncells.bytes + lcell.bytes +
            lcell_t.bytes + tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
   }
 };
@@ -173,18 +174,22 @@ void build_dec(const DecSpec& spec, DType dtype, DecOp& out, cudaStream_t stream
 //  dec_apply: y[c][ro][ri] = (D or D^T) x, row (ro, ri) of pixel c at
 //    c pix + ro outer + ri.
 //  With err (device int, set on a timed-out copy wait), operators with tile
-//  tables use the tiled forward; otherwise the per-row gather.
+//  tables use the tiled forward; otherwise the per-row gather.  rc (R FP64
+//  constants, or null): the input rows are deviations from rc, whose
+//  response rc x rowsum is added to the outputs.
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                  cudaStream_t s, int* err = nullptr);
+                  cudaStream_t s, int* err = nullptr, const double* rc = nullptr);
 //  With scratch, operators with tile tables use the row-centric two-phase
 //  adjoint; otherwise the transposed gather.
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
                   const AdjScratch* scr = nullptr);
-template <typename T>
-void dec_apply(const DecOp& op, bool transpose, const T* x, int x_pix, int x_outer, T* y, int y_pix, int y_outer,
-               int R_outer, int R_inner, bool accumulate, cudaStream_t s);
+//    Input and output types may differ (FP32 and FP64 levels); the sums are
+//    in the operator's type.
+template <typename Tin, typename Tout>
+void dec_apply(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x_outer, Tout* y, int y_pix,
+               int y_outer, int R_outer, int R_inner, bool accumulate, cudaStream_t s);
 // gz[p][b][l] += g z / |z|, z and gz [N][B][L] complex, g at p g_pix + b g_row + l
 template <typename T>
 void modulus_vjp_add(const T* z, const T* g, int g_pix, int g_row, T* gz, i64 N, int B, int L, cudaStream_t s);
@@ -211,23 +216,37 @@ struct ProductShape {
 ProductShape product_shape(int n, int L, int B, i64 N, size_t elem);
 // z [N][B][L], br [N][B][(n+1) L][L] complex, x0 [N][B] (level 0) ->
 // sums [B][L][slots] (FP64)
-// *err becomes nonzero when a wait on a staged copy timed out.
+// *err becomes nonzero when a wait on a staged copy timed out.  x0 holds
+// the level-0 maps as deviations from x0c [B].
 template <typename T>
-void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials,
-                      double* sums, int* err, cudaStream_t s);
+void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
+                      double* partials, double* sums, int* err, cudaStream_t s);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
                       cudaStream_t s);
-// gx[p][b] += coefs[b][0] + coefs[b][1] x0[p][b]
+// gx[p][b] += coefs[b][0] + coefs[b][1] (xc[b] + x0[p][b])
 template <typename T>
-void mean_var_grad(const T* x0, const double* coefs, int B, i64 N, T* gx, cudaStream_t s);
+void mean_var_grad(const T* x0, const double* xc, const double* coefs, int B, i64 N, T* gx, cudaStream_t s);
+// Per-row constants (kernels.cu): out[r] = mean over the N pixels of row r
+// of a pixel-major [N][R] field (complex_moduli: the moduli of a complex
+// field) or of a map-major [R][N] field; partials: kMeansBlocks x R doubles.
+constexpr int kMeansBlocks = 296;
+template <typename T>
+void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, double* partials, double* out,
+               cudaStream_t s);
+// mod[p mod_pix + b mod_row + mod_off + l] = |z[p][b][l]| - cz[b][l]
+template <typename T>
+void moduli_deviations(const T* z, i64 N, int B, int L, const double* cz, T* mod, int mod_pix, int mod_row,
+                       int mod_off, cudaStream_t s);
+// rc[(b, d, l)] = zc[d][b][l] for the branch rows of level n
+void branch_constants(const double* zc, int n, int B, int L, double* rc, cudaStream_t s);
 template <typename Tin, typename Tout>
 void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s);
-// [B][N] map-major <-> [N][B] pixel-major
+// [B][N] map-major <-> [N][B] pixel-major (minus sub[b] / plus add[b] in FP64)
 template <typename Tin, typename Tout>
-void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s);
+void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub = nullptr);
 template <typename Tin, typename Tout>
-void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s);
+void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* add = nullptr);
 
 }  // namespace stl

@@ -331,6 +331,17 @@ __global__ void k_adj_csr(const int32_t* cell, const uint16_t* lcell, int S, i64
   }
 }
 
+// sum over the slots of every stored row's coefficients, in FP64
+template <typename T>
+__global__ void k_rowsum(const T* coef, int S, i64 n_rep, T* out) {
+  const i64 u = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n_rep) return;
+  double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < S; ++s)
+    for (int j = 0; j < 8; ++j) a[j] += (double)coef[((i64)s * n_rep + u) * 8 + j];
+  for (int j = 0; j < 8; ++j) out[u * 8 + j] = (T)a[j];
+}
+
 // lcell [S][n_rep] -> tile-major [n_tiles][nch * 4][kAdjTile] (slots padded
 // to a multiple of 4 with index 0: their coefficients are never read)
 __global__ void k_lcell_tiles(const uint16_t* lcell, int S, i64 n_rep, int S4, i64 n_tiles, uint16_t* out) {
@@ -683,6 +694,9 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   op.coefT.alloc(sizeof(T) * 8 * op.ST * n_cells);
   k_conv_coefT<T><<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), op.coef.as<T>(), n_cells, op.ST,
                                                         op.tshift, op.coefT.as<T>());
+  STL_CUDA(cudaGetLastError());
+  op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
+  k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
   STL_CUDA(cudaGetLastError());
   // row-centric adjoint tiles
   op.adj_tiles = false;

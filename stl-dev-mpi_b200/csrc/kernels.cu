@@ -149,7 +149,8 @@ template <typename T, int NK, int RB>
 __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ cell, const T* __restrict__ coef, int S,
                                                   i64 n_rep, int o2, const T* __restrict__ x, int R,
                                                   T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row,
-                                                  int mod_off) {
+                                                  int mod_off, const T* __restrict__ rowsum,
+                                                  const double* __restrict__ rc) {
   const i64 u = (i64)blockIdx.x * blockDim.y + threadIdx.y;
   const int chunk = blockIdx.y * blockDim.x + threadIdx.x;
   if (u >= n_rep || chunk * RB >= R) return;
@@ -194,6 +195,18 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ ce
 #pragma unroll
     for (int j = 0; j < 8; ++j) w[j] = wn[j];
   }
+  if (rc) {  // the rows' constants times the row sums of the coefficients
+    T rs[8];
+    load8(rowsum + u * 8, rs);
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+      const double c = rc[r0 + rb];
+#pragma unroll
+      for (int k = 0; k < NK; ++k)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[k][rb][j] += (T)(c * (double)rs[j]);
+    }
+  }
 #pragma unroll
   for (int k = 0; k < NK; ++k) {
     const i64 p = NK == 1 ? u : rot_pixel(u, k, o2);
@@ -233,7 +246,7 @@ template <typename T, int RB>
 __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
     const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2,
     const int32_t* __restrict__ tile_cells, const int32_t* __restrict__ tile_nc, const T* __restrict__ x, int R,
-    T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err) {
+    T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err, const T* __restrict__ rowsum, const double* __restrict__ rc) {
   constexpr int SC = fwd_sc<T>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
@@ -327,6 +340,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
   if (row >= rows) return;
   const i64 p = rot_pixel(u0 + row, k, o2);
   const bool odd = k & 1;
+  if (rc) {  // the rows' constants times the row sums of the coefficients
+    T rs[8];
+    load8(rowsum + (u0 + row) * 8, rs);
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+      const double c = rc[r0 + rb];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[rb][j] += (T)(c * (double)rs[j]);
+    }
+  }
 #pragma unroll
   for (int rb = 0; rb < RB; ++rb) {
     const int r = r0 + rb;
@@ -572,39 +595,41 @@ __global__ void __launch_bounds__(128) k_adj_combine(const i64* __restrict__ cof
 // y[c][ro][ri] (+)= sum_e w[e][c] x[col[e][c]][ro][ri]; one thread per (stored
 // row u, chunk of RB rows of the R_outer x R_inner rows), NK rotations per
 // thread; threadIdx.x runs over the chunks of a pixel's rows.
-template <typename T, int NK, int RB>
-__global__ void k_ell(const int32_t* __restrict__ col, const T* __restrict__ w, int W, i64 n_rep, int o2_out,
-                      int o2_in, const T* __restrict__ x, int x_pix, int x_outer, T* __restrict__ y, int y_pix,
+// Input, output and weight types may differ (a decimation between an FP32
+// and an FP64 level): the sums are in the weights' type.
+template <typename Tin, typename Tout, typename Tw, int NK, int RB>
+__global__ void k_ell(const int32_t* __restrict__ col, const Tw* __restrict__ w, int W, i64 n_rep, int o2_out,
+                      int o2_in, const Tin* __restrict__ x, int x_pix, int x_outer, Tout* __restrict__ y, int y_pix,
                       int y_outer, int R_outer, int R_inner, int accumulate) {
   const i64 u = (i64)blockIdx.x * blockDim.y + threadIdx.y;
   const int chunk = blockIdx.y * blockDim.x + threadIdx.x;
   const int per = R_inner / RB;
   if (u >= n_rep || chunk >= R_outer * per) return;
   const int ro = chunk / per, ri = (chunk % per) * RB;
-  T acc[NK][RB];
+  Tw acc[NK][RB];
 #pragma unroll
   for (int k = 0; k < NK; ++k)
 #pragma unroll
-    for (int rb = 0; rb < RB; ++rb) acc[k][rb] = (T)0;
+    for (int rb = 0; rb < RB; ++rb) acc[k][rb] = (Tw)0;
   for (int e = 0; e < W; ++e) {
     const i64 idx = (i64)e * n_rep + u;
-    const T we = __ldg(w + idx);
+    const Tw we = __ldg(w + idx);
     const i64 c = __ldg(col + idx);
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
       const i64 ck = NK == 1 ? c : rot_cell(c, k, o2_in);
-      T xv[RB];
+      Tin xv[RB];
       loadR<RB>(x + ck * x_pix + (i64)ro * x_outer + ri, xv);
 #pragma unroll
-      for (int rb = 0; rb < RB; ++rb) acc[k][rb] = fma(we, xv[rb], acc[k][rb]);
+      for (int rb = 0; rb < RB; ++rb) acc[k][rb] = fma(we, (Tw)xv[rb], acc[k][rb]);
     }
   }
 #pragma unroll
   for (int k = 0; k < NK; ++k) {
     const i64 p = NK == 1 ? u : rot_pixel(u, k, o2_out);
-    T* yr = y + p * y_pix + (i64)ro * y_outer + ri;
+    Tout* yr = y + p * y_pix + (i64)ro * y_outer + ri;
 #pragma unroll
-    for (int rb = 0; rb < RB; ++rb) yr[rb] = accumulate ? yr[rb] + acc[k][rb] : acc[k][rb];
+    for (int rb = 0; rb < RB; ++rb) yr[rb] = accumulate ? (Tout)((Tw)yr[rb] + acc[k][rb]) : (Tout)acc[k][rb];
   }
 }
 
@@ -664,7 +689,7 @@ template <typename T>
 __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     int nd, i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0, int slots,
     const int32_t* __restrict__ roles, int W, int PC, i64 chunk, double* __restrict__ partials,
-    int* __restrict__ err) {
+    int* __restrict__ err, const double* __restrict__ x0c) {
   typedef typename V2<T>::type T2;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kProdStages];
@@ -770,7 +795,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
             acc[1] += m2;
             acc[2] += m2 * m2;
             if (x0 && l3 == 0) {
-              const double xv = (double)x0[(pc + j) * B + b];
+              const double xv = x0c[b] + (double)x0[(pc + j) * B + b];
               const double x2 = xv * xv;
               acc[3] += xv;
               acc[4] += x2;
@@ -918,12 +943,92 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, cons
 }
 
 template <typename T>
-__global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ coefs, i64 N, int B,
-                                T* __restrict__ gx) {
+__global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ xc,
+                                const double* __restrict__ coefs, i64 N, int B, T* __restrict__ gx) {
   const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N * B) return;
   const int b = (int)(i % B);
-  gx[i] += (T)(coefs[2 * b] + coefs[2 * b + 1] * (double)x0[i]);
+  const double x = (xc ? xc[b] : 0.0) + (double)x0[i];
+  gx[i] += (T)(coefs[2 * b] + coefs[2 * b + 1] * x);
+}
+
+// ---- per-row constants of the fields -------------------------------------------
+// Fields that the wavelet reads (maps, moduli) are stored as deviations from a
+// per-row FP64 constant (its mean over the level's pixels): the wavelet is
+// zero-mean, so a field of a large mean and small fluctuations would lose
+// the fluctuations to the rounding of the mean in FP32.  The constant's
+// contribution, constant x (row sums of the coefficients), is added in the
+// wavelet's epilogue; the decimation rows sum to one and carry a constant
+// unchanged.
+
+// pixel-major field [N][R] (complex: the moduli): CTA = a pixel range,
+// thread t adds the row t % R of its pixels; partials [CTA][R]
+template <typename T, bool CPLX>
+__global__ void k_means_pm(const T* __restrict__ f, i64 N, int R, i64 chunk, double* __restrict__ partials) {
+  __shared__ double red[256];
+  const int TR = (blockDim.x / R) * R;
+  const int t = threadIdx.x;
+  double a = 0.0;
+  if (t < TR) {
+    const i64 p0 = (i64)blockIdx.x * chunk, p1 = min(N, p0 + chunk);
+    for (i64 i = p0 * R + t; i < p1 * R; i += TR) {
+      if (CPLX) a += hypot((double)f[2 * i], (double)f[2 * i + 1]);
+      else a += (double)f[i];
+    }
+  }
+  red[t] = a;
+  __syncthreads();
+  if (t < R) {
+    double s = 0.0;
+    for (int j = t; j < TR; j += R) s += red[j];
+    partials[(i64)blockIdx.x * R + t] = s;
+  }
+}
+
+// map-major rows [R][N]: grid (pixel ranges, R)
+template <typename T>
+__global__ void k_means_mm(const T* __restrict__ f, i64 N, i64 chunk, double* __restrict__ partials) {
+  __shared__ double red[256];
+  const int r = blockIdx.y, t = threadIdx.x;
+  const i64 p0 = (i64)blockIdx.x * chunk, p1 = min(N, p0 + chunk);
+  double a = 0.0;
+  for (i64 p = p0 + t; p < p1; p += blockDim.x) a += (double)f[(i64)r * N + p];
+  red[t] = a;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (t < h) red[t] += red[t + h];
+    __syncthreads();
+  }
+  if (t == 0) partials[(i64)blockIdx.x * gridDim.y + r] = red[0];
+}
+
+__global__ void k_means_final(const double* __restrict__ partials, int nblk, int R, i64 N, double* __restrict__ out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  double s = 0.0;
+  for (int k = 0; k < nblk; ++k) s += partials[(i64)k * R + r];
+  out[r] = s / (double)N;
+}
+
+// moduli deviations: mod[p mod_pix + b mod_row + mod_off + l] = |z[p][b][l]| - cz[b][l]
+template <typename T>
+__global__ void k_mod_dev(const T* __restrict__ z, i64 N, int B, int L, const double* __restrict__ cz,
+                          T* __restrict__ mod, int mod_pix, int mod_row, int mod_off) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * B * L) return;
+  const i64 p = i / (B * L);
+  const int b = (int)((i / L) % B), l = (int)(i % L);
+  const double m = hypot((double)z[2 * i], (double)z[2 * i + 1]);
+  mod[p * mod_pix + (i64)b * mod_row + mod_off + l] = (T)(m - cz[b * L + l]);
+}
+
+// constants of the branch rows (b, d, l) of level n from the moduli constants [level][B][L]
+__global__ void k_branch_consts(const double* __restrict__ zc, int n, int B, int L, double* __restrict__ rc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int R = B * (n + 1) * L;
+  if (i >= R) return;
+  const int b = i / ((n + 1) * L), d = (i / L) % (n + 1), l = i % L;
+  rc[i] = zc[((i64)d * B + b) * L + l];
 }
 
 template <typename Tin, typename Tout>
@@ -934,20 +1039,24 @@ __global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, i6
 
 // [B][N] <-> [N][B] transposes of the level-0 maps at the boundary
 template <typename Tin, typename Tout>
-__global__ void k_to_pixel_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B) {
+__global__ void k_to_pixel_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B,
+                                 const double* __restrict__ sub) {
   const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over N * B, output order
   if (i >= N * B) return;
   const i64 p = i / B;
   const int b = (int)(i % B);
-  out[i] = (Tout)in[(i64)b * N + p];
+  const Tin v = in[(i64)b * N + p];
+  out[i] = sub ? (Tout)((double)v - sub[b]) : (Tout)v;
 }
 template <typename Tin, typename Tout>
-__global__ void k_to_map_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B) {
+__global__ void k_to_map_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B,
+                               const double* __restrict__ add) {
   const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over B * N, output order
   if (i >= N * B) return;
   const int b = (int)(i / N);
   const i64 p = i % N;
-  out[i] = (Tout)in[p * B + b];
+  const Tin v = in[p * B + b];
+  out[i] = add ? (Tout)((double)v + add[b]) : (Tout)v;
 }
 
 // CTA of 128 threads: blockDim.x = chunks of a row vector handled together
@@ -960,20 +1069,20 @@ inline dim3 cta_shape(int chunks) {
 
 template <typename T, int NK, int RB>
 void conv_forward_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                     cudaStream_t s) {
+                     const double* rc, cudaStream_t s) {
   const int chunks = R / RB;
   dim3 b = cta_shape(chunks);
   dim3 grid(nblocks(op.n_rep, b.y), (chunks + b.x - 1) / b.x);
   k_conv_fwd<T, NK, RB><<<grid, b, 0, s>>>(op.cell.as<int32_t>(), op.coef.as<T>(), op.S, op.n_rep, op.o2, x, R, out,
-                                           mod, mod_pix, mod_row, mod_off);
+                                           mod, mod_pix, mod_row, mod_off, op.rowsum.as<T>(), rc);
 }
 
 template <typename T, int NK>
 void conv_forward_nk(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                     cudaStream_t s) {
-  if (NK == 1 && R % 4 == 0) conv_forward_rb<T, NK, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
-  else if (R % 2 == 0) conv_forward_rb<T, NK, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
-  else conv_forward_rb<T, NK, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+                     const double* rc, cudaStream_t s) {
+  if (NK == 1 && R % 4 == 0) conv_forward_rb<T, NK, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+  else if (R % 2 == 0) conv_forward_rb<T, NK, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+  else conv_forward_rb<T, NK, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
 }
 
 template <typename T, int NK, int RB>
@@ -1020,23 +1129,41 @@ void conv_adjoint_nk(const ConvOp& op, const T* gy, int R, T* gx, bool accumulat
   else conv_adjoint_rb<T, NK, 1>(op, gy, R, gx, accumulate, s);
 }
 
-template <typename T, int NK, int RB>
-void ell_rb(const int32_t* col, const T* w, int W, i64 n_rep, int o2_out, int o2_in, const T* x, int x_pix,
-            int x_outer, T* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
+template <typename Tin, typename Tout, typename Tw, int NK, int RB>
+void ell_rb(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o2_in, const Tin* x, int x_pix,
+            int x_outer, Tout* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
   const int chunks = R_outer * (R_inner / RB);
   dim3 b = cta_shape(chunks);
   dim3 grid(nblocks(n_rep, b.y), (chunks + b.x - 1) / b.x);
-  k_ell<T, NK, RB><<<grid, b, 0, s>>>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
-                                      R_inner, acc ? 1 : 0);
+  k_ell<Tin, Tout, Tw, NK, RB><<<grid, b, 0, s>>>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix,
+                                                 y_outer, R_outer, R_inner, acc ? 1 : 0);
 }
 
-template <typename T, int NK>
-void ell_nk(const int32_t* col, const T* w, int W, i64 n_rep, int o2_out, int o2_in, const T* x, int x_pix,
-            int x_outer, T* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
+template <typename Tin, typename Tout, typename Tw, int NK>
+void ell_nk(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o2_in, const Tin* x, int x_pix,
+            int x_outer, Tout* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
   if (R_inner % 2 == 0)
-    ell_rb<T, NK, 2>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, acc, s);
+    ell_rb<Tin, Tout, Tw, NK, 2>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
+                                 R_inner, acc, s);
   else
-    ell_rb<T, NK, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, acc, s);
+    ell_rb<Tin, Tout, Tw, NK, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
+                                 R_inner, acc, s);
+}
+
+template <typename Tin, typename Tout, typename Tw>
+void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x_outer, Tout* y, int y_pix,
+                 int y_outer, int R_outer, int R_inner, bool accumulate, cudaStream_t s) {
+  const int32_t* col = transpose ? op.tcol.as<int32_t>() : op.col.as<int32_t>();
+  const Tw* w = transpose ? op.tw.as<Tw>() : op.w.as<Tw>();
+  const int W = transpose ? op.WT : op.W;
+  const i64 n_rep = transpose ? op.n_rep_in : op.n_rep_out;
+  const int o2_out = transpose ? op.o2 : op.co2, o2_in = transpose ? op.co2 : op.o2;
+  if (op.nk == 4)
+    ell_nk<Tin, Tout, Tw, 4>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner,
+                             accumulate, s);
+  else
+    ell_nk<Tin, Tout, Tw, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner,
+                             accumulate, s);
 }
 
 inline int adj_rb(size_t elem, int R) { return (elem == 4 && R % 2 == 0) ? 2 : 1; }
@@ -1051,7 +1178,7 @@ size_t fwd_tiles_smem(const ConvOp& op) {
 
 template <typename T, int RB>
 void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row,
-                           int mod_off, int* err, cudaStream_t s) {
+                           int mod_off, int* err, const double* rc, cudaStream_t s) {
   const size_t smem = fwd_tiles_smem<T, RB>(op);
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_conv_fwd_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1059,21 +1186,22 @@ void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, 
   k_conv_fwd_tiles<T, RB><<<grid, kFwdThreads, smem, s>>>(op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S,
                                                           op.n_rep, op.o2, op.tile_cells.as<int32_t>(),
                                                           op.tile_ncells.as<int32_t>(), x, R, out, mod, mod_pix,
-                                                          mod_row, mod_off, err);
+                                                          mod_row, mod_off, err, op.rowsum.as<T>(), rc);
 }
 
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                  cudaStream_t s, int* err) {
+                  cudaStream_t s, int* err, const double* rc) {
+  if (rc && !op.rowsum.p) throw std::runtime_error("wavelet operator without row sums");
   constexpr int RBmax = sizeof(T) == 4 ? 4 : 2;
   const int RB = R % RBmax == 0 ? RBmax : (R % 2 == 0 ? 2 : 1);
   const bool fits = (RB == RBmax ? fwd_tiles_smem<T, RBmax>(op) : fwd_tiles_smem<T, 2>(op)) <= 220 * 1024;
   if (err && op.nk == 4 && op.adj_tiles && op.lcell_t.p && op.n_tiles <= 65535 && fits) {
-    if (RB == RBmax) conv_forward_tiles_rb<T, RBmax>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, s);
-    else if (RB == 2) conv_forward_tiles_rb<T, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, s);
-    else conv_forward_tiles_rb<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, s);
-  } else if (op.nk == 4) conv_forward_nk<T, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
-  else conv_forward_nk<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, s);
+    if (RB == RBmax) conv_forward_tiles_rb<T, RBmax>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+    else if (RB == 2) conv_forward_tiles_rb<T, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+    else conv_forward_tiles_rb<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+  } else if (op.nk == 4) conv_forward_nk<T, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+  else conv_forward_nk<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1101,21 +1229,16 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
   STL_CUDA(cudaGetLastError());
 }
 
-template <typename T>
-void dec_apply(const DecOp& op, bool transpose, const T* x, int x_pix, int x_outer, T* y, int y_pix, int y_outer,
+template <typename Tin, typename Tout>
+void dec_apply(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x_outer, Tout* y, int y_pix, int y_outer,
                int R_outer, int R_inner, bool accumulate, cudaStream_t s) {
   if (R_outer <= 0 || R_inner <= 0) return;
-  const int32_t* col = transpose ? op.tcol.as<int32_t>() : op.col.as<int32_t>();
-  const T* w = transpose ? op.tw.as<T>() : op.w.as<T>();
-  const int W = transpose ? op.WT : op.W;
-  const i64 n_rep = transpose ? op.n_rep_in : op.n_rep_out;
-  const int o2_out = transpose ? op.o2 : op.co2, o2_in = transpose ? op.co2 : op.o2;
-  if (op.nk == 4)
-    ell_nk<T, 4>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
-                 s);
+  if (op.dtype == DType::F64)
+    dec_apply_w<Tin, Tout, double>(op, transpose, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
+                                   s);
   else
-    ell_nk<T, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
-                 s);
+    dec_apply_w<Tin, Tout, float>(op, transpose, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
+                                  s);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1206,15 +1329,17 @@ void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T
 }  // namespace
 
 template <typename T>
-void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, double* partials, double* sums,
-                      int* err, cudaStream_t s) {
+void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
+                      double* partials, double* sums, int* err, cudaStream_t s) {
+  if (sh.level0 && !x0c) throw std::runtime_error("level-0 products need the map constants");
   const int L = sh.L, nd = sh.nd;
   if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
   if (sh.smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
   dim3 grid(sh.blocks, 1, sh.item_chunks);
   k_products<T><<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots,
-                                                      sh.d_roles, sh.warps, sh.px_chunk, sh.chunk, partials, err);
+                                                      sh.d_roles, sh.warps, sh.px_chunk, sh.chunk, partials, err,
+                                                      x0c);
   STL_CUDA(cudaGetLastError());
   const i64 total = (i64)sh.B * L * sh.slots;
   k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
@@ -1242,8 +1367,42 @@ void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* 
 }
 
 template <typename T>
-void mean_var_grad(const T* x0, const double* coefs, int B, i64 N, T* gx, cudaStream_t s) {
-  k_mean_var_grad<T><<<nblocks(N * B, 256), 256, 0, s>>>(x0, coefs, N, B, gx);
+void mean_var_grad(const T* x0, const double* xc, const double* coefs, int B, i64 N, T* gx, cudaStream_t s) {
+  k_mean_var_grad<T><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, coefs, N, B, gx);
+  STL_CUDA(cudaGetLastError());
+}
+
+int means_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(kMeansBlocks, (N + 4095) / 4096)); }
+
+template <typename T>
+void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, double* partials, double* out,
+               cudaStream_t s) {
+  if (R <= 0 || R > 256) throw std::runtime_error("row means: 1 to 256 rows");
+  const int nblk = means_blocks(N);
+  const i64 chunk = (N + nblk - 1) / nblk;
+  if (pixel_major) {
+    const int threads = (256 / R) * R;
+    if (complex_moduli) k_means_pm<T, true><<<nblk, threads, 0, s>>>(f, N, R, chunk, partials);
+    else k_means_pm<T, false><<<nblk, threads, 0, s>>>(f, N, R, chunk, partials);
+  } else {
+    if (complex_moduli) throw std::runtime_error("row means: complex map-major fields are not used");
+    k_means_mm<T><<<dim3(nblk, R), 256, 0, s>>>(f, N, chunk, partials);
+  }
+  STL_CUDA(cudaGetLastError());
+  k_means_final<<<1, 256, 0, s>>>(partials, nblk, R, N, out);
+  STL_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void moduli_deviations(const T* z, i64 N, int B, int L, const double* cz, T* mod, int mod_pix, int mod_row,
+                       int mod_off, cudaStream_t s) {
+  k_mod_dev<T><<<nblocks(N * B * L, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
+  STL_CUDA(cudaGetLastError());
+}
+
+void branch_constants(const double* zc, int n, int B, int L, double* rc, cudaStream_t s) {
+  const int R = B * (n + 1) * L;
+  k_branch_consts<<<nblocks(R, 256), 256, 0, s>>>(zc, n, B, L, rc);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1255,40 +1414,50 @@ void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s) {
 }
 
 template <typename Tin, typename Tout>
-void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
-  k_to_pixel_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B);
+void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub) {
+  k_to_pixel_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename Tin, typename Tout>
-void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s) {
-  k_to_map_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B);
+void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* add) {
+  k_to_map_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, add);
   STL_CUDA(cudaGetLastError());
 }
 
 #define INST(T)                                                                                                   \
-  template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t, int*);               \
+  template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t, int*,          \
+                                const double*);               \
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*);                            \
-  template void dec_apply<T>(const DecOp&, bool, const T*, int, int, T*, int, int, int, int, bool, cudaStream_t); \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
-  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, double*, double*, int*,    \
-                                    cudaStream_t);                                                                \
+  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*, double*,  \
+                                    double*, int*, cudaStream_t);                                                                \
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, T*, T*,          \
                                     cudaStream_t);                                                                \
-  template void mean_var_grad<T>(const T*, const double*, int, i64, T*, cudaStream_t);
+  template void mean_var_grad<T>(const T*, const double*, const double*, int, i64, T*, cudaStream_t);            \
+  template void row_means<T>(const T*, bool, bool, i64, int, double*, double*, cudaStream_t);                     \
+  template void moduli_deviations<T>(const T*, i64, int, int, const double*, T*, int, int, int, cudaStream_t);
 INST(float)
 INST(double)
+template void dec_apply<float, float>(const DecOp&, bool, const float*, int, int, float*, int, int, int, int, bool,
+                                     cudaStream_t);
+template void dec_apply<double, double>(const DecOp&, bool, const double*, int, int, double*, int, int, int, int,
+                                       bool, cudaStream_t);
+template void dec_apply<float, double>(const DecOp&, bool, const float*, int, int, double*, int, int, int, int, bool,
+                                      cudaStream_t);
+template void dec_apply<double, float>(const DecOp&, bool, const double*, int, int, float*, int, int, int, int, bool,
+                                      cudaStream_t);
 template void convert<double, float>(const double*, float*, i64, cudaStream_t);
 template void convert<float, double>(const float*, double*, i64, cudaStream_t);
 template void convert<double, double>(const double*, double*, i64, cudaStream_t);
 template void convert<float, float>(const float*, float*, i64, cudaStream_t);
-template void to_pixel_major<double, float>(const double*, float*, i64, int, cudaStream_t);
-template void to_pixel_major<double, double>(const double*, double*, i64, int, cudaStream_t);
-template void to_pixel_major<float, float>(const float*, float*, i64, int, cudaStream_t);
-template void to_pixel_major<float, double>(const float*, double*, i64, int, cudaStream_t);
-template void to_map_major<float, double>(const float*, double*, i64, int, cudaStream_t);
-template void to_map_major<double, double>(const double*, double*, i64, int, cudaStream_t);
-template void to_map_major<float, float>(const float*, float*, i64, int, cudaStream_t);
-template void to_map_major<double, float>(const double*, float*, i64, int, cudaStream_t);
+template void to_pixel_major<double, float>(const double*, float*, i64, int, cudaStream_t, const double*);
+template void to_pixel_major<double, double>(const double*, double*, i64, int, cudaStream_t, const double*);
+template void to_pixel_major<float, float>(const float*, float*, i64, int, cudaStream_t, const double*);
+template void to_pixel_major<float, double>(const float*, double*, i64, int, cudaStream_t, const double*);
+template void to_map_major<float, double>(const float*, double*, i64, int, cudaStream_t, const double*);
+template void to_map_major<double, double>(const double*, double*, i64, int, cudaStream_t, const double*);
+template void to_map_major<float, float>(const float*, float*, i64, int, cudaStream_t, const double*);
+template void to_map_major<double, float>(const double*, float*, i64, int, cudaStream_t, const double*);
 
 }  // namespace stl

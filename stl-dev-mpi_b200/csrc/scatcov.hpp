@@ -86,6 +86,10 @@ class Engine {
   virtual void reverse_device(const double* cot, void* out, bool f32) = 0;
   // Device level-0 maps of the last load (T), for checkpoints.
   virtual void save_input(std::vector<double>& x) = 0;
+  // exact copy of the loaded level-0 state (fields are stored as deviations
+  // from per-map constants) and its restoration
+  virtual void save_state(std::vector<double>& state) = 0;
+  virtual void load_state(const std::vector<double>& state) = 0;
 
   size_t operator_bytes() const { return operator_bytes_; }
   size_t field_bytes() const { return field_bytes_; }

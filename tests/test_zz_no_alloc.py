@@ -41,8 +41,9 @@ def test_mean_var_noalloc_matches_forward(dtype):
         assert rc == 0, stl.lib().stlp_last_error()
         torch.cuda.synchronize()
         got = out.cpu().numpy()
-        # both are FP64 sums of the same (f32 or f64) pixel values, in different orders
-        np.testing.assert_allclose(got, want, rtol=1e-12, atol=0.0)
+        # FP64 sums of the pixel values; the FP32 engine holds its maps as FP32
+        # deviations from their FP64 means, so its mean / var carry that rounding
+        np.testing.assert_allclose(got, want, rtol=1e-12 if dtype == "float64" else 1e-6, atol=0.0)
     e.close()
 
 
