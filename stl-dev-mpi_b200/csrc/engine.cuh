@@ -111,6 +111,7 @@ struct ConvOp {
   bool adj_tiles = false;    // tables built (every tile within kAdjCells cells)
   DevMem tile_cells;         // int32 [n_tiles][kAdjCells]
   DevMem tile_ncells;        // int32 [n_tiles]
+  DevMem tile_slots;         // int32 [n_tiles]: most slots a row of the tile uses (later slots are zero)
   DevMem lcell;              // uint16 [S][n_rep]: tile cell of every (slot, row) (build only)
   DevMem lcell_t;            // uint16 [n_tiles][nch 4][kAdjTile]: the same, tile-major, slots padded to 4
   DevMem tile_ent;           // uint16 [n_tiles][S kAdjTile]: slot % kAdjSC << 8 | row
@@ -120,7 +121,8 @@ struct ConvOp {
   int G = 4;
   double mean_slots = 0.0;   // cells read per row, averaged over the rows
   size_t bytes() const {
-    return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + rowsum.bytes + tile_cells.bytes + tile_ncells.bytes + lcell.bytes +
+    return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + rowsum.bytes + tile_cells.bytes + tile_ncells.bytes +
+           tile_slots.bytes + lcell.bytes +
            lcell_t.bytes + tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
   }
 };
@@ -231,7 +233,7 @@ void mean_var_grad(const T* x0, const double* xc, const double* coefs, int B, i6
 // Per-row constants (kernels.cu): out[r] = mean over the N pixels of row r
 // of a pixel-major [N][R] field (complex_moduli: the moduli of a complex
 // field) or of a map-major [R][N] field; partials: kMeansBlocks x R doubles.
-constexpr int kMeansBlocks = 296;
+constexpr int kMeansBlocks = 2048;
 template <typename T>
 void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, double* partials, double* out,
                cudaStream_t s);

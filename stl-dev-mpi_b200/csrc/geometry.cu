@@ -331,6 +331,15 @@ __global__ void k_adj_csr(const int32_t* cell, const uint16_t* lcell, int S, i64
   }
 }
 
+// most slots used by a row of each adjoint tile
+__global__ void k_tile_slots(const int* counts, i64 n_rep, i64 n_tiles, int32_t* out) {
+  const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tiles) return;
+  int m = 1;
+  for (i64 u = t * kAdjTile; u < min(n_rep, (t + 1) * kAdjTile); ++u) m = max(m, counts[u]);
+  out[t] = m;
+}
+
 // sum over the slots of every stored row's coefficients, in FP64
 template <typename T>
 __global__ void k_rowsum(const T* coef, int S, i64 n_rep, T* out) {
@@ -702,6 +711,10 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   op.adj_tiles = false;
   if (op.S > 128) return;  // the tile sort holds 128 slots per row
   op.n_tiles = (a.n_rows + kAdjTile - 1) / kAdjTile;
+  op.tile_slots.alloc(sizeof(int32_t) * op.n_tiles);
+  k_tile_slots<<<nblocks(op.n_tiles, 256), 256, 0, s>>>(counts.as<int>(), a.n_rows, op.n_tiles,
+                                                        op.tile_slots.as<int32_t>());
+  STL_CUDA(cudaGetLastError());
   op.tile_cells.alloc(sizeof(int32_t) * kAdjCells * op.n_tiles);
   op.tile_ncells.alloc(sizeof(int32_t) * op.n_tiles);
   op.lcell.alloc(sizeof(uint16_t) * op.S * a.n_rows);

@@ -246,7 +246,8 @@ template <typename T, int RB>
 __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
     const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2,
     const int32_t* __restrict__ tile_cells, const int32_t* __restrict__ tile_nc, const T* __restrict__ x, int R,
-    T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err, const T* __restrict__ rowsum, const double* __restrict__ rc) {
+    T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err,
+    const T* __restrict__ rowsum, const double* __restrict__ rc, const int32_t* __restrict__ tile_slots) {
   constexpr int SC = fwd_sc<T>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
   const i64 u0 = (i64)tile * kAdjTile;
   const int rows = (int)min((i64)kAdjTile, n_rep - u0);
   const int S4 = ((S + 3) / 4) * 4;  // slots per tile in the tile-major index table
+  S = tile_slots[tile];              // the tile's rows use no later slot
   const int nch = (S + SC - 1) / SC;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -469,7 +471,7 @@ template <typename T, int RB>
 __global__ void __launch_bounds__(kAdjTile, 2) k_conv_adj_tiles(
     const T* __restrict__ coef, int S, i64 n_rep, int o2, int nch, int ncs, const int32_t* __restrict__ tile_nc,
     const uint16_t* __restrict__ tile_ent, const uint16_t* __restrict__ tile_off, const T* __restrict__ gy, int R,
-    T* __restrict__ part) {
+    T* __restrict__ part, const int32_t* __restrict__ tile_slots) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* P = reinterpret_cast<T*>(smem_raw);                 // [RB][4][kAdjPlane]
   T* acc = P + 4 * RB * kAdjPlane;                       // [RB][4][ncs]
@@ -501,18 +503,20 @@ __global__ void __launch_bounds__(kAdjTile, 2) k_conv_adj_tiles(
   const uint16_t* toff = tile_off + (i64)tile * nch * ncs;
   const uint16_t* tent = tile_ent + (i64)tile * S * kAdjTile;
   const T* cu = coef + u * 8;
+  const int St = tile_slots[tile];  // the tile's rows use no later slot (their entries end there too)
+  const int ncht = (St + kAdjSC - 1) / kAdjSC;
   const i64 cstride = n_rep * 8;
   T wn[8];
   if (valid) load8(cu, wn);
-  for (int ch = 0; ch < nch; ++ch) {
+  for (int ch = 0; ch < ncht; ++ch) {
     const int s0 = ch * kAdjSC;
-    const int sn = min(kAdjSC, S - s0);
+    const int sn = min(kAdjSC, St - s0);
     if (valid) {
       for (int sl = 0; sl < sn; ++sl) {
         T w[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) w[q] = wn[q];
-        if (s0 + sl + 1 < S) load8(cu + (i64)(s0 + sl + 1) * cstride, wn);
+        if (s0 + sl + 1 < St) load8(cu + (i64)(s0 + sl + 1) * cstride, wn);
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
@@ -971,10 +975,19 @@ __global__ void k_means_pm(const T* __restrict__ f, i64 N, int R, i64 chunk, dou
   double a = 0.0;
   if (t < TR) {
     const i64 p0 = (i64)blockIdx.x * chunk, p1 = min(N, p0 + chunk);
-    for (i64 i = p0 * R + t; i < p1 * R; i += TR) {
-      if (CPLX) a += hypot((double)f[2 * i], (double)f[2 * i + 1]);
-      else a += (double)f[i];
+    const i64 e1 = p1 * R;
+    // four independent sums (more loads in flight), added in a fixed order
+    double q[4] = {0.0, 0.0, 0.0, 0.0};
+    i64 i = p0 * R + t;
+    for (; i + 3 * (i64)TR < e1; i += 4 * (i64)TR) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const i64 j = i + k * (i64)TR;
+        q[k] += CPLX ? hypot((double)f[2 * j], (double)f[2 * j + 1]) : (double)f[j];
+      }
     }
+    for (; i < e1; i += TR) q[0] += CPLX ? hypot((double)f[2 * i], (double)f[2 * i + 1]) : (double)f[i];
+    a = (q[0] + q[1]) + (q[2] + q[3]);
   }
   red[t] = a;
   __syncthreads();
@@ -991,8 +1004,15 @@ __global__ void k_means_mm(const T* __restrict__ f, i64 N, i64 chunk, double* __
   __shared__ double red[256];
   const int r = blockIdx.y, t = threadIdx.x;
   const i64 p0 = (i64)blockIdx.x * chunk, p1 = min(N, p0 + chunk);
-  double a = 0.0;
-  for (i64 p = p0 + t; p < p1; p += blockDim.x) a += (double)f[(i64)r * N + p];
+  double q[4] = {0.0, 0.0, 0.0, 0.0};
+  const T* fr = f + (i64)r * N;
+  i64 p = p0 + t;
+  for (; p + 3 * (i64)blockDim.x < p1; p += 4 * (i64)blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] += (double)fr[p + k * (i64)blockDim.x];
+  }
+  for (; p < p1; p += blockDim.x) q[0] += (double)fr[p];
+  const double a = (q[0] + q[1]) + (q[2] + q[3]);
   red[t] = a;
   __syncthreads();
   for (int h = blockDim.x / 2; h > 0; h >>= 1) {
@@ -1110,7 +1130,8 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
   dim3 grid(R / RB, (unsigned)op.n_tiles);
   k_conv_adj_tiles<T, RB><<<grid, kAdjTile, smem, s>>>(op.coef.as<T>(), op.S, op.n_rep, op.o2, op.nch, op.ncs,
                                                        op.tile_ncells.as<int32_t>(), op.tile_ent.as<uint16_t>(),
-                                                       op.tile_off.as<uint16_t>(), gy, R, part);
+                                                       op.tile_off.as<uint16_t>(), gy, R, part,
+                                                       op.tile_slots.as<int32_t>());
   const i64 n_cells = op.n_in / op.nk;
   const int chunks = R / RB;
   dim3 b = cta_shape(chunks);
@@ -1186,7 +1207,8 @@ void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, 
   k_conv_fwd_tiles<T, RB><<<grid, kFwdThreads, smem, s>>>(op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S,
                                                           op.n_rep, op.o2, op.tile_cells.as<int32_t>(),
                                                           op.tile_ncells.as<int32_t>(), x, R, out, mod, mod_pix,
-                                                          mod_row, mod_off, err, op.rowsum.as<T>(), rc);
+                                                          mod_row, mod_off, err, op.rowsum.as<T>(), rc,
+                                                          op.tile_slots.as<int32_t>());
 }
 
 template <typename T>
@@ -1372,7 +1394,7 @@ void mean_var_grad(const T* x0, const double* xc, const double* coefs, int B, i6
   STL_CUDA(cudaGetLastError());
 }
 
-int means_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(kMeansBlocks, (N + 4095) / 4096)); }
+int means_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(kMeansBlocks, (N + 1023) / 1024)); }
 
 template <typename T>
 void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, double* partials, double* out,
