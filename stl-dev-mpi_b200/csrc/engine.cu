@@ -647,8 +647,14 @@ class EngineImpl final : public Engine {
         mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mv_.as<double>(), B, npix(0), gX_[0].as<U>(), s);
       });
     });
+    int err = 0;
+    STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     STL_CUDA(cudaStreamSynchronize(s));
     prof_.collect();
+    if (err) {
+      STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
+      throw std::runtime_error("a wait on a staged device copy timed out in the reverse sweep");
+    }
     timers.reverse_ms += ms_since(t0);
     timers.reverses += 1;
   }
