@@ -123,7 +123,7 @@ static std::vector<double> wavelet_kernel(int ksz, int G) {
   return out;
 }
 
-Engine::Engine(const Options& o) : opt_(o) {
+Engine::Engine(const Options& o, const Support* sup) : opt_(o) {
   if (o.nside < 1 || (o.nside & (o.nside - 1)) != 0) throw std::runtime_error("nside must be a power of two");
   int order = 0;
   while ((i64(1) << order) < o.nside) ++order;
@@ -133,6 +133,29 @@ Engine::Engine(const Options& o) : opt_(o) {
   if (o.ksz != 5 && o.ksz != 3) throw std::runtime_error("kernel must be 3 or 5");
   plan_ = build_plan(o.J, o.L);
   levels_ = o.J;
+  for (int d = 0; d < levels_; ++d) {
+    const i64 n = 12 * (o.nside >> d) * (o.nside >> d);
+    npix_.push_back(n);
+    ncore_.push_back(n);
+  }
+  if (sup) {
+    if ((int)sup->ids.size() != levels_ || (int)sup->core.size() != levels_)
+      throw std::runtime_error("support levels mismatch");
+    if (o.B != 1) throw std::runtime_error("a patch engine holds one patch");
+    for (int d = 0; d < levels_; ++d) {
+      const auto& ids = sup->ids[d];
+      if (ids.empty()) throw std::runtime_error("empty support level");
+      for (size_t i = 0; i < ids.size(); ++i)
+        if (ids[i] < 0 || ids[i] >= npix_[d] || (i && ids[i] <= ids[i - 1]))
+          throw std::runtime_error("support ids must be sorted, unique and in range");
+      if (sup->core[d].empty()) throw std::runtime_error("empty core level");
+      for (i64 c : sup->core[d])
+        if (c < 0 || c >= (i64)ids.size()) throw std::runtime_error("core position out of range");
+      npix_[d] = (i64)ids.size();
+      ncore_[d] = (i64)sup->core[d].size();
+    }
+    support_ = *sup;
+  }
 }
 
 static double ms_since(std::chrono::steady_clock::time_point t0) {
@@ -201,13 +224,14 @@ class Profiler {
 // the wavelet sums would pass the 1e-6 criterion on S1-S3; those levels hold
 // well under 1 % of the work.
 constexpr int kFp64Nside = 32;
+constexpr double kBindEps = 1e-9;  // binding threshold of grid-mode wavelets (disc.rs BIND_EPS)
 
 template <typename U> struct Tag { typedef U type; };
 
 template <typename T>
 class EngineImpl final : public Engine {
  public:
-  explicit EngineImpl(const Options& o) : Engine(o) {
+  explicit EngineImpl(const Options& o, const Support* sup = nullptr) : Engine(o, sup) {
     int K0 = 0;
     (void)K0;
     // plan -> slot map of the product sums
@@ -234,15 +258,44 @@ class EngineImpl final : public Engine {
     std::vector<double> ker = wavelet_kernel(opt_.ksz, L);
     conv_.resize(levels_);
     dec_.resize(levels_ > 1 ? levels_ - 1 : 0);
+    if (grid_mode()) {
+      // supports and core masks on the device
+      ids_dev_.resize(levels_);
+      core_mask_.resize(levels_);
+      for (int d = 0; d < levels_; ++d) {
+        const auto& ids = support_.ids[d];
+        ids_dev_[d].alloc(sizeof(i64) * ids.size());
+        STL_CUDA(cudaMemcpyAsync(ids_dev_[d].p, ids.data(), sizeof(i64) * ids.size(), cudaMemcpyHostToDevice,
+                                 stream_));
+        std::vector<uint8_t> m(ids.size(), 0);
+        for (i64 c : support_.core[d]) m[c] = 1;
+        core_mask_[d].alloc(m.size());
+        STL_CUDA(cudaMemcpyAsync(core_mask_[d].p, m.data(), m.size(), cudaMemcpyHostToDevice, stream_));
+        STL_CUDA(cudaStreamSynchronize(stream_));
+      }
+    }
     for (int n = 0; n < levels_; ++n) {
       ConvSpec cs;
       cs.nside = opt_.nside >> n; cs.ksz = opt_.ksz; cs.G = L; cs.gauge = 0;
+      if (grid_mode()) {
+        cs.d_grid = ids_dev_[n].as<i64>();
+        cs.n_in = npix(n);
+        cs.eps = kBindEps;
+        cs.symmetric = false;
+      }
       build_conv(cs, ker, dtype_of(n), conv_[n], stream_);
       operator_bytes_ += conv_[n].bytes();
     }
     for (int d = 0; d + 1 < levels_; ++d) {
       DecSpec ds;
       ds.nside = opt_.nside >> d;
+      if (grid_mode()) {
+        ds.d_ids = ids_dev_[d].as<i64>();
+        ds.n_in = npix(d);
+        ds.d_out = ids_dev_[d + 1].as<i64>();
+        ds.n_out = npix(d + 1);
+        ds.symmetric = false;
+      }
       build_dec(ds, dtype_of(d + 1), dec_[d], stream_);  // FP64 weights into an FP64 level
       operator_bytes_ += dec_[d].bytes();
     }
@@ -482,8 +535,8 @@ class EngineImpl final : public Engine {
     prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
                  [&] {
                    products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
-                                       xc_.as<double>(), partials_.as<double>(), sums_.as<double>() + sum_off_[n],
-                                       err_.as<int>(), s);
+                                       xc_.as<double>(), mask(n), partials_.as<double>(),
+                                       sums_.as<double>() + sum_off_[n], err_.as<int>(), s);
                  });
   }
 
@@ -589,7 +642,7 @@ class EngineImpl final : public Engine {
         const Loc& l = map_[i];
         const ProductShape& sh = shapes_[l.level];
         const double* row = h_sums_.data() + sum_off_[l.level] + ((size_t)b * L + l.l3) * sh.slots;
-        const double N = (double)npix(l.level);
+        const double N = (double)ncore(l.level);
         const double re = row[l.re], im = l.im >= 0 ? row[l.im] : 0.0, second = row[l.second];
         const double vr = re / N, vi = im / N;
         values[2 * (b * np + i)] = vr;
@@ -615,7 +668,7 @@ class EngineImpl final : public Engine {
         if (g == std::complex<double>(0.0, 0.0)) continue;
         const Coef& c = plan_[i];
         int n = c.native, K = shapes_[n].K, z = K - 1;
-        double N = (double)npix(n);
+        double N = (double)ncore(n);
         auto at = [&](int l3, int r, int q) -> std::complex<double>& {
           return M[n][(((size_t)b * L + l3) * K + r) * K + q];
         };
@@ -644,7 +697,8 @@ class EngineImpl final : public Engine {
     prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
       typed(0, [&](auto t) {
         using U = typename decltype(t)::type;
-        mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mv_.as<double>(), B, npix(0), gX_[0].as<U>(), s);
+        mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mask(0), mv_.as<double>(), B, npix(0), gX_[0].as<U>(),
+                         s);
       });
     });
     int err = 0;
@@ -689,8 +743,8 @@ class EngineImpl final : public Engine {
     const double sz = sizeof(U);
     prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0, s,
                  [&] {
-                   products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), M_.as<U>(), s1c_.as<U>(), gZ_.as<U>(),
-                                       gBr_.as<U>(), s);
+                   products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), M_.as<U>(), s1c_.as<U>(), mask(n),
+                                       gZ_.as<U>(), gBr_.as<U>(), s);
                  });
     const int R = B * (n + 1) * L;
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), R, adj_ptr()) ? 2 : 1,
@@ -725,12 +779,19 @@ class EngineImpl final : public Engine {
   std::vector<size_t> sum_off_;
   DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_, roles_;
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
+  std::vector<DevMem> ids_dev_, core_mask_;  // grid mode: supports and core masks per level
+  const uint8_t* mask(int n) const { return grid_mode() ? core_mask_[n].as<uint8_t>() : nullptr; }
   DevMem adj_part_;
   AdjScratch adj_;
   const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }
   std::vector<double> h_sums_;
   std::vector<Loc> map_;
 };
+
+std::unique_ptr<Engine> Engine::create_patch(const Options& o, const Support& s) {
+  if (o.fp32) return std::unique_ptr<Engine>(new EngineImpl<float>(o, &s));
+  return std::unique_ptr<Engine>(new EngineImpl<double>(o, &s));
+}
 
 std::unique_ptr<Engine> Engine::create(const Options& o) {
   if (o.fp32) return std::unique_ptr<Engine>(new EngineImpl<float>(o));

@@ -220,16 +220,18 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem);
 // sums [B][L][slots] (FP64)
 // *err becomes nonzero when a wait on a staged copy timed out.  x0 holds
 // the level-0 maps as deviations from x0c [B].
+// mask (or null): 1 on the pixels the sums cover.
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
-                      double* partials, double* sums, int* err, cudaStream_t s);
+                      const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
 template <typename T>
-void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
-                      cudaStream_t s);
+void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, const uint8_t* mask,
+                      T* gz, T* gbr, cudaStream_t s);
 // gx[p][b] += coefs[b][0] + coefs[b][1] (xc[b] + x0[p][b])
 template <typename T>
-void mean_var_grad(const T* x0, const double* xc, const double* coefs, int B, i64 N, T* gx, cudaStream_t s);
+void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const double* coefs, int B, i64 N, T* gx,
+                   cudaStream_t s);
 // Per-row constants (kernels.cu): out[r] = mean over the N pixels of row r
 // of a pixel-major [N][R] field (complex_moduli: the moduli of a complex
 // field) or of a map-major [R][N] field; partials: kMeansBlocks x R doubles.

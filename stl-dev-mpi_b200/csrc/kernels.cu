@@ -693,7 +693,7 @@ template <typename T>
 __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     int nd, i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0, int slots,
     const int32_t* __restrict__ roles, int W, int PC, i64 chunk, double* __restrict__ partials,
-    int* __restrict__ err, const double* __restrict__ x0c) {
+    int* __restrict__ err, const double* __restrict__ x0c, const uint8_t* __restrict__ mask) {
   typedef typename V2<T>::type T2;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kProdStages];
@@ -764,6 +764,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
       if (kind == 0) {
         const int ra = (d1 * 4 + l1) * L + l3, rb = (d2 * 4 + 2 * hx) * L + l3;
         for (int j = rep; j < np; j += nrep) {
+          if (mask && !mask[pc + j]) continue;
           const T2* rowp = sb + ((size_t)j * B + b) * K1 * L;
           const T2 a = rowp[ra], y0 = rowp[rb], y1 = rowp[rb + L];
           const T am = fma(a.x, a.x, a.y * a.y);
@@ -779,7 +780,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
         const int ni = (np + 1) >> 1;
         for (int it = rep; it < ni; it += nrep) {
           const int j = 2 * it + hx;
-          if (j < np) {
+          if (j < np && (!mask || mask[pc + j])) {
             const T2 x = sb[((size_t)j * B + b) * K1 * L + ra];
             const T2 zz = sz[((size_t)j * B + b) * L + l3];
             f[0] = fma(x.x, zz.x, fma(x.y, zz.y, f[0]));
@@ -791,7 +792,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
         const int ni = (np + 7) >> 3;
         for (int it = rep; it < ni; it += nrep) {
           const int j = 8 * it + q8;
-          if (j < np) {
+          if (j < np && (!mask || mask[pc + j])) {
             const T2 zz = sz[((size_t)j * B + b) * L + l3];
             const double m = hypot((double)zz.x, (double)zz.y);
             const double m2 = m * m;
@@ -897,7 +898,8 @@ constexpr int kRevThreads = 256;
 template <typename T, int K>
 __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, const T* __restrict__ z,
                                                               const T* __restrict__ br, const T* __restrict__ M,
-                                                              const T* __restrict__ s1c, T* __restrict__ gz,
+                                                              const T* __restrict__ s1c,
+                                                              const uint8_t* __restrict__ mask, T* __restrict__ gz,
                                                               T* __restrict__ gbr) {
   extern __shared__ __align__(16) unsigned char smem[];
   typedef typename V2<T>::type T2;
@@ -917,6 +919,13 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, cons
   constexpr int TPX = kRevThreads / 4;
   for (i64 p = (i64)blockIdx.x * TPX + px; p < N; p += (i64)gridDim.x * TPX) {
     const i64 row = (p * B + b) * K1;
+    if (mask && !mask[p]) {  // outside the averaged pixels: no cotangent
+      T2 zero;
+      zero.x = (T)0; zero.y = (T)0;
+      for (int i = 0; i < K1; ++i) gbrv[(row + i) * L + l3] = zero;
+      gzv[(p * B + b) * L + l3] = zero;
+      continue;
+    }
     T2 v[K];
 #pragma unroll
     for (int i = 0; i < K1; ++i) v[i] = brv[(row + i) * L + l3];
@@ -948,9 +957,11 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, cons
 
 template <typename T>
 __global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ xc,
-                                const double* __restrict__ coefs, i64 N, int B, T* __restrict__ gx) {
+                                const uint8_t* __restrict__ mask, const double* __restrict__ coefs, i64 N, int B,
+                                T* __restrict__ gx) {
   const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N * B) return;
+  if (mask && !mask[i / B]) return;
   const int b = (int)(i % B);
   const double x = (xc ? xc[b] : 0.0) + (double)x0[i];
   gx[i] += (T)(coefs[2 * b] + coefs[2 * b + 1] * x);
@@ -1338,21 +1349,21 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
 
 namespace {
 template <typename T, int K>
-void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
-                        cudaStream_t s) {
+void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c,
+                        const uint8_t* mask, T* gz, T* gbr, cudaStream_t s) {
   const size_t smem = (size_t)4 * K * K * 2 * sizeof(T);
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products_rev<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const i64 tiles = (sh.N + kRevThreads / 4 - 1) / (kRevThreads / 4);
   const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 / sh.B));
   dim3 grid(gx, sh.B);
-  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, z, br, M, s1c, gz, gbr);
+  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, z, br, M, s1c, mask, gz, gbr);
 }
 }  // namespace
 
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
-                      double* partials, double* sums, int* err, cudaStream_t s) {
+                      const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s) {
   if (sh.level0 && !x0c) throw std::runtime_error("level-0 products need the map constants");
   const int L = sh.L, nd = sh.nd;
   if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
@@ -1361,7 +1372,7 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
   dim3 grid(sh.blocks, 1, sh.item_chunks);
   k_products<T><<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots,
                                                       sh.d_roles, sh.warps, sh.px_chunk, sh.chunk, partials, err,
-                                                      x0c);
+                                                      x0c, mask);
   STL_CUDA(cudaGetLastError());
   const i64 total = (i64)sh.B * L * sh.slots;
   k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
@@ -1370,27 +1381,28 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
 }
 
 template <typename T>
-void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, T* gz, T* gbr,
-                      cudaStream_t s) {
+void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c,
+                      const uint8_t* mask, T* gz, T* gbr, cudaStream_t s) {
   switch (sh.nd) {
-    case 1: products_reverse_k<T, 5>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 2: products_reverse_k<T, 9>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 3: products_reverse_k<T, 13>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 4: products_reverse_k<T, 17>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 5: products_reverse_k<T, 21>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 6: products_reverse_k<T, 25>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 7: products_reverse_k<T, 29>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 8: products_reverse_k<T, 33>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 9: products_reverse_k<T, 37>(sh, z, br, M, s1c, gz, gbr, s); break;
-    case 10: products_reverse_k<T, 41>(sh, z, br, M, s1c, gz, gbr, s); break;
+    case 1: products_reverse_k<T, 5>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 2: products_reverse_k<T, 9>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 3: products_reverse_k<T, 13>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 4: products_reverse_k<T, 17>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 5: products_reverse_k<T, 21>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 6: products_reverse_k<T, 25>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 7: products_reverse_k<T, 29>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 8: products_reverse_k<T, 33>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 9: products_reverse_k<T, 37>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 10: products_reverse_k<T, 41>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
     default: throw std::runtime_error("more levels than the products are built for (10)");
   }
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename T>
-void mean_var_grad(const T* x0, const double* xc, const double* coefs, int B, i64 N, T* gx, cudaStream_t s) {
-  k_mean_var_grad<T><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, coefs, N, B, gx);
+void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const double* coefs, int B, i64 N, T* gx,
+                   cudaStream_t s) {
+  k_mean_var_grad<T><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1452,11 +1464,12 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
                                 const double*);               \
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*);                            \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
-  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*, double*,  \
-                                    double*, int*, cudaStream_t);                                                                \
-  template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, T*, T*,          \
-                                    cudaStream_t);                                                                \
-  template void mean_var_grad<T>(const T*, const double*, const double*, int, i64, T*, cudaStream_t);            \
+  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
+                                    const uint8_t*, double*, double*, int*, cudaStream_t);                                                                \
+  template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, const uint8_t*, \
+                                    T*, T*, cudaStream_t);                                                                \
+  template void mean_var_grad<T>(const T*, const double*, const uint8_t*, const double*, int, i64, T*,           \
+                                 cudaStream_t);            \
   template void row_means<T>(const T*, bool, bool, i64, int, double*, double*, cudaStream_t);                     \
   template void moduli_deviations<T>(const T*, i64, int, int, const double*, T*, int, int, int, cudaStream_t);
 INST(float)

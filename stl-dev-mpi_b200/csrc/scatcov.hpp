@@ -54,15 +54,32 @@ struct KernelStat {
   double ms = 0.0, bytes = 0.0, flops = 0.0;
 };
 
+// A disc patch (or any sky region) of the engine's grid mode: per level the
+// sorted NESTED ids of the support (level d + 1: the parents of level d)
+// and the positions in them of the pixels the coefficients average (the
+// core).
+struct Support {
+  std::vector<std::vector<int64_t>> ids;
+  std::vector<std::vector<int64_t>> core;
+};
+
 class Engine {
  public:
   static std::unique_ptr<Engine> create(const Options& o);
+  // Grid mode: the fields live on the support only, the wavelets are bound
+  // to it (binding threshold 1e-9), the decimations restricted to it, and
+  // the coefficients average the core.  Batch 1.
+  static std::unique_ptr<Engine> create_patch(const Options& o, const Support& s);
   virtual ~Engine() = default;
 
   const Options& options() const { return opt_; }
   const std::vector<Coef>& plan() const { return plan_; }
   int levels() const { return levels_; }
-  i64 npix(int d) const { return 12 * (opt_.nside >> d) * (opt_.nside >> d); }
+  i64 npix(int d) const { return npix_[d]; }
+  // pixels a coefficient of native level d averages
+  i64 ncore(int d) const { return ncore_[d]; }
+  bool grid_mode() const { return !support_.ids.empty(); }
+  const Support& support() const { return support_; }
   bool fp32() const { return opt_.fp32; }
 
   void set_stream(cudaStream_t s) { stream_ = s; }
@@ -74,8 +91,8 @@ class Engine {
   virtual void load_host(const double* x) = 0;
   virtual void load_device(const void* x, bool f32) = 0;
   // Maps given at every level (host f64, the concatenation over d of
-  // [B][12 (nside / 2^d)^2]): the next forward uses them instead of the
-  // decimation pyramid of level 0.
+  // [B][npix(d)]): the next forward uses them instead of the decimation
+  // pyramid of level 0.
   virtual void load_levels(const double* x) = 0;
   // Forward sweep on the loaded maps: values [B][np] complex (interleaved),
   // var [B][np] when moments.  Host outputs; the call synchronises.
@@ -104,10 +121,12 @@ class Engine {
   virtual std::vector<double> mean_slots() const = 0;
 
  protected:
-  explicit Engine(const Options& o);
+  explicit Engine(const Options& o, const Support* s = nullptr);
   Options opt_;
   std::vector<Coef> plan_;
   int levels_ = 1;
+  Support support_;
+  std::vector<i64> npix_, ncore_;
   cudaStream_t stream_ = nullptr;
   size_t operator_bytes_ = 0, field_bytes_ = 0;
 };

@@ -74,6 +74,17 @@ def lib():
             "stlp_restore": ([_VOID, _VOID, u64, u64, u64], C.c_int),
             "stlp_forward_levels": ([_VOID, _D, sz, _D], C.c_int),
             "stlp_lbfgs": ([_D, sz, C.c_char_p, _CALLBACK, _VOID], C.c_int64),
+            "stlp_patch_new": ([C.c_char_p], _VOID),
+            "stlp_patch_free": ([_VOID], None),
+            "stlp_patch_info": ([_VOID], _VOID),
+            "stlp_pixel_vectors": ([sz, C.POINTER(C.c_int64), sz, _D], C.c_int),
+            "stlp_patch_select": ([_VOID, _D, sz, C.c_double, C.c_double, _SIZE], C.c_int),
+            "stlp_patch_ids": ([_VOID, sz, C.POINTER(C.c_int64)], C.c_int),
+            "stlp_patch_core_pixels": ([_VOID, _SIZE], C.c_int),
+            "stlp_patch_forward": ([_VOID, _D, sz, u64, b, _D, _D], C.c_int),
+            "stlp_patch_vjp": ([_VOID, _D, sz, u64, _D], C.c_int),
+            "stlp_patch_forward_device": ([_VOID, u64, sz, u64, b, _D, _D], C.c_int),
+            "stlp_patch_vjp_device": ([_VOID, _D, sz, u64, u64], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(l, name)
@@ -442,3 +453,152 @@ def synthesis_objective(engine, target, weights=None):
         return loss, grad.reshape(np.shape(x))
 
     return f
+
+
+class PatchEngine:
+    """Statistics of disc patches and their VJP on the GPU (the reference's
+    PatchEngine, native.py:1074-1370, one channel).  Discs are selected by centre
+    (NESTED pixel ids at nside, or vectors [B, 3]), radius and optional core
+    radius in degrees; the coefficients average the core (else the whole disc)."""
+
+    def __init__(self, nside, j, kernel=5, orientations=4, dtype="float64", device=0, cache=256, threads=0):
+        cfg = dict(nside=int(nside), j=int(j), kernel=int(kernel), orientations=int(orientations), backend="gpu",
+                   dtype=dtype, device=int(device), cache=int(cache), threads=int(threads))
+        self._lib = lib()
+        self._mutex = threading.RLock()
+        self._handle = self._lib.stlp_patch_new(json.dumps(cfg).encode())
+        if not self._handle:
+            raise _error()
+        self.nside, self.j, self.dtype = int(nside), int(j), dtype
+        info = self.info()
+        self.plan = info["plan"]
+        self.ncoeff = len(self.plan)
+        self.levels = info["levels"]
+        self._native = np.array([c["native_dg"] for c in self.plan], dtype=np.int64)
+        self.ids, self._selection, self._generation, self._dense = [], None, None, False
+
+    def _open(self):
+        if not self._handle:
+            raise RuntimeError("patch engine is closed")
+
+    def info(self):
+        with self._mutex:
+            self._open()
+            p = self._lib.stlp_patch_info(self._handle)
+            if not p:
+                raise _error()
+            try:
+                return json.loads(C.string_at(p))
+            finally:
+                self._lib.stlp_string_free(p)
+
+    def centre_vectors(self, centres):
+        c = np.asarray(centres)
+        if np.issubdtype(c.dtype, np.integer):
+            ids = np.ascontiguousarray(c.reshape(-1), dtype=np.int64)
+            out = np.empty((ids.size, 3), dtype=np.float64)
+            if self._lib.stlp_pixel_vectors(self.nside, ids.ctypes.data_as(C.POINTER(C.c_int64)), ids.size, _ptr(out)):
+                raise _error()
+            return out
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        if c.ndim == 1:
+            c = c[None]
+        if c.ndim != 2 or c.shape[1] != 3:
+            raise ValueError("centres must be NESTED pixel indices [B] or vectors [B, 3]")
+        return c
+
+    def select(self, centres, radius, core=None):
+        """Selects the discs (radius, core in degrees); returns their sorted NESTED pixels."""
+        with self._mutex:
+            self._open()
+            v = np.ascontiguousarray(self.centre_vectors(centres))
+            key = (v.tobytes(), float(radius), None if core is None else float(core))
+            if key == self._selection:
+                return self.ids
+            b = v.shape[0]
+            counts = np.empty(b, dtype=np.uintp)
+            rc = 0.0 if core is None else np.radians(float(core))
+            self._generation, self._selection = None, None
+            if self._lib.stlp_patch_select(self._handle, _ptr(v), b, np.radians(float(radius)), rc,
+                                           counts.ctypes.data_as(_SIZE)):
+                raise _error()
+            ids = []
+            for i, n in enumerate(counts):
+                a = np.empty(int(n), dtype=np.int64)
+                if self._lib.stlp_patch_ids(self._handle, i, a.ctypes.data_as(C.POINTER(C.c_int64))):
+                    raise _error()
+                ids.append(a)
+            core_pixels = np.empty((b, self.levels), dtype=np.uintp)
+            if self._lib.stlp_patch_core_pixels(self._handle, core_pixels.ctypes.data_as(_SIZE)):
+                raise _error()
+            self.ids, self._selection = ids, key
+            self.native_pixels = core_pixels.astype(np.float64)[:, self._native]
+            return ids
+
+    def gather(self, maps):
+        m = np.asarray(maps)
+        if m.ndim == 1:
+            return [m[i] for i in self.ids]
+        return [m[k][..., i] for k, i in enumerate(self.ids)]
+
+    def forward(self, maps, centres=None, radius=None, core=None, moments=True, generation=0):
+        """Statistics [B, ncoeff] (and variances) of the patches of the selected discs."""
+        with self._mutex:
+            self._open()
+            if centres is not None:
+                if radius is None:
+                    raise ValueError("radius (degrees) is required with centres")
+                self.select(centres, radius, core)
+            if not self.ids:
+                raise RuntimeError("no disc selected")
+            b = len(self.ids)
+            if len(maps) != b:
+                raise ValueError(f"expected {b} patches, got {len(maps)}")
+            parts = []
+            for i, (m, ids) in enumerate(zip(maps, self.ids)):
+                m = np.asarray(m, dtype=np.float64)
+                if m.shape != (ids.size,):
+                    raise ValueError(f"patch {i}: expected {(ids.size,)}, got {m.shape}")
+                parts.append(m.reshape(-1))
+            x = np.ascontiguousarray(np.concatenate(parts))
+            if not np.isfinite(x).all():
+                raise ValueError("input patch contains non-finite values")
+            self._dense = isinstance(maps, np.ndarray)
+            values = np.empty((b, self.ncoeff), dtype=np.complex128)
+            variance = np.empty((b, self.ncoeff if moments else 0), dtype=np.float64)
+            self._generation = None
+            if self._lib.stlp_patch_forward(self._handle, _ptr(x), x.size, int(generation), bool(moments),
+                                            _ptr(values.view(np.float64)), _ptr(variance) if moments else None):
+                raise _error()
+            self._generation = int(generation)
+            return values, variance
+
+    def vjp(self, cotangents, generation=0):
+        """Gradients of Re sum(conj(cotangents) values) with respect to the patches."""
+        with self._mutex:
+            self._open()
+            if self._generation is None or int(generation) != self._generation:
+                raise RuntimeError("stale forward state")
+            b = len(self.ids)
+            c = np.ascontiguousarray(cotangents, dtype=np.complex128)
+            if c.shape != (b, self.ncoeff):
+                raise ValueError(f"expected cotangents {(b, self.ncoeff)}, got {c.shape}")
+            if not np.isfinite(c.view(np.float64)).all():
+                raise ValueError("non-finite coefficient cotangent")
+            total = sum(i.size for i in self.ids)
+            g = np.empty(total, dtype=np.float64)
+            if self._lib.stlp_patch_vjp(self._handle, _ptr(c.view(np.float64)), c.size, int(generation), _ptr(g)):
+                raise _error()
+            out, off = [], 0
+            for ids in self.ids:
+                out.append(g[off:off + ids.size])
+                off += ids.size
+            return np.stack(out) if self._dense else out
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.stlp_patch_free(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
