@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--batch", type=int, default=4)
     p.add_argument("--skip-fp64", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches"],
+                   help="scatcov: the headline metric; patches: 512 ragged disc patches (nside 512, J 5)")
     return p.parse_args()
 
 
@@ -180,6 +182,83 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def patch_workload(nside=512, n=512, seed=3):
+    """Centres uniform on the sphere; pixel counts log-uniform in [1024, 65536]
+    through R = acos(1 - n Omega_pix / (2 pi)), Omega_pix = 4 pi / (12 nside^2)."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    counts = np.exp(rng.uniform(np.log(1024.0), np.log(65536.0), n))
+    omega = 4.0 * np.pi / (12.0 * nside * nside)
+    radii = np.degrees(np.arccos(1.0 - counts * omega / (2.0 * np.pi)))
+    return v, radii
+
+
+def run_patches(args, torch, dist, world, rank, dev):
+    """Forward + VJP of 512 disc patches (nside 512, J 5, L 4, FP32 fields, values
+    N(0, 1)): patches per second, device-resident patches and through the host API."""
+    import stl_b200
+    nside, J = 512, 5
+    centres, radii = patch_workload(nside)
+    pe = stl_b200.PatchEngine(nside, J, dtype="float32", device=dev.index)
+    t0 = time.perf_counter()
+    ids = pe.select(centres, radii)
+    sizes = np.array([i.size for i in ids])
+    rng = np.random.default_rng(100 + rank)
+    patches = [rng.standard_normal(k) for k in sizes]
+    x_host = np.concatenate(patches)
+    x_dev = torch.tensor(x_host, dtype=torch.float64, device=dev)
+    g_dev = torch.empty_like(x_dev)
+    ncoeff = pe.ncoeff
+    lib = stl_b200.lib()
+    vals = np.empty((len(ids), ncoeff), np.complex128)
+    cot = np.ascontiguousarray(np.ones((len(ids), ncoeff), np.complex128))
+    gen = iter(range(1, 10 ** 9))
+    dptr = stl_b200._ptr
+
+    def step_dev():
+        g = next(gen)
+        torch.cuda.current_stream().synchronize()
+        if lib.stlp_patch_forward_device(pe._handle, x_dev.data_ptr(), x_host.size, g, False,
+                                         dptr(vals.view(np.float64)), None):
+            raise stl_b200._error()
+        if lib.stlp_patch_vjp_device(pe._handle, dptr(cot.view(np.float64)), cot.size, g, g_dev.data_ptr()):
+            raise stl_b200._error()
+
+    step_dev()  # builds the discs' engines
+    build_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step_dev()
+    with Clocks(dev.index) as clk:
+        ms = time_steps(torch, step_dev, args.steps, 0, dist)
+    clocks = clk.summary()
+
+    def step_host():
+        g = next(gen)
+        v, _ = pe.forward(patches, moments=False, generation=g)
+        pe.vjp(np.ones_like(v), generation=g)
+
+    ms_e2e = time_steps(torch, step_host, max(2, args.steps // 2), 1, dist)
+    e2e_steps = max(2, args.steps // 2)
+    if rank == 0:
+        b = len(ids)
+        line = {"metric": "disc-patch fwd+VJP patches/s (512 ragged discs, nside 512, J=5)",
+                "value": world * b * args.steps / (ms / 1e3), "unit": "patches/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "512 disc patches, nside 512, J 5, L 4, FP32 fields, values N(0,1)",
+                           "pixels_min": int(sizes.min()), "pixels_max": int(sizes.max()),
+                           "pixels_total": int(sizes.sum()), "build_s": build_s,
+                           "parallelism": f"replicas x{world}"},
+                "e2e": {"value": world * b * e2e_steps / (ms_e2e / 1e3), "unit": "patches/s",
+                        "h2d_bytes_per_step": int(x_host.size * 8 + cot.size * 16),
+                        "d2h_bytes_per_step": int(vals.size * 16 + x_host.size * 8)},
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    pe.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -198,6 +277,12 @@ def main():
         torch.cuda.set_device(0)
     import stl_b200
 
+    if args.workload == "patches":
+        run_patches(args, torch, dist, world, rank, torch.device("cuda", local if world > 1 else 0))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     nside, J, B = args.nside, args.J, args.batch
     npix = 12 * nside * nside
     dev = torch.device("cuda", local if world > 1 else 0)

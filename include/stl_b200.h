@@ -132,6 +132,11 @@ void stlp_patch_free(StlpPatchHandle* h);
 char* stlp_patch_info(StlpPatchHandle* h);
 int stlp_pixel_vectors(size_t nside, const int64_t* ids, size_t n, double* out);
 int stlp_patch_select(StlpPatchHandle* h, const double* centres, size_t b, double radius, double core, size_t* counts);
+/* stlp_patch_select with a radius and a core radius per disc (radii, cores:
+ * b values in radians; cores NULL or a value <= 0: average the whole disc).
+ * No reference counterpart: the reference takes one radius per call. */
+int stlp_patch_select_radii(StlpPatchHandle* h, const double* centres, size_t b, const double* radii,
+                            const double* cores, size_t* counts);
 int stlp_patch_ids(StlpPatchHandle* h, size_t patch, int64_t* out);
 int stlp_patch_core_pixels(StlpPatchHandle* h, size_t* out);
 int stlp_patch_forward(StlpPatchHandle* h, const double* x, size_t n, uint64_t generation, bool moments, double* out,

@@ -267,23 +267,24 @@ int stlp_pixel_vectors(size_t nside, const int64_t* ids, size_t n, double* out) 
   });
 }
 
-int stlp_patch_select(StlpPatchHandle* h, const double* centres, size_t b, double radius, double core,
-                      size_t* counts) {
-  return guard<int>(-1, [&] {
+static int select_discs(StlpPatchHandle* h, const double* centres, size_t b, const double* radii,
+                        const double* cores, size_t* counts) {
     require(h != nullptr && centres != nullptr && counts != nullptr, "null argument");
     h->has_current = false;
     h->selected.clear();
     require(b > 0, "empty batch");
-    require(std::isfinite(radius) && radius > 0.0, "disc radius must be positive");
-    const double cr = (std::isfinite(core) && core > 0.0 && core < radius) ? core : -1.0;
     std::vector<Key> keys(b);
     std::vector<std::array<double, 3>> unit(b);
+    std::vector<double> rad(b), cor(b);
     for (size_t i = 0; i < b; ++i) {
+      rad[i] = radii[i];
+      require(std::isfinite(rad[i]) && rad[i] > 0.0, "disc radius must be positive");
+      cor[i] = (std::isfinite(cores[i]) && cores[i] > 0.0 && cores[i] < rad[i]) ? cores[i] : -1.0;
       const double* c = centres + 3 * i;
       const double nrm = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
       require(nrm > 0.0 && std::isfinite(nrm), "disc centre must be a nonzero finite vector");
       unit[i] = {c[0] / nrm, c[1] / nrm, c[2] / nrm};
-      keys[i] = Key{{bits(unit[i][0]), bits(unit[i][1]), bits(unit[i][2]), bits(radius), bits(cr)}};
+      keys[i] = Key{{bits(unit[i][0]), bits(unit[i][1]), bits(unit[i][2]), bits(rad[i]), bits(cor[i])}};
     }
     // supports of the discs not cached, built on the host threads
     std::vector<size_t> missing;
@@ -302,7 +303,8 @@ int stlp_patch_select(StlpPatchHandle* h, const double* centres, size_t b, doubl
     auto work = [&](size_t k0, size_t k1) {
       for (size_t k = k0; k < k1; ++k) {
         try {
-          built[k] = disc_support(h->opt.nside, h->levels, unit[missing[k]].data(), radius, cr);
+          const size_t i = missing[k];
+          built[k] = disc_support(h->opt.nside, h->levels, unit[i].data(), rad[i], cor[i]);
         } catch (const std::exception& e) {
           errors[k] = e.what();
         }
@@ -333,6 +335,23 @@ int stlp_patch_select(StlpPatchHandle* h, const double* centres, size_t b, doubl
     }
     for (size_t i = 0; i < b; ++i) counts[i] = h->size(i);
     return 0;
+}
+
+int stlp_patch_select(StlpPatchHandle* h, const double* centres, size_t b, double radius, double core,
+                      size_t* counts) {
+  return guard<int>(-1, [&] {
+    std::vector<double> r(b, radius), c(b, core);
+    return select_discs(h, centres, b, r.data(), c.data(), counts);
+  });
+}
+
+int stlp_patch_select_radii(StlpPatchHandle* h, const double* centres, size_t b, const double* radii,
+                            const double* cores, size_t* counts) {
+  return guard<int>(-1, [&] {
+    require(radii != nullptr, "null argument");
+    std::vector<double> c(b, 0.0);
+    if (cores) c.assign(cores, cores + b);
+    return select_discs(h, centres, b, radii, c.data(), counts);
   });
 }
 

@@ -79,6 +79,7 @@ def lib():
             "stlp_patch_info": ([_VOID], _VOID),
             "stlp_pixel_vectors": ([sz, C.POINTER(C.c_int64), sz, _D], C.c_int),
             "stlp_patch_select": ([_VOID, _D, sz, C.c_double, C.c_double, _SIZE], C.c_int),
+            "stlp_patch_select_radii": ([_VOID, _D, sz, _D, _D, _SIZE], C.c_int),
             "stlp_patch_ids": ([_VOID, sz, C.POINTER(C.c_int64)], C.c_int),
             "stlp_patch_core_pixels": ([_VOID, _SIZE], C.c_int),
             "stlp_patch_forward": ([_VOID, _D, sz, u64, b, _D, _D], C.c_int),
@@ -508,19 +509,29 @@ class PatchEngine:
         return c
 
     def select(self, centres, radius, core=None):
-        """Selects the discs (radius, core in degrees); returns their sorted NESTED pixels."""
+        """Selects the discs (radius, core in degrees: one for all, or one per disc);
+        returns their sorted NESTED pixels."""
         with self._mutex:
             self._open()
             v = np.ascontiguousarray(self.centre_vectors(centres))
-            key = (v.tobytes(), float(radius), None if core is None else float(core))
+            key = (v.tobytes(), np.asarray(radius, np.float64).tobytes(),
+                   None if core is None else np.asarray(core, np.float64).tobytes())
             if key == self._selection:
                 return self.ids
             b = v.shape[0]
             counts = np.empty(b, dtype=np.uintp)
-            rc = 0.0 if core is None else np.radians(float(core))
             self._generation, self._selection = None, None
-            if self._lib.stlp_patch_select(self._handle, _ptr(v), b, np.radians(float(radius)), rc,
-                                           counts.ctypes.data_as(_SIZE)):
+            if np.ndim(radius) == 0 and (core is None or np.ndim(core) == 0):
+                rc = 0.0 if core is None else np.radians(float(core))
+                status = self._lib.stlp_patch_select(self._handle, _ptr(v), b, np.radians(float(radius)), rc,
+                                                     counts.ctypes.data_as(_SIZE))
+            else:  # a radius (and core) per disc
+                r = np.ascontiguousarray(np.radians(np.broadcast_to(np.asarray(radius, np.float64), (b,))))
+                c = np.zeros(b) if core is None else np.radians(np.broadcast_to(np.asarray(core, np.float64), (b,)))
+                c = np.ascontiguousarray(c)
+                status = self._lib.stlp_patch_select_radii(self._handle, _ptr(v), b, _ptr(r), _ptr(c),
+                                                           counts.ctypes.data_as(_SIZE))
+            if status:
                 raise _error()
             ids = []
             for i, n in enumerate(counts):
