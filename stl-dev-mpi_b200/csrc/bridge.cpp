@@ -77,7 +77,10 @@ struct StlpHandle {
   Identity current;
   int device = 0;
   size_t input_len() const { return (size_t)engine->options().B * (size_t)engine->npix(0); }
-  size_t values_len() const { return (size_t)engine->options().B * engine->plan().size(); }
+  // B K np: K masks (1 without)
+  size_t values_len() const {
+    return (size_t)engine->options().B * std::max(1, engine->nmasks()) * engine->plan().size();
+  }
   void activate() { STL_CUDA(cudaSetDevice(device)); }
 };
 
@@ -168,7 +171,7 @@ char* stlp_info(StlpHandle* h) {
        << ", \"j\": " << o.J << ", \"batch\": " << o.B << ", \"channels\": 1, \"cross\": false"
        << ", \"dtype\": " << jstr(o.fp32 ? "float32 fields, float64 sums/complex128" : "float64/complex128")
        << ", \"fewer\": false, \"orientations\": " << o.L << ", \"kernel\": " << o.ksz
-       << ", \"levels\": " << e.levels() << ", \"masks\": 0, \"spin\": 0, \"device\": " << o.device
+       << ", \"levels\": " << e.levels() << ", \"masks\": " << e.nmasks() << ", \"spin\": 0, \"device\": " << o.device
        << ", \"conv\": \"folded-stencil\", \"fields\": \"keep\"";
     js << ", \"device_memory\": {\"operator_bytes\": " << e.operator_bytes() << ", \"field_bytes\": " << e.field_bytes()
        << ", \"live_bytes\": " << device_bytes_live() << ", \"peak_bytes\": " << device_bytes_peak() << "}";
@@ -207,7 +210,11 @@ int stlp_native_pixels(StlpHandle* h, size_t* out) {
   return guard<int>(-1, [&] {
     require(h != nullptr && out != nullptr, "null argument");
     const auto& plan = h->engine->plan();
-    for (size_t i = 0; i < plan.size(); ++i) out[i] = (size_t)h->engine->npix(plan[i].native);
+    const int K = std::max(1, h->engine->nmasks());
+    for (int k = 0; k < K; ++k)
+      for (size_t i = 0; i < plan.size(); ++i)
+        out[k * plan.size() + i] = (size_t)(h->engine->nmasks() ? h->engine->mask_count(k, plan[i].native)
+                                                               : h->engine->npix(plan[i].native));
     return 0;
   });
 }
@@ -215,9 +222,10 @@ int stlp_native_pixels(StlpHandle* h, size_t* out) {
 int stlp_set_masks(StlpHandle* h, const double* weights, size_t k) {
   return guard<int>(-1, [&] {
     require(h != nullptr, "null handle");
-    (void)weights;
+    require(k == 0 || weights != nullptr, "null mask weights");
     h->has_current = false;
-    require(k == 0, "masked averages are not built in this library yet");
+    h->activate();
+    h->engine->set_masks(weights, k);
     return 0;
   });
 }

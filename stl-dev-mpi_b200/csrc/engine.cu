@@ -239,6 +239,63 @@ class EngineImpl final : public Engine {
     for (size_t i = 0; i < plan_.size(); ++i) map_[i] = locate(plan_[i]);
   }
 
+  // Averages over k masks (level-0 indicators [k][npix(0)], nonzero: in
+  // the mask; level n + 1 keeps a parent when one of its children is in the
+  // mask, mask.rs:42-66), or over every pixel (k = 0).
+  void set_masks(const double* w, size_t k) override {
+    if (grid_mode()) throw std::runtime_error("a patch engine averages its core: no masks");
+    std::vector<std::vector<std::vector<uint8_t>>> levels(k);
+    const i64 n0 = npix(0);
+    for (size_t q = 0; q < k; ++q) {
+      auto& lv = levels[q];
+      lv.resize(levels_);
+      lv[0].resize(n0);
+      for (i64 p = 0; p < n0; ++p) {
+        const double v = w[q * n0 + p];
+        if (!std::isfinite(v)) throw std::runtime_error("mask weights must be finite");
+        lv[0][p] = v != 0.0;
+      }
+      for (int d = 1; d < levels_; ++d) {
+        lv[d].assign(npix(d), 0);
+        for (i64 p = 0; p < npix(d); ++p)
+          lv[d][p] = lv[d - 1][4 * p] | lv[d - 1][4 * p + 1] | lv[d - 1][4 * p + 2] | lv[d - 1][4 * p + 3];
+      }
+    }
+    upload_masks(levels);
+  }
+  int nmasks() const override { return kmask_.empty() || grid_mode() ? 0 : K_; }
+  i64 mask_count(int k, int n) const override { return count(k, n); }
+
+  // masks [k][level][pixel] (empty: every pixel) to the device; the sums
+  // hold one set per mask
+  void upload_masks(const std::vector<std::vector<std::vector<uint8_t>>>& levels) {
+    std::vector<std::vector<DevMem>> km(levels.size());
+    std::vector<std::vector<i64>> kc(levels.size());
+    for (size_t q = 0; q < levels.size(); ++q) {
+      km[q].resize(levels_);
+      kc[q].resize(levels_);
+      for (int d = 0; d < levels_; ++d) {
+        const auto& m = levels[q][d];
+        i64 c = 0;
+        for (uint8_t v : m) c += v;
+        if (c == 0) throw std::runtime_error("empty mask");
+        kc[q][d] = c;
+        km[q][d].alloc(m.size());
+        STL_CUDA(cudaMemcpyAsync(km[q][d].p, m.data(), m.size(), cudaMemcpyHostToDevice, stream_));
+      }
+      STL_CUDA(cudaStreamSynchronize(stream_));
+    }
+    kmask_ = std::move(km);
+    kcount_ = std::move(kc);
+    K_ = std::max<int>(1, (int)levels.size());
+    if (ready_) {
+      sums_.alloc(sizeof(double) * total_sums_ * K_);
+      h_sums_.resize(total_sums_ * K_);
+      mv_.alloc(sizeof(double) * 2 * opt_.B * K_);
+    }
+    forward_done_ = false;
+  }
+
   // field precision of level n
   bool hi(int n) const { return sizeof(T) == 8 || (opt_.nside >> n) <= kFp64Nside; }
   size_t esz(int n) const { return hi(n) ? 8 : sizeof(T); }
@@ -261,18 +318,17 @@ class EngineImpl final : public Engine {
     if (grid_mode()) {
       // supports and core masks on the device
       ids_dev_.resize(levels_);
-      core_mask_.resize(levels_);
+      std::vector<std::vector<uint8_t>> core(levels_);
       for (int d = 0; d < levels_; ++d) {
         const auto& ids = support_.ids[d];
         ids_dev_[d].alloc(sizeof(i64) * ids.size());
         STL_CUDA(cudaMemcpyAsync(ids_dev_[d].p, ids.data(), sizeof(i64) * ids.size(), cudaMemcpyHostToDevice,
                                  stream_));
-        std::vector<uint8_t> m(ids.size(), 0);
-        for (i64 c : support_.core[d]) m[c] = 1;
-        core_mask_[d].alloc(m.size());
-        STL_CUDA(cudaMemcpyAsync(core_mask_[d].p, m.data(), m.size(), cudaMemcpyHostToDevice, stream_));
         STL_CUDA(cudaStreamSynchronize(stream_));
+        core[d].assign(ids.size(), 0);
+        for (i64 c : support_.core[d]) core[d][c] = 1;
       }
+      upload_masks({core});
     }
     for (int n = 0; n < levels_; ++n) {
       ConvSpec cs;
@@ -340,8 +396,9 @@ class EngineImpl final : public Engine {
       sum_off_[n] = total_sums;
       total_sums += (size_t)B * L * shapes_[n].slots;
     }
-    sums_.alloc(sizeof(double) * total_sums);
-    h_sums_.resize(total_sums);
+    total_sums_ = total_sums;
+    sums_.alloc(sizeof(double) * total_sums * K_);
+    h_sums_.resize(total_sums * K_);
     gZ_.alloc(max_gz);
     gBr_.alloc(max_gbr);
     size_t max_m = 0;
@@ -349,7 +406,7 @@ class EngineImpl final : public Engine {
       max_m = std::max(max_m, esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K);
     M_.alloc(max_m);
     s1c_.alloc(sizeof(double) * B * L);
-    mv_.alloc(sizeof(double) * 2 * B);
+    mv_.alloc(sizeof(double) * 2 * B * K_);
     err_.alloc(sizeof(int));
     STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
     // per-row constants of the fields: maps [level][B], moduli [level][B][L],
@@ -532,12 +589,13 @@ class EngineImpl final : public Engine {
     });
     const ProductShape& sh = shapes_[n];
     const double E = sh.K * (sh.K + 1) / 2.0;
-    prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
-                 [&] {
-                   products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
-                                       xc_.as<double>(), mask(n), partials_.as<double>(),
-                                       sums_.as<double>() + sum_off_[n], err_.as<int>(), s);
-                 });
+    for (int k = 0; k < K_; ++k)
+      prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
+                   [&] {
+                     products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
+                                         xc_.as<double>(), mask(k, n), partials_.as<double>(),
+                                         sums_.as<double>() + k * total_sums_ + sum_off_[n], err_.as<int>(), s);
+                   });
   }
 
   void reverse_host(const double* cot, double* out) override {
@@ -634,21 +692,24 @@ class EngineImpl final : public Engine {
     return l;
   }
 
+  // values [B][K][np] complex, var [B][K][np]
   void assemble(double* values, double* var) const {
     const int L = opt_.L, B = opt_.B;
     const i64 np = (i64)plan_.size();
     for (int b = 0; b < B; ++b)
-      for (i64 i = 0; i < np; ++i) {
-        const Loc& l = map_[i];
-        const ProductShape& sh = shapes_[l.level];
-        const double* row = h_sums_.data() + sum_off_[l.level] + ((size_t)b * L + l.l3) * sh.slots;
-        const double N = (double)ncore(l.level);
-        const double re = row[l.re], im = l.im >= 0 ? row[l.im] : 0.0, second = row[l.second];
-        const double vr = re / N, vi = im / N;
-        values[2 * (b * np + i)] = vr;
-        values[2 * (b * np + i) + 1] = vi;
-        if (var) var[b * np + i] = std::max(second / N - (vr * vr + vi * vi), 0.0);
-      }
+      for (int k = 0; k < K_; ++k)
+        for (i64 i = 0; i < np; ++i) {
+          const Loc& l = map_[i];
+          const ProductShape& sh = shapes_[l.level];
+          const double* row = h_sums_.data() + k * total_sums_ + sum_off_[l.level] + ((size_t)b * L + l.l3) * sh.slots;
+          const double N = (double)count(k, l.level);
+          const double re = row[l.re], im = l.im >= 0 ? row[l.im] : 0.0, second = row[l.second];
+          const double vr = re / N, vi = im / N;
+          const i64 o = ((i64)b * K_ + k) * np + i;
+          values[2 * o] = vr;
+          values[2 * o + 1] = vi;
+          if (var) var[o] = std::max(second / N - (vr * vr + vi * vi), 0.0);
+        }
   }
 
   void reverse_impl(const double* cot) {
@@ -657,24 +718,30 @@ class EngineImpl final : public Engine {
     const int L = opt_.L, B = opt_.B;
     const i64 np = (i64)plan_.size();
     cudaStream_t s = stream_;
-    // host: per-level cotangent matrices, auto-S1 scales, mean/var scales
-    std::vector<std::vector<std::complex<double>>> M(levels_);
-    std::vector<std::vector<double>> s1(levels_, std::vector<double>((size_t)B * L, 0.0));
-    std::vector<double> mv((size_t)2 * B, 0.0);
-    for (int n = 0; n < levels_; ++n) M[n].assign((size_t)B * L * shapes_[n].K * shapes_[n].K, 0.0);
+    // host: per mask and level, cotangent matrices, auto-S1 scales, mean/var scales
+    std::vector<std::vector<std::vector<std::complex<double>>>> Mk(K_, std::vector<std::vector<std::complex<double>>>(levels_));
+    std::vector<std::vector<std::vector<double>>> s1k(
+        K_, std::vector<std::vector<double>>(levels_, std::vector<double>((size_t)B * L, 0.0)));
+    std::vector<double> mv((size_t)2 * B * K_, 0.0);
+    for (int k = 0; k < K_; ++k)
+      for (int n = 0; n < levels_; ++n) Mk[k][n].assign((size_t)B * L * shapes_[n].K * shapes_[n].K, 0.0);
     for (int b = 0; b < B; ++b)
+      for (int mk = 0; mk < K_; ++mk)
       for (i64 i = 0; i < np; ++i) {
-        std::complex<double> g(cot[2 * (b * np + i)], cot[2 * (b * np + i) + 1]);
+        const i64 o = ((i64)b * K_ + mk) * np + i;
+        std::complex<double> g(cot[2 * o], cot[2 * o + 1]);
         if (g == std::complex<double>(0.0, 0.0)) continue;
         const Coef& c = plan_[i];
         int n = c.native, K = shapes_[n].K, z = K - 1;
-        double N = (double)ncore(n);
+        double N = (double)count(mk, n);
+        auto& M = Mk[mk];
+        auto& s1 = s1k[mk];
         auto at = [&](int l3, int r, int q) -> std::complex<double>& {
           return M[n][(((size_t)b * L + l3) * K + r) * K + q];
         };
         switch (c.family) {
-          case MEAN: mv[2 * b] += g.real() / N; break;
-          case VAR: mv[2 * b + 1] += 2.0 * g.real() / N; break;
+          case MEAN: mv[(size_t)mk * 2 * B + 2 * b] += g.real() / N; break;
+          case VAR: mv[(size_t)mk * 2 * B + 2 * b + 1] += 2.0 * g.real() / N; break;
           case S1: s1[n][(size_t)b * L + c.l1] += g.real() / N; break;
           case S2: at(c.l1, z, z) += 2.0 * g.real() / N; break;
           case S3: {
@@ -692,15 +759,16 @@ class EngineImpl final : public Engine {
         }
       }
     for (int n = levels_ - 1; n >= 0; --n)
-      typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n, M[n], s1[n]); });
+      typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n, Mk, s1k); });
     STL_CUDA(cudaMemcpyAsync(mv_.p, mv.data(), mv.size() * 8, cudaMemcpyHostToDevice, s));
-    prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
-      typed(0, [&](auto t) {
-        using U = typename decltype(t)::type;
-        mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mask(0), mv_.as<double>(), B, npix(0), gX_[0].as<U>(),
-                         s);
+    for (int k = 0; k < K_; ++k)
+      prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
+        typed(0, [&](auto t) {
+          using U = typename decltype(t)::type;
+          mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mask(k, 0), mv_.as<double>() + (size_t)k * 2 * B, B,
+                           npix(0), gX_[0].as<U>(), s);
+        });
       });
-    });
     int err = 0;
     STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     STL_CUDA(cudaStreamSynchronize(s));
@@ -716,7 +784,8 @@ class EngineImpl final : public Engine {
   // one level of the reverse sweep (field type U); M: the level's cotangent
   // matrices [B][L][K][K], s1: the auto-S1 scales [B][L]
   template <typename U>
-  void reverse_level(int n, const std::vector<std::complex<double>>& M, const std::vector<double>& s1) {
+  void reverse_level(int n, const std::vector<std::vector<std::vector<std::complex<double>>>>& Mk,
+                     const std::vector<std::vector<std::vector<double>>>& s1k) {
     const int L = opt_.L, B = opt_.B;
     cudaStream_t s = stream_;
     const i64 N = npix(n);
@@ -734,18 +803,25 @@ class EngineImpl final : public Engine {
                    });
     else
       STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
-    // cotangent matrices in the field precision
-    std::vector<U> hm(2 * M.size()), hs(s1.size());
-    for (size_t q = 0; q < M.size(); ++q) { hm[2 * q] = (U)M[q].real(); hm[2 * q + 1] = (U)M[q].imag(); }
-    for (size_t q = 0; q < s1.size(); ++q) hs[q] = (U)s1[q];
-    STL_CUDA(cudaMemcpyAsync(M_.p, hm.data(), hm.size() * sizeof(U), cudaMemcpyHostToDevice, s));
-    STL_CUDA(cudaMemcpyAsync(s1c_.p, hs.data(), hs.size() * sizeof(U), cudaMemcpyHostToDevice, s));
+    // cotangent matrices in the field precision, one set per mask; the
+    // products VJP of mask k > 0 adds to that of the masks before it
     const double sz = sizeof(U);
-    prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0, s,
-                 [&] {
-                   products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), M_.as<U>(), s1c_.as<U>(), mask(n),
-                                       gZ_.as<U>(), gBr_.as<U>(), s);
-                 });
+    std::vector<std::vector<U>> hm(K_), hs(K_);
+    for (int k = 0; k < K_; ++k) {
+      const auto& M = Mk[k][n];
+      const auto& s1 = s1k[k][n];
+      hm[k].resize(2 * M.size());
+      hs[k].resize(s1.size());
+      for (size_t q = 0; q < M.size(); ++q) { hm[k][2 * q] = (U)M[q].real(); hm[k][2 * q + 1] = (U)M[q].imag(); }
+      for (size_t q = 0; q < s1.size(); ++q) hs[k][q] = (U)s1[q];
+      STL_CUDA(cudaMemcpyAsync(M_.p, hm[k].data(), hm[k].size() * sizeof(U), cudaMemcpyHostToDevice, s));
+      STL_CUDA(cudaMemcpyAsync(s1c_.p, hs[k].data(), hs[k].size() * sizeof(U), cudaMemcpyHostToDevice, s));
+      prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0,
+                   s, [&] {
+                     products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), M_.as<U>(), s1c_.as<U>(), mask(k, n),
+                                         k > 0, gZ_.as<U>(), gBr_.as<U>(), s);
+                   });
+    }
     const int R = B * (n + 1) * L;
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), R, adj_ptr()) ? 2 : 1,
                  conv_bytes(op, R, false, true), conv_flops(op, R), s,
@@ -779,8 +855,15 @@ class EngineImpl final : public Engine {
   std::vector<size_t> sum_off_;
   DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_, roles_;
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
-  std::vector<DevMem> ids_dev_, core_mask_;  // grid mode: supports and core masks per level
-  const uint8_t* mask(int n) const { return grid_mode() ? core_mask_[n].as<uint8_t>() : nullptr; }
+  std::vector<DevMem> ids_dev_;  // grid mode: supports per level
+  // averaging masks [k][level] (grid mode: the core; none: every pixel) and
+  // their pixel counts
+  int K_ = 1;
+  std::vector<std::vector<DevMem>> kmask_;
+  std::vector<std::vector<i64>> kcount_;
+  size_t total_sums_ = 0;
+  const uint8_t* mask(int k, int n) const { return kmask_.empty() ? nullptr : kmask_[k][n].as<uint8_t>(); }
+  i64 count(int k, int n) const { return kcount_.empty() ? npix(n) : kcount_[k][n]; }
   DevMem adj_part_;
   AdjScratch adj_;
   const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }

@@ -225,9 +225,10 @@ template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
                       const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
+// accumulate: add to gz / gbr (on the mask's pixels) instead of writing them
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, const uint8_t* mask,
-                      T* gz, T* gbr, cudaStream_t s);
+                      bool accumulate, T* gz, T* gbr, cudaStream_t s);
 // gx[p][b] += coefs[b][0] + coefs[b][1] (xc[b] + x0[p][b])
 template <typename T>
 void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const double* coefs, int B, i64 N, T* gx,

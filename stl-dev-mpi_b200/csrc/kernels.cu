@@ -899,8 +899,8 @@ template <typename T, int K>
 __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, const T* __restrict__ z,
                                                               const T* __restrict__ br, const T* __restrict__ M,
                                                               const T* __restrict__ s1c,
-                                                              const uint8_t* __restrict__ mask, T* __restrict__ gz,
-                                                              T* __restrict__ gbr) {
+                                                              const uint8_t* __restrict__ mask, int accumulate,
+                                                              T* __restrict__ gz, T* __restrict__ gbr) {
   extern __shared__ __align__(16) unsigned char smem[];
   typedef typename V2<T>::type T2;
   constexpr int L = 4, K1 = K - 1;
@@ -920,10 +920,12 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, cons
   for (i64 p = (i64)blockIdx.x * TPX + px; p < N; p += (i64)gridDim.x * TPX) {
     const i64 row = (p * B + b) * K1;
     if (mask && !mask[p]) {  // outside the averaged pixels: no cotangent
-      T2 zero;
-      zero.x = (T)0; zero.y = (T)0;
-      for (int i = 0; i < K1; ++i) gbrv[(row + i) * L + l3] = zero;
-      gzv[(p * B + b) * L + l3] = zero;
+      if (!accumulate) {
+        T2 zero;
+        zero.x = (T)0; zero.y = (T)0;
+        for (int i = 0; i < K1; ++i) gbrv[(row + i) * L + l3] = zero;
+        gzv[(p * B + b) * L + l3] = zero;
+      }
       continue;
     }
     T2 v[K];
@@ -940,17 +942,24 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, cons
         ai = fma(mm.x, v[j].y, fma(mm.y, v[j].x, ai));
       }
       T2 o;
+      T2* dst;
       if (i == K1) {
         const T mag = hypot(v[K1].x, v[K1].y);
         const T c = c1 / (mag == (T)0 ? (T)1 : mag);
         o.x = ar + c * v[K1].x;
         o.y = ai + c * v[K1].y;
-        gzv[(p * B + b) * L + l3] = o;
+        dst = gzv + (p * B + b) * L + l3;
       } else {
         o.x = ar;
         o.y = ai;
-        gbrv[(row + i) * L + l3] = o;
+        dst = gbrv + (row + i) * L + l3;
       }
+      if (accumulate) {
+        const T2 prev = *dst;
+        o.x += prev.x;
+        o.y += prev.y;
+      }
+      *dst = o;
     }
   }
 }
@@ -1350,14 +1359,15 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
 namespace {
 template <typename T, int K>
 void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c,
-                        const uint8_t* mask, T* gz, T* gbr, cudaStream_t s) {
+                        const uint8_t* mask, bool accumulate, T* gz, T* gbr, cudaStream_t s) {
   const size_t smem = (size_t)4 * K * K * 2 * sizeof(T);
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products_rev<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const i64 tiles = (sh.N + kRevThreads / 4 - 1) / (kRevThreads / 4);
   const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 / sh.B));
   dim3 grid(gx, sh.B);
-  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, z, br, M, s1c, mask, gz, gbr);
+  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, z, br, M, s1c, mask, accumulate ? 1 : 0, gz,
+                                                       gbr);
 }
 }  // namespace
 
@@ -1382,18 +1392,18 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
 
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c,
-                      const uint8_t* mask, T* gz, T* gbr, cudaStream_t s) {
+                      const uint8_t* mask, bool accumulate, T* gz, T* gbr, cudaStream_t s) {
   switch (sh.nd) {
-    case 1: products_reverse_k<T, 5>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 2: products_reverse_k<T, 9>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 3: products_reverse_k<T, 13>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 4: products_reverse_k<T, 17>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 5: products_reverse_k<T, 21>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 6: products_reverse_k<T, 25>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 7: products_reverse_k<T, 29>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 8: products_reverse_k<T, 33>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 9: products_reverse_k<T, 37>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
-    case 10: products_reverse_k<T, 41>(sh, z, br, M, s1c, mask, gz, gbr, s); break;
+    case 1: products_reverse_k<T, 5>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 2: products_reverse_k<T, 9>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 3: products_reverse_k<T, 13>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 4: products_reverse_k<T, 17>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 5: products_reverse_k<T, 21>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 6: products_reverse_k<T, 25>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 7: products_reverse_k<T, 29>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 8: products_reverse_k<T, 33>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 9: products_reverse_k<T, 37>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
+    case 10: products_reverse_k<T, 41>(sh, z, br, M, s1c, mask, accumulate, gz, gbr, s); break;
     default: throw std::runtime_error("more levels than the products are built for (10)");
   }
   STL_CUDA(cudaGetLastError());
@@ -1467,7 +1477,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
                                     const uint8_t*, double*, double*, int*, cudaStream_t);                                                                \
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, const uint8_t*, \
-                                    T*, T*, cudaStream_t);                                                                \
+                                    bool, T*, T*, cudaStream_t);                                                                \
   template void mean_var_grad<T>(const T*, const double*, const uint8_t*, const double*, int, i64, T*,           \
                                  cudaStream_t);            \
   template void row_means<T>(const T*, bool, bool, i64, int, double*, double*, cudaStream_t);                     \

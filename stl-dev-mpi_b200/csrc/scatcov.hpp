@@ -94,6 +94,12 @@ class Engine {
   // [B][npix(d)]): the next forward uses them instead of the decimation
   // pyramid of level 0.
   virtual void load_levels(const double* x) = 0;
+  // Averages over k masks (level-0 indicators [k][npix(0)], nonzero: in the
+  // mask) from the next forward on, or over every pixel (k = 0); values,
+  // variances and cotangents are then [B][K][np].
+  virtual void set_masks(const double* w, size_t k) = 0;
+  virtual int nmasks() const = 0;                   // 0: no masks
+  virtual i64 mask_count(int k, int n) const = 0;   // pixels mask k averages at level n
   // Forward sweep on the loaded maps: values [B][np] complex (interleaved),
   // var [B][np] when moments.  Host outputs; the call synchronises.
   virtual void forward(bool moments, double* values, double* var) = 0;

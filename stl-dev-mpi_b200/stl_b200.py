@@ -132,6 +132,25 @@ class Snapshot:
         self.close()
 
 
+def _mask_weights(masks, npix):
+    """[K, npix] float64 indicators of the accepted mask forms (K = 0 for None)."""
+    if masks is None:
+        return np.zeros((0, npix))
+    arr = masks if isinstance(masks, np.ndarray) else None
+    if arr is not None and arr.dtype != object and arr.ndim in (1, 2) and arr.shape[-1] == npix:
+        w = np.array(arr.reshape(-1, npix), dtype=np.float64, order="C")
+    else:
+        w = np.zeros((len(masks), npix))
+        for k, ids in enumerate(masks):
+            ids = np.asarray(ids, dtype=np.int64).ravel()
+            if ids.size and not (0 <= ids.min() and ids.max() < npix):
+                raise ValueError(f"mask {k}: pixel ids out of range")
+            w[k][ids] = 1.0
+    if not np.all(np.isfinite(w)):
+        raise ValueError("mask weights must be finite")
+    return w
+
+
 class NativeEngine:
     """One persistent B200 workspace with an immutable plan, resolution and batch.
 
@@ -163,6 +182,7 @@ class NativeEngine:
         self.plan = info["plan"]
         self.levels = info["levels"]
         self.ncoeff = len(self.plan)
+        self.nmasks = 0
         self._current_key = None
         self._stream = None
         if prepare:
@@ -209,19 +229,38 @@ class NativeEngine:
         with self._mutex:
             self._open()
             x = np.ascontiguousarray(np.concatenate([np.asarray(v, dtype=np.float64).ravel() for v in levels]))
-            values = np.empty((self.batch, self.ncoeff), dtype=np.complex128)
+            values = np.empty(self._shape(), dtype=np.complex128)
             self._current_key = None
             if self._lib.stlp_forward_levels(self._handle, _ptr(x), x.size, _ptr(values.view(np.float64))):
                 raise _error()
             return values
 
-    def native_pixels(self):
+    def set_masks(self, masks):
+        """Averages every coefficient over each of K masks from the next forward
+        on; None restores the whole sky.  masks: [npix] or [K, npix] indicators
+        (nonzero: in the mask) or a sequence of K arrays of NESTED ids
+        (native.py:243-264).  Values, variances and cotangents become
+        [batch, K, ncoeff]."""
+        w = _mask_weights(masks, self.npix)
         with self._mutex:
             self._open()
-            out = np.empty(self.ncoeff, dtype=np.uintp)
+            self._current_key = None
+            if self._lib.stlp_set_masks(self._handle, _ptr(w), w.shape[0]):
+                raise _error()
+            self.nmasks = w.shape[0]
+
+    def _shape(self):
+        return (self.batch, self.nmasks, self.ncoeff) if self.nmasks else (self.batch, self.ncoeff)
+
+    def native_pixels(self):
+        """Pixels each coefficient averages: [K, ncoeff] with masks, else [ncoeff]."""
+        with self._mutex:
+            self._open()
+            out = np.empty((max(self.nmasks, 1), self.ncoeff), dtype=np.uintp)
             if self._lib.stlp_native_pixels(self._handle, out.ctypes.data_as(_SIZE)):
                 raise _error()
-            return out.astype(np.int64)
+            out = out.astype(np.int64)
+            return out if self.nmasks else out[0]
 
     def close(self):
         if getattr(self, "_handle", None):
@@ -249,8 +288,8 @@ class NativeEngine:
                 raise ValueError(f"expected maps {(self.batch, self.npix)}, got {x.shape}")
             if not np.isfinite(x).all():
                 raise ValueError("input map contains non-finite values")
-            values = np.empty((self.batch, self.ncoeff), dtype=np.complex128)
-            var = np.empty((self.batch, self.ncoeff) if moments else (self.batch, 0))
+            values = np.empty(self._shape(), dtype=np.complex128)
+            var = np.empty(self._shape() if moments else (self.batch, 0))
             self._current_key = None
             if self._lib.stlp_forward(self._handle, _ptr(x), x.size, *key, bool(moments),
                                       _ptr(values.view(np.float64)), _ptr(var)):
@@ -260,10 +299,10 @@ class NativeEngine:
 
     def _cotangent(self, cotangents):
         c = np.ascontiguousarray(cotangents, dtype=np.complex128)
-        if c.shape == (self.ncoeff,) and self.batch == 1:
+        if c.shape == self._shape()[1:] and self.batch == 1:
             c = c[None]
-        if c.shape != (self.batch, self.ncoeff):
-            raise ValueError(f"expected cotangents {(self.batch, self.ncoeff)}, got {c.shape}")
+        if c.shape != self._shape():
+            raise ValueError(f"expected cotangents {self._shape()}, got {c.shape}")
         if not np.isfinite(c).all():
             raise ValueError("non-finite coefficient cotangent")
         return c
@@ -322,8 +361,8 @@ class NativeEngine:
                 raise ValueError("forward_tensor needs a float32/float64 CUDA tensor")
             x = x.detach().reshape(self.batch, self.npix).contiguous()
             self._bind_stream(torch)
-            values = np.empty((self.batch, self.ncoeff), dtype=np.complex128)
-            var = np.empty((self.batch, self.ncoeff) if moments else (self.batch, 0))
+            values = np.empty(self._shape(), dtype=np.complex128)
+            var = np.empty(self._shape() if moments else (self.batch, 0))
             self._current_key = None
             if self._lib.stlp_forward_device(self._handle, x.data_ptr(), x.numel(), int(x.dtype == torch.float32),
                                              *key, bool(moments), _ptr(values.view(np.float64)), _ptr(var)):

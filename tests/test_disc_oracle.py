@@ -56,3 +56,38 @@ def test_disc_gradient_matches_finite_differences(core):
         fd = (f(x + h * d) - f(x - h * d)) / (2 * h)
         an = float(g @ d)
         assert abs(fd - an) <= 1e-6 * max(abs(an), 1.0)
+
+
+def test_masked_oracle_equals_full_sky_discs_with_the_mask_as_core():
+    """K masks at once against one whole-sky disc per mask whose core is the
+    mask (crates/stl-core/tests/mask.rs:38-97): values, variances and the
+    summed map cotangent."""
+    nside, J, B = 16, 3, 2
+    npix = 12 * nside * nside
+    theta = O.centres(nside, np.arange(npix))[3]
+    sets = [np.arange(npix)] + [np.nonzero(np.abs(np.cos(theta)) > np.sin(np.radians(b)))[0] for b in (20.0, 45.0)]
+    w = np.zeros((len(sets), npix))
+    for k, s in enumerate(sets):
+        w[k, s] = 1.0
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1, 1, (B, npix))
+    o = O.OracleEngine(nside, J, batch=B)
+    o.set_masks(w)
+    v, var = o.forward(x, moments=True)
+    cot = rng.uniform(-1, 1, v.shape) + 1j * rng.uniform(-1, 1, v.shape)
+    g = o.vjp(cot)
+    m = D.DiscModel(J)
+    g_ref = np.zeros_like(x)
+    for k, s in enumerate(sets):
+        disc = D.Disc(nside, J, [0.0, 0.0, 1.0], np.pi)
+        core, cc = [], s
+        for n in range(J):
+            core.append(np.searchsorted(disc.ids[n], cc))
+            cc = np.unique(cc >> 2)
+        disc.core = core
+        for b in range(B):
+            vr, varr = m.forward(disc, x[b], moments=True)
+            assert close_ratio(v[b, k], vr, 1e-11, 1e-10) <= 1.0
+            assert close_ratio(var[b, k], varr, 1e-11, 1e-10) <= 1.0
+            g_ref[b] += m.reverse(disc, cot[b, k])
+    assert np.max(np.abs(g - g_ref)) <= 1e-10 * np.max(np.abs(g_ref))
