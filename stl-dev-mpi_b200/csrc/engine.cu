@@ -363,7 +363,7 @@ class EngineImpl final : public Engine {
     for (int n = 0; n < levels_; ++n) {
       i64 N = npix(n);
       const size_t e = esz(n);
-      X_[n].alloc(e * B * N);
+      X_[n].alloc(e * B * N + 16);  // padded: the products stage their maps in 16-byte units
       Z_[n].alloc(e * 2 * B * L * N);
       Mod_[n].alloc(e * B * (n + 1) * L * N);
       Br_[n].alloc(e * 2 * B * (n + 1) * L * L * N);

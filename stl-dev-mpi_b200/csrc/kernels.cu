@@ -15,6 +15,7 @@
 // reduction has a fixed order (no floating-point atomics): results are
 // bit-reproducible run to run.
 #include <algorithm>
+#include <numeric>
 #include <cstdio>
 
 #include "engine.cuh"
@@ -717,10 +718,13 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     d1 = item - nBB;
   }
   const int l3 = lane & 3, l1 = (lane >> 2) & 3, hx = lane >> 4, q8 = lane >> 2;
-  // stage s: branch rows [PC][B][K1][L], then z [PC][B][L]
+  // stage s: branch rows [PC][B][K1][L], z [PC][B][L], then at level 0 the
+  // maps [PC][B] (PC B sizeof(T) and the range starts are multiples of 16
+  // bytes there)
   const size_t br_px = (size_t)B * K1 * L, z_px = (size_t)B * L;  // T2 per pixel
-  const size_t stage_t2 = (size_t)PC * (br_px + z_px);
-  T2* stage0 = reinterpret_cast<T2*>(smem);
+  const size_t x_bytes = x0 ? (size_t)PC * B * sizeof(T) : 0;
+  const size_t stage_bytes = (size_t)PC * (br_px + z_px) * sizeof(T2) + x_bytes;
+  unsigned char* stage0 = smem;
   const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
   const int nchunks = P1 > P0 ? (int)((P1 - P0 + PC - 1) / PC) : 0;
   const T2* brv = reinterpret_cast<const T2*>(br);
@@ -732,16 +736,22 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  // the map copy rounds up to 16 bytes: its buffer is padded
+  auto round16 = [](unsigned n) { return (n + 15u) & ~15u; };
   auto issue = [&](int c) {
     const int st = c % kProdStages;
     const i64 pc = P0 + (i64)c * PC;
     const int np = (int)min((i64)PC, P1 - pc);
-    T2* sb = stage0 + st * stage_t2;
+    unsigned char* base = stage0 + st * stage_bytes;
+    T2* sb = reinterpret_cast<T2*>(base);
     T2* sz = sb + (size_t)PC * br_px;
+    unsigned char* sx = reinterpret_cast<unsigned char*>(sz + (size_t)PC * z_px);
     const unsigned nb = (unsigned)(np * br_px * sizeof(T2)), nz = (unsigned)(np * z_px * sizeof(T2));
-    mbar_expect_tx(&bar[st], nb + nz);
+    const unsigned nx = x0 ? round16((unsigned)(np * B * sizeof(T))) : 0u;
+    mbar_expect_tx(&bar[st], nb + nz + nx);
     bulk_g2s(sb, brv + pc * br_px, nb, &bar[st]);
     bulk_g2s(sz, zv + pc * z_px, nz, &bar[st]);
+    if (x0) bulk_g2s(sx, x0 + pc * B, nx, &bar[st]);
   };
   if (threadIdx.x == 0)
     for (int c = 0; c < min(nchunks, kProdStages); ++c) issue(c);
@@ -758,8 +768,9 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     if (fail) break;
     const i64 pc = P0 + (i64)c * PC;
     const int np = (int)min((i64)PC, P1 - pc);
-    const T2* sb = stage0 + st * stage_t2;
+    const T2* sb = reinterpret_cast<const T2*>(stage0 + st * stage_bytes);
     const T2* sz = sb + (size_t)PC * br_px;
+    const T* sx = reinterpret_cast<const T*>(sz + (size_t)PC * z_px);
     if (active) {
       if (kind == 0) {
         const int ra = (d1 * 4 + l1) * L + l3, rb = (d2 * 4 + 2 * hx) * L + l3;
@@ -794,13 +805,13 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
           const int j = 8 * it + q8;
           if (j < np && (!mask || mask[pc + j])) {
             const T2 zz = sz[((size_t)j * B + b) * L + l3];
-            const double m = hypot((double)zz.x, (double)zz.y);
-            const double m2 = m * m;
-            acc[0] += m;
-            acc[1] += m2;
-            acc[2] += m2 * m2;
+            const T m = hypot(zz.x, zz.y);
+            const T m2 = m * m;
+            f[0] += m;
+            f[1] += m2;
+            f[2] = fma(m2, m2, f[2]);
             if (x0 && l3 == 0) {
-              const double xv = x0c[b] + (double)x0[(pc + j) * B + b];
+              const double xv = x0c[b] + (double)sx[(size_t)j * B + b];
               const double x2 = xv * xv;
               acc[3] += xv;
               acc[4] += x2;
@@ -1343,15 +1354,18 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
       for (int rp = 0; rp < reps[zc][k]; ++rp)
         sh.roles[(size_t)zc * W + w++] = chunk_roles[zc][k] | (rp << 16) | (reps[zc][k] << 24);
   }
-  const size_t px_bytes = (size_t)B * sh.K * L * 2 * elem;
-  if (px_bytes > (size_t)kProdStageBytes) throw std::runtime_error("a pixel's operands exceed a products stage");
-  sh.px_chunk = (int)(kProdStageBytes / px_bytes);
+  // per pixel: operands and, at level 0, the maps; there the chunks and
+  // ranges are whole 16-byte units of the maps [N][B]
+  const size_t px_bytes = (size_t)B * sh.K * L * 2 * elem + (sh.level0 ? (size_t)B * elem : 0);
+  const int align = sh.level0 ? 16 / (int)std::gcd((size_t)16, (size_t)B * elem) : 1;
+  sh.px_chunk = (int)(kProdStageBytes / px_bytes) / align * align;
+  if (sh.px_chunk < 1) throw std::runtime_error("a pixel's operands exceed a products stage");
   // one CTA per SM over (pixel ranges, role chunks); ranges of at least 4
   // pixel chunks
   const i64 want = std::max<i64>(1, (i64)148 / sh.item_chunks);
   const i64 most = std::max<i64>(1, N / (4 * (i64)sh.px_chunk));
   sh.blocks = (int)std::max<i64>(1, std::min(want, most));
-  sh.chunk = (N + sh.blocks - 1) / sh.blocks;
+  sh.chunk = ((N + sh.blocks - 1) / sh.blocks + align - 1) / align * align;
   sh.smem = std::max((size_t)kProdStages * sh.px_chunk * px_bytes, (size_t)W * 32 * 6 * sizeof(double));
   return sh;
 }
