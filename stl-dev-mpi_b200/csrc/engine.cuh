@@ -109,9 +109,16 @@ struct ConvOp {
   int ncs = 0;               // stride of the tile cell lists: most cells of a tile + 1
   int max_tile_cells = 0;
   bool adj_tiles = false;    // tables built (every tile within kAdjCells cells)
+  // Coloured layout: within a tile, slot k of every row holds its entry of
+  // colour k of an edge colouring of the tile's (row, cell) entries, so no
+  // two rows of a tile read one cell in the same slot; padding slots have
+  // zero coefficients and tile cell ncells (none).  The adjoint then adds
+  // every product straight into its cell's sums, slot by slot; the
+  // transposed table and the entry lists are not built.
+  bool colored = false;
   DevMem tile_cells;         // int32 [n_tiles][kAdjCells]
   DevMem tile_ncells;        // int32 [n_tiles]
-  DevMem tile_slots;         // int32 [n_tiles]: most slots a row of the tile uses (later slots are zero)
+  DevMem tile_slots;         // int32 [n_tiles]: slots the tile's rows use (later slots are zero)
   DevMem lcell;              // uint16 [S][n_rep]: tile cell of every (slot, row) (build only)
   DevMem lcell_t;            // uint16 [n_tiles][nch 4][kAdjTile]: the same, tile-major, slots padded to 4
   DevMem tile_ent;           // uint16 [n_tiles][S kAdjTile]: slot % kAdjSC << 8 | row
@@ -183,10 +190,11 @@ template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
                   cudaStream_t s, int* err = nullptr, const double* rc = nullptr);
 //  With scratch, operators with tile tables use the row-centric two-phase
-//  adjoint; otherwise the transposed gather.
+//  adjoint (in FP32 with an error flag: its staged form, whose bounded waits
+//  on the bulk copies set *err on timeout); otherwise the transposed gather.
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
-                  const AdjScratch* scr = nullptr);
+                  const AdjScratch* scr = nullptr, int* err = nullptr);
 //    Input and output types may differ (FP32 and FP64 levels); the sums are
 //    in the operator's type.
 template <typename Tin, typename Tout>

@@ -351,6 +351,160 @@ __global__ void k_rowsum(const T* coef, int S, i64 n_rep, T* out) {
   for (int j = 0; j < 8; ++j) out[u * 8 + j] = (T)a[j];
 }
 
+// Edge colouring of a tile's (row, tile cell) entries with D colours, D the
+// largest degree of a row or of a cell in the tile: a bipartite graph needs
+// no more (Konig's line colouring theorem).  The entries are coloured in
+// (row, slot) order; when the colour a free at the row is taken at the cell,
+// the path from the cell alternating a and b (a colour free at the cell) has
+// its two colours swapped, which frees a at the cell and cannot reach the
+// row (rows are entered on a-edges and a is free at the row).  Every colour
+// class is then a matching -- no two rows of the tile read one cell in the
+// same colour -- and the colouring is deterministic.  col[s][u] gets the
+// colour of slot s of row u; tile_d the tile's D (above kColMax: *fail).
+constexpr int kColMax = 64;
+
+__global__ void k_color_tiles(const uint16_t* lcell, const int* counts, int S, i64 n_rep, const int32_t* tile_nc,
+                              uint8_t* col, int32_t* tile_d, int* fail) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  uint64_t* row_used = reinterpret_cast<uint64_t*>(sm);                      // [kAdjTile]
+  uint64_t* cell_used = row_used + kAdjTile;                                 // [kAdjCells]
+  int* cdeg = reinterpret_cast<int*>(cell_used + kAdjCells);                 // [kAdjCells]
+  uint16_t* row_at = reinterpret_cast<uint16_t*>(cdeg + kAdjCells);          // [kAdjTile][kColMax]: cell
+  uint16_t* path = row_at + kAdjTile * kColMax;                              // [kAdjTile + kAdjCells + 2]
+  uint16_t* lc = path + (kAdjTile + kAdjCells + 2);                          // [S][kAdjTile]
+  uint8_t* cell_at = reinterpret_cast<uint8_t*>(lc + (size_t)S * kAdjTile);  // [kAdjCells][kColMax]: row
+  const int tile = blockIdx.x, lane = threadIdx.x;
+  const i64 u0 = (i64)tile * kAdjTile;
+  const int rows = (int)min((i64)kAdjTile, n_rep - u0);
+  const int nc = min(tile_nc[tile], kAdjCells);
+  for (int i = lane; i < kAdjCells; i += 32) { cell_used[i] = 0; cdeg[i] = 0; }
+  for (int i = lane; i < kAdjTile; i += 32) row_used[i] = 0;
+  for (int i = lane; i < S * kAdjTile; i += 32) {
+    const int sl = i / kAdjTile, r = i % kAdjTile;
+    lc[i] = r < rows ? lcell[(i64)sl * n_rep + u0 + r] : (uint16_t)0;
+  }
+  __syncwarp();
+  int dmax = 0;
+  for (int r = lane; r < rows; r += 32) {
+    const int cnt = counts[u0 + r];
+    dmax = max(dmax, cnt);
+    for (int sl = 0; sl < cnt; ++sl) atomicAdd(&cdeg[lc[sl * kAdjTile + r]], 1);
+  }
+  __syncwarp();
+  for (int c = lane; c < nc; c += 32) dmax = max(dmax, cdeg[c]);
+  for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+  if (lane == 0) tile_d[tile] = dmax;
+  if (dmax > kColMax) {
+    if (lane == 0) atomicExch(fail, 1);
+    return;
+  }
+  // (every walk and colour is checked against its bound: an inconsistent
+  // state ends the colouring with *fail set instead of running on)
+  int bad = 0;
+  if (lane == 0) {
+    for (int r = 0; r < rows && !bad; ++r) {
+      const int cnt = counts[u0 + r];
+      for (int sl = 0; sl < cnt && !bad; ++sl) {
+        const int c = lc[sl * kAdjTile + r];
+        const int a = __ffsll((long long)~row_used[r]) - 1;
+        if (c >= nc || a < 0 || a >= dmax) { bad = 1; break; }
+        if ((cell_used[c] >> a) & 1ull) {
+          const int b = __ffsll((long long)~cell_used[c]) - 1;
+          if (b < 0 || b >= dmax) { bad = 1; break; }
+          // path[0] = c, then row, cell, ...; edge i colour a (i even) or b
+          int len = 1, v = c, k = a;
+          bool at_cell = true;
+          path[0] = (uint16_t)c;
+          while (true) {
+            if (len > kAdjTile + kAdjCells) { bad = 1; break; }
+            int w;
+            if (at_cell) {
+              if (!((cell_used[v] >> k) & 1ull)) break;
+              w = cell_at[v * kColMax + k];
+            } else {
+              if (!((row_used[v] >> k) & 1ull)) break;
+              w = row_at[v * kColMax + k];
+            }
+            path[len++] = (uint16_t)w;
+            v = w;
+            at_cell = !at_cell;
+            k = k == a ? b : a;
+          }
+          if (bad) break;
+          for (int i = 0; i + 1 < len; ++i) {
+            const int kc = (i & 1) ? b : a;
+            const int cv = (i & 1) ? path[i + 1] : path[i], rv = (i & 1) ? path[i] : path[i + 1];
+            cell_used[cv] &= ~(1ull << kc);
+            row_used[rv] &= ~(1ull << kc);
+          }
+          for (int i = 0; i + 1 < len; ++i) {
+            const int kn = (i & 1) ? a : b;
+            const int cv = (i & 1) ? path[i + 1] : path[i], rv = (i & 1) ? path[i] : path[i + 1];
+            cell_used[cv] |= 1ull << kn;
+            row_used[rv] |= 1ull << kn;
+            cell_at[cv * kColMax + kn] = (uint8_t)rv;
+            row_at[rv * kColMax + kn] = (uint16_t)cv;
+          }
+        }
+        row_used[r] |= 1ull << a;
+        cell_used[c] |= 1ull << a;
+        row_at[r * kColMax + a] = (uint16_t)c;
+        cell_at[c * kColMax + a] = (uint8_t)r;
+      }
+    }
+    if (bad) atomicExch(fail, 1);
+  }
+  bad = __shfl_sync(0xffffffffu, bad, 0);
+  if (bad) return;
+  __syncwarp();
+  // the colour of every entry: the row's cells are distinct
+  for (int r = lane; r < rows; r += 32) {
+    const int cnt = counts[u0 + r];
+    uint64_t m = row_used[r];
+    while (m) {
+      const int k = __ffsll((long long)m) - 1;
+      m &= m - 1;
+      const int c = row_at[r * kColMax + k];
+      for (int sl = 0; sl < cnt; ++sl)
+        if (lc[sl * kAdjTile + r] == c) {
+          col[(i64)sl * n_rep + u0 + r] = (uint8_t)k;
+          break;
+        }
+    }
+  }
+}
+
+size_t color_smem(int S) {
+  return sizeof(uint64_t) * (kAdjTile + kAdjCells) + sizeof(int) * kAdjCells +
+         sizeof(uint16_t) * ((size_t)kAdjTile * kColMax + kAdjTile + kAdjCells + 2 + (size_t)S * kAdjTile) +
+         (size_t)kAdjCells * kColMax;
+}
+
+// Coloured layout: slot k of row u holds its entry of colour k, or padding
+// (zero coefficients, the row's first cell, tile cell nc = none).
+template <typename T>
+__global__ void k_color_apply(const int32_t* cell, const T* coef, const uint16_t* lcell, const uint8_t* col,
+                              const int* counts, int S, int S2, i64 n_rep, const int32_t* tile_nc, int32_t* cell2,
+                              T* coef2, uint16_t* lcell2) {
+  const i64 u = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n_rep) return;
+  const uint16_t none = (uint16_t)tile_nc[u / kAdjTile];
+  const int32_t c0 = cell[u];
+  for (int k = 0; k < S2; ++k) {
+    const i64 e = (i64)k * n_rep + u;
+    cell2[e] = c0;
+    lcell2[e] = none;
+    for (int j = 0; j < 8; ++j) coef2[e * 8 + j] = (T)0;
+  }
+  const int cnt = counts[u];
+  for (int sl = 0; sl < cnt; ++sl) {
+    const i64 e = (i64)sl * n_rep + u, e2 = (i64)col[e] * n_rep + u;
+    cell2[e2] = cell[e];
+    lcell2[e2] = lcell[e];
+    for (int j = 0; j < 8; ++j) coef2[e2 * 8 + j] = coef[e * 8 + j];
+  }
+}
+
 // lcell [S][n_rep] -> tile-major [n_tiles][nch * 4][kAdjTile] (slots padded
 // to a multiple of 4 with index 0: their coefficients are never read)
 __global__ void k_lcell_tiles(const uint16_t* lcell, int S, i64 n_rep, int S4, i64 n_tiles, uint16_t* out) {
@@ -675,50 +829,22 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   k_fold<T><<<nblocks(a.n_rows, TB), TB, 0, s>>>(a, counts.as<int>(), op.S, op.cell.as<int32_t>(), op.coef.as<T>(),
                                                 flag.as<int>());
   STL_CUDA(cudaGetLastError());
-  // transposed gather table over the stored cells: entries (u, s, j)
-  int sbits = 1;
-  while ((1 << sbits) < op.S) ++sbits;
-  op.tshift = sbits + 2;
-  if ((uint64_t)std::max<i64>(a.n_rows - 1, 0) >= ((uint64_t)1 << (32 - op.tshift)) - 1)
-    throw std::runtime_error("level too large for the 32-bit transposed table");
   const i64 n_cells = sym ? a.n_in / 4 : a.n_in;  // stored cells == stored rows on the full sky
   if (sym && n_cells != a.n_rows) throw std::runtime_error("symmetric operator needs rows == cells");
-  DevMem tcount(sizeof(int) * n_cells), tfill(sizeof(int) * n_cells);
-  STL_CUDA(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
-  STL_CUDA(cudaMemsetAsync(tfill.p, 0, tfill.bytes, s));
-  k_conv_tcount<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, a.sym,
-                                                       a.sym_o2, tcount.as<int>());
-  STL_CUDA(cudaGetLastError());
-  op.ST = std::max(1, device_max(tcount.as<int>(), n_cells, s));
-  if (!sym && n_cells != a.n_rows) {
-    // partial grids keep the transposed table over the grid cells
-    throw std::runtime_error("rows and grid must coincide");
-  }
-  op.tent.alloc(sizeof(uint32_t) * op.ST * n_cells);
-  k_conv_tfill<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, a.sym,
-                                                      a.sym_o2, op.tshift, tfill.as<int>(), op.tent.as<uint32_t>());
-  STL_CUDA(cudaGetLastError());
-  k_tsort<<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), tcount.as<int>(), n_cells, op.ST);
-  STL_CUDA(cudaGetLastError());
-  op.coefT.alloc(sizeof(T) * 8 * op.ST * n_cells);
-  k_conv_coefT<T><<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), op.coef.as<T>(), n_cells, op.ST,
-                                                        op.tshift, op.coefT.as<T>());
-  STL_CUDA(cudaGetLastError());
-  op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
-  k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
-  STL_CUDA(cudaGetLastError());
-  // row-centric adjoint tiles
+  if (!sym && n_cells != a.n_rows) throw std::runtime_error("rows and grid must coincide");
+  // row-centric adjoint tiles (full sky): the distinct cells of every tile
+  // of kAdjTile stored rows, then the edge colouring of its entries
   op.adj_tiles = false;
-  if (op.S > 128) return;  // the tile sort holds 128 slots per row
-  op.n_tiles = (a.n_rows + kAdjTile - 1) / kAdjTile;
-  op.tile_slots.alloc(sizeof(int32_t) * op.n_tiles);
-  k_tile_slots<<<nblocks(op.n_tiles, 256), 256, 0, s>>>(counts.as<int>(), a.n_rows, op.n_tiles,
-                                                        op.tile_slots.as<int32_t>());
-  STL_CUDA(cudaGetLastError());
-  op.tile_cells.alloc(sizeof(int32_t) * kAdjCells * op.n_tiles);
-  op.tile_ncells.alloc(sizeof(int32_t) * op.n_tiles);
-  op.lcell.alloc(sizeof(uint16_t) * op.S * a.n_rows);
-  {
+  op.colored = false;
+  if (sym && op.S <= 128) {  // the tile sort holds 128 slots per row
+    op.n_tiles = (a.n_rows + kAdjTile - 1) / kAdjTile;
+    op.tile_slots.alloc(sizeof(int32_t) * op.n_tiles);
+    k_tile_slots<<<nblocks(op.n_tiles, 256), 256, 0, s>>>(counts.as<int>(), a.n_rows, op.n_tiles,
+                                                          op.tile_slots.as<int32_t>());
+    STL_CUDA(cudaGetLastError());
+    op.tile_cells.alloc(sizeof(int32_t) * kAdjCells * op.n_tiles);
+    op.tile_ncells.alloc(sizeof(int32_t) * op.n_tiles);
+    op.lcell.alloc(sizeof(uint16_t) * op.S * a.n_rows);
     int P2 = 1;
     while (P2 < op.S * kAdjTile) P2 <<= 1;
     const size_t smem = sizeof(int32_t) * ((size_t)P2 + kAdjCells + 256);
@@ -735,26 +861,82 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
     STL_CUDA(cudaStreamSynchronize(s));
     op.max_tile_cells = 0;
     for (int32_t v : nc) op.max_tile_cells = std::max(op.max_tile_cells, (int)v);
+    if ((uint64_t)op.n_tiles >= (1ull << 20)) op.adj_tiles = false;
+    if (op.adj_tiles && op.max_tile_cells < kAdjCells) {
+      // every colour a matching: the coloured layout replaces the slots
+      DevMem col((size_t)op.S * a.n_rows), tile_d(sizeof(int32_t) * op.n_tiles);
+      const size_t csm = color_smem(op.S);
+      STL_CUDA(cudaFuncSetAttribute(k_color_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+      STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+      k_color_tiles<<<(unsigned)op.n_tiles, 32, csm, s>>>(op.lcell.as<uint16_t>(), counts.as<int>(), op.S, a.n_rows,
+                                                          op.tile_ncells.as<int32_t>(), col.as<uint8_t>(),
+                                                          tile_d.as<int32_t>(), flag.as<int>());
+      STL_CUDA(cudaGetLastError());
+      if (!read_flag(flag, s)) {
+        const int S2 = std::max(1, device_max(tile_d.as<int32_t>(), op.n_tiles, s));
+        DevMem cell2(sizeof(int32_t) * S2 * a.n_rows), coef2(sizeof(T) * 8 * S2 * a.n_rows),
+            lcell2(sizeof(uint16_t) * S2 * a.n_rows);
+        k_color_apply<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(
+            op.cell.as<int32_t>(), op.coef.as<T>(), op.lcell.as<uint16_t>(), col.as<uint8_t>(), counts.as<int>(),
+            op.S, S2, a.n_rows, op.tile_ncells.as<int32_t>(), cell2.as<int32_t>(), coef2.as<T>(),
+            lcell2.as<uint16_t>());
+        STL_CUDA(cudaGetLastError());
+        STL_CUDA(cudaMemcpyAsync(op.tile_slots.p, tile_d.p, tile_d.bytes, cudaMemcpyDeviceToDevice, s));
+        STL_CUDA(cudaStreamSynchronize(s));
+        op.cell = std::move(cell2);
+        op.coef = std::move(coef2);
+        op.lcell = std::move(lcell2);
+        op.S = S2;
+        op.colored = true;
+      }
+    }
   }
-  if (!op.adj_tiles || (uint64_t)op.n_tiles >= (1ull << 20)) {
-    op.adj_tiles = false;
-    return;
+  op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
+  k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
+  STL_CUDA(cudaGetLastError());
+  if (!op.colored) {
+    // transposed gather table over the stored cells: entries (u, s, j)
+    int sbits = 1;
+    while ((1 << sbits) < op.S) ++sbits;
+    op.tshift = sbits + 2;
+    if ((uint64_t)std::max<i64>(a.n_rows - 1, 0) >= ((uint64_t)1 << (32 - op.tshift)) - 1)
+      throw std::runtime_error("level too large for the 32-bit transposed table");
+    DevMem tcount(sizeof(int) * n_cells), tfill(sizeof(int) * n_cells);
+    STL_CUDA(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
+    STL_CUDA(cudaMemsetAsync(tfill.p, 0, tfill.bytes, s));
+    k_conv_tcount<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, a.sym,
+                                                         a.sym_o2, tcount.as<int>());
+    STL_CUDA(cudaGetLastError());
+    op.ST = std::max(1, device_max(tcount.as<int>(), n_cells, s));
+    op.tent.alloc(sizeof(uint32_t) * op.ST * n_cells);
+    k_conv_tfill<<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.cell.as<int32_t>(), counts.as<int>(), a.n_rows, a.sym,
+                                                        a.sym_o2, op.tshift, tfill.as<int>(), op.tent.as<uint32_t>());
+    STL_CUDA(cudaGetLastError());
+    k_tsort<<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), tcount.as<int>(), n_cells, op.ST);
+    STL_CUDA(cudaGetLastError());
+    op.coefT.alloc(sizeof(T) * 8 * op.ST * n_cells);
+    k_conv_coefT<T><<<nblocks(n_cells, 256), 256, 0, s>>>(op.tent.as<uint32_t>(), op.coef.as<T>(), n_cells, op.ST,
+                                                          op.tshift, op.coefT.as<T>());
+    STL_CUDA(cudaGetLastError());
   }
-  // per tile and slot chunk: the entries of every tile cell
+  if (!op.adj_tiles) return;
   op.nch = (op.S + kAdjSC - 1) / kAdjSC;
   op.ncs = op.max_tile_cells + 1;
-  op.tile_ent.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * op.S * kAdjTile);
-  op.tile_off.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * op.nch * op.ncs);
-  {
-    int P2 = 1;
-    while (P2 < op.S * kAdjTile) P2 <<= 1;
-    const size_t smem = sizeof(uint32_t) * (size_t)P2;
-    if (smem > 48 * 1024)
-      STL_CUDA(cudaFuncSetAttribute(k_adj_csr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_adj_csr<<<(unsigned)op.n_tiles, 256, smem, s>>>(op.cell.as<int32_t>(), op.lcell.as<uint16_t>(), op.S,
-                                                        a.n_rows, P2, op.nch, op.ncs, op.tile_ncells.as<int32_t>(),
-                                                        op.tile_ent.as<uint16_t>(), op.tile_off.as<uint16_t>());
-    STL_CUDA(cudaGetLastError());
+  if (!op.colored) {
+    // per tile and slot chunk: the entries of every tile cell
+    op.tile_ent.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * op.S * kAdjTile);
+    op.tile_off.alloc(sizeof(uint16_t) * (size_t)op.n_tiles * op.nch * op.ncs);
+    {
+      int P2 = 1;
+      while (P2 < op.S * kAdjTile) P2 <<= 1;
+      const size_t smem = sizeof(uint32_t) * (size_t)P2;
+      if (smem > 48 * 1024)
+        STL_CUDA(cudaFuncSetAttribute(k_adj_csr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_adj_csr<<<(unsigned)op.n_tiles, 256, smem, s>>>(op.cell.as<int32_t>(), op.lcell.as<uint16_t>(), op.S,
+                                                          a.n_rows, P2, op.nch, op.ncs, op.tile_ncells.as<int32_t>(),
+                                                          op.tile_ent.as<uint16_t>(), op.tile_off.as<uint16_t>());
+      STL_CUDA(cudaGetLastError());
+    }
   }
   {
     const int S4 = ((op.S + 3) / 4) * 4;

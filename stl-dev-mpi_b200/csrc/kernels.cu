@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
   // stage: coef [SC][kAdjTile][8] T, then indices [SC][kAdjTile] uint16
   constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
   constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
-  T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][nc][RB]
+  T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][nc + 1][RB]: cell nc (padding) is zero
   const int tile = blockIdx.y, tid = threadIdx.x;
   const int k = tid & 3, row = tid >> 2;
   const int r0 = blockIdx.x * RB;
@@ -291,11 +291,13 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
     if (nch > 1) issue(1);
   }
   const int32_t* tc = tile_cells + (i64)tile * kAdjCells;
-  for (int i = tid; i < 4 * nc; i += kFwdThreads) {
-    const int kk = i / nc, lc = i - kk * nc;
-    const i64 c = rot_cell(tc[lc], kk, o2);
+  for (int i = tid; i < 4 * (nc + 1); i += kFwdThreads) {
+    const int kk = i / (nc + 1), lc = i - kk * (nc + 1);
     T v[RB];
-    loadR<RB>(x + c * R + r0, v);
+    if (lc < nc) loadR<RB>(x + rot_cell(tc[lc], kk, o2) * R + r0, v);
+    else
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) v[rb] = (T)0;
 #pragma unroll
     for (int rb = 0; rb < RB; ++rb) sx[(size_t)i * RB + rb] = v[rb];
   }
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
   for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[rb][j] = (T)0;
-  const T* sxk = sx + (size_t)k * nc * RB;
+  const T* sxk = sx + (size_t)k * (nc + 1) * RB;
   int c = 0;
   for (; c < nch; ++c) {
     const int st = c & 1;
@@ -555,6 +557,129 @@ __global__ void __launch_bounds__(kAdjTile, 2) k_conv_adj_tiles(
     const int q = i / nc, lc = i - q * nc;
     const int rb = q >> 2, kk = q & 3;
     part[(((i64)tile * 4 + kk) * ncs + lc) * R + r0 + rb] = acc[q * ncs + lc];
+  }
+}
+
+// Coloured adjoint (operators in the coloured layout): a CTA takes a tile
+// of kAdjTile stored rows and RB cotangent rows; thread (row, rotation k), k
+// fastest, keeps the row's cotangents under rotation k in registers.  No two
+// rows of a tile read one cell in the same slot, so per slot every thread
+// adds its RB products into its cell's sums in shared memory ([cell][k][rb])
+// with no two threads on one address, and a barrier separates the slots.
+// The coefficients and tile cells of SC slots arrive by bulk asynchronous
+// copies, two stages deep.  Every cell sums its products in slot order, so
+// the results are bit-reproducible.
+constexpr int kAdjCThreads = 4 * kAdjTile;
+
+template <typename T>
+__host__ __device__ constexpr int adjc_sc() { return sizeof(T) == 4 ? 8 : 4; }
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(kAdjCThreads, 1) k_conv_adj_colored(
+    const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2, int ncs,
+    const int32_t* __restrict__ tile_nc, const T* __restrict__ gy, int R, T* __restrict__ part,
+    const int32_t* __restrict__ tile_slots, int* __restrict__ err) {
+  constexpr int SC = adjc_sc<T>();
+  constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
+  constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int fail;
+  T* acc = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [nc + 1][4][RB]
+  const int tile = blockIdx.y, tid = threadIdx.x;
+  const int k = tid & 3, row = tid >> 2;
+  const int r0 = blockIdx.x * RB;
+  const int nc = tile_nc[tile];
+  const i64 u0 = (i64)tile * kAdjTile;
+  const int rows = (int)min((i64)kAdjTile, n_rep - u0);
+  const int S4 = ((S + 3) / 4) * 4;  // slots per tile in the tile-major cell table
+  const int St = tile_slots[tile];
+  const int nch = (St + SC - 1) / SC;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int c) {
+    const int st = c & 1;
+    unsigned char* base = smem_raw + st * kStage;
+    const int s0 = c * SC, sn = min(SC, St - s0);
+    const int sn4 = min(SC, S4 - s0);  // cell rows are padded to 4 slots
+    const unsigned cb = (unsigned)(rows * 8 * sizeof(T));
+    const unsigned lb = (unsigned)(sn4 * kAdjTile * sizeof(uint16_t));
+    mbar_expect_tx(&bar[st], sn * cb + lb);
+    for (int sl = 0; sl < sn; ++sl)
+      bulk_g2s(base + (size_t)sl * kAdjTile * 8 * sizeof(T), coef + ((i64)(s0 + sl) * n_rep + u0) * 8, cb, &bar[st]);
+    bulk_g2s(base + kStageCoef, lcell_t + ((i64)tile * S4 + s0) * kAdjTile, lb, &bar[st]);
+  };
+  if (tid == 0) {
+    if (nch > 0) issue(0);
+    if (nch > 1) issue(1);
+  }
+  for (int i = tid; i < (nc + 1) * 4 * RB; i += kAdjCThreads) acc[i] = (T)0;
+  // the row's cotangents under rotation k (gauge permutation and
+  // conjugation folded in): every product is a plain 8-term dot; the
+  // permutation is selected without indexing registers by the runtime k
+  T g[RB][8];
+  const bool valid = row < rows, odd = k & 1;
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb) {
+    T t[8];
+    if (valid) load8(gy + (rot_pixel(u0 + row, k, o2) * R + r0 + rb) * 8, t);
+    else
+#pragma unroll
+      for (int q = 0; q < 8; ++q) t[q] = (T)0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int gg = odd ? (q ^ 2) : q;
+      const T re = odd ? t[2 * (q ^ 2)] : t[2 * q];
+      const T im = odd ? t[2 * (q ^ 2) + 1] : t[2 * q + 1];
+      g[rb][2 * q] = re;
+      g[rb][2 * q + 1] = rot_conj(k, gg) ? -im : im;
+    }
+  }
+  int c = 0;
+  for (; c < nch; ++c) {
+    const int st = c & 1;
+    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    __syncthreads();  // the stage (and, first, the zeroed sums) everywhere
+    if (fail) break;
+    const unsigned char* base = smem_raw + st * kStage;
+    const T* cs = reinterpret_cast<const T*>(base);
+    const uint16_t* ls = reinterpret_cast<const uint16_t*>(base + kStageCoef);
+    const int sn = min(SC, St - c * SC);
+    for (int sl = 0; sl < sn; ++sl) {
+      const int lc = ls[sl * kAdjTile + row];
+      if (valid && lc < nc) {
+        T w[8];
+        load8_shared(cs + ((size_t)sl * kAdjTile + row) * 8, w);
+        T* p = acc + ((size_t)lc * 4 + k) * RB;
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) {
+          T a = (T)0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) a = fma(w[q], g[rb][q], a);
+          p[rb] += a;
+        }
+      }
+      __syncthreads();  // the slot's sums are in: the next slot may read them
+    }
+    if (tid == 0 && c + 2 < nch) issue(c + 2);
+  }
+  if (fail) {
+    for (int q = c; q < min(nch, c + 2); ++q) mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  // partials [tile][k][ncs][R]
+  for (int i = tid; i < nc * 4; i += kAdjCThreads) {
+    const int lc = i >> 2, kk = i & 3;
+    T* o = part + (((i64)tile * 4 + kk) * ncs + lc) * R + r0;
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) o[rb] = acc[(size_t)i * RB + rb];
   }
 }
 
@@ -1151,18 +1276,10 @@ size_t adj_tiles_smem(const ConvOp& op) {
          sizeof(uint16_t) * (kAdjSC * kAdjTile + (size_t)op.ncs + 1);
 }
 
+// partials of every tile cell -> gx, k_adj_combine
 template <typename T, int RB>
-void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, const AdjScratch& scr,
-                           cudaStream_t s) {
-  const size_t smem = adj_tiles_smem<T, RB>(op);
-  if (smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(k_conv_adj_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  T* part = static_cast<T*>(scr.part);
-  dim3 grid(R / RB, (unsigned)op.n_tiles);
-  k_conv_adj_tiles<T, RB><<<grid, kAdjTile, smem, s>>>(op.coef.as<T>(), op.S, op.n_rep, op.o2, op.nch, op.ncs,
-                                                       op.tile_ncells.as<int32_t>(), op.tile_ent.as<uint16_t>(),
-                                                       op.tile_off.as<uint16_t>(), gy, R, part,
-                                                       op.tile_slots.as<int32_t>());
+void adj_combine_rb(const ConvOp& op, int R, T* gx, bool accumulate, const AdjScratch& scr, cudaStream_t s) {
+  const T* part = static_cast<const T*>(scr.part);
   const i64 n_cells = op.n_in / op.nk;
   const int chunks = R / RB;
   dim3 b = cta_shape(chunks);
@@ -1173,6 +1290,36 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
   else
     k_adj_combine<T, 1, RB><<<g2, b, 0, s>>>(op.coff.as<i64>(), op.clist.as<uint32_t>(), n_cells, op.o2, op.ncs, part,
                                              R, gx, accumulate ? 1 : 0);
+}
+
+template <typename T, int RB>
+size_t adjc_smem(const ConvOp& op) {
+  return 2 * (size_t)adjc_sc<T>() * kAdjTile * (8 * sizeof(T) + sizeof(uint16_t)) +
+         sizeof(T) * (size_t)op.ncs * 4 * RB;
+}
+
+template <typename T, int RB>
+void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, const AdjScratch& scr,
+                           cudaStream_t s, int* err) {
+  if (op.colored) {
+    if (!err) throw std::runtime_error("the coloured adjoint needs an error flag");
+    const size_t smem = adjc_smem<T, RB>(op);
+    STL_CUDA(cudaFuncSetAttribute(k_conv_adj_colored<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(R / RB, (unsigned)op.n_tiles);
+    k_conv_adj_colored<T, RB><<<grid, kAdjCThreads, smem, s>>>(
+        op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S, op.n_rep, op.o2, op.ncs, op.tile_ncells.as<int32_t>(), gy,
+        R, static_cast<T*>(scr.part), op.tile_slots.as<int32_t>(), err);
+  } else {
+    const size_t smem = adj_tiles_smem<T, RB>(op);
+    if (smem > 48 * 1024)
+      STL_CUDA(cudaFuncSetAttribute(k_conv_adj_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(R / RB, (unsigned)op.n_tiles);
+    k_conv_adj_tiles<T, RB><<<grid, kAdjTile, smem, s>>>(op.coef.as<T>(), op.S, op.n_rep, op.o2, op.nch, op.ncs,
+                                                         op.tile_ncells.as<int32_t>(), op.tile_ent.as<uint16_t>(),
+                                                         op.tile_off.as<uint16_t>(), gy, R,
+                                                         static_cast<T*>(scr.part), op.tile_slots.as<int32_t>());
+  }
+  adj_combine_rb<T, RB>(op, R, gx, accumulate, scr, s);
 }
 
 template <typename T, int NK>
@@ -1218,14 +1365,20 @@ void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x
                              accumulate, s);
 }
 
-inline int adj_rb(size_t elem, int R) { return (elem == 4 && R % 2 == 0) ? 2 : 1; }
+// cotangent rows per CTA: FP32 up to 4 (coloured) or 2; FP64 1 (the
+// coloured kernel's 1024 threads hold 64 registers each)
+inline int adj_rb(const ConvOp& op, size_t elem, int R) {
+  if (elem != 4) return 1;
+  if (op.colored && R % 4 == 0) return 4;
+  return R % 2 == 0 ? 2 : 1;
+}
 
 }  // namespace
 
 template <typename T, int RB>
 size_t fwd_tiles_smem(const ConvOp& op) {
   const size_t stage = (size_t)fwd_sc<T>() * kAdjTile * (8 * sizeof(T) + sizeof(uint16_t));
-  return 2 * stage + sizeof(T) * 4 * (size_t)op.max_tile_cells * RB;
+  return 2 * stage + sizeof(T) * 4 * (size_t)(op.max_tile_cells + 1) * RB;
 }
 
 template <typename T, int RB>
@@ -1266,17 +1419,22 @@ size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R) {
 bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
   if (!scr || !op.adj_tiles || op.nk != 4 || op.n_tiles > 65535) return false;
   if (adjoint_part_bytes(op, elem, R) > scr->capacity) return false;
-  const size_t smem = elem == 4 ? (adj_rb(elem, R) == 2 ? adj_tiles_smem<float, 2>(op) : adj_tiles_smem<float, 1>(op))
+  if (op.colored) return (elem == 4 ? adjc_smem<float, 4>(op) : adjc_smem<double, 1>(op)) <= 227 * 1024;
+  const size_t smem = elem == 4 ? (adj_rb(op, elem, R) == 2 ? adj_tiles_smem<float, 2>(op) : adj_tiles_smem<float, 1>(op))
                                 : adj_tiles_smem<double, 1>(op);
   return smem <= 200 * 1024;
 }
 
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
-                  const AdjScratch* scr) {
+                  const AdjScratch* scr, int* err) {
   if (adjoint_tiles_usable(op, sizeof(T), R, scr)) {
-    if (adj_rb(sizeof(T), R) == 2) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 2 : 1>(op, gy, R, gx, accumulate, *scr, s);
-    else conv_adjoint_tiles_rb<T, 1>(op, gy, R, gx, accumulate, *scr, s);
+    const int rb = adj_rb(op, sizeof(T), R);
+    if (rb == 4) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 4 : 1>(op, gy, R, gx, accumulate, *scr, s, err);
+    else if (rb == 2) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 2 : 1>(op, gy, R, gx, accumulate, *scr, s, err);
+    else conv_adjoint_tiles_rb<T, 1>(op, gy, R, gx, accumulate, *scr, s, err);
+  } else if (op.colored) {
+    throw std::runtime_error("the coloured adjoint needs scratch for its tile partials");
   } else if (op.nk == 4) conv_adjoint_nk<T, 4>(op, gy, R, gx, accumulate, s);
   else conv_adjoint_nk<T, 1>(op, gy, R, gx, accumulate, s);
   STL_CUDA(cudaGetLastError());
@@ -1486,7 +1644,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
 #define INST(T)                                                                                                   \
   template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t, int*,          \
                                 const double*);               \
-  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*);                            \
+  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*, int*);                            \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
                                     const uint8_t*, double*, double*, int*, cudaStream_t);                                                                \
