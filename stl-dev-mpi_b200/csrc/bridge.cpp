@@ -186,6 +186,11 @@ char* stlp_info(StlpHandle* h) {
     js << "], \"mean_cells_per_row\": [";
     auto ms = e.mean_slots();
     for (size_t i = 0; i < ms.size(); ++i) js << (i ? ", " : "") << ms[i];
+    js << "], \"operators\": [";
+    auto ol = e.operator_layout();
+    for (size_t i = 0; i < ol.size(); ++i)
+      js << (i ? ", " : "") << "{\"slots\": " << ol[i][0] << ", \"tile_cells\": " << ol[i][1]
+         << ", \"coloured\": " << (ol[i][2] ? "true" : "false") << "}";
     js << "]";
     js << ", \"plan\": [";
     const auto& plan = e.plan();

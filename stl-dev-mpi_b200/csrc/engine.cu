@@ -540,7 +540,7 @@ class EngineImpl final : public Engine {
         });
       });
     for (int n = 0; n < levels_; ++n)
-      typed(n, [&](auto t) { forward_level<typename decltype(t)::type>(n); });
+      typed(n, [&](auto t) { forward_level<typename decltype(t)::type>(n, moments); });
     STL_CUDA(cudaMemcpyAsync(h_sums_.data(), sums_.p, h_sums_.size() * 8, cudaMemcpyDeviceToHost, s));
     int err = 0;
     STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -557,7 +557,7 @@ class EngineImpl final : public Engine {
   }
 
   template <typename U>
-  void forward_level(int n) {
+  void forward_level(int n, bool moments) {
     const int L = opt_.L, B = opt_.B;
     cudaStream_t s = stream_;
     const i64 N = npix(n);
@@ -594,7 +594,8 @@ class EngineImpl final : public Engine {
                    [&] {
                      products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
                                          xc_.as<double>(), mask(k, n), partials_.as<double>(),
-                                         sums_.as<double>() + k * total_sums_ + sum_off_[n], err_.as<int>(), s);
+                                         sums_.as<double>() + k * total_sums_ + sum_off_[n], err_.as<int>(), s,
+                                         moments);
                    });
   }
 
@@ -632,6 +633,11 @@ class EngineImpl final : public Engine {
   std::vector<double> mean_slots() const override {
     std::vector<double> v;
     for (const auto& c : conv_) v.push_back(c.mean_slots);
+    return v;
+  }
+  std::vector<std::array<int, 3>> operator_layout() const override {
+    std::vector<std::array<int, 3>> v;
+    for (const auto& c : conv_) v.push_back({c.S, c.max_tile_cells, c.colored ? 1 : 0});
     return v;
   }
 

@@ -133,7 +133,7 @@ struct ConvOp {
            lcell_t.bytes + tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
   }
 };
-constexpr int kAdjTile = 256;    // stored rows per adjoint tile
+constexpr int kAdjTile = 128;    // stored rows per tile of the tiled forward and adjoint
 constexpr int kAdjCells = 1024;  // cells a tile may read
 constexpr int kAdjSC = 8;        // slots per chunk of the two-phase adjoint
 
@@ -228,10 +228,11 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem);
 // sums [B][L][slots] (FP64)
 // *err becomes nonzero when a wait on a staged copy timed out.  x0 holds
 // the level-0 maps as deviations from x0c [B].
-// mask (or null): 1 on the pixels the sums cover.
+// mask (or null): 1 on the pixels the sums cover.  moments: also the
+// second sums the coefficient variances need (otherwise zero).
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
-                      const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s);
+                      const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s, bool moments);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
 // accumulate: add to gz / gbr (on the mask's pixels) instead of writing them
 template <typename T>

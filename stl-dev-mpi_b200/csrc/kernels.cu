@@ -244,7 +244,7 @@ template <typename T>
 __host__ __device__ constexpr int fwd_sc() { return sizeof(T) == 4 ? 8 : 4; }
 
 template <typename T, int RB>
-__global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
+__global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2,
     const int32_t* __restrict__ tile_cells, const int32_t* __restrict__ tile_nc, const T* __restrict__ x, int R,
     T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err,
@@ -257,9 +257,10 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_conv_fwd_tiles(
   constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
   constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
   T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][nc + 1][RB]: cell nc (padding) is zero
-  const int tile = blockIdx.y, tid = threadIdx.x;
+  const int ngroups = R / RB;  // CTAs of a tile: consecutive, so its coefficients stay in L2
+  const int tile = blockIdx.x / ngroups, tid = threadIdx.x;
   const int k = tid & 3, row = tid >> 2;
-  const int r0 = blockIdx.x * RB;
+  const int r0 = (blockIdx.x % ngroups) * RB;
   const int nc = tile_nc[tile];
   const i64 u0 = (i64)tile * kAdjTile;
   const int rows = (int)min((i64)kAdjTile, n_rep - u0);
@@ -480,8 +481,9 @@ __global__ void __launch_bounds__(kAdjTile, 2) k_conv_adj_tiles(
   T* acc = P + 4 * RB * kAdjPlane;                       // [RB][4][ncs]
   uint16_t* ent = reinterpret_cast<uint16_t*>(acc + 4 * RB * ncs);  // [kAdjSC kAdjTile]
   uint16_t* off = ent + kAdjSC * kAdjTile;               // [ncs + 1]
-  const int tile = blockIdx.y, tid = threadIdx.x;
-  const int r0 = blockIdx.x * RB;
+  const int ngroups = R / RB;
+  const int tile = blockIdx.x / ngroups, tid = threadIdx.x;
+  const int r0 = (blockIdx.x % ngroups) * RB;
   const int nc = tile_nc[tile];
   const i64 u = (i64)tile * kAdjTile + tid;
   const bool valid = u < n_rep;
@@ -575,7 +577,7 @@ template <typename T>
 __host__ __device__ constexpr int adjc_sc() { return sizeof(T) == 4 ? 8 : 4; }
 
 template <typename T, int RB>
-__global__ void __launch_bounds__(kAdjCThreads, 1) k_conv_adj_colored(
+__global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
     const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2, int ncs,
     const int32_t* __restrict__ tile_nc, const T* __restrict__ gy, int R, T* __restrict__ part,
     const int32_t* __restrict__ tile_slots, int* __restrict__ err) {
@@ -586,9 +588,10 @@ __global__ void __launch_bounds__(kAdjCThreads, 1) k_conv_adj_colored(
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int fail;
   T* acc = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [nc + 1][4][RB]
-  const int tile = blockIdx.y, tid = threadIdx.x;
+  const int ngroups = R / RB;  // CTAs of a tile: consecutive, so its coefficients stay in L2
+  const int tile = blockIdx.x / ngroups, tid = threadIdx.x;
   const int k = tid & 3, row = tid >> 2;
-  const int r0 = blockIdx.x * RB;
+  const int r0 = (blockIdx.x % ngroups) * RB;
   const int nc = tile_nc[tile];
   const i64 u0 = (i64)tile * kAdjTile;
   const int rows = (int)min((i64)kAdjTile, n_rep - u0);
@@ -815,7 +818,9 @@ constexpr int kProdMaxWarps = 32;
 constexpr int kProdStages = 3;
 constexpr int kProdStageBytes = 48 * 1024;
 
-template <typename T>
+// MOM: also the second sums (|a|^2 |b|^2, |z|^4, x^4) that only the
+// variances of the coefficients need; without them their slots stay zero.
+template <typename T, bool MOM>
 __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     int nd, i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0, int slots,
     const int32_t* __restrict__ roles, int W, int PC, i64 chunk, double* __restrict__ partials,
@@ -908,8 +913,10 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
           f[1] = fma(a.y, y0.x, fma(-a.x, y0.y, f[1]));
           f[2] = fma(a.x, y1.x, fma(a.y, y1.y, f[2]));
           f[3] = fma(a.y, y1.x, fma(-a.x, y1.y, f[3]));
-          f[4] = fma(am, fma(y0.x, y0.x, y0.y * y0.y), f[4]);
-          f[5] = fma(am, fma(y1.x, y1.x, y1.y * y1.y), f[5]);
+          if (MOM) {
+            f[4] = fma(am, fma(y0.x, y0.x, y0.y * y0.y), f[4]);
+            f[5] = fma(am, fma(y1.x, y1.x, y1.y * y1.y), f[5]);
+          }
         }
       } else if (kind == 1) {
         const int ra = (d1 * 4 + l1) * L + l3;
@@ -921,7 +928,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
             const T2 zz = sz[((size_t)j * B + b) * L + l3];
             f[0] = fma(x.x, zz.x, fma(x.y, zz.y, f[0]));
             f[1] = fma(x.y, zz.x, fma(-x.x, zz.y, f[1]));
-            f[2] = fma(fma(x.x, x.x, x.y * x.y), fma(zz.x, zz.x, zz.y * zz.y), f[2]);
+            if (MOM) f[2] = fma(fma(x.x, x.x, x.y * x.y), fma(zz.x, zz.x, zz.y * zz.y), f[2]);
           }
         }
       } else {
@@ -934,13 +941,13 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
             const T m2 = m * m;
             f[0] += m;
             f[1] += m2;
-            f[2] = fma(m2, m2, f[2]);
+            if (MOM) f[2] = fma(m2, m2, f[2]);
             if (x0 && l3 == 0) {
               const double xv = x0c[b] + (double)sx[(size_t)j * B + b];
               const double x2 = xv * xv;
               acc[3] += xv;
               acc[4] += x2;
-              acc[5] += x2 * x2;
+              if (MOM) acc[5] += x2 * x2;
             }
           }
         }
@@ -1305,7 +1312,7 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
     if (!err) throw std::runtime_error("the coloured adjoint needs an error flag");
     const size_t smem = adjc_smem<T, RB>(op);
     STL_CUDA(cudaFuncSetAttribute(k_conv_adj_colored<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid(R / RB, (unsigned)op.n_tiles);
+    dim3 grid((unsigned)(op.n_tiles * (R / RB)));
     k_conv_adj_colored<T, RB><<<grid, kAdjCThreads, smem, s>>>(
         op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S, op.n_rep, op.o2, op.ncs, op.tile_ncells.as<int32_t>(), gy,
         R, static_cast<T*>(scr.part), op.tile_slots.as<int32_t>(), err);
@@ -1313,7 +1320,7 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
     const size_t smem = adj_tiles_smem<T, RB>(op);
     if (smem > 48 * 1024)
       STL_CUDA(cudaFuncSetAttribute(k_conv_adj_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid(R / RB, (unsigned)op.n_tiles);
+    dim3 grid((unsigned)(op.n_tiles * (R / RB)));
     k_conv_adj_tiles<T, RB><<<grid, kAdjTile, smem, s>>>(op.coef.as<T>(), op.S, op.n_rep, op.o2, op.nch, op.ncs,
                                                          op.tile_ncells.as<int32_t>(), op.tile_ent.as<uint16_t>(),
                                                          op.tile_off.as<uint16_t>(), gy, R,
@@ -1387,7 +1394,7 @@ void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, 
   const size_t smem = fwd_tiles_smem<T, RB>(op);
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_conv_fwd_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(R / RB, (unsigned)op.n_tiles);
+  dim3 grid((unsigned)(op.n_tiles * (R / RB)));
   k_conv_fwd_tiles<T, RB><<<grid, kFwdThreads, smem, s>>>(op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S,
                                                           op.n_rep, op.o2, op.tile_cells.as<int32_t>(),
                                                           op.tile_ncells.as<int32_t>(), x, R, out, mod, mod_pix,
@@ -1402,7 +1409,7 @@ void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_p
   constexpr int RBmax = sizeof(T) == 4 ? 4 : 2;
   const int RB = R % RBmax == 0 ? RBmax : (R % 2 == 0 ? 2 : 1);
   const bool fits = (RB == RBmax ? fwd_tiles_smem<T, RBmax>(op) : fwd_tiles_smem<T, 2>(op)) <= 220 * 1024;
-  if (err && op.nk == 4 && op.adj_tiles && op.lcell_t.p && op.n_tiles <= 65535 && fits) {
+  if (err && op.nk == 4 && op.adj_tiles && op.lcell_t.p && fits) {
     if (RB == RBmax) conv_forward_tiles_rb<T, RBmax>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
     else if (RB == 2) conv_forward_tiles_rb<T, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
     else conv_forward_tiles_rb<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
@@ -1417,7 +1424,7 @@ size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R) {
 }
 
 bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
-  if (!scr || !op.adj_tiles || op.nk != 4 || op.n_tiles > 65535) return false;
+  if (!scr || !op.adj_tiles || op.nk != 4) return false;
   if (adjoint_part_bytes(op, elem, R) > scr->capacity) return false;
   if (op.colored) return (elem == 4 ? adjc_smem<float, 4>(op) : adjc_smem<double, 1>(op)) <= 227 * 1024;
   const size_t smem = elem == 4 ? (adj_rb(op, elem, R) == 2 ? adj_tiles_smem<float, 2>(op) : adj_tiles_smem<float, 1>(op))
@@ -1545,16 +1552,16 @@ void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T
 
 template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
-                      const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s) {
+                      const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s, bool moments) {
   if (sh.level0 && !x0c) throw std::runtime_error("level-0 products need the map constants");
   const int L = sh.L, nd = sh.nd;
   if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
+  auto kern = moments ? k_products<T, true> : k_products<T, false>;
   if (sh.smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(k_products<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    STL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
   dim3 grid(sh.blocks, 1, sh.item_chunks);
-  k_products<T><<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots,
-                                                      sh.d_roles, sh.warps, sh.px_chunk, sh.chunk, partials, err,
-                                                      x0c, mask);
+  kern<<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots, sh.d_roles,
+                                             sh.warps, sh.px_chunk, sh.chunk, partials, err, x0c, mask);
   STL_CUDA(cudaGetLastError());
   const i64 total = (i64)sh.B * L * sh.slots;
   k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
@@ -1647,7 +1654,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*, int*);                            \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
-                                    const uint8_t*, double*, double*, int*, cudaStream_t);                                                                \
+                                    const uint8_t*, double*, double*, int*, cudaStream_t, bool);                                                                \
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, const uint8_t*, \
                                     bool, T*, T*, cudaStream_t);                                                                \
   template void mean_var_grad<T>(const T*, const double*, const uint8_t*, const double*, int, i64, T*,           \

@@ -125,6 +125,8 @@ class Engine {
   virtual void set_profiling(bool on) = 0;
   // Mean cells read per row of each level's wavelet operator.
   virtual std::vector<double> mean_slots() const = 0;
+  // Per level: slots per stored row, most cells of a tile, coloured layout (0/1).
+  virtual std::vector<std::array<int, 3>> operator_layout() const = 0;
 
  protected:
   explicit Engine(const Options& o, const Support* s = nullptr);
