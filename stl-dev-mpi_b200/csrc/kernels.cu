@@ -1039,7 +1039,7 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
 constexpr int kRevThreads = 256;
 
 template <typename T, int K>
-__global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, const T* __restrict__ z,
+__global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int bs, const T* __restrict__ z,
                                                               const T* __restrict__ br, const T* __restrict__ M,
                                                               const T* __restrict__ s1c,
                                                               const uint8_t* __restrict__ mask, int accumulate,
@@ -1047,19 +1047,22 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, cons
   extern __shared__ __align__(16) unsigned char smem[];
   typedef typename V2<T>::type T2;
   constexpr int L = 4, K1 = K - 1;
-  T2* m = reinterpret_cast<T2*>(smem);  // [L][K][K]
-  const int b = blockIdx.y, t = threadIdx.x;
-  const T2* Mb = reinterpret_cast<const T2*>(M) + (i64)b * L * K * K;
-  for (int i = t; i < L * K * K; i += kRevThreads) m[i] = Mb[i];
+  T2* m = reinterpret_cast<T2*>(smem);  // [bs][L][K][K]
+  // a CTA takes maps b0 .. b0 + bs - 1: thread (pixel, map, l3), l3 fastest,
+  // so the maps of a pixel (contiguous rows) are read and written together
+  const int b0 = blockIdx.y * bs, t = threadIdx.x;
+  const T2* Mb = reinterpret_cast<const T2*>(M) + (i64)b0 * L * K * K;
+  for (int i = t; i < bs * L * K * K; i += kRevThreads) m[i] = Mb[i];
   __syncthreads();
-  const int l3 = t & 3, px = t >> 2;
-  const T2* ml = m + l3 * K * K;
+  const int l3 = t & 3, bl = (t >> 2) % bs, px = (t >> 2) / bs, b = b0 + bl;
+  const int TPX = kRevThreads / (4 * bs);
+  if (px >= TPX) return;
+  const T2* ml = m + (bl * L + l3) * K * K;
   const T c1 = s1c[(i64)b * L + l3];
   const T2* brv = reinterpret_cast<const T2*>(br);
   const T2* zv = reinterpret_cast<const T2*>(z);
   T2* gbrv = reinterpret_cast<T2*>(gbr);
   T2* gzv = reinterpret_cast<T2*>(gz);
-  constexpr int TPX = kRevThreads / 4;
   for (i64 p = (i64)blockIdx.x * TPX + px; p < N; p += (i64)gridDim.x * TPX) {
     const i64 row = (p * B + b) * K1;
     if (mask && !mask[p]) {  // outside the averaged pixels: no cotangent
@@ -1539,14 +1542,18 @@ namespace {
 template <typename T, int K>
 void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c,
                         const uint8_t* mask, bool accumulate, T* gz, T* gbr, cudaStream_t s) {
-  const size_t smem = (size_t)4 * K * K * 2 * sizeof(T);
+  // all maps in one CTA while their cotangent matrices fit in 48 KB
+  const size_t per_map = (size_t)4 * K * K * 2 * sizeof(T);
+  const int bs = (sh.B * per_map <= 48 * 1024 && 4 * sh.B <= kRevThreads) ? sh.B : 1;
+  const size_t smem = bs * per_map;
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products_rev<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const i64 tiles = (sh.N + kRevThreads / 4 - 1) / (kRevThreads / 4);
-  const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 / sh.B));
-  dim3 grid(gx, sh.B);
-  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, z, br, M, s1c, mask, accumulate ? 1 : 0, gz,
-                                                       gbr);
+  const int tpx = kRevThreads / (4 * bs);
+  const i64 tiles = (sh.N + tpx - 1) / tpx;
+  const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 * bs / sh.B));
+  dim3 grid(gx, sh.B / bs);
+  k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, bs, z, br, M, s1c, mask, accumulate ? 1 : 0,
+                                                       gz, gbr);
 }
 }  // namespace
 
