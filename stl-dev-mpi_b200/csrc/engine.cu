@@ -832,12 +832,23 @@ class EngineImpl final : public Engine {
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), R, adj_ptr()) ? 2 : 1,
                  conv_bytes(op, R, false, true), conv_flops(op, R), s,
                  [&] { conv_adjoint<U>(op, gBr_.as<U>(), R, gmod, true, s, adj_ptr(), err_.as<int>()); });
-    prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
-      modulus_vjp_add<U>(Z_[n].as<U>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<U>(), N, B, L, s);
-    });
+    // the modulus VJP of z (gZ += gmod z / |z|): inside the coloured adjoint
+    // of z when the operator has it, else its own pass
+    ModulusAdd<U> madd;
+    madd.z = Z_[n].as<U>();
+    madd.g = gmod + n * L;
+    madd.g_pix = B * (n + 1) * L;
+    madd.g_row = (n + 1) * L;
+    const bool fuse = conv_adjoint_fuses_modulus(op, sizeof(U), B, adj_ptr(), err_.as<int>());
+    if (!fuse)
+      prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
+        modulus_vjp_add<U>(Z_[n].as<U>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<U>(), N, B, L, s);
+      });
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), B, adj_ptr()) ? 2 : 1,
-                 conv_bytes(op, B, false, false), conv_flops(op, B), s,
-                 [&] { conv_adjoint<U>(op, gZ_.as<U>(), B, gX_[n].as<U>(), false, s, adj_ptr(), err_.as<int>()); });
+                 conv_bytes(op, B, false, false), conv_flops(op, B), s, [&] {
+                   conv_adjoint<U>(op, gZ_.as<U>(), B, gX_[n].as<U>(), false, s, adj_ptr(), err_.as<int>(),
+                                   fuse ? &madd : nullptr);
+                 });
     if (n + 1 < levels_)
       prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
                    [&] {

@@ -189,12 +189,22 @@ void build_dec(const DecSpec& spec, DType dtype, DecOp& out, cudaStream_t stream
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
                   cudaStream_t s, int* err = nullptr, const double* rc = nullptr);
-//  With scratch, operators with tile tables use the row-centric two-phase
-//  adjoint (in FP32 with an error flag: its staged form, whose bounded waits
-//  on the bulk copies set *err on timeout); otherwise the transposed gather.
+//  With scratch, operators in the coloured layout use the coloured adjoint
+//  (bounded waits on its bulk copies set *err on timeout), other operators
+//  with tile tables the two-phase adjoint; otherwise the transposed gather.
+//  madd (coloured adjoint only): first add the modulus VJP to the input,
+//  gy[p][r][l] += g[p g_pix + r g_row + l] z[p][r][l] / |z[p][r][l]| (0 at
+//  z = 0), the rows r being the maps.
+template <typename T>
+struct ModulusAdd {
+  const T* z = nullptr;
+  const T* g = nullptr;
+  int g_pix = 0, g_row = 0;
+};
+bool conv_adjoint_fuses_modulus(const ConvOp& op, size_t elem, int R, const AdjScratch* scr, int* err);
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
-                  const AdjScratch* scr = nullptr, int* err = nullptr);
+                  const AdjScratch* scr = nullptr, int* err = nullptr, const ModulusAdd<T>* madd = nullptr);
 //    Input and output types may differ (FP32 and FP64 levels); the sums are
 //    in the operator's type.
 template <typename Tin, typename Tout>

@@ -580,7 +580,7 @@ template <typename T, int RB>
 __global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
     const uint16_t* __restrict__ lcell_t, const T* __restrict__ coef, int S, i64 n_rep, int o2, int ncs,
     const int32_t* __restrict__ tile_nc, const T* __restrict__ gy, int R, T* __restrict__ part,
-    const int32_t* __restrict__ tile_slots, int* __restrict__ err) {
+    const int32_t* __restrict__ tile_slots, int* __restrict__ err, ModulusAdd<T> madd) {
   constexpr int SC = adjc_sc<T>();
   constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
   constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
@@ -628,13 +628,29 @@ __global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
   // permutation is selected without indexing registers by the runtime k
   T g[RB][8];
   const bool valid = row < rows, odd = k & 1;
+  const i64 pk = valid ? rot_pixel(u0 + row, k, o2) : 0;
 #pragma unroll
   for (int rb = 0; rb < RB; ++rb) {
     T t[8];
-    if (valid) load8(gy + (rot_pixel(u0 + row, k, o2) * R + r0 + rb) * 8, t);
-    else
+    if (valid) {
+      load8(gy + (pk * R + r0 + rb) * 8, t);
+      if (madd.z) {  // the modulus VJP of row r0 + rb (map b): t += g z / |z|
+        T zz[8];
+        load8(madd.z + (pk * R + r0 + rb) * 8, zz);
+        const T* gm = madd.g + pk * madd.g_pix + (i64)(r0 + rb) * madd.g_row;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          const T mag = hypot(zz[2 * l], zz[2 * l + 1]);
+          const T dd = mag == (T)0 ? (T)1 : mag;
+          const T gv = gm[l];
+          t[2 * l] += gv * zz[2 * l] / dd;
+          t[2 * l + 1] += gv * zz[2 * l + 1] / dd;
+        }
+      }
+    } else {
 #pragma unroll
       for (int q = 0; q < 8; ++q) t[q] = (T)0;
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int gg = odd ? (q ^ 2) : q;
@@ -1310,7 +1326,7 @@ size_t adjc_smem(const ConvOp& op) {
 
 template <typename T, int RB>
 void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, const AdjScratch& scr,
-                           cudaStream_t s, int* err) {
+                           cudaStream_t s, int* err, const ModulusAdd<T>* madd) {
   if (op.colored) {
     if (!err) throw std::runtime_error("the coloured adjoint needs an error flag");
     const size_t smem = adjc_smem<T, RB>(op);
@@ -1318,7 +1334,7 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
     dim3 grid((unsigned)(op.n_tiles * (R / RB)));
     k_conv_adj_colored<T, RB><<<grid, kAdjCThreads, smem, s>>>(
         op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S, op.n_rep, op.o2, op.ncs, op.tile_ncells.as<int32_t>(), gy,
-        R, static_cast<T*>(scr.part), op.tile_slots.as<int32_t>(), err);
+        R, static_cast<T*>(scr.part), op.tile_slots.as<int32_t>(), err, madd ? *madd : ModulusAdd<T>());
   } else {
     const size_t smem = adj_tiles_smem<T, RB>(op);
     if (smem > 48 * 1024)
@@ -1435,14 +1451,20 @@ bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch
   return smem <= 200 * 1024;
 }
 
+bool conv_adjoint_fuses_modulus(const ConvOp& op, size_t elem, int R, const AdjScratch* scr, int* err) {
+  return op.colored && err && adjoint_tiles_usable(op, elem, R, scr);
+}
+
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
-                  const AdjScratch* scr, int* err) {
+                  const AdjScratch* scr, int* err, const ModulusAdd<T>* madd) {
+  if (madd && !conv_adjoint_fuses_modulus(op, sizeof(T), R, scr, err))
+    throw std::runtime_error("this adjoint cannot add the modulus VJP");
   if (adjoint_tiles_usable(op, sizeof(T), R, scr)) {
     const int rb = adj_rb(op, sizeof(T), R);
-    if (rb == 4) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 4 : 1>(op, gy, R, gx, accumulate, *scr, s, err);
-    else if (rb == 2) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 2 : 1>(op, gy, R, gx, accumulate, *scr, s, err);
-    else conv_adjoint_tiles_rb<T, 1>(op, gy, R, gx, accumulate, *scr, s, err);
+    if (rb == 4) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 4 : 1>(op, gy, R, gx, accumulate, *scr, s, err, madd);
+    else if (rb == 2) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 2 : 1>(op, gy, R, gx, accumulate, *scr, s, err, madd);
+    else conv_adjoint_tiles_rb<T, 1>(op, gy, R, gx, accumulate, *scr, s, err, madd);
   } else if (op.colored) {
     throw std::runtime_error("the coloured adjoint needs scratch for its tile partials");
   } else if (op.nk == 4) conv_adjoint_nk<T, 4>(op, gy, R, gx, accumulate, s);
@@ -1658,7 +1680,8 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
 #define INST(T)                                                                                                   \
   template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t, int*,          \
                                 const double*);               \
-  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*, int*);                            \
+  template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*, int*,        \
+                                const ModulusAdd<T>*);                            \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
                                     const uint8_t*, double*, double*, int*, cudaStream_t, bool);                                                                \
