@@ -1165,10 +1165,10 @@ __global__ void k_means_pm(const T* __restrict__ f, i64 N, int R, i64 chunk, dou
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const i64 j = i + k * (i64)TR;
-        q[k] += CPLX ? hypot((double)f[2 * j], (double)f[2 * j + 1]) : (double)f[j];
+        q[k] += CPLX ? (double)hypot(f[2 * j], f[2 * j + 1]) : (double)f[j];
       }
     }
-    for (; i < e1; i += TR) q[0] += CPLX ? hypot((double)f[2 * i], (double)f[2 * i + 1]) : (double)f[i];
+    for (; i < e1; i += TR) q[0] += CPLX ? (double)hypot(f[2 * i], f[2 * i + 1]) : (double)f[i];
     a = (q[0] + q[1]) + (q[2] + q[3]);
   }
   red[t] = a;
@@ -1204,12 +1204,20 @@ __global__ void k_means_mm(const T* __restrict__ f, i64 N, i64 chunk, double* __
   if (t == 0) partials[(i64)blockIdx.x * gridDim.y + r] = red[0];
 }
 
+// one CTA per row: strided partial sums per thread, then a tree, all in a
+// fixed order
 __global__ void k_means_final(const double* __restrict__ partials, int nblk, int R, i64 N, double* __restrict__ out) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= R) return;
-  double s = 0.0;
-  for (int k = 0; k < nblk; ++k) s += partials[(i64)k * R + r];
-  out[r] = s / (double)N;
+  __shared__ double red[256];
+  const int r = blockIdx.x, t = threadIdx.x;
+  double a = 0.0;
+  for (int k = t; k < nblk; k += blockDim.x) a += partials[(i64)k * R + r];
+  red[t] = a;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (t < h) red[t] += red[t + h];
+    __syncthreads();
+  }
+  if (t == 0) out[r] = red[0] / (double)N;
 }
 
 // moduli deviations: mod[p mod_pix + b mod_row + mod_off + l] = |z[p][b][l]| - cz[b][l]
@@ -1220,8 +1228,10 @@ __global__ void k_mod_dev(const T* __restrict__ z, i64 N, int B, int L, const do
   if (i >= N * B * L) return;
   const i64 p = i / (B * L);
   const int b = (int)((i / L) % B), l = (int)(i % L);
-  const double m = hypot((double)z[2 * i], (double)z[2 * i + 1]);
-  mod[p * mod_pix + (i64)b * mod_row + mod_off + l] = (T)(m - cz[b * L + l]);
+  // |z| in the field type (z carries that type's rounding already); the
+  // constant is subtracted in FP64 before the one rounding to T
+  const T m = hypot(z[2 * i], z[2 * i + 1]);
+  mod[p * mod_pix + (i64)b * mod_row + mod_off + l] = (T)((double)m - cz[b * L + l]);
 }
 
 // constants of the branch rows (b, d, l) of level n from the moduli constants [level][B][L]
@@ -1367,7 +1377,10 @@ void ell_rb(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o
 template <typename Tin, typename Tout, typename Tw, int NK>
 void ell_nk(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o2_in, const Tin* x, int x_pix,
             int x_outer, Tout* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
-  if (R_inner % 2 == 0)
+  if (R_inner % 4 == 0 && sizeof(Tin) == 4)
+    ell_rb<Tin, Tout, Tw, NK, 4>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
+                                 R_inner, acc, s);
+  else if (R_inner % 2 == 0)
     ell_rb<Tin, Tout, Tw, NK, 2>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
                                  R_inner, acc, s);
   else
@@ -1641,7 +1654,7 @@ void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, 
     k_means_mm<T><<<dim3(nblk, R), 256, 0, s>>>(f, N, chunk, partials);
   }
   STL_CUDA(cudaGetLastError());
-  k_means_final<<<1, 256, 0, s>>>(partials, nblk, R, N, out);
+  k_means_final<<<R, 256, 0, s>>>(partials, nblk, R, N, out);
   STL_CUDA(cudaGetLastError());
 }
 
