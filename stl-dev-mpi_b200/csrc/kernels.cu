@@ -114,9 +114,12 @@ __device__ __forceinline__ void store8(double* p, const double w[8]) {
 // RB consecutive values of a row vector (RB in 1, 2, 4)
 template <int RB>
 __device__ __forceinline__ void loadR(const float* p, float v[RB]) {
-  if (RB == 4) {
-    float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  if (RB % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < RB / 4; ++k) {
+      float4 a = __ldg(reinterpret_cast<const float4*>(p) + k);
+      v[4 * k] = a.x; v[4 * k + 1] = a.y; v[4 * k + 2] = a.z; v[4 * k + 3] = a.w;
+    }
   } else if (RB == 2) {
     float2 a = __ldg(reinterpret_cast<const float2*>(p));
     v[0] = a.x; v[1] = a.y;
