@@ -835,7 +835,7 @@ __global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, int g
 // on a copy is bounded: on timeout the CTA records the failure in *err.
 constexpr int kProdMaxWarps = 32;
 constexpr int kProdStages = 3;
-constexpr int kProdStageBytes = 48 * 1024;
+constexpr int kProdStageBytes = 72 * 1024;
 
 // MOM: also the second sums (|a|^2 |b|^2, |z|^4, x^4) that only the
 // variances of the coefficients need; without them their slots stay zero.
