@@ -49,8 +49,9 @@ def parse():
     p.add_argument("--batch", type=int, default=4)
     p.add_argument("--skip-fp64", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
-    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches"],
-                   help="scatcov: the headline metric; patches: 512 ragged disc patches (nside 512, J 5)")
+    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches", "synthesis"],
+                   help="scatcov: the headline metric; patches: 512 ragged disc patches (nside 512, J 5); "
+                        "synthesis: 200 L-BFGS iterations at nside 1024, J 9")
     return p.parse_args()
 
 
@@ -259,6 +260,65 @@ def run_patches(args, torch, dist, world, rank, dev):
     pe.close()
 
 
+def run_synthesis(args, torch, dist, world, rank, dev):
+    """L-BFGS synthesis at nside 1024, J 9, L 4, m = 10, FP32 engine: target the
+    lognormal map of seed 7, start from N(0, 1) (seed 8) rescaled to the target's
+    mean and standard deviation, loss sum_k |S_k - T_k|^2 / var_k with var_k the
+    target's variance of coefficient k; the iterate, gradients and curvature pairs
+    stay in device memory (stlp_synthesize_device).  A step is one L-BFGS
+    iteration; the timed call runs 200 (or --steps, if larger)."""
+    import stl_b200
+    nside, J, B = 1024, 9, 1
+    npix = 12 * nside * nside
+    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True)
+    xt = lognormal(7 + 1000 * rank, npix)[None]
+    target, var_t = eng.forward(xt, moments=True)
+    v = var_t.reshape(-1)
+    w = 1.0 / np.maximum(v, 1e-12 * v.max())
+    g0 = np.random.default_rng(8 + 1000 * rank).standard_normal(npix)
+    x0 = ((g0 - g0.mean()) / g0.std() * xt.std() + xt.mean())[None]
+    iters = max(200, args.steps)
+    # warm-up: a short run from the same start (operators, pools, clocks)
+    xw = torch.tensor(x0, dtype=torch.float64, device=dev)
+    eng.synthesize(xw, target, weights=w, options={"max_iter": max(3, args.warmup), "history_size": 10})
+    opts = {"max_iter": iters, "history_size": 10, "max_eval": iters * 2}
+    x_dev = torch.tensor(x0, dtype=torch.float64, device=dev)
+    res = {}
+
+    def run_dev():
+        res["n"], res["losses"] = eng.synthesize(x_dev, target, weights=w, options=opts)
+
+    with Clocks(dev.index) as clk:
+        ms = time_steps(torch, run_dev, 1, 0, dist)
+    clocks = clk.summary()
+    x_pin = torch.tensor(x0, dtype=torch.float64).pin_memory()
+    out_pin = torch.empty_like(x_pin).pin_memory()
+
+    def run_e2e():
+        xd = x_pin.to(dev, non_blocking=True)
+        eng.synthesize(xd, target, weights=w, options=opts)
+        out_pin.copy_(xd, non_blocking=True)
+        torch.cuda.synchronize(dev)
+
+    ms_e2e = time_steps(torch, run_e2e, 1, 0, dist)
+    if rank == 0:
+        losses = res["losses"]
+        line = {"metric": "L-BFGS synthesis iterations/s (nside 1024, J=9, m=10, FP32 engine, FP64 L-BFGS)",
+                "value": world * iters / (ms / 1e3), "unit": "iterations/s", "n_gpus": world, "steps": iters,
+                "warmup": max(3, args.warmup), "ms_per_step": ms / iters, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "synthesis nside1024 J9 L4 m10, lognormal target seed 7, start seed 8",
+                           "evaluations": res["n"], "loss_first": float(losses[0]),
+                           "loss_last": float(losses[-1]), "parallelism": f"replicas x{world}",
+                           "graph": "none: the line search branches on host scalars"},
+                # the maps cross PCIe once per run (start in, result out): per iteration
+                "e2e": {"value": world * iters / (ms_e2e / 1e3), "unit": "iterations/s",
+                        "h2d_bytes_per_step": int(npix * 8 / iters), "d2h_bytes_per_step": int(npix * 8 / iters)},
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -277,8 +337,9 @@ def main():
         torch.cuda.set_device(0)
     import stl_b200
 
-    if args.workload == "patches":
-        run_patches(args, torch, dist, world, rank, torch.device("cuda", local if world > 1 else 0))
+    if args.workload in ("patches", "synthesis"):
+        run = run_patches if args.workload == "patches" else run_synthesis
+        run(args, torch, dist, world, rank, torch.device("cuda", local if world > 1 else 0))
         if dist:
             dist.barrier()
             dist.destroy_process_group()

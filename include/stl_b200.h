@@ -126,6 +126,20 @@ int stlp_forward_levels(StlpHandle* h, const double* x, size_t n, double* out);
 typedef double (*stlp_callback)(const double* x, size_t n, double* grad, void* ctx);
 int64_t stlp_lbfgs(double* x, size_t n, const char* options, stlp_callback callback, void* ctx);
 
+/* Synthesis with every vector on the device: L-BFGS (the steps and options
+ * of stlp_lbfgs) of the loss sum_i w_(i mod ncoeff) |S_i(x) - T_i|^2 over the
+ * maps x (device pointer, float64 [batch][12 nside^2], updated in place), the
+ * statistics and their VJP from this handle's engine.  target: the values T
+ * (complex interleaved, n_target = batch x masks x ncoeff complex values);
+ * weights: ncoeff values or NULL (all 1).  losses (NULL allowed) receives the
+ * loss of each evaluation, at most n_losses of them.  Returns the number of
+ * evaluations, -1 on failure; the handle's forward state is cleared.  The
+ * loop of crates/stl-mpi/src/synthesis.rs:207-316 with the optimiser of
+ * stlp_lbfgs (lib.rs:711-741); no reference entry point holds the vectors
+ * on the device. */
+int64_t stlp_synthesize_device(StlpHandle* h, uint64_t x, size_t n, const double* target, size_t n_target,
+                               const double* weights, const char* options, double* losses, size_t n_losses);
+
 /* Disc patches (lib.rs:743-1176). */
 StlpPatchHandle* stlp_patch_new(const char* config);
 void stlp_patch_free(StlpPatchHandle* h);

@@ -20,6 +20,7 @@
 
 #include "engine.cuh"
 #include "json.hpp"
+#include "lbfgs.hpp"
 #include "scatcov.hpp"
 #include "../../include/stl_b200.h"
 
@@ -68,6 +69,8 @@ std::string jstr(const std::string& s) {
 
 namespace stl {
 void set_error(const std::string& msg) { g_error = msg; }
+long long synthesize_device(Engine& e, double* x, size_t n, const double* target, const double* weights,
+                            const lbfgs::Options& o, std::vector<double>* losses);
 }  // namespace stl
 
 struct StlpHandle {
@@ -294,6 +297,23 @@ int stlp_vjp_device(StlpHandle* h, const double* cot, size_t n, uint64_t generat
     h->activate();
     h->engine->reverse_device(cot, reinterpret_cast<void*>(out), f32 != 0);
     return 0;
+  });
+}
+
+int64_t stlp_synthesize_device(StlpHandle* h, uint64_t x, size_t n, const double* target, size_t n_target,
+                               const double* weights, const char* options, double* losses, size_t n_losses) {
+  return guard<int64_t>(-1, [&]() -> int64_t {
+    require(h != nullptr && x != 0 && target != nullptr, "null argument");
+    require(n == h->input_len(), "map shape mismatch");
+    require(n_target == h->values_len(), "target shape mismatch");
+    const lbfgs::Options o = lbfgs::parse_options(options);
+    h->activate();
+    h->has_current = false;  // the engine's forward state moves with the iterate
+    std::vector<double> hist;
+    const long long evals = synthesize_device(*h->engine, reinterpret_cast<double*>(x), n, target, weights, o,
+                                              losses ? &hist : nullptr);
+    if (losses) std::copy(hist.begin(), hist.begin() + std::min(hist.size(), n_losses), losses);
+    return evals;
   });
 }
 

@@ -154,18 +154,27 @@ struct Objective {
 
 }  // namespace
 
+namespace stl {
+namespace lbfgs {
+Options parse_options(const char* json) {
+  const stl::Json v = stl::Json::parse(json && *json ? json : "{}");
+  Options o;
+  o.lr = v.real("lr", 1.0);
+  o.max_iter = v.integer("max_iter", 20);
+  o.max_eval = v.has("max_eval") ? v.integer("max_eval", 0) : -1;
+  o.tol_grad = v.real("tolerance_grad", 1e-12);
+  o.tol_change = v.real("tolerance_change", 1e-15);
+  o.history = v.integer("history_size", 10);
+  if (o.history <= 0 || !(o.lr > 0.0) || !std::isfinite(o.lr)) throw std::runtime_error("invalid L-BFGS options");
+  return o;
+}
+}  // namespace lbfgs
+}  // namespace stl
+
 extern "C" int64_t stlp_lbfgs(double* x, size_t n, const char* options, stlp_callback callback, void* ctx) {
   try {
     if (!x || !callback) throw std::runtime_error("null argument");
-    const stl::Json v = stl::Json::parse(options && *options ? options : "{}");
-    stl::lbfgs::Options o;
-    o.lr = v.real("lr", 1.0);
-    o.max_iter = v.integer("max_iter", 20);
-    o.max_eval = v.has("max_eval") ? v.integer("max_eval", 0) : -1;
-    o.tol_grad = v.real("tolerance_grad", 1e-12);
-    o.tol_change = v.real("tolerance_change", 1e-15);
-    o.history = v.integer("history_size", 10);
-    if (o.history <= 0 || !(o.lr > 0.0) || !std::isfinite(o.lr)) throw std::runtime_error("invalid L-BFGS options");
+    const stl::lbfgs::Options o = stl::lbfgs::parse_options(options);
     Vec xv(x, x + n);
     Objective obj{callback, ctx};
     long long evals = 0;

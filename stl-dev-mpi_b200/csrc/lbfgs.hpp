@@ -50,6 +50,9 @@ struct Options {
   long long max_iter = 20, max_eval = -1, history = 10;
   double tol_grad = 1e-12, tol_change = 1e-15;
 };
+// options JSON (lr, max_iter, max_eval, tolerance_grad, tolerance_change,
+// history_size), validated; throws on invalid values
+Options parse_options(const char* json);
 
 template <typename Vec>
 struct LineResult {

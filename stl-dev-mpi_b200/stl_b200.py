@@ -63,6 +63,7 @@ def lib():
             "stlp_set_stream": ([_VOID, u64], C.c_int),
             "stlp_profile": ([_VOID, C.c_int, C.c_int], C.c_int),
             "stlp_set_masks": ([_VOID, _D, sz], C.c_int),
+            "stlp_synthesize_device": ([_VOID, u64, sz, _D, sz, _D, C.c_char_p, _D, sz], C.c_int64),
             "stlp_native_pixels": ([_VOID, _SIZE], C.c_int),
             "stlp_forward": ([_VOID, _D, sz, u64, u64, u64, b, _D, _D], C.c_int),
             "stlp_vjp": ([_VOID, _D, sz, u64, u64, u64, _D], C.c_int),
@@ -248,6 +249,34 @@ class NativeEngine:
             if self._lib.stlp_set_masks(self._handle, _ptr(w), w.shape[0]):
                 raise _error()
             self.nmasks = w.shape[0]
+
+    def synthesize(self, x, target, weights=None, options=None):
+        """Synthesis on the device: L-BFGS (options of native_lbfgs) of
+        sum_i w_i |S_i(x) - T_i|^2 from the CUDA float64 maps x [batch, npix],
+        updated in place; the iterate, gradients and curvature pairs stay in
+        device memory.  Returns (evaluations, losses per evaluation)."""
+        import torch
+        if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float64 and x.is_contiguous()):
+            raise ValueError("x must be a contiguous CUDA float64 tensor")
+        if x.numel() != self.batch * self.npix:
+            raise ValueError(f"expected {self.batch * self.npix} map values, got {x.numel()}")
+        t = np.ascontiguousarray(target, dtype=np.complex128).reshape(-1)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        if w is not None and w.shape != (self.ncoeff,):
+            raise ValueError(f"expected {self.ncoeff} weights, got {w.shape}")
+        opts = dict(options or {})
+        cap = int(opts.get("max_eval") or int(opts.get("max_iter", 20)) * 5 // 4) + 1
+        losses = np.zeros(cap)
+        with self._mutex:
+            self._open()
+            self._current_key = None
+            torch.cuda.synchronize(x.device)
+            n = self._lib.stlp_synthesize_device(self._handle, x.data_ptr(), x.numel(), _ptr(t.view(np.float64)),
+                                                 t.size, None if w is None else _ptr(w),
+                                                 json.dumps(opts).encode(), _ptr(losses), losses.size)
+            if n < 0:
+                raise _error()
+        return int(n), losses[:min(int(n), losses.size)]
 
     def _shape(self):
         return (self.batch, self.nmasks, self.ncoeff) if self.nmasks else (self.batch, self.ncoeff)

@@ -49,3 +49,39 @@ def test_fp32_synthesis_decreases_loss(stl):
     x, rep = stl.native_lbfgs(stl.synthesis_objective(e, target), x0.copy(), dict(max_iter=15))
     h = np.array(rep["loss_history"])
     assert np.isfinite(h).all() and h.min() < 0.5 * h[0]
+
+
+def test_device_synthesis_follows_host_lbfgs(stl):
+    """stlp_synthesize_device (iterate, gradients and history in device memory)
+    takes the steps of the host L-BFGS over the same FP64 engine: the same loss
+    after every evaluation, up to the order of the dot-product sums."""
+    import torch
+    nside, J = 16, 3
+    rng = np.random.default_rng(10)
+    target_map = np.exp(rng.standard_normal((1, 12 * nside * nside)) - 0.5)
+    x0 = rng.standard_normal((1, 12 * nside * nside)) * target_map.std() + target_map.mean()
+    e = stl.NativeEngine(nside, J, dtype="float64")
+    target, _ = e.forward(target_map)
+    w = 1.0 / (1.0 + np.arange(e.ncoeff) % 7)
+    opts = dict(max_iter=8, history_size=4)
+    xh, rep = stl.native_lbfgs(stl.synthesis_objective(e, target, weights=w), x0.copy(), opts)
+    xd = torch.tensor(x0, device="cuda")
+    n, losses = e.synthesize(xd, target, weights=w, options=opts)
+    want = np.array(rep["loss_history"])
+    assert n == len(want) == len(losses)
+    assert np.max(np.abs(losses - want) / want) <= 1e-9
+    assert np.max(np.abs(xd.cpu().numpy() - xh)) <= 1e-9 * np.max(np.abs(xh))
+    # the handle's forward state was cleared: a vjp needs a new forward
+    with pytest.raises(RuntimeError, match="stale"):
+        e.vjp(np.zeros((1, e.ncoeff), complex), generation=0)
+
+
+def test_device_synthesis_refuses_bad_shapes(stl):
+    import torch
+    e = stl.NativeEngine(16, 3, dtype="float32")
+    x = torch.zeros(1, 12 * 16 * 16, device="cuda", dtype=torch.float64)
+    with pytest.raises(RuntimeError, match="target shape mismatch"):
+        e.synthesize(x, np.zeros(e.ncoeff - 1, complex))
+    with pytest.raises(ValueError, match="CUDA float64"):
+        e.synthesize(x.float(), np.zeros(e.ncoeff, complex))
+    e.close()
