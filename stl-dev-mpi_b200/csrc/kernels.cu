@@ -1040,6 +1040,143 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
   }
 }
 
+// Level-0 products without variances: one thread per (pixel, map b, l3)
+// holds the pixel's operand vector (branches a_0..a_3 of l1, and z) and adds
+// the Gram entries it feeds: |a_l|^2, a_l1 conj(a_l2) for l1 < l2 (the
+// entries l1 > l2 are their conjugates), a_l conj(z), |z|, |z|^2, and at
+// l3 = 0 the map value and its square (FP64).  Lanes: (l3, b) fastest, then
+// the pixel, so the P = 32 / 4B pixels of a warp read whole operand rows.
+// No staging and no barrier in the loop: the operand rows are read once
+// through L1.  Every kP0Flush pixels a thread's T sums are added over the
+// warp's pixel lanes (a fixed xor tree) and into the warp's FP64 sums in
+// shared memory; at the end the warps' sums are added in warp order into
+// the partials of the general products kernel's layout.
+constexpr int kP0Flush = 16;
+constexpr int kP0Sums = 26;  // 4 |a|^2, 6 complex a conj a, 4 complex a conj z, |z|, |z|^2
+
+// warps of a CTA: the FP64 sums of the warps fit in 200 KB; FP64 operands
+// hold twice the registers, so at most 16 warps
+template <typename T>
+__host__ __device__ inline int p0_warps(int B) {
+  const int per_warp = 4 * B * kP0Sums * 8 + B * 2 * 8;  // bytes of a warp's FP64 sums
+  const int w = (200 * 1024) / per_warp, most = sizeof(T) == 4 ? 32 : 16;
+  return w < most ? w : most;
+}
+
+// source of partial slot s (level-0 layout) in the per-thread sums: index,
+// or -1 (zero), -2 - i (minus sum i), 100 / 101 (the map value / its square)
+__device__ __forceinline__ int p0_source(int s) {
+  if (s < 32) {
+    const int e = s >> 1, im = s & 1, l1 = e >> 2, l2 = e & 3;
+    if (l1 == l2) return im ? -1 : l1;
+    const int a = l1 < l2 ? l1 : l2, c = l1 < l2 ? l2 : l1;
+    const int k = a * (7 - a) / 2 + (c - a - 1);
+    if (!im) return 4 + 2 * k;
+    return l1 < l2 ? 5 + 2 * k : -2 - (5 + 2 * k);
+  }
+  if (s >= 48 && s < 56) return 16 + (s - 48);
+  if (s == 60) return 24;
+  if (s == 61) return 25;
+  if (s == 63) return 100;
+  if (s == 64) return 101;
+  return -1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 1024 : 512, 1) k_products0(i64 N, int B, const T* __restrict__ z,
+                                                        const T* __restrict__ br, const T* __restrict__ x0,
+                                                        const double* __restrict__ x0c,
+                                                        const uint8_t* __restrict__ mask, i64 chunk, int slots,
+                                                        double* __restrict__ partials) {
+  typedef typename V2<T>::type T2;
+  extern __shared__ __align__(16) double p0s[];  // [warps][4B][kP0Sums], then x sums [warps][B][2]
+  const int rows = 4 * B, P = 32 / rows;
+  const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = lane % rows, pw = lane / rows, b = r >> 2, l3 = r & 3;
+  double* acc = p0s + ((size_t)warp * rows + r) * kP0Sums;
+  double* xacc = p0s + (size_t)nw * rows * kP0Sums;
+  for (int i = lane; i < rows * kP0Sums; i += 32) p0s[(size_t)warp * rows * kP0Sums + i] = 0.0;
+  T f[kP0Sums];
+#pragma unroll
+  for (int i = 0; i < kP0Sums; ++i) f[i] = (T)0;
+  double xs = 0.0, xs2 = 0.0;
+  const T2* brv = reinterpret_cast<const T2*>(br);
+  const T2* zv = reinterpret_cast<const T2*>(z);
+  __syncwarp();
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i < kP0Sums; ++i) {
+      T v = f[i];
+      for (int o = rows; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (pw == 0) acc[i] += (double)v;
+      f[i] = (T)0;
+    }
+  };
+  const i64 p0 = (i64)blockIdx.x * chunk, p1 = min(N, p0 + chunk);
+  int cnt = 0;
+  for (i64 base = p0 + (i64)warp * P; base < p1; base += (i64)nw * P) {
+    const i64 p = base + pw;
+    if (p < p1 && (!mask || mask[p])) {
+      const i64 q = (p * B + b) * 16 + l3;  // Br [N][B][l1][l3]
+      const T2 a0 = __ldg(brv + q), a1 = __ldg(brv + q + 4), a2 = __ldg(brv + q + 8), a3 = __ldg(brv + q + 12);
+      const T2 zz = __ldg(zv + (p * B + b) * 4 + l3);
+      const T2 a[4] = {a0, a1, a2, a3};
+#pragma unroll
+      for (int l = 0; l < 4; ++l) f[l] = fma(a[l].x, a[l].x, fma(a[l].y, a[l].y, f[l]));
+      int k = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i + 1; j < 4; ++j, ++k) {
+          f[4 + 2 * k] = fma(a[i].x, a[j].x, fma(a[i].y, a[j].y, f[4 + 2 * k]));
+          f[5 + 2 * k] = fma(a[i].y, a[j].x, fma(-a[i].x, a[j].y, f[5 + 2 * k]));
+        }
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        f[16 + 2 * l] = fma(a[l].x, zz.x, fma(a[l].y, zz.y, f[16 + 2 * l]));
+        f[17 + 2 * l] = fma(a[l].y, zz.x, fma(-a[l].x, zz.y, f[17 + 2 * l]));
+      }
+      const T m = hypot(zz.x, zz.y);
+      f[24] += m;
+      f[25] = fma(m, m, f[25]);
+      if (x0 && l3 == 0) {
+        const double xv = x0c[b] + (double)x0[p * B + b];
+        xs += xv;
+        xs2 += xv * xv;
+      }
+    }
+    if (++cnt == kP0Flush) {
+      flush();
+      cnt = 0;
+    }
+  }
+  flush();
+  for (int o = rows; o < 32; o <<= 1) {
+    xs += __shfl_xor_sync(0xffffffffu, xs, o);
+    xs2 += __shfl_xor_sync(0xffffffffu, xs2, o);
+  }
+  if (pw == 0 && l3 == 0) {
+    xacc[((size_t)warp * B + b) * 2] = xs;
+    xacc[((size_t)warp * B + b) * 2 + 1] = xs2;
+  }
+  __syncthreads();
+  // partial row (blk, b, l3): every slot from its source, warps in order
+  for (int o = threadIdx.x; o < rows * slots; o += blockDim.x) {
+    const int rr = o / slots, sl = o - rr * slots, bb = rr >> 2, ll = rr & 3;
+    const int src = p0_source(sl);
+    double v = 0.0;
+    if (src >= 100) {
+      if (x0 && ll == 0)
+        for (int w = 0; w < nw; ++w) v += xacc[((size_t)w * B + bb) * 2 + (src - 100)];
+    } else if (src != -1) {
+      const int i = src >= 0 ? src : -2 - src;
+      for (int w = 0; w < nw; ++w) v += p0s[((size_t)w * rows + rr) * kP0Sums + i];
+      if (src < -1) v = -v;
+    }
+    partials[((i64)blockIdx.x * rows + rr) * slots + sl] = v;
+  }
+}
+
 // sums[row][slot] = sum over blocks of partials[blk][row][slot] in block order
 __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk, int rows, int slots,
                                   double* __restrict__ sums) {
@@ -1601,6 +1738,19 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
   if (sh.level0 && !x0c) throw std::runtime_error("level-0 products need the map constants");
   const int L = sh.L, nd = sh.nd;
   if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
+  if (sh.level0 && !moments && sh.K == 5 && 32 % (4 * sh.B) == 0 && sh.slots == 66 && x0) {
+    const int nw = p0_warps<T>(sh.B);
+    const size_t smem = (size_t)nw * (4 * sh.B * kP0Sums + sh.B * 2) * sizeof(double);
+    STL_CUDA(cudaFuncSetAttribute(k_products0<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const i64 chunk = (sh.N + sh.blocks - 1) / sh.blocks;
+    k_products0<T><<<sh.blocks, 32 * nw, smem, s>>>(sh.N, sh.B, z, br, x0, x0c, mask, chunk, sh.slots, partials);
+    STL_CUDA(cudaGetLastError());
+    const i64 total = (i64)sh.B * L * sh.slots;
+    k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
+                                                                                          sh.B * L, sh.slots, sums);
+    STL_CUDA(cudaGetLastError());
+    return;
+  }
   auto kern = moments ? k_products<T, true> : k_products<T, false>;
   if (sh.smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
