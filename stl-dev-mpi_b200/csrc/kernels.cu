@@ -1040,72 +1040,100 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
   }
 }
 
-// Level-0 products without variances: one thread per (pixel, map b, l3)
-// holds the pixel's operand vector (branches a_0..a_3 of l1, and z) and adds
-// the Gram entries it feeds: |a_l|^2, a_l1 conj(a_l2) for l1 < l2 (the
-// entries l1 > l2 are their conjugates), a_l conj(z), |z|, |z|^2, and at
-// l3 = 0 the map value and its square (FP64).  Lanes: (l3, b) fastest, then
-// the pixel, so the P = 32 / 4B pixels of a warp read whole operand rows.
-// No staging and no barrier in the loop: the operand rows are read once
-// through L1.  Every kP0Flush pixels a thread's T sums are added over the
-// warp's pixel lanes (a fixed xor tree) and into the warp's FP64 sums in
-// shared memory; at the end the warps' sums are added in warp order into
-// the partials of the general products kernel's layout.
+// Products without variances at the levels with ND = 1 or 2 branch blocks
+// (levels 0 and 1): one thread per (pixel, map b, l3) holds the pixel's
+// operand vector (branches a_(d, l), d < ND, l < 4, and z) and adds every
+// Gram entry the coefficients read: the diagonal blocks (d, d) through
+// |a|^2 and a_l1 conj(a_l2) for l1 < l2 (l1 > l2 are conjugates), the blocks
+// (d1 < d2) in full, a_(d, l) conj(z), |z|, |z|^2 and, at level 0 (l3 = 0),
+// the map value and its square in FP64.  Lanes: (l3, b) fastest, then the
+// pixel, so the P = 32 / 4B pixels of a warp read whole operand rows.  No
+// staging and no barrier in the loop: the operand rows are read once through
+// L1.  Every kP0Flush pixels a thread's sums in T are added over the warp's
+// pixel lanes (a fixed xor tree) and into the warp's FP64 sums in shared
+// memory; at the end the warps' sums are added in warp order into the
+// partials of the general products kernel's layout.
 constexpr int kP0Flush = 16;
-constexpr int kP0Sums = 26;  // 4 |a|^2, 6 complex a conj a, 4 complex a conj z, |z|, |z|^2
 
-// warps of a CTA: the FP64 sums of the warps fit in 200 KB; FP64 operands
-// hold twice the registers, so at most 16 warps
-template <typename T>
-__host__ __device__ inline int p0_warps(int B) {
-  const int per_warp = 4 * B * kP0Sums * 8 + B * 2 * 8;  // bytes of a warp's FP64 sums
-  const int w = (200 * 1024) / per_warp, most = sizeof(T) == 4 ? 32 : 16;
+template <int ND>
+__host__ __device__ constexpr int p0_sums() {  // diag blocks, full blocks, (d, z) blocks, |z|, |z|^2
+  return ND * 16 + ND * (ND - 1) / 2 * 32 + ND * 8 + 2;
+}
+template <typename T, int ND>
+__host__ __device__ constexpr int p0_threads() {
+  return (sizeof(T) == 4 ? 1024 : 512) / ND;
+}
+
+// warps of a CTA: the FP64 sums of the warps fit in 200 KB
+template <typename T, int ND>
+inline int p0_warps(int B) {
+  const int per_warp = 4 * B * p0_sums<ND>() * 8 + B * 2 * 8;
+  const int w = (200 * 1024) / per_warp, most = p0_threads<T, ND>() / 32;
   return w < most ? w : most;
 }
 
-// source of partial slot s (level-0 layout) in the per-thread sums: index,
-// or -1 (zero), -2 - i (minus sum i), 100 / 101 (the map value / its square)
+// source of partial slot s (layout of k_products, ND blocks) in the thread
+// sums: index i, -1 (zero), -2 - i (minus sum i), 100 / 101 (map value / square)
+template <int ND>
 __device__ __forceinline__ int p0_source(int s) {
-  if (s < 32) {
-    const int e = s >> 1, im = s & 1, l1 = e >> 2, l2 = e & 3;
-    if (l1 == l2) return im ? -1 : l1;
-    const int a = l1 < l2 ? l1 : l2, c = l1 < l2 ? l2 : l1;
-    const int k = a * (7 - a) / 2 + (c - a - 1);
-    if (!im) return 4 + 2 * k;
-    return l1 < l2 ? 5 + 2 * k : -2 - (5 + 2 * k);
+  constexpr int nBB = ND * (ND + 1) / 2, NF = p0_sums<ND>();
+  if (s < nBB * 48) {
+    int t = s / 48, d1 = 0;
+    const int w = s % 48;
+    while (t >= ND - d1) { t -= ND - d1; ++d1; }
+    const int d2 = d1 + t;
+    if (w >= 32) return -1;
+    const int e = w >> 1, im = w & 1, l1 = e >> 2, l2 = e & 3;
+    if (d1 == d2) {
+      const int base = d1 * 16;
+      if (l1 == l2) return im ? -1 : base + l1;
+      const int a = l1 < l2 ? l1 : l2, c = l1 < l2 ? l2 : l1;
+      const int k = a * (7 - a) / 2 + (c - a - 1);
+      if (!im) return base + 4 + 2 * k;
+      return l1 < l2 ? base + 5 + 2 * k : -2 - (base + 5 + 2 * k);
+    }
+    int pair = 0;  // index of (d1, d2) among the pairs d1 < d2, lexicographic
+    for (int x = 0; x < d1; ++x) pair += ND - 1 - x;
+    pair += d2 - d1 - 1;
+    return ND * 16 + pair * 32 + 2 * e + im;
   }
-  if (s >= 48 && s < 56) return 16 + (s - 48);
-  if (s == 60) return 24;
-  if (s == 61) return 25;
-  if (s == 63) return 100;
-  if (s == 64) return 101;
+  s -= nBB * 48;
+  if (s < 12 * ND) {
+    const int d = s / 12, w = s % 12;
+    return w < 8 ? ND * 16 + ND * (ND - 1) / 2 * 32 + d * 8 + w : -1;
+  }
+  s -= 12 * ND;
+  if (s == 0) return NF - 2;
+  if (s == 1) return NF - 1;
+  if (s == 3) return 100;
+  if (s == 4) return 101;
   return -1;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(sizeof(T) == 4 ? 1024 : 512, 1) k_products0(i64 N, int B, const T* __restrict__ z,
-                                                        const T* __restrict__ br, const T* __restrict__ x0,
-                                                        const double* __restrict__ x0c,
-                                                        const uint8_t* __restrict__ mask, i64 chunk, int slots,
-                                                        double* __restrict__ partials) {
+template <typename T, int ND>
+__global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
+    i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0,
+    const double* __restrict__ x0c, const uint8_t* __restrict__ mask, i64 chunk, int slots,
+    double* __restrict__ partials) {
   typedef typename V2<T>::type T2;
-  extern __shared__ __align__(16) double p0s[];  // [warps][4B][kP0Sums], then x sums [warps][B][2]
+  constexpr int NF = p0_sums<ND>(), OFF = ND * 16 + ND * (ND - 1) / 2 * 32, ZB = OFF;  // (d, z) blocks start
+  extern __shared__ __align__(16) double p0s[];  // [warps][4B][NF], then map sums [warps][B][2]
   const int rows = 4 * B, P = 32 / rows;
   const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = lane % rows, pw = lane / rows, b = r >> 2, l3 = r & 3;
-  double* acc = p0s + ((size_t)warp * rows + r) * kP0Sums;
-  double* xacc = p0s + (size_t)nw * rows * kP0Sums;
-  for (int i = lane; i < rows * kP0Sums; i += 32) p0s[(size_t)warp * rows * kP0Sums + i] = 0.0;
-  T f[kP0Sums];
+  double* acc = p0s + ((size_t)warp * rows + r) * NF;
+  double* xacc = p0s + (size_t)nw * rows * NF;
+  for (int i = lane; i < rows * NF; i += 32) p0s[(size_t)warp * rows * NF + i] = 0.0;
+  T f[NF];
 #pragma unroll
-  for (int i = 0; i < kP0Sums; ++i) f[i] = (T)0;
+  for (int i = 0; i < NF; ++i) f[i] = (T)0;
   double xs = 0.0, xs2 = 0.0;
   const T2* brv = reinterpret_cast<const T2*>(br);
   const T2* zv = reinterpret_cast<const T2*>(z);
   __syncwarp();
   auto flush = [&]() {
 #pragma unroll
-    for (int i = 0; i < kP0Sums; ++i) {
+    for (int i = 0; i < NF; ++i) {
       T v = f[i];
       for (int o = rows; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
       if (pw == 0) acc[i] += (double)v;
@@ -1117,28 +1145,53 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 1024 : 512, 1) k_products0(i6
   for (i64 base = p0 + (i64)warp * P; base < p1; base += (i64)nw * P) {
     const i64 p = base + pw;
     if (p < p1 && (!mask || mask[p])) {
-      const i64 q = (p * B + b) * 16 + l3;  // Br [N][B][l1][l3]
-      const T2 a0 = __ldg(brv + q), a1 = __ldg(brv + q + 4), a2 = __ldg(brv + q + 8), a3 = __ldg(brv + q + 12);
+      const i64 q = (p * B + b) * (ND * 16) + l3;  // Br [N][B][ND L][L]
+      T2 a[ND][4];
+#pragma unroll
+      for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) a[d][l] = __ldg(brv + q + (d * 4 + l) * 4);
       const T2 zz = __ldg(zv + (p * B + b) * 4 + l3);
-      const T2 a[4] = {a0, a1, a2, a3};
 #pragma unroll
-      for (int l = 0; l < 4; ++l) f[l] = fma(a[l].x, a[l].x, fma(a[l].y, a[l].y, f[l]));
-      int k = 0;
+      for (int d = 0; d < ND; ++d) {
+        T* fd = f + d * 16;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+        for (int l = 0; l < 4; ++l) fd[l] = fma(a[d][l].x, a[d][l].x, fma(a[d][l].y, a[d][l].y, fd[l]));
+        int k = 0;
 #pragma unroll
-        for (int j = i + 1; j < 4; ++j, ++k) {
-          f[4 + 2 * k] = fma(a[i].x, a[j].x, fma(a[i].y, a[j].y, f[4 + 2 * k]));
-          f[5 + 2 * k] = fma(a[i].y, a[j].x, fma(-a[i].x, a[j].y, f[5 + 2 * k]));
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = i + 1; j < 4; ++j, ++k) {
+            fd[4 + 2 * k] = fma(a[d][i].x, a[d][j].x, fma(a[d][i].y, a[d][j].y, fd[4 + 2 * k]));
+            fd[5 + 2 * k] = fma(a[d][i].y, a[d][j].x, fma(-a[d][i].x, a[d][j].y, fd[5 + 2 * k]));
+          }
+      }
+      int pair = 0;
+#pragma unroll
+      for (int d1 = 0; d1 < ND; ++d1)
+#pragma unroll
+        for (int d2 = d1 + 1; d2 < ND; ++d2, ++pair) {
+          T* fp = f + ND * 16 + pair * 32;
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int e = i * 4 + j;
+              fp[2 * e] = fma(a[d1][i].x, a[d2][j].x, fma(a[d1][i].y, a[d2][j].y, fp[2 * e]));
+              fp[2 * e + 1] = fma(a[d1][i].y, a[d2][j].x, fma(-a[d1][i].x, a[d2][j].y, fp[2 * e + 1]));
+            }
         }
 #pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        f[16 + 2 * l] = fma(a[l].x, zz.x, fma(a[l].y, zz.y, f[16 + 2 * l]));
-        f[17 + 2 * l] = fma(a[l].y, zz.x, fma(-a[l].x, zz.y, f[17 + 2 * l]));
-      }
+      for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          T* fz = f + ZB + d * 8;
+          fz[2 * l] = fma(a[d][l].x, zz.x, fma(a[d][l].y, zz.y, fz[2 * l]));
+          fz[2 * l + 1] = fma(a[d][l].y, zz.x, fma(-a[d][l].x, zz.y, fz[2 * l + 1]));
+        }
       const T m = hypot(zz.x, zz.y);
-      f[24] += m;
-      f[25] = fma(m, m, f[25]);
+      f[NF - 2] += m;
+      f[NF - 1] = fma(m, m, f[NF - 1]);
       if (x0 && l3 == 0) {
         const double xv = x0c[b] + (double)x0[p * B + b];
         xs += xv;
@@ -1163,18 +1216,30 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 1024 : 512, 1) k_products0(i6
   // partial row (blk, b, l3): every slot from its source, warps in order
   for (int o = threadIdx.x; o < rows * slots; o += blockDim.x) {
     const int rr = o / slots, sl = o - rr * slots, bb = rr >> 2, ll = rr & 3;
-    const int src = p0_source(sl);
+    const int src = p0_source<ND>(sl);
     double v = 0.0;
     if (src >= 100) {
       if (x0 && ll == 0)
         for (int w = 0; w < nw; ++w) v += xacc[((size_t)w * B + bb) * 2 + (src - 100)];
     } else if (src != -1) {
       const int i = src >= 0 ? src : -2 - src;
-      for (int w = 0; w < nw; ++w) v += p0s[((size_t)w * rows + rr) * kP0Sums + i];
+      for (int w = 0; w < nw; ++w) v += p0s[((size_t)w * rows + rr) * NF + i];
       if (src < -1) v = -v;
     }
     partials[((i64)blockIdx.x * rows + rr) * slots + sl] = v;
   }
+}
+
+template <typename T, int ND>
+void products0_launch(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
+                      const uint8_t* mask, double* partials, cudaStream_t s) {
+  const int nw = p0_warps<T, ND>(sh.B);
+  const size_t smem = (size_t)nw * (4 * sh.B * p0_sums<ND>() + sh.B * 2) * sizeof(double);
+  STL_CUDA(cudaFuncSetAttribute(k_products0<T, ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const i64 chunk = (sh.N + sh.blocks - 1) / sh.blocks;
+  k_products0<T, ND><<<sh.blocks, 32 * nw, smem, s>>>(sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, x0c, mask, chunk,
+                                                      sh.slots, partials);
+  STL_CUDA(cudaGetLastError());
 }
 
 // sums[row][slot] = sum over blocks of partials[blk][row][slot] in block order
@@ -1738,13 +1803,10 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
   if (sh.level0 && !x0c) throw std::runtime_error("level-0 products need the map constants");
   const int L = sh.L, nd = sh.nd;
   if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
-  if (sh.level0 && !moments && sh.K == 5 && 32 % (4 * sh.B) == 0 && sh.slots == 66 && x0) {
-    const int nw = p0_warps<T>(sh.B);
-    const size_t smem = (size_t)nw * (4 * sh.B * kP0Sums + sh.B * 2) * sizeof(double);
-    STL_CUDA(cudaFuncSetAttribute(k_products0<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const i64 chunk = (sh.N + sh.blocks - 1) / sh.blocks;
-    k_products0<T><<<sh.blocks, 32 * nw, smem, s>>>(sh.N, sh.B, z, br, x0, x0c, mask, chunk, sh.slots, partials);
-    STL_CUDA(cudaGetLastError());
+  // levels 0 and 1 without variances: the register-resident kernel
+  if (!moments && (sh.nd == 1 || sh.nd == 2) && 32 % (4 * sh.B) == 0 && (!sh.level0 || x0)) {
+    if (sh.nd == 1) products0_launch<T, 1>(sh, z, br, x0, x0c, mask, partials, s);
+    else products0_launch<T, 2>(sh, z, br, x0, x0c, mask, partials, s);
     const i64 total = (i64)sh.B * L * sh.slots;
     k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
                                                                                           sh.B * L, sh.slots, sums);
