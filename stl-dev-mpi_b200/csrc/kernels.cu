@@ -1284,49 +1284,69 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
   const T2* zv = reinterpret_cast<const T2*>(z);
   T2* gbrv = reinterpret_cast<T2*>(gbr);
   T2* gzv = reinterpret_cast<T2*>(gz);
-  for (i64 p = (i64)blockIdx.x * TPX + px; p < N; p += (i64)gridDim.x * TPX) {
-    const i64 row = (p * B + b) * K1;
-    if (mask && !mask[p]) {  // outside the averaged pixels: no cotangent
-      if (!accumulate) {
+  // PPT adjacent pixels per thread: every cotangent matrix entry read from
+  // shared memory serves PPT pixels
+  constexpr int PPT = K <= 21 ? 2 : 1;
+  for (i64 g = (i64)blockIdx.x * TPX + px; g * PPT < N; g += (i64)gridDim.x * TPX) {
+    T2 v[PPT][K];
+    bool on[PPT];
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const i64 p = g * PPT + q;
+      const i64 row = (p * B + b) * K1;
+      on[q] = p < N && (!mask || mask[p]);
+      if (p < N && !on[q] && !accumulate) {  // outside the averaged pixels: no cotangent
         T2 zero;
         zero.x = (T)0; zero.y = (T)0;
         for (int i = 0; i < K1; ++i) gbrv[(row + i) * L + l3] = zero;
         gzv[(p * B + b) * L + l3] = zero;
       }
-      continue;
-    }
-    T2 v[K];
 #pragma unroll
-    for (int i = 0; i < K1; ++i) v[i] = brv[(row + i) * L + l3];
-    v[K1] = zv[(p * B + b) * L + l3];
+      for (int i = 0; i < K1; ++i) {
+        if (on[q]) v[q][i] = brv[(row + i) * L + l3];
+        else { v[q][i].x = (T)0; v[q][i].y = (T)0; }
+      }
+      if (on[q]) v[q][K1] = zv[(p * B + b) * L + l3];
+      else { v[q][K1].x = (T)0; v[q][K1].y = (T)0; }
+    }
 #pragma unroll 1
     for (int i = 0; i < K; ++i) {
-      T ar = (T)0, ai = (T)0;
+      T ar[PPT], ai[PPT];
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) { ar[q] = (T)0; ai[q] = (T)0; }
 #pragma unroll
       for (int j = 0; j < K; ++j) {
         const T2 mm = ml[i * K + j];
-        ar = fma(mm.x, v[j].x, fma(-mm.y, v[j].y, ar));
-        ai = fma(mm.x, v[j].y, fma(mm.y, v[j].x, ai));
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          ar[q] = fma(mm.x, v[q][j].x, fma(-mm.y, v[q][j].y, ar[q]));
+          ai[q] = fma(mm.x, v[q][j].y, fma(mm.y, v[q][j].x, ai[q]));
+        }
       }
-      T2 o;
-      T2* dst;
-      if (i == K1) {
-        const T mag = hypot(v[K1].x, v[K1].y);
-        const T c = c1 / (mag == (T)0 ? (T)1 : mag);
-        o.x = ar + c * v[K1].x;
-        o.y = ai + c * v[K1].y;
-        dst = gzv + (p * B + b) * L + l3;
-      } else {
-        o.x = ar;
-        o.y = ai;
-        dst = gbrv + (row + i) * L + l3;
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) {
+        if (!on[q]) continue;
+        const i64 p = g * PPT + q;
+        T2 o;
+        T2* dst;
+        if (i == K1) {
+          const T mag = hypot(v[q][K1].x, v[q][K1].y);
+          const T c = c1 / (mag == (T)0 ? (T)1 : mag);
+          o.x = ar[q] + c * v[q][K1].x;
+          o.y = ai[q] + c * v[q][K1].y;
+          dst = gzv + (p * B + b) * L + l3;
+        } else {
+          o.x = ar[q];
+          o.y = ai[q];
+          dst = gbrv + ((p * B + b) * K1 + i) * L + l3;
+        }
+        if (accumulate) {
+          const T2 prev = *dst;
+          o.x += prev.x;
+          o.y += prev.y;
+        }
+        *dst = o;
       }
-      if (accumulate) {
-        const T2 prev = *dst;
-        o.x += prev.x;
-        o.y += prev.y;
-      }
-      *dst = o;
     }
   }
 }
@@ -1788,7 +1808,7 @@ void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T
   const size_t smem = bs * per_map;
   if (smem > 48 * 1024)
     STL_CUDA(cudaFuncSetAttribute(k_products_rev<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int tpx = kRevThreads / (4 * bs);
+  const int tpx = kRevThreads / (4 * bs) * (K <= 21 ? 2 : 1);  // pixels per CTA pass
   const i64 tiles = (sh.N + tpx - 1) / tpx;
   const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 * bs / sh.B));
   dim3 grid(gx, sh.B / bs);
