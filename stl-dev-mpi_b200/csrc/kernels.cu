@@ -763,7 +763,8 @@ __global__ void k_ell(const int32_t* __restrict__ col, const Tw* __restrict__ w,
   for (int k = 0; k < NK; ++k)
 #pragma unroll
     for (int rb = 0; rb < RB; ++rb) acc[k][rb] = (Tw)0;
-  for (int e = 0; e < W; ++e) {
+#pragma unroll 4
+  for (int e = 0; e < W; ++e) {  // unrolled: the loads of several entries in flight
     const i64 idx = (i64)e * n_rep + u;
     const Tw we = __ldg(w + idx);
     const i64 c = __ldg(col + idx);
@@ -1351,14 +1352,15 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
   }
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ xc,
                                 const uint8_t* __restrict__ mask, const double* __restrict__ coefs, i64 N, int B,
                                 T* __restrict__ gx) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * B) return;
-  if (mask && !mask[i / B]) return;
-  const int b = (int)(i % B);
+  const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i64)i >= N * B) return;
+  const I p = i / (I)B;
+  if (mask && !mask[p]) return;
+  const int b = (int)(i - p * (I)B);
   const double x = (xc ? xc[b] : 0.0) + (double)x0[i];
   gx[i] += (T)(coefs[2 * b] + coefs[2 * b + 1] * x);
 }
@@ -1446,13 +1448,16 @@ __global__ void k_means_final(const double* __restrict__ partials, int nblk, int
 }
 
 // moduli deviations: mod[p mod_pix + b mod_row + mod_off + l] = |z[p][b][l]| - cz[b][l]
-template <typename T>
+// (I: the index type, 32-bit when N B L fits: a 64-bit division by a runtime
+// value costs far more than the element's work)
+template <typename T, typename I>
 __global__ void k_mod_dev(const T* __restrict__ z, i64 N, int B, int L, const double* __restrict__ cz,
                           T* __restrict__ mod, int mod_pix, int mod_row, int mod_off) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * B * L) return;
-  const i64 p = i / (B * L);
-  const int b = (int)((i / L) % B), l = (int)(i % L);
+  const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i64)i >= N * B * L) return;
+  const I BL = (I)(B * L);
+  const i64 p = (i64)(i / BL);
+  const int j = (int)(i - (I)p * BL), b = j / L, l = j - b * L;
   // |z| in the field type (z carries that type's rounding already); the
   // constant is subtracted in FP64 before the one rounding to T
   const T m = hypot(z[2 * i], z[2 * i + 1]);
@@ -1475,23 +1480,23 @@ __global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, i6
 }
 
 // [B][N] <-> [N][B] transposes of the level-0 maps at the boundary
-template <typename Tin, typename Tout>
+template <typename Tin, typename Tout, typename I>
 __global__ void k_to_pixel_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B,
                                  const double* __restrict__ sub) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over N * B, output order
-  if (i >= N * B) return;
-  const i64 p = i / B;
-  const int b = (int)(i % B);
+  const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;  // over N * B, output order
+  if ((i64)i >= N * B) return;
+  const I p = i / (I)B;
+  const int b = (int)(i - p * (I)B);
   const Tin v = in[(i64)b * N + p];
   out[i] = sub ? (Tout)((double)v - sub[b]) : (Tout)v;
 }
-template <typename Tin, typename Tout>
+template <typename Tin, typename Tout, typename I>
 __global__ void k_to_map_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B,
                                const double* __restrict__ add) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;  // over B * N, output order
-  if (i >= N * B) return;
-  const int b = (int)(i / N);
-  const i64 p = i % N;
+  const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;  // over B * N, output order
+  if ((i64)i >= N * B) return;
+  const int b = (int)(i / (I)N);
+  const i64 p = (i64)(i - (I)b * (I)N);
   const Tin v = in[p * B + b];
   out[i] = add ? (Tout)((double)v + add[b]) : (Tout)v;
 }
@@ -1868,7 +1873,8 @@ void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* 
 template <typename T>
 void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const double* coefs, int B, i64 N, T* gx,
                    cudaStream_t s) {
-  k_mean_var_grad<T><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx);
+  if (N * B < ((i64)1 << 31)) k_mean_var_grad<T, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx);
+  else k_mean_var_grad<T, i64><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1896,7 +1902,10 @@ void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, 
 template <typename T>
 void moduli_deviations(const T* z, i64 N, int B, int L, const double* cz, T* mod, int mod_pix, int mod_row,
                        int mod_off, cudaStream_t s) {
-  k_mod_dev<T><<<nblocks(N * B * L, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
+  if (N * B * L < ((i64)1 << 31))
+    k_mod_dev<T, uint32_t><<<nblocks(N * B * L, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
+  else
+    k_mod_dev<T, i64><<<nblocks(N * B * L, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1915,13 +1924,15 @@ void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s) {
 
 template <typename Tin, typename Tout>
 void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub) {
-  k_to_pixel_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub);
+  if (N * B < ((i64)1 << 31)) k_to_pixel_major<Tin, Tout, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub);
+  else k_to_pixel_major<Tin, Tout, i64><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub);
   STL_CUDA(cudaGetLastError());
 }
 
 template <typename Tin, typename Tout>
 void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* add) {
-  k_to_map_major<Tin, Tout><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, add);
+  if (N * B < ((i64)1 << 31)) k_to_map_major<Tin, Tout, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, add);
+  else k_to_map_major<Tin, Tout, i64><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, add);
   STL_CUDA(cudaGetLastError());
 }
 
