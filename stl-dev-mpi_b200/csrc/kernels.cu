@@ -242,6 +242,15 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ ce
 // tile-cell indices of the tile stream through shared memory in chunks of
 // SC slots, two stages deep, by bulk asynchronous copies.
 constexpr int kFwdThreads = 4 * kAdjTile;
+// cells of a gather plane: at least nc + 1, plane bytes = 32 mod 128 when
+// reachable (within 32 extra cells)
+template <typename T, int RB>
+__host__ __device__ inline int fwd_plane_cells(int nc) {
+  const int cb = RB * (int)sizeof(T);
+  int pc = nc + 1;
+  for (int e = 0; e < 32 && (pc * cb) % 128 != 32; ++e) ++pc;
+  return (pc * cb) % 128 == 32 ? pc : nc + 1;
+}
 
 template <typename T>
 __host__ __device__ constexpr int fwd_sc() { return sizeof(T) == 4 ? 8 : 4; }
@@ -259,7 +268,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   // stage: coef [SC][kAdjTile][8] T, then indices [SC][kAdjTile] uint16
   constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
   constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
-  T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][nc + 1][RB]: cell nc (padding) is zero
+  T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][pc][RB]: cell nc (padding) is zero
   const int ngroups = R / RB;  // CTAs of a tile: consecutive, so its coefficients stay in L2
   const int tile = blockIdx.x / ngroups, tid = threadIdx.x;
   const int k = tid & 3, row = tid >> 2;
@@ -295,10 +304,14 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     if (nch > 1) issue(1);
   }
   const int32_t* tc = tile_cells + (i64)tile * kAdjCells;
-  for (int i = tid; i < 4 * (nc + 1); i += kFwdThreads) {
-    const int kk = i / (nc + 1), lc = i - kk * (nc + 1);
+  // planes of pc >= nc + 1 cells, pc chosen so that consecutive planes start
+  // 32 bytes apart modulo 128: the 4 rotations of a row, which read the same
+  // cell index in the 4 planes, then read different banks
+  const int pc = fwd_plane_cells<T, RB>(nc);
+  for (int i = tid; i < 4 * pc; i += kFwdThreads) {
+    const int kk = i / pc, lc = i - kk * pc;
     T v[RB];
-    if (lc < nc) loadR<RB>(x + rot_cell(tc[lc], kk, o2) * R + r0, v);
+    if (lc < nc) loadR<RB>(x + rot_cell(tc[lc], kk, o2) * R + r0, v);  // cells >= nc: zero
     else
 #pragma unroll
       for (int rb = 0; rb < RB; ++rb) v[rb] = (T)0;
@@ -310,7 +323,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[rb][j] = (T)0;
-  const T* sxk = sx + (size_t)k * (nc + 1) * RB;
+  const T* sxk = sx + (size_t)k * pc * RB;
   int c = 0;
   for (; c < nch; ++c) {
     const int st = c & 1;
@@ -1647,7 +1660,7 @@ inline int adj_rb(const ConvOp& op, size_t elem, int R) {
 template <typename T, int RB>
 size_t fwd_tiles_smem(const ConvOp& op) {
   const size_t stage = (size_t)fwd_sc<T>() * kAdjTile * (8 * sizeof(T) + sizeof(uint16_t));
-  return 2 * stage + sizeof(T) * 4 * (size_t)(op.max_tile_cells + 1) * RB;
+  return 2 * stage + sizeof(T) * 4 * (size_t)(op.max_tile_cells + 1 + 32) * RB;
 }
 
 template <typename T, int RB>
