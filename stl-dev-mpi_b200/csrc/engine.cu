@@ -52,6 +52,22 @@ void DevMem::release() {
   p = nullptr;
   bytes = 0;
 }
+void PinnedMem::alloc(size_t n) {
+  release();
+  if (n == 0) return;
+  cudaError_t e = cudaMallocHost(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    throw std::runtime_error("pinned host allocation of " + std::to_string(n) + " bytes failed: " +
+                             cudaGetErrorString(e));
+  }
+  bytes = n;
+}
+void PinnedMem::release() {
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  bytes = 0;
+}
 size_t device_bytes_live() { std::lock_guard<std::mutex> g(g_mem_mu); return g_live; }
 size_t device_bytes_peak() { std::lock_guard<std::mutex> g(g_mem_mu); return g_peak; }
 void device_bytes_reset_peak() { std::lock_guard<std::mutex> g(g_mem_mu); g_peak = g_live; }
@@ -401,11 +417,6 @@ class EngineImpl final : public Engine {
     h_sums_.resize(total_sums * K_);
     gZ_.alloc(max_gz);
     gBr_.alloc(max_gbr);
-    size_t max_m = 0;
-    for (int n = 0; n < levels_; ++n)
-      max_m = std::max(max_m, esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K);
-    M_.alloc(max_m);
-    s1c_.alloc(sizeof(double) * B * L);
     mv_.alloc(sizeof(double) * 2 * B * K_);
     err_.alloc(sizeof(int));
     STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
@@ -416,7 +427,7 @@ class EngineImpl final : public Engine {
     rc_.alloc(sizeof(double) * B * levels_ * L);
     mpart_.alloc(sizeof(double) * kMeansBlocks * B * L);
     in_f64_.alloc(sizeof(double) * B * npix(0));
-    field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + M_.bytes + in_f64_.bytes;
+    field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + in_f64_.bytes;
     // partial sums of the row-centric adjoint
     {
       size_t cap = 0;
@@ -764,8 +775,9 @@ class EngineImpl final : public Engine {
           }
         }
       }
+    stage_cotangents(Mk, s1k);
     for (int n = levels_ - 1; n >= 0; --n)
-      typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n, Mk, s1k); });
+      typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n); });
     STL_CUDA(cudaMemcpyAsync(mv_.p, mv.data(), mv.size() * 8, cudaMemcpyHostToDevice, s));
     for (int k = 0; k < K_; ++k)
       prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
@@ -790,8 +802,7 @@ class EngineImpl final : public Engine {
   // one level of the reverse sweep (field type U); M: the level's cotangent
   // matrices [B][L][K][K], s1: the auto-S1 scales [B][L]
   template <typename U>
-  void reverse_level(int n, const std::vector<std::vector<std::vector<std::complex<double>>>>& Mk,
-                     const std::vector<std::vector<std::vector<double>>>& s1k) {
+  void reverse_level(int n) {
     const int L = opt_.L, B = opt_.B;
     cudaStream_t s = stream_;
     const i64 N = npix(n);
@@ -809,23 +820,17 @@ class EngineImpl final : public Engine {
                    });
     else
       STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
-    // cotangent matrices in the field precision, one set per mask; the
-    // products VJP of mask k > 0 adds to that of the masks before it
+    // cotangent matrices and S1 scales in the field precision, one set per
+    // mask, staged for every level before the sweep; the products VJP of
+    // mask k > 0 adds to that of the masks before it
     const double sz = sizeof(U);
-    std::vector<std::vector<U>> hm(K_), hs(K_);
     for (int k = 0; k < K_; ++k) {
-      const auto& M = Mk[k][n];
-      const auto& s1 = s1k[k][n];
-      hm[k].resize(2 * M.size());
-      hs[k].resize(s1.size());
-      for (size_t q = 0; q < M.size(); ++q) { hm[k][2 * q] = (U)M[q].real(); hm[k][2 * q + 1] = (U)M[q].imag(); }
-      for (size_t q = 0; q < s1.size(); ++q) hs[k][q] = (U)s1[q];
-      STL_CUDA(cudaMemcpyAsync(M_.p, hm[k].data(), hm[k].size() * sizeof(U), cudaMemcpyHostToDevice, s));
-      STL_CUDA(cudaMemcpyAsync(s1c_.p, hs[k].data(), hs[k].size() * sizeof(U), cudaMemcpyHostToDevice, s));
+      const U* Mdev = reinterpret_cast<const U*>(stage_dev_.as<unsigned char>() + stage_m_[(size_t)n * K_ + k]);
+      const U* sdev = reinterpret_cast<const U*>(stage_dev_.as<unsigned char>() + stage_s_[(size_t)n * K_ + k]);
       prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0,
                    s, [&] {
-                     products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), M_.as<U>(), s1c_.as<U>(), mask(k, n),
-                                         k > 0, gZ_.as<U>(), gBr_.as<U>(), s);
+                     products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), Mdev, sdev, mask(k, n), k > 0,
+                                         gZ_.as<U>(), gBr_.as<U>(), s);
                    });
     }
     const int R = B * (n + 1) * L;
@@ -858,8 +863,42 @@ class EngineImpl final : public Engine {
                                         s);
                      });
                    });
-    // the host staging vectors are released at return: wait for the copies
-    STL_CUDA(cudaStreamSynchronize(s));
+  }
+
+  // every level's and mask's cotangent matrices [B][L][K][K] and S1 scales
+  // [B][L] in the level's field type, in pinned host memory, then one copy
+  // to the device: the reverse sweep then runs without a host round trip
+  void stage_cotangents(const std::vector<std::vector<std::vector<std::complex<double>>>>& Mk,
+                        const std::vector<std::vector<std::vector<double>>>& s1k) {
+    const int L = opt_.L, B = opt_.B;
+    stage_m_.assign((size_t)levels_ * K_, 0);
+    stage_s_.assign((size_t)levels_ * K_, 0);
+    size_t bytes = 0;
+    auto align = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    for (int n = 0; n < levels_; ++n)
+      for (int k = 0; k < K_; ++k) {
+        stage_m_[(size_t)n * K_ + k] = bytes;
+        bytes = align(bytes + esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K);
+        stage_s_[(size_t)n * K_ + k] = bytes;
+        bytes = align(bytes + esz(n) * B * L);
+      }
+    if (bytes > stage_dev_.bytes) {
+      stage_dev_.alloc(bytes);
+      stage_pin_.alloc(bytes);
+    }
+    unsigned char* h = static_cast<unsigned char*>(stage_pin_.p);
+    for (int n = 0; n < levels_; ++n)
+      typed(n, [&](auto t) {
+        using U = typename decltype(t)::type;
+        for (int k = 0; k < K_; ++k) {
+          U* m = reinterpret_cast<U*>(h + stage_m_[(size_t)n * K_ + k]);
+          U* s1 = reinterpret_cast<U*>(h + stage_s_[(size_t)n * K_ + k]);
+          const auto& M = Mk[k][n];
+          for (size_t q = 0; q < M.size(); ++q) { m[2 * q] = (U)M[q].real(); m[2 * q + 1] = (U)M[q].imag(); }
+          for (size_t q = 0; q < s1k[k][n].size(); ++q) s1[q] = (U)s1k[k][n][q];
+        }
+      });
+    STL_CUDA(cudaMemcpyAsync(stage_dev_.p, stage_pin_.p, bytes, cudaMemcpyHostToDevice, stream_));
   }
 
   Profiler prof_;
@@ -870,7 +909,10 @@ class EngineImpl final : public Engine {
   std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
-  DevMem partials_, sums_, gZ_, gBr_, M_, s1c_, mv_, in_f64_, err_, roles_;
+  DevMem partials_, sums_, gZ_, gBr_, mv_, in_f64_, err_, roles_;
+  DevMem stage_dev_;                      // staged cotangent matrices and S1 scales
+  PinnedMem stage_pin_;
+  std::vector<size_t> stage_m_, stage_s_;  // byte offsets per (level, mask)
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
   std::vector<DevMem> ids_dev_;  // grid mode: supports per level
   // averaging masks [k][level] (grid mode: the core; none: every pixel) and

@@ -57,6 +57,18 @@ struct DevMem {
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Page-locked host memory (copies from it run asynchronously).
+struct PinnedMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  PinnedMem() = default;
+  PinnedMem(const PinnedMem&) = delete;
+  PinnedMem& operator=(const PinnedMem&) = delete;
+  ~PinnedMem() { release(); }
+  void alloc(size_t n);
+  void release();
+};
+
 // Device memory accounting (bytes held by live DevMem allocations).
 size_t device_bytes_live();
 size_t device_bytes_peak();
