@@ -849,7 +849,7 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
     while (P2 < op.S * kAdjTile) P2 <<= 1;
     const size_t smem = sizeof(int32_t) * ((size_t)P2 + kAdjCells + 256);
     if (smem > 48 * 1024)
-      STL_CUDA(cudaFuncSetAttribute(k_adj_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_dynamic_smem(k_adj_tiles);
     STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
     k_adj_tiles<<<(unsigned)op.n_tiles, 256, smem, s>>>(op.cell.as<int32_t>(), op.S, a.n_rows, P2,
                                                           op.tile_cells.as<int32_t>(), op.tile_ncells.as<int32_t>(),
@@ -866,7 +866,7 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
       // every colour a matching: the coloured layout replaces the slots
       DevMem col((size_t)op.S * a.n_rows), tile_d(sizeof(int32_t) * op.n_tiles);
       const size_t csm = color_smem(op.S);
-      STL_CUDA(cudaFuncSetAttribute(k_color_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+      allow_dynamic_smem(k_color_tiles);
       STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
       k_color_tiles<<<(unsigned)op.n_tiles, 32, csm, s>>>(op.lcell.as<uint16_t>(), counts.as<int>(), op.S, a.n_rows,
                                                           op.tile_ncells.as<int32_t>(), col.as<uint8_t>(),
@@ -931,7 +931,7 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
       while (P2 < op.S * kAdjTile) P2 <<= 1;
       const size_t smem = sizeof(uint32_t) * (size_t)P2;
       if (smem > 48 * 1024)
-        STL_CUDA(cudaFuncSetAttribute(k_adj_csr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        allow_dynamic_smem(k_adj_csr);
       k_adj_csr<<<(unsigned)op.n_tiles, 256, smem, s>>>(op.cell.as<int32_t>(), op.lcell.as<uint16_t>(), op.S,
                                                           a.n_rows, P2, op.nch, op.ncs, op.tile_ncells.as<int32_t>(),
                                                           op.tile_ent.as<uint16_t>(), op.tile_off.as<uint16_t>());

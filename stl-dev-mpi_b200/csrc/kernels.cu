@@ -1249,7 +1249,7 @@ void products0_launch(const ProductShape& sh, const T* z, const T* br, const T* 
                       const uint8_t* mask, double* partials, cudaStream_t s) {
   const int nw = p0_warps<T, ND>(sh.B);
   const size_t smem = (size_t)nw * (4 * sh.B * p0_sums<ND>() + sh.B * 2) * sizeof(double);
-  STL_CUDA(cudaFuncSetAttribute(k_products0<T, ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(k_products0<T, ND>);
   const i64 chunk = (sh.N + sh.blocks - 1) / sh.blocks;
   k_products0<T, ND><<<sh.blocks, 32 * nw, smem, s>>>(sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, x0c, mask, chunk,
                                                       sh.slots, partials);
@@ -1583,7 +1583,7 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
   if (op.colored) {
     if (!err) throw std::runtime_error("the coloured adjoint needs an error flag");
     const size_t smem = adjc_smem<T, RB>(op);
-    STL_CUDA(cudaFuncSetAttribute(k_conv_adj_colored<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(k_conv_adj_colored<T, RB>);
     dim3 grid((unsigned)(op.n_tiles * (R / RB)));
     k_conv_adj_colored<T, RB><<<grid, kAdjCThreads, smem, s>>>(
         op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S, op.n_rep, op.o2, op.ncs, op.tile_ncells.as<int32_t>(), gy,
@@ -1591,7 +1591,7 @@ void conv_adjoint_tiles_rb(const ConvOp& op, const T* gy, int R, T* gx, bool acc
   } else {
     const size_t smem = adj_tiles_smem<T, RB>(op);
     if (smem > 48 * 1024)
-      STL_CUDA(cudaFuncSetAttribute(k_conv_adj_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_dynamic_smem(k_conv_adj_tiles<T, RB>);
     dim3 grid((unsigned)(op.n_tiles * (R / RB)));
     k_conv_adj_tiles<T, RB><<<grid, kAdjTile, smem, s>>>(op.coef.as<T>(), op.S, op.n_rep, op.o2, op.nch, op.ncs,
                                                          op.tile_ncells.as<int32_t>(), op.tile_ent.as<uint16_t>(),
@@ -1668,7 +1668,7 @@ void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, 
                            int mod_off, int* err, const double* rc, cudaStream_t s) {
   const size_t smem = fwd_tiles_smem<T, RB>(op);
   if (smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(k_conv_fwd_tiles<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(k_conv_fwd_tiles<T, RB>);
   dim3 grid((unsigned)(op.n_tiles * (R / RB)));
   k_conv_fwd_tiles<T, RB><<<grid, kFwdThreads, smem, s>>>(op.lcell_t.as<uint16_t>(), op.coef.as<T>(), op.S,
                                                           op.n_rep, op.o2, op.tile_cells.as<int32_t>(),
@@ -1825,7 +1825,7 @@ void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T
   const int bs = (sh.B * per_map <= 48 * 1024 && 4 * sh.B <= kRevThreads) ? sh.B : 1;
   const size_t smem = bs * per_map;
   if (smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(k_products_rev<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(k_products_rev<T, K>);
   const int tpx = kRevThreads / (4 * bs) * (K <= 21 ? 2 : 1);  // pixels per CTA pass
   const i64 tiles = (sh.N + tpx - 1) / tpx;
   const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 * bs / sh.B));
@@ -1853,7 +1853,7 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
   }
   auto kern = moments ? k_products<T, true> : k_products<T, false>;
   if (sh.smem > 48 * 1024)
-    STL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    allow_dynamic_smem(kern);
   dim3 grid(sh.blocks, 1, sh.item_chunks);
   kern<<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots, sh.d_roles,
                                              sh.warps, sh.px_chunk, sh.chunk, partials, err, x0c, mask);

@@ -9,11 +9,15 @@
 // binding threshold 1e-9, decimations restricted to it, coefficients
 // averaged over the core.  Supports are cached by (centre, radius, core);
 // each selected disc has its own engine (a disc selected twice gets two),
-// built at its first forward.
+// built at its first forward.  The discs' engines run concurrently: host
+// threads take discs in turn, each thread launching on its own stream, so
+// the many small launches of different discs overlap on the GPU.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <deque>
@@ -175,6 +179,11 @@ struct StlpPatchHandle {
   std::vector<std::pair<std::shared_ptr<CachedDisc>, int>> selected;  // disc, occurrence
   bool has_current = false;
   uint64_t current = 0;
+  int nstreams = 8;
+  std::vector<cudaStream_t> streams;
+  ~StlpPatchHandle() {
+    for (cudaStream_t s : streams) cudaStreamDestroy(s);
+  }
 
   Engine& engine(size_t i) {
     auto& d = *selected[i].first;
@@ -190,6 +199,43 @@ struct StlpPatchHandle {
     return *d.engines[k];
   }
   size_t size(size_t i) const { return selected[i].first->support.ids[0].size(); }
+  // f(disc index, its engine) for every selected disc: engines built first
+  // (in order, on this thread), then up to nstreams threads take the discs
+  // in turn, each on its own non-blocking stream; the first error is
+  // rethrown once every thread has stopped.
+  void for_discs(const std::function<void(size_t, Engine&)>& f) {
+    for (size_t i = 0; i < selected.size(); ++i) engine(i);
+    if (cudaSetDevice(opt.device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+      throw std::runtime_error("device synchronisation before the disc sweep failed");
+    const int T = (int)std::min<size_t>((size_t)std::max(1, nstreams), selected.size());
+    while ((int)streams.size() < T) {
+      cudaStream_t st;
+      if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        throw std::runtime_error("stream creation failed");
+      streams.push_back(st);
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::string> errors(T);
+    auto work = [&](int t) {
+      try {
+        if (cudaSetDevice(opt.device) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
+        for (size_t i = next++; i < selected.size(); i = next++) {
+          Engine& e = engine(i);
+          e.set_stream(streams[t]);
+          f(i, e);
+        }
+      } catch (const std::exception& ex) {
+        errors[t] = ex.what();
+        next = selected.size();
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    for (const auto& e : errors)
+      if (!e.empty()) throw std::runtime_error(e);
+  }
   size_t total() const {
     size_t t = 0;
     for (size_t i = 0; i < selected.size(); ++i) t += size(i);
@@ -218,6 +264,8 @@ StlpPatchHandle* stlp_patch_new(const char* config) {
     h->capacity = (size_t)v.integer("cache", 256);
     const long long t = v.integer("threads", 0);
     h->threads = t > 0 ? (int)t : std::max(1, (int)std::thread::hardware_concurrency());
+    h->nstreams = (int)v.integer("streams", 8);
+    require(h->nstreams >= 1 && h->nstreams <= 64, "streams must be 1 to 64");
     // validates nside, J, L, kernel as the full-sky engine does
     std::unique_ptr<Engine> probe = Engine::create(h->opt);
     h->plan = probe->plan();
@@ -382,19 +430,15 @@ static int patch_forward(StlpPatchHandle* h, const double* x_host, uint64_t x_de
   require(!h->selected.empty(), "no disc selected");
   require(n == h->total(), "input shape mismatch");
   const size_t np = h->plan.size();
-  size_t off = 0;
-  for (size_t i = 0; i < h->selected.size(); ++i) {
-    Engine& e = h->engine(i);
-    if (x_host) {
-      for (size_t q = 0; q < h->size(i); ++q)
-        require(std::isfinite(x_host[off + q]), "input patch contains non-finite values");
-      e.load_host(x_host + off);
-    } else {
-      e.load_device(reinterpret_cast<const double*>(x_dev) + off, false);
-    }
+  std::vector<size_t> off(h->selected.size() + 1, 0);
+  for (size_t i = 0; i < h->selected.size(); ++i) off[i + 1] = off[i] + h->size(i);
+  if (x_host)
+    for (size_t q = 0; q < n; ++q) require(std::isfinite(x_host[q]), "input patch contains non-finite values");
+  h->for_discs([&](size_t i, Engine& e) {
+    if (x_host) e.load_host(x_host + off[i]);
+    else e.load_device(reinterpret_cast<const double*>(x_dev) + off[i], false);
     e.forward(moments, out + 2 * i * np, moments ? var + i * np : nullptr);
-    off += h->size(i);
-  }
+  });
   h->has_current = true;
   h->current = generation;
   return 0;
@@ -422,13 +466,12 @@ static int patch_vjp(StlpPatchHandle* h, const double* cot, size_t n, uint64_t g
   require(h->has_current && h->current == generation, "stale forward state");
   const size_t np = h->plan.size();
   require(n == h->selected.size() * np, "cotangent shape mismatch");
-  size_t off = 0;
-  for (size_t i = 0; i < h->selected.size(); ++i) {
-    Engine& e = h->engine(i);
-    if (out_host) e.reverse_host(cot + 2 * i * np, out_host + off);
-    else e.reverse_device(cot + 2 * i * np, reinterpret_cast<double*>(out_dev) + off, false);
-    off += h->size(i);
-  }
+  std::vector<size_t> off(h->selected.size() + 1, 0);
+  for (size_t i = 0; i < h->selected.size(); ++i) off[i + 1] = off[i] + h->size(i);
+  h->for_discs([&](size_t i, Engine& e) {
+    if (out_host) e.reverse_host(cot + 2 * i * np, out_host + off[i]);
+    else e.reverse_device(cot + 2 * i * np, reinterpret_cast<double*>(out_dev) + off[i], false);
+  });
   return 0;
 }
 
