@@ -21,6 +21,7 @@
 #include <complex>
 #include <cstring>
 #include <mutex>
+#include <set>
 
 #include "engine.cuh"
 #include "scatcov.hpp"
@@ -51,6 +52,22 @@ void DevMem::release() {
   }
   p = nullptr;
   bytes = 0;
+}
+// once per (kernel, device), under a lock: a thread that returns has seen the
+// attribute set
+void allow_dynamic_smem_fn(const void* f) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  STL_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (done.count({f, dev})) return;
+  int most = 0;
+  cudaFuncAttributes fa;
+  STL_CUDA(cudaDeviceGetAttribute(&most, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  STL_CUDA(cudaFuncGetAttributes(&fa, f));  // the kernel's static shared memory counts against the limit
+  STL_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, most - (int)fa.sharedSizeBytes));
+  done.insert({f, dev});
 }
 void PinnedMem::alloc(size_t n) {
   release();

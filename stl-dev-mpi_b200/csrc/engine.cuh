@@ -61,14 +61,10 @@ struct DevMem {
 // attribute is process-wide and the launch's own size decides occupancy, so
 // it is always set to the maximum: threads launching f with different sizes
 // cannot undo each other's setting.
+void allow_dynamic_smem_fn(const void* f);
 template <typename F>
 inline void allow_dynamic_smem(F* f) {
-  int dev = 0, most = 0;
-  cudaFuncAttributes fa;
-  STL_CUDA(cudaGetDevice(&dev));
-  STL_CUDA(cudaDeviceGetAttribute(&most, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  STL_CUDA(cudaFuncGetAttributes(&fa, f));  // the kernel's static shared memory counts against the limit
-  STL_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, most - (int)fa.sharedSizeBytes));
+  allow_dynamic_smem_fn(reinterpret_cast<const void*>(f));
 }
 
 // Page-locked host memory (copies from it run asynchronously).

@@ -185,26 +185,33 @@ struct StlpPatchHandle {
     for (cudaStream_t s : streams) cudaStreamDestroy(s);
   }
 
-  Engine& engine(size_t i) {
+  // the engine of selected disc i, built (on stream s) at its first use;
+  // the caller has sized the disc's engine list (reserve_engines)
+  Engine& engine(size_t i, cudaStream_t s = nullptr) {
     auto& d = *selected[i].first;
     const int k = selected[i].second;
-    while ((int)d.engines.size() <= k) d.engines.push_back(nullptr);
     if (!d.engines[k]) {
       Options o = opt;
       o.B = 1;
       if (cudaSetDevice(opt.device) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
-      d.engines[k] = Engine::create_patch(o, d.support);
-      d.engines[k]->prepare();
+      std::unique_ptr<Engine> e = Engine::create_patch(o, d.support);
+      e->set_stream(s);
+      e->prepare();
+      d.engines[k] = std::move(e);
     }
     return *d.engines[k];
   }
+  void reserve_engines() {
+    for (auto& sel : selected)
+      while ((int)sel.first->engines.size() <= sel.second) sel.first->engines.push_back(nullptr);
+  }
   size_t size(size_t i) const { return selected[i].first->support.ids[0].size(); }
-  // f(disc index, its engine) for every selected disc: engines built first
-  // (in order, on this thread), then up to nstreams threads take the discs
-  // in turn, each on its own non-blocking stream; the first error is
+  // f(disc index, its engine) for every selected disc: up to nstreams
+  // threads take the discs in turn, each on its own non-blocking stream
+  // (building a disc's engine there at its first use); the first error is
   // rethrown once every thread has stopped.
   void for_discs(const std::function<void(size_t, Engine&)>& f) {
-    for (size_t i = 0; i < selected.size(); ++i) engine(i);
+    reserve_engines();
     if (cudaSetDevice(opt.device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
       throw std::runtime_error("device synchronisation before the disc sweep failed");
     const int T = (int)std::min<size_t>((size_t)std::max(1, nstreams), selected.size());
@@ -220,7 +227,7 @@ struct StlpPatchHandle {
       try {
         if (cudaSetDevice(opt.device) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
         for (size_t i = next++; i < selected.size(); i = next++) {
-          Engine& e = engine(i);
+          Engine& e = engine(i, streams[t]);
           e.set_stream(streams[t]);
           f(i, e);
         }
