@@ -174,18 +174,33 @@ Engine::Engine(const Options& o, const Support* sup) : opt_(o) {
   if (sup) {
     if ((int)sup->ids.size() != levels_ || (int)sup->core.size() != levels_)
       throw std::runtime_error("support levels mismatch");
-    if (o.B != 1) throw std::runtime_error("a patch engine holds one patch");
+    if (o.B != 1) throw std::runtime_error("a patch engine holds one patch per segment");
+    if (!sup->seg.empty() && (int)sup->seg.size() != levels_) throw std::runtime_error("segment levels mismatch");
     for (int d = 0; d < levels_; ++d) {
       const auto& ids = sup->ids[d];
       if (ids.empty()) throw std::runtime_error("empty support level");
-      for (size_t i = 0; i < ids.size(); ++i)
-        if (ids[i] < 0 || ids[i] >= npix_[d] || (i && ids[i] <= ids[i - 1]))
-          throw std::runtime_error("support ids must be sorted, unique and in range");
-      if (sup->core[d].empty()) throw std::runtime_error("empty core level");
-      for (i64 c : sup->core[d])
-        if (c < 0 || c >= (i64)ids.size()) throw std::runtime_error("core position out of range");
+      std::vector<i64> seg = sup->seg.empty() ? std::vector<i64>{0, (i64)ids.size()} : sup->seg[d];
+      if (seg.size() < 2 || seg.front() != 0 || seg.back() != (i64)ids.size() ||
+          (d > 0 && seg.size() != (sup->seg.empty() ? 2 : sup->seg[0].size())))
+        throw std::runtime_error("segment offsets must run from 0 to the support size, equal in number per level");
+      const auto& core = sup->core[d];
+      size_t c = 0;
+      for (size_t k = 0; k + 1 < seg.size(); ++k) {
+        if (seg[k + 1] <= seg[k]) throw std::runtime_error("empty support segment");
+        for (i64 i = seg[k]; i < seg[k + 1]; ++i)
+          if (ids[i] < 0 || ids[i] >= npix_[d] || (i > seg[k] && ids[i] <= ids[i - 1]))
+            throw std::runtime_error("support ids must be sorted, unique and in range");
+        const size_t c0 = c;
+        while (c < core.size() && core[c] < seg[k + 1]) {
+          if (core[c] < seg[k] || (c > c0 && core[c] <= core[c - 1]))
+            throw std::runtime_error("core positions must be ascending and in range");
+          ++c;
+        }
+        if (c == c0) throw std::runtime_error("empty core level");
+      }
+      if (c != core.size()) throw std::runtime_error("core position out of range");
       npix_[d] = (i64)ids.size();
-      ncore_[d] = (i64)sup->core[d].size();
+      ncore_[d] = (i64)core.size();
     }
     support_ = *sup;
   }
@@ -321,11 +336,7 @@ class EngineImpl final : public Engine {
     kmask_ = std::move(km);
     kcount_ = std::move(kc);
     K_ = std::max<int>(1, (int)levels.size());
-    if (ready_) {
-      sums_.alloc(sizeof(double) * total_sums_ * K_);
-      h_sums_.resize(total_sums_ * K_);
-      mv_.alloc(sizeof(double) * 2 * opt_.B * K_);
-    }
+    if (ready_) size_mask_buffers();
     forward_done_ = false;
   }
 
@@ -349,19 +360,39 @@ class EngineImpl final : public Engine {
     conv_.resize(levels_);
     dec_.resize(levels_ > 1 ? levels_ - 1 : 0);
     if (grid_mode()) {
-      // supports and core masks on the device
+      // supports (and their segments) and core masks on the device
       ids_dev_.resize(levels_);
+      seg_dev_.resize(segmented() ? levels_ : 0);
       std::vector<std::vector<uint8_t>> core(levels_);
       for (int d = 0; d < levels_; ++d) {
         const auto& ids = support_.ids[d];
         ids_dev_[d].alloc(sizeof(i64) * ids.size());
         STL_CUDA(cudaMemcpyAsync(ids_dev_[d].p, ids.data(), sizeof(i64) * ids.size(), cudaMemcpyHostToDevice,
                                  stream_));
+        if (segmented()) {
+          const auto& sg = support_.seg[d];
+          seg_dev_[d].alloc(sizeof(i64) * sg.size());
+          STL_CUDA(cudaMemcpyAsync(seg_dev_[d].p, sg.data(), sizeof(i64) * sg.size(), cudaMemcpyHostToDevice,
+                                   stream_));
+        }
         STL_CUDA(cudaStreamSynchronize(stream_));
         core[d].assign(ids.size(), 0);
         for (i64 c : support_.core[d]) core[d][c] = 1;
       }
       upload_masks({core});
+      if (segmented()) {
+        // one set of sums per segment, over its core pixels
+        K_ = segments();
+        kcount_.assign(K_, std::vector<i64>(levels_, 0));
+        for (int d = 0; d < levels_; ++d) {
+          const auto& sg = support_.seg[d];
+          int k = 0;
+          for (i64 c : support_.core[d]) {
+            while (c >= sg[k + 1]) ++k;
+            ++kcount_[k][d];
+          }
+        }
+      }
     }
     for (int n = 0; n < levels_; ++n) {
       ConvSpec cs;
@@ -371,6 +402,10 @@ class EngineImpl final : public Engine {
         cs.n_in = npix(n);
         cs.eps = kBindEps;
         cs.symmetric = false;
+        if (segmented()) {
+          cs.d_seg = seg_dev_[n].as<i64>();
+          cs.nseg = segments();
+        }
       }
       build_conv(cs, ker, dtype_of(n), conv_[n], stream_);
       operator_bytes_ += conv_[n].bytes();
@@ -384,6 +419,11 @@ class EngineImpl final : public Engine {
         ds.d_out = ids_dev_[d + 1].as<i64>();
         ds.n_out = npix(d + 1);
         ds.symmetric = false;
+        if (segmented()) {
+          ds.d_seg_in = seg_dev_[d].as<i64>();
+          ds.d_seg_out = seg_dev_[d + 1].as<i64>();
+          ds.nseg = segments();
+        }
       }
       build_dec(ds, dtype_of(d + 1), dec_[d], stream_);  // FP64 weights into an FP64 level
       operator_bytes_ += dec_[d].bytes();
@@ -403,6 +443,7 @@ class EngineImpl final : public Engine {
       gMod_[n].alloc(e * B * (n + 1) * L * N);
       gX_[n].alloc(e * B * N);
       shapes_[n] = product_shape(n, L, B, N, e);
+      if (segmented()) segment_ranges(shapes_[n], support_.seg[n]);
       max_part = std::max(max_part, (size_t)B * L * shapes_[n].blocks * shapes_[n].slots);
       max_gz = std::max(max_gz, e * 2 * B * L * N);
       max_gbr = std::max(max_gbr, e * 2 * B * (n + 1) * L * L * N);
@@ -430,11 +471,11 @@ class EngineImpl final : public Engine {
       total_sums += (size_t)B * L * shapes_[n].slots;
     }
     total_sums_ = total_sums;
-    sums_.alloc(sizeof(double) * total_sums * K_);
-    h_sums_.resize(total_sums * K_);
+    if (segmented()) upload_ranges();
+    plan_tables();
+    size_mask_buffers();
     gZ_.alloc(max_gz);
     gBr_.alloc(max_gbr);
-    mv_.alloc(sizeof(double) * 2 * B * K_);
     err_.alloc(sizeof(int));
     STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
     // per-row constants of the fields: maps [level][B], moduli [level][B][L],
@@ -569,7 +610,13 @@ class EngineImpl final : public Engine {
       });
     for (int n = 0; n < levels_; ++n)
       typed(n, [&](auto t) { forward_level<typename decltype(t)::type>(n, moments); });
-    STL_CUDA(cudaMemcpyAsync(h_sums_.data(), sums_.p, h_sums_.size() * 8, cudaMemcpyDeviceToHost, s));
+    // the coefficients (and variances) of every map and mask, from the sums
+    const size_t nv = (size_t)B * K_ * plan_.size();
+    assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
+                    counts_dev_.as<double>(), levels_, B, K_, vals_dev_.as<double>(),
+                    moments ? var_dev_.as<double>() : nullptr, s);
+    STL_CUDA(cudaMemcpyAsync(values, vals_dev_.p, 16 * nv, cudaMemcpyDeviceToHost, s));
+    if (moments && var) STL_CUDA(cudaMemcpyAsync(var, var_dev_.p, 8 * nv, cudaMemcpyDeviceToHost, s));
     int err = 0;
     STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     STL_CUDA(cudaStreamSynchronize(s));
@@ -578,7 +625,6 @@ class EngineImpl final : public Engine {
       STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
       throw std::runtime_error("a wait on a staged device copy timed out in the forward sweep");
     }
-    assemble(values, moments ? var : nullptr);
     forward_done_ = true;
     timers.forward_ms += ms_since(t0);
     timers.forwards += 1;
@@ -617,7 +663,7 @@ class EngineImpl final : public Engine {
     });
     const ProductShape& sh = shapes_[n];
     const double E = sh.K * (sh.K + 1) / 2.0;
-    for (int k = 0; k < K_; ++k)
+    for (int k = 0; k < launch_sets(); ++k)
       prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
                    [&] {
                      products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
@@ -726,82 +772,43 @@ class EngineImpl final : public Engine {
     return l;
   }
 
-  // values [B][K][np] complex, var [B][K][np]
-  void assemble(double* values, double* var) const {
-    const int L = opt_.L, B = opt_.B;
-    const i64 np = (i64)plan_.size();
-    for (int b = 0; b < B; ++b)
-      for (int k = 0; k < K_; ++k)
-        for (i64 i = 0; i < np; ++i) {
-          const Loc& l = map_[i];
-          const ProductShape& sh = shapes_[l.level];
-          const double* row = h_sums_.data() + k * total_sums_ + sum_off_[l.level] + ((size_t)b * L + l.l3) * sh.slots;
-          const double N = (double)count(k, l.level);
-          const double re = row[l.re], im = l.im >= 0 ? row[l.im] : 0.0, second = row[l.second];
-          const double vr = re / N, vi = im / N;
-          const i64 o = ((i64)b * K_ + k) * np + i;
-          values[2 * o] = vr;
-          values[2 * o + 1] = vi;
-          if (var) var[o] = std::max(second / N - (vr * vr + vi * vi), 0.0);
-        }
-  }
-
   void reverse_impl(const double* cot) {
     if (!forward_done_) throw std::runtime_error("vjp before forward");
+    STL_CUDA(cudaMemcpyAsync(cot_dev_.p, cot, 16 * (size_t)opt_.B * K_ * plan_.size(), cudaMemcpyHostToDevice,
+                             stream_));
+    reverse_sweep();
+  }
+
+  // the reverse sweep from the coefficient cotangents in cot_dev_
+  void reverse_sweep() {
     auto t0 = std::chrono::steady_clock::now();
     const int L = opt_.L, B = opt_.B;
-    const i64 np = (i64)plan_.size();
+    const int np = (int)plan_.size();
     cudaStream_t s = stream_;
-    // host: per mask and level, cotangent matrices, auto-S1 scales, mean/var scales
-    std::vector<std::vector<std::vector<std::complex<double>>>> Mk(K_, std::vector<std::vector<std::complex<double>>>(levels_));
-    std::vector<std::vector<std::vector<double>>> s1k(
-        K_, std::vector<std::vector<double>>(levels_, std::vector<double>((size_t)B * L, 0.0)));
-    std::vector<double> mv((size_t)2 * B * K_, 0.0);
-    for (int k = 0; k < K_; ++k)
-      for (int n = 0; n < levels_; ++n) Mk[k][n].assign((size_t)B * L * shapes_[n].K * shapes_[n].K, 0.0);
-    for (int b = 0; b < B; ++b)
-      for (int mk = 0; mk < K_; ++mk)
-      for (i64 i = 0; i < np; ++i) {
-        const i64 o = ((i64)b * K_ + mk) * np + i;
-        std::complex<double> g(cot[2 * o], cot[2 * o + 1]);
-        if (g == std::complex<double>(0.0, 0.0)) continue;
-        const Coef& c = plan_[i];
-        int n = c.native, K = shapes_[n].K, z = K - 1;
-        double N = (double)count(mk, n);
-        auto& M = Mk[mk];
-        auto& s1 = s1k[mk];
-        auto at = [&](int l3, int r, int q) -> std::complex<double>& {
-          return M[n][(((size_t)b * L + l3) * K + r) * K + q];
-        };
-        switch (c.family) {
-          case MEAN: mv[(size_t)mk * 2 * B + 2 * b] += g.real() / N; break;
-          case VAR: mv[(size_t)mk * 2 * B + 2 * b + 1] += 2.0 * g.real() / N; break;
-          case S1: s1[n][(size_t)b * L + c.l1] += g.real() / N; break;
-          case S2: at(c.l1, z, z) += 2.0 * g.real() / N; break;
-          case S3: {
-            int r = c.j1 * L + c.l1;
-            at(c.l3, r, z) += g / N;
-            at(c.l3, z, r) += std::conj(g) / N;
-            break;
-          }
-          case S4: {
-            int r = c.j1 * L + c.l1, q = c.j2 * L + c.l2;
-            at(c.l3, r, q) += g / N;
-            at(c.l3, q, r) += std::conj(g) / N;
-            break;
-          }
-        }
-      }
-    stage_cotangents(Mk, s1k);
+    // per level and mask: cotangent matrices and S1 scales in the level's
+    // field type; the mean and variance scales
+    for (int n = 0; n < levels_; ++n)
+      prof_.launch(Profiler::ELEM, 1, (double)K_ * B * (L * shapes_[n].K * shapes_[n].K + L) * 16.0, 0.0, s, [&] {
+        typed(n, [&](auto t) {
+          using U = typename decltype(t)::type;
+          unsigned char* base = stage_dev_.as<unsigned char>();
+          build_cotangents<U>(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, n, shapes_[n].K, L,
+                              cotsrc_dev_.as<CotSources>() + cotsrc_off_[n],
+                              cotsrc_dev_.as<CotSources>() + cotsrc_off_[n] + (size_t)L * shapes_[n].K * shapes_[n].K,
+                              reinterpret_cast<U*>(base + stage_m_[(size_t)n * K_]),
+                              reinterpret_cast<U*>(base + stage_s_[(size_t)n * K_]), s);
+        });
+      });
+    build_mean_var(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, i_mean_, i_var_,
+                   mv_.as<double>(), s);
     for (int n = levels_ - 1; n >= 0; --n)
       typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n); });
-    STL_CUDA(cudaMemcpyAsync(mv_.p, mv.data(), mv.size() * 8, cudaMemcpyHostToDevice, s));
-    for (int k = 0; k < K_; ++k)
+    for (int k = 0; k < launch_sets(); ++k)
       prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
         typed(0, [&](auto t) {
           using U = typename decltype(t)::type;
           mean_var_grad<U>(X_[0].as<U>(), xc_.as<double>(), mask(k, 0), mv_.as<double>() + (size_t)k * 2 * B, B,
-                           npix(0), gX_[0].as<U>(), s);
+                           npix(0), gX_[0].as<U>(), s, segmented() ? seg_dev_[0].as<i64>() : nullptr, K_);
         });
       });
     int err = 0;
@@ -841,7 +848,7 @@ class EngineImpl final : public Engine {
     // mask, staged for every level before the sweep; the products VJP of
     // mask k > 0 adds to that of the masks before it
     const double sz = sizeof(U);
-    for (int k = 0; k < K_; ++k) {
+    for (int k = 0; k < launch_sets(); ++k) {
       const U* Mdev = reinterpret_cast<const U*>(stage_dev_.as<unsigned char>() + stage_m_[(size_t)n * K_ + k]);
       const U* sdev = reinterpret_cast<const U*>(stage_dev_.as<unsigned char>() + stage_s_[(size_t)n * K_ + k]);
       prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0,
@@ -882,40 +889,93 @@ class EngineImpl final : public Engine {
                    });
   }
 
-  // every level's and mask's cotangent matrices [B][L][K][K] and S1 scales
-  // [B][L] in the level's field type, in pinned host memory, then one copy
-  // to the device: the reverse sweep then runs without a host round trip
-  void stage_cotangents(const std::vector<std::vector<std::vector<std::complex<double>>>>& Mk,
-                        const std::vector<std::vector<std::vector<double>>>& s1k) {
+  // buffers whose size follows the number of masks: the sums, the
+  // coefficients, their variances and cotangents, the staged cotangent
+  // matrices (per level the masks' matrices one after the other, then their
+  // S1 scales: a segmented launch reads all of them) and the mask counts
+  void size_mask_buffers() {
     const int L = opt_.L, B = opt_.B;
+    const size_t nv = (size_t)B * K_ * plan_.size();
+    sums_.alloc(sizeof(double) * total_sums_ * K_);
+    mv_.alloc(sizeof(double) * 2 * B * K_);
+    vals_dev_.alloc(16 * nv);
+    var_dev_.alloc(8 * nv);
+    cot_dev_.alloc(16 * nv);
     stage_m_.assign((size_t)levels_ * K_, 0);
     stage_s_.assign((size_t)levels_ * K_, 0);
     size_t bytes = 0;
     auto align = [](size_t v) { return (v + 255) & ~(size_t)255; };
-    for (int n = 0; n < levels_; ++n)
-      for (int k = 0; k < K_; ++k) {
-        stage_m_[(size_t)n * K_ + k] = bytes;
-        bytes = align(bytes + esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K);
-        stage_s_[(size_t)n * K_ + k] = bytes;
-        bytes = align(bytes + esz(n) * B * L);
-      }
-    if (bytes > stage_dev_.bytes) {
-      stage_dev_.alloc(bytes);
-      stage_pin_.alloc(bytes);
+    for (int n = 0; n < levels_; ++n) {
+      const size_t ms = esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K, ss = esz(n) * B * L;
+      for (int k = 0; k < K_; ++k) stage_m_[(size_t)n * K_ + k] = bytes + k * ms;
+      bytes = align(bytes + K_ * ms);
+      for (int k = 0; k < K_; ++k) stage_s_[(size_t)n * K_ + k] = bytes + k * ss;
+      bytes = align(bytes + K_ * ss);
     }
-    unsigned char* h = static_cast<unsigned char*>(stage_pin_.p);
+    stage_dev_.alloc(bytes);
+    std::vector<double> counts((size_t)K_ * levels_);
+    for (int k = 0; k < K_; ++k)
+      for (int n = 0; n < levels_; ++n) counts[(size_t)k * levels_ + n] = (double)count(k, n);
+    counts_dev_.alloc(sizeof(double) * counts.size());
+    STL_CUDA(cudaMemcpyAsync(counts_dev_.p, counts.data(), sizeof(double) * counts.size(), cudaMemcpyHostToDevice,
+                             stream_));
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  // where every plan coefficient's sums live, and the sources of every
+  // cotangent matrix entry (the adjoint of the assembly: the S3 and S4
+  // terms enter (r, q) as g and (q, r) as conj(g), S2 the diagonal z entry
+  // as 2 Re g, engine.rs:1062-1113)
+  void plan_tables() {
+    const int L = opt_.L;
+    const size_t np = plan_.size();
+    std::vector<PlanSlots> ps(np);
+    for (size_t i = 0; i < np; ++i) {
+      const Loc& l = map_[i];
+      const ProductShape& sh = shapes_[l.level];
+      ps[i] = PlanSlots{l.level, (int32_t)(sum_off_[l.level] + (size_t)l.l3 * sh.slots), L * sh.slots, l.re, l.im,
+                        l.second};
+    }
+    plan_dev_.alloc(sizeof(PlanSlots) * np);
+    STL_CUDA(cudaMemcpyAsync(plan_dev_.p, ps.data(), sizeof(PlanSlots) * np, cudaMemcpyHostToDevice, stream_));
+    cotsrc_off_.assign(levels_ + 1, 0);
     for (int n = 0; n < levels_; ++n)
-      typed(n, [&](auto t) {
-        using U = typename decltype(t)::type;
-        for (int k = 0; k < K_; ++k) {
-          U* m = reinterpret_cast<U*>(h + stage_m_[(size_t)n * K_ + k]);
-          U* s1 = reinterpret_cast<U*>(h + stage_s_[(size_t)n * K_ + k]);
-          const auto& M = Mk[k][n];
-          for (size_t q = 0; q < M.size(); ++q) { m[2 * q] = (U)M[q].real(); m[2 * q + 1] = (U)M[q].imag(); }
-          for (size_t q = 0; q < s1k[k][n].size(); ++q) s1[q] = (U)s1k[k][n][q];
+      cotsrc_off_[n + 1] = cotsrc_off_[n] + (size_t)L * shapes_[n].K * shapes_[n].K + L;
+    std::vector<CotSources> src(cotsrc_off_[levels_], CotSources{-1, -1, 0, 0});
+    for (size_t i = 0; i < np; ++i) {
+      const Coef& c = plan_[i];
+      const int n = c.native, Kd = shapes_[n].K, z = Kd - 1;
+      CotSources* base = src.data() + cotsrc_off_[n];
+      const size_t E = (size_t)L * Kd * Kd;
+      auto put = [&](size_t e, int mode) {
+        CotSources& x = base[e];
+        if (x.i0 < 0) { x.i0 = (int32_t)i; x.m0 = mode; }
+        else if (x.i1 < 0) { x.i1 = (int32_t)i; x.m1 = mode; }
+        else throw std::runtime_error("a cotangent entry with more than two sources");
+      };
+      switch (c.family) {
+        case MEAN: i_mean_ = (int)i; break;
+        case VAR: i_var_ = (int)i; break;
+        case S1: put(E + c.l1, 0); break;
+        case S2: put(((size_t)c.l1 * Kd + z) * Kd + z, 2); break;
+        case S3: {
+          const int r = c.j1 * L + c.l1;
+          put(((size_t)c.l3 * Kd + r) * Kd + z, 0);
+          put(((size_t)c.l3 * Kd + z) * Kd + r, 1);
+          break;
         }
-      });
-    STL_CUDA(cudaMemcpyAsync(stage_dev_.p, stage_pin_.p, bytes, cudaMemcpyHostToDevice, stream_));
+        case S4: {
+          const int r = c.j1 * L + c.l1, q = c.j2 * L + c.l2;
+          put(((size_t)c.l3 * Kd + r) * Kd + q, 0);
+          put(((size_t)c.l3 * Kd + q) * Kd + r, 1);
+          break;
+        }
+      }
+    }
+    cotsrc_dev_.alloc(sizeof(CotSources) * src.size());
+    STL_CUDA(cudaMemcpyAsync(cotsrc_dev_.p, src.data(), sizeof(CotSources) * src.size(), cudaMemcpyHostToDevice,
+                             stream_));
+    STL_CUDA(cudaStreamSynchronize(stream_));
   }
 
   Profiler prof_;
@@ -927,9 +987,11 @@ class EngineImpl final : public Engine {
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
   DevMem partials_, sums_, gZ_, gBr_, mv_, in_f64_, err_, roles_;
-  DevMem stage_dev_;                      // staged cotangent matrices and S1 scales
-  PinnedMem stage_pin_;
+  DevMem stage_dev_;                      // cotangent matrices and S1 scales of every level
   std::vector<size_t> stage_m_, stage_s_;  // byte offsets per (level, mask)
+  DevMem plan_dev_, counts_dev_, vals_dev_, var_dev_, cot_dev_, cotsrc_dev_;
+  std::vector<size_t> cotsrc_off_;  // per level: first cotangent source entry
+  int i_mean_ = -1, i_var_ = -1;    // plan entries of the mean and the variance
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
   std::vector<DevMem> ids_dev_;  // grid mode: supports per level
   // averaging masks [k][level] (grid mode: the core; none: every pixel) and
@@ -938,12 +1000,47 @@ class EngineImpl final : public Engine {
   std::vector<std::vector<DevMem>> kmask_;
   std::vector<std::vector<i64>> kcount_;
   size_t total_sums_ = 0;
-  const uint8_t* mask(int k, int n) const { return kmask_.empty() ? nullptr : kmask_[k][n].as<uint8_t>(); }
+  const uint8_t* mask(int k, int n) const {
+    return kmask_.empty() ? nullptr : kmask_[kmask_.size() == 1 ? 0 : k][n].as<uint8_t>();
+  }
+  // several regions: one launch covers the sums of all of them
+  bool segmented() const { return grid_mode() && segments() > 1; }
+  int launch_sets() const { return segmented() ? 1 : K_; }
+  std::vector<DevMem> seg_dev_;  // segment starts per level (device)
+  DevMem ranges_;                // the products' range tables of every level
+  // the range tables of the products to the device
+  void upload_ranges() {
+    size_t bytes = 0;
+    auto add = [&](size_t b) { size_t o = bytes; bytes += (b + 255) & ~(size_t)255; return o; };
+    std::vector<std::array<size_t, 4>> off(levels_);
+    for (int n = 0; n < levels_; ++n) {
+      const ProductShape& sh = shapes_[n];
+      off[n] = {add(sizeof(i64) * sh.blk.size()), add(sizeof(i64) * sh.rev_blk.size()),
+                add(sizeof(int32_t) * sh.rev_seg.size()), add(sizeof(int32_t) * sh.seg_blk.size())};
+    }
+    ranges_.alloc(bytes);
+    unsigned char* base = ranges_.as<unsigned char>();
+    for (int n = 0; n < levels_; ++n) {
+      ProductShape& sh = shapes_[n];
+      auto put = [&](size_t o, const void* src, size_t b) {
+        STL_CUDA(cudaMemcpyAsync(base + o, src, b, cudaMemcpyHostToDevice, stream_));
+      };
+      put(off[n][0], sh.blk.data(), sizeof(i64) * sh.blk.size());
+      put(off[n][1], sh.rev_blk.data(), sizeof(i64) * sh.rev_blk.size());
+      put(off[n][2], sh.rev_seg.data(), sizeof(int32_t) * sh.rev_seg.size());
+      put(off[n][3], sh.seg_blk.data(), sizeof(int32_t) * sh.seg_blk.size());
+      sh.d_blk = reinterpret_cast<const i64*>(base + off[n][0]);
+      sh.d_rev_blk = reinterpret_cast<const i64*>(base + off[n][1]);
+      sh.d_rev_seg = reinterpret_cast<const int32_t*>(base + off[n][2]);
+      sh.d_seg_blk = reinterpret_cast<const int32_t*>(base + off[n][3]);
+      sh.seg_stride = total_sums_;
+    }
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
   i64 count(int k, int n) const { return kcount_.empty() ? npix(n) : kcount_[k][n]; }
   DevMem adj_part_;
   AdjScratch adj_;
   const AdjScratch* adj_ptr() const { return adj_.part ? &adj_ : nullptr; }
-  std::vector<double> h_sums_;
   std::vector<Loc> map_;
 };
 

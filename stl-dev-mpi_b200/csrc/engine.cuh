@@ -96,6 +96,8 @@ struct ConvSpec {
   i64 n_in = 0;
   const i64* d_rows = nullptr;  // NESTED ids of the output rows (device), nullptr: rows == grid
   i64 n_rows = 0;
+  const i64* d_seg = nullptr;   // segments of the grid: nseg + 1 starts (device), nullptr: one
+  int nseg = 0;
   bool symmetric = true;        // full sky: store the rows of faces 0, 4, 8 only
 };
 
@@ -174,6 +176,11 @@ struct DecSpec {
   i64 n_in = 0;
   const i64* d_out = nullptr;  // sorted coarse ids = parents of the grid (device), nullptr: whole sky
   i64 n_out = 0;
+  // segments of both grids (nseg + 1 starts each, device; coarse segment k
+  // holds the parents of fine segment k), nullptr: one
+  const i64* d_seg_in = nullptr;
+  const i64* d_seg_out = nullptr;
+  int nseg = 0;
   bool symmetric = true;       // full sky: store the rows of faces 0, 4, 8 only
 };
 
@@ -254,10 +261,27 @@ struct ProductShape {
   int px_chunk = 0;  // pixels per staged chunk
   i64 chunk = 0;     // pixels per range
   size_t smem = 0;   // staged chunks
+  // Several regions (segments), each with its own sums: the CTAs take pixel
+  // ranges inside one segment -- forward ranges blk (blocks + 1 starts),
+  // reverse ranges rev_blk (rev_blocks + 1 starts) with their segments
+  // rev_seg -- and the partials of segment k are the forward ranges
+  // seg_blk[k] .. seg_blk[k + 1] - 1; its sums start k seg_stride after
+  // those of segment 0.  Empty tables: one region, uniform ranges.
+  int nseg = 1, rev_blocks = 0;
+  size_t seg_stride = 0;
+  std::vector<i64> blk, rev_blk;
+  std::vector<int32_t> rev_seg, seg_blk;
+  const i64* d_blk = nullptr;
+  const i64* d_rev_blk = nullptr;
+  const int32_t* d_rev_seg = nullptr;
+  const int32_t* d_seg_blk = nullptr;
 };
 ProductShape product_shape(int n, int L, int B, i64 N, size_t elem);
+// fills the range tables of sh for the segments seg (nseg + 1 starts) of its
+// level; the device copies are the caller's
+void segment_ranges(ProductShape& sh, const std::vector<i64>& seg);
 // z [N][B][L], br [N][B][(n+1) L][L] complex, x0 [N][B] (level 0) ->
-// sums [B][L][slots] (FP64)
+// sums [B][L][slots] (FP64), per segment with segments
 // *err becomes nonzero when a wait on a staged copy timed out.  x0 holds
 // the level-0 maps as deviations from x0c [B].
 // mask (or null): 1 on the pixels the sums cover.  moments: also the
@@ -266,14 +290,49 @@ template <typename T>
 void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
                       const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s, bool moments);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
+// (with segments: M [nseg][B][L][K][K], s1c [nseg][B][L])
 // accumulate: add to gz / gbr (on the mask's pixels) instead of writing them
 template <typename T>
 void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c, const uint8_t* mask,
                       bool accumulate, T* gz, T* gbr, cudaStream_t s);
-// gx[p][b] += coefs[b][0] + coefs[b][1] (xc[b] + x0[p][b])
+// gx[p][b] += coefs[b][0] + coefs[b][1] (xc[b] + x0[p][b]); with segments
+// (seg: nseg + 1 starts, device) the coefficients of p's segment,
+// coefs [nseg][B][2]
 template <typename T>
 void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const double* coefs, int B, i64 N, T* gx,
-                   cudaStream_t s);
+                   cudaStream_t s, const i64* seg = nullptr, int nseg = 1);
+// ---- coefficients <-> sums on the device (kernels.cu) -------------------------
+// Where plan coefficient i reads a mask's sums: the row of map 0 of its
+// level and l3 at base, that of map b at base + b stride; the slots of its
+// real part, imaginary part (-1: exactly zero) and second moment.
+struct PlanSlots {
+  int32_t level, base, stride, re, im, second;
+};
+// values [B][K][np] complex and var [B][K][np] (or null) from the sums of K
+// masks (mask k at sums + k mask_stride); counts [K][levels]: the pixels
+// mask k averages at every level.  value = sum / count, var = max(second /
+// count - |value|^2, 0).
+void assemble_values(const double* sums, size_t mask_stride, const PlanSlots* plan, int np, const double* counts,
+                     int levels, int B, int K, double* values, double* var, cudaStream_t s);
+// Sources of one entry of a level's cotangent matrices (or of an S1 scale,
+// or of the mean / variance scales): up to two plan coefficients, each
+// entering as g (mode 0), conj(g) (1) or 2 Re g (2), divided by the mask's
+// pixel count, added in that order (plan order).
+struct CotSources {
+  int32_t i0, i1, m0, m1;
+};
+// Cotangent matrices M [K][B][L][Kd][Kd] complex and S1 scales s1 [K][B][L]
+// of level n in the field type U, from the coefficient cotangents cot
+// [B][K][np] complex: entry (b, l3, r, q) from src[(l3 Kd + r) Kd + q], the
+// real S1 scale (b, l) from s1src[l].
+template <typename U>
+void build_cotangents(const double* cot, int np, int B, int K, const double* counts, int levels, int n, int Kd,
+                      int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s);
+// mv [K][B][2]: the scales of the mean (plan entry i_mean) and variance
+// (i_var) cotangents of every map
+void build_mean_var(const double* cot, int np, int B, int K, const double* counts, int levels, int i_mean, int i_var,
+                    double* mv, cudaStream_t s);
+
 // Per-row constants (kernels.cu): out[r] = mean over the N pixels of row r
 // of a pixel-major [N][R] field (complex_moduli: the moduli of a complex
 // field) or of a map-major [R][N] field; partials: kMeansBlocks x R doubles.

@@ -28,14 +28,25 @@ constexpr int kFoldCap = 128;  // distinct cells one row may read
 constexpr int kDecCap = 256;   // candidates of one decimation row
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 
-__device__ __forceinline__ i64 grid_find(const i64* grid, i64 n, i64 v) {
-  if (!grid) return (v >= 0 && v < n) ? v : -1;
-  i64 lo = 0, hi = n;
+// position of v in the sorted grid[lo, hi) (whole sky: v itself), or -1
+__device__ __forceinline__ i64 grid_find(const i64* grid, i64 lo, i64 hi, i64 v) {
+  if (!grid) return (v >= 0 && v < hi) ? v : -1;
+  const i64 end = hi;
   while (lo < hi) {
     i64 mid = (lo + hi) >> 1;
     if (grid[mid] < v) lo = mid + 1; else hi = mid;
   }
-  return (lo < n && grid[lo] == v) ? lo : -1;
+  return (lo < end && grid[lo] == v) ? lo : -1;
+}
+
+// index of the segment of seg (nseg + 1 ascending starts) holding position k
+__device__ __forceinline__ int segment_index(const i64* seg, int nseg, i64 k) {
+  int a = 0, b = nseg;  // seg[a] <= k < seg[b]
+  while (b - a > 1) {
+    const int m = (a + b) >> 1;
+    if (seg[m] <= k) a = m; else b = m;
+  }
+  return a;
 }
 
 struct FoldArgs {
@@ -44,6 +55,8 @@ struct FoldArgs {
   double eps;
   const i64* grid;
   i64 n_in;
+  const i64* seg;         // segments of grid (rows == grid), or nullptr
+  int nseg;
   const i64* rows;
   i64 n_rows;             // rows built (the stored rows)
   int sym;                // stored row u is pixel (4 (u >> sym_o2)) << sym_o2 | local
@@ -64,6 +77,12 @@ __global__ void k_fold(FoldArgs a, int* counts, int S, int32_t* cell, T* coef, i
     id = ((4 * (k >> a.sym_o2)) << a.sym_o2) | (k & mask);
   } else {
     id = a.rows ? a.rows[k] : (a.grid ? a.grid[k] : k);
+  }
+  i64 g_lo = 0, g_hi = a.n_in;  // the cells this row may read
+  if (a.seg) {
+    const int sg = segment_index(a.seg, a.nseg, k);
+    g_lo = a.seg[sg];
+    g_hi = a.seg[sg + 1];
   }
   double theta, phi;
   pix2ang_nest(id, a.nside, theta, phi);
@@ -95,14 +114,14 @@ __global__ void k_fold(FoldArgs a, int* counts, int S, int32_t* cell, T* coef, i
       const i64* ix = ipx;
       const double* wx = iw;
       for (int q = 0; q < 4; ++q) {
-        found[q] = grid_find(a.grid, a.n_in, ix[q]);
+        found[q] = grid_find(a.grid, g_lo, g_hi, ix[q]);
         if (a.eps > 0.0 && wx[q] <= a.eps) found[q] = -1;
       }
       if (found[0] < 0 && found[1] < 0 && found[2] < 0 && found[3] < 0) {  // empty tap: central tap
         ix = ref_pix;
         wx = ref_w;
         for (int q = 0; q < 4; ++q) {
-          found[q] = grid_find(a.grid, a.n_in, ix[q]);
+          found[q] = grid_find(a.grid, g_lo, g_hi, ix[q]);
           if (a.eps > 0.0 && wx[q] <= a.eps) found[q] = -1;
         }
       }
@@ -591,6 +610,9 @@ struct DecArgs {
   int order, corder;
   const i64* ids;  // fine grid (nullptr: whole sky)
   i64 n_in;
+  const i64* seg_in;   // segments of the fine grid and of the coarse rows, or nullptr
+  const i64* seg_out;
+  int nseg;
   const i64* out;  // coarse rows (nullptr: whole sky)
   i64 n_out;       // rows built (the stored rows)
   int sym;         // stored row u is coarse pixel (4 (u >> sym_co2)) << sym_co2 | local
@@ -615,11 +637,17 @@ __global__ void k_dec_rows(DecArgs a, int* counts, int W, int32_t* col, T* wout,
   if (a.sym) c = ((4 * (r >> a.sym_co2)) << a.sym_co2) | (r & ((i64(1) << a.sym_co2) - 1));
   else c = a.out ? a.out[r] : r;
   i64 cn = a.nside / 2;
+  i64 f_lo = 0, f_hi = a.n_in;  // the fine cells this row may read: its segment's
+  if (a.seg_out) {
+    const int sg = segment_index(a.seg_out, a.nseg, r);
+    f_lo = a.seg_in[sg];
+    f_hi = a.seg_in[sg + 1];
+  }
   i64 cand[kDecCap];
   int n = 0;
   bool over = false;
   auto push = [&](i64 fine) {
-    i64 q = grid_find(a.ids, a.n_in, fine);
+    i64 q = grid_find(a.ids, f_lo, f_hi, fine);
     if (q < 0) return;
     if (n >= kDecCap) { over = true; return; }
     cand[n++] = q;
@@ -806,6 +834,8 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   a.nside = sp.nside; a.order = order_of(sp.nside); a.ksz = sp.ksz; a.P = P; a.G = sp.G; a.gauge = sp.gauge;
   a.p_ref = (sp.ksz / 2) * (sp.ksz + 1); a.eps = sp.eps;
   a.grid = sp.d_grid; a.n_in = sp.d_grid ? sp.n_in : npix_of(sp.nside);
+  if (sp.d_seg && (!sp.d_grid || sp.d_rows)) throw std::runtime_error("segments need a grid whose cells are the rows");
+  a.seg = sp.d_seg; a.nseg = sp.nseg;
   a.rows = sp.d_rows;
   i64 n_rows = sp.d_rows ? sp.n_rows : a.n_in;
   a.n_rows = sym ? n_rows / 4 : n_rows;
@@ -988,6 +1018,9 @@ static void build_dec_t(const DecSpec& sp, DecOp& op, cudaStream_t s) {
   DecArgs a;
   a.nside = sp.nside; a.order = order_of(sp.nside); a.corder = order_of(sp.nside / 2);
   a.ids = sp.d_ids; a.n_in = sp.d_ids ? sp.n_in : npix_of(sp.nside);
+  if ((sp.d_seg_in != nullptr) != (sp.d_seg_out != nullptr) || (sp.d_seg_in && (!sp.d_ids || !sp.d_out)))
+    throw std::runtime_error("decimation segments need both grids");
+  a.seg_in = sp.d_seg_in; a.seg_out = sp.d_seg_out; a.nseg = sp.nseg;
   a.out = sp.d_out;
   i64 n_out = sp.d_out ? sp.n_out : npix_of(sp.nside / 2);
   a.n_out = sym ? n_out / 4 : n_out;

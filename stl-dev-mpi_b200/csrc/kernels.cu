@@ -857,7 +857,8 @@ template <typename T, bool MOM>
 __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     int nd, i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0, int slots,
     const int32_t* __restrict__ roles, int W, int PC, i64 chunk, double* __restrict__ partials,
-    int* __restrict__ err, const double* __restrict__ x0c, const uint8_t* __restrict__ mask) {
+    int* __restrict__ err, const double* __restrict__ x0c, const uint8_t* __restrict__ mask,
+    const i64* __restrict__ blk) {
   typedef typename V2<T>::type T2;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kProdStages];
@@ -882,13 +883,16 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
   }
   const int l3 = lane & 3, l1 = (lane >> 2) & 3, hx = lane >> 4, q8 = lane >> 2;
   // stage s: branch rows [PC][B][K1][L], z [PC][B][L], then at level 0 the
-  // maps [PC][B] (PC B sizeof(T) and the range starts are multiples of 16
-  // bytes there)
+  // maps [PC][B], copied from the 16-byte boundary at or below the chunk's
+  // first map value (x_off(pc) bytes before it)
   const size_t br_px = (size_t)B * K1 * L, z_px = (size_t)B * L;  // T2 per pixel
-  const size_t x_bytes = x0 ? (size_t)PC * B * sizeof(T) : 0;
+  const size_t x_bytes = x0 ? (((size_t)PC * B * sizeof(T) + 15) & ~(size_t)15) + 16 : 0;
   const size_t stage_bytes = (size_t)PC * (br_px + z_px) * sizeof(T2) + x_bytes;
   unsigned char* stage0 = smem;
-  const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
+  // the pixel range: uniform, or from the range table (segments)
+  const i64 P0 = blk ? blk[blockIdx.x] : (i64)blockIdx.x * chunk;
+  const i64 P1 = blk ? blk[blockIdx.x + 1] : min(N, P0 + chunk);
+  auto x_off = [&](i64 pc) { return (unsigned)(((size_t)pc * B * sizeof(T)) & 15u); };
   const int nchunks = P1 > P0 ? (int)((P1 - P0 + PC - 1) / PC) : 0;
   const T2* brv = reinterpret_cast<const T2*>(br);
   const T2* zv = reinterpret_cast<const T2*>(z);
@@ -910,11 +914,12 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     T2* sz = sb + (size_t)PC * br_px;
     unsigned char* sx = reinterpret_cast<unsigned char*>(sz + (size_t)PC * z_px);
     const unsigned nb = (unsigned)(np * br_px * sizeof(T2)), nz = (unsigned)(np * z_px * sizeof(T2));
-    const unsigned nx = x0 ? round16((unsigned)(np * B * sizeof(T))) : 0u;
+    const unsigned xo = x_off(pc);
+    const unsigned nx = x0 ? round16((unsigned)(np * B * sizeof(T)) + xo) : 0u;
     mbar_expect_tx(&bar[st], nb + nz + nx);
     bulk_g2s(sb, brv + pc * br_px, nb, &bar[st]);
     bulk_g2s(sz, zv + pc * z_px, nz, &bar[st]);
-    if (x0) bulk_g2s(sx, x0 + pc * B, nx, &bar[st]);
+    if (x0) bulk_g2s(sx, reinterpret_cast<const unsigned char*>(x0 + pc * B) - xo, nx, &bar[st]);
   };
   if (threadIdx.x == 0)
     for (int c = 0; c < min(nchunks, kProdStages); ++c) issue(c);
@@ -933,7 +938,8 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     const int np = (int)min((i64)PC, P1 - pc);
     const T2* sb = reinterpret_cast<const T2*>(stage0 + st * stage_bytes);
     const T2* sz = sb + (size_t)PC * br_px;
-    const T* sx = reinterpret_cast<const T*>(sz + (size_t)PC * z_px);
+    const T* sx = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(sz + (size_t)PC * z_px) +
+                                             x_off(pc));
     if (active) {
       if (kind == 0) {
         const int ra = (d1 * 4 + l1) * L + l3, rb = (d2 * 4 + 2 * hx) * L + l3;
@@ -1128,7 +1134,7 @@ template <typename T, int ND>
 __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
     i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0,
     const double* __restrict__ x0c, const uint8_t* __restrict__ mask, i64 chunk, int slots,
-    double* __restrict__ partials) {
+    double* __restrict__ partials, const i64* __restrict__ blk) {
   typedef typename V2<T>::type T2;
   constexpr int NF = p0_sums<ND>(), OFF = ND * 16 + ND * (ND - 1) / 2 * 32, ZB = OFF;  // (d, z) blocks start
   extern __shared__ __align__(16) double p0s[];  // [warps][4B][NF], then map sums [warps][B][2]
@@ -1154,7 +1160,8 @@ __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
       f[i] = (T)0;
     }
   };
-  const i64 p0 = (i64)blockIdx.x * chunk, p1 = min(N, p0 + chunk);
+  const i64 p0 = blk ? blk[blockIdx.x] : (i64)blockIdx.x * chunk;
+  const i64 p1 = blk ? blk[blockIdx.x + 1] : min(N, p0 + chunk);
   int cnt = 0;
   for (i64 base = p0 + (i64)warp * P; base < p1; base += (i64)nw * P) {
     const i64 p = base + pw;
@@ -1252,7 +1259,7 @@ void products0_launch(const ProductShape& sh, const T* z, const T* br, const T* 
   allow_dynamic_smem(k_products0<T, ND>);
   const i64 chunk = (sh.N + sh.blocks - 1) / sh.blocks;
   k_products0<T, ND><<<sh.blocks, 32 * nw, smem, s>>>(sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, x0c, mask, chunk,
-                                                      sh.slots, partials);
+                                                      sh.slots, partials, sh.d_blk);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1267,6 +1274,21 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
   }
 }
 
+// segments: sums[k stride + i] = sum over the ranges seg_blk[k] ..
+// seg_blk[k + 1] - 1 of partials[blk][i] in range order
+__global__ void k_reduce_segments(const double* __restrict__ partials, const int32_t* __restrict__ seg_blk, int nseg,
+                                  int rows, int slots, double* __restrict__ sums, size_t stride) {
+  const i64 total = (i64)rows * slots;
+  for (int k = blockIdx.y; k < nseg; k += gridDim.y) {
+    const int b0 = seg_blk[k], b1 = seg_blk[k + 1];
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (i64)gridDim.x * blockDim.x) {
+      double a = 0.0;
+      for (int j = b0; j < b1; ++j) a += partials[(i64)j * total + i];
+      sums[(size_t)k * stride + i] = a;
+    }
+  }
+}
+
 // gv = M v per pixel and l3 (M: K x K complex of the coefficient cotangents
 // of one (b, l3), in shared memory); gz additionally gets s1c z / |z| (auto
 // S1).  Thread (pixel, l3), l3 fastest, holds v in registers; CTAs stride
@@ -1278,22 +1300,25 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
                                                               const T* __restrict__ br, const T* __restrict__ M,
                                                               const T* __restrict__ s1c,
                                                               const uint8_t* __restrict__ mask, int accumulate,
-                                                              T* __restrict__ gz, T* __restrict__ gbr) {
+                                                              T* __restrict__ gz, T* __restrict__ gbr,
+                                                              const i64* __restrict__ blk,
+                                                              const int32_t* __restrict__ bseg) {
   extern __shared__ __align__(16) unsigned char smem[];
   typedef typename V2<T>::type T2;
   constexpr int L = 4, K1 = K - 1;
   T2* m = reinterpret_cast<T2*>(smem);  // [bs][L][K][K]
   // a CTA takes maps b0 .. b0 + bs - 1: thread (pixel, map, l3), l3 fastest,
   // so the maps of a pixel (contiguous rows) are read and written together
-  const int b0 = blockIdx.y * bs, t = threadIdx.x;
-  const T2* Mb = reinterpret_cast<const T2*>(M) + (i64)b0 * L * K * K;
+  // with a range table: the CTA's pixel range, inside segment sg
+  const int b0 = blockIdx.y * bs, t = threadIdx.x, sg = blk ? bseg[blockIdx.x] : 0;
+  const T2* Mb = reinterpret_cast<const T2*>(M) + ((i64)sg * B + b0) * L * K * K;
   for (int i = t; i < bs * L * K * K; i += kRevThreads) m[i] = Mb[i];
   __syncthreads();
   const int l3 = t & 3, bl = (t >> 2) % bs, px = (t >> 2) / bs, b = b0 + bl;
   const int TPX = kRevThreads / (4 * bs);
   if (px >= TPX) return;
   const T2* ml = m + (bl * L + l3) * K * K;
-  const T c1 = s1c[(i64)b * L + l3];
+  const T c1 = s1c[((i64)sg * B + b) * L + l3];
   const T2* brv = reinterpret_cast<const T2*>(br);
   const T2* zv = reinterpret_cast<const T2*>(z);
   T2* gbrv = reinterpret_cast<T2*>(gbr);
@@ -1301,15 +1326,17 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
   // PPT adjacent pixels per thread: every cotangent matrix entry read from
   // shared memory serves PPT pixels
   constexpr int PPT = K <= 21 ? 2 : 1;
-  for (i64 g = (i64)blockIdx.x * TPX + px; g * PPT < N; g += (i64)gridDim.x * TPX) {
+  const i64 lo = blk ? blk[blockIdx.x] : 0, hi = blk ? blk[blockIdx.x + 1] : N;
+  const i64 g0 = blk ? (i64)px : (i64)blockIdx.x * TPX + px, gstep = blk ? (i64)TPX : (i64)gridDim.x * TPX;
+  for (i64 g = g0; lo + g * PPT < hi; g += gstep) {
     T2 v[PPT][K];
     bool on[PPT];
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
-      const i64 p = g * PPT + q;
+      const i64 p = lo + g * PPT + q;
       const i64 row = (p * B + b) * K1;
-      on[q] = p < N && (!mask || mask[p]);
-      if (p < N && !on[q] && !accumulate) {  // outside the averaged pixels: no cotangent
+      on[q] = p < hi && (!mask || mask[p]);
+      if (p < hi && !on[q] && !accumulate) {  // outside the averaged pixels: no cotangent
         T2 zero;
         zero.x = (T)0; zero.y = (T)0;
         for (int i = 0; i < K1; ++i) gbrv[(row + i) * L + l3] = zero;
@@ -1340,7 +1367,7 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
 #pragma unroll
       for (int q = 0; q < PPT; ++q) {
         if (!on[q]) continue;
-        const i64 p = g * PPT + q;
+        const i64 p = lo + g * PPT + q;
         T2 o;
         T2* dst;
         if (i == K1) {
@@ -1368,12 +1395,20 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
 template <typename T, typename I>
 __global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restrict__ xc,
                                 const uint8_t* __restrict__ mask, const double* __restrict__ coefs, i64 N, int B,
-                                T* __restrict__ gx) {
+                                T* __restrict__ gx, const i64* __restrict__ seg, int nseg) {
   const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;
   if ((i64)i >= N * B) return;
   const I p = i / (I)B;
   if (mask && !mask[p]) return;
   const int b = (int)(i - p * (I)B);
+  if (seg) {  // the coefficients of p's segment
+    int a = 0, e = nseg;
+    while (e - a > 1) {
+      const int m = (a + e) >> 1;
+      if (seg[m] <= (i64)p) a = m; else e = m;
+    }
+    coefs += (size_t)a * 2 * B;
+  }
   const double x = (xc ? xc[b] : 0.0) + (double)x0[i];
   gx[i] += (T)(coefs[2 * b] + coefs[2 * b + 1] * x);
 }
@@ -1800,11 +1835,13 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
       for (int rp = 0; rp < reps[zc][k]; ++rp)
         sh.roles[(size_t)zc * W + w++] = chunk_roles[zc][k] | (rp << 16) | (reps[zc][k] << 24);
   }
-  // per pixel: operands and, at level 0, the maps; there the chunks and
-  // ranges are whole 16-byte units of the maps [N][B]
-  const size_t px_bytes = (size_t)B * sh.K * L * 2 * elem + (sh.level0 ? (size_t)B * elem : 0);
+  // per pixel: operands and, at level 0, the maps; there the uniform chunks
+  // and ranges are whole 16-byte units of the maps [N][B], and a stage
+  // holds 16 bytes more (ranges of a range table start anywhere)
+  const size_t op_bytes = (size_t)B * sh.K * L * 2 * elem, x_px = sh.level0 ? (size_t)B * elem : 0;
+  const size_t px_bytes = op_bytes + x_px;
   const int align = sh.level0 ? 16 / (int)std::gcd((size_t)16, (size_t)B * elem) : 1;
-  sh.px_chunk = (int)(kProdStageBytes / px_bytes) / align * align;
+  sh.px_chunk = (int)((kProdStageBytes - (sh.level0 ? 32 : 0)) / px_bytes) / align * align;
   if (sh.px_chunk < 1) throw std::runtime_error("a pixel's operands exceed a products stage");
   // one CTA per SM over (pixel ranges, role chunks); ranges of at least 4
   // pixel chunks
@@ -1812,11 +1849,54 @@ ProductShape product_shape(int n, int L, int B, i64 N, size_t elem) {
   const i64 most = std::max<i64>(1, N / (4 * (i64)sh.px_chunk));
   sh.blocks = (int)std::max<i64>(1, std::min(want, most));
   sh.chunk = ((N + sh.blocks - 1) / sh.blocks + align - 1) / align * align;
-  sh.smem = std::max((size_t)kProdStages * sh.px_chunk * px_bytes, (size_t)W * 32 * 6 * sizeof(double));
+  const size_t stage = (size_t)sh.px_chunk * op_bytes + (sh.level0 ? ((sh.px_chunk * x_px + 15) & ~(size_t)15) + 16 : 0);
+  sh.smem = std::max((size_t)kProdStages * stage, (size_t)W * 32 * 6 * sizeof(double));
   return sh;
 }
 
+// Forward ranges of about N / 296 pixels (2 per SM) and reverse ranges of
+// at most 2048 pixels, split evenly inside every segment.
+void segment_ranges(ProductShape& sh, const std::vector<i64>& seg) {
+  if (seg.size() < 2 || seg.front() != 0 || seg.back() != sh.N) throw std::runtime_error("bad segment table");
+  sh.nseg = (int)seg.size() - 1;
+  const i64 fwd = std::max<i64>(1024, (sh.N + 295) / 296), rev = 2048;
+  sh.blk.clear(); sh.rev_blk.clear(); sh.rev_seg.clear(); sh.seg_blk.clear();
+  for (int k = 0; k < sh.nseg; ++k) {
+    const i64 n = seg[k + 1] - seg[k];
+    if (n <= 0) throw std::runtime_error("empty segment");
+    const i64 nf = (n + fwd - 1) / fwd, nr = (n + rev - 1) / rev;
+    sh.seg_blk.push_back((int32_t)sh.blk.size());
+    for (i64 j = 0; j < nf; ++j) sh.blk.push_back(seg[k] + n * j / nf);
+    for (i64 j = 0; j < nr; ++j) {
+      sh.rev_blk.push_back(seg[k] + n * j / nr);
+      sh.rev_seg.push_back(k);
+    }
+  }
+  sh.blk.push_back(sh.N);
+  sh.rev_blk.push_back(sh.N);
+  sh.seg_blk.push_back((int32_t)sh.blk.size() - 1);
+  if (sh.blk.size() - 1 > (size_t)INT32_MAX || sh.rev_blk.size() - 1 > (size_t)INT32_MAX)
+    throw std::runtime_error("too many product ranges");
+  sh.blocks = (int)sh.blk.size() - 1;
+  sh.rev_blocks = (int)sh.rev_blk.size() - 1;
+}
+
 namespace {
+// partials [blocks][B L][slots] -> sums [B L][slots] (per segment with a
+// range table)
+void reduce_partials(const ProductShape& sh, const double* partials, double* sums, cudaStream_t s) {
+  const i64 total = (i64)sh.B * sh.L * sh.slots;
+  const unsigned gx = (unsigned)std::min<i64>((total + 255) / 256, 1024);
+  if (sh.d_seg_blk) {
+    dim3 grid(gx, (unsigned)std::min(sh.nseg, 65535));
+    k_reduce_segments<<<grid, 256, 0, s>>>(partials, sh.d_seg_blk, sh.nseg, sh.B * sh.L, sh.slots, sums,
+                                           sh.seg_stride);
+  } else {
+    k_reduce_partials<<<gx, 256, 0, s>>>(partials, sh.blocks, sh.B * sh.L, sh.slots, sums);
+  }
+  STL_CUDA(cudaGetLastError());
+}
+
 template <typename T, int K>
 void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T* M, const T* s1c,
                         const uint8_t* mask, bool accumulate, T* gz, T* gbr, cudaStream_t s) {
@@ -1828,10 +1908,11 @@ void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T
     allow_dynamic_smem(k_products_rev<T, K>);
   const int tpx = kRevThreads / (4 * bs) * (K <= 21 ? 2 : 1);  // pixels per CTA pass
   const i64 tiles = (sh.N + tpx - 1) / tpx;
-  const unsigned gx = (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 * bs / sh.B));
+  const unsigned gx = sh.d_rev_blk ? (unsigned)sh.rev_blocks
+                                   : (unsigned)std::max<i64>(1, std::min<i64>(tiles, (i64)148 * 8 * bs / sh.B));
   dim3 grid(gx, sh.B / bs);
   k_products_rev<T, K><<<grid, kRevThreads, smem, s>>>(sh.N, sh.B, bs, z, br, M, s1c, mask, accumulate ? 1 : 0,
-                                                       gz, gbr);
+                                                       gz, gbr, sh.d_rev_blk, sh.d_rev_seg);
 }
 }  // namespace
 
@@ -1845,10 +1926,7 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
   if (!moments && (sh.nd == 1 || sh.nd == 2) && 32 % (4 * sh.B) == 0 && (!sh.level0 || x0)) {
     if (sh.nd == 1) products0_launch<T, 1>(sh, z, br, x0, x0c, mask, partials, s);
     else products0_launch<T, 2>(sh, z, br, x0, x0c, mask, partials, s);
-    const i64 total = (i64)sh.B * L * sh.slots;
-    k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
-                                                                                          sh.B * L, sh.slots, sums);
-    STL_CUDA(cudaGetLastError());
+    reduce_partials(sh, partials, sums, s);
     return;
   }
   auto kern = moments ? k_products<T, true> : k_products<T, false>;
@@ -1856,12 +1934,9 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
     allow_dynamic_smem(kern);
   dim3 grid(sh.blocks, 1, sh.item_chunks);
   kern<<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots, sh.d_roles,
-                                             sh.warps, sh.px_chunk, sh.chunk, partials, err, x0c, mask);
+                                             sh.warps, sh.px_chunk, sh.chunk, partials, err, x0c, mask, sh.d_blk);
   STL_CUDA(cudaGetLastError());
-  const i64 total = (i64)sh.B * L * sh.slots;
-  k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, sh.blocks,
-                                                                                        sh.B * L, sh.slots, sums);
-  STL_CUDA(cudaGetLastError());
+  reduce_partials(sh, partials, sums, s);
 }
 
 template <typename T>
@@ -1885,9 +1960,108 @@ void products_reverse(const ProductShape& sh, const T* z, const T* br, const T* 
 
 template <typename T>
 void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const double* coefs, int B, i64 N, T* gx,
-                   cudaStream_t s) {
-  if (N * B < ((i64)1 << 31)) k_mean_var_grad<T, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx);
-  else k_mean_var_grad<T, i64><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx);
+                   cudaStream_t s, const i64* seg, int nseg) {
+  if (N * B < ((i64)1 << 31))
+    k_mean_var_grad<T, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx, seg, nseg);
+  else k_mean_var_grad<T, i64><<<nblocks(N * B, 256), 256, 0, s>>>(x0, xc, mask, coefs, N, B, gx, seg, nseg);
+  STL_CUDA(cudaGetLastError());
+}
+
+// ---- coefficients <-> sums ------------------------------------------------
+// The arithmetic below is that of a plain sequential FP64 loop: products and
+// sums rounded one by one (no fused multiply-add), so the results do not
+// depend on the device.
+__global__ void k_assemble(const double* __restrict__ sums, size_t mstride, const PlanSlots* __restrict__ plan,
+                           int np, const double* __restrict__ counts, int levels, int B, int K,
+                           double* __restrict__ values, double* __restrict__ var) {
+  const i64 total = (i64)B * K * np;
+  for (i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x; o < total; o += (i64)gridDim.x * blockDim.x) {
+    const int i = (int)(o % np);
+    const i64 bk = o / np;
+    const int k = (int)(bk % K), b = (int)(bk / K);
+    const PlanSlots p = plan[i];
+    const double* row = sums + (size_t)k * mstride + p.base + (i64)b * p.stride;
+    const double N = counts[(size_t)k * levels + p.level];
+    const double vr = row[p.re] / N, vi = p.im >= 0 ? row[p.im] / N : 0.0;
+    values[2 * o] = vr;
+    values[2 * o + 1] = vi;
+    if (var) {
+      const double m2 = __dadd_rn(__dmul_rn(vr, vr), __dmul_rn(vi, vi));
+      var[o] = fmax(__dsub_rn(row[p.second] / N, m2), 0.0);
+    }
+  }
+}
+
+__device__ __forceinline__ void add_source(const double* g, int mode, double N, double& ar, double& ai) {
+  if (mode == 2) {
+    ar = __dadd_rn(ar, __dmul_rn(2.0, g[0]) / N);
+  } else {
+    ar = __dadd_rn(ar, g[0] / N);
+    ai = __dadd_rn(ai, (mode ? -g[1] : g[1]) / N);
+  }
+}
+
+template <typename U>
+__global__ void k_build_cot(const double* __restrict__ cot, int np, int B, int K, const double* __restrict__ counts,
+                            int levels, int n, int Kd, int L, const CotSources* __restrict__ src,
+                            const CotSources* __restrict__ s1src, U* __restrict__ M, U* __restrict__ s1) {
+  const int E = L * Kd * Kd, per = E + L;  // matrix entries, then the S1 scales, of one (k, b)
+  const i64 total = (i64)K * B * per;
+  for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
+    const int e = (int)(t % per);
+    const i64 kb = t / per;  // k B + b
+    const int k = (int)(kb / B), b = (int)(kb % B);
+    const CotSources c = e < E ? src[e] : s1src[e - E];
+    const double N = counts[(size_t)k * levels + n];
+    const double* g = cot + 2 * ((i64)b * K + k) * np;
+    double ar = 0.0, ai = 0.0;
+    if (c.i0 >= 0) add_source(g + 2 * (i64)c.i0, c.m0, N, ar, ai);
+    if (c.i1 >= 0) add_source(g + 2 * (i64)c.i1, c.m1, N, ar, ai);
+    if (e < E) {
+      U* m = M + 2 * (kb * E + e);
+      m[0] = (U)ar;
+      m[1] = (U)ai;
+    } else {
+      s1[kb * L + (e - E)] = (U)ar;
+    }
+  }
+}
+
+__global__ void k_build_mean_var(const double* __restrict__ cot, int np, int B, int K,
+                                 const double* __restrict__ counts, int levels, int i_mean, int i_var,
+                                 double* __restrict__ mv) {
+  const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (i64)K * B) return;
+  const int k = (int)(t / B), b = (int)(t % B);
+  const double N = counts[(size_t)k * levels];
+  const double* g = cot + 2 * ((i64)b * K + k) * np;
+  double a = 0.0, v = 0.0;
+  if (i_mean >= 0) a = __dadd_rn(a, g[2 * (i64)i_mean] / N);
+  if (i_var >= 0) v = __dadd_rn(v, __dmul_rn(2.0, g[2 * (i64)i_var]) / N);
+  mv[2 * t] = a;
+  mv[2 * t + 1] = v;
+}
+
+void assemble_values(const double* sums, size_t mask_stride, const PlanSlots* plan, int np, const double* counts,
+                     int levels, int B, int K, double* values, double* var, cudaStream_t s) {
+  const i64 total = (i64)B * K * np;
+  k_assemble<<<(unsigned)std::max<i64>(1, std::min<i64>(nblocks(total, 256), 148 * 16)), 256, 0, s>>>(
+      sums, mask_stride, plan, np, counts, levels, B, K, values, var);
+  STL_CUDA(cudaGetLastError());
+}
+
+template <typename U>
+void build_cotangents(const double* cot, int np, int B, int K, const double* counts, int levels, int n, int Kd,
+                      int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s) {
+  const i64 total = (i64)K * B * (L * Kd * Kd + L);
+  k_build_cot<U><<<(unsigned)std::max<i64>(1, std::min<i64>(nblocks(total, 256), 148 * 16)), 256, 0, s>>>(
+      cot, np, B, K, counts, levels, n, Kd, L, src, s1src, M, s1);
+  STL_CUDA(cudaGetLastError());
+}
+
+void build_mean_var(const double* cot, int np, int B, int K, const double* counts, int levels, int i_mean, int i_var,
+                    double* mv, cudaStream_t s) {
+  k_build_mean_var<<<nblocks((i64)K * B, 256), 256, 0, s>>>(cot, np, B, K, counts, levels, i_mean, i_var, mv);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -1960,8 +2134,10 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, const uint8_t*, \
                                     bool, T*, T*, cudaStream_t);                                                                \
   template void mean_var_grad<T>(const T*, const double*, const uint8_t*, const double*, int, i64, T*,           \
-                                 cudaStream_t);            \
+                                 cudaStream_t, const i64*, int);                                                  \
   template void row_means<T>(const T*, bool, bool, i64, int, double*, double*, cudaStream_t);                     \
+  template void build_cotangents<T>(const double*, int, int, int, const double*, int, int, int, int,             \
+                                    const CotSources*, const CotSources*, T*, T*, cudaStream_t);                 \
   template void moduli_deviations<T>(const T*, i64, int, int, const double*, T*, int, int, int, cudaStream_t);
 INST(float)
 INST(double)

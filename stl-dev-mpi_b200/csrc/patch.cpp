@@ -4,20 +4,19 @@
 // A disc's support (level 0: the NESTED pixels whose centre lies within the
 // angle R of the centre; level d + 1: the parents of level d) and its core
 // (the pixels within the core radius, then their parents) are built on the
-// host (crates/stl-core/src/disc.rs:62-140); every selected disc then runs
-// on a grid-mode engine (engine.cu): wavelets bound to the support with the
-// binding threshold 1e-9, decimations restricted to it, coefficients
-// averaged over the core.  Supports are cached by (centre, radius, core);
-// each selected disc has its own engine (a disc selected twice gets two),
-// built at its first forward.  The discs' engines run concurrently: host
-// threads take discs in turn, each thread launching on its own stream, so
-// the many small launches of different discs overlap on the GPU.
+// host (crates/stl-core/src/disc.rs:62-140) and cached by (centre, radius,
+// core).  The selected discs then run batched: consecutive discs, up to
+// group_pixels level-0 pixels in all, form one grid-mode engine (engine.cu)
+// whose support is the concatenation of their supports, one segment per
+// disc -- wavelets bound to the disc's support with the binding threshold
+// 1e-9, decimations restricted to it, coefficients averaged over its core
+// -- so that every kernel of a sweep is one launch over all the discs of a
+// group.  The engines of a selection are built at its first forward and
+// kept while the same discs are selected again.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <array>
-#include <atomic>
-#include <functional>
 #include <cmath>
 #include <cstring>
 #include <deque>
@@ -146,8 +145,25 @@ uint64_t bits(double x) {
 
 struct CachedDisc {
   Support support;
-  std::vector<std::unique_ptr<Engine>> engines;  // one per occurrence in the selection
 };
+
+// the supports of discs one after the other, one segment each
+Support concatenate(const std::vector<const Support*>& discs, int levels) {
+  Support s;
+  s.ids.resize(levels);
+  s.core.resize(levels);
+  s.seg.resize(levels);
+  for (int d = 0; d < levels; ++d) {
+    s.seg[d].push_back(0);
+    for (const Support* q : discs) {
+      const i64 off = (i64)s.ids[d].size();
+      s.ids[d].insert(s.ids[d].end(), q->ids[d].begin(), q->ids[d].end());
+      for (i64 c : q->core[d]) s.core[d].push_back(off + c);
+      s.seg[d].push_back((i64)s.ids[d].size());
+    }
+  }
+  return s;
+}
 
 template <typename R, typename F>
 R guard(R fail, F&& f) {
@@ -173,80 +189,60 @@ struct StlpPatchHandle {
   int levels = 0;
   size_t capacity = 256;
   int threads = 1;
+  i64 group_pixels = i64(1) << 23;  // level-0 pixels of one batched engine (at least one disc)
   std::map<Key, std::shared_ptr<CachedDisc>> cache;
   std::deque<Key> order;
   long hits = 0, misses = 0;
-  std::vector<std::pair<std::shared_ptr<CachedDisc>, int>> selected;  // disc, occurrence
+  std::vector<std::shared_ptr<CachedDisc>> selected;
+  std::vector<Key> selected_keys;
+  // consecutive selected discs first .. first + count - 1, level-0 pixels
+  // from offset, in one segmented engine
+  struct Group {
+    size_t first = 0, count = 0;
+    i64 offset = 0;
+    std::unique_ptr<Engine> engine;
+  };
+  std::vector<Group> groups;
+  std::vector<Key> group_keys;  // the selection the groups were built for
   bool has_current = false;
   uint64_t current = 0;
-  int nstreams = 8;
-  std::vector<cudaStream_t> streams;
-  ~StlpPatchHandle() {
-    for (cudaStream_t s : streams) cudaStreamDestroy(s);
-  }
+  bool profile = false;  // time every launch of the engines (CUDA events)
 
-  // the engine of selected disc i, built (on stream s) at its first use;
-  // the caller has sized the disc's engine list (reserve_engines)
-  Engine& engine(size_t i, cudaStream_t s = nullptr) {
-    auto& d = *selected[i].first;
-    const int k = selected[i].second;
-    if (!d.engines[k]) {
-      Options o = opt;
-      o.B = 1;
-      if (cudaSetDevice(opt.device) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
-      std::unique_ptr<Engine> e = Engine::create_patch(o, d.support);
-      e->set_stream(s);
-      e->prepare();
-      d.engines[k] = std::move(e);
-    }
-    return *d.engines[k];
-  }
-  void reserve_engines() {
-    for (auto& sel : selected)
-      while ((int)sel.first->engines.size() <= sel.second) sel.first->engines.push_back(nullptr);
-  }
-  size_t size(size_t i) const { return selected[i].first->support.ids[0].size(); }
-  // f(disc index, its engine) for every selected disc: up to nstreams
-  // threads take the discs in turn, each on its own non-blocking stream
-  // (building a disc's engine there at its first use); the first error is
-  // rethrown once every thread has stopped.
-  void for_discs(const std::function<void(size_t, Engine&)>& f) {
-    reserve_engines();
-    if (cudaSetDevice(opt.device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
-      throw std::runtime_error("device synchronisation before the disc sweep failed");
-    const int T = (int)std::min<size_t>((size_t)std::max(1, nstreams), selected.size());
-    while ((int)streams.size() < T) {
-      cudaStream_t st;
-      if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
-        throw std::runtime_error("stream creation failed");
-      streams.push_back(st);
-    }
-    std::atomic<size_t> next{0};
-    std::vector<std::string> errors(T);
-    auto work = [&](int t) {
-      try {
-        if (cudaSetDevice(opt.device) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
-        for (size_t i = next++; i < selected.size(); i = next++) {
-          Engine& e = engine(i, streams[t]);
-          e.set_stream(streams[t]);
-          f(i, e);
-        }
-      } catch (const std::exception& ex) {
-        errors[t] = ex.what();
-        next = selected.size();
-      }
-    };
-    std::vector<std::thread> pool;
-    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto& th : pool) th.join();
-    for (const auto& e : errors)
-      if (!e.empty()) throw std::runtime_error(e);
-  }
+  size_t size(size_t i) const { return selected[i]->support.ids[0].size(); }
   size_t total() const {
     size_t t = 0;
     for (size_t i = 0; i < selected.size(); ++i) t += size(i);
     return t;
+  }
+  // the engines of the current selection, built at its first use
+  std::vector<Group>& engines() {
+    if (!groups.empty() && group_keys == selected_keys) return groups;
+    groups.clear();
+    group_keys.clear();
+    if (cudaSetDevice(opt.device) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
+    i64 off = 0;
+    for (size_t i = 0; i < selected.size();) {
+      Group g;
+      g.first = i;
+      g.offset = off;
+      i64 px = 0;
+      std::vector<const Support*> discs;
+      while (i < selected.size() && (discs.empty() || px + (i64)size(i) <= group_pixels)) {
+        discs.push_back(&selected[i]->support);
+        px += (i64)size(i);
+        ++i;
+      }
+      g.count = discs.size();
+      off += px;
+      Options o = opt;
+      o.B = 1;
+      g.engine = Engine::create_patch(o, concatenate(discs, levels));
+      g.engine->set_profiling(profile);
+      g.engine->prepare();
+      groups.push_back(std::move(g));
+    }
+    group_keys = selected_keys;
+    return groups;
   }
 };
 
@@ -271,8 +267,9 @@ StlpPatchHandle* stlp_patch_new(const char* config) {
     h->capacity = (size_t)v.integer("cache", 256);
     const long long t = v.integer("threads", 0);
     h->threads = t > 0 ? (int)t : std::max(1, (int)std::thread::hardware_concurrency());
-    h->nstreams = (int)v.integer("streams", 8);
-    require(h->nstreams >= 1 && h->nstreams <= 64, "streams must be 1 to 64");
+    h->group_pixels = (i64)v.integer("group_pixels", (long long)h->group_pixels);
+    h->profile = v.boolean("profile", false);
+    require(h->group_pixels >= 1, "group_pixels must be positive");
     // validates nside, J, L, kernel as the full-sky engine does
     std::unique_ptr<Engine> probe = Engine::create(h->opt);
     h->plan = probe->plan();
@@ -290,6 +287,31 @@ char* stlp_patch_info(StlpPatchHandle* h) {
     js << "{\"version\": \"stl-b200-patch-0.1\", \"nside\": " << h->opt.nside << ", \"j\": " << h->opt.J
        << ", \"levels\": " << h->levels << ", \"channels\": 1, \"cross\": false, \"dtype\": \""
        << (h->opt.fp32 ? "float32" : "float64") << "\", \"fewer\": false, \"threads\": " << h->threads
+       << ", \"group_pixels\": " << h->group_pixels << ", \"groups\": " << h->groups.size();
+    // the engines' timers and kernel classes, summed
+    double fwd = 0.0, rev = 0.0, build = 0.0;
+    std::vector<KernelStat> ks;
+    for (const auto& g : h->groups) {
+      fwd += g.engine->timers.forward_ms;
+      rev += g.engine->timers.reverse_ms;
+      build += g.engine->timers.build_s;
+      auto k = g.engine->kernel_stats();
+      if (ks.empty()) ks = k;
+      else
+        for (size_t i = 0; i < ks.size() && i < k.size(); ++i) {
+          ks[i].launches += k[i].launches;
+          ks[i].ms += k[i].ms;
+          ks[i].bytes += k[i].bytes;
+          ks[i].flops += k[i].flops;
+        }
+    }
+    js << ", \"timers\": {\"build_s\": " << build << ", \"forward_ms\": " << fwd << ", \"reverse_ms\": " << rev
+       << "}, \"kernels\": [";
+    for (size_t i = 0; i < ks.size(); ++i)
+      js << (i ? ", " : "") << "{\"name\": \"" << ks[i].name << "\", \"launches\": " << ks[i].launches
+         << ", \"ms\": " << ks[i].ms << ", \"bytes\": " << ks[i].bytes << "}";
+    js << "]";
+    js
        << ", \"backend\": \"gpu\", \"cache\": {\"capacity\": " << h->capacity << ", \"entries\": " << h->cache.size()
        << ", \"hits\": " << h->hits << ", \"misses\": " << h->misses << "}, \"selected\": [";
     for (size_t i = 0; i < h->selected.size(); ++i) js << (i ? ", " : "") << h->size(i);
@@ -327,6 +349,7 @@ static int select_discs(StlpPatchHandle* h, const double* centres, size_t b, con
     require(h != nullptr && centres != nullptr && counts != nullptr, "null argument");
     h->has_current = false;
     h->selected.clear();
+    h->selected_keys.clear();
     require(b > 0, "empty batch");
     std::vector<Key> keys(b);
     std::vector<std::array<double, 3>> unit(b);
@@ -381,8 +404,8 @@ static int select_discs(StlpPatchHandle* h, const double* centres, size_t b, con
       h->cache[keys[missing[k]]] = d;
       h->order.push_back(keys[missing[k]]);
     }
-    std::map<Key, int> seen;
-    for (size_t i = 0; i < b; ++i) h->selected.push_back({h->cache.at(keys[i]), seen[keys[i]]++});
+    for (size_t i = 0; i < b; ++i) h->selected.push_back(h->cache.at(keys[i]));
+    h->selected_keys = keys;
     // the cache keeps the last `capacity` discs (selected ones stay alive here)
     while (h->cache.size() > h->capacity && !h->order.empty()) {
       h->cache.erase(h->order.front());
@@ -414,7 +437,7 @@ int stlp_patch_ids(StlpPatchHandle* h, size_t i, int64_t* out) {
   return guard<int>(-1, [&] {
     require(h != nullptr && out != nullptr, "null argument");
     require(i < h->selected.size(), "disc index out of range");
-    const auto& ids = h->selected[i].first->support.ids[0];
+    const auto& ids = h->selected[i]->support.ids[0];
     std::memcpy(out, ids.data(), ids.size() * sizeof(int64_t));
     return 0;
   });
@@ -424,7 +447,7 @@ int stlp_patch_core_pixels(StlpPatchHandle* h, size_t* out) {
   return guard<int>(-1, [&] {
     require(h != nullptr && out != nullptr, "null argument");
     for (size_t i = 0; i < h->selected.size(); ++i)
-      for (int n = 0; n < h->levels; ++n) out[i * h->levels + n] = h->selected[i].first->support.core[n].size();
+      for (int n = 0; n < h->levels; ++n) out[i * h->levels + n] = h->selected[i]->support.core[n].size();
     return 0;
   });
 }
@@ -437,15 +460,14 @@ static int patch_forward(StlpPatchHandle* h, const double* x_host, uint64_t x_de
   require(!h->selected.empty(), "no disc selected");
   require(n == h->total(), "input shape mismatch");
   const size_t np = h->plan.size();
-  std::vector<size_t> off(h->selected.size() + 1, 0);
-  for (size_t i = 0; i < h->selected.size(); ++i) off[i + 1] = off[i] + h->size(i);
   if (x_host)
     for (size_t q = 0; q < n; ++q) require(std::isfinite(x_host[q]), "input patch contains non-finite values");
-  h->for_discs([&](size_t i, Engine& e) {
-    if (x_host) e.load_host(x_host + off[i]);
-    else e.load_device(reinterpret_cast<const double*>(x_dev) + off[i], false);
-    e.forward(moments, out + 2 * i * np, moments ? var + i * np : nullptr);
-  });
+  for (auto& g : h->engines()) {
+    Engine& e = *g.engine;
+    if (x_host) e.load_host(x_host + g.offset);
+    else e.load_device(reinterpret_cast<const double*>(x_dev) + g.offset, false);
+    e.forward(moments, out + 2 * g.first * np, moments ? var + g.first * np : nullptr);
+  }
   h->has_current = true;
   h->current = generation;
   return 0;
@@ -473,12 +495,11 @@ static int patch_vjp(StlpPatchHandle* h, const double* cot, size_t n, uint64_t g
   require(h->has_current && h->current == generation, "stale forward state");
   const size_t np = h->plan.size();
   require(n == h->selected.size() * np, "cotangent shape mismatch");
-  std::vector<size_t> off(h->selected.size() + 1, 0);
-  for (size_t i = 0; i < h->selected.size(); ++i) off[i + 1] = off[i] + h->size(i);
-  h->for_discs([&](size_t i, Engine& e) {
-    if (out_host) e.reverse_host(cot + 2 * i * np, out_host + off[i]);
-    else e.reverse_device(cot + 2 * i * np, reinterpret_cast<double*>(out_dev) + off[i], false);
-  });
+  for (auto& g : h->engines()) {
+    Engine& e = *g.engine;
+    if (out_host) e.reverse_host(cot + 2 * g.first * np, out_host + g.offset);
+    else e.reverse_device(cot + 2 * g.first * np, reinterpret_cast<double*>(out_dev) + g.offset, false);
+  }
   return 0;
 }
 

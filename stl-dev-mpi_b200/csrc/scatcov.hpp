@@ -54,13 +54,18 @@ struct KernelStat {
   double ms = 0.0, bytes = 0.0, flops = 0.0;
 };
 
-// A disc patch (or any sky region) of the engine's grid mode: per level the
-// sorted NESTED ids of the support (level d + 1: the parents of level d)
-// and the positions in them of the pixels the coefficients average (the
-// core).
+// Sky regions of the engine's grid mode (disc patches): per level the NESTED
+// ids of the support (level d + 1: the parents of level d) and the
+// ascending positions in them of the pixels the coefficients average (the
+// core).  The support may hold several regions one after the other
+// (segments): seg[d] gives their starts in ids[d] and, last, its size
+// (empty: one region).  Every segment is sorted and unique; the wavelets
+// and decimations of a segment read its own cells only, and every segment
+// has its own coefficients, averaged over its own core pixels.
 struct Support {
   std::vector<std::vector<int64_t>> ids;
   std::vector<std::vector<int64_t>> core;
+  std::vector<std::vector<int64_t>> seg;
 };
 
 class Engine {
@@ -79,6 +84,8 @@ class Engine {
   // pixels a coefficient of native level d averages
   i64 ncore(int d) const { return ncore_[d]; }
   bool grid_mode() const { return !support_.ids.empty(); }
+  // regions of the support (1 on the full sky)
+  int segments() const { return support_.seg.empty() ? 1 : (int)support_.seg[0].size() - 1; }
   const Support& support() const { return support_; }
   bool fp32() const { return opt_.fp32; }
 

@@ -530,9 +530,14 @@ class PatchEngine:
     (NESTED pixel ids at nside, or vectors [B, 3]), radius and optional core
     radius in degrees; the coefficients average the core (else the whole disc)."""
 
-    def __init__(self, nside, j, kernel=5, orientations=4, dtype="float64", device=0, cache=256, threads=0):
+    def __init__(self, nside, j, kernel=5, orientations=4, dtype="float64", device=0, cache=256, threads=0,
+                 group_pixels=None, profile=False):
         cfg = dict(nside=int(nside), j=int(j), kernel=int(kernel), orientations=int(orientations), backend="gpu",
                    dtype=dtype, device=int(device), cache=int(cache), threads=int(threads))
+        if group_pixels is not None:  # level-0 pixels of the discs one batched engine holds
+            cfg["group_pixels"] = int(group_pixels)
+        if profile:  # per kernel class device times in info()["kernels"]
+            cfg["profile"] = True
         self._lib = lib()
         self._mutex = threading.RLock()
         self._handle = self._lib.stlp_patch_new(json.dumps(cfg).encode())

@@ -98,3 +98,50 @@ def test_fp32_disc_within_1e6(stl):
                     worst = max(worst, float(np.max(np.abs(part(a) - part(r)) / (1e-6 * scale + 1e-6 * np.abs(part(r))))))
     print(f"patch FP32 vs FP64: worst ratio to the 1e-6 family tolerance {worst:.3f}")
     assert worst <= 1.0
+
+
+def test_batched_discs_match_one_engine_per_disc(stl):
+    """Discs of different sizes (one selected twice, cores on some) in one
+    segmented engine, in two groups, and one engine per disc: the same
+    statistics and cotangents (FP64, summation order only), and the FP32
+    batch within the 1e-6 criterion of the FP64 one."""
+    nside, J = 64, 4
+    centres = np.array([10, 9000, 30000, 47000, 9000, 21000, 300], dtype=np.int64)
+    radii = np.array([9.0, 25.0, 14.0, 30.0, 25.0, 6.0, 18.0])
+    cores = np.array([0.0, 15.0, 0.0, 20.0, 15.0, 0.0, 10.0])
+    rng = np.random.default_rng(11)
+    runs = {}
+    for name, kw in (("batch", {}), ("single", {"group_pixels": 1}), ("groups", {"group_pixels": 6000}),
+                     ("batch32", {"dtype": "float32"})):
+        pe = stl.PatchEngine(nside, J, **({"dtype": "float64"} | kw))
+        ids = pe.select(centres, radii, cores)
+        if name == "batch":
+            patches = [np.exp(rng.standard_normal(i.size) - 0.5).astype(np.float32).astype(np.float64) for i in ids]
+            cot = rng.uniform(-1, 1, (len(ids), pe.ncoeff)) + 1j * rng.uniform(-1, 1, (len(ids), pe.ncoeff))
+        v, var = pe.forward(patches, moments=True, generation=3)
+        g = pe.vjp(cot, generation=3)
+        runs[name] = (v, var, g, pe.info()["groups"])
+        plan = pe.plan
+        pe.close()
+    assert runs["batch"][3] == 1 and runs["single"][3] == len(centres) and 1 < runs["groups"][3] < len(centres)
+    v, var, g, _ = runs["batch"]
+    for name in ("single", "groups"):
+        v2, var2, g2, _ = runs[name]
+        assert close_ratio(v2, v, 1e-13, 1e-12) <= 1.0
+        assert close_ratio(var2, var, 1e-13, 1e-12) <= 1.0
+        for a, b in zip(g2, g):
+            assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+    v32 = runs["batch32"][0]
+    fam = np.array([c["family"] for c in plan])
+    lev = np.array([c["native_dg"] for c in plan])
+    for k in range(len(centres)):
+        for f in set(fam):
+            for n in set(lev):
+                sel = (fam == f) & (lev == n)
+                if not sel.any():
+                    continue
+                r, a = v[k, sel], v32[k, sel]
+                scale = np.max(np.abs(r))
+                for part in (np.real, np.imag):
+                    assert np.max(np.abs(part(a) - part(r)) / (1e-6 * scale + 1e-6 * np.abs(part(r)))) <= 1.0
+        assert np.max(np.abs(runs["batch32"][2][k] - g[k])) <= 1e-5 * np.max(np.abs(g[k]))
