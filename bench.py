@@ -310,7 +310,9 @@ def run_synthesis(args, torch, dist, world, rank, dev):
                 "config": {"workload": "synthesis nside1024 J9 L4 m10, lognormal target seed 7, start seed 8",
                            "evaluations": res["n"], "loss_first": float(losses[0]),
                            "loss_last": float(losses[-1]), "parallelism": f"replicas x{world}",
-                           "graph": "none: the line search branches on host scalars"},
+                           "graph": "iterations 2 on: one CUDA graph launch each (curvature pair, two-loop "
+                                    "recursion, first line-search trial, objective and VJP); the host runs "
+                                    "the strong Wolfe test on one copy of scalars"},
                 # the maps cross PCIe once per run (start in, result out): per iteration
                 "e2e": {"value": world * iters / (ms_e2e / 1e3), "unit": "iterations/s",
                         "h2d_bytes_per_step": int(npix * 8 / iters), "d2h_bytes_per_step": int(npix * 8 / iters)},

@@ -165,6 +165,7 @@ Options parse_options(const char* json) {
   o.tol_grad = v.real("tolerance_grad", 1e-12);
   o.tol_change = v.real("tolerance_change", 1e-15);
   o.history = v.integer("history_size", 10);
+  o.graph = v.boolean("graph", true);
   if (o.history <= 0 || !(o.lr > 0.0) || !std::isfinite(o.lr)) throw std::runtime_error("invalid L-BFGS options");
   return o;
 }

@@ -49,9 +49,10 @@ struct Options {
   double lr = 1.0;
   long long max_iter = 20, max_eval = -1, history = 10;
   double tol_grad = 1e-12, tol_change = 1e-15;
+  bool graph = true;  // device synthesis: iterations 2 on as one CUDA graph launch each
 };
 // options JSON (lr, max_iter, max_eval, tolerance_grad, tolerance_change,
-// history_size), validated; throws on invalid values
+// history_size, graph), validated; throws on invalid values
 Options parse_options(const char* json);
 
 template <typename Vec>
@@ -61,11 +62,20 @@ struct LineResult {
   long long evals;
 };
 
+// the search's first evaluation when the caller made it already: loss f and
+// gradient g at x0 + t d, g.d = gtd, and max |d_i| = d_norm
+template <typename Vec>
+struct FirstTrial {
+  double f, gtd, d_norm;
+  const Vec* g;
+};
+
 // strong Wolfe search along d from x0 (loss f, gradient g, g.d = gtd)
 template <typename Ops, typename Obj>
 LineResult<typename Ops::Vec> strong_wolfe(Ops& ops, Obj& obj, const typename Ops::Vec& x0,
                                            const typename Ops::Vec& d, double t, double f,
-                                           const typename Ops::Vec& g, double gtd, long long max_ls, size_t n) {
+                                           const typename Ops::Vec& g, double gtd, long long max_ls, size_t n,
+                                           const FirstTrial<typename Ops::Vec>* first = nullptr) {
   typedef typename Ops::Vec Vec;
   const double c1 = 1e-4, c2 = 0.9, tol = 1e-9;
   max_ls = std::max(max_ls, 0LL);
@@ -76,10 +86,18 @@ LineResult<typename Ops::Vec> strong_wolfe(Ops& ops, Obj& obj, const typename Op
     ++evals;
     return obj(xt, gout);
   };
-  const double d_norm = ops.abs_max(d);
+  const double d_norm = first ? first->d_norm : ops.abs_max(d);
   Vec g_new = ops.make(n);
-  double f_new = eval(t, g_new);
-  double gtd_new = ops.dot(g_new, d);
+  double f_new, gtd_new;
+  if (first) {
+    ++evals;
+    f_new = first->f;
+    ops.copy(g_new, *first->g);
+    gtd_new = first->gtd;
+  } else {
+    f_new = eval(t, g_new);
+    gtd_new = ops.dot(g_new, d);
+  }
   double t_prev = 0.0, f_prev = f, gtd_prev = gtd;
   Vec g_prev = ops.make(n);
   ops.copy(g_prev, g);

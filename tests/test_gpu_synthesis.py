@@ -85,3 +85,35 @@ def test_device_synthesis_refuses_bad_shapes(stl):
     with pytest.raises(ValueError, match="CUDA float64"):
         e.synthesize(x.float(), np.zeros(e.ncoeff, complex))
     e.close()
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_graph_iterations_equal_step_by_step(stl, dtype):
+    """Iterations 2 on as one CUDA graph launch each (the default) take the
+    same steps as the step-by-step device path: the same losses after every
+    evaluation and the same iterate, bit for bit (same reductions, same
+    order); with FP64 both follow the host L-BFGS."""
+    import torch
+    nside, J = 32, 4
+    rng = np.random.default_rng(12)
+    target_map = np.exp(rng.standard_normal((1, 12 * nside * nside)) - 0.5)
+    x0 = rng.standard_normal((1, 12 * nside * nside)) * target_map.std() + target_map.mean()
+    e = stl.NativeEngine(nside, J, dtype=dtype)
+    target, var = e.forward(target_map, moments=True)
+    w = 1.0 / np.maximum(var.reshape(-1), 1e-12 * var.max())
+    opts = dict(max_iter=12, history_size=4)
+    runs = {}
+    for graph in (False, True):
+        xd = torch.tensor(x0, device="cuda")
+        n, losses = e.synthesize(xd, target, weights=w, options=dict(opts, graph=graph))
+        runs[graph] = (n, losses, xd.cpu().numpy())
+    assert runs[True][0] == runs[False][0] > 12
+    np.testing.assert_array_equal(runs[True][1], runs[False][1])
+    np.testing.assert_array_equal(runs[True][2], runs[False][2])
+    assert runs[True][1][-1] < 0.5 * runs[True][1][0]
+    if dtype == "float64":
+        xh, rep = stl.native_lbfgs(stl.synthesis_objective(e, target, weights=w), x0.copy(), opts)
+        want = np.array(rep["loss_history"])
+        assert len(want) == runs[True][0]
+        assert np.max(np.abs(runs[True][1] - want) / want) <= 1e-9
+    e.close()
