@@ -116,6 +116,7 @@ StlpHandle* stlp_new(const char* config) {
     std::string dtype = v.string("dtype", "float64");
     require(dtype == "float64" || dtype == "float32", "dtype must be float64 or float32");
     o.fp32 = dtype == "float32";
+    o.autotune = v.boolean("autotune", true);
     require(!v.boolean("cross", false), "cross statistics (two channels) are not built in this library");
     require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
     require(o.nside > 0 && (o.nside & (o.nside - 1)) == 0, "nside must be a power of two");
@@ -194,6 +195,13 @@ char* stlp_info(StlpHandle* h) {
     for (size_t i = 0; i < ol.size(); ++i)
       js << (i ? ", " : "") << "{\"slots\": " << ol[i][0] << ", \"tile_cells\": " << ol[i][1]
          << ", \"coloured\": " << (ol[i][2] ? "true" : "false") << "}";
+    js << "], \"tile_heights\": [";
+    auto th = e.tile_heights();
+    for (size_t i = 0; i < th.size(); ++i) {
+      js << (i ? ", " : "") << "[";
+      for (size_t k = 0; k < th[i].size(); ++k) js << (k ? ", " : "") << th[i][k];
+      js << "]";
+    }
     js << "]";
     js << ", \"plan\": [";
     const auto& plan = e.plan();

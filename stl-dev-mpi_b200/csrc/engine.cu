@@ -20,8 +20,12 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <mutex>
 #include <set>
+#include <sstream>
+#include <string>
 
 #include "engine.cuh"
 #include "scatcov.hpp"
@@ -497,6 +501,7 @@ class EngineImpl final : public Engine {
       field_bytes_ += adj_part_.bytes;
     }
     STL_CUDA(cudaStreamSynchronize(stream_));
+    tune();
     ready_ = true;
     timers.build_s += ms_since(t0) / 1000.0;
   }
@@ -596,20 +601,9 @@ class EngineImpl final : public Engine {
   void forward(bool moments, double* values, double* var) override {
     if (!loaded_) throw std::runtime_error("forward before the maps were loaded");
     auto t0 = std::chrono::steady_clock::now();
-    const int L = opt_.L, B = opt_.B;
+    const int B = opt_.B;
     cudaStream_t s = stream_;
-    for (int d = 0; d + 1 < levels_ && !levels_given_; ++d)
-      prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[d], B, false), dec_flops(dec_[d], B, false), s, [&] {
-        typed(d, [&](auto ti) {
-          typed(d + 1, [&](auto to) {
-            using Ui = typename decltype(ti)::type;
-            using Uo = typename decltype(to)::type;
-            dec_apply<Ui, Uo>(dec_[d], false, X_[d].as<Ui>(), B, 0, X_[d + 1].as<Uo>(), B, 0, 1, B, false, s);
-          });
-        });
-      });
-    for (int n = 0; n < levels_; ++n)
-      typed(n, [&](auto t) { forward_level<typename decltype(t)::type>(n, moments); });
+    forward_sweep(moments);
     // the coefficients (and variances) of every map and mask, from the sums
     const size_t nv = (size_t)B * K_ * plan_.size();
     assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
@@ -630,6 +624,61 @@ class EngineImpl final : public Engine {
     timers.forwards += 1;
   }
 
+  // the forward launches: pyramid, then every level's fields and sums
+  void forward_sweep(bool moments) {
+    const int B = opt_.B;
+    cudaStream_t s = stream_;
+    for (int d = 0; d + 1 < levels_ && !levels_given_; ++d)
+      prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[d], B, false), dec_flops(dec_[d], B, false), s, [&] {
+        typed(d, [&](auto ti) {
+          typed(d + 1, [&](auto to) {
+            using Ui = typename decltype(ti)::type;
+            using Uo = typename decltype(to)::type;
+            dec_apply<Ui, Uo>(dec_[d], false, X_[d].as<Ui>(), B, 0, X_[d + 1].as<Uo>(), B, 0, 1, B, false, s,
+                              tile(d, T_DEC_X));
+          });
+        });
+      });
+    for (int n = 0; n < levels_; ++n)
+      typed(n, [&](auto t) { forward_level<typename decltype(t)::type>(n, moments); });
+  }
+
+  void set_objective(const double* target, const double* weights) override {
+    prepare();
+    const size_t nv = (size_t)opt_.B * K_ * plan_.size(), np = plan_.size();
+    target_dev_.alloc(16 * nv);
+    STL_CUDA(cudaMemcpyAsync(target_dev_.p, target, 16 * nv, cudaMemcpyHostToDevice, stream_));
+    weights_dev_.release();
+    if (weights) {
+      weights_dev_.alloc(8 * np);
+      STL_CUDA(cudaMemcpyAsync(weights_dev_.p, weights, 8 * np, cudaMemcpyHostToDevice, stream_));
+    }
+    STL_CUDA(cudaStreamSynchronize(stream_));
+    objective_set_ = true;
+  }
+
+  void objective(const double* x, double* g, double* loss) override {
+    if (!objective_set_) throw std::runtime_error("objective before set_objective");
+    cudaStream_t s = stream_;
+    const int B = opt_.B;
+    load_maps(x);
+    forward_sweep(false);
+    const i64 nv = (i64)B * K_ * plan_.size();
+    assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
+                    counts_dev_.as<double>(), levels_, B, K_, vals_dev_.as<double>(), nullptr, s);
+    objective_terms(vals_dev_.as<double>(), target_dev_.as<double>(),
+                    weights_dev_.p ? weights_dev_.as<double>() : nullptr, nv, (int)plan_.size(),
+                    cot_dev_.as<double>(), loss, s);
+    reverse_launches();
+    typed(0, [&](auto t) {
+      using U = typename decltype(t)::type;
+      to_map_major<U, double>(gX_[0].as<U>(), g, npix(0), B, s);
+    });
+    forward_done_ = true;
+  }
+
+  int* error_flag() override { return err_.as<int>(); }
+
   template <typename U>
   void forward_level(int n, bool moments) {
     const int L = opt_.L, B = opt_.B;
@@ -639,7 +688,7 @@ class EngineImpl final : public Engine {
     const ConvOp& op = conv_[n];
     prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, false), conv_flops(op, B), s, [&] {
       conv_forward<U>(op, X_[n].as<U>(), B, Z_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(),
-                      xc_.as<double>() + (size_t)n * B);
+                      xc_.as<double>() + (size_t)n * B, tile(n, T_FWD_Z));
     });
     // |z| as deviations from their means per (map, orientation)
     double* zc = zc_.as<double>() + (size_t)n * B * L;
@@ -653,13 +702,14 @@ class EngineImpl final : public Engine {
                      typed(n - 1, [&](auto ti) {
                        using Ui = typename decltype(ti)::type;
                        dec_apply<Ui, U>(dec_[n - 1], false, Mod_[n - 1].as<Ui>(), B * n * L, n * L, mod,
-                                        B * (n + 1) * L, (n + 1) * L, B, n * L, false, s);
+                                        B * (n + 1) * L, (n + 1) * L, B, n * L, false, s, tile(n, T_DEC_MOD));
                      });
                    });
     const int R = B * (n + 1) * L;
     branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s);
     prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
-      conv_forward<U>(op, mod, R, Br_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>());
+      conv_forward<U>(op, mod, R, Br_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>(),
+                      tile(n, T_FWD_BR));
     });
     const ProductShape& sh = shapes_[n];
     const double E = sh.K * (sh.K + 1) / 2.0;
@@ -704,11 +754,13 @@ class EngineImpl final : public Engine {
   }
   void reset_kernel_stats() override { prof_.reset(); }
   void set_profiling(bool on) override { prof_.on = on; }
+  bool profiling() const override { return prof_.on; }
   std::vector<double> mean_slots() const override {
     std::vector<double> v;
     for (const auto& c : conv_) v.push_back(c.mean_slots);
     return v;
   }
+  std::vector<std::array<int, 8>> tile_heights() const override { return tiles_; }
   std::vector<std::array<int, 3>> operator_layout() const override {
     std::vector<std::array<int, 3>> v;
     for (const auto& c : conv_) v.push_back({c.S, c.max_tile_cells, c.colored ? 1 : 0});
@@ -782,6 +834,23 @@ class EngineImpl final : public Engine {
   // the reverse sweep from the coefficient cotangents in cot_dev_
   void reverse_sweep() {
     auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t s = stream_;
+    reverse_launches();
+    int err = 0;
+    STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    STL_CUDA(cudaStreamSynchronize(s));
+    prof_.collect();
+    if (err) {
+      STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
+      throw std::runtime_error("a wait on a staged device copy timed out in the reverse sweep");
+    }
+    timers.reverse_ms += ms_since(t0);
+    timers.reverses += 1;
+  }
+
+  // the reverse launches: cotangent matrices, then the levels descending and
+  // the mean / variance terms into gX_[0]
+  void reverse_launches() {
     const int L = opt_.L, B = opt_.B;
     const int np = (int)plan_.size();
     cudaStream_t s = stream_;
@@ -811,16 +880,6 @@ class EngineImpl final : public Engine {
                            npix(0), gX_[0].as<U>(), s, segmented() ? seg_dev_[0].as<i64>() : nullptr, K_);
         });
       });
-    int err = 0;
-    STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    STL_CUDA(cudaStreamSynchronize(s));
-    prof_.collect();
-    if (err) {
-      STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
-      throw std::runtime_error("a wait on a staged device copy timed out in the reverse sweep");
-    }
-    timers.reverse_ms += ms_since(t0);
-    timers.reverses += 1;
   }
 
   // one level of the reverse sweep (field type U); M: the level's cotangent
@@ -839,7 +898,7 @@ class EngineImpl final : public Engine {
                      typed(n + 1, [&](auto ti) {
                        using Ui = typename decltype(ti)::type;
                        dec_apply<Ui, U>(dec_[n], true, gMod_[n + 1].as<Ui>(), B * (n + 2) * L, (n + 2) * L, gmod,
-                                        B * (n + 1) * L, (n + 1) * L, B, (n + 1) * L, false, s);
+                                        B * (n + 1) * L, (n + 1) * L, B, (n + 1) * L, false, s, tile(n, T_DECT_MOD));
                      });
                    });
     else
@@ -860,7 +919,10 @@ class EngineImpl final : public Engine {
     const int R = B * (n + 1) * L;
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), R, adj_ptr()) ? 2 : 1,
                  conv_bytes(op, R, false, true), conv_flops(op, R), s,
-                 [&] { conv_adjoint<U>(op, gBr_.as<U>(), R, gmod, true, s, adj_ptr(), err_.as<int>()); });
+                 [&] {
+                   conv_adjoint<U>(op, gBr_.as<U>(), R, gmod, true, s, adj_ptr(), err_.as<int>(), nullptr,
+                                   tile(n, T_ADJ_BR));
+                 });
     // the modulus VJP of z (gZ += gmod z / |z|): inside the coloured adjoint
     // of z when the operator has it, else its own pass
     ModulusAdd<U> madd;
@@ -876,7 +938,7 @@ class EngineImpl final : public Engine {
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), B, adj_ptr()) ? 2 : 1,
                  conv_bytes(op, B, false, false), conv_flops(op, B), s, [&] {
                    conv_adjoint<U>(op, gZ_.as<U>(), B, gX_[n].as<U>(), false, s, adj_ptr(), err_.as<int>(),
-                                   fuse ? &madd : nullptr);
+                                   fuse ? &madd : nullptr, tile(n, T_ADJ_Z));
                  });
     if (n + 1 < levels_)
       prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
@@ -884,7 +946,7 @@ class EngineImpl final : public Engine {
                      typed(n + 1, [&](auto ti) {
                        using Ui = typename decltype(ti)::type;
                        dec_apply<Ui, U>(dec_[n], true, gX_[n + 1].as<Ui>(), B, 0, gX_[n].as<U>(), B, 0, 1, B, true,
-                                        s);
+                                        s, tile(n, T_DECT_X));
                      });
                    });
   }
@@ -992,6 +1054,8 @@ class EngineImpl final : public Engine {
   DevMem plan_dev_, counts_dev_, vals_dev_, var_dev_, cot_dev_, cotsrc_dev_;
   std::vector<size_t> cotsrc_off_;  // per level: first cotangent source entry
   int i_mean_ = -1, i_var_ = -1;    // plan entries of the mean and the variance
+  DevMem target_dev_, weights_dev_;  // the synthesis objective
+  bool objective_set_ = false;
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
   std::vector<DevMem> ids_dev_;  // grid mode: supports per level
   // averaging masks [k][level] (grid mode: the core; none: every pixel) and
@@ -1003,6 +1067,140 @@ class EngineImpl final : public Engine {
   const uint8_t* mask(int k, int n) const {
     return kmask_.empty() ? nullptr : kmask_[kmask_.size() == 1 ? 0 : k][n].as<uint8_t>();
   }
+  // tile heights per level and launch (0: the default)
+  enum { T_FWD_Z, T_FWD_BR, T_ADJ_BR, T_ADJ_Z, T_DEC_X, T_DEC_MOD, T_DECT_MOD, T_DECT_X };
+  std::vector<std::array<int, 8>> tiles_;
+  int tile(int n, int k) const { return tiles_.empty() ? 0 : tiles_[n][k]; }
+
+  // The tile heights, by timing: every valid height of a launch runs once to
+  // warm up and three times between CUDA events, on the engine's own
+  // buffers (cleared first: the timing reads zeros), and the fastest is
+  // kept.  The choice does not change any result.  A process-wide table
+  // keyed by the launch's geometry spares engines of the same shapes the
+  // timing.
+  void tune() {
+    tiles_.assign(levels_, std::array<int, 8>{});
+    if (!opt_.autotune) return;
+    const int L = opt_.L, B = opt_.B;
+    cudaStream_t s = stream_;
+    for (int n = 0; n < levels_; ++n)
+      for (DevMem* f : {&X_[n], &Z_[n], &Mod_[n], &Br_[n], &gMod_[n], &gX_[n]})
+        STL_CUDA(cudaMemsetAsync(f->p, 0, f->bytes, s));
+    STL_CUDA(cudaMemsetAsync(gZ_.p, 0, gZ_.bytes, s));
+    STL_CUDA(cudaMemsetAsync(gBr_.p, 0, gBr_.bytes, s));
+    for (DevMem* c : {&xc_, &zc_, &rc_}) STL_CUDA(cudaMemsetAsync(c->p, 0, c->bytes, s));
+    int dev = 0;
+    STL_CUDA(cudaGetDevice(&dev));
+    cudaEvent_t ea, eb;
+    STL_CUDA(cudaEventCreate(&ea));
+    STL_CUDA(cudaEventCreate(&eb));
+    auto pick = [&](const char* what, const ConvOp* op, const DecOp* dop, int R, const std::vector<int>& cand,
+                    const std::function<void(int)>& run) -> int {
+      if (cand.size() < 2) return 0;
+      std::ostringstream k;
+      k << dev << '|' << what << '|' << opt_.fp32 << '|' << R << '|' << B;
+      if (op) k << '|' << op->n_rep << '|' << op->S << '|' << op->nk << '|' << op->colored << '|' << op->max_tile_cells;
+      if (dop) k << '|' << dop->n_rep_out << '|' << dop->n_rep_in << '|' << dop->W << '|' << dop->WT << '|' << dop->nk;
+      const std::string key = k.str();
+      {
+        std::lock_guard<std::mutex> g(tune_mu());
+        auto it = tune_cache().find(key);
+        if (it != tune_cache().end()) return it->second;
+      }
+      int best = cand.back();
+      float best_ms = 0.f;
+      for (int c : cand) {
+        run(c);
+        STL_CUDA(cudaEventRecord(ea, s));
+        for (int r = 0; r < 3; ++r) run(c);
+        STL_CUDA(cudaEventRecord(eb, s));
+        STL_CUDA(cudaEventSynchronize(eb));
+        float ms = 0.f;
+        STL_CUDA(cudaEventElapsedTime(&ms, ea, eb));
+        if (c == cand.front() || ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
+      }
+      std::lock_guard<std::mutex> g(tune_mu());
+      tune_cache()[key] = best;
+      return best;
+    };
+    try {
+      for (int n = 0; n < levels_; ++n)
+        typed(n, [&](auto t) {
+          using U = typename decltype(t)::type;
+          const ConvOp& op = conv_[n];
+          const size_t e = esz(n);
+          const int R = B * (n + 1) * L;
+          int* err = err_.as<int>();
+          U* mod = Mod_[n].as<U>();
+          U* gmod = gMod_[n].as<U>();
+          tiles_[n][T_FWD_Z] = pick("fz", &op, nullptr, B, conv_forward_choices(op, e, B, true), [&](int rb) {
+            conv_forward<U>(op, X_[n].as<U>(), B, Z_[n].as<U>(), nullptr, 0, 0, 0, s, err,
+                            xc_.as<double>() + (size_t)n * B, rb);
+          });
+          tiles_[n][T_FWD_BR] = pick("fb", &op, nullptr, R, conv_forward_choices(op, e, R, true), [&](int rb) {
+            conv_forward<U>(op, mod, R, Br_[n].as<U>(), nullptr, 0, 0, 0, s, err, rc_.as<double>(), rb);
+          });
+          tiles_[n][T_ADJ_BR] = pick("ab", &op, nullptr, R, conv_adjoint_choices(op, e, R, adj_ptr()), [&](int rb) {
+            conv_adjoint<U>(op, gBr_.as<U>(), R, gmod, true, s, adj_ptr(), err, nullptr, rb);
+          });
+          ModulusAdd<U> madd;
+          madd.z = Z_[n].as<U>();
+          madd.g = gmod + n * L;
+          madd.g_pix = B * (n + 1) * L;
+          madd.g_row = (n + 1) * L;
+          const bool fuse = conv_adjoint_fuses_modulus(op, e, B, adj_ptr(), err);
+          tiles_[n][T_ADJ_Z] = pick(fuse ? "azm" : "az", &op, nullptr, B, conv_adjoint_choices(op, e, B, adj_ptr()),
+                                    [&](int rb) {
+                                      conv_adjoint<U>(op, gZ_.as<U>(), B, gX_[n].as<U>(), false, s, adj_ptr(), err,
+                                                      fuse ? &madd : nullptr, rb);
+                                    });
+          if (n > 0)
+            typed(n - 1, [&](auto ti) {
+              using Ui = typename decltype(ti)::type;
+              tiles_[n][T_DEC_MOD] =
+                  pick("dm", nullptr, &dec_[n - 1], n * L, dec_choices(esz(n - 1), n * L), [&](int rb) {
+                    dec_apply<Ui, U>(dec_[n - 1], false, Mod_[n - 1].as<Ui>(), B * n * L, n * L, mod, B * (n + 1) * L,
+                                     (n + 1) * L, B, n * L, false, s, rb);
+                  });
+            });
+          if (n + 1 < levels_)
+            typed(n + 1, [&](auto tn) {
+              using Un = typename decltype(tn)::type;
+              tiles_[n][T_DEC_X] = pick("dx", nullptr, &dec_[n], B, dec_choices(e, B), [&](int rb) {
+                dec_apply<U, Un>(dec_[n], false, X_[n].as<U>(), B, 0, X_[n + 1].as<Un>(), B, 0, 1, B, false, s, rb);
+              });
+              tiles_[n][T_DECT_MOD] =
+                  pick("tm", nullptr, &dec_[n], (n + 1) * L, dec_choices(esz(n + 1), (n + 1) * L), [&](int rb) {
+                    dec_apply<Un, U>(dec_[n], true, gMod_[n + 1].as<Un>(), B * (n + 2) * L, (n + 2) * L, gmod,
+                                     B * (n + 1) * L, (n + 1) * L, B, (n + 1) * L, false, s, rb);
+                  });
+              tiles_[n][T_DECT_X] = pick("tx", nullptr, &dec_[n], B, dec_choices(esz(n + 1), B), [&](int rb) {
+                dec_apply<Un, U>(dec_[n], true, gX_[n + 1].as<Un>(), B, 0, gX_[n].as<U>(), B, 0, 1, B, true, s, rb);
+              });
+            });
+        });
+    } catch (...) {
+      cudaEventDestroy(ea);
+      cudaEventDestroy(eb);
+      throw;
+    }
+    STL_CUDA(cudaEventDestroy(ea));
+    STL_CUDA(cudaEventDestroy(eb));
+    STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
+    STL_CUDA(cudaStreamSynchronize(s));
+  }
+  static std::mutex& tune_mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::map<std::string, int>& tune_cache() {
+    static std::map<std::string, int> c;
+    return c;
+  }
+
   // several regions: one launch covers the sums of all of them
   bool segmented() const { return grid_mode() && segments() > 1; }
   int launch_sets() const { return segmented() ? 1 : K_; }

@@ -215,9 +215,13 @@ void build_dec(const DecSpec& spec, DType dtype, DecOp& out, cudaStream_t stream
 //  tables use the tiled forward; otherwise the per-row gather.  rc (R FP64
 //  constants, or null): the input rows are deviations from rc, whose
 //  response rc x rowsum is added to the outputs.
+//  rb: rows of the field a thread takes (the tile height of the launch); 0
+//  picks the default, else one of conv_forward_choices.  Results do not
+//  depend on it: every output row is computed alone, in the same order.
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                  cudaStream_t s, int* err = nullptr, const double* rc = nullptr);
+                  cudaStream_t s, int* err = nullptr, const double* rc = nullptr, int rb = 0);
+std::vector<int> conv_forward_choices(const ConvOp& op, size_t elem, int R, bool err);
 //  With scratch, operators in the coloured layout use the coloured adjoint
 //  (bounded waits on its bulk copies set *err on timeout), other operators
 //  with tile tables the two-phase adjoint; otherwise the transposed gather.
@@ -233,12 +237,15 @@ struct ModulusAdd {
 bool conv_adjoint_fuses_modulus(const ConvOp& op, size_t elem, int R, const AdjScratch* scr, int* err);
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
-                  const AdjScratch* scr = nullptr, int* err = nullptr, const ModulusAdd<T>* madd = nullptr);
+                  const AdjScratch* scr = nullptr, int* err = nullptr, const ModulusAdd<T>* madd = nullptr,
+                  int rb = 0);
+std::vector<int> conv_adjoint_choices(const ConvOp& op, size_t elem, int R, const AdjScratch* scr);
 //    Input and output types may differ (FP32 and FP64 levels); the sums are
 //    in the operator's type.
 template <typename Tin, typename Tout>
 void dec_apply(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x_outer, Tout* y, int y_pix,
-               int y_outer, int R_outer, int R_inner, bool accumulate, cudaStream_t s);
+               int y_outer, int R_outer, int R_inner, bool accumulate, cudaStream_t s, int rb = 0);
+std::vector<int> dec_choices(size_t elem_in, int R_inner);
 // gz[p][b][l] += g z / |z|, z and gz [N][B][L] complex, g at p g_pix + b g_row + l
 template <typename T>
 void modulus_vjp_add(const T* z, const T* g, int g_pix, int g_row, T* gz, i64 N, int B, int L, cudaStream_t s);
@@ -328,6 +335,10 @@ struct CotSources {
 template <typename U>
 void build_cotangents(const double* cot, int np, int B, int K, const double* counts, int levels, int n, int Kd,
                       int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s);
+// Synthesis terms: cot_o = 2 w (v_o - t_o) and *loss = sum_o w |v_o - t_o|^2
+// (w = weights[o mod np], or 1) over nv complex values, in a fixed order.
+void objective_terms(const double* values, const double* target, const double* weights, i64 nv, int np,
+                     double* cot, double* loss, cudaStream_t s);
 // mv [K][B][2]: the scales of the mean (plan entry i_mean) and variance
 // (i_var) cotangents of every map
 void build_mean_var(const double* cot, int np, int B, int K, const double* counts, int levels, int i_mean, int i_var,

@@ -1654,8 +1654,15 @@ void ell_rb(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o
 
 template <typename Tin, typename Tout, typename Tw, int NK>
 void ell_nk(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o2_in, const Tin* x, int x_pix,
-            int x_outer, Tout* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s) {
-  if (R_inner % 4 == 0 && sizeof(Tin) == 4)
+            int x_outer, Tout* y, int y_pix, int y_outer, int R_outer, int R_inner, bool acc, cudaStream_t s,
+            int rb) {
+  if (rb == 1)
+    ell_rb<Tin, Tout, Tw, NK, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
+                                 R_inner, acc, s);
+  else if (rb == 2)
+    ell_rb<Tin, Tout, Tw, NK, 2>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
+                                 R_inner, acc, s);
+  else if (rb == 4 || (R_inner % 4 == 0 && sizeof(Tin) == 4))
     ell_rb<Tin, Tout, Tw, NK, 4>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer,
                                  R_inner, acc, s);
   else if (R_inner % 2 == 0)
@@ -1668,7 +1675,7 @@ void ell_nk(const int32_t* col, const Tw* w, int W, i64 n_rep, int o2_out, int o
 
 template <typename Tin, typename Tout, typename Tw>
 void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x_outer, Tout* y, int y_pix,
-                 int y_outer, int R_outer, int R_inner, bool accumulate, cudaStream_t s) {
+                 int y_outer, int R_outer, int R_inner, bool accumulate, cudaStream_t s, int rb) {
   const int32_t* col = transpose ? op.tcol.as<int32_t>() : op.col.as<int32_t>();
   const Tw* w = transpose ? op.tw.as<Tw>() : op.w.as<Tw>();
   const int W = transpose ? op.WT : op.W;
@@ -1676,10 +1683,10 @@ void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x
   const int o2_out = transpose ? op.o2 : op.co2, o2_in = transpose ? op.co2 : op.o2;
   if (op.nk == 4)
     ell_nk<Tin, Tout, Tw, 4>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner,
-                             accumulate, s);
+                             accumulate, s, rb);
   else
     ell_nk<Tin, Tout, Tw, 1>(col, w, W, n_rep, o2_out, o2_in, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner,
-                             accumulate, s);
+                             accumulate, s, rb);
 }
 
 // cotangent rows per CTA: FP32 up to 4 (coloured) or 2; FP64 1 (the
@@ -1712,20 +1719,57 @@ void conv_forward_tiles_rb(const ConvOp& op, const T* x, int R, T* out, T* mod, 
                                                           op.tile_slots.as<int32_t>());
 }
 
+bool forward_tiles(const ConvOp& op, size_t elem, bool err);
+
 template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
-                  cudaStream_t s, int* err, const double* rc) {
+                  cudaStream_t s, int* err, const double* rc, int rb) {
   if (rc && !op.rowsum.p) throw std::runtime_error("wavelet operator without row sums");
-  constexpr int RBmax = sizeof(T) == 4 ? 4 : 2;
-  const int RB = R % RBmax == 0 ? RBmax : (R % 2 == 0 ? 2 : 1);
-  const bool fits = (RB == RBmax ? fwd_tiles_smem<T, RBmax>(op) : fwd_tiles_smem<T, 2>(op)) <= 220 * 1024;
-  if (err && op.nk == 4 && op.adj_tiles && op.lcell_t.p && fits) {
-    if (RB == RBmax) conv_forward_tiles_rb<T, RBmax>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
-    else if (RB == 2) conv_forward_tiles_rb<T, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+  const std::vector<int> ok = conv_forward_choices(op, sizeof(T), R, err != nullptr);
+  if (ok.empty() || (rb && std::find(ok.begin(), ok.end(), rb) == ok.end()))
+    throw std::runtime_error("invalid wavelet tile height");
+  if (!rb) rb = ok.back();  // default: the tallest tile
+  if (forward_tiles(op, sizeof(T), err != nullptr)) {
+    if (rb == 4) conv_forward_tiles_rb<T, sizeof(T) == 4 ? 4 : 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err,
+                                                                  rc, s);
+    else if (rb == 2) conv_forward_tiles_rb<T, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
     else conv_forward_tiles_rb<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
-  } else if (op.nk == 4) conv_forward_nk<T, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
-  else conv_forward_nk<T, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+  } else if (op.nk == 4) {
+    if (rb == 2) conv_forward_rb<T, 4, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+    else conv_forward_rb<T, 4, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+  } else {
+    if (rb == 4) conv_forward_rb<T, 1, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+    else if (rb == 2) conv_forward_rb<T, 1, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+    else conv_forward_rb<T, 1, 1>(op, x, R, out, mod, mod_pix, mod_row, mod_off, rc, s);
+  }
   STL_CUDA(cudaGetLastError());
+}
+
+// the tiled forward serves full-sky operators with tile tables when its
+// shared memory fits at the smallest tile height
+bool forward_tiles(const ConvOp& op, size_t elem, bool err) {
+  if (!err || op.nk != 4 || !op.adj_tiles || !op.lcell_t.p) return false;
+  return (elem == 4 ? fwd_tiles_smem<float, 1>(op) : fwd_tiles_smem<double, 1>(op)) <= 220 * 1024;
+}
+
+// valid tile heights (rows of the field per thread) of a wavelet launch
+std::vector<int> conv_forward_choices(const ConvOp& op, size_t elem, int R, bool err) {
+  std::vector<int> v;
+  const bool tiles = forward_tiles(op, elem, err);
+  for (int rb : {1, 2, 4}) {
+    if (R % rb) continue;
+    if (tiles) {
+      if (rb == 4 && elem != 4) continue;
+      const size_t sm = elem == 4 ? (rb == 4 ? fwd_tiles_smem<float, 4>(op) : rb == 2 ? fwd_tiles_smem<float, 2>(op)
+                                                                                        : fwd_tiles_smem<float, 1>(op))
+                                  : (rb == 2 ? fwd_tiles_smem<double, 2>(op) : fwd_tiles_smem<double, 1>(op));
+      if (sm > 220 * 1024) continue;
+    } else if (op.nk == 4 && rb == 4) {
+      continue;
+    }
+    v.push_back(rb);
+  }
+  return v;
 }
 
 size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R) {
@@ -1748,32 +1792,78 @@ bool conv_adjoint_fuses_modulus(const ConvOp& op, size_t elem, int R, const AdjS
 
 template <typename T>
 void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, cudaStream_t s,
-                  const AdjScratch* scr, int* err, const ModulusAdd<T>* madd) {
+                  const AdjScratch* scr, int* err, const ModulusAdd<T>* madd, int rb) {
   if (madd && !conv_adjoint_fuses_modulus(op, sizeof(T), R, scr, err))
     throw std::runtime_error("this adjoint cannot add the modulus VJP");
+  if (rb) {
+    const std::vector<int> ok = conv_adjoint_choices(op, sizeof(T), R, scr);
+    if (std::find(ok.begin(), ok.end(), rb) == ok.end()) throw std::runtime_error("invalid adjoint tile height");
+  }
   if (adjoint_tiles_usable(op, sizeof(T), R, scr)) {
-    const int rb = adj_rb(op, sizeof(T), R);
+    if (!rb) rb = adj_rb(op, sizeof(T), R);
     if (rb == 4) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 4 : 1>(op, gy, R, gx, accumulate, *scr, s, err, madd);
     else if (rb == 2) conv_adjoint_tiles_rb<T, sizeof(T) == 4 ? 2 : 1>(op, gy, R, gx, accumulate, *scr, s, err, madd);
     else conv_adjoint_tiles_rb<T, 1>(op, gy, R, gx, accumulate, *scr, s, err, madd);
   } else if (op.colored) {
     throw std::runtime_error("the coloured adjoint needs scratch for its tile partials");
-  } else if (op.nk == 4) conv_adjoint_nk<T, 4>(op, gy, R, gx, accumulate, s);
-  else conv_adjoint_nk<T, 1>(op, gy, R, gx, accumulate, s);
+  } else {
+    if (!rb) rb = R % 2 == 0 ? 2 : 1;
+    if (op.nk == 4) {
+      if (rb == 2) conv_adjoint_rb<T, 4, 2>(op, gy, R, gx, accumulate, s);
+      else conv_adjoint_rb<T, 4, 1>(op, gy, R, gx, accumulate, s);
+    } else {
+      if (rb == 4) conv_adjoint_rb<T, 1, sizeof(T) == 4 ? 4 : 2>(op, gy, R, gx, accumulate, s);
+      else if (rb == 2) conv_adjoint_rb<T, 1, 2>(op, gy, R, gx, accumulate, s);
+      else conv_adjoint_rb<T, 1, 1>(op, gy, R, gx, accumulate, s);
+    }
+  }
   STL_CUDA(cudaGetLastError());
+}
+
+// valid tile heights of an adjoint launch
+std::vector<int> conv_adjoint_choices(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
+  std::vector<int> v;
+  const bool tiles = adjoint_tiles_usable(op, elem, R, scr);
+  for (int rb : {1, 2, 4}) {
+    if (R % rb) continue;
+    if (tiles) {
+      if (elem != 4 && rb > 1) continue;
+      if (!op.colored && rb == 4) continue;
+      if (op.colored && elem == 4 &&
+          (rb == 4 ? adjc_smem<float, 4>(op) : rb == 2 ? adjc_smem<float, 2>(op) : adjc_smem<float, 1>(op)) >
+              227 * 1024)
+        continue;
+    } else if (rb == 4 && (op.nk == 4 || elem != 4)) {
+      continue;
+    }
+    v.push_back(rb);
+  }
+  return v;
 }
 
 template <typename Tin, typename Tout>
 void dec_apply(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x_outer, Tout* y, int y_pix, int y_outer,
-               int R_outer, int R_inner, bool accumulate, cudaStream_t s) {
+               int R_outer, int R_inner, bool accumulate, cudaStream_t s, int rb) {
   if (R_outer <= 0 || R_inner <= 0) return;
+  if (rb) {
+    const std::vector<int> ok = dec_choices(sizeof(Tin), R_inner);
+    if (std::find(ok.begin(), ok.end(), rb) == ok.end()) throw std::runtime_error("invalid decimation tile height");
+  }
   if (op.dtype == DType::F64)
     dec_apply_w<Tin, Tout, double>(op, transpose, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
-                                   s);
+                                   s, rb);
   else
     dec_apply_w<Tin, Tout, float>(op, transpose, x, x_pix, x_outer, y, y_pix, y_outer, R_outer, R_inner, accumulate,
-                                  s);
+                                  s, rb);
   STL_CUDA(cudaGetLastError());
+}
+
+// valid tile heights of a decimation launch
+std::vector<int> dec_choices(size_t elem_in, int R_inner) {
+  std::vector<int> v;
+  for (int rb : {1, 2, 4})
+    if (R_inner % rb == 0 && (rb < 4 || elem_in == 4)) v.push_back(rb);
+  return v;
 }
 
 template <typename T>
@@ -2042,6 +2132,36 @@ __global__ void k_build_mean_var(const double* __restrict__ cot, int np, int B, 
   mv[2 * t + 1] = v;
 }
 
+constexpr int kObjThreads = 1024;
+__global__ void __launch_bounds__(kObjThreads) k_objective(const double* __restrict__ v, const double* __restrict__ t,
+                                                           const double* __restrict__ w, i64 nv, int np,
+                                                           double* __restrict__ cot, double* __restrict__ loss) {
+  __shared__ double red[kObjThreads];
+  const i64 chunk = (nv + kObjThreads - 1) / kObjThreads;
+  const i64 lo = (i64)threadIdx.x * chunk, hi = min(nv, lo + chunk);
+  double acc = 0.0;
+  for (i64 o = lo; o < hi; ++o) {
+    const double ww = w ? w[o % np] : 1.0;
+    const double rr = __dsub_rn(v[2 * o], t[2 * o]), ri = __dsub_rn(v[2 * o + 1], t[2 * o + 1]);
+    acc = __dadd_rn(acc, __dmul_rn(ww, __dadd_rn(__dmul_rn(rr, rr), __dmul_rn(ri, ri))));
+    cot[2 * o] = __dmul_rn(__dmul_rn(2.0, ww), rr);
+    cot[2 * o + 1] = __dmul_rn(__dmul_rn(2.0, ww), ri);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int h = kObjThreads / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] = __dadd_rn(red[threadIdx.x], red[threadIdx.x + h]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *loss = red[0];
+}
+
+void objective_terms(const double* values, const double* target, const double* weights, i64 nv, int np,
+                     double* cot, double* loss, cudaStream_t s) {
+  k_objective<<<1, kObjThreads, 0, s>>>(values, target, weights, nv, np, cot, loss);
+  STL_CUDA(cudaGetLastError());
+}
+
 void assemble_values(const double* sums, size_t mask_stride, const PlanSlots* plan, int np, const double* counts,
                      int levels, int B, int K, double* values, double* var, cudaStream_t s) {
   const i64 total = (i64)B * K * np;
@@ -2125,9 +2245,9 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
 
 #define INST(T)                                                                                                   \
   template void conv_forward<T>(const ConvOp&, const T*, int, T*, T*, int, int, int, cudaStream_t, int*,          \
-                                const double*);               \
+                                const double*, int);                                                              \
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*, int*,        \
-                                const ModulusAdd<T>*);                            \
+                                const ModulusAdd<T>*, int);                                                           \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
   template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
                                     const uint8_t*, double*, double*, int*, cudaStream_t, bool);                                                                \
@@ -2142,13 +2262,13 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
 INST(float)
 INST(double)
 template void dec_apply<float, float>(const DecOp&, bool, const float*, int, int, float*, int, int, int, int, bool,
-                                     cudaStream_t);
+                                     cudaStream_t, int);
 template void dec_apply<double, double>(const DecOp&, bool, const double*, int, int, double*, int, int, int, int,
-                                       bool, cudaStream_t);
+                                       bool, cudaStream_t, int);
 template void dec_apply<float, double>(const DecOp&, bool, const float*, int, int, double*, int, int, int, int, bool,
-                                      cudaStream_t);
+                                      cudaStream_t, int);
 template void dec_apply<double, float>(const DecOp&, bool, const double*, int, int, float*, int, int, int, int, bool,
-                                      cudaStream_t);
+                                      cudaStream_t, int);
 template void convert<double, float>(const double*, float*, i64, cudaStream_t);
 template void convert<float, double>(const float*, double*, i64, cudaStream_t);
 template void convert<double, double>(const double*, double*, i64, cudaStream_t);

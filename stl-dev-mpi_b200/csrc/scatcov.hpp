@@ -37,6 +37,7 @@ struct Options {
   int ksz = 5;
   bool fp32 = false;  // compute precision of the fields (sums are FP64 in both)
   int device = 0;
+  bool autotune = true;  // time the tile heights of the wavelet and decimation launches at prepare
 };
 
 struct Timers {
@@ -114,6 +115,17 @@ class Engine {
   // complex interleaved (host).  Output to host f64 or device f64/f32.
   virtual void reverse_host(const double* cot, double* out) = 0;
   virtual void reverse_device(const double* cot, void* out, bool f32) = 0;
+  // The synthesis objective on the device: loss = sum_o w_(o mod np)
+  // |S_o(x) - T_o|^2 over the coefficients [B][K][np] of the maps x (f64
+  // [B][N_0], device), its gradient into g (f64, device) and the loss into
+  // *loss (one f64, device), every step on the engine's stream with no host
+  // synchronisation (a CUDA graph may capture it; the first call, outside a
+  // capture, sets the kernels' attributes).  set_objective copies the
+  // target [B][K][np] complex and weights [np] (null: 1) to the device.
+  // Failed bounded waits set *error_flag().
+  virtual void set_objective(const double* target, const double* weights) = 0;
+  virtual void objective(const double* x, double* g, double* loss) = 0;
+  virtual int* error_flag() = 0;
   // Device level-0 maps of the last load (T), for checkpoints.
   virtual void save_input(std::vector<double>& x) = 0;
   // exact copy of the loaded level-0 state (fields are stored as deviations
@@ -130,10 +142,16 @@ class Engine {
   virtual std::vector<KernelStat> kernel_stats() const = 0;
   virtual void reset_kernel_stats() = 0;
   virtual void set_profiling(bool on) = 0;
+  virtual bool profiling() const = 0;
   // Mean cells read per row of each level's wavelet operator.
   virtual std::vector<double> mean_slots() const = 0;
   // Per level: slots per stored row, most cells of a tile, coloured layout (0/1).
   virtual std::vector<std::array<int, 3>> operator_layout() const = 0;
+  // Per level, the tile heights (rows of the field a thread takes) chosen
+  // for: the wavelet of the maps, of the moduli, their adjoints, the
+  // decimation of the maps (to the next level), of the moduli (from the
+  // level before), their transposes (from the next level); 0: the default.
+  virtual std::vector<std::array<int, 8>> tile_heights() const = 0;
 
  protected:
   explicit Engine(const Options& o, const Support* s = nullptr);
