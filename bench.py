@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--batch", type=int, default=4)
     p.add_argument("--skip-fp64", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="default tile heights instead of timing them at prepare (for runs under a profiler, whose "
+                        "replays make the timing meaningless)")
     p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches", "synthesis"],
                    help="scatcov: the headline metric; patches: 512 ragged disc patches (nside 512, J 5); "
                         "synthesis: 200 L-BFGS iterations at nside 1024, J 9")
@@ -270,7 +273,8 @@ def run_synthesis(args, torch, dist, world, rank, dev):
     import stl_b200
     nside, J, B = 1024, 9, 1
     npix = 12 * nside * nside
-    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True)
+    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True,
+                                autotune=not args.no_autotune)
     xt = lognormal(7 + 1000 * rank, npix)[None]
     target, var_t = eng.forward(xt, moments=True)
     v = var_t.reshape(-1)
@@ -351,7 +355,8 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
 
     # -- FP32 batched: the headline -------------------------------------------
-    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True)
+    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True,
+                                autotune=not args.no_autotune)
     seeds = [rank * B + s for s in range(B)]
     x_host = np.stack([lognormal(s, npix) for s in seeds])
     x = torch.tensor(x_host, dtype=torch.float32, device=dev)
@@ -413,7 +418,8 @@ def main():
     # -- FP64 plain single map --------------------------------------------------
     fp64 = None
     if not args.skip_fp64:
-        e64 = stl_b200.NativeEngine(nside, J, batch=1, dtype="float64", device=dev.index, prepare=True)
+        e64 = stl_b200.NativeEngine(nside, J, batch=1, dtype="float64", device=dev.index, prepare=True,
+                                      autotune=not args.no_autotune)
         x64 = torch.tensor(x_host[:1], dtype=torch.float64, device=dev)
         t64, _ = e64.forward_tensor(torch.tensor(lognormal(100, npix)[None], dtype=torch.float64, device=dev),
                                     generation=1)

@@ -17,6 +17,8 @@
 // (map_cotangent, engine.rs:757-779).
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <thread>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -92,6 +94,139 @@ void PinnedMem::release() {
 size_t device_bytes_live() { std::lock_guard<std::mutex> g(g_mem_mu); return g_live; }
 size_t device_bytes_peak() { std::lock_guard<std::mutex> g(g_mem_mu); return g_peak; }
 void device_bytes_reset_peak() { std::lock_guard<std::mutex> g(g_mem_mu); g_peak = g_live; }
+
+// ---- host <-> device copies of large host buffers ---------------------------
+// Caller buffers are pageable: the driver would move them through its own
+// small staging at the rate of one host thread.  Instead host threads copy
+// chunks into two pinned buffers while the DMA engine moves the chunk before
+// (and the reverse for device-to-host), so the transfer runs at the PCIe rate.
+namespace {
+
+// a fixed pool of host threads that split one memcpy between them
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool* pool = new CopyPool();  // threads live until the process exits
+    return *pool;
+  }
+  // dst[0, n) = src[0, n), split over the threads; returns when done
+  void copy(void* dst, const void* src, size_t n) {
+    if (n < (size_t(1) << 20) || workers_.empty()) {
+      std::memcpy(dst, src, n);
+      return;
+    }
+    std::unique_lock<std::mutex> lk(call_mu_);  // one copy at a time
+    const size_t parts = workers_.size() + 1;
+    const size_t part = ((n + parts - 1) / parts + 63) & ~(size_t)63;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      dst_ = static_cast<char*>(dst);
+      src_ = static_cast<const char*>(src);
+      n_ = n;
+      part_ = part;
+      pending_ = (int)workers_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    run(0);
+    std::unique_lock<std::mutex> g(mu_);
+    done_.wait(g, [&] { return pending_ == 0; });
+  }
+
+ private:
+  CopyPool() {
+    const unsigned h = std::thread::hardware_concurrency();
+    const int t = (int)std::min<unsigned>(16, h > 1 ? h : 1) - 1;
+    for (int i = 0; i < t; ++i) workers_.emplace_back([this, i] { loop(i + 1); });
+    for (auto& w : workers_) w.detach();
+  }
+  void run(size_t k) {
+    const size_t lo = std::min(n_, k * part_), hi = std::min(n_, lo + part_);
+    if (hi > lo) std::memcpy(dst_ + lo, src_ + lo, hi - lo);
+  }
+  void loop(size_t k) {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      run(k);
+      std::lock_guard<std::mutex> g(mu_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex mu_, call_mu_;
+  std::condition_variable cv_, done_;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t n_ = 0, part_ = 0;
+  int pending_ = 0;
+  uint64_t gen_ = 0;
+};
+
+// two pinned chunks and their copy events
+class HostStage {
+ public:
+  ~HostStage() {
+    for (cudaEvent_t& e : ev_)
+      if (e) cudaEventDestroy(e);
+  }
+  // device dst <- host src (n bytes), queued on s; src is read before the return
+  void to_device(void* dst, const void* src, size_t n, cudaStream_t s) {
+    if (n < kDirect) {
+      STL_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s));
+      return;
+    }
+    ensure();
+    for (size_t off = 0, c = 0; off < n; off += kChunk, ++c) {
+      const size_t len = std::min(kChunk, n - off), b = c & 1;
+      STL_CUDA(cudaEventSynchronize(ev_[b]));  // the last DMA out of this buffer has finished
+      CopyPool::get().copy(buf_[b].p, static_cast<const char*>(src) + off, len);
+      STL_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, buf_[b].p, len, cudaMemcpyHostToDevice, s));
+      STL_CUDA(cudaEventRecord(ev_[b], s));
+    }
+  }
+  // host dst <- device src (n bytes) after the work queued on s; synchronises
+  void to_host(void* dst, const void* src, size_t n, cudaStream_t s) {
+    if (n < kDirect) {
+      STL_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s));
+      STL_CUDA(cudaStreamSynchronize(s));
+      return;
+    }
+    ensure();
+    const size_t nc = (n + kChunk - 1) / kChunk;
+    auto drain = [&](size_t c) {  // chunk c: from its pinned buffer to dst
+      const size_t off = c * kChunk, len = std::min(kChunk, n - off);
+      STL_CUDA(cudaEventSynchronize(ev_[c & 1]));
+      CopyPool::get().copy(static_cast<char*>(dst) + off, buf_[c & 1].p, len);
+    };
+    for (size_t c = 0; c < nc; ++c) {
+      const size_t off = c * kChunk, len = std::min(kChunk, n - off);
+      STL_CUDA(cudaMemcpyAsync(buf_[c & 1].p, static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, s));
+      STL_CUDA(cudaEventRecord(ev_[c & 1], s));
+      if (c > 0) drain(c - 1);
+    }
+    drain(nc - 1);
+  }
+
+ private:
+  static constexpr size_t kChunk = size_t(32) << 20, kDirect = size_t(4) << 20;
+  void ensure() {
+    if (buf_[0].p) return;
+    for (int b = 0; b < 2; ++b) {
+      buf_[b].alloc(kChunk);
+      STL_CUDA(cudaEventCreateWithFlags(&ev_[b], cudaEventDisableTiming));
+      STL_CUDA(cudaEventRecord(ev_[b], 0));  // completed: the buffers start free
+    }
+  }
+  PinnedMem buf_[2];
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+};
+
+}  // namespace
 
 // ---- plan (crates/stl-core/src/plan.rs:80-158, one channel) ---------------
 const char* family_name(int f) {
@@ -509,7 +644,7 @@ class EngineImpl final : public Engine {
   void load_host(const double* x) override {
     prepare();
     size_t n = (size_t)opt_.B * npix(0);
-    STL_CUDA(cudaMemcpyAsync(in_f64_.p, x, n * 8, cudaMemcpyHostToDevice, stream_));
+    io_.to_device(in_f64_.p, x, n * 8, stream_);
     load_maps(in_f64_.as<double>());
   }
 
@@ -732,8 +867,7 @@ class EngineImpl final : public Engine {
         to_map_major<U, double>(gX_[0].as<U>(), in_f64_.as<double>(), npix(0), opt_.B, stream_);
       });
     });
-    STL_CUDA(cudaMemcpyAsync(out, in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
-    STL_CUDA(cudaStreamSynchronize(stream_));
+    io_.to_host(out, in_f64_.p, n * 8, stream_);
   }
 
   void reverse_device(const double* cot, void* out, bool f32) override {
@@ -826,8 +960,7 @@ class EngineImpl final : public Engine {
 
   void reverse_impl(const double* cot) {
     if (!forward_done_) throw std::runtime_error("vjp before forward");
-    STL_CUDA(cudaMemcpyAsync(cot_dev_.p, cot, 16 * (size_t)opt_.B * K_ * plan_.size(), cudaMemcpyHostToDevice,
-                             stream_));
+    io_.to_device(cot_dev_.p, cot, 16 * (size_t)opt_.B * K_ * plan_.size(), stream_);
     reverse_sweep();
   }
 
@@ -1055,6 +1188,7 @@ class EngineImpl final : public Engine {
   std::vector<size_t> cotsrc_off_;  // per level: first cotangent source entry
   int i_mean_ = -1, i_var_ = -1;    // plan entries of the mean and the variance
   DevMem target_dev_, weights_dev_;  // the synthesis objective
+  HostStage io_;                     // large host <-> device copies
   bool objective_set_ = false;
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
   std::vector<DevMem> ids_dev_;  // grid mode: supports per level

@@ -162,7 +162,7 @@ class NativeEngine:
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
-                 prepare=False, **unused):
+                 prepare=False, autotune=True, **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -174,6 +174,8 @@ class NativeEngine:
         self.device = int(device)
         self.config = dict(nside=self.nside, j=self.j, batch=self.batch, backend="gpu", kernel=int(kernel),
                            orientations=int(orientations), device=self.device, dtype=dtype)
+        if not autotune:  # keep the default tile heights (no timing at prepare)
+            self.config["autotune"] = False
         self._lib = lib()
         self._handle = self._lib.stlp_new(json.dumps(self.config).encode())
         if not self._handle:
@@ -531,13 +533,15 @@ class PatchEngine:
     radius in degrees; the coefficients average the core (else the whole disc)."""
 
     def __init__(self, nside, j, kernel=5, orientations=4, dtype="float64", device=0, cache=256, threads=0,
-                 group_pixels=None, profile=False):
+                 group_pixels=None, profile=False, autotune=True):
         cfg = dict(nside=int(nside), j=int(j), kernel=int(kernel), orientations=int(orientations), backend="gpu",
                    dtype=dtype, device=int(device), cache=int(cache), threads=int(threads))
         if group_pixels is not None:  # level-0 pixels of the discs one batched engine holds
             cfg["group_pixels"] = int(group_pixels)
         if profile:  # per kernel class device times in info()["kernels"]
             cfg["profile"] = True
+        if not autotune:  # keep the default tile heights
+            cfg["autotune"] = False
         self._lib = lib()
         self._mutex = threading.RLock()
         self._handle = self._lib.stlp_patch_new(json.dumps(cfg).encode())
