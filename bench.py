@@ -204,7 +204,7 @@ def run_patches(args, torch, dist, world, rank, dev):
     import stl_b200
     nside, J = 512, 5
     centres, radii = patch_workload(nside)
-    pe = stl_b200.PatchEngine(nside, J, dtype="float32", device=dev.index)
+    pe = stl_b200.PatchEngine(nside, J, dtype="float32", device=dev.index, autotune=not args.no_autotune)
     t0 = time.perf_counter()
     ids = pe.select(centres, radii)
     sizes = np.array([i.size for i in ids])

@@ -260,6 +260,10 @@ int stlp_forward(StlpHandle* h, const double* x, size_t n, uint64_t generation, 
     require(h != nullptr && x != nullptr && out != nullptr, "null argument");
     require(n == h->input_len(), "input shape mismatch");
     require(!moments || var != nullptr, "moments need a variance buffer");
+    // small inputs are checked here; larger ones while their copy to the
+    // device is staged (load_host), on several host threads
+    if (n < (size_t(1) << 19))
+      for (size_t i = 0; i < n; ++i) require(std::isfinite(x[i]), "input map contains non-finite values");
     h->activate();
     h->has_current = false;
     h->engine->load_host(x);

@@ -109,12 +109,11 @@ class CopyPool {
     static CopyPool* pool = new CopyPool();  // threads live until the process exits
     return *pool;
   }
-  // dst[0, n) = src[0, n), split over the threads; returns when done
-  void copy(void* dst, const void* src, size_t n) {
-    if (n < (size_t(1) << 20) || workers_.empty()) {
-      std::memcpy(dst, src, n);
-      return;
-    }
+  // dst[0, n) = src[0, n), split over the threads; returns when done.  With
+  // check (n a multiple of 8): the number of non-finite doubles copied.
+  size_t copy(void* dst, const void* src, size_t n, bool check = false) {
+    if (n < (size_t(1) << 20) || workers_.empty()) return copy_part(static_cast<char*>(dst),
+                                                                     static_cast<const char*>(src), n, check);
     std::unique_lock<std::mutex> lk(call_mu_);  // one copy at a time
     const size_t parts = workers_.size() + 1;
     const size_t part = ((n + parts - 1) / parts + 63) & ~(size_t)63;
@@ -124,13 +123,33 @@ class CopyPool {
       src_ = static_cast<const char*>(src);
       n_ = n;
       part_ = part;
+      check_ = check;
+      bad_ = 0;
       pending_ = (int)workers_.size();
       ++gen_;
     }
     cv_.notify_all();
-    run(0);
+    const size_t b0 = run(0);
     std::unique_lock<std::mutex> g(mu_);
     done_.wait(g, [&] { return pending_ == 0; });
+    return bad_ + b0;
+  }
+  static size_t copy_part(char* dst, const char* src, size_t n, bool check) {
+    if (!check) {
+      std::memcpy(dst, src, n);
+      return 0;
+    }
+    // doubles whose exponent bits are all ones are inf or nan
+    const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
+    uint64_t* d = reinterpret_cast<uint64_t*>(dst);
+    const uint64_t e = 0x7FF0000000000000ull;
+    size_t bad = 0;
+    for (size_t i = 0, m = n / 8; i < m; ++i) {
+      const uint64_t v = s[i];
+      d[i] = v;
+      bad += (v & e) == e;
+    }
+    return bad;
   }
 
  private:
@@ -140,9 +159,9 @@ class CopyPool {
     for (int i = 0; i < t; ++i) workers_.emplace_back([this, i] { loop(i + 1); });
     for (auto& w : workers_) w.detach();
   }
-  void run(size_t k) {
+  size_t run(size_t k) {
     const size_t lo = std::min(n_, k * part_), hi = std::min(n_, lo + part_);
-    if (hi > lo) std::memcpy(dst_ + lo, src_ + lo, hi - lo);
+    return hi > lo ? copy_part(dst_ + lo, src_ + lo, hi - lo, check_) : 0;
   }
   void loop(size_t k) {
     uint64_t seen = 0;
@@ -152,8 +171,9 @@ class CopyPool {
         cv_.wait(g, [&] { return gen_ != seen; });
         seen = gen_;
       }
-      run(k);
+      const size_t b = run(k);
       std::lock_guard<std::mutex> g(mu_);
+      bad_ += b;
       if (--pending_ == 0) done_.notify_one();
     }
   }
@@ -162,7 +182,8 @@ class CopyPool {
   std::condition_variable cv_, done_;
   char* dst_ = nullptr;
   const char* src_ = nullptr;
-  size_t n_ = 0, part_ = 0;
+  size_t n_ = 0, part_ = 0, bad_ = 0;
+  bool check_ = false;
   int pending_ = 0;
   uint64_t gen_ = 0;
 };
@@ -174,20 +195,28 @@ class HostStage {
     for (cudaEvent_t& e : ev_)
       if (e) cudaEventDestroy(e);
   }
-  // device dst <- host src (n bytes), queued on s; src is read before the return
-  void to_device(void* dst, const void* src, size_t n, cudaStream_t s) {
+  // device dst <- host src (n bytes), queued on s; src is read before the
+  // return.  With check (src holds doubles): the number of non-finite values.
+  size_t to_device(void* dst, const void* src, size_t n, cudaStream_t s, bool check = false) {
     if (n < kDirect) {
+      size_t bad = 0;
+      if (check) {
+        const double* v = static_cast<const double*>(src);
+        for (size_t i = 0; i < n / 8; ++i) bad += !std::isfinite(v[i]);
+      }
       STL_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s));
-      return;
+      return bad;
     }
     ensure();
+    size_t bad = 0;
     for (size_t off = 0, c = 0; off < n; off += kChunk, ++c) {
       const size_t len = std::min(kChunk, n - off), b = c & 1;
       STL_CUDA(cudaEventSynchronize(ev_[b]));  // the last DMA out of this buffer has finished
-      CopyPool::get().copy(buf_[b].p, static_cast<const char*>(src) + off, len);
+      bad += CopyPool::get().copy(buf_[b].p, static_cast<const char*>(src) + off, len, check);
       STL_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, buf_[b].p, len, cudaMemcpyHostToDevice, s));
       STL_CUDA(cudaEventRecord(ev_[b], s));
     }
+    return bad;
   }
   // host dst <- device src (n bytes) after the work queued on s; synchronises
   void to_host(void* dst, const void* src, size_t n, cudaStream_t s) {
@@ -644,7 +673,8 @@ class EngineImpl final : public Engine {
   void load_host(const double* x) override {
     prepare();
     size_t n = (size_t)opt_.B * npix(0);
-    io_.to_device(in_f64_.p, x, n * 8, stream_);
+    if (io_.to_device(in_f64_.p, x, n * 8, stream_, true))
+      throw std::runtime_error("input map contains non-finite values");
     load_maps(in_f64_.as<double>());
   }
 

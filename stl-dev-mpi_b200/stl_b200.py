@@ -96,7 +96,9 @@ def lib():
 
 
 def _error():
-    return RuntimeError(lib().stlp_last_error().decode("utf-8", errors="replace"))
+    msg = lib().stlp_last_error().decode("utf-8", errors="replace")
+    # non-finite input maps (the library counts them while it copies the maps) are value errors
+    return ValueError(msg) if msg.startswith("input") and "non-finite" in msg else RuntimeError(msg)
 
 
 def _ptr(a):
@@ -317,8 +319,7 @@ class NativeEngine:
                 x = x[None]
             if x.shape != (self.batch, self.npix):
                 raise ValueError(f"expected maps {(self.batch, self.npix)}, got {x.shape}")
-            if not np.isfinite(x).all():
-                raise ValueError("input map contains non-finite values")
+            # non-finite values: the library counts them while it copies the maps (ValueError)
             values = np.empty(self._shape(), dtype=np.complex128)
             var = np.empty(self._shape() if moments else (self.batch, 0))
             self._current_key = None
@@ -649,8 +650,7 @@ class PatchEngine:
                     raise ValueError(f"patch {i}: expected {(ids.size,)}, got {m.shape}")
                 parts.append(m.reshape(-1))
             x = np.ascontiguousarray(np.concatenate(parts))
-            if not np.isfinite(x).all():
-                raise ValueError("input patch contains non-finite values")
+            # non-finite values: the library counts them while it copies the patches (ValueError)
             self._dense = isinstance(maps, np.ndarray)
             values = np.empty((b, self.ncoeff), dtype=np.complex128)
             variance = np.empty((b, self.ncoeff if moments else 0), dtype=np.float64)
