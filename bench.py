@@ -114,6 +114,28 @@ class Clocks:
                 "reasons": reasons}
 
 
+def max_over_ranks(torch, dist, value, device):
+    """The largest of the ranks' values, on every rank (the job's time is that
+    of its slowest rank); the value itself on one process.  device: "cuda"
+    under NCCL, "cpu" under gloo."""
+    if not dist:
+        return value
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seeds(rank, batch):
+    """Seeds of the maps rank `rank` holds: rank * batch .. rank * batch + batch - 1
+    (replicas: disjoint maps per rank, no exchange between ranks)."""
+    return [rank * batch + s for s in range(batch)]
+
+
+def job_rate(world, units_per_rank, ms):
+    """Whole-job throughput: units of all ranks per second of the slowest rank."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def time_steps(torch, step, steps, warmup, dist):
     for _ in range(warmup):
         step()
@@ -127,12 +149,7 @@ def time_steps(torch, step, steps, warmup, dist):
         step()
     b.record()
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    return ms
+    return max_over_ranks(torch, dist, a.elapsed_time(b), "cuda")
 
 
 def load_peaks():
@@ -357,7 +374,7 @@ def main():
     # -- FP32 batched: the headline -------------------------------------------
     eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True,
                                 autotune=not args.no_autotune)
-    seeds = [rank * B + s for s in range(B)]
+    seeds = rank_seeds(rank, B)
     x_host = np.stack([lognormal(s, npix) for s in seeds])
     x = torch.tensor(x_host, dtype=torch.float32, device=dev)
     # target statistics S_t: the FP32 engine on the map of seed 100 (replicated over the batch)
@@ -379,7 +396,7 @@ def main():
     clocks = clk.summary()
     stats = eng.kernel_stats()
     eng.profile(on=False, reset=False)
-    value = world * B * args.steps / (ms32 / 1e3)
+    value = job_rate(world, B * args.steps, ms32)
     launches = sum(s["launches"] for s in stats.values())
 
     # roofline of the dominant kernel class, timed live with CUDA events
