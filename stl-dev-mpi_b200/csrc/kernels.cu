@@ -110,6 +110,13 @@ __device__ __forceinline__ void store8(double* p, const double w[8]) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) reinterpret_cast<double2*>(p)[k] = make_double2(w[2 * k], w[2 * k + 1]);
 }
+__device__ __forceinline__ void store4(float* p, const float w[4]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(w[0], w[1], w[2], w[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double w[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(w[0], w[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(w[2], w[3]);
+}
 
 // RB consecutive values of a row vector (RB in 1, 2, 4)
 template <int RB>
@@ -1424,6 +1431,13 @@ __global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restri
 
 // pixel-major field [N][R] (complex: the moduli): CTA = a pixel range,
 // thread t adds the row t % R of its pixels; partials [CTA][R]
+// |f[j]| of the complex value j of an interleaved array, one vector load
+template <typename T>
+__device__ __forceinline__ T cabs2(const T* f, i64 j) {
+  const typename V2<T>::type v = reinterpret_cast<const typename V2<T>::type*>(f)[j];
+  return hypot(v.x, v.y);
+}
+
 template <typename T, bool CPLX>
 __global__ void k_means_pm(const T* __restrict__ f, i64 N, int R, i64 chunk, double* __restrict__ partials) {
   __shared__ double red[256];
@@ -1440,10 +1454,10 @@ __global__ void k_means_pm(const T* __restrict__ f, i64 N, int R, i64 chunk, dou
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const i64 j = i + k * (i64)TR;
-        q[k] += CPLX ? (double)hypot(f[2 * j], f[2 * j + 1]) : (double)f[j];
+        q[k] += CPLX ? (double)cabs2(f, j) : (double)f[j];
       }
     }
-    for (; i < e1; i += TR) q[0] += CPLX ? (double)hypot(f[2 * i], f[2 * i + 1]) : (double)f[i];
+    for (; i < e1; i += TR) q[0] += CPLX ? (double)cabs2(f, i) : (double)f[i];
     a = (q[0] + q[1]) + (q[2] + q[3]);
   }
   red[t] = a;
@@ -1501,15 +1515,22 @@ __global__ void k_means_final(const double* __restrict__ partials, int nblk, int
 template <typename T, typename I>
 __global__ void k_mod_dev(const T* __restrict__ z, i64 N, int B, int L, const double* __restrict__ cz,
                           T* __restrict__ mod, int mod_pix, int mod_row, int mod_off) {
+  // thread (pixel, map): the L = 4 orientations, contiguous in z and in mod
+  typedef typename V2<T>::type T2;
   const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((i64)i >= N * B * L) return;
-  const I BL = (I)(B * L);
-  const i64 p = (i64)(i / BL);
-  const int j = (int)(i - (I)p * BL), b = j / L, l = j - b * L;
+  if ((i64)i >= N * B) return;
+  const i64 p = (i64)(i / (I)B);
+  const int b = (int)(i - (I)p * (I)B);
+  const T2* zv = reinterpret_cast<const T2*>(z) + (i64)i * 4;
+  T2 v[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) v[l] = zv[l];
   // |z| in the field type (z carries that type's rounding already); the
   // constant is subtracted in FP64 before the one rounding to T
-  const T m = hypot(z[2 * i], z[2 * i + 1]);
-  mod[p * mod_pix + (i64)b * mod_row + mod_off + l] = (T)((double)m - cz[b * L + l]);
+  T o[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) o[l] = (T)((double)hypot(v[l].x, v[l].y) - cz[b * 4 + l]);
+  store4(mod + p * mod_pix + (i64)b * mod_row + mod_off, o);
 }
 
 // constants of the branch rows (b, d, l) of level n from the moduli constants [level][B][L]
@@ -2209,10 +2230,11 @@ void row_means(const T* f, bool complex_moduli, bool pixel_major, i64 N, int R, 
 template <typename T>
 void moduli_deviations(const T* z, i64 N, int B, int L, const double* cz, T* mod, int mod_pix, int mod_row,
                        int mod_off, cudaStream_t s) {
-  if (N * B * L < ((i64)1 << 31))
-    k_mod_dev<T, uint32_t><<<nblocks(N * B * L, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
+  if (L != 4 || mod_pix % 4 || mod_row % 4 || mod_off % 4) throw std::runtime_error("moduli layout not in 4-row units");
+  if (N * B < ((i64)1 << 31))
+    k_mod_dev<T, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
   else
-    k_mod_dev<T, i64><<<nblocks(N * B * L, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
+    k_mod_dev<T, i64><<<nblocks(N * B, 256), 256, 0, s>>>(z, N, B, L, cz, mod, mod_pix, mod_row, mod_off);
   STL_CUDA(cudaGetLastError());
 }
 
