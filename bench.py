@@ -136,6 +136,30 @@ def job_rate(world, units_per_rank, ms):
     return world * units_per_rank / (ms / 1e3)
 
 
+def evaluation_roofline(nside, J, batch, elem, cells_per_row, plan, ms, hbm_gbs, sms, sm_mhz, fp64):
+    """Roofline of one forward + VJP of a batch (the scope contract's formula):
+    t_roof = max(bytes_alg / HBM, flops_alg / P), with, over the levels n (N_n
+    pixels, D_n cells read per wavelet row, c_n coefficients native at n, s the
+    field element size, L = 4),
+      bytes_alg = sum_n N_n [2 (2 L D_n s + 12) + B s (4 + L (2 + 5 n))]
+      flops_alg = B sum_n N_n [6 (2 L D_n) (1 + (n + 1) L) + 24 c_n]
+    and P the CUDA-core FMA peak at the maximum SM clock (128 FP32 or 64 FP64
+    FMA per clock and SM); frac = t_roof / the measured time."""
+    L = 4
+    native = [c["native_dg"] for c in plan]
+    b = f = 0.0
+    for n in range(J):
+        N = 12.0 * (nside >> n) ** 2
+        D = cells_per_row[n]
+        b += N * (2 * (2 * L * D * elem + 12) + batch * elem * (4 + L * (2 + 5 * n)))
+        f += batch * N * (6 * (2 * L * D) * (1 + (n + 1) * L) + 24 * native.count(n))
+    peak = sms * (64 if fp64 else 128) * 2 * sm_mhz * 1e6
+    t_mem, t_fma = b / (hbm_gbs * 1e9), f / peak
+    t_roof = max(t_mem, t_fma)
+    return {"t_roof_ms": t_roof * 1e3, "ms": ms, "frac": t_roof * 1e3 / ms, "bound": "hbm" if t_mem >= t_fma else "fma",
+            "bytes_alg": b, "flops_alg": f, "fma_peak_tflops": peak / 1e12, "hbm_gbs": hbm_gbs}
+
+
 def time_steps(torch, step, steps, warmup, dist):
     for _ in range(warmup):
         step()
@@ -156,8 +180,8 @@ def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured", "sm_max_mhz": d.get("sm_max_mhz")}
+    return {"hbm_gbs": 6650.0, "source": "fallback", "sm_max_mhz": None}
 
 
 def cpu_baseline(nside=256, J=7):
@@ -398,9 +422,15 @@ def main():
     eng.profile(on=False, reset=False)
     value = job_rate(world, B * args.steps, ms32)
     launches = sum(s["launches"] for s in stats.values())
+    peaks = load_peaks()
+    props = torch.cuda.get_device_properties(dev)
+    sm_max = peaks.get("sm_max_mhz") or 1965.0
+    info32 = eng.info()
+    eval_roof = {"fp32_batched": evaluation_roofline(nside, J, B, 4, info32["mean_cells_per_row"], eng.plan,
+                                                     ms32 / args.steps, peaks["hbm_gbs"], props.multi_processor_count,
+                                                     sm_max, False)}
 
     # roofline of the dominant kernel class, timed live with CUDA events
-    peaks = load_peaks()
     dom = max(stats.values(), key=lambda s: s["ms"])
     achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9 if dom["ms"] > 0 else 0.0
     traffic = None
@@ -449,6 +479,9 @@ def main():
 
         ms64 = time_steps(torch, step64, args.steps, args.warmup, dist)
         fp64 = world * args.steps / (ms64 / 1e3)
+        eval_roof["fp64_plain"] = evaluation_roofline(nside, J, 1, 8, e64.info()["mean_cells_per_row"], e64.plan,
+                                                      ms64 / args.steps, peaks["hbm_gbs"],
+                                                      props.multi_processor_count, sm_max, True)
         e64.close()
         del x64, g64
         torch.cuda.empty_cache()
@@ -467,7 +500,8 @@ def main():
                            "l2": "inputs larger than L2 (fields and operators of tens of GB per step)",
                            "parallelism": f"replicas x{world}",
                            "fp64_plain_evals_per_s": fp64,
-                           "fp32_batched_over_fp64_plain": (value / world) / (fp64 / world) if fp64 else None},
+                           "fp32_batched_over_fp64_plain": (value / world) / (fp64 / world) if fp64 else None,
+                           "evaluation_roofline": eval_roof},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)

@@ -117,6 +117,7 @@ StlpHandle* stlp_new(const char* config) {
     require(dtype == "float64" || dtype == "float32", "dtype must be float64 or float32");
     o.fp32 = dtype == "float32";
     o.autotune = v.boolean("autotune", true);
+    o.tune_cache = v.string("autotune_cache", "");
     require(!v.boolean("cross", false), "cross statistics (two channels) are not built in this library");
     require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
     require(o.nside > 0 && (o.nside & (o.nside - 1)) == 0, "nside must be a power of two");

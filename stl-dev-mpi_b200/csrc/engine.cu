@@ -22,6 +22,8 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <cstdlib>
+#include <fstream>
 #include <functional>
 #include <map>
 #include <mutex>
@@ -1268,8 +1270,12 @@ class EngineImpl final : public Engine {
       const std::string key = k.str();
       {
         std::lock_guard<std::mutex> g(tune_mu());
-        auto it = tune_cache().find(key);
-        if (it != tune_cache().end()) return it->second;
+        load_tune_file(opt_.tune_cache);
+        auto it = tune_cache().find(key);  // a height that is not valid here is timed again
+        if (it != tune_cache().end() && std::find(cand.begin(), cand.end(), it->second) != cand.end()) {
+          record_tune(opt_.tune_cache, key, it->second);
+          return it->second;
+        }
       }
       int best = cand.back();
       float best_ms = 0.f;
@@ -1288,6 +1294,7 @@ class EngineImpl final : public Engine {
       }
       std::lock_guard<std::mutex> g(tune_mu());
       tune_cache()[key] = best;
+      record_tune(opt_.tune_cache, key, best);
       return best;
     };
     try {
@@ -1363,6 +1370,35 @@ class EngineImpl final : public Engine {
   static std::map<std::string, int>& tune_cache() {
     static std::map<std::string, int> c;
     return c;
+  }
+  // keys a cache file holds (read or appended by this process)
+  static std::map<std::string, std::set<std::string>>& file_keys() {
+    static std::map<std::string, std::set<std::string>> k;
+    return k;
+  }
+  // the heights a cache file holds (once per file and process; a missing
+  // file is an empty cache; malformed lines are skipped)
+  static void load_tune_file(const std::string& path) {
+    static std::set<std::string> read;
+    if (path.empty() || read.count(path)) return;
+    read.insert(path);
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {
+      const size_t tab = line.rfind('\t');
+      if (tab == std::string::npos) continue;
+      const int h = std::atoi(line.c_str() + tab + 1);
+      if (h != 1 && h != 2 && h != 4) continue;
+      tune_cache()[line.substr(0, tab)] = h;
+      file_keys()[path].insert(line.substr(0, tab));
+    }
+  }
+  // a height an engine uses into its cache file, one line per launch key:
+  // key, tab, height (appended once)
+  static void record_tune(const std::string& path, const std::string& key, int h) {
+    if (path.empty() || !file_keys()[path].insert(key).second) return;
+    std::ofstream f(path, std::ios::app);
+    if (f) f << key << '\t' << h << '\n';
   }
 
   // several regions: one launch covers the sums of all of them

@@ -38,6 +38,7 @@ struct Options {
   bool fp32 = false;  // compute precision of the fields (sums are FP64 in both)
   int device = 0;
   bool autotune = true;  // time the tile heights of the wavelet and decimation launches at prepare
+  std::string tune_cache;  // file of tile heights already timed (read, then extended); empty: none
 };
 
 struct Timers {

@@ -164,7 +164,7 @@ class NativeEngine:
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
-                 prepare=False, autotune=True, **unused):
+                 prepare=False, autotune=True, autotune_cache=None, **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -178,6 +178,8 @@ class NativeEngine:
                            orientations=int(orientations), device=self.device, dtype=dtype)
         if not autotune:  # keep the default tile heights (no timing at prepare)
             self.config["autotune"] = False
+        if autotune_cache:  # a file of tile heights timed before (read, then extended)
+            self.config["autotune_cache"] = str(autotune_cache)
         self._lib = lib()
         self._handle = self._lib.stlp_new(json.dumps(self.config).encode())
         if not self._handle:

@@ -53,3 +53,38 @@ def test_tuned_tiles_change_nothing_discs(stl):
         pe.close()
     for a, b in zip(out[True], out[False]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_tile_cache_file_is_written_and_read(stl, tmp_path):
+    """autotune_cache: the heights an engine times are written to the file, and
+    a new process takes them from it instead of timing (every height set to 1
+    in the file, a valid choice everywhere, comes back as 1; unknown and
+    malformed lines are skipped); the statistics stay the same."""
+    import json
+    import subprocess
+    import sys
+    nside, J = 64, 4
+    path = tmp_path / "tiles.txt"
+    x = np.exp(np.random.default_rng(24).standard_normal((2, 12 * nside * nside)) - 0.5)
+    e1 = stl.NativeEngine(nside, J, batch=2, dtype="float32", autotune_cache=path)
+    v1, _ = e1.forward(x)
+    t1 = np.array(e1.info()["tile_heights"])
+    e1.close()
+    lines = path.read_text().splitlines()
+    assert lines and all(line.count("\t") == 1 and line.split("\t")[1] in {"1", "2", "4"} for line in lines)
+    path.write_text("".join(line.split("\t")[0] + "\t1\n" for line in lines) + "no such launch\t4\nmalformed\n")
+    np.save(tmp_path / "x.npy", x)
+    code = f"""
+import sys, json, numpy as np
+sys.path.insert(0, {str(stl.HERE)!r})
+import stl_b200
+e = stl_b200.NativeEngine({nside}, {J}, batch=2, dtype="float32", autotune_cache={str(path)!r})
+v, _ = e.forward(np.load({str(tmp_path / 'x.npy')!r}))
+np.save({str(tmp_path / 'v.npy')!r}, v)
+print(json.dumps(e.info()["tile_heights"]))
+"""
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    t2 = np.array(json.loads(out.stdout.strip().splitlines()[-1]))
+    np.testing.assert_array_equal(t2, np.where(t1 > 0, 1, 0))
+    np.testing.assert_array_equal(np.load(tmp_path / "v.npy"), v1)
