@@ -430,6 +430,40 @@ __global__ void __launch_bounds__(128) k_conv_adj(const uint32_t* __restrict__ t
   for (int k = 0; k < NK; ++k)
 #pragma unroll
     for (int rb = 0; rb < RB; ++rb) acc[k][rb] = (T)0;
+  if (NK == 1) {
+    // Grid operators: a two-stage software pipeline, as in k_conv_fwd: the
+    // coefficients and cotangent rows of entry q + 1 and the entry index of
+    // q + 2 are in flight while entry q is added (entries in order).
+    T w[8], g[RB][8], wn[8], gn[RB][8];
+    uint32_t ent = ST > 0 ? __ldg(tent + v) : kSentinel;
+    if (ent != kSentinel) {
+      load8(coefT + v * 8, w);
+      const i64 u = (i64)(ent >> tshift);
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) load8(gy + (u * R + r0 + rb) * 8, g[rb]);
+    }
+    uint32_t ent1 = (ST > 1 && ent != kSentinel) ? __ldg(tent + n_rep + v) : kSentinel;
+    for (int q = 0; q < ST && ent != kSentinel; ++q) {
+      uint32_t ent2 = kSentinel;
+      if (ent1 != kSentinel) {
+        load8(coefT + ((i64)(q + 1) * n_rep + v) * 8, wn);
+        const i64 u = (i64)(ent1 >> tshift);
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) load8(gy + (u * R + r0 + rb) * 8, gn[rb]);
+        if (q + 2 < ST) ent2 = __ldg(tent + (i64)(q + 2) * n_rep + v);
+      }
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) acc[0][rb] += rot_dot<T, 0>(w, g[rb]);
+      ent = ent1;
+      ent1 = ent2;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) w[j] = wn[j];
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) g[rb][j] = gn[rb][j];
+    }
+  } else {
   for (int q = 0; q < ST; ++q) {
     const i64 e = (i64)q * n_rep + v;
     const uint32_t ent = __ldg(tent + e);
@@ -466,6 +500,7 @@ __global__ void __launch_bounds__(128) k_conv_adj(const uint32_t* __restrict__ t
         acc[NK > 3 ? 3 : 0][rb] += t3;
       }
     }
+  }
   }
 #pragma unroll
   for (int k = 0; k < NK; ++k) {
@@ -1828,7 +1863,7 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
   } else if (op.colored) {
     throw std::runtime_error("the coloured adjoint needs scratch for its tile partials");
   } else {
-    if (!rb) rb = R % 2 == 0 ? 2 : 1;
+    if (!rb) rb = op.nk == 1 ? conv_adjoint_choices(op, sizeof(T), R, scr).back() : (R % 2 == 0 ? 2 : 1);
     if (op.nk == 4) {
       if (rb == 2) conv_adjoint_rb<T, 4, 2>(op, gy, R, gx, accumulate, s);
       else conv_adjoint_rb<T, 4, 1>(op, gy, R, gx, accumulate, s);
