@@ -1863,7 +1863,7 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
   } else if (op.colored) {
     throw std::runtime_error("the coloured adjoint needs scratch for its tile partials");
   } else {
-    if (!rb) rb = op.nk == 1 ? conv_adjoint_choices(op, sizeof(T), R, scr).back() : (R % 2 == 0 ? 2 : 1);
+    if (!rb) rb = R % 2 == 0 ? 2 : 1;  // 4 rows per thread: more registers, fewer warps (measured slower)
     if (op.nk == 4) {
       if (rb == 2) conv_adjoint_rb<T, 4, 2>(op, gy, R, gx, accumulate, s);
       else conv_adjoint_rb<T, 4, 1>(op, gy, R, gx, accumulate, s);
