@@ -82,7 +82,7 @@ struct StlpHandle {
   size_t input_len() const { return (size_t)engine->options().B * (size_t)engine->npix(0); }
   // B K np: K masks (1 without)
   size_t values_len() const {
-    return (size_t)engine->options().B * std::max(1, engine->nmasks()) * engine->plan().size();
+    return (size_t)engine->value_batch() * std::max(1, engine->nmasks()) * engine->plan().size();
   }
   void activate() { STL_CUDA(cudaSetDevice(device)); }
 };
@@ -118,7 +118,7 @@ StlpHandle* stlp_new(const char* config) {
     o.fp32 = dtype == "float32";
     o.autotune = v.boolean("autotune", true);
     o.tune_cache = v.string("autotune_cache", "");
-    require(!v.boolean("cross", false), "cross statistics (two channels) are not built in this library");
+    o.cross = v.boolean("cross", false);  // two channels, the plan of their cross terms (lib.rs:238-245)
     require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
     require(o.nside > 0 && (o.nside & (o.nside - 1)) == 0, "nside must be a power of two");
     auto h = std::make_unique<StlpHandle>();
@@ -173,7 +173,8 @@ char* stlp_info(StlpHandle* h) {
     std::ostringstream js;
     js.precision(17);
     js << "{\"version\": " << jstr(kVersion) << ", \"engine\": \"b200\", \"nside\": " << o.nside
-       << ", \"j\": " << o.J << ", \"batch\": " << o.B << ", \"channels\": 1, \"cross\": false"
+       << ", \"j\": " << o.J << ", \"batch\": " << e.value_batch() << ", \"channels\": " << e.channels()
+       << ", \"cross\": " << (o.cross ? "true" : "false")
        << ", \"dtype\": " << jstr(o.fp32 ? "float32 fields, float64 sums/complex128" : "float64/complex128")
        << ", \"fewer\": false, \"orientations\": " << o.L << ", \"kernel\": " << o.ksz
        << ", \"levels\": " << e.levels() << ", \"masks\": " << e.nmasks() << ", \"spin\": 0, \"device\": " << o.device

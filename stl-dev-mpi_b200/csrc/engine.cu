@@ -298,6 +298,39 @@ std::vector<Coef> build_plan(int J, int L) {
   return plan;
 }
 
+std::vector<Coef> build_plan_cross(int J, int L) {
+  std::vector<Coef> plan;
+  auto mk = [](int fam, int nat, int c1, int c2) { return Coef{fam, nat, c1, c2, -1, -1, -1, -1, -1, -1}; };
+  for (int j3 = 0; j3 < J; ++j3) {
+    for (int fam : {S1, S2})
+      for (int l = 0; l < L; ++l) {
+        Coef c = mk(fam, j3, 0, 1);
+        c.j1 = j3; c.l1 = l;
+        plan.push_back(c);
+      }
+    for (int ca = 0; ca < 2; ++ca) {  // channel orders (0, 1), then (1, 0)
+      const int cb = 1 - ca;
+      for (int j2 = 0; j2 <= j3; ++j2) {
+        for (int l2 = 0; l2 < L; ++l2)
+          for (int l3 = 0; l3 < L; ++l3) {
+            Coef c = mk(S3, j3, ca, cb);
+            c.j1 = j2; c.j3 = j3; c.l1 = l2; c.l3 = l3;
+            plan.push_back(c);
+          }
+        for (int j1 = 0; j1 <= j2; ++j1)
+          for (int l1 = 0; l1 < L; ++l1)
+            for (int l2 = 0; l2 < L; ++l2)
+              for (int l3 = 0; l3 < L; ++l3) {
+                Coef c = mk(S4, j3, ca, cb);
+                c.j1 = j1; c.j2 = j2; c.j3 = j3; c.l1 = l1; c.l2 = l2; c.l3 = l3;
+                plan.push_back(c);
+              }
+      }
+    }
+  }
+  return plan;
+}
+
 // f32-rounded wavelet kernel [G][2][P] (wavelet.rs:11-35, conv.rs:167-172)
 static std::vector<double> wavelet_kernel(int ksz, int G) {
   int P = ksz * ksz;
@@ -334,7 +367,12 @@ Engine::Engine(const Options& o, const Support* sup) : opt_(o) {
   if (o.B < 1) throw std::runtime_error("batch must be positive");
   if (o.L != 4) throw std::runtime_error("the B200 engine is built for orientations = 4");
   if (o.ksz != 5 && o.ksz != 3) throw std::runtime_error("kernel must be 3 or 5");
-  plan_ = build_plan(o.J, o.L);
+  plan_ = o.cross ? build_plan_cross(o.J, o.L) : build_plan(o.J, o.L);
+  vb_ = o.B;
+  if (o.cross) {
+    if (sup) throw std::runtime_error("cross statistics are not built for disc patches");
+    opt_.B = 2 * o.B;  // the fields' maps: channel c of batch entry b is map 2 b + c
+  }
   levels_ = o.J;
   for (int d = 0; d < levels_; ++d) {
     const i64 n = 12 * (o.nside >> d) * (o.nside >> d);
@@ -615,6 +653,8 @@ class EngineImpl final : public Engine {
       shapes_[n] = product_shape(n, L, B, N, e);
       if (segmented()) segment_ranges(shapes_[n], support_.seg[n]);
       max_part = std::max(max_part, (size_t)B * L * shapes_[n].blocks * shapes_[n].slots);
+      if (opt_.cross)
+        max_part = std::max(max_part, (size_t)cross_blocks(N) * vb_ * L * cross_slots(shapes_[n].K));
       max_gz = std::max(max_gz, e * 2 * B * L * N);
       max_gbr = std::max(max_gbr, e * 2 * B * (n + 1) * L * L * N);
       field_bytes_ += X_[n].bytes + Z_[n].bytes + Mod_[n].bytes + Br_[n].bytes + gMod_[n].bytes + gX_[n].bytes;
@@ -638,7 +678,7 @@ class EngineImpl final : public Engine {
     sum_off_.resize(levels_);
     for (int n = 0; n < levels_; ++n) {
       sum_off_[n] = total_sums;
-      total_sums += (size_t)B * L * shapes_[n].slots;
+      total_sums += opt_.cross ? (size_t)vb_ * L * cross_slots(shapes_[n].K) : (size_t)B * L * shapes_[n].slots;
     }
     total_sums_ = total_sums;
     if (segmented()) upload_ranges();
@@ -772,9 +812,9 @@ class EngineImpl final : public Engine {
     cudaStream_t s = stream_;
     forward_sweep(moments);
     // the coefficients (and variances) of every map and mask, from the sums
-    const size_t nv = (size_t)B * K_ * plan_.size();
+    const size_t nv = (size_t)vb_ * K_ * plan_.size();
     assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
-                    counts_dev_.as<double>(), levels_, B, K_, vals_dev_.as<double>(),
+                    counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(),
                     moments ? var_dev_.as<double>() : nullptr, s);
     STL_CUDA(cudaMemcpyAsync(values, vals_dev_.p, 16 * nv, cudaMemcpyDeviceToHost, s));
     if (moments && var) STL_CUDA(cudaMemcpyAsync(var, var_dev_.p, 8 * nv, cudaMemcpyDeviceToHost, s));
@@ -812,7 +852,7 @@ class EngineImpl final : public Engine {
 
   void set_objective(const double* target, const double* weights) override {
     prepare();
-    const size_t nv = (size_t)opt_.B * K_ * plan_.size(), np = plan_.size();
+    const size_t nv = (size_t)vb_ * K_ * plan_.size(), np = plan_.size();
     target_dev_.alloc(16 * nv);
     STL_CUDA(cudaMemcpyAsync(target_dev_.p, target, 16 * nv, cudaMemcpyHostToDevice, stream_));
     weights_dev_.release();
@@ -830,9 +870,9 @@ class EngineImpl final : public Engine {
     const int B = opt_.B;
     load_maps(x);
     forward_sweep(false);
-    const i64 nv = (i64)B * K_ * plan_.size();
+    const i64 nv = (i64)vb_ * K_ * plan_.size();
     assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
-                    counts_dev_.as<double>(), levels_, B, K_, vals_dev_.as<double>(), nullptr, s);
+                    counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(), nullptr, s);
     objective_terms(vals_dev_.as<double>(), target_dev_.as<double>(),
                     weights_dev_.p ? weights_dev_.as<double>() : nullptr, nv, (int)plan_.size(),
                     cot_dev_.as<double>(), loss, s);
@@ -880,6 +920,16 @@ class EngineImpl final : public Engine {
     });
     const ProductShape& sh = shapes_[n];
     const double E = sh.K * (sh.K + 1) / 2.0;
+    if (opt_.cross) {  // the cross terms of each channel pair only
+      for (int k = 0; k < launch_sets(); ++k)
+        prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U),
+                     (double)vb_ * L * N * sh.K * sh.K * 8.0, s, [&] {
+                       cross_forward<U>(sh.K, N, B, Z_[n].as<U>(), Br_[n].as<U>(), mask(k, n), moments,
+                                        partials_.as<double>(), cross_blocks(N),
+                                        sums_.as<double>() + k * total_sums_ + sum_off_[n], s);
+                     });
+      return;
+    }
     for (int k = 0; k < launch_sets(); ++k)
       prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
                    [&] {
@@ -959,16 +1009,53 @@ class EngineImpl final : public Engine {
   // its real part, imaginary part (-1: exactly zero) and second moment
   struct Loc {
     int level, l3, re, im, second;
+    int conj = 0;  // the coefficient is the conjugate of the sum
   };
+
+  // cross terms (the cross_slots layout of kernels.cu): S1 the rn term, S2
+  // G[z][z], terms in channel order (0, 1) G[r][q] and in order (1, 0)
+  // conj(G[q][r]), r and q the operand entries (branch (d, l) at d L + l, z
+  // last) of channels 0 and 1 (operands of engine.rs:956-984)
+  Loc locate_cross(const Coef& c) const {
+    const int L = opt_.L, n = c.native, K = (n + 1) * L + 1, z = K - 1, K2 = K * K;
+    Loc l{n, 0, 0, 0, 0, 0};
+    auto entry = [&](int e, bool conj) {
+      l.re = 2 * e;
+      l.im = 2 * e + 1;
+      l.second = 2 * K2 + 2 + e;
+      l.conj = conj ? 1 : 0;
+    };
+    switch (c.family) {
+      case S1: l.l3 = c.l1; l.re = 2 * K2; l.im = 2 * K2 + 1; l.second = 3 * K2 + 2; break;
+      case S2: l.l3 = c.l1; entry(z * K + z, false); break;
+      case S3: {
+        const int r = c.j1 * L + c.l1;
+        l.l3 = c.l3;
+        if (c.c1 == 0) entry(r * K + z, false);
+        else entry(z * K + r, true);
+        break;
+      }
+      case S4: {
+        const int r = c.j1 * L + c.l1, q = c.j2 * L + c.l2;
+        l.l3 = c.l3;
+        if (c.c1 == 0) entry(r * K + q, false);
+        else entry(q * K + r, true);
+        break;
+      }
+      default: throw std::runtime_error("cross plans hold S1-S4 only");
+    }
+    return l;
+  }
 
   // Sums of the products kernel per (b, l3) (kernels.cu): 4 x 4 Gram blocks
   // (d1 <= d2) of the branches, 4 x 1 blocks (d, z), then the per-pixel sums.
   Loc locate(const Coef& c) const {
+    if (opt_.cross) return locate_cross(c);
     const int L = opt_.L;
     const int n = c.native, nd = n + 1;
     const int nBB = nd * (nd + 1) / 2, zb = nBB * 48 + nd * 12;
     auto tblock = [&](int d1, int d2) { return d1 * nd - d1 * (d1 - 1) / 2 + (d2 - d1); };
-    Loc l{n, 0, 0, 0, 0};
+    Loc l{n, 0, 0, 0, 0, 0};
     switch (c.family) {
       case MEAN: l.re = zb + 3; l.second = zb + 4; l.im = -1; break;
       case VAR: l.re = zb + 4; l.second = zb + 5; l.im = -1; break;
@@ -992,7 +1079,7 @@ class EngineImpl final : public Engine {
 
   void reverse_impl(const double* cot) {
     if (!forward_done_) throw std::runtime_error("vjp before forward");
-    io_.to_device(cot_dev_.p, cot, 16 * (size_t)opt_.B * K_ * plan_.size(), stream_);
+    io_.to_device(cot_dev_.p, cot, 16 * (size_t)vb_ * K_ * plan_.size(), stream_);
     reverse_sweep();
   }
 
@@ -1026,18 +1113,19 @@ class EngineImpl final : public Engine {
         typed(n, [&](auto t) {
           using U = typename decltype(t)::type;
           unsigned char* base = stage_dev_.as<unsigned char>();
-          build_cotangents<U>(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, n, shapes_[n].K, L,
-                              cotsrc_dev_.as<CotSources>() + cotsrc_off_[n],
+          build_cotangents<U>(cot_dev_.as<double>(), np, vb_, K_, counts_dev_.as<double>(), levels_, n, shapes_[n].K,
+                              L, cotsrc_dev_.as<CotSources>() + cotsrc_off_[n],
                               cotsrc_dev_.as<CotSources>() + cotsrc_off_[n] + (size_t)L * shapes_[n].K * shapes_[n].K,
                               reinterpret_cast<U*>(base + stage_m_[(size_t)n * K_]),
-                              reinterpret_cast<U*>(base + stage_s_[(size_t)n * K_]), s);
+                              reinterpret_cast<U*>(base + stage_s_[(size_t)n * K_]), s, opt_.cross);
         });
       });
-    build_mean_var(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, i_mean_, i_var_,
-                   mv_.as<double>(), s);
+    if (!opt_.cross)
+      build_mean_var(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, i_mean_, i_var_,
+                     mv_.as<double>(), s);
     for (int n = levels_ - 1; n >= 0; --n)
       typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n); });
-    for (int k = 0; k < launch_sets(); ++k)
+    for (int k = 0; k < launch_sets() && !opt_.cross; ++k)  // the cross plan has no mean or variance
       prof_.launch(Profiler::ELEM, 1, (double)B * npix(0) * 3 * esz(0), (double)B * npix(0) * 2.0, s, [&] {
         typed(0, [&](auto t) {
           using U = typename decltype(t)::type;
@@ -1077,8 +1165,12 @@ class EngineImpl final : public Engine {
       const U* sdev = reinterpret_cast<const U*>(stage_dev_.as<unsigned char>() + stage_s_[(size_t)n * K_ + k]);
       prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0,
                    s, [&] {
-                     products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), Mdev, sdev, mask(k, n), k > 0,
-                                         gZ_.as<U>(), gBr_.as<U>(), s);
+                     if (opt_.cross)
+                       cross_reverse<U>(sh.K, N, B, Z_[n].as<U>(), Br_[n].as<U>(), Mdev, sdev, mask(k, n), k > 0,
+                                        gZ_.as<U>(), gBr_.as<U>(), s);
+                     else
+                       products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), Mdev, sdev, mask(k, n), k > 0,
+                                           gZ_.as<U>(), gBr_.as<U>(), s);
                    });
     }
     const int R = B * (n + 1) * L;
@@ -1122,7 +1214,7 @@ class EngineImpl final : public Engine {
   // S1 scales: a segmented launch reads all of them) and the mask counts
   void size_mask_buffers() {
     const int L = opt_.L, B = opt_.B;
-    const size_t nv = (size_t)B * K_ * plan_.size();
+    const size_t nv = (size_t)vb_ * K_ * plan_.size();
     sums_.alloc(sizeof(double) * total_sums_ * K_);
     mv_.alloc(sizeof(double) * 2 * B * K_);
     vals_dev_.alloc(16 * nv);
@@ -1133,7 +1225,8 @@ class EngineImpl final : public Engine {
     size_t bytes = 0;
     auto align = [](size_t v) { return (v + 255) & ~(size_t)255; };
     for (int n = 0; n < levels_; ++n) {
-      const size_t ms = esz(n) * 2 * B * L * shapes_[n].K * shapes_[n].K, ss = esz(n) * B * L;
+      // with cross: one matrix per channel pair (batch entry), complex cross-S1 scales
+      const size_t ms = esz(n) * 2 * vb_ * L * shapes_[n].K * shapes_[n].K, ss = esz(n) * vb_ * L * (opt_.cross ? 2 : 1);
       for (int k = 0; k < K_; ++k) stage_m_[(size_t)n * K_ + k] = bytes + k * ms;
       bytes = align(bytes + K_ * ms);
       for (int k = 0; k < K_; ++k) stage_s_[(size_t)n * K_ + k] = bytes + k * ss;
@@ -1160,8 +1253,9 @@ class EngineImpl final : public Engine {
     for (size_t i = 0; i < np; ++i) {
       const Loc& l = map_[i];
       const ProductShape& sh = shapes_[l.level];
-      ps[i] = PlanSlots{l.level, (int32_t)(sum_off_[l.level] + (size_t)l.l3 * sh.slots), L * sh.slots, l.re, l.im,
-                        l.second};
+      const int row = opt_.cross ? cross_slots(sh.K) : sh.slots;  // doubles per (map or pair, l3)
+      ps[i] = PlanSlots{l.level, (int32_t)(sum_off_[l.level] + (size_t)l.l3 * row), L * row, l.re, l.im,
+                        l.second, l.conj};
     }
     plan_dev_.alloc(sizeof(PlanSlots) * np);
     STL_CUDA(cudaMemcpyAsync(plan_dev_.p, ps.data(), sizeof(PlanSlots) * np, cudaMemcpyHostToDevice, stream_));
@@ -1180,6 +1274,26 @@ class EngineImpl final : public Engine {
         else if (x.i1 < 0) { x.i1 = (int32_t)i; x.m1 = mode; }
         else throw std::runtime_error("a cotangent entry with more than two sources");
       };
+      if (opt_.cross) {  // the cotangents of G (the cross S1's complex)
+        switch (c.family) {
+          case S1: put(E + c.l1, 0); break;
+          case S2: put(((size_t)c.l1 * Kd + z) * Kd + z, 0); break;
+          case S3: {
+            const int r = c.j1 * L + c.l1;
+            if (c.c1 == 0) put(((size_t)c.l3 * Kd + r) * Kd + z, 0);
+            else put(((size_t)c.l3 * Kd + z) * Kd + r, 1);
+            break;
+          }
+          case S4: {
+            const int r = c.j1 * L + c.l1, q = c.j2 * L + c.l2;
+            if (c.c1 == 0) put(((size_t)c.l3 * Kd + r) * Kd + q, 0);
+            else put(((size_t)c.l3 * Kd + q) * Kd + r, 1);
+            break;
+          }
+          default: throw std::runtime_error("cross plans hold S1-S4 only");
+        }
+        continue;
+      }
       switch (c.family) {
         case MEAN: i_mean_ = (int)i; break;
         case VAR: i_var_ = (int)i; break;

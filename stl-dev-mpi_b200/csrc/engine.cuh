@@ -314,6 +314,7 @@ void mean_var_grad(const T* x0, const double* xc, const uint8_t* mask, const dou
 // real part, imaginary part (-1: exactly zero) and second moment.
 struct PlanSlots {
   int32_t level, base, stride, re, im, second;
+  int32_t conj;  // the coefficient is the conjugate of the sum (a cross term in channel order (1, 0))
 };
 // values [B][K][np] complex and var [B][K][np] (or null) from the sums of K
 // masks (mask k at sums + k mask_stride); counts [K][levels]: the pixels
@@ -332,9 +333,25 @@ struct CotSources {
 // of level n in the field type U, from the coefficient cotangents cot
 // [B][K][np] complex: entry (b, l3, r, q) from src[(l3 Kd + r) Kd + q], the
 // real S1 scale (b, l) from s1src[l].
+// (s1_complex: s1 [K][B][L] complex, the cross S1 terms' cotangents)
 template <typename U>
 void build_cotangents(const double* cot, int np, int B, int K, const double* counts, int levels, int n, int Kd,
-                      int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s);
+                      int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s,
+                      bool s1_complex = false);
+// Cross terms of channel pairs (kernels.cu): maps 2 b + c; per level the
+// sums [B][L][cross_slots(K)] of G = sum v_0 conj(v_1) (K x K), of the cross
+// S1 and, with moments, their second sums; nblk pixel ranges (cross_blocks),
+// partials [nblk][B][L][cross_slots(K)].
+int cross_blocks(i64 N);
+__host__ __device__ constexpr int cross_slots(int K) { return 3 * K * K + 3; }
+template <typename T>
+void cross_forward(int K, i64 N, int Bm, const T* z, const T* br, const uint8_t* mask, bool moments,
+                   double* partials, int nblk, double* sums, cudaStream_t s);
+// their VJP: M [B][L][K][K] complex (cotangents of G), s1 [B][L] complex
+// (of the cross S1) -> gz, gbr of both channels (accumulate: add)
+template <typename T>
+void cross_reverse(int K, i64 N, int Bm, const T* z, const T* br, const T* M, const T* s1, const uint8_t* mask,
+                   bool accumulate, T* gz, T* gbr, cudaStream_t s);
 // Synthesis terms: cot_o = 2 w (v_o - t_o) and *loss = sum_o w |v_o - t_o|^2
 // (w = weights[o mod np], or 1) over nv complex values, in a fixed order.
 void objective_terms(const double* values, const double* target, const double* weights, i64 nv, int np,

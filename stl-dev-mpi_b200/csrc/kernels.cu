@@ -2128,7 +2128,7 @@ __global__ void k_assemble(const double* __restrict__ sums, size_t mstride, cons
     const PlanSlots p = plan[i];
     const double* row = sums + (size_t)k * mstride + p.base + (i64)b * p.stride;
     const double N = counts[(size_t)k * levels + p.level];
-    const double vr = row[p.re] / N, vi = p.im >= 0 ? row[p.im] / N : 0.0;
+    const double vr = row[p.re] / N, vi = p.im >= 0 ? (p.conj ? -row[p.im] : row[p.im]) / N : 0.0;
     values[2 * o] = vr;
     values[2 * o + 1] = vi;
     if (var) {
@@ -2150,7 +2150,8 @@ __device__ __forceinline__ void add_source(const double* g, int mode, double N, 
 template <typename U>
 __global__ void k_build_cot(const double* __restrict__ cot, int np, int B, int K, const double* __restrict__ counts,
                             int levels, int n, int Kd, int L, const CotSources* __restrict__ src,
-                            const CotSources* __restrict__ s1src, U* __restrict__ M, U* __restrict__ s1) {
+                            const CotSources* __restrict__ s1src, U* __restrict__ M, U* __restrict__ s1,
+                            int s1_complex) {
   const int E = L * Kd * Kd, per = E + L;  // matrix entries, then the S1 scales, of one (k, b)
   const i64 total = (i64)K * B * per;
   for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
@@ -2167,6 +2168,9 @@ __global__ void k_build_cot(const double* __restrict__ cot, int np, int B, int K
       U* m = M + 2 * (kb * E + e);
       m[0] = (U)ar;
       m[1] = (U)ai;
+    } else if (s1_complex) {
+      s1[2 * (kb * L + (e - E))] = (U)ar;
+      s1[2 * (kb * L + (e - E)) + 1] = (U)ai;
     } else {
       s1[kb * L + (e - E)] = (U)ar;
     }
@@ -2228,10 +2232,11 @@ void assemble_values(const double* sums, size_t mask_stride, const PlanSlots* pl
 
 template <typename U>
 void build_cotangents(const double* cot, int np, int B, int K, const double* counts, int levels, int n, int Kd,
-                      int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s) {
+                      int L, const CotSources* src, const CotSources* s1src, U* M, U* s1, cudaStream_t s,
+                      bool s1_complex) {
   const i64 total = (i64)K * B * (L * Kd * Kd + L);
   k_build_cot<U><<<(unsigned)std::max<i64>(1, std::min<i64>(nblocks(total, 256), 148 * 16)), 256, 0, s>>>(
-      cot, np, B, K, counts, levels, n, Kd, L, src, s1src, M, s1);
+      cot, np, B, K, counts, levels, n, Kd, L, src, s1src, M, s1, s1_complex ? 1 : 0);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -2240,6 +2245,236 @@ void build_mean_var(const double* cot, int np, int B, int K, const double* count
   k_build_mean_var<<<nblocks((i64)K * B, 256), 256, 0, s>>>(cot, np, B, K, counts, levels, i_mean, i_var, mv);
   STL_CUDA(cudaGetLastError());
 }
+
+// ---- cross terms of two channels ------------------------------------------
+// Maps come in channel pairs (map 2 b + c).  Per pixel, batch entry b and
+// gauge l3 the operand vector of channel c is v_c = (branches (d, l1) of
+// Br[p][2 b + c][.][l3], then z[p][2 b + c][l3]), K values.  The cross sums
+// of a level are, per (b, l3), the K x K block G[r][q] = sum_p v_0[r]
+// conj(v_1[q]) (every S2, S3 and S4 cross term is an entry of G or the
+// conjugate of one), the sum of rn(z_0) conj(rn(z_1)), rn(z) = z / sqrt(|z| +
+// 1e-8) (the cross S1, engine.rs:29-33, 1201-1206), and with moments the sums
+// of the squared moduli of those terms.  Layout per (b, l3), xslots = 3 K^2 +
+// 3 doubles: G (re, im) at 2 (r K + q), the S1 term at 2 K^2, the second
+// sums of G at 2 K^2 + 2 + r K + q and of the S1 term at 3 K^2 + 2.
+constexpr int kCrossThreads = 256;
+constexpr int kCrossChunk = 32;  // pixels staged at a time
+constexpr int kCrossMaxEnt = 8;  // entries per thread (K^2 + 1 <= 8 x 256)
+
+
+__device__ __forceinline__ double2 cmul_conj(double2 a, double2 b) {  // a conj(b), products rounded one by one
+  return make_double2(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y)));
+}
+__device__ __forceinline__ double2 root_normalise(double2 z) {
+  const double s = sqrt(hypot(z.x, z.y) + 1e-8);
+  return make_double2(z.x / s, z.y / s);
+}
+
+// stage the chunk's operand vectors of both channels as FP64: sv[j][c][i]
+template <typename T>
+__device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, int Bm, int b, int l3,
+                                            const T* __restrict__ z, const T* __restrict__ br,
+                                            const uint8_t* __restrict__ mask) {
+  typedef typename V2<T>::type T2;
+  const T2* zv = reinterpret_cast<const T2*>(z);
+  const T2* bv = reinterpret_cast<const T2*>(br);
+  const int K1 = K - 1, L = 4;
+  for (int t = threadIdx.x; t < np * 2 * K; t += blockDim.x) {
+    const int j = t / (2 * K), rem = t - j * 2 * K, c = rem / K, i = rem - c * K;
+    const i64 p = p0 + j;
+    const i64 m = 2 * b + c;
+    double2 v = make_double2(0.0, 0.0);
+    if (!mask || mask[p]) {
+      const T2 w = i < K1 ? bv[((p * Bm + m) * K1 + i) * L + l3] : zv[(p * Bm + m) * L + l3];
+      v = make_double2((double)w.x, (double)w.y);
+    }
+    sv[t] = v;
+  }
+}
+
+// grid (pixel ranges, B L): partials [range][b][l3][xslots]
+template <typename T, bool MOM>
+__global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int Bm, const T* __restrict__ z,
+                                                             const T* __restrict__ br,
+                                                             const uint8_t* __restrict__ mask, i64 chunk,
+                                                             double* __restrict__ partials) {
+  extern __shared__ __align__(16) double2 sv[];  // [kCrossChunk][2][K], then the lane sums
+  const int B = Bm / 2, b = blockIdx.y / 4, l3 = blockIdx.y % 4;
+  const int E = K * K + 1, NE = min(E, kCrossThreads), Q = kCrossThreads / NE;
+  const int t = threadIdx.x, q = t / NE, e0 = t - q * NE;
+  const int nent = (E - e0 + NE - 1) / NE;  // entries of this thread: e0, e0 + NE, ...
+  const bool lane = q < Q;
+  double acc[kCrossMaxEnt][3];
+#pragma unroll
+  for (int s = 0; s < kCrossMaxEnt; ++s) acc[s][0] = acc[s][1] = acc[s][2] = 0.0;
+  const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
+  for (i64 pc = P0; pc < P1; pc += kCrossChunk) {
+    const int np = (int)min((i64)kCrossChunk, P1 - pc);
+    __syncthreads();
+    cross_stage<T>(sv, pc, np, K, Bm, b, l3, z, br, mask);
+    __syncthreads();
+    if (!lane) continue;
+    for (int j = q; j < np; j += Q) {
+      const double2* v0 = sv + (size_t)j * 2 * K;
+      const double2* v1 = v0 + K;
+#pragma unroll
+      for (int s = 0; s < kCrossMaxEnt; ++s) {
+        if (s >= nent) break;
+        const int e = e0 + s * NE;
+        const double2 f = e < K * K ? cmul_conj(v0[e / K], v1[e % K])
+                                    : cmul_conj(root_normalise(v0[K - 1]), root_normalise(v1[K - 1]));
+        acc[s][0] = __dadd_rn(acc[s][0], f.x);
+        acc[s][1] = __dadd_rn(acc[s][1], f.y);
+        if (MOM) acc[s][2] = __dadd_rn(acc[s][2], __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y)));
+      }
+    }
+  }
+  // lanes of an entry added in lane order (through the staging memory)
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(sv);  // [Q][NE][kCrossMaxEnt][3]
+  if (lane)
+    for (int s = 0; s < nent; ++s)
+      for (int k = 0; k < 3; ++k) red[(((size_t)q * NE + e0) * kCrossMaxEnt + s) * 3 + k] = acc[s][k];
+  __syncthreads();
+  if (q != 0) return;
+  double* out = partials + (((i64)blockIdx.x * B + b) * 4 + l3) * cross_slots(K);
+  for (int s = 0; s < nent; ++s) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int r = 0; r < Q; ++r)
+      for (int k = 0; k < 3; ++k) v[k] = __dadd_rn(v[k], red[(((size_t)r * NE + e0) * kCrossMaxEnt + s) * 3 + k]);
+    const int e = e0 + s * NE;
+    const int at = e < K * K ? 2 * e : 2 * K * K;
+    out[at] = v[0];
+    out[at + 1] = v[1];
+    out[e < K * K ? 2 * K * K + 2 + e : 3 * K * K + 2] = v[2];
+  }
+}
+
+// d rn(z)^H-side cotangent: g / sqrt(r + eps) - (Re(conj(g) z) / 2 / (r +
+// eps)^1.5) z / |z| (|z| taken as 1 at z = 0), engine.rs:35-46
+__device__ __forceinline__ double2 root_modulus_vjp(double2 z, double2 g) {
+  const double r = hypot(z.x, z.y);
+  const double radial = __dadd_rn(__dmul_rn(g.x, z.x), __dmul_rn(g.y, z.y));
+  const double mag = r == 0.0 ? 1.0 : r;
+  const double s = sqrt(r + 1e-8), c = 0.5 * radial / pow(r + 1e-8, 1.5);
+  return make_double2(__dsub_rn(g.x / s, __dmul_rn(c, z.x) / mag), __dsub_rn(g.y / s, __dmul_rn(c, z.y) / mag));
+}
+
+// grid (pixel ranges, B L); thread (entry i, pixel lane): the cotangents of
+// entry i of both channels, gv_0 = M v_1 and gv_1 = M^H v_0 (M [K][K]: the
+// cotangents of G), plus through rn the cross S1's (cotangent s):
+// rn-VJP(z_0, s rn(z_1)) and rn-VJP(z_1, conj(s) rn(z_0)).  Pixels outside the
+// mask get zero (accumulate: nothing).
+template <typename T>
+__global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int Bm, const T* __restrict__ z,
+                                                             const T* __restrict__ br, const T* __restrict__ M,
+                                                             const T* __restrict__ s1, const uint8_t* __restrict__ mask,
+                                                             int accumulate, i64 chunk, T* __restrict__ gz,
+                                                             T* __restrict__ gbr) {
+  typedef typename V2<T>::type T2;
+  extern __shared__ __align__(16) double2 sm[];  // M [K][K], then [kCrossChunk][2][K]
+  const int B = Bm / 2, b = blockIdx.y / 4, l3 = blockIdx.y % 4, L = 4, K1 = K - 1;
+  double2* mk = sm;
+  double2* sv = sm + K * K;
+  const T2* Mb = reinterpret_cast<const T2*>(M) + ((i64)b * L + l3) * K * K;
+  for (int i = threadIdx.x; i < K * K; i += blockDim.x) mk[i] = make_double2((double)Mb[i].x, (double)Mb[i].y);
+  const T2 s1v = reinterpret_cast<const T2*>(s1)[(i64)b * L + l3];
+  const double2 sc = make_double2((double)s1v.x, (double)s1v.y);
+  const int Q = kCrossThreads / K, q = threadIdx.x / K, i = threadIdx.x - q * K;
+  const bool lane = q < Q;
+  T2* gzv = reinterpret_cast<T2*>(gz);
+  T2* gbv = reinterpret_cast<T2*>(gbr);
+  const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
+  for (i64 pc = P0; pc < P1; pc += kCrossChunk) {
+    const int np = (int)min((i64)kCrossChunk, P1 - pc);
+    __syncthreads();
+    cross_stage<T>(sv, pc, np, K, Bm, b, l3, z, br, mask);
+    __syncthreads();
+    if (!lane) continue;
+    for (int j = q; j < np; j += Q) {
+      const i64 p = pc + j;
+      const double2* v0 = sv + (size_t)j * 2 * K;
+      const double2* v1 = v0 + K;
+      double2 g0 = make_double2(0.0, 0.0), g1 = make_double2(0.0, 0.0);
+      const bool on = !mask || mask[p];
+      if (on) {
+        for (int k = 0; k < K; ++k) {
+          const double2 a = mk[i * K + k], c = mk[k * K + i];
+          // g0 += M[i][k] v1[k]; g1 += conj(M[k][i]) v0[k]
+          g0.x = __dadd_rn(g0.x, __dsub_rn(__dmul_rn(a.x, v1[k].x), __dmul_rn(a.y, v1[k].y)));
+          g0.y = __dadd_rn(g0.y, __dadd_rn(__dmul_rn(a.x, v1[k].y), __dmul_rn(a.y, v1[k].x)));
+          g1.x = __dadd_rn(g1.x, __dadd_rn(__dmul_rn(c.x, v0[k].x), __dmul_rn(c.y, v0[k].y)));
+          g1.y = __dadd_rn(g1.y, __dsub_rn(__dmul_rn(c.x, v0[k].y), __dmul_rn(c.y, v0[k].x)));
+        }
+        if (i == K1) {  // the cross S1 through rn
+          const double2 r0 = root_normalise(v0[K1]), r1 = root_normalise(v1[K1]);
+          const double2 ga = make_double2(__dsub_rn(__dmul_rn(sc.x, r1.x), __dmul_rn(sc.y, r1.y)),
+                                          __dadd_rn(__dmul_rn(sc.x, r1.y), __dmul_rn(sc.y, r1.x)));
+          const double2 gb = make_double2(__dadd_rn(__dmul_rn(sc.x, r0.x), __dmul_rn(sc.y, r0.y)),
+                                          __dsub_rn(__dmul_rn(sc.x, r0.y), __dmul_rn(sc.y, r0.x)));
+          const double2 d0 = root_modulus_vjp(v0[K1], ga), d1 = root_modulus_vjp(v1[K1], gb);
+          g0.x = __dadd_rn(g0.x, d0.x); g0.y = __dadd_rn(g0.y, d0.y);
+          g1.x = __dadd_rn(g1.x, d1.x); g1.y = __dadd_rn(g1.y, d1.y);
+        }
+      } else if (accumulate) {
+        continue;
+      }
+      for (int c = 0; c < 2; ++c) {
+        const double2 gv = c ? g1 : g0;
+        const i64 m = 2 * b + c;
+        T2* dst = i < K1 ? gbv + ((p * Bm + m) * K1 + i) * L + l3 : gzv + (p * Bm + m) * L + l3;
+        T2 o;
+        o.x = (T)gv.x;
+        o.y = (T)gv.y;
+        if (accumulate) {
+          const T2 prev = *dst;
+          o.x += prev.x;
+          o.y += prev.y;
+        }
+        *dst = o;
+      }
+    }
+  }
+}
+
+template <typename T>
+void cross_forward(int K, i64 N, int Bm, const T* z, const T* br, const uint8_t* mask, bool moments,
+                   double* partials, int nblk, double* sums, cudaStream_t s) {
+  const int E = K * K + 1, NE = std::min(E, kCrossThreads), Q = kCrossThreads / NE;
+  if ((E + NE - 1) / NE > kCrossMaxEnt) throw std::runtime_error("too many cross terms per level");
+  const size_t smem = std::max(sizeof(double2) * kCrossChunk * 2 * K,
+                               sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
+  const i64 chunk = (N + nblk - 1) / nblk;
+  dim3 grid((unsigned)nblk, (unsigned)(Bm / 2 * 4));
+  if (moments) {
+    if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, true>);
+    k_cross_fwd<T, true><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, partials);
+  } else {
+    if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, false>);
+    k_cross_fwd<T, false><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, partials);
+  }
+  STL_CUDA(cudaGetLastError());
+  const i64 rows = (i64)Bm / 2 * 4, total = rows * cross_slots(K);
+  k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, nblk, (int)rows,
+                                                                                        cross_slots(K), sums);
+  STL_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void cross_reverse(int K, i64 N, int Bm, const T* z, const T* br, const T* M, const T* s1, const uint8_t* mask,
+                   bool accumulate, T* gz, T* gbr, cudaStream_t s) {
+  if (K > kCrossThreads) throw std::runtime_error("too many operands for the cross VJP");
+  const size_t smem = sizeof(double2) * ((size_t)K * K + kCrossChunk * 2 * K);
+  if (smem > 48 * 1024) allow_dynamic_smem(k_cross_rev<T>);
+  const i64 per = 1024;  // pixels per CTA
+  const unsigned nblk = (unsigned)std::max<i64>(1, (N + per - 1) / per);
+  dim3 grid(nblk, (unsigned)(Bm / 2 * 4));
+  k_cross_rev<T><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, M, s1, mask, accumulate ? 1 : 0, per, gz, gbr);
+  STL_CUDA(cudaGetLastError());
+}
+
+int cross_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(296, (N + 4095) / 4096)); }
 
 int means_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(kMeansBlocks, (N + 1023) / 1024)); }
 
@@ -2314,7 +2549,11 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
                                  cudaStream_t, const i64*, int);                                                  \
   template void row_means<T>(const T*, bool, bool, i64, int, double*, double*, cudaStream_t);                     \
   template void build_cotangents<T>(const double*, int, int, int, const double*, int, int, int, int,             \
-                                    const CotSources*, const CotSources*, T*, T*, cudaStream_t);                 \
+                                    const CotSources*, const CotSources*, T*, T*, cudaStream_t, bool);           \
+  template void cross_forward<T>(int, i64, int, const T*, const T*, const uint8_t*, bool, double*, int, double*,  \
+                                 cudaStream_t);                                                                   \
+  template void cross_reverse<T>(int, i64, int, const T*, const T*, const T*, const T*, const uint8_t*, bool, T*, \
+                                 T*, cudaStream_t);                                                               \
   template void moduli_deviations<T>(const T*, i64, int, int, const double*, T*, int, int, int, cudaStream_t);
 INST(float)
 INST(double)

@@ -28,6 +28,10 @@ struct Coef {
 const char* family_name(int f);
 // build_plan of one channel, dg(j) = j, all families (plan.rs:80-158)
 std::vector<Coef> build_plan(int J, int L);
+// the cross terms of two channels (c1 != c2) of build_plan with two
+// channels, in its order (plan.rs:80-158 filtered as the bridge's plan_of,
+// crates/stl-bridge/src/lib.rs:238-245)
+std::vector<Coef> build_plan_cross(int J, int L);
 
 struct Options {
   i64 nside = 128;
@@ -38,6 +42,10 @@ struct Options {
   bool fp32 = false;  // compute precision of the fields (sums are FP64 in both)
   int device = 0;
   bool autotune = true;  // time the tile heights of the wavelet and decimation launches at prepare
+  // Two channels and the plan of their cross terms only (c1 != c2: S1 of the
+  // root-normalised z, S2, S3 and S4 in both channel orders), maps
+  // [B][2][N]; the fields then hold 2 B maps (map 2 b + c).
+  bool cross = false;
   std::string tune_cache;  // file of tile heights already timed (read, then extended); empty: none
 };
 
@@ -82,6 +90,10 @@ class Engine {
   const Options& options() const { return opt_; }
   const std::vector<Coef>& plan() const { return plan_; }
   int levels() const { return levels_; }
+  // maps of the values and cotangents (the batch; options().B counts the
+  // fields' maps, two per batch entry with cross)
+  int value_batch() const { return vb_; }
+  int channels() const { return opt_.cross ? 2 : 1; }
   i64 npix(int d) const { return npix_[d]; }
   // pixels a coefficient of native level d averages
   i64 ncore(int d) const { return ncore_[d]; }
@@ -159,6 +171,7 @@ class Engine {
   Options opt_;
   std::vector<Coef> plan_;
   int levels_ = 1;
+  int vb_ = 1;
   Support support_;
   std::vector<i64> npix_, ncore_;
   cudaStream_t stream_ = nullptr;

@@ -164,7 +164,7 @@ class NativeEngine:
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
-                 prepare=False, autotune=True, autotune_cache=None, **unused):
+                 prepare=False, autotune=True, autotune_cache=None, cross=False, **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -172,12 +172,17 @@ class NativeEngine:
                 raise ValueError("engine sizes must be positive integers")
         self.nside, self.j, self.batch = int(nside), int(j), int(batch)
         self.npix = 12 * self.nside ** 2
+        # cross: two channels and the plan of their cross terms, maps [batch, 2, npix] (native.py's cross engine)
+        self.cross, self.channels = bool(cross), 2 if cross else 1
+        self._map_shape = (self.batch, 2, self.npix) if cross else (self.batch, self.npix)
         self.dtype = dtype
         self.device = int(device)
         self.config = dict(nside=self.nside, j=self.j, batch=self.batch, backend="gpu", kernel=int(kernel),
                            orientations=int(orientations), device=self.device, dtype=dtype)
         if not autotune:  # keep the default tile heights (no timing at prepare)
             self.config["autotune"] = False
+        if cross:
+            self.config["cross"] = True
         if autotune_cache:  # a file of tile heights timed before (read, then extended)
             self.config["autotune_cache"] = str(autotune_cache)
         self._lib = lib()
@@ -264,8 +269,8 @@ class NativeEngine:
         import torch
         if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float64 and x.is_contiguous()):
             raise ValueError("x must be a contiguous CUDA float64 tensor")
-        if x.numel() != self.batch * self.npix:
-            raise ValueError(f"expected {self.batch * self.npix} map values, got {x.numel()}")
+        if x.numel() != self.batch * self.channels * self.npix:
+            raise ValueError(f"expected {self.batch * self.channels * self.npix} map values, got {x.numel()}")
         t = np.ascontiguousarray(target, dtype=np.complex128).reshape(-1)
         w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
         if w is not None and w.shape != (self.ncoeff,):
@@ -317,10 +322,10 @@ class NativeEngine:
             self._open()
             key = _key(generation, member, objective)
             x = np.ascontiguousarray(maps, dtype=np.float64)
-            if x.shape == (self.npix,) and self.batch == 1:
+            if x.shape == (self.npix,) and self.batch == 1 and not self.cross:
                 x = x[None]
-            if x.shape != (self.batch, self.npix):
-                raise ValueError(f"expected maps {(self.batch, self.npix)}, got {x.shape}")
+            if x.shape != self._map_shape:
+                raise ValueError(f"expected maps {self._map_shape}, got {x.shape}")
             # non-finite values: the library counts them while it copies the maps (ValueError)
             values = np.empty(self._shape(), dtype=np.complex128)
             var = np.empty(self._shape() if moments else (self.batch, 0))
@@ -349,7 +354,7 @@ class NativeEngine:
             if key != self._current_key:
                 raise RuntimeError("stale/wrong-member/objective forward state")
             c = self._cotangent(cotangents)
-            grad = np.empty((self.batch, self.npix))
+            grad = np.empty(self._map_shape)
             if self._lib.stlp_vjp(self._handle, _ptr(c.view(np.float64)), c.size, *key, _ptr(grad)):
                 raise _error()
             return grad
@@ -393,7 +398,7 @@ class NativeEngine:
             key = _key(generation, member, objective)
             if not x.is_cuda or x.dtype not in (torch.float32, torch.float64):
                 raise ValueError("forward_tensor needs a float32/float64 CUDA tensor")
-            x = x.detach().reshape(self.batch, self.npix).contiguous()
+            x = x.detach().reshape(self.batch * self.channels, self.npix).contiguous()
             self._bind_stream(torch)
             values = np.empty(self._shape(), dtype=np.complex128)
             var = np.empty(self._shape() if moments else (self.batch, 0))
@@ -412,7 +417,7 @@ class NativeEngine:
             key = _key(generation, member, objective)
             if key != self._current_key:
                 raise RuntimeError("stale/wrong-member/objective forward state")
-            if not (out.is_cuda and out.is_contiguous() and out.numel() == self.batch * self.npix
+            if not (out.is_cuda and out.is_contiguous() and out.numel() == self.batch * self.channels * self.npix
                     and out.dtype in (torch.float32, torch.float64)):
                 raise ValueError("out must be a contiguous float32/float64 CUDA tensor [batch, npix]")
             c = self._cotangent(cotangents)
