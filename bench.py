@@ -52,9 +52,10 @@ def parse():
     p.add_argument("--no-autotune", action="store_true",
                    help="default tile heights instead of timing them at prepare (for runs under a profiler, whose "
                         "replays make the timing meaningless)")
-    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches", "synthesis"],
+    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches", "synthesis", "cross"],
                    help="scatcov: the headline metric; patches: 512 ragged disc patches (nside 512, J 5); "
-                        "synthesis: 200 L-BFGS iterations at nside 1024, J 9")
+                        "synthesis: 200 L-BFGS iterations at nside 1024, J 9; cross: the cross terms of two "
+                        "channels at nside 1024, J 9")
     return p.parse_args()
 
 
@@ -304,6 +305,65 @@ def run_patches(args, torch, dist, world, rank, dev):
     pe.close()
 
 
+def run_cross(args, torch, dist, world, rank, dev):
+    """Cross statistics of two channels (config "cross": the cross-only plan) at
+    nside 1024, J 9, L 4, FP32 fields, a batch of 2 channel pairs (4 maps):
+    channel c of pair b is exp(0.7 g_b + 0.5 e_bc - 1/2) (g, e ~ N(0, 1), seeds
+    per rank), the cotangent that of sum |S - S_t|^2 with S_t the statistics of
+    pair 0 shifted by a seed.  Forward + VJP evaluations (pairs) per second,
+    device-resident and through the host API."""
+    import stl_b200
+    nside, J, B = 1024, 9, 2
+    npix = 12 * nside * nside
+    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True, cross=True,
+                                autotune=not args.no_autotune)
+    rng = np.random.default_rng(500 + rank)
+    g = rng.standard_normal((B, 1, npix))
+    x_host = np.exp(0.7 * g + 0.5 * rng.standard_normal((B, 2, npix)) - 0.5)
+    x = torch.tensor(x_host, dtype=torch.float32, device=dev)
+    xt = torch.tensor(np.roll(x_host, 1, axis=0), dtype=torch.float32, device=dev)
+    target, _ = eng.forward_tensor(xt, generation=1)
+    grad = torch.empty_like(x)
+    gen = iter(range(10, 10 ** 9))
+
+    def step():
+        k = next(gen)
+        values, _ = eng.forward_tensor(x, generation=k)
+        eng.vjp_tensor(2.0 * (values - target), grad, generation=k)
+
+    for _ in range(args.warmup):
+        step()
+    with Clocks(dev.index) as clk:
+        ms = time_steps(torch, step, args.steps, 0, dist)
+    clocks = clk.summary()
+    eng.profile(on=True, reset=True)
+    step()
+    torch.cuda.synchronize()
+    stats = eng.kernel_stats()
+    eng.profile(on=False, reset=False)
+
+    def step_host():
+        k = next(gen)
+        values, _ = eng.forward(x_host, generation=k)
+        eng.vjp(2.0 * (values - target), generation=k)
+
+    e2e_steps = max(2, args.steps // 2)
+    ms_e2e = time_steps(torch, step_host, e2e_steps, 1, dist)
+    if rank == 0:
+        line = {"metric": "cross S1-S4 fwd+VJP evals/s (two channels, nside 1024, J=9, FP32)",
+                "value": job_rate(world, B * args.steps, ms), "unit": "evals/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "cross terms of 2 channels, nside 1024, J 9, L 4, 2 pairs (4 maps), FP32 fields",
+                           "ncoeff": eng.ncoeff, "parallelism": f"replicas x{world}",
+                           "kernels_ms_per_step": {k: v["ms"] for k, v in stats.items()}},
+                "e2e": {"value": job_rate(world, B * e2e_steps, ms_e2e), "unit": "evals/s",
+                        "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(x_host.nbytes)},
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def run_synthesis(args, torch, dist, world, rank, dev):
     """L-BFGS synthesis at nside 1024, J 9, L 4, m = 10, FP32 engine: target the
     lognormal map of seed 7, start from N(0, 1) (seed 8) rescaled to the target's
@@ -384,8 +444,8 @@ def main():
         torch.cuda.set_device(0)
     import stl_b200
 
-    if args.workload in ("patches", "synthesis"):
-        run = run_patches if args.workload == "patches" else run_synthesis
+    if args.workload in ("patches", "synthesis", "cross"):
+        run = {"patches": run_patches, "synthesis": run_synthesis, "cross": run_cross}[args.workload]
         run(args, torch, dist, world, rank, torch.device("cuda", local if world > 1 else 0))
         if dist:
             dist.barrier()
