@@ -313,7 +313,7 @@ def run_cross(args, torch, dist, world, rank, dev):
     pair 0 shifted by a seed.  Forward + VJP evaluations (pairs) per second,
     device-resident and through the host API."""
     import stl_b200
-    nside, J, B = 1024, 9, 2
+    nside, J, B = args.nside, args.J, 2
     npix = 12 * nside * nside
     eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, prepare=True, cross=True,
                                 autotune=not args.no_autotune)
@@ -350,11 +350,11 @@ def run_cross(args, torch, dist, world, rank, dev):
     e2e_steps = max(2, args.steps // 2)
     ms_e2e = time_steps(torch, step_host, e2e_steps, 1, dist)
     if rank == 0:
-        line = {"metric": "cross S1-S4 fwd+VJP evals/s (two channels, nside 1024, J=9, FP32)",
+        line = {"metric": f"cross S1-S4 fwd+VJP evals/s (two channels, nside {nside}, J={J}, FP32)",
                 "value": job_rate(world, B * args.steps, ms), "unit": "evals/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "cross terms of 2 channels, nside 1024, J 9, L 4, 2 pairs (4 maps), FP32 fields",
+                "config": {"workload": f"cross terms of 2 channels, nside {nside}, J {J}, L 4, 2 pairs (4 maps), FP32 fields",
                            "ncoeff": eng.ncoeff, "parallelism": f"replicas x{world}",
                            "kernels_ms_per_step": {k: v["ms"] for k, v in stats.items()}},
                 "e2e": {"value": job_rate(world, B * e2e_steps, ms_e2e), "unit": "evals/s",

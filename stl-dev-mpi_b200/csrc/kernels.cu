@@ -2258,7 +2258,8 @@ void build_mean_var(const double* cot, int np, int B, int K, const double* count
 // 3 doubles: G (re, im) at 2 (r K + q), the S1 term at 2 K^2, the second
 // sums of G at 2 K^2 + 2 + r K + q and of the S1 term at 3 K^2 + 2.
 constexpr int kCrossThreads = 256;
-constexpr int kCrossChunk = 32;  // pixels staged at a time
+// pixels staged at a time: as many as 48 KB hold (both channels, FP64), 16 to 256
+inline int cross_chunk(int K) { return std::max(16, std::min(256, (48 * 1024) / (2 * K * 16))); }
 constexpr int kCrossMaxEnt = 8;  // entries per thread (K^2 + 1 <= 8 x 256)
 
 
@@ -2297,9 +2298,9 @@ __device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, 
 template <typename T, bool MOM>
 __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int Bm, const T* __restrict__ z,
                                                              const T* __restrict__ br,
-                                                             const uint8_t* __restrict__ mask, i64 chunk,
+                                                             const uint8_t* __restrict__ mask, i64 chunk, int PC,
                                                              double* __restrict__ partials) {
-  extern __shared__ __align__(16) double2 sv[];  // [kCrossChunk][2][K], then the lane sums
+  extern __shared__ __align__(16) double2 sv[];  // [PC][2][K], then the lane sums
   const int B = Bm / 2, b = blockIdx.y / 4, l3 = blockIdx.y % 4;
   const int E = K * K + 1, NE = min(E, kCrossThreads), Q = kCrossThreads / NE;
   const int t = threadIdx.x, q = t / NE, e0 = t - q * NE;
@@ -2309,8 +2310,8 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
 #pragma unroll
   for (int s = 0; s < kCrossMaxEnt; ++s) acc[s][0] = acc[s][1] = acc[s][2] = 0.0;
   const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
-  for (i64 pc = P0; pc < P1; pc += kCrossChunk) {
-    const int np = (int)min((i64)kCrossChunk, P1 - pc);
+  for (i64 pc = P0; pc < P1; pc += PC) {
+    const int np = (int)min((i64)PC, P1 - pc);
     __syncthreads();
     cross_stage<T>(sv, pc, np, K, Bm, b, l3, z, br, mask);
     __syncthreads();
@@ -2319,8 +2320,8 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
       const double2* v0 = sv + (size_t)j * 2 * K;
       const double2* v1 = v0 + K;
 #pragma unroll
-      for (int s = 0; s < kCrossMaxEnt; ++s) {
-        if (s >= nent) break;
+      for (int s = 0; s < kCrossMaxEnt; ++s) {  // static indices: the sums stay in registers
+        if (s >= nent) continue;
         const int e = e0 + s * NE;
         const double2 f = e < K * K ? cmul_conj(v0[e / K], v1[e % K])
                                     : cmul_conj(root_normalise(v0[K - 1]), root_normalise(v1[K - 1]));
@@ -2333,9 +2334,13 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
   // lanes of an entry added in lane order (through the staging memory)
   __syncthreads();
   double* red = reinterpret_cast<double*>(sv);  // [Q][NE][kCrossMaxEnt][3]
-  if (lane)
-    for (int s = 0; s < nent; ++s)
-      for (int k = 0; k < 3; ++k) red[(((size_t)q * NE + e0) * kCrossMaxEnt + s) * 3 + k] = acc[s][k];
+  if (lane) {
+#pragma unroll
+    for (int s = 0; s < kCrossMaxEnt; ++s)
+      if (s < nent)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) red[(((size_t)q * NE + e0) * kCrossMaxEnt + s) * 3 + k] = acc[s][k];
+  }
   __syncthreads();
   if (q != 0) return;
   double* out = partials + (((i64)blockIdx.x * B + b) * 4 + l3) * cross_slots(K);
@@ -2370,10 +2375,10 @@ template <typename T>
 __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int Bm, const T* __restrict__ z,
                                                              const T* __restrict__ br, const T* __restrict__ M,
                                                              const T* __restrict__ s1, const uint8_t* __restrict__ mask,
-                                                             int accumulate, i64 chunk, T* __restrict__ gz,
+                                                             int accumulate, i64 chunk, int PC, T* __restrict__ gz,
                                                              T* __restrict__ gbr) {
   typedef typename V2<T>::type T2;
-  extern __shared__ __align__(16) double2 sm[];  // M [K][K], then [kCrossChunk][2][K]
+  extern __shared__ __align__(16) double2 sm[];  // M [K][K], then [PC][2][K]
   const int B = Bm / 2, b = blockIdx.y / 4, l3 = blockIdx.y % 4, L = 4, K1 = K - 1;
   double2* mk = sm;
   double2* sv = sm + K * K;
@@ -2386,8 +2391,8 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
   T2* gzv = reinterpret_cast<T2*>(gz);
   T2* gbv = reinterpret_cast<T2*>(gbr);
   const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
-  for (i64 pc = P0; pc < P1; pc += kCrossChunk) {
-    const int np = (int)min((i64)kCrossChunk, P1 - pc);
+  for (i64 pc = P0; pc < P1; pc += PC) {
+    const int np = (int)min((i64)PC, P1 - pc);
     __syncthreads();
     cross_stage<T>(sv, pc, np, K, Bm, b, l3, z, br, mask);
     __syncthreads();
@@ -2443,16 +2448,16 @@ void cross_forward(int K, i64 N, int Bm, const T* z, const T* br, const uint8_t*
                    double* partials, int nblk, double* sums, cudaStream_t s) {
   const int E = K * K + 1, NE = std::min(E, kCrossThreads), Q = kCrossThreads / NE;
   if ((E + NE - 1) / NE > kCrossMaxEnt) throw std::runtime_error("too many cross terms per level");
-  const size_t smem = std::max(sizeof(double2) * kCrossChunk * 2 * K,
-                               sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
+  const int PC = cross_chunk(K);
+  const size_t smem = std::max(sizeof(double2) * PC * 2 * K, sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
   const i64 chunk = (N + nblk - 1) / nblk;
   dim3 grid((unsigned)nblk, (unsigned)(Bm / 2 * 4));
   if (moments) {
     if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, true>);
-    k_cross_fwd<T, true><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, partials);
+    k_cross_fwd<T, true><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
   } else {
     if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, false>);
-    k_cross_fwd<T, false><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, partials);
+    k_cross_fwd<T, false><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
   }
   STL_CUDA(cudaGetLastError());
   const i64 rows = (i64)Bm / 2 * 4, total = rows * cross_slots(K);
@@ -2465,12 +2470,14 @@ template <typename T>
 void cross_reverse(int K, i64 N, int Bm, const T* z, const T* br, const T* M, const T* s1, const uint8_t* mask,
                    bool accumulate, T* gz, T* gbr, cudaStream_t s) {
   if (K > kCrossThreads) throw std::runtime_error("too many operands for the cross VJP");
-  const size_t smem = sizeof(double2) * ((size_t)K * K + kCrossChunk * 2 * K);
+  const int PC = cross_chunk(K);
+  const size_t smem = sizeof(double2) * ((size_t)K * K + (size_t)PC * 2 * K);
   if (smem > 48 * 1024) allow_dynamic_smem(k_cross_rev<T>);
-  const i64 per = 1024;  // pixels per CTA
+  const i64 per = 4 * (i64)PC;  // pixels per CTA
   const unsigned nblk = (unsigned)std::max<i64>(1, (N + per - 1) / per);
   dim3 grid(nblk, (unsigned)(Bm / 2 * 4));
-  k_cross_rev<T><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, M, s1, mask, accumulate ? 1 : 0, per, gz, gbr);
+  k_cross_rev<T><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, M, s1, mask, accumulate ? 1 : 0, per, PC, gz,
+                                                   gbr);
   STL_CUDA(cudaGetLastError());
 }
 
