@@ -2258,8 +2258,8 @@ void build_mean_var(const double* cot, int np, int B, int K, const double* count
 // 3 doubles: G (re, im) at 2 (r K + q), the S1 term at 2 K^2, the second
 // sums of G at 2 K^2 + 2 + r K + q and of the S1 term at 3 K^2 + 2.
 constexpr int kCrossThreads = 256;
-// pixels staged at a time: as many as 48 KB hold (both channels, FP64), 16 to 256
-inline int cross_chunk(int K) { return std::max(16, std::min(256, (48 * 1024) / (2 * K * 16))); }
+// pixels staged at a time: as many as 48 KB hold (both channels, K + 1 values, FP64), 16 to 256
+inline int cross_chunk(int K) { return std::max(16, std::min(256, (48 * 1024) / (2 * (K + 1) * 16))); }
 constexpr int kCrossMaxEnt = 8;  // entries per thread (K^2 + 1 <= 8 x 256)
 
 
@@ -2272,15 +2272,31 @@ __device__ __forceinline__ double2 root_normalise(double2 z) {
   return make_double2(z.x / s, z.y / s);
 }
 
-// stage the chunk's operand vectors of both channels as FP64: sv[j][c][i]
-template <typename T>
+// d rn(z)^H-side cotangent: g / sqrt(r + eps) - (Re(conj(g) z) / 2 / (r +
+// eps)^1.5) z / |z| (|z| taken as 1 at z = 0), engine.rs:35-46
+__device__ __forceinline__ double2 root_modulus_vjp(double2 z, double2 g) {
+  const double r = hypot(z.x, z.y);
+  const double radial = __dadd_rn(__dmul_rn(g.x, z.x), __dmul_rn(g.y, z.y));
+  const double mag = r == 0.0 ? 1.0 : r;
+  const double s = sqrt(r + 1e-8), c = 0.5 * radial / pow(r + 1e-8, 1.5);
+  return make_double2(__dsub_rn(g.x / s, __dmul_rn(c, z.x) / mag), __dsub_rn(g.y / s, __dmul_rn(c, z.y) / mag));
+}
+
+// stage the chunk's operand vectors of both channels as FP64, K + 1 values a
+// channel: sv[j][c][i], i < K the operands, i = K the channel's S1 factor,
+// computed here once per pixel and channel in a pass of its own (one (j, c) a
+// thread, the same instructions for both channels) instead of in the thread
+// that owns the S1 term: rn(z_c) for the sums, and for the VJP (REV) the
+// rn-VJP of the S1 term with cotangent sc, rn-VJP(z_c, sc_c rn(z_{1-c})), sc_0
+// = sc and sc_1 = conj(sc).  Pixels outside the mask stage zeros.
+template <typename T, bool REV>
 __device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, int Bm, int b, int l3,
                                             const T* __restrict__ z, const T* __restrict__ br,
-                                            const uint8_t* __restrict__ mask) {
+                                            const uint8_t* __restrict__ mask, double2 sc) {
   typedef typename V2<T>::type T2;
   const T2* zv = reinterpret_cast<const T2*>(z);
   const T2* bv = reinterpret_cast<const T2*>(br);
-  const int K1 = K - 1, L = 4;
+  const int K1 = K - 1, KS = K + 1, L = 4;
   for (int t = threadIdx.x; t < np * 2 * K; t += blockDim.x) {
     const int j = t / (2 * K), rem = t - j * 2 * K, c = rem / K, i = rem - c * K;
     const i64 p = p0 + j;
@@ -2290,41 +2306,68 @@ __device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, 
       const T2 w = i < K1 ? bv[((p * Bm + m) * K1 + i) * L + l3] : zv[(p * Bm + m) * L + l3];
       v = make_double2((double)w.x, (double)w.y);
     }
-    sv[t] = v;
+    sv[(size_t)j * 2 * KS + c * KS + i] = v;
+  }
+  for (int t = threadIdx.x; t < np * 2; t += blockDim.x) {
+    const int j = t >> 1, c = t & 1;
+    const i64 p = p0 + j;
+    double2 v = make_double2(0.0, 0.0);
+    if (!mask || mask[p]) {
+      const T2 w = zv[(p * Bm + 2 * b + c) * L + l3];
+      const double2 zs = make_double2((double)w.x, (double)w.y);
+      if (!REV) {
+        v = root_normalise(zs);
+      } else {
+        const T2 wo = zv[(p * Bm + 2 * b + 1 - c) * L + l3];
+        const double2 r = root_normalise(make_double2((double)wo.x, (double)wo.y));
+        const double sy = c ? -sc.y : sc.y;
+        v = root_modulus_vjp(zs, make_double2(__dsub_rn(__dmul_rn(sc.x, r.x), __dmul_rn(sy, r.y)),
+                                              __dadd_rn(__dmul_rn(sc.x, r.y), __dmul_rn(sy, r.x))));
+      }
+    }
+    sv[(size_t)j * 2 * KS + c * KS + K] = v;
   }
 }
 
-// grid (pixel ranges, B L): partials [range][b][l3][xslots]
+// grid: pixel ranges x (B L), (b, l3) fastest so that the four gauges of a
+// range, which share the operands' 32-byte sectors, run together; partials
+// [range][b][l3][xslots]
 template <typename T, bool MOM>
 __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int Bm, const T* __restrict__ z,
                                                              const T* __restrict__ br,
                                                              const uint8_t* __restrict__ mask, i64 chunk, int PC,
                                                              double* __restrict__ partials) {
-  extern __shared__ __align__(16) double2 sv[];  // [PC][2][K], then the lane sums
-  const int B = Bm / 2, b = blockIdx.y / 4, l3 = blockIdx.y % 4;
+  extern __shared__ __align__(16) double2 sv[];  // [PC][2][K + 1], then the lane sums
+  const int B = Bm / 2, bl = (int)(blockIdx.x % (unsigned)(B * 4)), b = bl / 4, l3 = bl % 4;
+  const i64 range = blockIdx.x / (unsigned)(B * 4);
   const int E = K * K + 1, NE = min(E, kCrossThreads), Q = kCrossThreads / NE;
   const int t = threadIdx.x, q = t / NE, e0 = t - q * NE;
   const int nent = (E - e0 + NE - 1) / NE;  // entries of this thread: e0, e0 + NE, ...
   const bool lane = q < Q;
+  const int KS = K + 1;
   double acc[kCrossMaxEnt][3];
+  int ri[kCrossMaxEnt], qi[kCrossMaxEnt];  // the entry's operands: (r, q) of G, (K, K) for the S1 term
 #pragma unroll
-  for (int s = 0; s < kCrossMaxEnt; ++s) acc[s][0] = acc[s][1] = acc[s][2] = 0.0;
-  const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
+  for (int s = 0; s < kCrossMaxEnt; ++s) {
+    acc[s][0] = acc[s][1] = acc[s][2] = 0.0;
+    const int e = e0 + s * NE;
+    ri[s] = e < K * K ? e / K : K;
+    qi[s] = e < K * K ? e - (e / K) * K : K;
+  }
+  const i64 P0 = range * chunk, P1 = min(N, P0 + chunk);
   for (i64 pc = P0; pc < P1; pc += PC) {
     const int np = (int)min((i64)PC, P1 - pc);
     __syncthreads();
-    cross_stage<T>(sv, pc, np, K, Bm, b, l3, z, br, mask);
+    cross_stage<T, false>(sv, pc, np, K, Bm, b, l3, z, br, mask, make_double2(0.0, 0.0));
     __syncthreads();
     if (!lane) continue;
     for (int j = q; j < np; j += Q) {
-      const double2* v0 = sv + (size_t)j * 2 * K;
-      const double2* v1 = v0 + K;
+      const double2* v0 = sv + (size_t)j * 2 * KS;
+      const double2* v1 = v0 + KS;
 #pragma unroll
       for (int s = 0; s < kCrossMaxEnt; ++s) {  // static indices: the sums stay in registers
         if (s >= nent) continue;
-        const int e = e0 + s * NE;
-        const double2 f = e < K * K ? cmul_conj(v0[e / K], v1[e % K])
-                                    : cmul_conj(root_normalise(v0[K - 1]), root_normalise(v1[K - 1]));
+        const double2 f = cmul_conj(v0[ri[s]], v1[qi[s]]);
         acc[s][0] = __dadd_rn(acc[s][0], f.x);
         acc[s][1] = __dadd_rn(acc[s][1], f.y);
         if (MOM) acc[s][2] = __dadd_rn(acc[s][2], __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y)));
@@ -2343,7 +2386,7 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
   }
   __syncthreads();
   if (q != 0) return;
-  double* out = partials + (((i64)blockIdx.x * B + b) * 4 + l3) * cross_slots(K);
+  double* out = partials + ((range * B + b) * 4 + l3) * cross_slots(K);
   for (int s = 0; s < nent; ++s) {
     double v[3] = {0.0, 0.0, 0.0};
     for (int r = 0; r < Q; ++r)
@@ -2356,17 +2399,7 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
   }
 }
 
-// d rn(z)^H-side cotangent: g / sqrt(r + eps) - (Re(conj(g) z) / 2 / (r +
-// eps)^1.5) z / |z| (|z| taken as 1 at z = 0), engine.rs:35-46
-__device__ __forceinline__ double2 root_modulus_vjp(double2 z, double2 g) {
-  const double r = hypot(z.x, z.y);
-  const double radial = __dadd_rn(__dmul_rn(g.x, z.x), __dmul_rn(g.y, z.y));
-  const double mag = r == 0.0 ? 1.0 : r;
-  const double s = sqrt(r + 1e-8), c = 0.5 * radial / pow(r + 1e-8, 1.5);
-  return make_double2(__dsub_rn(g.x / s, __dmul_rn(c, z.x) / mag), __dsub_rn(g.y / s, __dmul_rn(c, z.y) / mag));
-}
-
-// grid (pixel ranges, B L); thread (entry i, pixel lane): the cotangents of
+// grid: pixel ranges x (B L), (b, l3) fastest; thread (entry i, pixel lane): the cotangents of
 // entry i of both channels, gv_0 = M v_1 and gv_1 = M^H v_0 (M [K][K]: the
 // cotangents of G), plus through rn the cross S1's (cotangent s):
 // rn-VJP(z_0, s rn(z_1)) and rn-VJP(z_1, conj(s) rn(z_0)).  Pixels outside the
@@ -2378,8 +2411,10 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
                                                              int accumulate, i64 chunk, int PC, T* __restrict__ gz,
                                                              T* __restrict__ gbr) {
   typedef typename V2<T>::type T2;
-  extern __shared__ __align__(16) double2 sm[];  // M [K][K], then [PC][2][K]
-  const int B = Bm / 2, b = blockIdx.y / 4, l3 = blockIdx.y % 4, L = 4, K1 = K - 1;
+  extern __shared__ __align__(16) double2 sm[];  // M [K][K], then [PC][2][K + 1]
+  const int B = Bm / 2, bl = (int)(blockIdx.x % (unsigned)(B * 4)), b = bl / 4, l3 = bl % 4, L = 4, K1 = K - 1;
+  const i64 range = blockIdx.x / (unsigned)(B * 4);
+  const int KS = K + 1;
   double2* mk = sm;
   double2* sv = sm + K * K;
   const T2* Mb = reinterpret_cast<const T2*>(M) + ((i64)b * L + l3) * K * K;
@@ -2390,17 +2425,17 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
   const bool lane = q < Q;
   T2* gzv = reinterpret_cast<T2*>(gz);
   T2* gbv = reinterpret_cast<T2*>(gbr);
-  const i64 P0 = (i64)blockIdx.x * chunk, P1 = min(N, P0 + chunk);
+  const i64 P0 = range * chunk, P1 = min(N, P0 + chunk);
   for (i64 pc = P0; pc < P1; pc += PC) {
     const int np = (int)min((i64)PC, P1 - pc);
     __syncthreads();
-    cross_stage<T>(sv, pc, np, K, Bm, b, l3, z, br, mask);
+    cross_stage<T, true>(sv, pc, np, K, Bm, b, l3, z, br, mask, sc);
     __syncthreads();
     if (!lane) continue;
     for (int j = q; j < np; j += Q) {
       const i64 p = pc + j;
-      const double2* v0 = sv + (size_t)j * 2 * K;
-      const double2* v1 = v0 + K;
+      const double2* v0 = sv + (size_t)j * 2 * KS;
+      const double2* v1 = v0 + KS;
       double2 g0 = make_double2(0.0, 0.0), g1 = make_double2(0.0, 0.0);
       const bool on = !mask || mask[p];
       if (on) {
@@ -2412,15 +2447,9 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
           g1.x = __dadd_rn(g1.x, __dadd_rn(__dmul_rn(c.x, v0[k].x), __dmul_rn(c.y, v0[k].y)));
           g1.y = __dadd_rn(g1.y, __dsub_rn(__dmul_rn(c.x, v0[k].y), __dmul_rn(c.y, v0[k].x)));
         }
-        if (i == K1) {  // the cross S1 through rn
-          const double2 r0 = root_normalise(v0[K1]), r1 = root_normalise(v1[K1]);
-          const double2 ga = make_double2(__dsub_rn(__dmul_rn(sc.x, r1.x), __dmul_rn(sc.y, r1.y)),
-                                          __dadd_rn(__dmul_rn(sc.x, r1.y), __dmul_rn(sc.y, r1.x)));
-          const double2 gb = make_double2(__dadd_rn(__dmul_rn(sc.x, r0.x), __dmul_rn(sc.y, r0.y)),
-                                          __dsub_rn(__dmul_rn(sc.x, r0.y), __dmul_rn(sc.y, r0.x)));
-          const double2 d0 = root_modulus_vjp(v0[K1], ga), d1 = root_modulus_vjp(v1[K1], gb);
-          g0.x = __dadd_rn(g0.x, d0.x); g0.y = __dadd_rn(g0.y, d0.y);
-          g1.x = __dadd_rn(g1.x, d1.x); g1.y = __dadd_rn(g1.y, d1.y);
+        if (i == K1) {  // the cross S1 through rn, staged
+          g0.x = __dadd_rn(g0.x, v0[K].x); g0.y = __dadd_rn(g0.y, v0[K].y);
+          g1.x = __dadd_rn(g1.x, v1[K].x); g1.y = __dadd_rn(g1.y, v1[K].y);
         }
       } else if (accumulate) {
         continue;
@@ -2449,9 +2478,9 @@ void cross_forward(int K, i64 N, int Bm, const T* z, const T* br, const uint8_t*
   const int E = K * K + 1, NE = std::min(E, kCrossThreads), Q = kCrossThreads / NE;
   if ((E + NE - 1) / NE > kCrossMaxEnt) throw std::runtime_error("too many cross terms per level");
   const int PC = cross_chunk(K);
-  const size_t smem = std::max(sizeof(double2) * PC * 2 * K, sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
+  const size_t smem = std::max(sizeof(double2) * PC * 2 * (K + 1), sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
   const i64 chunk = (N + nblk - 1) / nblk;
-  dim3 grid((unsigned)nblk, (unsigned)(Bm / 2 * 4));
+  const unsigned grid = (unsigned)nblk * (unsigned)(Bm / 2 * 4);
   if (moments) {
     if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, true>);
     k_cross_fwd<T, true><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
@@ -2471,17 +2500,18 @@ void cross_reverse(int K, i64 N, int Bm, const T* z, const T* br, const T* M, co
                    bool accumulate, T* gz, T* gbr, cudaStream_t s) {
   if (K > kCrossThreads) throw std::runtime_error("too many operands for the cross VJP");
   const int PC = cross_chunk(K);
-  const size_t smem = sizeof(double2) * ((size_t)K * K + (size_t)PC * 2 * K);
+  const size_t smem = sizeof(double2) * ((size_t)K * K + (size_t)PC * 2 * (K + 1));
   if (smem > 48 * 1024) allow_dynamic_smem(k_cross_rev<T>);
   const i64 per = 4 * (i64)PC;  // pixels per CTA
-  const unsigned nblk = (unsigned)std::max<i64>(1, (N + per - 1) / per);
-  dim3 grid(nblk, (unsigned)(Bm / 2 * 4));
+  const i64 nblk = std::max<i64>(1, (N + per - 1) / per);
+  if (nblk * (Bm / 2 * 4) > INT32_MAX) throw std::runtime_error("too many pixels for the cross VJP");
+  const unsigned grid = (unsigned)(nblk * (Bm / 2 * 4));
   k_cross_rev<T><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, M, s1, mask, accumulate ? 1 : 0, per, PC, gz,
                                                    gbr);
   STL_CUDA(cudaGetLastError());
 }
 
-int cross_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(296, (N + 4095) / 4096)); }
+int cross_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(296, (N + 1023) / 1024)); }
 
 int means_blocks(i64 N) { return (int)std::max<i64>(1, std::min<i64>(kMeansBlocks, (N + 1023) / 1024)); }
 
