@@ -2258,8 +2258,11 @@ void build_mean_var(const double* cot, int np, int B, int K, const double* count
 // 3 doubles: G (re, im) at 2 (r K + q), the S1 term at 2 K^2, the second
 // sums of G at 2 K^2 + 2 + r K + q and of the S1 term at 3 K^2 + 2.
 constexpr int kCrossThreads = 256;
-// pixels staged at a time: as many as 48 KB hold (both channels, K + 1 values, FP64), 16 to 256
-inline int cross_chunk(int K) { return std::max(16, std::min(256, (48 * 1024) / (2 * (K + 1) * 16))); }
+// pixels staged at a time: as many as 48 KB hold (both channels, K + 1 values,
+// FP64, with moduli 24 bytes a value), 16 to 256
+inline int cross_chunk(int K, bool moduli = false) {
+  return std::max(16, std::min(256, (48 * 1024) / (2 * (K + 1) * (moduli ? 24 : 16))));
+}
 constexpr int kCrossMaxEnt = 8;  // entries per thread (K^2 + 1 <= 8 x 256)
 
 
@@ -2288,9 +2291,10 @@ __device__ __forceinline__ double2 root_modulus_vjp(double2 z, double2 g) {
 // thread, the same instructions for both channels) instead of in the thread
 // that owns the S1 term: rn(z_c) for the sums, and for the VJP (REV) the
 // rn-VJP of the S1 term with cotangent sc, rn-VJP(z_c, sc_c rn(z_{1-c})), sc_0
-// = sc and sc_1 = conj(sc).  Pixels outside the mask stage zeros.
+// = sc and sc_1 = conj(sc).  Pixels outside the mask stage zeros.  With nv,
+// the squared moduli of the staged values go to nv[j][c][i] as well.
 template <typename T, bool REV>
-__device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, int Bm, int b, int l3,
+__device__ __forceinline__ void cross_stage(double2* sv, double* nv, i64 p0, int np, int K, int Bm, int b, int l3,
                                             const T* __restrict__ z, const T* __restrict__ br,
                                             const uint8_t* __restrict__ mask, double2 sc) {
   typedef typename V2<T>::type T2;
@@ -2307,6 +2311,7 @@ __device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, 
       v = make_double2((double)w.x, (double)w.y);
     }
     sv[(size_t)j * 2 * KS + c * KS + i] = v;
+    if (nv) nv[(size_t)j * 2 * KS + c * KS + i] = fma(v.x, v.x, v.y * v.y);
   }
   for (int t = threadIdx.x; t < np * 2; t += blockDim.x) {
     const int j = t >> 1, c = t & 1;
@@ -2326,18 +2331,23 @@ __device__ __forceinline__ void cross_stage(double2* sv, i64 p0, int np, int K, 
       }
     }
     sv[(size_t)j * 2 * KS + c * KS + K] = v;
+    if (nv) nv[(size_t)j * 2 * KS + c * KS + K] = fma(v.x, v.x, v.y * v.y);
   }
 }
 
 // grid: pixel ranges x (B L), (b, l3) fastest so that the four gauges of a
 // range, which share the operands' 32-byte sectors, run together; partials
 // [range][b][l3][xslots]
-template <typename T, bool MOM>
+// NENT: entries a thread holds (the power of two at or above ceil((K^2 + 1) /
+// 256)), so that the sums of one entry take 3 registers pairs, not 3 kCrossMaxEnt.
+// The products go through FMAs, and the second sums use |a conj(b)|^2 = |a|^2
+// |b|^2 with the staged squared moduli.
+template <typename T, bool MOM, int NENT>
 __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int Bm, const T* __restrict__ z,
                                                              const T* __restrict__ br,
                                                              const uint8_t* __restrict__ mask, i64 chunk, int PC,
                                                              double* __restrict__ partials) {
-  extern __shared__ __align__(16) double2 sv[];  // [PC][2][K + 1], then the lane sums
+  extern __shared__ __align__(16) double2 sv[];  // [PC][2][K + 1], (MOM) moduli [PC][2][K + 1]; then the lane sums
   const int B = Bm / 2, bl = (int)(blockIdx.x % (unsigned)(B * 4)), b = bl / 4, l3 = bl % 4;
   const i64 range = blockIdx.x / (unsigned)(B * 4);
   const int E = K * K + 1, NE = min(E, kCrossThreads), Q = kCrossThreads / NE;
@@ -2345,10 +2355,11 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
   const int nent = (E - e0 + NE - 1) / NE;  // entries of this thread: e0, e0 + NE, ...
   const bool lane = q < Q;
   const int KS = K + 1;
-  double acc[kCrossMaxEnt][3];
-  int ri[kCrossMaxEnt], qi[kCrossMaxEnt];  // the entry's operands: (r, q) of G, (K, K) for the S1 term
+  double* nv = MOM ? reinterpret_cast<double*>(sv + (size_t)PC * 2 * KS) : nullptr;
+  double acc[NENT][3];
+  int ri[NENT], qi[NENT];  // the entry's operands: (r, q) of G, (K, K) for the S1 term
 #pragma unroll
-  for (int s = 0; s < kCrossMaxEnt; ++s) {
+  for (int s = 0; s < NENT; ++s) {
     acc[s][0] = acc[s][1] = acc[s][2] = 0.0;
     const int e = e0 + s * NE;
     ri[s] = e < K * K ? e / K : K;
@@ -2358,31 +2369,34 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
   for (i64 pc = P0; pc < P1; pc += PC) {
     const int np = (int)min((i64)PC, P1 - pc);
     __syncthreads();
-    cross_stage<T, false>(sv, pc, np, K, Bm, b, l3, z, br, mask, make_double2(0.0, 0.0));
+    cross_stage<T, false>(sv, nv, pc, np, K, Bm, b, l3, z, br, mask, make_double2(0.0, 0.0));
     __syncthreads();
     if (!lane) continue;
     for (int j = q; j < np; j += Q) {
       const double2* v0 = sv + (size_t)j * 2 * KS;
       const double2* v1 = v0 + KS;
 #pragma unroll
-      for (int s = 0; s < kCrossMaxEnt; ++s) {  // static indices: the sums stay in registers
+      for (int s = 0; s < NENT; ++s) {  // static indices: the sums stay in registers
         if (s >= nent) continue;
-        const double2 f = cmul_conj(v0[ri[s]], v1[qi[s]]);
-        acc[s][0] = __dadd_rn(acc[s][0], f.x);
-        acc[s][1] = __dadd_rn(acc[s][1], f.y);
-        if (MOM) acc[s][2] = __dadd_rn(acc[s][2], __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y)));
+        const double2 a = v0[ri[s]], c = v1[qi[s]];
+        acc[s][0] = fma(a.y, c.y, fma(a.x, c.x, acc[s][0]));
+        acc[s][1] = fma(-a.x, c.y, fma(a.y, c.x, acc[s][1]));
+        if (MOM) {
+          const double* n0 = nv + (size_t)j * 2 * KS;
+          acc[s][2] = fma(n0[ri[s]], n0[KS + qi[s]], acc[s][2]);
+        }
       }
     }
   }
   // lanes of an entry added in lane order (through the staging memory)
   __syncthreads();
-  double* red = reinterpret_cast<double*>(sv);  // [Q][NE][kCrossMaxEnt][3]
+  double* red = reinterpret_cast<double*>(sv);  // [Q][NE][NENT][3]
   if (lane) {
 #pragma unroll
-    for (int s = 0; s < kCrossMaxEnt; ++s)
+    for (int s = 0; s < NENT; ++s)
       if (s < nent)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) red[(((size_t)q * NE + e0) * kCrossMaxEnt + s) * 3 + k] = acc[s][k];
+        for (int k = 0; k < 3; ++k) red[(((size_t)q * NE + e0) * NENT + s) * 3 + k] = acc[s][k];
   }
   __syncthreads();
   if (q != 0) return;
@@ -2390,7 +2404,7 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_fwd(i64 N, int K, int B
   for (int s = 0; s < nent; ++s) {
     double v[3] = {0.0, 0.0, 0.0};
     for (int r = 0; r < Q; ++r)
-      for (int k = 0; k < 3; ++k) v[k] = __dadd_rn(v[k], red[(((size_t)r * NE + e0) * kCrossMaxEnt + s) * 3 + k]);
+      for (int k = 0; k < 3; ++k) v[k] = __dadd_rn(v[k], red[(((size_t)r * NE + e0) * NENT + s) * 3 + k]);
     const int e = e0 + s * NE;
     const int at = e < K * K ? 2 * e : 2 * K * K;
     out[at] = v[0];
@@ -2429,7 +2443,7 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
   for (i64 pc = P0; pc < P1; pc += PC) {
     const int np = (int)min((i64)PC, P1 - pc);
     __syncthreads();
-    cross_stage<T, true>(sv, pc, np, K, Bm, b, l3, z, br, mask, sc);
+    cross_stage<T, true>(sv, nullptr, pc, np, K, Bm, b, l3, z, br, mask, sc);
     __syncthreads();
     if (!lane) continue;
     for (int j = q; j < np; j += Q) {
@@ -2472,22 +2486,38 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
   }
 }
 
+template <typename T, bool MOM, int NENT>
+void launch_cross_fwd(unsigned grid, size_t smem, cudaStream_t s, i64 N, int K, int Bm, const T* z, const T* br,
+                      const uint8_t* mask, i64 chunk, int PC, double* partials) {
+  if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, MOM, NENT>);
+  k_cross_fwd<T, MOM, NENT><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
+}
+
+template <typename T, bool MOM>
+void launch_cross_fwd(int nent, unsigned grid, size_t smem, cudaStream_t s, i64 N, int K, int Bm, const T* z,
+                      const T* br, const uint8_t* mask, i64 chunk, int PC, double* partials) {
+  if (nent <= 1) launch_cross_fwd<T, MOM, 1>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else if (nent <= 2) launch_cross_fwd<T, MOM, 2>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else if (nent <= 4) launch_cross_fwd<T, MOM, 4>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else launch_cross_fwd<T, MOM, kCrossMaxEnt>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+}
+
 template <typename T>
 void cross_forward(int K, i64 N, int Bm, const T* z, const T* br, const uint8_t* mask, bool moments,
                    double* partials, int nblk, double* sums, cudaStream_t s) {
   const int E = K * K + 1, NE = std::min(E, kCrossThreads), Q = kCrossThreads / NE;
-  if ((E + NE - 1) / NE > kCrossMaxEnt) throw std::runtime_error("too many cross terms per level");
-  const int PC = cross_chunk(K);
-  const size_t smem = std::max(sizeof(double2) * PC * 2 * (K + 1), sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
+  const int nent = (E + NE - 1) / NE;
+  if (nent > kCrossMaxEnt) throw std::runtime_error("too many cross terms per level");
+  const int NENT = nent <= 1 ? 1 : nent <= 2 ? 2 : nent <= 4 ? 4 : kCrossMaxEnt;
+  const int PC = cross_chunk(K, moments);
+  const size_t stage = (sizeof(double2) + (moments ? sizeof(double) : 0)) * (size_t)PC * 2 * (K + 1);
+  const size_t smem = std::max(stage, sizeof(double) * (size_t)Q * NE * NENT * 3);
   const i64 chunk = (N + nblk - 1) / nblk;
   const unsigned grid = (unsigned)nblk * (unsigned)(Bm / 2 * 4);
-  if (moments) {
-    if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, true>);
-    k_cross_fwd<T, true><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
-  } else {
-    if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd<T, false>);
-    k_cross_fwd<T, false><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
-  }
+  if (moments)
+    launch_cross_fwd<T, true>(nent, grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else
+    launch_cross_fwd<T, false>(nent, grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
   STL_CUDA(cudaGetLastError());
   const i64 rows = (i64)Bm / 2 * 4, total = rows * cross_slots(K);
   k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, nblk, (int)rows,
