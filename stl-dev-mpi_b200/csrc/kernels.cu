@@ -2270,19 +2270,23 @@ __device__ __forceinline__ double2 cmul_conj(double2 a, double2 b) {  // a conj(
   return make_double2(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
                       __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y)));
 }
+// rn(z) = z / sqrt(|z| + 1e-8) as z times one reciprocal square root (a few
+// ulp from the quotient; the operands are far from overflow, so |z| needs no
+// hypot scaling)
 __device__ __forceinline__ double2 root_normalise(double2 z) {
-  const double s = sqrt(hypot(z.x, z.y) + 1e-8);
-  return make_double2(z.x / s, z.y / s);
+  const double inv = rsqrt(sqrt(fma(z.x, z.x, z.y * z.y)) + 1e-8);
+  return make_double2(z.x * inv, z.y * inv);
 }
 
 // d rn(z)^H-side cotangent: g / sqrt(r + eps) - (Re(conj(g) z) / 2 / (r +
 // eps)^1.5) z / |z| (|z| taken as 1 at z = 0), engine.rs:35-46
+// with inv = (|z| + eps)^-1/2: (r + eps)^-1.5 = inv^3, and z / |z| takes one reciprocal
 __device__ __forceinline__ double2 root_modulus_vjp(double2 z, double2 g) {
-  const double r = hypot(z.x, z.y);
-  const double radial = __dadd_rn(__dmul_rn(g.x, z.x), __dmul_rn(g.y, z.y));
-  const double mag = r == 0.0 ? 1.0 : r;
-  const double s = sqrt(r + 1e-8), c = 0.5 * radial / pow(r + 1e-8, 1.5);
-  return make_double2(__dsub_rn(g.x / s, __dmul_rn(c, z.x) / mag), __dsub_rn(g.y / s, __dmul_rn(c, z.y) / mag));
+  const double r = sqrt(fma(z.x, z.x, z.y * z.y));
+  const double radial = fma(g.x, z.x, g.y * z.y);
+  const double inv = rsqrt(r + 1e-8);
+  const double c = 0.5 * radial * (inv * inv * inv) * (1.0 / (r == 0.0 ? 1.0 : r));
+  return make_double2(fma(g.x, inv, -c * z.x), fma(g.y, inv, -c * z.y));
 }
 
 // stage the chunk's operand vectors of both channels as FP64, K + 1 values a
@@ -2446,41 +2450,49 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
     cross_stage<T, true>(sv, nullptr, pc, np, K, Bm, b, l3, z, br, mask, sc);
     __syncthreads();
     if (!lane) continue;
-    for (int j = q; j < np; j += Q) {
-      const i64 p = pc + j;
-      const double2* v0 = sv + (size_t)j * 2 * KS;
-      const double2* v1 = v0 + KS;
-      double2 g0 = make_double2(0.0, 0.0), g1 = make_double2(0.0, 0.0);
-      const bool on = !mask || mask[p];
-      if (on) {
-        for (int k = 0; k < K; ++k) {
-          const double2 a = mk[i * K + k], c = mk[k * K + i];
-          // g0 += M[i][k] v1[k]; g1 += conj(M[k][i]) v0[k]
-          g0.x = __dadd_rn(g0.x, __dsub_rn(__dmul_rn(a.x, v1[k].x), __dmul_rn(a.y, v1[k].y)));
-          g0.y = __dadd_rn(g0.y, __dadd_rn(__dmul_rn(a.x, v1[k].y), __dmul_rn(a.y, v1[k].x)));
-          g1.x = __dadd_rn(g1.x, __dadd_rn(__dmul_rn(c.x, v0[k].x), __dmul_rn(c.y, v0[k].y)));
-          g1.y = __dadd_rn(g1.y, __dsub_rn(__dmul_rn(c.x, v0[k].y), __dmul_rn(c.y, v0[k].x)));
+    // two pixels a step (j and j + Q; the second repeats the first past the
+    // chunk's end and is not written), so each entry of M loaded serves both;
+    // pixels outside the mask staged zeros, so their cotangents come out zero
+    for (int j = q; j < np; j += 2 * Q) {
+      const int jb = j + Q < np ? j + Q : j;
+      const double2* v0[2] = {sv + (size_t)j * 2 * KS, sv + (size_t)jb * 2 * KS};
+      double2 g[2][2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) g[u][0] = g[u][1] = make_double2(0.0, 0.0);
+      for (int k = 0; k < K; ++k) {
+        const double2 a = mk[i * K + k], c = mk[k * K + i];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {  // g_0 += M[i][k] v_1[k]; g_1 += conj(M[k][i]) v_0[k]
+          const double2 w0 = v0[u][k], w1 = v0[u][KS + k];
+          g[u][0].x = fma(a.x, w1.x, fma(-a.y, w1.y, g[u][0].x));
+          g[u][0].y = fma(a.x, w1.y, fma(a.y, w1.x, g[u][0].y));
+          g[u][1].x = fma(c.x, w0.x, fma(c.y, w0.y, g[u][1].x));
+          g[u][1].y = fma(c.x, w0.y, fma(-c.y, w0.x, g[u][1].y));
         }
-        if (i == K1) {  // the cross S1 through rn, staged
-          g0.x = __dadd_rn(g0.x, v0[K].x); g0.y = __dadd_rn(g0.y, v0[K].y);
-          g1.x = __dadd_rn(g1.x, v1[K].x); g1.y = __dadd_rn(g1.y, v1[K].y);
-        }
-      } else if (accumulate) {
-        continue;
       }
-      for (int c = 0; c < 2; ++c) {
-        const double2 gv = c ? g1 : g0;
-        const i64 m = 2 * b + c;
-        T2* dst = i < K1 ? gbv + ((p * Bm + m) * K1 + i) * L + l3 : gzv + (p * Bm + m) * L + l3;
-        T2 o;
-        o.x = (T)gv.x;
-        o.y = (T)gv.y;
-        if (accumulate) {
-          const T2 prev = *dst;
-          o.x += prev.x;
-          o.y += prev.y;
+      for (int u = 0; u < 2; ++u) {
+        if (u == 1 && jb == j) break;
+        const int jj = u ? jb : j;
+        const i64 p = pc + jj;
+        if (accumulate && mask && !mask[p]) continue;
+        if (i == K1) {  // the cross S1 through rn, staged
+          g[u][0].x += v0[u][K].x; g[u][0].y += v0[u][K].y;
+          g[u][1].x += v0[u][KS + K].x; g[u][1].y += v0[u][KS + K].y;
         }
-        *dst = o;
+        for (int c = 0; c < 2; ++c) {
+          const double2 gv = g[u][c];
+          const i64 m = 2 * b + c;
+          T2* dst = i < K1 ? gbv + ((p * Bm + m) * K1 + i) * L + l3 : gzv + (p * Bm + m) * L + l3;
+          T2 o;
+          o.x = (T)gv.x;
+          o.y = (T)gv.y;
+          if (accumulate) {
+            const T2 prev = *dst;
+            o.x += prev.x;
+            o.y += prev.y;
+          }
+          *dst = o;
+        }
       }
     }
   }
