@@ -2264,6 +2264,7 @@ inline int cross_chunk(int K, bool moduli = false) {
   return std::max(16, std::min(256, (48 * 1024) / (2 * (K + 1) * (moduli ? 24 : 16))));
 }
 constexpr int kCrossMaxEnt = 8;  // entries per thread (K^2 + 1 <= 8 x 256)
+constexpr int kStageLoads = 4;   // operand loads a staging thread keeps in flight
 
 
 __device__ __forceinline__ double2 cmul_conj(double2 a, double2 b) {  // a conj(b), products rounded one by one
@@ -2304,18 +2305,33 @@ __device__ __forceinline__ void cross_stage(double2* sv, double* nv, i64 p0, int
   typedef typename V2<T>::type T2;
   const T2* zv = reinterpret_cast<const T2*>(z);
   const T2* bv = reinterpret_cast<const T2*>(br);
-  const int K1 = K - 1, KS = K + 1, L = 4;
-  for (int t = threadIdx.x; t < np * 2 * K; t += blockDim.x) {
-    const int j = t / (2 * K), rem = t - j * 2 * K, c = rem / K, i = rem - c * K;
-    const i64 p = p0 + j;
-    const i64 m = 2 * b + c;
-    double2 v = make_double2(0.0, 0.0);
-    if (!mask || mask[p]) {
-      const T2 w = i < K1 ? bv[((p * Bm + m) * K1 + i) * L + l3] : zv[(p * Bm + m) * L + l3];
-      v = make_double2((double)w.x, (double)w.y);
+  const int K1 = K - 1, KS = K + 1, L = 4, n = np * 2 * K;
+  // kStageLoads independent loads in flight a thread (the pixel's mask byte
+  // among them, applied after the loads return: every load is in range)
+  for (int t0 = threadIdx.x; t0 < n; t0 += kStageLoads * (int)blockDim.x) {
+    T2 w[kStageLoads];
+    int at[kStageLoads];
+    uint8_t on[kStageLoads];
+#pragma unroll
+    for (int u = 0; u < kStageLoads; ++u) {
+      const int t = t0 + u * (int)blockDim.x;
+      at[u] = -1;
+      if (t < n) {
+        const int j = t / (2 * K), rem = t - j * 2 * K, c = rem / K, i = rem - c * K;
+        const i64 p = p0 + j;
+        const i64 m = 2 * b + c;
+        w[u] = i < K1 ? bv[((p * Bm + m) * K1 + i) * L + l3] : zv[(p * Bm + m) * L + l3];
+        on[u] = mask ? mask[p] : 1;
+        at[u] = j * 2 * KS + c * KS + i;
+      }
     }
-    sv[(size_t)j * 2 * KS + c * KS + i] = v;
-    if (nv) nv[(size_t)j * 2 * KS + c * KS + i] = fma(v.x, v.x, v.y * v.y);
+#pragma unroll
+    for (int u = 0; u < kStageLoads; ++u) {
+      if (at[u] < 0) continue;
+      const double2 v = on[u] ? make_double2((double)w[u].x, (double)w[u].y) : make_double2(0.0, 0.0);
+      sv[at[u]] = v;
+      if (nv) nv[at[u]] = fma(v.x, v.x, v.y * v.y);
+    }
   }
   for (int t = threadIdx.x; t < np * 2; t += blockDim.x) {
     const int j = t >> 1, c = t & 1;
