@@ -2359,7 +2359,7 @@ __device__ __forceinline__ void cross_stage(double2* sv, double* nv, i64 p0, int
 // range, which share the operands' 32-byte sectors, run together; partials
 // [range][b][l3][xslots]
 // NENT: entries a thread holds (the power of two at or above ceil((K^2 + 1) /
-// 256)), so that the sums of one entry take 3 registers pairs, not 3 kCrossMaxEnt.
+// 256)), so that a thread's sums take 3 NENT register pairs, not 3 kCrossMaxEnt.
 // The products go through FMAs, and the second sums use |a conj(b)|^2 = |a|^2
 // |b|^2 with the staged squared moduli.
 template <typename T, bool MOM, int NENT>
