@@ -91,9 +91,10 @@ int stlp_set_stream(StlpHandle* h, uint64_t stream);
  * (cudaStream_t as an integer); returns after the launches, without waiting.
  * Allocates nothing: the partial sums sit in a fixed device array of at most
  * 64 maps (296 KiB); a larger batch is refused.  Calls in flight together on
- * one device race on that array.  The first call on a device looks up the
- * array's address (make it before any stream capture).  No reference
- * counterpart. */
+ * one device race on that array.  The first call on a device, and the
+ * first after a reset of the device (a new context), looks up the array's
+ * address (make it before any stream capture).  The stream must belong to
+ * the current device (refused otherwise).  No reference counterpart. */
 int stlp_mean_var_noalloc(uint64_t x, size_t n_pix, size_t batch, int f32, uint64_t out, uint64_t stream);
 
 /* Builds the device operators now instead of at the first forward.  No

@@ -824,7 +824,7 @@ class EngineImpl final : public Engine {
     prof_.collect();
     if (err) {
       STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
-      throw std::runtime_error("a wait on a staged device copy timed out in the forward sweep");
+      throw std::runtime_error(wait_timeout_message(err, "the forward sweep"));
     }
     forward_done_ = true;
     timers.forward_ms += ms_since(t0);
@@ -1094,7 +1094,7 @@ class EngineImpl final : public Engine {
     prof_.collect();
     if (err) {
       STL_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s));
-      throw std::runtime_error("a wait on a staged device copy timed out in the reverse sweep");
+      throw std::runtime_error(wait_timeout_message(err, "the reverse sweep"));
     }
     timers.reverse_ms += ms_since(t0);
     timers.reverses += 1;

@@ -79,6 +79,15 @@ struct PinnedMem {
   void release();
 };
 
+// Message of a kernel's timed-out copy wait (the error flag's value: 1 a
+// wait ran out, 2 also the drain of the copies in flight); the results of
+// the sweep are discarded either way.
+inline std::string wait_timeout_message(int err, const char* where) {
+  std::string m = std::string("a wait on a staged device copy timed out in ") + where;
+  if (err >= 2) m += " while copies were still in flight (rebuild the engine before using it again)";
+  return m;
+}
+
 // Device memory accounting (bytes held by live DevMem allocations).
 size_t device_bytes_live();
 size_t device_bytes_peak();

@@ -44,8 +44,13 @@ __device__ __forceinline__ i64 rot_cell(i64 c, int k, int o2) {
 
 // ---- bulk asynchronous copies ------------------------------------------------
 // Every wait on an mbarrier is bounded (kWaitLimit polls); a kernel that
-// gives up records the failure in an error flag the host reads.
+// gives up records the failure in an error flag the host reads: kErrWait
+// when a wait ran out and the CTA then saw its copies in flight land,
+// kErrDrain when that drain ran out too (a copy may still have been writing
+// the CTA's shared memory when it exited).  Either way the launch's results
+// are discarded by the host.
 constexpr int kWaitLimit = 1 << 20;
+constexpr int kErrWait = 1, kErrDrain = 2;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -362,8 +367,9 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     if (tid == 0 && c + 2 < nch) issue(c + 2);
   }
   if (fail) {
-    for (int q = c; q < min(nch, c + 2); ++q) mbar_wait(&bar[q & 1], (q >> 1) & 1);
-    if (tid == 0) atomicExch(err, 1);
+    bool drained = true;
+    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
     return;
   }
   if (row >= rows) return;
@@ -747,8 +753,9 @@ __global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
     if (tid == 0 && c + 2 < nch) issue(c + 2);
   }
   if (fail) {
-    for (int q = c; q < min(nch, c + 2); ++q) mbar_wait(&bar[q & 1], (q >> 1) & 1);
-    if (tid == 0) atomicExch(err, 1);
+    bool drained = true;
+    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
     return;
   }
   // partials [tile][k][ncs][R]
@@ -1046,8 +1053,10 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
   }
   if (fail) {
     // wait (bounded) for the copies still in flight into this CTA's stages
-    for (int k = c; k < min(nchunks, c + kProdStages); ++k) mbar_wait(&bar[k % kProdStages], (k / kProdStages) & 1);
-    if (threadIdx.x == 0) atomicExch(err, 1);
+    bool drained = true;
+    for (int k = c; k < min(nchunks, c + kProdStages); ++k)
+      drained &= mbar_wait(&bar[k % kProdStages], (k / kProdStages) & 1);
+    if (threadIdx.x == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
   }
   if (!kSplit) {
 #pragma unroll

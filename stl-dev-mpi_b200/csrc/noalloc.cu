@@ -48,26 +48,51 @@ static __device__ __align__(256) double g_noalloc_partials[kNoAllocScratch];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
+// per device: the context the address was looked up in, and the address
+void* g_ctx[kMaxDevices] = {};
 double* g_partials[kMaxDevices] = {};
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// The driver's current context (cuCtxGetCurrent through the runtime's entry
+// point table, so the library needs no link to the driver library).  A
+// device reset destroys the device's primary context, and the runtime makes
+// a new one at the next call: the scratch then has another address.
+void* current_context() {
+  typedef int (*GetCtx)(void**);
+  static GetCtx get = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCtx>(f);
+  }();
+  void* ctx = nullptr;
+  if (!get || get(&ctx) != 0) throw std::runtime_error("cuCtxGetCurrent failed");
+  return ctx;
+}
+
 // Device address of the scratch on the current device, looked up once per
-// device (cudaGetSymbolAddress may load the module on that device).  The
-// first call on a device therefore does this set-up; when the call is to be
-// recorded in a stream capture, make one call on that device before the
-// capture starts.
+// device and context (cudaGetSymbolAddress may load the module on that
+// device).  The first call on a device -- and the first after a reset of
+// the device -- therefore does this set-up; when the call is to be recorded
+// in a stream capture, make one call on that device before the capture
+// starts.
 double* partials_on_current_device() {
   int dev = -1;
   check(cudaGetDevice(&dev), "cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("device ordinal out of range");
+  void* ctx = current_context();  // null before the runtime first binds a context on this thread
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_partials[dev]) {
+  if (!g_partials[dev] || !ctx || g_ctx[dev] != ctx) {
     void* p = nullptr;
+    // binds the device's primary context when none is current
     check(cudaGetSymbolAddress(&p, g_noalloc_partials), "cudaGetSymbolAddress of the fixed scratch");
     g_partials[dev] = static_cast<double*>(p);
+    g_ctx[dev] = current_context();
   }
   return g_partials[dev];
 }
@@ -133,8 +158,14 @@ extern "C" int stlp_mean_var_noalloc(uint64_t x, size_t n_pix, size_t batch, int
       throw std::runtime_error("batch " + std::to_string(batch) + " exceeds the " +
                                std::to_string(kNoAllocMaxMaps) + " maps the fixed device scratch holds");
     if (n_pix > (size_t)INT64_MAX / batch) throw std::runtime_error("map size out of range");
-    double* part = partials_on_current_device();
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int dev = -1, sdev = -1;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaStreamGetDevice(s, &sdev), "cudaStreamGetDevice");
+    if (sdev != dev)
+      throw std::runtime_error("the stream belongs to device " + std::to_string(sdev) + ", the current device is " +
+                               std::to_string(dev) + ": make the stream's device current before the call");
+    double* part = partials_on_current_device();
     const dim3 grid(kNoAllocBlocks, (unsigned)batch);
     if (f32)
       k_mv_partials<float><<<grid, kNoAllocThreads, 0, s>>>(reinterpret_cast<const float*>(x), (i64)n_pix, part);

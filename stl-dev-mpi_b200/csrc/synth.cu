@@ -221,7 +221,7 @@ struct SynthObjective {
     std::memcpy(&err, h + 2, sizeof(int));
     if (err) {
       STL_CUDA(cudaMemsetAsync(e.error_flag(), 0, sizeof(int), s));
-      throw std::runtime_error("a wait on a staged device copy timed out in the synthesis objective");
+      throw std::runtime_error(wait_timeout_message(err, "the synthesis objective"));
     }
     const double loss = h[0];
     if (!std::isfinite(loss) || h[1] != 0.0) throw std::runtime_error("non-finite synthesis loss or gradient");
@@ -499,9 +499,9 @@ long long minimize_graph(Engine& e, DeviceOps& ops, SynthObjective& obj, double*
   for (long long it = 2; it <= o.max_iter; ++it) {
     G.launch(ops.s, t);
     const double* h = G.host();
-    if (G.err()) {
+    if (const int err = G.err()) {
       STL_CUDA(cudaMemsetAsync(e.error_flag(), 0, sizeof(int), ops.s));
-      throw std::runtime_error("a wait on a staged device copy timed out in the synthesis objective");
+      throw std::runtime_error(wait_timeout_message(err, "the synthesis objective"));
     }
     const double prev_loss = loss;
     gtd = h[SC_GTD];

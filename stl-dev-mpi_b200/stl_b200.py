@@ -336,6 +336,11 @@ class NativeEngine:
             self._current_key = key
             return values, var
 
+    def _require_state(self, key):
+        # a VJP runs on the forward state of its own identity only
+        if key != self._current_key:
+            raise RuntimeError("no forward state of this identity: it is stale or was never computed")
+
     def _cotangent(self, cotangents):
         c = np.ascontiguousarray(cotangents, dtype=np.complex128)
         if c.shape == self._shape()[1:] and self.batch == 1:
@@ -351,8 +356,7 @@ class NativeEngine:
         with self._mutex:
             self._open()
             key = _key(generation, member, objective)
-            if key != self._current_key:
-                raise RuntimeError("stale/wrong-member/objective forward state")
+            self._require_state(key)
             c = self._cotangent(cotangents)
             grad = np.empty(self._map_shape)
             if self._lib.stlp_vjp(self._handle, _ptr(c.view(np.float64)), c.size, *key, _ptr(grad)):
@@ -360,26 +364,32 @@ class NativeEngine:
             return grad
 
     def checkpoint(self):
+        """A copy of the current forward state (the level-0 maps it ran on),
+        tagged with that state's identity; restore() brings it back."""
         with self._mutex:
             self._open()
-            p = self._lib.stlp_checkpoint(self._handle)
-            if not p:
+            saved = self._lib.stlp_checkpoint(self._handle)
+            if not saved:
                 raise _error()
-            return Snapshot(p, self._current_key, self._handle)
+            return Snapshot(saved, self._current_key, self._handle)
 
     def restore(self, snapshot, generation=0, member=0, objective="gaussian"):
+        """Reinstates a Snapshot of this engine as the forward state of the
+        identity (generation, member, objective), which must be the one the
+        snapshot was taken under."""
+        wanted = _key(generation, member, objective)
+        live = isinstance(snapshot, Snapshot) and bool(snapshot._handle)
+        if not live:
+            raise ValueError("restore needs an open Snapshot from checkpoint()")
         with self._mutex:
             self._open()
-            key = _key(generation, member, objective)
-            if not isinstance(snapshot, Snapshot) or not snapshot._handle:
-                raise ValueError("checkpoint is closed or invalid")
-            if snapshot.key != key:
-                raise RuntimeError("stale/wrong-member/objective checkpoint state")
             if snapshot.owner != self._handle:
-                raise ValueError("checkpoint engine/plan owner mismatch")
-            if self._lib.stlp_restore(self._handle, snapshot._handle, *key):
+                raise ValueError("the snapshot belongs to another engine")
+            if snapshot.key != wanted:
+                raise RuntimeError("the snapshot holds a stale or different forward identity")
+            if self._lib.stlp_restore(self._handle, snapshot._handle, *wanted):
                 raise _error()
-            self._current_key = key
+            self._current_key = wanted
 
     # -- CUDA tensors -----------------------------------------------------------
     def _bind_stream(self, torch):
@@ -415,8 +425,7 @@ class NativeEngine:
         with self._mutex:
             self._open()
             key = _key(generation, member, objective)
-            if key != self._current_key:
-                raise RuntimeError("stale/wrong-member/objective forward state")
+            self._require_state(key)
             if not (out.is_cuda and out.is_contiguous() and out.numel() == self.batch * self.channels * self.npix
                     and out.dtype in (torch.float32, torch.float64)):
                 raise ValueError("out must be a contiguous float32/float64 CUDA tensor [batch, npix]")
@@ -467,52 +476,88 @@ def scattering(engine, x):
     return _ScatCov.apply(x, engine)
 
 
-def native_lbfgs(callback, x, options=None):
-    """L-BFGS with the strong Wolfe line search (stlp_lbfgs) of
-    ``callback(x) -> (loss, gradient)`` from ``x``; a float64 C-contiguous ``x``
-    is updated in place.  Options: lr, max_iter, max_eval, tolerance_grad,
-    tolerance_change, history_size.  Returns (x, report) as native.py:1023-1056."""
-    resolved = dict(lr=1.0, max_iter=20, max_eval=None, tolerance_grad=1e-12, tolerance_change=1e-15,
-                    history_size=10)
-    if options:
-        unknown = set(options) - set(resolved)
-        if unknown:
-            raise ValueError(f"unknown native L-BFGS options: {sorted(unknown)}")
-        resolved.update(options)
-    for k in ("max_iter", "history_size"):
-        if isinstance(resolved[k], bool) or int(resolved[k]) != resolved[k] or resolved[k] < 1:
-            raise ValueError(f"{k} must be a positive integer")
-    if resolved["max_eval"] is not None and (int(resolved["max_eval"]) != resolved["max_eval"]
-                                             or resolved["max_eval"] < 1):
+# options stlp_lbfgs reads (csrc/lbfgs.cpp), with their defaults
+_LBFGS_DEFAULTS = {"lr": 1.0, "max_iter": 20, "max_eval": None, "tolerance_grad": 1e-12,
+                   "tolerance_change": 1e-15, "history_size": 10}
+
+
+def _is_count(v):
+    """A positive whole number (bool excluded)."""
+    if isinstance(v, bool) or not isinstance(v, (int, float, np.integer, np.floating)):
+        return False
+    return v >= 1 and float(v) == int(v)
+
+
+def _lbfgs_options(options):
+    opts = dict(_LBFGS_DEFAULTS)
+    given = dict(options or {})
+    extra = sorted(k for k in given if k not in opts)
+    if extra:
+        raise ValueError(f"unknown native L-BFGS options: {extra}")
+    opts.update(given)
+    for name in ("max_iter", "history_size"):
+        if not _is_count(opts[name]):
+            raise ValueError(f"{name} must be a positive integer")
+    if opts["max_eval"] is not None and not _is_count(opts["max_eval"]):
         raise ValueError("max_eval must be a positive integer or None")
-    x = np.ascontiguousarray(x, dtype=np.float64)
-    if x.size == 0 or not np.isfinite(x).all():
-        raise ValueError("finite nonempty initial point required")
-    shape, history, errors = x.shape, [], []
+    return opts
 
-    @_CALLBACK
-    def evaluate(p, n, gp, _context):
-        try:
-            trial = np.ctypeslib.as_array(p, shape=(n,)).reshape(shape)
-            trial.flags.writeable = False
-            value, grad = callback(trial)
-            grad = np.asarray(grad, dtype=np.float64)
-            if grad.shape != shape:
-                raise ValueError(f"gradient shape {grad.shape} != {shape}")
-            np.ctypeslib.as_array(gp, shape=(n,))[:] = grad.ravel()
-            history.append(float(value))
-            return float(value)
-        except BaseException as exc:  # reported after the native call returns
-            errors.append(exc)
+
+class _LbfgsObjective:
+    """The C callback of stlp_lbfgs around a Python callback(x) -> (loss, grad).
+
+    The library owns the trial point and the gradient buffer: the callback
+    sees the trial as a read-only array of the caller's shape and the gradient
+    is copied into the library's buffer.  A Python exception cannot cross the
+    C frames, so the first one is kept here and NaN is returned, which ends
+    the library's iteration; native_lbfgs raises it afterwards."""
+
+    def __init__(self, callback, shape):
+        self.callback, self.shape = callback, shape
+        self.losses, self.failure = [], None
+        self.c_function = _CALLBACK(self._call)
+
+    def _call(self, point, n, grad_out, _context):
+        if self.failure is not None:
             return float("nan")
+        try:
+            trial = np.ctypeslib.as_array(point, shape=(n,)).reshape(self.shape)
+            trial.flags.writeable = False
+            loss, grad = self.callback(trial)
+            grad = np.asarray(grad, dtype=np.float64)
+            if grad.shape != self.shape:
+                raise ValueError(f"callback gradient has shape {grad.shape}, the maps {self.shape}")
+            np.copyto(np.ctypeslib.as_array(grad_out, shape=(n,)).reshape(self.shape), grad)
+            loss = float(loss)
+        except BaseException as exc:  # raised by native_lbfgs once the library returns
+            self.failure = exc
+            return float("nan")
+        self.losses.append(loss)
+        return loss
 
-    count = lib().stlp_lbfgs(_ptr(x), x.size, json.dumps(resolved).encode(), evaluate, None)
-    if errors:
-        raise errors[0]
-    if count < 0:
+
+def native_lbfgs(callback, x, options=None):
+    """Minimises callback(x) -> (loss, gradient) from x with the library's
+    L-BFGS and strong Wolfe line search (stlp_lbfgs, the reference's
+    native_lbfgs contract: options lr, max_iter, max_eval, tolerance_grad,
+    tolerance_change, history_size).  A float64 C-contiguous x is updated in
+    place (other arrays are converted first).  Returns (x, report) with the
+    evaluation count and the loss of every evaluation."""
+    opts = _lbfgs_options(options)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.size == 0:
+        raise ValueError("native_lbfgs needs a nonempty starting point")
+    if not np.isfinite(x).all():
+        raise ValueError("native_lbfgs needs a finite starting point")
+    objective = _LbfgsObjective(callback, x.shape)
+    evaluations = lib().stlp_lbfgs(_ptr(x), x.size, json.dumps(opts).encode(), objective.c_function, None)
+    if objective.failure is not None:
+        raise objective.failure
+    if evaluations < 0:
         raise _error()
-    return x, dict(evaluations=int(count), loss_history=history, options=resolved,
-                   optimizer="native L-BFGS", line_search="strong_wolfe")
+    report = {"evaluations": int(evaluations), "loss_history": objective.losses, "options": opts,
+              "optimizer": "B200 engine L-BFGS (stlp_lbfgs)", "line_search": "strong_wolfe"}
+    return x, report
 
 
 def synthesis_objective(engine, target, weights=None):
@@ -594,101 +639,109 @@ class PatchEngine:
         return c
 
     def select(self, centres, radius, core=None):
-        """Selects the discs (radius, core in degrees: one for all, or one per disc);
-        returns their sorted NESTED pixels."""
+        """Selects the discs (radius and core radius in degrees, one value for
+        all discs or one per disc) and returns each disc's sorted NESTED
+        pixels.  Selecting the same discs again costs nothing."""
+        vectors = np.ascontiguousarray(self.centre_vectors(centres))
+        n = vectors.shape[0]
+        uniform = np.ndim(radius) == 0 and (core is None or np.ndim(core) == 0)
+        radii = np.ascontiguousarray(np.radians(np.broadcast_to(np.asarray(radius, np.float64), (n,))))
+        cores = np.zeros(n) if core is None else np.radians(np.broadcast_to(np.asarray(core, np.float64), (n,)))
+        cores = np.ascontiguousarray(cores)
+        ident = (vectors.tobytes(), radii.tobytes(), cores.tobytes())
         with self._mutex:
             self._open()
-            v = np.ascontiguousarray(self.centre_vectors(centres))
-            key = (v.tobytes(), np.asarray(radius, np.float64).tobytes(),
-                   None if core is None else np.asarray(core, np.float64).tobytes())
-            if key == self._selection:
+            if ident == self._selection:
                 return self.ids
-            b = v.shape[0]
-            counts = np.empty(b, dtype=np.uintp)
-            self._generation, self._selection = None, None
-            if np.ndim(radius) == 0 and (core is None or np.ndim(core) == 0):
-                rc = 0.0 if core is None else np.radians(float(core))
-                status = self._lib.stlp_patch_select(self._handle, _ptr(v), b, np.radians(float(radius)), rc,
-                                                     counts.ctypes.data_as(_SIZE))
-            else:  # a radius (and core) per disc
-                r = np.ascontiguousarray(np.radians(np.broadcast_to(np.asarray(radius, np.float64), (b,))))
-                c = np.zeros(b) if core is None else np.radians(np.broadcast_to(np.asarray(core, np.float64), (b,)))
-                c = np.ascontiguousarray(c)
-                status = self._lib.stlp_patch_select_radii(self._handle, _ptr(v), b, _ptr(r), _ptr(c),
-                                                           counts.ctypes.data_as(_SIZE))
+            self._generation = self._selection = None
+            counts = np.empty(n, dtype=np.uintp)
+            counts_p = counts.ctypes.data_as(_SIZE)
+            if uniform:  # the reference's entry point: one radius per call
+                status = self._lib.stlp_patch_select(self._handle, _ptr(vectors), n, np.radians(float(radius)),
+                                                     0.0 if core is None else np.radians(float(core)), counts_p)
+            else:
+                status = self._lib.stlp_patch_select_radii(self._handle, _ptr(vectors), n, _ptr(radii),
+                                                           _ptr(cores), counts_p)
             if status:
                 raise _error()
-            ids = []
-            for i, n in enumerate(counts):
-                a = np.empty(int(n), dtype=np.int64)
-                if self._lib.stlp_patch_ids(self._handle, i, a.ctypes.data_as(C.POINTER(C.c_int64))):
-                    raise _error()
-                ids.append(a)
-            core_pixels = np.empty((b, self.levels), dtype=np.uintp)
-            if self._lib.stlp_patch_core_pixels(self._handle, core_pixels.ctypes.data_as(_SIZE)):
+            self.ids = [self._disc_pixels(i, int(c)) for i, c in enumerate(counts)]
+            per_level = np.empty((n, self.levels), dtype=np.uintp)
+            if self._lib.stlp_patch_core_pixels(self._handle, per_level.ctypes.data_as(_SIZE)):
                 raise _error()
-            self.ids, self._selection = ids, key
-            self.native_pixels = core_pixels.astype(np.float64)[:, self._native]
-            return ids
+            self.native_pixels = per_level.astype(np.float64)[:, self._native]
+            self._selection = ident
+            return self.ids
+
+    def _disc_pixels(self, i, count):
+        out = np.empty(count, dtype=np.int64)
+        if self._lib.stlp_patch_ids(self._handle, i, out.ctypes.data_as(C.POINTER(C.c_int64))):
+            raise _error()
+        return out
 
     def gather(self, maps):
+        """The patches of the selected discs cut from full-sky maps ([npix]: one
+        map for every disc; [B, npix]: map i for disc i)."""
         m = np.asarray(maps)
         if m.ndim == 1:
             return [m[i] for i in self.ids]
         return [m[k][..., i] for k, i in enumerate(self.ids)]
 
+    def _pack(self, maps):
+        """One float64 vector of the patches in disc order, checked against the
+        selection's pixel counts."""
+        if len(maps) != len(self.ids):
+            raise ValueError(f"{len(maps)} patches given for {len(self.ids)} selected discs")
+        sizes = [i.size for i in self.ids]
+        flat = [np.asarray(m, dtype=np.float64) for m in maps]
+        for i, (m, size) in enumerate(zip(flat, sizes)):
+            if m.shape != (size,):
+                raise ValueError(f"patch {i} has shape {m.shape}; its disc holds {size} pixels")
+        return np.ascontiguousarray(np.concatenate(flat)) if flat else np.zeros(0)
+
     def forward(self, maps, centres=None, radius=None, core=None, moments=True, generation=0):
-        """Statistics [B, ncoeff] (and variances) of the patches of the selected discs."""
+        """Statistics [B, ncoeff] (and variances, or [B, 0]) of the patches of
+        the selected discs (selecting them first when centres are given)."""
         with self._mutex:
             self._open()
             if centres is not None:
                 if radius is None:
-                    raise ValueError("radius (degrees) is required with centres")
+                    raise ValueError("selecting discs needs a radius in degrees")
                 self.select(centres, radius, core)
             if not self.ids:
-                raise RuntimeError("no disc selected")
+                raise RuntimeError("forward before any disc was selected")
+            x = self._pack(maps)  # non-finite values are counted by the library's copy (ValueError)
             b = len(self.ids)
-            if len(maps) != b:
-                raise ValueError(f"expected {b} patches, got {len(maps)}")
-            parts = []
-            for i, (m, ids) in enumerate(zip(maps, self.ids)):
-                m = np.asarray(m, dtype=np.float64)
-                if m.shape != (ids.size,):
-                    raise ValueError(f"patch {i}: expected {(ids.size,)}, got {m.shape}")
-                parts.append(m.reshape(-1))
-            x = np.ascontiguousarray(np.concatenate(parts))
-            # non-finite values: the library counts them while it copies the patches (ValueError)
-            self._dense = isinstance(maps, np.ndarray)
             values = np.empty((b, self.ncoeff), dtype=np.complex128)
             variance = np.empty((b, self.ncoeff if moments else 0), dtype=np.float64)
             self._generation = None
-            if self._lib.stlp_patch_forward(self._handle, _ptr(x), x.size, int(generation), bool(moments),
-                                            _ptr(values.view(np.float64)), _ptr(variance) if moments else None):
+            self._dense = isinstance(maps, np.ndarray)
+            status = self._lib.stlp_patch_forward(self._handle, _ptr(x), x.size, int(generation), bool(moments),
+                                                  _ptr(values.view(np.float64)), _ptr(variance) if moments else None)
+            if status:
                 raise _error()
             self._generation = int(generation)
             return values, variance
 
     def vjp(self, cotangents, generation=0):
-        """Gradients of Re sum(conj(cotangents) values) with respect to the patches."""
+        """Gradients of Re sum(conj(cotangents) values) with respect to the
+        patches of the forward of this generation, shaped like its maps."""
         with self._mutex:
             self._open()
             if self._generation is None or int(generation) != self._generation:
-                raise RuntimeError("stale forward state")
+                raise RuntimeError("no forward state of this generation: it is stale or was never computed")
             b = len(self.ids)
             c = np.ascontiguousarray(cotangents, dtype=np.complex128)
             if c.shape != (b, self.ncoeff):
-                raise ValueError(f"expected cotangents {(b, self.ncoeff)}, got {c.shape}")
+                raise ValueError(f"cotangents have shape {c.shape}, the statistics {(b, self.ncoeff)}")
             if not np.isfinite(c.view(np.float64)).all():
                 raise ValueError("non-finite coefficient cotangent")
-            total = sum(i.size for i in self.ids)
-            g = np.empty(total, dtype=np.float64)
-            if self._lib.stlp_patch_vjp(self._handle, _ptr(c.view(np.float64)), c.size, int(generation), _ptr(g)):
+            sizes = np.array([i.size for i in self.ids], dtype=np.int64)
+            grad = np.empty(int(sizes.sum()), dtype=np.float64)
+            if self._lib.stlp_patch_vjp(self._handle, _ptr(c.view(np.float64)), c.size, int(generation),
+                                        _ptr(grad)):
                 raise _error()
-            out, off = [], 0
-            for ids in self.ids:
-                out.append(g[off:off + ids.size])
-                off += ids.size
-            return np.stack(out) if self._dense else out
+            parts = np.split(grad, np.cumsum(sizes)[:-1])
+            return np.stack(parts) if self._dense else parts
 
     def close(self):
         if getattr(self, "_handle", None):

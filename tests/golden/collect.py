@@ -7,10 +7,14 @@ that has the reference mounted:
 
     python tests/golden/collect.py /path/to/STL-Dev-MPI/fixtures
 
+Without an argument the fixtures are read from $STL_REFERENCE_ROOT/fixtures
+(STL_REFERENCE_ROOT defaults to /root/reference).
+
 Only a subset is copied, to keep the repository small: every stats case,
 and per geometry kind the cases listed in ``SELECT`` below.
 """
 import json
+import os
 import shutil
 import sys
 from pathlib import Path
@@ -48,4 +52,5 @@ def main(src: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/fixtures"))
+    root = Path(os.environ.get("STL_REFERENCE_ROOT", "/root/reference"))
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else root / "fixtures")

@@ -4,6 +4,7 @@ reports configuration errors the way the reference's bridge does
 (crates/stl-bridge/src/lib.rs:75-94: -1 / NULL and stlp_last_error)."""
 import ctypes as C
 import json
+import os
 import re
 import subprocess
 import sys
@@ -112,7 +113,10 @@ def test_out_of_scope_entry_points_fail_cleanly(stl):
     assert b"not built" in lib.stlp_last_error()
 
 
-REFERENCE_NATIVE = Path("/root/reference/python/stl_ensemble/stl_port/native.py")
+# the reference checkout (STL_REFERENCE_ROOT, default /root/reference): its
+# unmodified Python binding, where the checkout is mounted
+REFERENCE_ROOT = Path(os.environ.get("STL_REFERENCE_ROOT", "/root/reference"))
+REFERENCE_NATIVE = REFERENCE_ROOT / "python" / "stl_ensemble" / "stl_port" / "native.py"
 
 
 @pytest.mark.skipif(not REFERENCE_NATIVE.exists(), reason="the reference checkout is not mounted")

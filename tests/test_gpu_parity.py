@@ -43,10 +43,13 @@ def family_scale(plan, values):
     return scale
 
 
-def test_config1_fixture_fp64(stl):
-    """nside 16, J 3, L 4: the reference's golden statistics and gradient."""
-    case = next(c for c in cases("stats", "stats") if c.name == "stats_n16_J3_L4_k5_C1_B1_full_b256")
-    e = stl.NativeEngine(16, 3, dtype="float64")
+@pytest.mark.parametrize("name,nside,J", [("stats_n16_J3_L4_k5_C1_B1_full_b256", 16, 3),
+                                          ("stats_n32_J4_L4_k5_C1_B1_full_b256", 32, 4)])
+def test_reference_fixture_fp64(stl, name, nside, J):
+    """The reference's golden statistics and map gradient of the L 4, kernel 5,
+    one-channel fixtures (config 1 is the nside 16 one)."""
+    case = next(c for c in cases("stats", "stats") if c.name == name)
+    e = stl.NativeEngine(nside, J, dtype="float64")
     x = case.npy("map0").reshape(1, -1)
     values, _ = e.forward(x)
     ref = case.complex("values").reshape(values.shape)
@@ -64,6 +67,27 @@ def test_fp64_matches_oracle(stl, nside, J, B):
     o = O.OracleEngine(nside, J, batch=B)
     ref, ref_var = o.forward(x, moments=True)
     e = stl.NativeEngine(nside, J, batch=B, dtype="float64")
+    values, var = e.forward(x, moments=True)
+    assert close_ratio(values.real, ref.real, 1e-11, 1e-10) <= 1.0
+    assert close_ratio(values.imag, ref.imag, 1e-11, 1e-10) <= 1.0
+    assert close_ratio(var, ref_var, 1e-11, 1e-9) <= 1.0
+    cot = rng.standard_normal(values.shape) + 1j * rng.standard_normal(values.shape)
+    g_ref = o.vjp(cot)
+    grad = e.vjp(cot)
+    assert close_ratio(grad, g_ref, 1e-10 * np.max(np.abs(g_ref)), 1e-9) <= 1.0
+
+
+def test_fp64_matches_oracle_nside256(stl):
+    """The FP64 path against the oracle at config 2's size (nside 256, J 7, one
+    lognormal map): values and variances at the reference's tolerances
+    (crates/stl-core/tests/stats.rs:175-190), the gradient of a random
+    cotangent at the map-cotangent tolerance."""
+    nside, J = 256, 7
+    rng = np.random.default_rng(256)
+    x = lognormal(rng, (1, 12 * nside * nside))
+    o = O.OracleEngine(nside, J, batch=1)
+    ref, ref_var = o.forward(x, moments=True)
+    e = stl.NativeEngine(nside, J, batch=1, dtype="float64")
     values, var = e.forward(x, moments=True)
     assert close_ratio(values.real, ref.real, 1e-11, 1e-10) <= 1.0
     assert close_ratio(values.imag, ref.imag, 1e-11, 1e-10) <= 1.0

@@ -17,14 +17,17 @@ def _entry(stl):
     return f
 
 
-@pytest.mark.parametrize("dtype", ["float64", "float32"])
-def test_mean_var_noalloc_matches_forward(dtype):
+@pytest.mark.parametrize("dtype,nside,B", [("float64", 16, 3), ("float32", 16, 3),
+                                           # more pixels than one pass of the 296 x 256-thread grid
+                                           ("float64", 128, 2), ("float32", 128, 2),
+                                           # the largest batch the fixed scratch holds
+                                           ("float64", 16, 64)])
+def test_mean_var_noalloc_matches_forward(dtype, nside, B):
     import torch
     if not torch.cuda.is_available():
         pytest.fail("a CUDA device is required")
     import stl_b200 as stl
     f = _entry(stl)
-    nside, B = 16, 3
     tdt = torch.float64 if dtype == "float64" else torch.float32
     g = torch.Generator(device="cuda").manual_seed(7)
     x = torch.exp(torch.randn(B, 12 * nside * nside, device="cuda", dtype=tdt, generator=g) - 0.5)
