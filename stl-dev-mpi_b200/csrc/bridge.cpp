@@ -117,6 +117,7 @@ StlpHandle* stlp_new(const char* config) {
     require(dtype == "float64" || dtype == "float32", "dtype must be float64 or float32");
     o.fp32 = dtype == "float32";
     o.autotune = v.boolean("autotune", true);
+    o.tensor_cores = v.boolean("tensor_cores", true);
     o.tune_cache = v.string("autotune_cache", "");
     o.cross = v.boolean("cross", false);  // two channels, the plan of their cross terms (lib.rs:238-245)
     require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
@@ -196,7 +197,8 @@ char* stlp_info(StlpHandle* h) {
     auto ol = e.operator_layout();
     for (size_t i = 0; i < ol.size(); ++i)
       js << (i ? ", " : "") << "{\"slots\": " << ol[i][0] << ", \"tile_cells\": " << ol[i][1]
-         << ", \"coloured\": " << (ol[i][2] ? "true" : "false") << "}";
+         << ", \"coloured\": " << (ol[i][2] == 1 ? "true" : "false") << ", \"layout\": \""
+         << (ol[i][2] == 2 ? "tensor_cores" : ol[i][2] == 1 ? "coloured" : "rows") << "\"}";
     js << "], \"tile_heights\": [";
     auto th = e.tile_heights();
     for (size_t i = 0; i < th.size(); ++i) {

@@ -605,6 +605,7 @@ class EngineImpl final : public Engine {
     for (int n = 0; n < levels_; ++n) {
       ConvSpec cs;
       cs.nside = opt_.nside >> n; cs.ksz = opt_.ksz; cs.G = L; cs.gauge = 0;
+      cs.tensor_cores = opt_.tensor_cores;
       if (grid_mode()) {
         cs.d_grid = ids_dev_[n].as<i64>();
         cs.n_in = npix(n);
@@ -979,7 +980,8 @@ class EngineImpl final : public Engine {
   std::vector<std::array<int, 8>> tile_heights() const override { return tiles_; }
   std::vector<std::array<int, 3>> operator_layout() const override {
     std::vector<std::array<int, 3>> v;
-    for (const auto& c : conv_) v.push_back({c.S, c.max_tile_cells, c.colored ? 1 : 0});
+    for (const auto& c : conv_)
+      v.push_back({c.mma ? c.m_S : c.S, c.mma ? c.m_pc : c.max_tile_cells, c.mma ? 2 : c.colored ? 1 : 0});
     return v;
   }
 

@@ -99,6 +99,7 @@ inline size_t dsize(DType t) { return t == DType::F64 ? 8 : 4; }
 // Geometry of one wavelet operator: output rows reading an input grid.
 struct ConvSpec {
   i64 nside = 0;
+  bool tensor_cores = true;     // FP32 full sky: the tensor-core layout (else the coloured one)
   int ksz = 5, G = 4, gauge = 0;
   double eps = 0.0;
   const i64* d_grid = nullptr;  // sorted NESTED ids of the grid (device), nullptr: whole sky
@@ -160,12 +161,42 @@ struct ConvOp {
   DevMem clist;              // uint32 tile << 12 | tile cell << 2 | rotation
   int G = 4;
   double mean_slots = 0.0;   // cells read per row, averaged over the rows
+  // Tensor-core layout (FP32 full sky; replaces the coloured one).  Tiles of
+  // kMmaRows stored rows; per tile a plane of input cells in which cell c
+  // sits at 4 (its rank among the tile's cells of its class) + class, the
+  // class being c's NESTED bits x0 + 2 y0 (the parity of its face
+  // coordinates); slots in chunks of 8 whose position p holds a cell of
+  // class kMmaClass[p] (zero coefficients where a row has none left), so the
+  // 8 cells an mma step gathers fall in distinct shared-memory banks.  The
+  // adjoint adds into per-warp sums over the distinct cells of the warp's
+  // kMmaWarpRows rows (numbered the same way), combined per tile cell in
+  // warp order.  Every sum has a fixed order.
+  bool mma = false;
+  i64 m_tiles = 0;
+  int m_S = 0;               // slots: 8 x the most chunks of a row
+  int m_pc = 0;              // plane stride (cells; 4 mod 8)
+  int m_wl = 0;              // stride of a warp's private sums (cells; 4 mod 8)
+  DevMem m_coef;             // float [m_S][n_rep][8]
+  DevMem m_cells;            // int32 [m_tiles][m_pc]: plane cell ids (-1: none)
+  DevMem m_lc;               // uint16 [m_tiles][m_S][kMmaRows]: plane cell of every (slot, row)
+  DevMem m_wlc;              // uint8 [m_tiles][m_S / 8][kMmaRows][8]: warp-local cell of every (row, slot)
+  DevMem m_winv;             // uint8 [m_tiles][kMmaRows / kMmaWarpRows][m_pc]: warp-local cell of each plane cell (255: none)
+  DevMem m_rowch;            // uint8 [n_rep]: chunks of every row
+  DevMem m_tch;              // int32 [m_tiles]: chunks of the tile (its rows' most)
   size_t bytes() const {
     return cell.bytes + coef.bytes + tent.bytes + coefT.bytes + rowsum.bytes + tile_cells.bytes + tile_ncells.bytes +
-           tile_slots.bytes + lcell.bytes +
-           lcell_t.bytes + tile_ent.bytes + tile_off.bytes + coff.bytes + clist.bytes;
+           tile_slots.bytes + lcell.bytes + lcell_t.bytes + tile_ent.bytes + tile_off.bytes + coff.bytes +
+           clist.bytes + m_coef.bytes + m_cells.bytes + m_lc.bytes + m_wlc.bytes + m_winv.bytes + m_rowch.bytes +
+           m_tch.bytes;
   }
 };
+constexpr int kMmaRows = 64;      // stored rows per tile of the tensor-core layout
+constexpr int kMmaWarpRows = 8;   // rows per warp (one block of private adjoint sums)
+constexpr int kMmaPlaneMax = 1024;  // plane cells a tile may index
+constexpr int kMmaWarpMax = 252;    // warp-local cells (uint8 indices, 255: none)
+// class of the cell at position p of a chunk: every class twice, positions
+// 0-3 and 4-7 all four, positions 0, 2, 4, 6 and 1, 3, 5, 7 all four
+__host__ __device__ constexpr int mma_class(int p) { return (0x23013210 >> (4 * p)) & 3; }
 constexpr int kAdjTile = 128;    // stored rows per tile of the tiled forward and adjoint
 constexpr int kAdjCells = 1024;  // cells a tile may read
 constexpr int kAdjSC = 8;        // slots per chunk of the two-phase adjoint

@@ -16,6 +16,7 @@
 // within 3 fine pixels, l1-normalised, zeros dropped; then the transpose.
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "engine.cuh"
 #include "healpix.cuh"
@@ -604,6 +605,231 @@ __global__ void k_tsort(uint32_t* tent, const int* tcount, i64 n_in, int ST) {
   for (int i = n; i < ST; ++i) tent[(i64)i * n_in + c] = kSentinel;
 }
 
+// ---- tensor-core layout -------------------------------------------------------
+// One block (256 threads) per tile of kMmaRows stored rows, run twice: pass
+// 0 measures (chunks of every row and tile, plane cells, warp-local cells),
+// pass 1 writes the layout with the strides pass 0 fixed.  The tile's
+// distinct cells are sorted (bitonic) and numbered 4 rank + class within
+// their class (class = the cell's NESTED bits x0 + 2 y0, which the 4-face
+// rotations keep); a row's cells keep their slot order within each class,
+// the j-th of class q going to chunk j / 2 at position mma_pos(q, j % 2).
+struct MmaArgs {
+  const int32_t* cell;  // [S][n_rep]
+  const int* counts;    // cells per row
+  const float* coef;    // [S][n_rep][8]
+  int S;
+  i64 n_rep;
+  int Sm, pcs;          // pass 1: slots and plane stride
+  int32_t* tile_ch;     // [tiles] chunks
+  int32_t* tile_pc;     // [tiles] plane cells used: 4 (largest class + 1)
+  int32_t* tile_wl;     // [tiles] warp-local cells used: 4 (largest class + 1), most over the tile's warps
+  uint8_t* rowch;       // [n_rep]
+  float* m_coef;        // pass 1 outputs (ConvOp::m_*)
+  int32_t* m_cells;
+  uint16_t* m_lc;
+  uint8_t* m_wlc;
+  uint8_t* m_winv;
+  int* overflow;
+};
+
+__host__ __device__ constexpr int mma_pos(int q, int j) { return j == 0 ? q : 4 + (q ^ 1); }
+
+constexpr int kMmaMaxSlots = 128;  // slots of the layout (16 chunks)
+
+__global__ void __launch_bounds__(256) k_mma_layout(MmaArgs a, int pass, int P2) {
+  extern __shared__ int32_t mbuf[];
+  int32_t* sorted = mbuf;                       // [P2]
+  int32_t* uniq = sorted + P2;                  // [kMmaPlaneMax]
+  int16_t* upl = reinterpret_cast<int16_t*>(uniq + kMmaPlaneMax);      // [kMmaPlaneMax] plane index
+  uint8_t* gmap = reinterpret_cast<uint8_t*>(upl + kMmaPlaneMax);      // [groups][kMmaPlaneMax]
+  __shared__ int cnt[256];
+  __shared__ int s_nc, s_mc, s_ch, s_wl, s_bad;
+  __shared__ int s_mcw[kMmaRows / kMmaWarpRows];
+  constexpr int NG = kMmaRows / kMmaWarpRows;
+  const int tid = threadIdx.x;
+  const i64 tile = blockIdx.x, u0 = tile * kMmaRows;
+  const int n = a.S * kMmaRows;
+  if (tid == 0) { s_ch = 0; s_wl = 0; s_bad = 0; }
+  for (int i = tid; i < P2; i += blockDim.x) {
+    int32_t v = 0x7fffffff;
+    if (i < n) {
+      const int sl = i / kMmaRows, ul = i % kMmaRows;
+      const i64 u = u0 + ul;
+      if (u < a.n_rep && sl < a.counts[u]) v = a.cell[(i64)sl * a.n_rep + u];
+    }
+    sorted[i] = v;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < P2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const int32_t x = sorted[i], y = sorted[l];
+          if (((i & k) == 0) ? (x > y) : (x < y)) { sorted[i] = y; sorted[l] = x; }
+        }
+      }
+      __syncthreads();
+    }
+  const int per = P2 / blockDim.x;
+  int mine = 0;
+  for (int i = tid * per; i < (tid + 1) * per; ++i)
+    if (sorted[i] != 0x7fffffff && (i == 0 || sorted[i - 1] != sorted[i])) ++mine;
+  cnt[tid] = mine;
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) { const int c = cnt[t]; cnt[t] = acc; acc += c; }
+    s_nc = acc;
+    if (acc > kMmaPlaneMax) s_bad = 1;
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) atomicExch(a.overflow, 1);
+    return;
+  }
+  int pos = cnt[tid];
+  for (int i = tid * per; i < (tid + 1) * per; ++i)
+    if (sorted[i] != 0x7fffffff && (i == 0 || sorted[i - 1] != sorted[i])) uniq[pos++] = sorted[i];
+  __syncthreads();
+  const int nc = s_nc;
+  // plane index of every tile cell: 4 (rank in its class) + class
+  if (tid < 4) {
+    int r = 0;
+    for (int i = 0; i < nc; ++i)
+      if ((uniq[i] & 3) == tid) upl[i] = (int16_t)(4 * r++ + tid);
+    cnt[tid] = r;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    s_mc = max(max(cnt[0], cnt[1]), max(cnt[2], cnt[3]));
+    if (4 * (s_mc + 1) > kMmaPlaneMax) s_bad = 1;
+  }
+  for (int i = tid; i < NG * kMmaPlaneMax; i += blockDim.x) gmap[i] = 255;
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) atomicExch(a.overflow, 1);
+    return;
+  }
+  const int mc = s_mc;
+  auto find = [&](int32_t v) {
+    int lo = 0, hi = nc;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (uniq[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return (int)upl[lo];
+  };
+  // warp groups: the distinct plane cells of each group's rows, numbered
+  // 4 rank + class in plane order
+  if (tid < NG) {
+    uint8_t* gm = gmap + tid * kMmaPlaneMax;
+    for (int ul = tid * kMmaWarpRows; ul < (tid + 1) * kMmaWarpRows; ++ul) {
+      const i64 u = u0 + ul;
+      if (u >= a.n_rep) break;
+      for (int sl = 0; sl < a.counts[u]; ++sl) gm[find(a.cell[(i64)sl * a.n_rep + u])] = 0;
+    }
+    int r[4] = {0, 0, 0, 0};
+    for (int pl = 0; pl < 4 * mc; ++pl)
+      if (gm[pl] == 0) gm[pl] = (uint8_t)(4 * r[pl & 3]++ + (pl & 3));
+    const int mcw = max(max(r[0], r[1]), max(r[2], r[3]));
+    s_mcw[tid] = mcw;
+    if (4 * mcw + 3 > kMmaWarpMax) atomicExch(&s_bad, 1);
+    atomicMax(&s_wl, 4 * (mcw + 1));
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) atomicExch(a.overflow, 1);
+    return;
+  }
+  // rows: chunks (pass 0) or the layout (pass 1)
+  if (tid < kMmaRows) {
+    const int ul = tid;
+    const i64 u = u0 + ul;
+    int nq[4] = {0, 0, 0, 0};
+    const int n_u = u < a.n_rep ? a.counts[u] : 0;
+    for (int sl = 0; sl < n_u; ++sl) ++nq[find(a.cell[(i64)sl * a.n_rep + u]) & 3];
+    int ch = 0;
+    for (int q = 0; q < 4; ++q) ch = max(ch, (nq[q] + 1) / 2);
+    if (8 * ch > kMmaMaxSlots) atomicExch(&s_bad, 1);
+    if (pass == 0) {
+      if (u < a.n_rep) a.rowch[u] = (uint8_t)ch;
+      atomicMax(&s_ch, ch);
+    } else if (u < a.n_rep && 8 * ch <= kMmaMaxSlots) {
+      int16_t src[kMmaMaxSlots];
+      for (int ns = 0; ns < a.Sm; ++ns) src[ns] = -1;
+      int jq[4] = {0, 0, 0, 0};
+      for (int sl = 0; sl < n_u; ++sl) {
+        const int q = find(a.cell[(i64)sl * a.n_rep + u]) & 3;
+        const int j = jq[q]++;
+        src[8 * (j >> 1) + mma_pos(q, j & 1)] = (int16_t)sl;
+      }
+      const int g = ul / kMmaWarpRows;
+      const uint8_t* gm = gmap + g * kMmaPlaneMax;
+      const int mcw = s_mcw[g];
+      for (int ns = 0; ns < a.Sm; ++ns) {
+        const int q = mma_class(ns & 7), sl = src[ns];
+        float* dst = a.m_coef + ((i64)ns * a.n_rep + u) * 8;
+        int pl, wl;
+        if (sl >= 0) {
+          const float* c = a.coef + ((i64)sl * a.n_rep + u) * 8;
+          for (int o = 0; o < 8; ++o) dst[o] = c[o];
+          pl = find(a.cell[(i64)sl * a.n_rep + u]);
+          wl = gm[pl];
+        } else {  // padding: zero coefficients on the class's spare cells
+          for (int o = 0; o < 8; ++o) dst[o] = 0.0f;
+          pl = 4 * mc + q;
+          wl = 4 * mcw + q;
+        }
+        a.m_lc[((i64)tile * a.Sm + ns) * kMmaRows + ul] = (uint16_t)pl;
+        a.m_wlc[(((i64)tile * (a.Sm / 8) + (ns >> 3)) * kMmaRows + ul) * 8 + (ns & 7)] = (uint8_t)wl;
+      }
+    }
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) atomicExch(a.overflow, 1);
+    return;
+  }
+  if (pass == 0) {
+    if (tid == 0) {
+      a.tile_ch[tile] = s_ch;
+      a.tile_pc[tile] = 4 * (mc + 1);
+      a.tile_wl[tile] = s_wl;
+    }
+    return;
+  }
+  for (int pl = tid; pl < a.pcs; pl += blockDim.x) a.m_cells[(i64)tile * a.pcs + pl] = -1;
+  __syncthreads();
+  for (int i = tid; i < nc; i += blockDim.x) a.m_cells[(i64)tile * a.pcs + upl[i]] = uniq[i];
+  for (int i = tid; i < NG * a.pcs; i += blockDim.x) {
+    const int g = i / a.pcs, pl = i % a.pcs;
+    a.m_winv[((i64)tile * NG + g) * a.pcs + pl] = pl < kMmaPlaneMax ? gmap[g * kMmaPlaneMax + pl] : (uint8_t)255;
+  }
+}
+
+// tile plane cells -> stored input cells (holes, -1, have none)
+__global__ void k_mma_ccount(const int32_t* cells, i64 n, int pcs, int o2, int* ccount) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || cells[i] < 0) return;
+  i64 v; int j;
+  tile_cell_owner(cells[i], 4, o2, v, j);
+  atomicAdd(ccount + v, 1);
+  (void)pcs;
+}
+
+__global__ void k_mma_cfill(const int32_t* cells, i64 n, int pcs, int o2, const i64* coff, int* cursor,
+                            uint32_t* clist) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || cells[i] < 0) return;
+  i64 v; int j;
+  tile_cell_owner(cells[i], 4, o2, v, j);
+  const i64 tile = i / pcs;
+  const int pl = (int)(i % pcs);
+  const int pos = atomicAdd(cursor + v, 1);
+  clist[coff[v] + pos] = ((uint32_t)tile << 12) | ((uint32_t)pl << 2) | (uint32_t)j;
+}
+
 // ---- decimation ------------------------------------------------------------
 struct DecArgs {
   i64 nside;      // fine
@@ -821,6 +1047,91 @@ static std::vector<double> kernel_grid(int ksz, i64 nside) {
   return out;
 }
 
+// The tensor-core layout of an FP32 full-sky operator (ConvOp::m_*) from its
+// per-row slots; false (nothing kept) when a tile does not fit its limits.
+static bool build_mma_layout(ConvOp& op, const DevMem& counts, cudaStream_t s) {
+  const i64 n_rep = op.n_rep;
+  if (op.S > 64 || op.o2 < 2) return false;
+  const i64 n_tiles = (n_rep + kMmaRows - 1) / kMmaRows;
+  if ((uint64_t)n_tiles >= (1ull << 20)) return false;  // the combine lists hold 20-bit tiles
+  int P2 = 256;  // at least one entry per thread of the sort's block
+  while (P2 < op.S * kMmaRows) P2 <<= 1;
+  const int NG = kMmaRows / kMmaWarpRows;
+  const size_t smem = sizeof(int32_t) * ((size_t)P2 + kMmaPlaneMax) + sizeof(int16_t) * kMmaPlaneMax +
+                      (size_t)NG * kMmaPlaneMax;
+  allow_dynamic_smem(k_mma_layout);
+  DevMem tch(sizeof(int32_t) * n_tiles), tpc(sizeof(int32_t) * n_tiles), twl(sizeof(int32_t) * n_tiles),
+      rowch(std::max<i64>(n_rep, 1)), flag(sizeof(int));
+  STL_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+  MmaArgs a{};
+  a.cell = op.cell.as<int32_t>();
+  a.counts = counts.as<int>();
+  a.coef = op.coef.as<float>();
+  a.S = op.S;
+  a.n_rep = n_rep;
+  a.tile_ch = tch.as<int32_t>();
+  a.tile_pc = tpc.as<int32_t>();
+  a.tile_wl = twl.as<int32_t>();
+  a.rowch = rowch.as<uint8_t>();
+  a.overflow = flag.as<int>();
+  k_mma_layout<<<(unsigned)n_tiles, 256, smem, s>>>(a, 0, P2);
+  STL_CUDA(cudaGetLastError());
+  if (read_flag(flag, s)) return false;
+  const int chunks = device_max(tch.as<int32_t>(), n_tiles, s);
+  const int pc = device_max(tpc.as<int32_t>(), n_tiles, s);
+  const int wl = device_max(twl.as<int32_t>(), n_tiles, s);
+  auto stride = [](int v) { return ((v + 3) / 8) * 8 + 4; };  // the least value >= v that is 4 mod 8
+  op.m_S = 8 * std::max(chunks, 1);
+  op.m_pc = stride(pc);
+  op.m_wl = stride(wl);
+  if (op.m_S > kMmaMaxSlots || op.m_pc > kMmaPlaneMax) return false;
+  op.m_tiles = n_tiles;
+  op.m_coef.alloc(sizeof(float) * 8 * (size_t)op.m_S * n_rep);
+  op.m_cells.alloc(sizeof(int32_t) * (size_t)n_tiles * op.m_pc);
+  op.m_lc.alloc(sizeof(uint16_t) * (size_t)n_tiles * op.m_S * kMmaRows);
+  op.m_wlc.alloc((size_t)n_tiles * op.m_S * kMmaRows);
+  op.m_winv.alloc((size_t)n_tiles * NG * op.m_pc);
+  STL_CUDA(cudaMemsetAsync(op.m_lc.p, 0, op.m_lc.bytes, s));
+  STL_CUDA(cudaMemsetAsync(op.m_wlc.p, 0, op.m_wlc.bytes, s));
+  a.Sm = op.m_S;
+  a.pcs = op.m_pc;
+  a.m_coef = op.m_coef.as<float>();
+  a.m_cells = op.m_cells.as<int32_t>();
+  a.m_lc = op.m_lc.as<uint16_t>();
+  a.m_wlc = op.m_wlc.as<uint8_t>();
+  a.m_winv = op.m_winv.as<uint8_t>();
+  k_mma_layout<<<(unsigned)n_tiles, 256, smem, s>>>(a, 1, P2);
+  STL_CUDA(cudaGetLastError());
+  if (read_flag(flag, s)) return false;
+  op.m_rowch = std::move(rowch);
+  op.m_tch = std::move(tch);
+  // per stored input cell: the (tile, plane cell, rotation) entries of the
+  // adjoint's tile partials, sorted
+  const i64 n_cells = op.n_in / 4, nt = n_tiles * op.m_pc;
+  DevMem cnt(sizeof(int) * n_cells);
+  STL_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+  k_mma_ccount<<<nblocks(nt, 256), 256, 0, s>>>(op.m_cells.as<int32_t>(), nt, op.m_pc, op.o2, cnt.as<int>());
+  STL_CUDA(cudaGetLastError());
+  std::vector<int> hc(n_cells);
+  STL_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, cnt.bytes, cudaMemcpyDeviceToHost, s));
+  STL_CUDA(cudaStreamSynchronize(s));
+  std::vector<i64> ho(n_cells + 1, 0);
+  for (i64 v = 0; v < n_cells; ++v) ho[v + 1] = ho[v] + hc[v];
+  op.coff.alloc(sizeof(i64) * (n_cells + 1));
+  op.clist.alloc(sizeof(uint32_t) * std::max<i64>(ho[n_cells], 1));
+  STL_CUDA(cudaMemcpyAsync(op.coff.p, ho.data(), op.coff.bytes, cudaMemcpyHostToDevice, s));
+  STL_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+  k_mma_cfill<<<nblocks(nt, 256), 256, 0, s>>>(op.m_cells.as<int32_t>(), nt, op.m_pc, op.o2, op.coff.as<i64>(),
+                                               cnt.as<int>(), op.clist.as<uint32_t>());
+  STL_CUDA(cudaGetLastError());
+  k_adj_csort<<<nblocks(n_cells, 256), 256, 0, s>>>(op.coff.as<i64>(), n_cells, op.clist.as<uint32_t>());
+  STL_CUDA(cudaGetLastError());
+  STL_CUDA(cudaStreamSynchronize(s));
+  op.ncs = op.m_pc;
+  op.mma = true;
+  return true;
+}
+
 template <typename T>
 static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, ConvOp& op, cudaStream_t s) {
   const int P = sp.ksz * sp.ksz;
@@ -866,6 +1177,20 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   // of kAdjTile stored rows, then the edge colouring of its entries
   op.adj_tiles = false;
   op.colored = false;
+  op.mma = false;
+  if (std::is_same<T, float>::value && sym && sp.tensor_cores) {
+    // FP32 full sky: the tensor-core layout when every tile fits it
+    op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
+    k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
+    STL_CUDA(cudaGetLastError());
+    if (build_mma_layout(op, counts, s)) {
+      op.cell.release();
+      op.coef.release();
+      return;
+    }
+    op.rowsum.release();
+    op.m_coef.release(); op.m_cells.release(); op.m_lc.release(); op.m_wlc.release(); op.m_winv.release();
+  }
   if (sym && op.S <= 128) {  // the tile sort holds 128 slots per row
     op.n_tiles = (a.n_rows + kAdjTile - 1) / kAdjTile;
     op.tile_slots.alloc(sizeof(int32_t) * op.n_tiles);

@@ -805,6 +805,362 @@ __global__ void __launch_bounds__(128) k_adj_combine(const i64* __restrict__ cof
   }
 }
 
+// ---- tensor-core wavelets (FP32 fields, ConvOp::mma) ---------------------------
+// Per stored row u the wavelet is a small product: for the 16 (rotation k,
+// field row r) pairs of an M tile, out[(k, r)][o] = sum_s X[k][cell(u, s)][r]
+// C_u[s][o] (o = the 4 gauges' re, im), so one mma.sync m16n8k8 covers one
+// row and a chunk of 8 slots.  FP32 accuracy from TF32 operands by the
+// 3xTF32 split: a = a_hi + a_lo (a_hi = tf32(a), a_lo = tf32(a - a_hi)),
+// a b ~ a_lo b_hi + a_hi b_lo + a_hi b_hi, the three products of a chunk
+// accumulated from zero (small ones first) and the chunk's result added in
+// FP32 registers -- the tensor core's own accumulation truncates, which
+// would bias sums carried across chunks.
+// Fragments (lane = 4 g + t): A a0 (g, t), a1 (g + 8, t), a2 (g, t + 4),
+// a3 (g + 8, t + 4); B b0 (t, g), b1 (t + 4, g); D d0 (g, 2 t), d1 (g,
+// 2 t + 1), d2 (g + 8, 2 t), d3 (g + 8, 2 t + 1).  M row g is (k = g >> 1,
+// field row r(h = 0)) and g + 8 (k, r(h = 1)) with r = (g & 1) 2 MT + 2 mt
+// + h in M tile mt, so a lane's rows of one cell are contiguous.
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float d[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+// one chunk (K = 8) in 3xTF32, from zero
+__device__ __forceinline__ void mma3(float d[4], const uint32_t ah[4], const uint32_t al[4], const uint32_t bh[2],
+                                     const uint32_t bl[2]) {
+  d[0] = d[1] = d[2] = d[3] = 0.0f;
+  mma_tf32(d, al, bh);
+  mma_tf32(d, ah, bl);
+  mma_tf32(d, ah, bh);
+}
+
+constexpr int kMmaWarps = kMmaRows / kMmaWarpRows;
+constexpr int kMmaThreads = 32 * kMmaWarps;
+// floats per staged slot (kMmaRows rows of 8 coefficients, then padding):
+// slot stride 8 (forward) or 4 (adjoint) banks mod 32, so the B fragments'
+// 32 words fall in distinct banks
+constexpr int kMmaFwdSlot = kMmaRows * 8 + 8;
+constexpr int kMmaAdjSlot = kMmaRows * 8 + 4;
+constexpr size_t kMmaFwdStage = 8 * kMmaFwdSlot * sizeof(float) + 8 * kMmaRows * sizeof(uint16_t);
+constexpr size_t kMmaAdjStage = 8 * kMmaAdjSlot * sizeof(float) + 8 * kMmaRows;
+
+// Forward: one CTA per (tile, group of 4 MT field rows), warp w the rows
+// 8 w .. 8 w + 7 of the tile.  The tile's plane [4 k][pcs][4 MT] of input
+// rows (cell -1: zero) is gathered once; per chunk of 8 slots the
+// coefficients and plane cells of every row arrive by bulk copies (two
+// stages); every row's accumulators live in registers across the chunks.
+template <int MT>
+__global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
+    const uint16_t* __restrict__ m_lc, const float* __restrict__ coef, int Sm, i64 n_rep, int o2,
+    const int32_t* __restrict__ cells, int pcs, const int32_t* __restrict__ tch, const uint8_t* __restrict__ rowch,
+    const float* __restrict__ x, int R, float* __restrict__ out, float* __restrict__ mod, int mod_pix, int mod_row,
+    int mod_off, int* __restrict__ err, const float* __restrict__ rowsum, const double* __restrict__ rc) {
+  constexpr int RM = 4 * MT;
+  constexpr size_t kCoefBytes = 8 * kMmaFwdSlot * sizeof(float);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int fail;
+  float* plane = reinterpret_cast<float*>(smem_raw + 2 * kMmaFwdStage);
+  const int ngroups = (R + RM - 1) / RM;
+  const i64 tile = blockIdx.x / ngroups;
+  const int r0 = (int)(blockIdx.x % ngroups) * RM;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int k = g >> 1, rq = g & 1;
+  const i64 u0 = tile * kMmaRows;
+  const int rows = (int)min((i64)kMmaRows, n_rep - u0);
+  const int nch = tch[tile];
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int c) {
+    const int st = c & 1;
+    unsigned char* base = smem_raw + st * kMmaFwdStage;
+    const unsigned cb = (unsigned)(rows * 8 * sizeof(float));
+    const unsigned lb = (unsigned)(8 * kMmaRows * sizeof(uint16_t));
+    mbar_expect_tx(&bar[st], 8 * cb + lb);
+    for (int sl = 0; sl < 8; ++sl)
+      bulk_g2s(base + (size_t)sl * kMmaFwdSlot * sizeof(float), coef + ((i64)(8 * c + sl) * n_rep + u0) * 8, cb,
+               &bar[st]);
+    bulk_g2s(base + kCoefBytes, m_lc + ((i64)tile * Sm + 8 * c) * kMmaRows, lb, &bar[st]);
+  };
+  if (tid == 0) {
+    if (nch > 0) issue(0);
+    if (nch > 1) issue(1);
+  }
+  const int32_t* tc = cells + tile * pcs;
+  const bool whole = R % 4 == 0;  // whole groups of 16-byte aligned rows; else rows past R are zero
+  for (int i = tid; i < 4 * pcs; i += kMmaThreads) {
+    const int kk = i / pcs, pl = i - kk * pcs;
+    const int32_t cl = tc[pl];
+    float v[RM];
+#pragma unroll
+    for (int q = 0; q < RM; ++q) v[q] = 0.0f;
+    if (cl >= 0) {
+      const float* xp = x + rot_cell(cl, kk, o2) * R + r0;
+      if (whole) loadR<RM>(xp, v);
+      else
+#pragma unroll
+        for (int q = 0; q < RM; ++q)
+          if (r0 + q < R) v[q] = __ldg(xp + q);
+    }
+#pragma unroll
+    for (int q = 0; q < RM; ++q) plane[(size_t)i * RM + q] = v[q];
+  }
+  int rch[kMmaWarpRows];
+#pragma unroll
+  for (int i = 0; i < kMmaWarpRows; ++i) {
+    const int ul = warp * kMmaWarpRows + i;
+    rch[i] = ul < rows ? (int)rowch[u0 + ul] : 0;
+  }
+  float acc[kMmaWarpRows][MT][4];
+#pragma unroll
+  for (int i = 0; i < kMmaWarpRows; ++i)
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][mt][q] = 0.0f;
+  const float* pk = plane + (size_t)k * pcs * RM + rq * 2 * MT;
+  int c = 0;
+  for (; c < nch; ++c) {
+    const int st = c & 1;
+    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    __syncthreads();  // also orders the plane gather before the first chunk
+    if (fail) break;
+    const unsigned char* base = smem_raw + st * kMmaFwdStage;
+    const float* cs = reinterpret_cast<const float*>(base);
+    const uint16_t* ls = reinterpret_cast<const uint16_t*>(base + kCoefBytes);
+#pragma unroll
+    for (int i = 0; i < kMmaWarpRows; ++i) {
+      if (c >= rch[i]) continue;  // warp-uniform: the row has no more chunks
+      const int ul = warp * kMmaWarpRows + i;
+      const int lc0 = ls[t * kMmaRows + ul], lc1 = ls[(t + 4) * kMmaRows + ul];
+      uint32_t bh[2], bl[2];
+      split_tf32(cs[t * kMmaFwdSlot + ul * 8 + g], bh[0], bl[0]);
+      split_tf32(cs[(t + 4) * kMmaFwdSlot + ul * 8 + g], bh[1], bl[1]);
+      float va[2 * MT], vb[2 * MT];
+      if (MT == 2) {
+        const float4 p = *reinterpret_cast<const float4*>(pk + (size_t)lc0 * RM);
+        const float4 q = *reinterpret_cast<const float4*>(pk + (size_t)lc1 * RM);
+        va[0] = p.x; va[1] = p.y; va[2] = p.z; va[3] = p.w;
+        vb[0] = q.x; vb[1] = q.y; vb[2] = q.z; vb[3] = q.w;
+      } else {
+        const float2 p = *reinterpret_cast<const float2*>(pk + (size_t)lc0 * RM);
+        const float2 q = *reinterpret_cast<const float2*>(pk + (size_t)lc1 * RM);
+        va[0] = p.x; va[1] = p.y;
+        vb[0] = q.x; vb[1] = q.y;
+      }
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        uint32_t ah[4], al[4];
+        split_tf32(va[2 * mt], ah[0], al[0]);
+        split_tf32(va[2 * mt + 1], ah[1], al[1]);
+        split_tf32(vb[2 * mt], ah[2], al[2]);
+        split_tf32(vb[2 * mt + 1], ah[3], al[3]);
+        float d[4];
+        mma3(d, ah, al, bh, bl);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][mt][q] += d[q];
+      }
+    }
+    __syncthreads();  // the stage is read: refill it
+    if (tid == 0 && c + 2 < nch) issue(c + 2);
+  }
+  if (fail) {
+    bool drained = true;
+    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
+    return;
+  }
+  const bool odd = k & 1;
+  const int go = odd ? (t ^ 2) : t;  // output gauge of stored gauge t under rotation k
+  const bool cj = rot_conj(k, go);
+#pragma unroll
+  for (int i = 0; i < kMmaWarpRows; ++i) {
+    const int ul = warp * kMmaWarpRows + i;
+    if (ul >= rows) continue;
+    const i64 u = u0 + ul;
+    const i64 p = rot_pixel(u, k, o2);
+    float rs0 = 0.0f, rs1 = 0.0f;
+    if (rc) {
+      rs0 = rowsum[u * 8 + 2 * t];
+      rs1 = rowsum[u * 8 + 2 * t + 1];
+    }
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = r0 + rq * 2 * MT + 2 * mt + h;
+        if (r >= R) continue;
+        float re = acc[i][mt][2 * h], im = acc[i][mt][2 * h + 1];
+        if (rc) {  // the row's constant times the row sums of the coefficients
+          const double cr = rc[r];
+          re += (float)(cr * (double)rs0);
+          im += (float)(cr * (double)rs1);
+        }
+        if (cj) im = -im;
+        *reinterpret_cast<float2*>(out + (p * R + r) * 8 + 2 * go) = make_float2(re, im);
+        if (mod) mod[p * mod_pix + (i64)r * mod_row + mod_off + go] = hypotf(re, im);
+      }
+  }
+}
+
+// Adjoint: one CTA per (tile, 4 cotangent rows); warp w adds the products
+// of its rows into private sums [4 k][wls][4 r] over the distinct cells of
+// its rows (warp-local numbering), so no other warp touches them and no
+// barrier separates the slots; per chunk and row one mma gives the 16 x 8
+// products (rotation and row) x (slot) of the row's cotangents with its
+// coefficients.  Then every tile cell's partial is the sum over the warps,
+// in warp order, written to part[tile][k][pcs][R].  madd: the modulus VJP
+// added to the cotangents first, as k_conv_adj_colored.
+__global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
+    const uint8_t* __restrict__ m_wlc, const float* __restrict__ coef, int Sm, i64 n_rep, int o2,
+    const int32_t* __restrict__ tch, const uint8_t* __restrict__ rowch, const uint8_t* __restrict__ m_winv, int pcs,
+    int wls, const float* __restrict__ gy, int R, float* __restrict__ part, int* __restrict__ err,
+    ModulusAdd<float> madd) {
+  constexpr size_t kCoefBytes = 8 * kMmaAdjSlot * sizeof(float);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int fail;
+  float* sums = reinterpret_cast<float*>(smem_raw + 2 * kMmaAdjStage);  // [warps][4][wls][4]
+  const int ngroups = (R + 3) / 4;  // rows past R (the last group of R % 4 != 0) are zero
+  const i64 tile = blockIdx.x / ngroups;
+  const int r0 = (int)(blockIdx.x % ngroups) * 4;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int k = g >> 1, rp = g & 1;
+  const i64 u0 = tile * kMmaRows;
+  const int rows = (int)min((i64)kMmaRows, n_rep - u0);
+  const int nch = tch[tile];
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int c) {
+    const int st = c & 1;
+    unsigned char* base = smem_raw + st * kMmaAdjStage;
+    const unsigned cb = (unsigned)(rows * 8 * sizeof(float));
+    const unsigned wb = (unsigned)(8 * kMmaRows);
+    mbar_expect_tx(&bar[st], 8 * cb + wb);
+    for (int sl = 0; sl < 8; ++sl)
+      bulk_g2s(base + (size_t)sl * kMmaAdjSlot * sizeof(float), coef + ((i64)(8 * c + sl) * n_rep + u0) * 8, cb,
+               &bar[st]);
+    bulk_g2s(base + kCoefBytes, m_wlc + ((i64)tile * (Sm / 8) + c) * kMmaRows * 8, wb, &bar[st]);
+  };
+  if (tid == 0) {
+    if (nch > 0) issue(0);
+    if (nch > 1) issue(1);
+  }
+  float* mine = sums + (size_t)warp * 16 * wls;
+  for (int i = lane; i < 16 * wls; i += 32) mine[i] = 0.0f;
+  // the rows' cotangents under rotation k (gauge permutation, conjugation
+  // and the modulus VJP folded in) as split A fragments
+  const bool odd = k & 1;
+  auto cot = [&](i64 p, int rr, int o) {
+    if (r0 + rr >= R) return 0.0f;
+    const int q = o >> 1, pt = o & 1;
+    const int gg = odd ? (q ^ 2) : q;
+    const i64 e = (p * R + r0 + rr) * 8;
+    float v = gy[e + 2 * gg + pt];
+    if (madd.z) {
+      const float zr = madd.z[e + 2 * gg], zi = madd.z[e + 2 * gg + 1];
+      const float mag = hypotf(zr, zi);
+      const float dd = mag == 0.0f ? 1.0f : mag;
+      const float gv = madd.g[p * madd.g_pix + (i64)(r0 + rr) * madd.g_row + gg];
+      v += gv * (pt ? zi : zr) / dd;
+    }
+    return (pt && rot_conj(k, gg)) ? -v : v;
+  };
+  uint32_t ah[kMmaWarpRows][4], al[kMmaWarpRows][4];
+  int rch[kMmaWarpRows];
+#pragma unroll
+  for (int i = 0; i < kMmaWarpRows; ++i) {
+    const int ul = warp * kMmaWarpRows + i;
+    rch[i] = ul < rows ? (int)rowch[u0 + ul] : 0;
+    float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (ul < rows) {
+      const i64 p = rot_pixel(u0 + ul, k, o2);
+      a[0] = cot(p, 2 * rp, t);
+      a[1] = cot(p, 2 * rp + 1, t);
+      a[2] = cot(p, 2 * rp, t + 4);
+      a[3] = cot(p, 2 * rp + 1, t + 4);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) split_tf32(a[q], ah[i][q], al[i][q]);
+  }
+  float* mk = mine + (size_t)k * wls * 4 + 2 * rp;
+  int c = 0;
+  for (; c < nch; ++c) {
+    const int st = c & 1;
+    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    __syncthreads();  // also orders the zeroed sums before the first chunk
+    if (fail) break;
+    const unsigned char* base = smem_raw + st * kMmaAdjStage;
+    const float* cs = reinterpret_cast<const float*>(base);
+    const uint8_t* ws = base + kCoefBytes;
+#pragma unroll
+    for (int i = 0; i < kMmaWarpRows; ++i) {
+      if (c >= rch[i]) continue;  // warp-uniform
+      const int ul = warp * kMmaWarpRows + i;
+      uint32_t bh[2], bl[2];
+      split_tf32(cs[g * kMmaAdjSlot + ul * 8 + t], bh[0], bl[0]);
+      split_tf32(cs[g * kMmaAdjSlot + ul * 8 + t + 4], bh[1], bl[1]);
+      float d[4];
+      mma3(d, ah[i], al[i], bh, bl);
+      const uint16_t wp = *reinterpret_cast<const uint16_t*>(ws + ul * 8 + 2 * t);
+      float2* s0 = reinterpret_cast<float2*>(mk + (size_t)(wp & 0xff) * 4);
+      float2* s1 = reinterpret_cast<float2*>(mk + (size_t)(wp >> 8) * 4);
+      float2 v0 = *s0, v1 = *s1;
+      v0.x += d[0]; v0.y += d[2];
+      v1.x += d[1]; v1.y += d[3];
+      *s0 = v0;
+      *s1 = v1;
+      __syncwarp();  // the next row may add to the same cells
+    }
+    __syncthreads();  // the stage is read: refill it
+    if (tid == 0 && c + 2 < nch) issue(c + 2);
+  }
+  if (fail) {
+    bool drained = true;
+    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
+    return;
+  }
+  __syncthreads();  // every warp's sums are complete (also when the tile has no chunk)
+  // tile partials: per (k, plane cell, r) the warps' sums in warp order
+  const uint8_t* winv = m_winv + tile * kMmaWarps * pcs;
+  for (int i = tid; i < 16 * pcs; i += kMmaThreads) {
+    const int r = i & 3, pk = i >> 2;
+    if (r0 + r >= R) continue;
+    const int kk = pk / pcs, pl = pk - kk * pcs;
+    float v = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kMmaWarps; ++w) {
+      const int wl = winv[w * pcs + pl];
+      if (wl != 255) v += sums[(((size_t)w * 4 + kk) * wls + wl) * 4 + r];
+    }
+    part[((tile * 4 + kk) * pcs + pl) * R + r0 + r] = v;
+  }
+}
+
 // ---- decimation ---------------------------------------------------------------
 // y[c][ro][ri] (+)= sum_e w[e][c] x[col[e][c]][ro][ri]; one thread per (stored
 // row u, chunk of RB rows of the R_outer x R_inner rows), NK rotations per
@@ -1754,6 +2110,34 @@ void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x
                              accumulate, s, rb);
 }
 
+// tensor-core launches (FP32 operators in the tensor-core layout)
+inline size_t fwd_mma_smem(const ConvOp& op, int MT) { return 2 * kMmaFwdStage + sizeof(float) * 4 * op.m_pc * 4 * MT; }
+inline size_t adj_mma_smem(const ConvOp& op) { return 2 * kMmaAdjStage + sizeof(float) * kMmaWarps * 16 * op.m_wl; }
+
+template <int MT>
+void conv_forward_mma_mt(const ConvOp& op, const float* x, int R, float* out, float* mod, int mod_pix, int mod_row,
+                         int mod_off, int* err, const double* rc, cudaStream_t s) {
+  allow_dynamic_smem(k_conv_fwd_mma<MT>);
+  dim3 grid((unsigned)(op.m_tiles * ((R + 4 * MT - 1) / (4 * MT))));
+  k_conv_fwd_mma<MT><<<grid, kMmaThreads, fwd_mma_smem(op, MT), s>>>(
+      op.m_lc.as<uint16_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_cells.as<int32_t>(), op.m_pc,
+      op.m_tch.as<int32_t>(), op.m_rowch.as<uint8_t>(), x, R, out, mod, mod_pix, mod_row, mod_off, err,
+      op.rowsum.as<float>(), rc);
+}
+
+void conv_adjoint_mma(const ConvOp& op, const float* gy, int R, float* gx, bool accumulate, const AdjScratch& scr,
+                      cudaStream_t s, int* err, const ModulusAdd<float>* madd) {
+  allow_dynamic_smem(k_conv_adj_mma);
+  dim3 grid((unsigned)(op.m_tiles * ((R + 3) / 4)));
+  k_conv_adj_mma<<<grid, kMmaThreads, adj_mma_smem(op), s>>>(
+      op.m_wlc.as<uint8_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_tch.as<int32_t>(),
+      op.m_rowch.as<uint8_t>(), op.m_winv.as<uint8_t>(), op.m_pc, op.m_wl, gy, R, static_cast<float*>(scr.part), err,
+      madd ? *madd : ModulusAdd<float>());
+  if (R % 4 == 0) adj_combine_rb<float, 4>(op, R, gx, accumulate, scr, s);
+  else if (R % 2 == 0) adj_combine_rb<float, 2>(op, R, gx, accumulate, scr, s);
+  else adj_combine_rb<float, 1>(op, R, gx, accumulate, scr, s);
+}
+
 // cotangent rows per CTA: FP32 up to 4 (coloured) or 2; FP64 1 (the
 // coloured kernel's 1024 threads hold 64 registers each)
 inline int adj_rb(const ConvOp& op, size_t elem, int R) {
@@ -1790,6 +2174,18 @@ template <typename T>
 void conv_forward(const ConvOp& op, const T* x, int R, T* out, T* mod, int mod_pix, int mod_row, int mod_off,
                   cudaStream_t s, int* err, const double* rc, int rb) {
   if (rc && !op.rowsum.p) throw std::runtime_error("wavelet operator without row sums");
+  if (op.mma) {
+    if (sizeof(T) != 4 || !err) throw std::runtime_error("the tensor-core wavelet takes FP32 rows and an error flag");
+    const int MT = R % 8 == 0 ? 2 : 1;
+    if (rb && rb != 4 * MT) throw std::runtime_error("invalid wavelet tile height");
+    const float* xf = reinterpret_cast<const float*>(x);
+    float* of = reinterpret_cast<float*>(out);
+    float* mf = reinterpret_cast<float*>(mod);
+    if (MT == 2) conv_forward_mma_mt<2>(op, xf, R, of, mf, mod_pix, mod_row, mod_off, err, rc, s);
+    else conv_forward_mma_mt<1>(op, xf, R, of, mf, mod_pix, mod_row, mod_off, err, rc, s);
+    STL_CUDA(cudaGetLastError());
+    return;
+  }
   const std::vector<int> ok = conv_forward_choices(op, sizeof(T), R, err != nullptr);
   if (ok.empty() || (rb && std::find(ok.begin(), ok.end(), rb) == ok.end()))
     throw std::runtime_error("invalid wavelet tile height");
@@ -1820,6 +2216,10 @@ bool forward_tiles(const ConvOp& op, size_t elem, bool err) {
 // valid tile heights (rows of the field per thread) of a wavelet launch
 std::vector<int> conv_forward_choices(const ConvOp& op, size_t elem, int R, bool err) {
   std::vector<int> v;
+  if (op.mma) {  // one shape: M tiles of 16 (rotation, row) pairs, two per CTA when the rows allow
+    if (elem == 4 && err) v.push_back(R % 8 == 0 ? 8 : 4);
+    return v;
+  }
   const bool tiles = forward_tiles(op, elem, err);
   for (int rb : {1, 2, 4}) {
     if (R % rb) continue;
@@ -1838,11 +2238,14 @@ std::vector<int> conv_forward_choices(const ConvOp& op, size_t elem, int R, bool
 }
 
 size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R) {
+  if (op.mma) return elem * (size_t)op.m_tiles * 4 * op.m_pc * R;
   if (!op.adj_tiles) return 0;
   return elem * (size_t)op.n_tiles * 4 * op.ncs * R;
 }
 
 bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
+  if (op.mma)
+    return scr && elem == 4 && adjoint_part_bytes(op, elem, R) <= scr->capacity && adj_mma_smem(op) <= 227 * 1024;
   if (!scr || !op.adj_tiles || op.nk != 4) return false;
   if (adjoint_part_bytes(op, elem, R) > scr->capacity) return false;
   if (op.colored) return (elem == 4 ? adjc_smem<float, 4>(op) : adjc_smem<double, 1>(op)) <= 227 * 1024;
@@ -1852,7 +2255,7 @@ bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch
 }
 
 bool conv_adjoint_fuses_modulus(const ConvOp& op, size_t elem, int R, const AdjScratch* scr, int* err) {
-  return op.colored && err && adjoint_tiles_usable(op, elem, R, scr);
+  return (op.colored || op.mma) && err && adjoint_tiles_usable(op, elem, R, scr);
 }
 
 template <typename T>
@@ -1863,6 +2266,14 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
   if (rb) {
     const std::vector<int> ok = conv_adjoint_choices(op, sizeof(T), R, scr);
     if (std::find(ok.begin(), ok.end(), rb) == ok.end()) throw std::runtime_error("invalid adjoint tile height");
+  }
+  if (op.mma) {
+    if (!adjoint_tiles_usable(op, sizeof(T), R, scr) || !err)
+      throw std::runtime_error("the tensor-core adjoint needs FP32 rows, an error flag and tile scratch");
+    conv_adjoint_mma(op, reinterpret_cast<const float*>(gy), R, reinterpret_cast<float*>(gx), accumulate, *scr, s,
+                     err, reinterpret_cast<const ModulusAdd<float>*>(madd));
+    STL_CUDA(cudaGetLastError());
+    return;
   }
   if (adjoint_tiles_usable(op, sizeof(T), R, scr)) {
     if (!rb) rb = adj_rb(op, sizeof(T), R);
@@ -1888,6 +2299,10 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
 // valid tile heights of an adjoint launch
 std::vector<int> conv_adjoint_choices(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
   std::vector<int> v;
+  if (op.mma) {
+    if (adjoint_tiles_usable(op, elem, R, scr)) v.push_back(4);
+    return v;
+  }
   const bool tiles = adjoint_tiles_usable(op, elem, R, scr);
   for (int rb : {1, 2, 4}) {
     if (R % rb) continue;

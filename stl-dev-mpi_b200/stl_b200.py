@@ -164,7 +164,7 @@ class NativeEngine:
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
-                 prepare=False, autotune=True, autotune_cache=None, cross=False, **unused):
+                 prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=True, **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -181,6 +181,8 @@ class NativeEngine:
                            orientations=int(orientations), device=self.device, dtype=dtype)
         if not autotune:  # keep the default tile heights (no timing at prepare)
             self.config["autotune"] = False
+        if not tensor_cores:  # FP32 wavelets on the CUDA cores (the coloured layout)
+            self.config["tensor_cores"] = False
         if cross:
             self.config["cross"] = True
         if autotune_cache:  # a file of tile heights timed before (read, then extended)

@@ -1,0 +1,98 @@
+"""The FP32 wavelets on the tensor cores (3xTF32 mma.sync over the
+tensor-core operator layout) against the FP32 CUDA-core kernels of the
+coloured layout and the FP64 path: statistics under the 1e-6 family
+criterion, gradients, bit-reproducibility, and the layout each level gets."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def stl():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a CUDA device is required")
+    import stl_b200
+    return stl_b200
+
+
+def family_ratio(plan, values, ref):
+    """max over coefficients of |v - r| / (1e-6 max|r| of its (family, level, map) + 1e-6 |r|)."""
+    fam = np.array([c["family"] for c in plan])
+    lev = np.array([c["native_dg"] for c in plan])
+    worst = 0.0
+    for f in set(fam):
+        for n in set(lev):
+            sel = (fam == f) & (lev == n)
+            if not sel.any():
+                continue
+            r, v = ref[:, sel], values[:, sel]
+            scale = np.max(np.abs(r), axis=1, keepdims=True)
+            for part in (np.real, np.imag):
+                err = np.abs(part(v) - part(r))
+                worst = max(worst, float(np.max(err / (1e-6 * scale + 1e-6 * np.abs(part(r))))))
+    return worst
+
+
+def maps(seed, B, nside):
+    g = np.random.default_rng(seed).standard_normal((B, 12 * nside * nside))
+    return np.exp(g - 0.5).astype(np.float32).astype(np.float64)
+
+
+def test_layout_per_level(stl):
+    """FP32 levels above nside 32 hold the tensor-core layout; the FP64 coarse
+    levels (and every level with tensor_cores off) the coloured one."""
+    e = stl.NativeEngine(128, 5, dtype="float32")
+    e.prepare()
+    layouts = [o["layout"] for o in e.info()["operators"]]
+    assert layouts[:2] == ["tensor_cores", "tensor_cores"], layouts
+    assert all(v == "coloured" for v in layouts[2:]), layouts
+    off = stl.NativeEngine(128, 5, dtype="float32", tensor_cores=False)
+    off.prepare()
+    assert all(o["layout"] == "coloured" for o in off.info()["operators"])
+
+
+@pytest.mark.parametrize("nside,J,B", [(128, 5, 4), (256, 6, 2), (128, 4, 1), (64, 4, 3)])
+def test_tensor_cores_match_cuda_cores_and_fp64(stl, nside, J, B):
+    x = maps(nside + B, B, nside)
+    t = maps(1000 + nside, B, nside)
+    out = {}
+    for name, kw in (("tc", dict(dtype="float32")), ("cc", dict(dtype="float32", tensor_cores=False)),
+                     ("f64", dict(dtype="float64"))):
+        e = stl.NativeEngine(nside, J, batch=B, **kw)
+        tv, _ = e.forward(t, generation=1)
+        v, _ = e.forward(x, generation=2)
+        cot = 2.0 * (v - tv)
+        g = e.vjp(cot, generation=2)
+        out[name] = (v, g, e.plan)
+        e.close()
+    v64, g64, plan = out["f64"]
+    for name in ("tc", "cc"):
+        v, g, _ = out[name]
+        ratio = family_ratio(plan, v, v64)
+        gerr = float(np.max(np.abs(g - g64)) / np.max(np.abs(g64)))
+        print(f"nside {nside}: {name} vs FP64 family ratio {ratio:.3f}, gradient {gerr:.2e}")
+        assert ratio <= 1.0
+        assert gerr <= 1e-4
+    # the two FP32 forms agree with each other as closely as either with FP64
+    assert family_ratio(plan, out["tc"][0], out["cc"][0]) <= 1.0
+    assert np.max(np.abs(out["tc"][1] - out["cc"][1])) <= 1e-4 * np.max(np.abs(g64))
+
+
+def test_tensor_cores_bit_reproducible(stl):
+    nside, J, B = 128, 5, 2
+    x = maps(9, B, nside)
+    e = stl.NativeEngine(nside, J, batch=B, dtype="float32")
+    v1, _ = e.forward(x, generation=1)
+    cot = np.random.default_rng(10).standard_normal(v1.shape) + 1j * np.random.default_rng(11).standard_normal(v1.shape)
+    g1 = e.vjp(cot, generation=1)
+    v2, _ = e.forward(x, generation=2)
+    g2 = e.vjp(cot, generation=2)
+    assert np.array_equal(v1, v2)
+    assert np.array_equal(g1, g2)
+    e2 = stl.NativeEngine(nside, J, batch=B, dtype="float32", autotune=False)
+    v3, _ = e2.forward(x, generation=3)
+    g3 = e2.vjp(cot, generation=3)
+    assert np.array_equal(v1, v3)
+    assert np.array_equal(g1, g3)
