@@ -161,6 +161,45 @@ int stlp_patch_forward_device(StlpPatchHandle* h, uint64_t x, size_t n, uint64_t
                               double* out, double* var);
 int stlp_patch_vjp_device(StlpPatchHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t out);
 
+/* Objective terms of the synthesis on the device (the loss terms stl-synth
+ * adds after the statistics).  The reference has no C entry points for
+ * them: its CLI calls crates/stl-gpu/src/terms.rs in-process (DeviceTable,
+ * Pyramid, RadixSort, marginal_row, add_product; kernels.cu:1454-1707);
+ * these expose the same operations to C and Python callers.  Device
+ * addresses are uint64_t (f64 arrays unless noted), every launch goes to
+ * the handle's stream; calls that return host values wait for it.
+ * Configuration JSON: rows (1), len (cells per row, a multiple of
+ * 4^depth), depth (pyramid levels above the maps), sort (most values one
+ * sort takes), device (0).  Element-wise results equal the host
+ * expressions bit for bit; sums over pixels are fixed-order chunk trees. */
+typedef struct StlpTerms StlpTerms;
+StlpTerms* stlp_terms_new(const char* json);
+void stlp_terms_free(StlpTerms* h);
+int stlp_terms_set_stream(StlpTerms* h, uint64_t stream);
+/* knots x (increasing), values y and slopes d of the monotone cubic (terms.rs:20-35) */
+int stlp_terms_kappa_table(StlpTerms* h, const double* x, const double* y, const double* d, size_t n);
+/* k = (f(x gs + gm) - km) / ks and its derivative dk, n values (terms.rs:37-58) */
+int stlp_terms_kappa(StlpTerms* h, uint64_t x, size_t n, double gm, double gs, double km, double ks, uint64_t k,
+                     uint64_t dk);
+/* levels 1..depth of the 4-children pyramid of the rows x [rows][len] (terms.rs:78-102) */
+int stlp_terms_pyramid(StlpTerms* h, uint64_t x);
+/* out [rows][depth][2] = (sum d^2, sum d^4) of the details of every level (terms.rs:117-138) */
+int stlp_terms_moments(StlpTerms* h, uint64_t x, double* out);
+/* g [rows][len] += sum_{n < L} coef[r L + n] d_n (host coef [rows][L]) (terms.rs:148-163) */
+int stlp_terms_level_power_grad(StlpTerms* h, uint64_t x, const double* coef, size_t L, uint64_t g);
+/* g += (dk) sum_k cf0 (d^3 - c - cf1 cf2 d) over the levels (host levels [T], cf [rows][T][3];
+ * dk 0: none) (terms.rs:165-184) */
+int stlp_terms_kurtosis_grad(StlpTerms* h, uint64_t x, const int* levels, size_t T, const double* cf, uint64_t dk,
+                             uint64_t g);
+/* perm (u32) = positions of the n values x in increasing f64 total order, ties in position
+ * order (terms.rs:187-258) */
+int stlp_terms_sort(StlpTerms* h, uint64_t x, size_t n, uint64_t perm);
+/* g[perm[q]] += coef (x[perm[q]] - t[q]) and *sum_sq = sum of the squares (terms.rs:260-269) */
+int stlp_terms_marginal(StlpTerms* h, uint64_t x, uint64_t perm, uint64_t t_sorted, size_t n, double coef,
+                        uint64_t g, double* sum_sq);
+/* g += a b (b 0: g += a), n values (terms.rs:271-275) */
+int stlp_terms_add_product(StlpTerms* h, uint64_t g, uint64_t a, uint64_t b, size_t n);
+
 /* Entry points of subsystems outside this engine (spin-2 front end,
  * spectrum, U-Net training).  They exist so that native.py's signature
  * table binds; each returns failure with stlp_last_error() naming the

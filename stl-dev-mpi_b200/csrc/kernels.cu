@@ -81,6 +81,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
   return false;
 }
 
+// 16-byte global -> shared copy of src_bytes (16, or 0: zero fill), not waited
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // 8 values of one (slot, row): float4 x 2 or double2 x 4
 __device__ __forceinline__ void load8(const float* p, float w[8]) {
   float4 a = __ldg(reinterpret_cast<const float4*>(p));
@@ -903,25 +910,28 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
     if (nch > 0) issue(0);
     if (nch > 1) issue(1);
   }
+  // the plane: per tile cell and rotation, the CTA's RM input rows, by
+  // asynchronous 16-byte copies (all in flight at once; a hole or a missing
+  // cell copies zero bytes, which fills zeros); rows past R (R % 4 != 0)
+  // by plain loads
   const int32_t* tc = cells + tile * pcs;
-  const bool whole = R % 4 == 0;  // whole groups of 16-byte aligned rows; else rows past R are zero
-  for (int i = tid; i < 4 * pcs; i += kMmaThreads) {
-    const int kk = i / pcs, pl = i - kk * pcs;
+  const bool whole = R % 4 == 0;
+  for (int pl = tid; pl < pcs; pl += kMmaThreads) {
     const int32_t cl = tc[pl];
-    float v[RM];
 #pragma unroll
-    for (int q = 0; q < RM; ++q) v[q] = 0.0f;
-    if (cl >= 0) {
-      const float* xp = x + rot_cell(cl, kk, o2) * R + r0;
-      if (whole) loadR<RM>(xp, v);
-      else
+    for (int kk = 0; kk < 4; ++kk) {
+      float* dst = plane + ((size_t)kk * pcs + pl) * RM;
+      const float* xp = x + (cl >= 0 ? rot_cell(cl, kk, o2) * R + r0 : 0);
+      if (whole) {
 #pragma unroll
-        for (int q = 0; q < RM; ++q)
-          if (r0 + q < R) v[q] = __ldg(xp + q);
+        for (int q = 0; q < MT; ++q) cp_async16(dst + 4 * q, xp + 4 * q, cl >= 0 ? 16 : 0);
+      } else {
+#pragma unroll
+        for (int q = 0; q < RM; ++q) dst[q] = (cl >= 0 && r0 + q < R) ? __ldg(xp + q) : 0.0f;
+      }
     }
-#pragma unroll
-    for (int q = 0; q < RM; ++q) plane[(size_t)i * RM + q] = v[q];
   }
+  cp_async_wait_all();  // this thread's copies; the barrier before the first chunk publishes them
   int rch[kMmaWarpRows];
 #pragma unroll
   for (int i = 0; i < kMmaWarpRows; ++i) {
@@ -1133,7 +1143,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
       v1.x += d[1]; v1.y += d[3];
       *s0 = v0;
       *s1 = v1;
-      __syncwarp();  // the next row may add to the same cells
+      // the next row may add to the same cells: the warp's shared-memory
+      // accesses are issued in program order (no lane diverges here) and
+      // the compiler keeps the order (the addresses may alias)
     }
     __syncthreads();  // the stage is read: refill it
     if (tid == 0 && c + 2 < nch) issue(c + 2);
@@ -1145,19 +1157,32 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
     return;
   }
   __syncthreads();  // every warp's sums are complete (also when the tile has no chunk)
-  // tile partials: per (k, plane cell, r) the warps' sums in warp order
+  // tile partials: per plane cell, for every (k, r), the warps' sums in warp order
   const uint8_t* winv = m_winv + tile * kMmaWarps * pcs;
-  for (int i = tid; i < 16 * pcs; i += kMmaThreads) {
-    const int r = i & 3, pk = i >> 2;
-    if (r0 + r >= R) continue;
-    const int kk = pk / pcs, pl = pk - kk * pcs;
-    float v = 0.0f;
+  for (int pl = tid; pl < pcs; pl += kMmaThreads) {
+    float4 v[4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) v[kk] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
     for (int w = 0; w < kMmaWarps; ++w) {
       const int wl = winv[w * pcs + pl];
-      if (wl != 255) v += sums[(((size_t)w * 4 + kk) * wls + wl) * 4 + r];
+      if (wl == 255) continue;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const float4 a = *reinterpret_cast<const float4*>(sums + (((size_t)w * 4 + kk) * wls + wl) * 4);
+        v[kk].x += a.x; v[kk].y += a.y; v[kk].z += a.z; v[kk].w += a.w;
+      }
     }
-    part[((tile * 4 + kk) * pcs + pl) * R + r0 + r] = v;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      float* o = part + ((tile * 4 + kk) * pcs + pl) * R + r0;
+      if (R % 4 == 0) {
+        *reinterpret_cast<float4*>(o) = v[kk];
+      } else {
+        const float e[4] = {v[kk].x, v[kk].y, v[kk].z, v[kk].w};
+        for (int r = 0; r < 4 && r0 + r < R; ++r) o[r] = e[r];
+      }
+    }
   }
 }
 

@@ -87,6 +87,19 @@ def lib():
             "stlp_patch_vjp": ([_VOID, _D, sz, u64, _D], C.c_int),
             "stlp_patch_forward_device": ([_VOID, u64, sz, u64, b, _D, _D], C.c_int),
             "stlp_patch_vjp_device": ([_VOID, _D, sz, u64, u64], C.c_int),
+            "stlp_terms_new": ([C.c_char_p], _VOID),
+            "stlp_terms_free": ([_VOID], None),
+            "stlp_terms_set_stream": ([_VOID, u64], C.c_int),
+            "stlp_terms_kappa_table": ([_VOID, _D, _D, _D, sz], C.c_int),
+            "stlp_terms_kappa": ([_VOID, u64, sz, C.c_double, C.c_double, C.c_double, C.c_double, u64, u64],
+                                 C.c_int),
+            "stlp_terms_pyramid": ([_VOID, u64], C.c_int),
+            "stlp_terms_moments": ([_VOID, u64, _D], C.c_int),
+            "stlp_terms_level_power_grad": ([_VOID, u64, _D, sz, u64], C.c_int),
+            "stlp_terms_kurtosis_grad": ([_VOID, u64, C.POINTER(C.c_int), sz, _D, u64, u64], C.c_int),
+            "stlp_terms_sort": ([_VOID, u64, sz, u64], C.c_int),
+            "stlp_terms_marginal": ([_VOID, u64, u64, u64, sz, C.c_double, u64, _D], C.c_int),
+            "stlp_terms_add_product": ([_VOID, u64, u64, u64, sz], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(l, name)
@@ -752,3 +765,100 @@ class PatchEngine:
 
     def __del__(self):
         self.close()
+
+
+class Terms:
+    """The synthesis objective's extra terms on CUDA float64 tensors (the
+    reference's device terms, crates/stl-gpu/src/terms.rs): the kappa
+    transform of a monotone cubic table, the 4-children pyramid of rows
+    [rows, len] with its detail moments and the level-power and kurtosis
+    gradients, the stable sort of a row in f64 total order and the pixel
+    marginal, and g += a b.  Launches go to torch's current stream; methods
+    returning host values wait for it."""
+
+    def __init__(self, rows=1, length=0, depth=0, sort=0, device=0):
+        cfg = dict(rows=int(rows), len=int(length), depth=int(depth), sort=int(sort), device=int(device))
+        self._lib = lib()
+        self._handle = self._lib.stlp_terms_new(json.dumps(cfg).encode())
+        if not self._handle:
+            raise _error()
+        self.rows, self.len, self.depth, self.sort_max, self.device = (cfg["rows"], cfg["len"], cfg["depth"],
+                                                                       cfg["sort"], cfg["device"])
+
+    def _call(self, name, *args):
+        import torch
+        if not self._handle:
+            raise RuntimeError("terms handle is closed")
+        s = torch.cuda.current_stream(torch.device("cuda", self.device)).cuda_stream
+        if self._lib.stlp_terms_set_stream(self._handle, s) or getattr(self._lib, name)(self._handle, *args):
+            raise _error()
+
+    @staticmethod
+    def _dev(t, n=None, dtype=None):
+        import torch
+        want = dtype or torch.float64
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == want and t.is_contiguous()):
+            raise ValueError(f"expected a contiguous CUDA {want} tensor")
+        if n is not None and t.numel() != n:
+            raise ValueError(f"expected {n} values, got {t.numel()}")
+        return t.data_ptr()
+
+    def kappa_table(self, x, y, d):
+        kx, ky, kd = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, d))
+        if not (kx.shape == ky.shape == kd.shape and kx.ndim == 1):
+            raise ValueError("knots, values and slopes must be 1-d arrays of one length")
+        self._call("stlp_terms_kappa_table", _ptr(kx), _ptr(ky), _ptr(kd), kx.size)
+
+    def kappa(self, x, gm, gs, km, ks):
+        """(k, dk) of the values x: k = (f(x gs + gm) - km) / ks, dk its derivative."""
+        import torch
+        k, dk = torch.empty_like(x), torch.empty_like(x)
+        self._call("stlp_terms_kappa", self._dev(x), x.numel(), float(gm), float(gs), float(km), float(ks),
+                   k.data_ptr(), dk.data_ptr())
+        return k, dk
+
+    def pyramid(self, x):
+        self._call("stlp_terms_pyramid", self._dev(x, self.rows * self.len))
+
+    def moments(self, x):
+        """[rows, depth, 2]: (sum d^2, sum d^4) of the details of every level."""
+        out = np.empty((self.rows, self.depth, 2))
+        self._call("stlp_terms_moments", self._dev(x, self.rows * self.len), _ptr(out))
+        return out
+
+    def level_power_grad(self, x, coef, g):
+        c = np.ascontiguousarray(coef, dtype=np.float64).reshape(self.rows, -1)
+        self._call("stlp_terms_level_power_grad", self._dev(x, self.rows * self.len), _ptr(c), c.shape[1],
+                   self._dev(g, self.rows * self.len))
+
+    def kurtosis_grad(self, x, levels, cf, g, dk=None):
+        lev = np.ascontiguousarray(levels, dtype=np.int32)
+        c = np.ascontiguousarray(cf, dtype=np.float64).reshape(self.rows, lev.size, 3)
+        self._call("stlp_terms_kurtosis_grad", self._dev(x, self.rows * self.len),
+                   lev.ctypes.data_as(C.POINTER(C.c_int)), lev.size, _ptr(c),
+                   0 if dk is None else self._dev(dk, self.rows * self.len), self._dev(g, self.rows * self.len))
+
+    def sort(self, x):
+        """int32 CUDA tensor of the positions of x in increasing f64 total order (ties by position)."""
+        import torch
+        perm = torch.empty(x.numel(), dtype=torch.int32, device=x.device)
+        self._call("stlp_terms_sort", self._dev(x), x.numel(), perm.data_ptr())
+        return perm
+
+    def marginal(self, x, perm, t_sorted, coef, g):
+        import torch
+        out = np.zeros(1)
+        self._call("stlp_terms_marginal", self._dev(x), self._dev(perm, x.numel(), torch.int32),
+                   self._dev(t_sorted, x.numel()), x.numel(), float(coef), self._dev(g, x.numel()), _ptr(out))
+        return float(out[0])
+
+    def add_product(self, g, a, b=None):
+        n = g.numel()
+        self._call("stlp_terms_add_product", self._dev(g), self._dev(a, n), 0 if b is None else self._dev(b, n), n)
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.stlp_terms_free(self._handle)
+            self._handle = None
+
+    __del__ = close

@@ -133,3 +133,14 @@ print('NCOEFF', e.ncoeff)
 """
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
     assert "NCOEFF 762" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.parametrize("config,message", [
+    ({"rows": 2, "len": 100, "depth": 2}, "aligned"),
+    ({"rows": 1, "len": 64, "depth": 31}, "depth"),
+])
+def test_terms_configuration_errors(stl, config, message):
+    """stlp_terms_new validates its sizes before it touches a device."""
+    lib = stl.lib()
+    assert not lib.stlp_terms_new(json.dumps(config).encode())
+    assert message in lib.stlp_last_error().decode()
