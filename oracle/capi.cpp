@@ -1,5 +1,6 @@
 // C entry points of the oracle, for ctypes (oracle/oracle.py).
 // TEST INFRASTRUCTURE ONLY: the engine never links this library.
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -84,6 +85,33 @@ int or_bind(const i64* grid, i64 ngrid, i64 nside, int ksz, int G, int gauge, do
             pos[dst] = b.pos[src];
             w[dst] = b.w[src];
           }
+    }
+    return 0;
+  })
+}
+
+// The sorted distinct cells of nonzero weight each row reads, bound on the
+// whole sky (conv.rs rows_eps with every cell present): out [nrows][width]
+// padded with -1, counts [nrows]; -1 when a row has more than width cells.
+int or_row_cells(const i64* rows, i64 nrows, i64 nside, int ksz, int G, int gauge, i64* out, i64 width,
+                 i64* counts) {
+  GUARD(-1, {
+    Bound b;
+    bind_rows(nullptr, 12 * nside * nside, rows, nrows, nside, ksz, G, (Gauge)gauge, 0.0, b);
+    const int P = ksz * ksz;
+    for (i64 k = 0; k < nrows; ++k) {
+      std::vector<i64> c;
+      for (int g = 0; g < G; ++g)
+        for (int p = 0; p < P; ++p)
+          for (int n = 0; n < 4; ++n) {
+            const size_t e = (((size_t)k * G + g) * P + p) * 4 + n;
+            if (b.w[e] != 0.0) c.push_back(b.pos[e]);
+          }
+      std::sort(c.begin(), c.end());
+      c.erase(std::unique(c.begin(), c.end()), c.end());
+      if ((i64)c.size() > width) throw std::runtime_error("a row reads more cells than the width");
+      counts[k] = (i64)c.size();
+      for (i64 j = 0; j < width; ++j) out[k * width + j] = j < (i64)c.size() ? c[j] : -1;
     }
     return 0;
   })

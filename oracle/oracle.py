@@ -53,6 +53,8 @@ def lib():
             "or_kernel_grid": ([C.c_int, C.c_int64, _D], None),
             "or_wavelet_weights": ([C.c_int, _D], None),
             "or_bind": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, _I64, _D, _U8], C.c_int),
+            "or_row_cells": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, _I64, C.c_int64, _I64],
+                             C.c_int),
             "or_conv_forward": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, C.c_int64, _D], C.c_int),
             "or_conv_adjoint": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, C.c_int64, _D], C.c_int),
             "or_kth_neighbourhood": ([C.c_int64, C.c_int64, C.c_int, _I64], C.c_int64),
@@ -165,6 +167,17 @@ def bind(grid, nside, ksz, G, gauge="cosmo", eps=0.0):
     complete = np.empty(K, np.uint8)
     _check(lib().or_bind(_p(grid, _I64), K, nside, ksz, G, GAUGES[gauge], eps, _p(pos, _I64), _p(w), _p(complete, _U8)))
     return pos, w, complete.astype(bool)
+
+
+def row_cells(rows, nside, ksz=5, G=4, gauge="cosmo", width=128):
+    """[len(rows), width] int64: the sorted distinct cells of nonzero weight each
+    row reads in its bound stencils on the whole sky (padded with -1)."""
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    out = np.empty((rows.size, width), np.int64)
+    counts = np.empty(rows.size, np.int64)
+    _check(lib().or_row_cells(_p(rows, _I64), rows.size, nside, ksz, G, GAUGES[gauge], _p(out, _I64), width,
+                              _p(counts, _I64)))
+    return out[:, : max(int(counts.max()) if counts.size else 0, 1)]
 
 
 def _weights(weights, ksz):

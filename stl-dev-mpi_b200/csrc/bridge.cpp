@@ -198,7 +198,8 @@ char* stlp_info(StlpHandle* h) {
     for (size_t i = 0; i < ol.size(); ++i)
       js << (i ? ", " : "") << "{\"slots\": " << ol[i][0] << ", \"tile_cells\": " << ol[i][1]
          << ", \"coloured\": " << (ol[i][2] == 1 ? "true" : "false") << ", \"layout\": \""
-         << (ol[i][2] == 2 ? "tensor_cores" : ol[i][2] == 1 ? "coloured" : "rows") << "\"}";
+         << (ol[i][2] == 2 ? "tensor_cores" : ol[i][2] == 1 ? "coloured" : "rows") << "\", \"warp_cells\": "
+         << ol[i][3] << "}";
     js << "], \"tile_heights\": [";
     auto th = e.tile_heights();
     for (size_t i = 0; i < th.size(); ++i) {
@@ -235,6 +236,24 @@ int stlp_native_pixels(StlpHandle* h, size_t* out) {
       for (size_t i = 0; i < plan.size(); ++i)
         out[k * plan.size() + i] = (size_t)(h->engine->nmasks() ? h->engine->mask_count(k, plan[i].native)
                                                                : h->engine->npix(plan[i].native));
+    return 0;
+  });
+}
+
+int stlp_operator_rows(StlpHandle* h, size_t level, int kind, int64_t* out, size_t width, size_t* needed) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && needed != nullptr, "null argument");
+    std::vector<int64_t> rows;
+    int w = 0;
+    h->engine->operator_rows((int)level, kind, rows, w);
+    *needed = (size_t)w;
+    if (out && width >= (size_t)w && w > 0) {
+      const size_t n = rows.size() / (size_t)w;
+      for (size_t r = 0; r < n; ++r) {
+        std::copy(rows.begin() + r * w, rows.begin() + (r + 1) * w, out + r * width);
+        std::fill(out + r * width + w, out + (r + 1) * width, (int64_t)-1);
+      }
+    }
     return 0;
   });
 }

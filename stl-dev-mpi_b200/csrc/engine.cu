@@ -16,6 +16,7 @@
 // the next level's map cotangent is the map cotangent of level n
 // (map_cotangent, engine.rs:757-779).
 #include <algorithm>
+#include <type_traits>
 #include <chrono>
 #include <condition_variable>
 #include <thread>
@@ -978,10 +979,93 @@ class EngineImpl final : public Engine {
     return v;
   }
   std::vector<std::array<int, 8>> tile_heights() const override { return tiles_; }
-  std::vector<std::array<int, 3>> operator_layout() const override {
-    std::vector<std::array<int, 3>> v;
+  void operator_rows(int level, int kind, std::vector<int64_t>& out, int& width) override {
+    prepare();
+    if (grid_mode()) throw std::runtime_error("operator tables are exported for full-sky engines");
+    if (level < 0 || level >= levels_ || kind < 0 || kind > 1 || (kind == 1 && level + 1 >= levels_))
+      throw std::runtime_error("no such operator");
+    cudaStream_t s = stream_;
+    auto fetch = [&](const DevMem& m, auto* tag) {
+      using V = std::remove_pointer_t<decltype(tag)>;
+      std::vector<V> h(m.bytes / sizeof(V));
+      if (m.bytes) STL_CUDA(cudaMemcpyAsync(h.data(), m.p, m.bytes, cudaMemcpyDeviceToHost, s));
+      return h;
+    };
+    auto rotp = [](i64 u, int k, int o2) {
+      return ((4 * (u >> o2) + k) << o2) | (u & ((i64(1) << o2) - 1));
+    };
+    auto rotc = [](i64 c, int k, int o2) {
+      const i64 f = c >> o2;
+      return (((f & ~i64(3)) | ((f + k) & 3)) << o2) | (c & ((i64(1) << o2) - 1));
+    };
+    std::vector<std::vector<int64_t>> rows;  // per stored row
+    int nk = 1, o2_row = 0, o2_cell = 0;
+    if (kind == 0) {
+      const ConvOp& op = conv_[level];
+      nk = op.nk; o2_row = o2_cell = op.o2;
+      rows.resize(op.n_rep);
+      if (op.mma) {
+        auto lc = fetch(op.m_lc, (uint16_t*)nullptr);
+        auto cells = fetch(op.m_cells, (int32_t*)nullptr);
+        auto rch = fetch(op.m_rowch, (uint8_t*)nullptr);
+        STL_CUDA(cudaStreamSynchronize(s));
+        for (i64 u = 0; u < op.n_rep; ++u) {
+          const i64 tile = u / kMmaRows, ul = u % kMmaRows;
+          for (int c = 0; c < rch[u]; ++c)
+            for (int p = 0; p < 8; ++p) {
+              const int pl = lc[((tile * (op.m_S / 8) + c) * kMmaRows + ul) * 8 + p];
+              const int32_t cell = cells[tile * op.m_pc + pl];
+              if (cell >= 0) rows[u].push_back(cell);
+            }
+        }
+      } else {
+        auto cell = fetch(op.cell, (int32_t*)nullptr);
+        STL_CUDA(cudaStreamSynchronize(s));
+        for (i64 u = 0; u < op.n_rep; ++u)
+          for (int sl = 0; sl < op.S; ++sl) rows[u].push_back(cell[(i64)sl * op.n_rep + u]);
+      }
+    } else {
+      const DecOp& op = dec_[level];
+      nk = op.nk; o2_row = op.co2; o2_cell = op.o2;
+      rows.resize(op.n_rep_out);
+      auto col = fetch(op.col, (int32_t*)nullptr);
+      std::vector<double> w(col.size());
+      if (op.dtype == DType::F64) {
+        auto wd = fetch(op.w, (double*)nullptr);
+        STL_CUDA(cudaStreamSynchronize(s));
+        w.assign(wd.begin(), wd.end());
+      } else {
+        auto wf = fetch(op.w, (float*)nullptr);
+        STL_CUDA(cudaStreamSynchronize(s));
+        w.assign(wf.begin(), wf.end());
+      }
+      for (i64 u = 0; u < op.n_rep_out; ++u)
+        for (int e = 0; e < op.W; ++e)
+          if (w[(i64)e * op.n_rep_out + u] != 0.0) rows[u].push_back(col[(i64)e * op.n_rep_out + u]);
+    }
+    width = 0;
+    for (auto& r : rows) {
+      std::sort(r.begin(), r.end());
+      r.erase(std::unique(r.begin(), r.end()), r.end());
+      width = std::max(width, (int)r.size());
+    }
+    const i64 npx = (i64)rows.size() * nk;
+    out.assign((size_t)npx * width, -1);
+    for (i64 u = 0; u < (i64)rows.size(); ++u)
+      for (int k = 0; k < nk; ++k) {
+        const i64 p = nk == 4 ? rotp(u, k, o2_row) : u;
+        std::vector<int64_t> r;
+        for (int64_t c : rows[u]) r.push_back(nk == 4 ? rotc(c, k, o2_cell) : c);
+        std::sort(r.begin(), r.end());
+        std::copy(r.begin(), r.end(), out.begin() + (size_t)p * width);
+      }
+  }
+
+  std::vector<std::array<int, 4>> operator_layout() const override {
+    std::vector<std::array<int, 4>> v;
     for (const auto& c : conv_)
-      v.push_back({c.mma ? c.m_S : c.S, c.mma ? c.m_pc : c.max_tile_cells, c.mma ? 2 : c.colored ? 1 : 0});
+      v.push_back({c.mma ? c.m_S : c.S, c.mma ? c.m_pc : c.max_tile_cells, c.mma ? 2 : c.colored ? 1 : 0,
+                   c.mma ? c.m_wl : 0});
     return v;
   }
 

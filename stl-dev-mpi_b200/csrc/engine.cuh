@@ -178,7 +178,7 @@ struct ConvOp {
   int m_wl = 0;              // stride of a warp's private sums (cells; 4 mod 8)
   DevMem m_coef;             // float [m_S][n_rep][8]
   DevMem m_cells;            // int32 [m_tiles][m_pc]: plane cell ids (-1: none)
-  DevMem m_lc;               // uint16 [m_tiles][m_S][kMmaRows]: plane cell of every (slot, row)
+  DevMem m_lc;               // uint16 [m_tiles][m_S / 8][kMmaRows][8]: plane cell of every (row, slot)
   DevMem m_wlc;              // uint8 [m_tiles][m_S / 8][kMmaRows][8]: warp-local cell of every (row, slot)
   DevMem m_winv;             // uint8 [m_tiles][kMmaRows / kMmaWarpRows][m_pc]: warp-local cell of each plane cell (255: none)
   DevMem m_rowch;            // uint8 [n_rep]: chunks of every row
@@ -191,7 +191,7 @@ struct ConvOp {
   }
 };
 constexpr int kMmaRows = 64;      // stored rows per tile of the tensor-core layout
-constexpr int kMmaWarpRows = 8;   // rows per warp (one block of private adjoint sums)
+constexpr int kMmaWarpRows = 16;  // rows per warp of the adjoint (one block of private sums)
 constexpr int kMmaPlaneMax = 1024;  // plane cells a tile may index
 constexpr int kMmaWarpMax = 252;    // warp-local cells (uint8 indices, 255: none)
 // class of the cell at position p of a chunk: every class twice, positions

@@ -781,7 +781,7 @@ __global__ void __launch_bounds__(256) k_mma_layout(MmaArgs a, int pass, int P2)
           pl = 4 * mc + q;
           wl = 4 * mcw + q;
         }
-        a.m_lc[((i64)tile * a.Sm + ns) * kMmaRows + ul] = (uint16_t)pl;
+        a.m_lc[(((i64)tile * (a.Sm / 8) + (ns >> 3)) * kMmaRows + ul) * 8 + (ns & 7)] = (uint16_t)pl;
         a.m_wlc[(((i64)tile * (a.Sm / 8) + (ns >> 3)) * kMmaRows + ul) * 8 + (ns & 7)] = (uint8_t)wl;
       }
     }

@@ -852,8 +852,12 @@ __device__ __forceinline__ void mma3(float d[4], const uint32_t ah[4], const uin
   mma_tf32(d, ah, bh);
 }
 
-constexpr int kMmaWarps = kMmaRows / kMmaWarpRows;
-constexpr int kMmaThreads = 32 * kMmaWarps;
+constexpr int kMmaStages = 4;      // bulk-copy stages of the coefficient stream
+constexpr int kMmaFwdWarpRows = 8;     // rows per warp of the forward
+constexpr int kMmaFwdWarps = kMmaRows / kMmaFwdWarpRows;
+constexpr int kMmaFwdThreads = 32 * kMmaFwdWarps;
+constexpr int kMmaAdjWarps = kMmaRows / kMmaWarpRows;
+constexpr int kMmaAdjThreads = 32 * kMmaAdjWarps;
 // floats per staged slot (kMmaRows rows of 8 coefficients, then padding):
 // slot stride 8 (forward) or 4 (adjoint) banks mod 32, so the B fragments'
 // 32 words fall in distinct banks
@@ -868,7 +872,7 @@ constexpr size_t kMmaAdjStage = 8 * kMmaAdjSlot * sizeof(float) + 8 * kMmaRows;
 // coefficients and plane cells of every row arrive by bulk copies (two
 // stages); every row's accumulators live in registers across the chunks.
 template <int MT>
-__global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
+__global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
     const uint16_t* __restrict__ m_lc, const float* __restrict__ coef, int Sm, i64 n_rep, int o2,
     const int32_t* __restrict__ cells, int pcs, const int32_t* __restrict__ tch, const uint8_t* __restrict__ rowch,
     const float* __restrict__ x, int R, float* __restrict__ out, float* __restrict__ mod, int mod_pix, int mod_row,
@@ -876,9 +880,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
   constexpr int RM = 4 * MT;
   constexpr size_t kCoefBytes = 8 * kMmaFwdSlot * sizeof(float);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar[kMmaStages];
   __shared__ int fail;
-  float* plane = reinterpret_cast<float*>(smem_raw + 2 * kMmaFwdStage);
+  float* plane = reinterpret_cast<float*>(smem_raw + kMmaStages * kMmaFwdStage);
   const int ngroups = (R + RM - 1) / RM;
   const i64 tile = blockIdx.x / ngroups;
   const int r0 = (int)(blockIdx.x % ngroups) * RM;
@@ -888,15 +892,14 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
   const int rows = (int)min((i64)kMmaRows, n_rep - u0);
   const int nch = tch[tile];
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int b = 0; b < kMmaStages; ++b) mbar_init(&bar[b], 1);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int c) {
-    const int st = c & 1;
+    const int st = c % kMmaStages;
     unsigned char* base = smem_raw + st * kMmaFwdStage;
     const unsigned cb = (unsigned)(rows * 8 * sizeof(float));
     const unsigned lb = (unsigned)(8 * kMmaRows * sizeof(uint16_t));
@@ -904,19 +907,17 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
     for (int sl = 0; sl < 8; ++sl)
       bulk_g2s(base + (size_t)sl * kMmaFwdSlot * sizeof(float), coef + ((i64)(8 * c + sl) * n_rep + u0) * 8, cb,
                &bar[st]);
-    bulk_g2s(base + kCoefBytes, m_lc + ((i64)tile * Sm + 8 * c) * kMmaRows, lb, &bar[st]);
+    bulk_g2s(base + kCoefBytes, m_lc + ((i64)tile * (Sm / 8) + c) * kMmaRows * 8, lb, &bar[st]);
   };
-  if (tid == 0) {
-    if (nch > 0) issue(0);
-    if (nch > 1) issue(1);
-  }
+  if (tid == 0)
+    for (int c = 0; c < min(nch, kMmaStages); ++c) issue(c);
   // the plane: per tile cell and rotation, the CTA's RM input rows, by
   // asynchronous 16-byte copies (all in flight at once; a hole or a missing
   // cell copies zero bytes, which fills zeros); rows past R (R % 4 != 0)
   // by plain loads
   const int32_t* tc = cells + tile * pcs;
   const bool whole = R % 4 == 0;
-  for (int pl = tid; pl < pcs; pl += kMmaThreads) {
+  for (int pl = tid; pl < pcs; pl += kMmaFwdThreads) {
     const int32_t cl = tc[pl];
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
@@ -932,15 +933,15 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
     }
   }
   cp_async_wait_all();  // this thread's copies; the barrier before the first chunk publishes them
-  int rch[kMmaWarpRows];
+  int rch[kMmaFwdWarpRows];
 #pragma unroll
-  for (int i = 0; i < kMmaWarpRows; ++i) {
-    const int ul = warp * kMmaWarpRows + i;
+  for (int i = 0; i < kMmaFwdWarpRows; ++i) {
+    const int ul = warp * kMmaFwdWarpRows + i;
     rch[i] = ul < rows ? (int)rowch[u0 + ul] : 0;
   }
-  float acc[kMmaWarpRows][MT][4];
+  float acc[kMmaFwdWarpRows][MT][4];
 #pragma unroll
-  for (int i = 0; i < kMmaWarpRows; ++i)
+  for (int i = 0; i < kMmaFwdWarpRows; ++i)
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
@@ -948,18 +949,18 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
   const float* pk = plane + (size_t)k * pcs * RM + rq * 2 * MT;
   int c = 0;
   for (; c < nch; ++c) {
-    const int st = c & 1;
-    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    const int st = c % kMmaStages;
+    if (!mbar_wait(&bar[st], (c / kMmaStages) & 1)) fail = 1;
     __syncthreads();  // also orders the plane gather before the first chunk
     if (fail) break;
     const unsigned char* base = smem_raw + st * kMmaFwdStage;
     const float* cs = reinterpret_cast<const float*>(base);
     const uint16_t* ls = reinterpret_cast<const uint16_t*>(base + kCoefBytes);
 #pragma unroll
-    for (int i = 0; i < kMmaWarpRows; ++i) {
+    for (int i = 0; i < kMmaFwdWarpRows; ++i) {
       if (c >= rch[i]) continue;  // warp-uniform: the row has no more chunks
-      const int ul = warp * kMmaWarpRows + i;
-      const int lc0 = ls[t * kMmaRows + ul], lc1 = ls[(t + 4) * kMmaRows + ul];
+      const int ul = warp * kMmaFwdWarpRows + i;
+      const int lc0 = ls[ul * 8 + t], lc1 = ls[ul * 8 + t + 4];
       uint32_t bh[2], bl[2];
       split_tf32(cs[t * kMmaFwdSlot + ul * 8 + g], bh[0], bl[0]);
       split_tf32(cs[(t + 4) * kMmaFwdSlot + ul * 8 + g], bh[1], bl[1]);
@@ -989,11 +990,12 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
       }
     }
     __syncthreads();  // the stage is read: refill it
-    if (tid == 0 && c + 2 < nch) issue(c + 2);
+    if (tid == 0 && c + kMmaStages < nch) issue(c + kMmaStages);
   }
   if (fail) {
     bool drained = true;
-    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    for (int q = c; q < min(nch, c + kMmaStages); ++q)
+      drained &= mbar_wait(&bar[q % kMmaStages], (q / kMmaStages) & 1);
     if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
     return;
   }
@@ -1001,8 +1003,8 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
   const int go = odd ? (t ^ 2) : t;  // output gauge of stored gauge t under rotation k
   const bool cj = rot_conj(k, go);
 #pragma unroll
-  for (int i = 0; i < kMmaWarpRows; ++i) {
-    const int ul = warp * kMmaWarpRows + i;
+  for (int i = 0; i < kMmaFwdWarpRows; ++i) {
+    const int ul = warp * kMmaFwdWarpRows + i;
     if (ul >= rows) continue;
     const i64 u = u0 + ul;
     const i64 p = rot_pixel(u, k, o2);
@@ -1030,24 +1032,26 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_fwd_mma(
   }
 }
 
-// Adjoint: one CTA per (tile, 4 cotangent rows); warp w adds the products
-// of its rows into private sums [4 k][wls][4 r] over the distinct cells of
-// its rows (warp-local numbering), so no other warp touches them and no
-// barrier separates the slots; per chunk and row one mma gives the 16 x 8
-// products (rotation and row) x (slot) of the row's cotangents with its
-// coefficients.  Then every tile cell's partial is the sum over the warps,
-// in warp order, written to part[tile][k][pcs][R].  madd: the modulus VJP
-// added to the cotangents first, as k_conv_adj_colored.
-__global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
+// Adjoint: one CTA per (tile, 4 cotangent rows), warp w the rows 16 w ..
+// 16 w + 15 of the tile.  Warp w adds the products of its rows into
+// private sums [4 k][wls][4 r] over the distinct cells of its rows
+// (warp-local numbering), so no other warp touches them and no barrier
+// separates the slots; per chunk and row one mma gives the 16 x 8 products
+// (rotation and row) x (slot) of the row's cotangents with its
+// coefficients.  The coefficients and warp-local cells stream through
+// kMmaStages bulk-copy stages.  Then every tile cell's partial is the sum
+// over the warps, in warp order, written to part[tile][k][pcs][R].  madd:
+// the modulus VJP added to the cotangents first, as k_conv_adj_colored.
+__global__ void __launch_bounds__(kMmaAdjThreads, 2) k_conv_adj_mma(
     const uint8_t* __restrict__ m_wlc, const float* __restrict__ coef, int Sm, i64 n_rep, int o2,
     const int32_t* __restrict__ tch, const uint8_t* __restrict__ rowch, const uint8_t* __restrict__ m_winv, int pcs,
     int wls, const float* __restrict__ gy, int R, float* __restrict__ part, int* __restrict__ err,
     ModulusAdd<float> madd) {
   constexpr size_t kCoefBytes = 8 * kMmaAdjSlot * sizeof(float);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar[kMmaStages];
   __shared__ int fail;
-  float* sums = reinterpret_cast<float*>(smem_raw + 2 * kMmaAdjStage);  // [warps][4][wls][4]
+  float* sums = reinterpret_cast<float*>(smem_raw + kMmaStages * kMmaAdjStage);  // [warps][4][wls][4]
   const int ngroups = (R + 3) / 4;  // rows past R (the last group of R % 4 != 0) are zero
   const i64 tile = blockIdx.x / ngroups;
   const int r0 = (int)(blockIdx.x % ngroups) * 4;
@@ -1057,15 +1061,14 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
   const int rows = (int)min((i64)kMmaRows, n_rep - u0);
   const int nch = tch[tile];
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int b = 0; b < kMmaStages; ++b) mbar_init(&bar[b], 1);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int c) {
-    const int st = c & 1;
+    const int st = c % kMmaStages;
     unsigned char* base = smem_raw + st * kMmaAdjStage;
     const unsigned cb = (unsigned)(rows * 8 * sizeof(float));
     const unsigned wb = (unsigned)(8 * kMmaRows);
@@ -1075,14 +1078,12 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
                &bar[st]);
     bulk_g2s(base + kCoefBytes, m_wlc + ((i64)tile * (Sm / 8) + c) * kMmaRows * 8, wb, &bar[st]);
   };
-  if (tid == 0) {
-    if (nch > 0) issue(0);
-    if (nch > 1) issue(1);
-  }
+  if (tid == 0)
+    for (int c = 0; c < min(nch, kMmaStages); ++c) issue(c);
   float* mine = sums + (size_t)warp * 16 * wls;
   for (int i = lane; i < 16 * wls; i += 32) mine[i] = 0.0f;
   // the rows' cotangents under rotation k (gauge permutation, conjugation
-  // and the modulus VJP folded in) as split A fragments
+  // and the modulus VJP folded in), as A fragments split per chunk
   const bool odd = k & 1;
   auto cot = [&](i64 p, int rr, int o) {
     if (r0 + rr >= R) return 0.0f;
@@ -1099,28 +1100,26 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
     }
     return (pt && rot_conj(k, gg)) ? -v : v;
   };
-  uint32_t ah[kMmaWarpRows][4], al[kMmaWarpRows][4];
+  float av[kMmaWarpRows][4];
   int rch[kMmaWarpRows];
 #pragma unroll
   for (int i = 0; i < kMmaWarpRows; ++i) {
     const int ul = warp * kMmaWarpRows + i;
     rch[i] = ul < rows ? (int)rowch[u0 + ul] : 0;
-    float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    av[i][0] = av[i][1] = av[i][2] = av[i][3] = 0.0f;
     if (ul < rows) {
       const i64 p = rot_pixel(u0 + ul, k, o2);
-      a[0] = cot(p, 2 * rp, t);
-      a[1] = cot(p, 2 * rp + 1, t);
-      a[2] = cot(p, 2 * rp, t + 4);
-      a[3] = cot(p, 2 * rp + 1, t + 4);
+      av[i][0] = cot(p, 2 * rp, t);
+      av[i][1] = cot(p, 2 * rp + 1, t);
+      av[i][2] = cot(p, 2 * rp, t + 4);
+      av[i][3] = cot(p, 2 * rp + 1, t + 4);
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) split_tf32(a[q], ah[i][q], al[i][q]);
   }
   float* mk = mine + (size_t)k * wls * 4 + 2 * rp;
   int c = 0;
   for (; c < nch; ++c) {
-    const int st = c & 1;
-    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
+    const int st = c % kMmaStages;
+    if (!mbar_wait(&bar[st], (c / kMmaStages) & 1)) fail = 1;
     __syncthreads();  // also orders the zeroed sums before the first chunk
     if (fail) break;
     const unsigned char* base = smem_raw + st * kMmaAdjStage;
@@ -1130,11 +1129,13 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
     for (int i = 0; i < kMmaWarpRows; ++i) {
       if (c >= rch[i]) continue;  // warp-uniform
       const int ul = warp * kMmaWarpRows + i;
-      uint32_t bh[2], bl[2];
+      uint32_t ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) split_tf32(av[i][q], ah[q], al[q]);
       split_tf32(cs[g * kMmaAdjSlot + ul * 8 + t], bh[0], bl[0]);
       split_tf32(cs[g * kMmaAdjSlot + ul * 8 + t + 4], bh[1], bl[1]);
       float d[4];
-      mma3(d, ah[i], al[i], bh, bl);
+      mma3(d, ah, al, bh, bl);
       const uint16_t wp = *reinterpret_cast<const uint16_t*>(ws + ul * 8 + 2 * t);
       float2* s0 = reinterpret_cast<float2*>(mk + (size_t)(wp & 0xff) * 4);
       float2* s1 = reinterpret_cast<float2*>(mk + (size_t)(wp >> 8) * 4);
@@ -1148,23 +1149,24 @@ __global__ void __launch_bounds__(kMmaThreads, 2) k_conv_adj_mma(
       // the compiler keeps the order (the addresses may alias)
     }
     __syncthreads();  // the stage is read: refill it
-    if (tid == 0 && c + 2 < nch) issue(c + 2);
+    if (tid == 0 && c + kMmaStages < nch) issue(c + kMmaStages);
   }
   if (fail) {
     bool drained = true;
-    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    for (int q = c; q < min(nch, c + kMmaStages); ++q)
+      drained &= mbar_wait(&bar[q % kMmaStages], (q / kMmaStages) & 1);
     if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
     return;
   }
   __syncthreads();  // every warp's sums are complete (also when the tile has no chunk)
   // tile partials: per plane cell, for every (k, r), the warps' sums in warp order
-  const uint8_t* winv = m_winv + tile * kMmaWarps * pcs;
-  for (int pl = tid; pl < pcs; pl += kMmaThreads) {
+  const uint8_t* winv = m_winv + tile * kMmaAdjWarps * pcs;
+  for (int pl = tid; pl < pcs; pl += kMmaAdjThreads) {
     float4 v[4];
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) v[kk] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
-    for (int w = 0; w < kMmaWarps; ++w) {
+    for (int w = 0; w < kMmaAdjWarps; ++w) {
       const int wl = winv[w * pcs + pl];
       if (wl == 255) continue;
 #pragma unroll
@@ -2136,15 +2138,19 @@ void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x
 }
 
 // tensor-core launches (FP32 operators in the tensor-core layout)
-inline size_t fwd_mma_smem(const ConvOp& op, int MT) { return 2 * kMmaFwdStage + sizeof(float) * 4 * op.m_pc * 4 * MT; }
-inline size_t adj_mma_smem(const ConvOp& op) { return 2 * kMmaAdjStage + sizeof(float) * kMmaWarps * 16 * op.m_wl; }
+inline size_t fwd_mma_smem(const ConvOp& op, int MT) {
+  return kMmaStages * kMmaFwdStage + sizeof(float) * 4 * op.m_pc * 4 * MT;
+}
+inline size_t adj_mma_smem(const ConvOp& op) {
+  return kMmaStages * kMmaAdjStage + sizeof(float) * kMmaAdjWarps * 16 * op.m_wl;
+}
 
 template <int MT>
 void conv_forward_mma_mt(const ConvOp& op, const float* x, int R, float* out, float* mod, int mod_pix, int mod_row,
                          int mod_off, int* err, const double* rc, cudaStream_t s) {
   allow_dynamic_smem(k_conv_fwd_mma<MT>);
   dim3 grid((unsigned)(op.m_tiles * ((R + 4 * MT - 1) / (4 * MT))));
-  k_conv_fwd_mma<MT><<<grid, kMmaThreads, fwd_mma_smem(op, MT), s>>>(
+  k_conv_fwd_mma<MT><<<grid, kMmaFwdThreads, fwd_mma_smem(op, MT), s>>>(
       op.m_lc.as<uint16_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_cells.as<int32_t>(), op.m_pc,
       op.m_tch.as<int32_t>(), op.m_rowch.as<uint8_t>(), x, R, out, mod, mod_pix, mod_row, mod_off, err,
       op.rowsum.as<float>(), rc);
@@ -2154,7 +2160,7 @@ void conv_adjoint_mma(const ConvOp& op, const float* gy, int R, float* gx, bool 
                       cudaStream_t s, int* err, const ModulusAdd<float>* madd) {
   allow_dynamic_smem(k_conv_adj_mma);
   dim3 grid((unsigned)(op.m_tiles * ((R + 3) / 4)));
-  k_conv_adj_mma<<<grid, kMmaThreads, adj_mma_smem(op), s>>>(
+  k_conv_adj_mma<<<grid, kMmaAdjThreads, adj_mma_smem(op), s>>>(
       op.m_wlc.as<uint8_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_tch.as<int32_t>(),
       op.m_rowch.as<uint8_t>(), op.m_winv.as<uint8_t>(), op.m_pc, op.m_wl, gy, R, static_cast<float*>(scr.part), err,
       madd ? *madd : ModulusAdd<float>());

@@ -162,7 +162,13 @@ class Engine {
   // Mean cells read per row of each level's wavelet operator.
   virtual std::vector<double> mean_slots() const = 0;
   // Per level: slots per stored row, most cells of a tile, coloured layout (0/1).
-  virtual std::vector<std::array<int, 3>> operator_layout() const = 0;
+  virtual std::vector<std::array<int, 4>> operator_layout() const = 0;
+  // The integer tables of the operators, for exact checks: kind 0, the
+  // sorted distinct input cells of every output pixel of level `level`'s
+  // wavelet; kind 1, the sorted fine cells of nonzero weight of every coarse
+  // pixel of the decimation from level `level` to `level` + 1.  Rows of the
+  // full level in pixel order, padded with -1 to the widest (width).
+  virtual void operator_rows(int level, int kind, std::vector<int64_t>& out, int& width) = 0;
   // Per level, the tile heights (rows of the field a thread takes) chosen
   // for: the wavelet of the maps, of the moduli, their adjoints, the
   // decimation of the maps (to the next level), of the moduli (from the

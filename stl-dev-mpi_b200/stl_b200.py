@@ -87,6 +87,7 @@ def lib():
             "stlp_patch_vjp": ([_VOID, _D, sz, u64, _D], C.c_int),
             "stlp_patch_forward_device": ([_VOID, u64, sz, u64, b, _D, _D], C.c_int),
             "stlp_patch_vjp_device": ([_VOID, _D, sz, u64, u64], C.c_int),
+            "stlp_operator_rows": ([_VOID, sz, C.c_int, C.POINTER(C.c_int64), sz, _SIZE], C.c_int),
             "stlp_terms_new": ([C.c_char_p], _VOID),
             "stlp_terms_free": ([_VOID], None),
             "stlp_terms_set_stream": ([_VOID, u64], C.c_int),
@@ -261,6 +262,24 @@ class NativeEngine:
             if self._lib.stlp_forward_levels(self._handle, _ptr(x), x.size, _ptr(values.view(np.float64))):
                 raise _error()
             return values
+
+    def operator_rows(self, level, kind="wavelet"):
+        """Integer tables of the device operators, [pixels, width] int64 padded
+        with -1, rows in pixel order: "wavelet", the sorted input cells each
+        pixel of `level` reads; "decimation", the fine cells of nonzero weight
+        of each coarse pixel of level + 1."""
+        k = {"wavelet": 0, "decimation": 1}[kind]
+        with self._mutex:
+            self._open()
+            need = C.c_size_t(0)
+            if self._lib.stlp_operator_rows(self._handle, int(level), k, None, 0, C.byref(need)):
+                raise _error()
+            rows = 12 * (self.nside >> (level + k)) ** 2
+            out = np.empty((rows, need.value), dtype=np.int64)
+            if self._lib.stlp_operator_rows(self._handle, int(level), k, out.ctypes.data_as(C.POINTER(C.c_int64)),
+                                            need.value, C.byref(need)):
+                raise _error()
+            return out
 
     def set_masks(self, masks):
         """Averages every coefficient over each of K masks from the next forward
