@@ -161,6 +161,12 @@ int stlp_patch_forward_device(StlpPatchHandle* h, uint64_t x, size_t n, uint64_t
                               double* out, double* var);
 int stlp_patch_vjp_device(StlpPatchHandle* h, const double* cot, size_t n, uint64_t generation, uint64_t out);
 
+/* Device memory the library holds for all handles of the process: the live
+ * bytes and their high-water mark; reset_peak != 0 first restarts the mark
+ * at the live bytes.  No reference counterpart (the reference reports its
+ * engine's memory in stlp_info, lib.rs:365-391, as stlp_info does here). */
+int stlp_memory(size_t* live, size_t* peak, int reset_peak);
+
 /* The integer tables of the engine's operators, for exact checks: kind 0
  * the sorted distinct input cells (full-sky NESTED ids) each output pixel
  * of level `level` reads in its wavelet, kind 1 the sorted fine cells of

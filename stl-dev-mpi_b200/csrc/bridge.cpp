@@ -120,6 +120,10 @@ StlpHandle* stlp_new(const char* config) {
     o.tensor_cores = v.boolean("tensor_cores", true);
     o.tune_cache = v.string("autotune_cache", "");
     o.cross = v.boolean("cross", false);  // two channels, the plan of their cross terms (lib.rs:238-245)
+    const std::string fields = v.string("fields", "keep");  // lib.rs:273-345: auto | keep | recompute
+    require(fields == "keep" || fields == "recompute" || fields == "auto", "fields must be auto, keep or recompute");
+    o.recompute = fields == "recompute";
+    o.fields_auto = fields == "auto";
     require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
     require(o.nside > 0 && (o.nside & (o.nside - 1)) == 0, "nside must be a power of two");
     auto h = std::make_unique<StlpHandle>();
@@ -179,9 +183,11 @@ char* stlp_info(StlpHandle* h) {
        << ", \"dtype\": " << jstr(o.fp32 ? "float32 fields, float64 sums/complex128" : "float64/complex128")
        << ", \"fewer\": false, \"orientations\": " << o.L << ", \"kernel\": " << o.ksz
        << ", \"levels\": " << e.levels() << ", \"masks\": " << e.nmasks() << ", \"spin\": 0, \"device\": " << o.device
-       << ", \"conv\": \"folded-stencil\", \"fields\": \"keep\"";
+       << ", \"conv\": \"folded-stencil\", \"fields\": "
+       << jstr(e.recomputes() ? "recompute" : "keep");
     js << ", \"device_memory\": {\"operator_bytes\": " << e.operator_bytes() << ", \"field_bytes\": " << e.field_bytes()
-       << ", \"live_bytes\": " << device_bytes_live() << ", \"peak_bytes\": " << device_bytes_peak() << "}";
+       << ", \"live_bytes\": " << device_bytes_live() << ", \"peak_bytes\": " << device_bytes_peak()
+       << ", \"kept_field_bytes\": " << e.kept_field_bytes() << "}";
     js << ", \"timers\": {\"build_s\": " << e.timers.build_s << ", \"forward_ms\": " << e.timers.forward_ms
        << ", \"reverse_ms\": " << e.timers.reverse_ms << ", \"forwards\": " << e.timers.forwards
        << ", \"reverses\": " << e.timers.reverses << "}";
@@ -236,6 +242,15 @@ int stlp_native_pixels(StlpHandle* h, size_t* out) {
       for (size_t i = 0; i < plan.size(); ++i)
         out[k * plan.size() + i] = (size_t)(h->engine->nmasks() ? h->engine->mask_count(k, plan[i].native)
                                                                : h->engine->npix(plan[i].native));
+    return 0;
+  });
+}
+
+int stlp_memory(size_t* live, size_t* peak, int reset_peak) {
+  return guard<int>(-1, [&] {
+    if (reset_peak) device_bytes_reset_peak();
+    if (live) *live = device_bytes_live();
+    if (peak) *peak = device_bytes_peak();
     return 0;
   });
 }

@@ -643,13 +643,36 @@ class EngineImpl final : public Engine {
     gMod_.resize(levels_); gX_.resize(levels_);
     shapes_.resize(levels_);
     size_t max_part = 0, max_gz = 0, max_gbr = 0;
+    // field store: z and the branches of every level kept, or one buffer each
+    // (the largest level's) recomputed per level in the reverse sweep
+    {
+      size_t keep = 0, zmax = 0, bmax = 0;
+      for (int n = 0; n < levels_; ++n) {
+        const size_t e = esz(n), N = (size_t)npix(n);
+        keep += e * 2 * B * L * N + e * 2 * B * (n + 1) * L * L * N;
+        zmax = std::max(zmax, e * 2 * B * L * N);
+        bmax = std::max(bmax, e * 2 * B * (n + 1) * L * L * N);
+      }
+      keep_bytes_ = keep;
+      recompute_ = opt_.recompute;
+      if (opt_.fields_auto) {  // keep them when they fit the free memory with a quarter to spare
+        size_t free_b = 0, total_b = 0;
+        STL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        recompute_ = keep > free_b / 4 * 3;
+      }
+      if (recompute_) {
+        Zs_.alloc(zmax);
+        Brs_.alloc(bmax);
+        field_bytes_ += Zs_.bytes + Brs_.bytes;
+      }
+    }
     for (int n = 0; n < levels_; ++n) {
       i64 N = npix(n);
       const size_t e = esz(n);
       X_[n].alloc(e * B * N + 16);  // padded: the products stage their maps in 16-byte units
-      Z_[n].alloc(e * 2 * B * L * N);
+      if (!recompute_) Z_[n].alloc(e * 2 * B * L * N);
       Mod_[n].alloc(e * B * (n + 1) * L * N);
-      Br_[n].alloc(e * 2 * B * (n + 1) * L * L * N);
+      if (!recompute_) Br_[n].alloc(e * 2 * B * (n + 1) * L * L * N);
       gMod_[n].alloc(e * B * (n + 1) * L * N);
       gX_[n].alloc(e * B * N);
       shapes_[n] = product_shape(n, L, B, N, e);
@@ -896,14 +919,14 @@ class EngineImpl final : public Engine {
     U* mod = Mod_[n].as<U>();
     const ConvOp& op = conv_[n];
     prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, false), conv_flops(op, B), s, [&] {
-      conv_forward<U>(op, X_[n].as<U>(), B, Z_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(),
+      conv_forward<U>(op, X_[n].as<U>(), B, zf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(),
                       xc_.as<double>() + (size_t)n * B, tile(n, T_FWD_Z));
     });
     // |z| as deviations from their means per (map, orientation)
     double* zc = zc_.as<double>() + (size_t)n * B * L;
     prof_.launch(Profiler::ELEM, 3, (double)N * B * L * (2 * 2 * sizeof(U) + sizeof(U)), 0.0, s, [&] {
-      row_means<U>(Z_[n].as<U>(), true, true, N, B * L, mpart_.as<double>(), zc, s);
-      moduli_deviations<U>(Z_[n].as<U>(), N, B, L, zc, mod, B * (n + 1) * L, (n + 1) * L, n * L, s);
+      row_means<U>(zf<U>(n), true, true, N, B * L, mpart_.as<double>(), zc, s);
+      moduli_deviations<U>(zf<U>(n), N, B, L, zc, mod, B * (n + 1) * L, (n + 1) * L, n * L, s);
     });
     if (n > 0)
       prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n - 1], B * n * L, false), dec_flops(dec_[n - 1], B * n * L, false),
@@ -917,7 +940,7 @@ class EngineImpl final : public Engine {
     const int R = B * (n + 1) * L;
     branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s);
     prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
-      conv_forward<U>(op, mod, R, Br_[n].as<U>(), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>(),
+      conv_forward<U>(op, mod, R, brf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>(),
                       tile(n, T_FWD_BR));
     });
     const ProductShape& sh = shapes_[n];
@@ -926,7 +949,7 @@ class EngineImpl final : public Engine {
       for (int k = 0; k < launch_sets(); ++k)
         prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U),
                      (double)vb_ * L * N * sh.K * sh.K * 8.0, s, [&] {
-                       cross_forward<U>(sh.K, N, B, Z_[n].as<U>(), Br_[n].as<U>(), mask(k, n), moments,
+                       cross_forward<U>(sh.K, N, B, zf<U>(n), brf<U>(n), mask(k, n), moments,
                                         partials_.as<double>(), cross_blocks(N),
                                         sums_.as<double>() + k * total_sums_ + sum_off_[n], s);
                      });
@@ -935,7 +958,7 @@ class EngineImpl final : public Engine {
     for (int k = 0; k < launch_sets(); ++k)
       prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
                    [&] {
-                     products_forward<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), n == 0 ? X_[0].as<U>() : nullptr,
+                     products_forward<U>(sh, zf<U>(n), brf<U>(n), n == 0 ? X_[0].as<U>() : nullptr,
                                          xc_.as<double>(), mask(k, n), partials_.as<double>(),
                                          sums_.as<double>() + k * total_sums_ + sum_off_[n], err_.as<int>(), s,
                                          moments);
@@ -1060,6 +1083,9 @@ class EngineImpl final : public Engine {
         std::copy(r.begin(), r.end(), out.begin() + (size_t)p * width);
       }
   }
+
+  bool recomputes() const override { return recompute_; }
+  size_t kept_field_bytes() const override { return keep_bytes_; }
 
   std::vector<std::array<int, 4>> operator_layout() const override {
     std::vector<std::array<int, 4>> v;
@@ -1242,6 +1268,20 @@ class EngineImpl final : public Engine {
                    });
     else
       STL_CUDA(cudaMemsetAsync(gmod, 0, gMod_[n].bytes, s));
+    if (recompute_) {
+      // the level's z and branches again, from the kept maps and stored
+      // moduli (the forward's launches on the same inputs: identical values)
+      const int Rb = B * (n + 1) * L;
+      prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, B, true, false), conv_flops(op, B), s, [&] {
+        conv_forward<U>(op, X_[n].as<U>(), B, zf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(),
+                        xc_.as<double>() + (size_t)n * B, tile(n, T_FWD_Z));
+      });
+      branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s);
+      prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, Rb, true, false), conv_flops(op, Rb), s, [&] {
+        conv_forward<U>(op, Mod_[n].as<U>(), Rb, brf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>(),
+                        tile(n, T_FWD_BR));
+      });
+    }
     // cotangent matrices and S1 scales in the field precision, one set per
     // mask, staged for every level before the sweep; the products VJP of
     // mask k > 0 adds to that of the masks before it
@@ -1252,10 +1292,10 @@ class EngineImpl final : public Engine {
       prof_.launch(Profiler::PROD_REV, 1, (double)B * L * N * sh.K * 4 * sz, (double)B * L * N * sh.K * sh.K * 8.0,
                    s, [&] {
                      if (opt_.cross)
-                       cross_reverse<U>(sh.K, N, B, Z_[n].as<U>(), Br_[n].as<U>(), Mdev, sdev, mask(k, n), k > 0,
+                       cross_reverse<U>(sh.K, N, B, zf<U>(n), brf<U>(n), Mdev, sdev, mask(k, n), k > 0,
                                         gZ_.as<U>(), gBr_.as<U>(), s);
                      else
-                       products_reverse<U>(sh, Z_[n].as<U>(), Br_[n].as<U>(), Mdev, sdev, mask(k, n), k > 0,
+                       products_reverse<U>(sh, zf<U>(n), brf<U>(n), Mdev, sdev, mask(k, n), k > 0,
                                            gZ_.as<U>(), gBr_.as<U>(), s);
                    });
     }
@@ -1269,14 +1309,14 @@ class EngineImpl final : public Engine {
     // the modulus VJP of z (gZ += gmod z / |z|): inside the coloured adjoint
     // of z when the operator has it, else its own pass
     ModulusAdd<U> madd;
-    madd.z = Z_[n].as<U>();
+    madd.z = zf<U>(n);
     madd.g = gmod + n * L;
     madd.g_pix = B * (n + 1) * L;
     madd.g_row = (n + 1) * L;
     const bool fuse = conv_adjoint_fuses_modulus(op, sizeof(U), B, adj_ptr(), err_.as<int>());
     if (!fuse)
       prof_.launch(Profiler::ELEM, 1, (double)B * L * N * 5 * sz, (double)B * L * N * 6.0, s, [&] {
-        modulus_vjp_add<U>(Z_[n].as<U>(), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<U>(), N, B, L, s);
+        modulus_vjp_add<U>(zf<U>(n), gmod + n * L, B * (n + 1) * L, (n + 1) * L, gZ_.as<U>(), N, B, L, s);
       });
     prof_.launch(Profiler::CONV_ADJ, adjoint_tiles_usable(op, sizeof(U), B, adj_ptr()) ? 2 : 1,
                  conv_bytes(op, B, false, false), conv_flops(op, B), s, [&] {
@@ -1411,6 +1451,12 @@ class EngineImpl final : public Engine {
   std::vector<ConvOp> conv_;
   std::vector<DecOp> dec_;
   std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;
+  // recompute field store: the one z and branch buffer of every level
+  bool recompute_ = false;
+  size_t keep_bytes_ = 0;  // z and branches of every level (the kept store)
+  DevMem Zs_, Brs_;
+  template <typename U> U* zf(int n) { return recompute_ ? Zs_.as<U>() : Z_[n].as<U>(); }
+  template <typename U> U* brf(int n) { return recompute_ ? Brs_.as<U>() : Br_[n].as<U>(); }
   std::vector<ProductShape> shapes_;
   std::vector<size_t> sum_off_;
   DevMem partials_, sums_, gZ_, gBr_, mv_, in_f64_, err_, roles_;
@@ -1451,7 +1497,9 @@ class EngineImpl final : public Engine {
     cudaStream_t s = stream_;
     for (int n = 0; n < levels_; ++n)
       for (DevMem* f : {&X_[n], &Z_[n], &Mod_[n], &Br_[n], &gMod_[n], &gX_[n]})
-        STL_CUDA(cudaMemsetAsync(f->p, 0, f->bytes, s));
+        if (f->p) STL_CUDA(cudaMemsetAsync(f->p, 0, f->bytes, s));
+    for (DevMem* f : {&Zs_, &Brs_})
+      if (f->p) STL_CUDA(cudaMemsetAsync(f->p, 0, f->bytes, s));
     STL_CUDA(cudaMemsetAsync(gZ_.p, 0, gZ_.bytes, s));
     STL_CUDA(cudaMemsetAsync(gBr_.p, 0, gBr_.bytes, s));
     for (DevMem* c : {&xc_, &zc_, &rc_}) STL_CUDA(cudaMemsetAsync(c->p, 0, c->bytes, s));
@@ -1508,17 +1556,17 @@ class EngineImpl final : public Engine {
           U* mod = Mod_[n].as<U>();
           U* gmod = gMod_[n].as<U>();
           tiles_[n][T_FWD_Z] = pick("fz", &op, nullptr, B, conv_forward_choices(op, e, B, true), [&](int rb) {
-            conv_forward<U>(op, X_[n].as<U>(), B, Z_[n].as<U>(), nullptr, 0, 0, 0, s, err,
+            conv_forward<U>(op, X_[n].as<U>(), B, zf<U>(n), nullptr, 0, 0, 0, s, err,
                             xc_.as<double>() + (size_t)n * B, rb);
           });
           tiles_[n][T_FWD_BR] = pick("fb", &op, nullptr, R, conv_forward_choices(op, e, R, true), [&](int rb) {
-            conv_forward<U>(op, mod, R, Br_[n].as<U>(), nullptr, 0, 0, 0, s, err, rc_.as<double>(), rb);
+            conv_forward<U>(op, mod, R, brf<U>(n), nullptr, 0, 0, 0, s, err, rc_.as<double>(), rb);
           });
           tiles_[n][T_ADJ_BR] = pick("ab", &op, nullptr, R, conv_adjoint_choices(op, e, R, adj_ptr()), [&](int rb) {
             conv_adjoint<U>(op, gBr_.as<U>(), R, gmod, true, s, adj_ptr(), err, nullptr, rb);
           });
           ModulusAdd<U> madd;
-          madd.z = Z_[n].as<U>();
+          madd.z = zf<U>(n);
           madd.g = gmod + n * L;
           madd.g_pix = B * (n + 1) * L;
           madd.g_row = (n + 1) * L;

@@ -49,6 +49,13 @@ struct Options {
   // root-normalised z, S2, S3 and S4 in both channel orders), maps
   // [B][2][N]; the fields then hold 2 B maps (map 2 b + c).
   bool cross = false;
+  // Field store (the reference's `fields`, crates/stl-gpu/src/engine.rs:
+  // 174-204): keep every level's wavelet outputs z and branches from the
+  // forward for the reverse sweep, or recompute them per level in the
+  // reverse (one buffer of the largest level each; the stored moduli and
+  // the maps of the pyramid stay).  Results are identical either way.
+  bool recompute = false;
+  bool fields_auto = false;  // recompute only when keeping them would not fit the device's free memory
   std::string tune_cache;  // file of tile heights already timed (read, then extended); empty: none
 };
 
@@ -163,6 +170,8 @@ class Engine {
   virtual std::vector<double> mean_slots() const = 0;
   // Per level: slots per stored row, most cells of a tile, coloured layout (0/1).
   virtual std::vector<std::array<int, 4>> operator_layout() const = 0;
+  virtual bool recomputes() const = 0;  // the field store in use (after prepare)
+  virtual size_t kept_field_bytes() const = 0;  // bytes of z and branches of every level (after prepare)
   // The integer tables of the operators, for exact checks: kind 0, the
   // sorted distinct input cells of every output pixel of level `level`'s
   // wavelet; kind 1, the sorted fine cells of nonzero weight of every coarse

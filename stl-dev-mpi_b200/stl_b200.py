@@ -88,6 +88,7 @@ def lib():
             "stlp_patch_forward_device": ([_VOID, u64, sz, u64, b, _D, _D], C.c_int),
             "stlp_patch_vjp_device": ([_VOID, _D, sz, u64, u64], C.c_int),
             "stlp_operator_rows": ([_VOID, sz, C.c_int, C.POINTER(C.c_int64), sz, _SIZE], C.c_int),
+            "stlp_memory": ([_SIZE, _SIZE, C.c_int], C.c_int),
             "stlp_terms_new": ([C.c_char_p], _VOID),
             "stlp_terms_free": ([_VOID], None),
             "stlp_terms_set_stream": ([_VOID, u64], C.c_int),
@@ -107,6 +108,15 @@ def lib():
             f.argtypes, f.restype = args, res
         _lib = l
         return l
+
+
+def device_memory(reset_peak=False):
+    """(live, peak) bytes of device memory the library holds (all engines of the
+    process); reset_peak first restarts the high-water mark at the live bytes."""
+    live, peak = C.c_size_t(0), C.c_size_t(0)
+    if lib().stlp_memory(C.byref(live), C.byref(peak), int(bool(reset_peak))):
+        raise _error()
+    return live.value, peak.value
 
 
 def _error():
@@ -178,7 +188,8 @@ class NativeEngine:
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
-                 prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=True, **unused):
+                 prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=True, fields="keep",
+                 **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -197,6 +208,8 @@ class NativeEngine:
             self.config["autotune"] = False
         if not tensor_cores:  # FP32 wavelets on the CUDA cores (the coloured layout)
             self.config["tensor_cores"] = False
+        if fields != "keep":  # "recompute": z and branches recomputed per level in the VJP; "auto"
+            self.config["fields"] = fields
         if cross:
             self.config["cross"] = True
         if autotune_cache:  # a file of tile heights timed before (read, then extended)

@@ -2,7 +2,10 @@
 FP32 lognormal map (sigma 0.8, seed 11).  Forward + VJP fit in one B200's HBM
 (the peak device memory is reported), and every coefficient is within the
 1e-6 criterion of the FP64 engine (relative to the largest |S| of its family
-and level), the FP64 engine run afterwards on its own."""
+and level), the FP64 engine run afterwards on its own.  The field stores:
+recomputing z and the branches per level in the VJP ("fields": "recompute",
+the reference's FieldStore::Recompute) gives the kept store's values and
+gradients bit for bit at a lower peak, for FP32 with 1 and 4 maps and FP64."""
 import numpy as np
 import pytest
 
@@ -55,3 +58,48 @@ def test_nside2048_fits_and_meets_1e6(stl):
                 worst = max(worst, float(np.max(np.abs(part(a) - part(r)) / (1e-6 * scale + 1e-6 * np.abs(part(r))))))
     print(f"nside 2048 FP32 vs FP64: worst ratio to the 1e-6 family tolerance {worst:.3f}")
     assert worst <= 1.0
+
+
+def _run(stl, nside, J, x, dtype, fields):
+    """values, gradient and peak device bytes of one forward + VJP."""
+    import torch
+    stl.device_memory(reset_peak=True)
+    e = stl.NativeEngine(nside, J, batch=x.shape[0], dtype=dtype, autotune=False, fields=fields)
+    xt = torch.tensor(x, device="cuda", dtype=torch.float32 if dtype == "float32" else torch.float64)
+    v, _ = e.forward_tensor(xt, generation=1)
+    g = torch.empty_like(xt)
+    e.vjp_tensor(np.ones_like(v), g, generation=1)
+    torch.cuda.synchronize()
+    info = e.info()
+    _, peak = stl.device_memory()
+    e.close()
+    out = g.cpu().numpy()
+    del g, xt
+    torch.cuda.empty_cache()
+    return v, out, peak, info
+
+
+@pytest.mark.parametrize("dtype,B", [("float32", 1), ("float32", 4), ("float64", 1)])
+def test_nside2048_recompute_store(stl, dtype, B):
+    nside, J, sigma = 2048, 10, 0.8
+    npix = 12 * nside * nside
+    x = np.stack([np.exp(sigma * np.random.default_rng(11 + b).standard_normal(npix) - 0.5 * sigma * sigma)
+                  for b in range(B)]).astype(np.float32).astype(np.float64)
+    vr, gr, peak_r, info = _run(stl, nside, J, x, dtype, "recompute")
+    assert info["fields"] == "recompute"
+    kept = info["device_memory"]["kept_field_bytes"]
+    live_b, _ = stl.device_memory()
+    import torch
+    free_b, _ = torch.cuda.mem_get_info()
+    # the kept store is run only where it fits: its extra fields within the free memory
+    if peak_r + kept < free_b + live_b - 8e9:
+        vk, gk, peak_k, info_k = _run(stl, nside, J, x, dtype, "keep")
+        assert info_k["fields"] == "keep"
+        assert np.array_equal(vk, vr)
+        assert np.array_equal(gk, gr)
+        print(f"nside 2048 {dtype} B {B}: peak {peak_k / 1e9:.1f} GB kept, {peak_r / 1e9:.1f} GB recomputed")
+        assert peak_r < peak_k
+    else:
+        print(f"nside 2048 {dtype} B {B}: peak {peak_r / 1e9:.1f} GB recomputed; the kept store needs "
+              f"{kept / 1e9:.1f} GB more than the recomputing one's buffers and is not run")
+    assert peak_r < 180e9 and np.isfinite(gr).all()
