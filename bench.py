@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--batch", type=int, default=4)
     p.add_argument("--skip-fp64", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--profile-step", action="store_true",
+                   help="one forward + VJP of the batch and exit (no timing, no line): the launch sequence that "
+                        "the kernel profiles in profiles/ capture")
     p.add_argument("--no-autotune", action="store_true",
                    help="default tile heights instead of timing them at prepare (for runs under a profiler, whose "
                         "replays make the timing meaningless)")
@@ -500,6 +503,11 @@ def main():
         values, _ = eng.forward_tensor(x, generation=g)
         eng.vjp_tensor(2.0 * (values - target), grad, generation=g)
 
+    if args.profile_step:
+        step32()
+        torch.cuda.synchronize()
+        eng.close()
+        return
     for _ in range(args.warmup):
         step32()
     eng.profile(on=False, reset=True)

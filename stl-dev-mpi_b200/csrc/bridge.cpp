@@ -117,7 +117,13 @@ StlpHandle* stlp_new(const char* config) {
     require(dtype == "float64" || dtype == "float32", "dtype must be float64 or float32");
     o.fp32 = dtype == "float32";
     o.autotune = v.boolean("autotune", true);
-    o.tensor_cores = v.boolean("tensor_cores", true);
+    if (const Json* tcv = v.get("tensor_cores")) {  // true / false, or "forward", "all", "none"
+      if (tcv->kind == Json::Bool) o.tensor_cores = tcv->b ? 1 : 0;
+      else if (tcv->kind == Json::String && (tcv->str == "none" || tcv->str == "forward" || tcv->str == "all"))
+        o.tensor_cores = tcv->str == "none" ? 0 : tcv->str == "forward" ? 1 : 2;
+      else if (tcv->kind != Json::Null)
+        throw std::runtime_error("tensor_cores must be a boolean or one of \"none\", \"forward\", \"all\"");
+    }
     o.tune_cache = v.string("autotune_cache", "");
     o.cross = v.boolean("cross", false);  // two channels, the plan of their cross terms (lib.rs:238-245)
     const std::string fields = v.string("fields", "keep");  // lib.rs:273-345: auto | keep | recompute
@@ -203,8 +209,9 @@ char* stlp_info(StlpHandle* h) {
     auto ol = e.operator_layout();
     for (size_t i = 0; i < ol.size(); ++i)
       js << (i ? ", " : "") << "{\"slots\": " << ol[i][0] << ", \"tile_cells\": " << ol[i][1]
-         << ", \"coloured\": " << (ol[i][2] == 1 ? "true" : "false") << ", \"layout\": \""
-         << (ol[i][2] == 2 ? "tensor_cores" : ol[i][2] == 1 ? "coloured" : "rows") << "\", \"warp_cells\": "
+         << ", \"coloured\": " << (ol[i][2] == 1 || ol[i][2] == 2 ? "true" : "false") << ", \"layout\": \""
+         << (ol[i][2] == 3 ? "tensor_cores" : ol[i][2] == 2 ? "tensor_cores+coloured" : ol[i][2] == 1 ? "coloured" : "rows")
+         << "\", \"warp_cells\": "
          << ol[i][3] << "}";
     js << "], \"tile_heights\": [";
     auto th = e.tile_heights();

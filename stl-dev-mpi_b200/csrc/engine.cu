@@ -1090,8 +1090,8 @@ class EngineImpl final : public Engine {
   std::vector<std::array<int, 4>> operator_layout() const override {
     std::vector<std::array<int, 4>> v;
     for (const auto& c : conv_)
-      v.push_back({c.mma ? c.m_S : c.S, c.mma ? c.m_pc : c.max_tile_cells, c.mma ? 2 : c.colored ? 1 : 0,
-                   c.mma ? c.m_wl : 0});
+      v.push_back({c.mma ? c.m_S : c.S, c.mma ? c.m_pc : c.max_tile_cells,
+                   c.mma_adj ? 3 : c.mma ? 2 : c.colored ? 1 : 0, c.mma_adj ? c.m_wl : 0});
     return v;
   }
 

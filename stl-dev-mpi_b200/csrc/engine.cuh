@@ -99,7 +99,10 @@ inline size_t dsize(DType t) { return t == DType::F64 ? 8 : 4; }
 // Geometry of one wavelet operator: output rows reading an input grid.
 struct ConvSpec {
   i64 nside = 0;
-  bool tensor_cores = true;     // FP32 full sky: the tensor-core layout (else the coloured one)
+  // FP32 full sky: 0 the coloured layout only (CUDA cores), 1 the tensor-core
+  // layout for the forward and the coloured one for the adjoint, 2 the
+  // tensor-core layout for both
+  int tensor_cores = 1;
   int ksz = 5, G = 4, gauge = 0;
   double eps = 0.0;
   const i64* d_grid = nullptr;  // sorted NESTED ids of the grid (device), nullptr: whole sky
@@ -171,7 +174,8 @@ struct ConvOp {
   // adjoint adds into per-warp sums over the distinct cells of the warp's
   // kMmaWarpRows rows (numbered the same way), combined per tile cell in
   // warp order.  Every sum has a fixed order.
-  bool mma = false;
+  bool mma = false;          // the forward uses the tensor-core layout
+  bool mma_adj = false;      // the adjoint too (else the coloured layout's)
   i64 m_tiles = 0;
   int m_S = 0;               // slots: 8 x the most chunks of a row
   int m_pc = 0;              // plane stride (cells; 4 mod 8)
@@ -191,7 +195,7 @@ struct ConvOp {
   }
 };
 constexpr int kMmaRows = 64;      // stored rows per tile of the tensor-core layout
-constexpr int kMmaWarpRows = 16;  // rows per warp of the adjoint (one block of private sums)
+constexpr int kMmaWarpRows = 8;   // rows per warp of the adjoint (one block of private sums)
 constexpr int kMmaPlaneMax = 1024;  // plane cells a tile may index
 constexpr int kMmaWarpMax = 252;    // warp-local cells (uint8 indices, 255: none)
 // class of the cell at position p of a chunk: every class twice, positions

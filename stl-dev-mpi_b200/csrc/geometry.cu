@@ -1049,7 +1049,7 @@ static std::vector<double> kernel_grid(int ksz, i64 nside) {
 
 // The tensor-core layout of an FP32 full-sky operator (ConvOp::m_*) from its
 // per-row slots; false (nothing kept) when a tile does not fit its limits.
-static bool build_mma_layout(ConvOp& op, const DevMem& counts, cudaStream_t s) {
+static bool build_mma_layout(ConvOp& op, const DevMem& counts, bool adjoint, cudaStream_t s) {
   const i64 n_rep = op.n_rep;
   if (op.S > 64 || op.o2 < 2) return false;
   const i64 n_tiles = (n_rep + kMmaRows - 1) / kMmaRows;
@@ -1105,6 +1105,8 @@ static bool build_mma_layout(ConvOp& op, const DevMem& counts, cudaStream_t s) {
   if (read_flag(flag, s)) return false;
   op.m_rowch = std::move(rowch);
   op.m_tch = std::move(tch);
+  op.mma = true;
+  if (!adjoint) return true;
   // per stored input cell: the (tile, plane cell, rotation) entries of the
   // adjoint's tile partials, sorted
   const i64 n_cells = op.n_in / 4, nt = n_tiles * op.m_pc;
@@ -1128,7 +1130,7 @@ static bool build_mma_layout(ConvOp& op, const DevMem& counts, cudaStream_t s) {
   STL_CUDA(cudaGetLastError());
   STL_CUDA(cudaStreamSynchronize(s));
   op.ncs = op.m_pc;
-  op.mma = true;
+  op.mma_adj = true;
   return true;
 }
 
@@ -1177,19 +1179,25 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
   // of kAdjTile stored rows, then the edge colouring of its entries
   op.adj_tiles = false;
   op.colored = false;
-  op.mma = false;
-  if (std::is_same<T, float>::value && sym && sp.tensor_cores) {
-    // FP32 full sky: the tensor-core layout when every tile fits it
+  op.mma = op.mma_adj = false;
+  if (std::is_same<T, float>::value && sym && sp.tensor_cores > 0) {
+    // FP32 full sky: the tensor-core layout when every tile fits it, for the
+    // forward (the coloured layout below then serves the adjoint) or for both
     op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
     k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
     STL_CUDA(cudaGetLastError());
-    if (build_mma_layout(op, counts, s)) {
-      op.cell.release();
-      op.coef.release();
-      return;
+    if (build_mma_layout(op, counts, sp.tensor_cores == 2, s)) {
+      if (op.mma_adj) {
+        op.cell.release();
+        op.coef.release();
+        return;
+      }
+    } else {
+      op.mma = op.mma_adj = false;
+      op.rowsum.release();
+      op.m_coef.release(); op.m_cells.release(); op.m_lc.release(); op.m_wlc.release(); op.m_winv.release();
+      op.m_rowch.release(); op.m_tch.release();
     }
-    op.rowsum.release();
-    op.m_coef.release(); op.m_cells.release(); op.m_lc.release(); op.m_wlc.release(); op.m_winv.release();
   }
   if (sym && op.S <= 128) {  // the tile sort holds 128 slots per row
     op.n_tiles = (a.n_rows + kAdjTile - 1) / kAdjTile;
@@ -1246,9 +1254,11 @@ static void build_conv_t(const ConvSpec& sp, const std::vector<double>& kernel, 
       }
     }
   }
-  op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
-  k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
-  STL_CUDA(cudaGetLastError());
+  if (!op.rowsum.p) {  // the row sums (the tensor-core branch made them already)
+    op.rowsum.alloc(sizeof(T) * 8 * a.n_rows);
+    k_rowsum<T><<<nblocks(a.n_rows, 256), 256, 0, s>>>(op.coef.as<T>(), op.S, a.n_rows, op.rowsum.as<T>());
+    STL_CUDA(cudaGetLastError());
+  }
   if (!op.colored) {
     // transposed gather table over the stored cells: entries (u, s, j)
     int sbits = 1;

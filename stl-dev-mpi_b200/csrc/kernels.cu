@@ -852,7 +852,6 @@ __device__ __forceinline__ void mma3(float d[4], const uint32_t ah[4], const uin
   mma_tf32(d, ah, bh);
 }
 
-constexpr int kMmaStages = 4;      // bulk-copy stages of the coefficient stream
 constexpr int kMmaFwdWarpRows = 8;     // rows per warp of the forward
 constexpr int kMmaFwdWarps = kMmaRows / kMmaFwdWarpRows;
 constexpr int kMmaFwdThreads = 32 * kMmaFwdWarps;
@@ -868,21 +867,24 @@ constexpr size_t kMmaAdjStage = 8 * kMmaAdjSlot * sizeof(float) + 8 * kMmaRows;
 
 // Forward: one CTA per (tile, group of 4 MT field rows), warp w the rows
 // 8 w .. 8 w + 7 of the tile.  The tile's plane [4 k][pcs][4 MT] of input
-// rows (cell -1: zero) is gathered once; per chunk of 8 slots the
-// coefficients and plane cells of every row arrive by bulk copies (two
+// rows (cell -1: zero) is gathered once by asynchronous copies and split
+// once into its TF32 high and low parts (two planes: every element serves
+// about 44 rows, so no product splits its A operand); per chunk of 8 slots
+// the coefficients and plane cells of every row arrive by bulk copies (NS
 // stages); every row's accumulators live in registers across the chunks.
-template <int MT>
+template <int MT, int NS>
 __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
     const uint16_t* __restrict__ m_lc, const float* __restrict__ coef, int Sm, i64 n_rep, int o2,
-    const int32_t* __restrict__ cells, int pcs, const int32_t* __restrict__ tch, const uint8_t* __restrict__ rowch,
-    const float* __restrict__ x, int R, float* __restrict__ out, float* __restrict__ mod, int mod_pix, int mod_row,
-    int mod_off, int* __restrict__ err, const float* __restrict__ rowsum, const double* __restrict__ rc) {
+    const int32_t* __restrict__ cells, int pcs, const int32_t* __restrict__ tch, const float* __restrict__ x, int R,
+    float* __restrict__ out, float* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err,
+    const float* __restrict__ rowsum, const double* __restrict__ rc) {
   constexpr int RM = 4 * MT;
   constexpr size_t kCoefBytes = 8 * kMmaFwdSlot * sizeof(float);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[kMmaStages];
+  __shared__ __align__(8) uint64_t bar[NS];
   __shared__ int fail;
-  float* plane = reinterpret_cast<float*>(smem_raw + kMmaStages * kMmaFwdStage);
+  float* ph = reinterpret_cast<float*>(smem_raw + NS * kMmaFwdStage);  // high parts [4][pcs][RM]
+  float* pl_ = ph + (size_t)4 * pcs * RM;                                 // low parts
   const int ngroups = (R + RM - 1) / RM;
   const i64 tile = blockIdx.x / ngroups;
   const int r0 = (int)(blockIdx.x % ngroups) * RM;
@@ -892,14 +894,14 @@ __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
   const int rows = (int)min((i64)kMmaRows, n_rep - u0);
   const int nch = tch[tile];
   if (tid == 0) {
-    for (int b = 0; b < kMmaStages; ++b) mbar_init(&bar[b], 1);
+    for (int b = 0; b < NS; ++b) mbar_init(&bar[b], 1);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int c) {
-    const int st = c % kMmaStages;
+    const int st = c % NS;
     unsigned char* base = smem_raw + st * kMmaFwdStage;
     const unsigned cb = (unsigned)(rows * 8 * sizeof(float));
     const unsigned lb = (unsigned)(8 * kMmaRows * sizeof(uint16_t));
@@ -910,34 +912,41 @@ __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
     bulk_g2s(base + kCoefBytes, m_lc + ((i64)tile * (Sm / 8) + c) * kMmaRows * 8, lb, &bar[st]);
   };
   if (tid == 0)
-    for (int c = 0; c < min(nch, kMmaStages); ++c) issue(c);
+    for (int c = 0; c < min(nch, NS); ++c) issue(c);
   // the plane: per tile cell and rotation, the CTA's RM input rows, by
   // asynchronous 16-byte copies (all in flight at once; a hole or a missing
   // cell copies zero bytes, which fills zeros); rows past R (R % 4 != 0)
-  // by plain loads
+  // by plain loads.  Each thread then splits the elements it copied.
   const int32_t* tc = cells + tile * pcs;
   const bool whole = R % 4 == 0;
-  for (int pl = tid; pl < pcs; pl += kMmaFwdThreads) {
-    const int32_t cl = tc[pl];
+  for (int q = tid; q < pcs; q += kMmaFwdThreads) {
+    const int32_t cl = tc[q];
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
-      float* dst = plane + ((size_t)kk * pcs + pl) * RM;
+      float* dst = ph + ((size_t)kk * pcs + q) * RM;
       const float* xp = x + (cl >= 0 ? rot_cell(cl, kk, o2) * R + r0 : 0);
       if (whole) {
 #pragma unroll
-        for (int q = 0; q < MT; ++q) cp_async16(dst + 4 * q, xp + 4 * q, cl >= 0 ? 16 : 0);
+        for (int j = 0; j < MT; ++j) cp_async16(dst + 4 * j, xp + 4 * j, cl >= 0 ? 16 : 0);
       } else {
 #pragma unroll
-        for (int q = 0; q < RM; ++q) dst[q] = (cl >= 0 && r0 + q < R) ? __ldg(xp + q) : 0.0f;
+        for (int j = 0; j < RM; ++j) dst[j] = (cl >= 0 && r0 + j < R) ? __ldg(xp + j) : 0.0f;
       }
     }
   }
-  cp_async_wait_all();  // this thread's copies; the barrier before the first chunk publishes them
-  int rch[kMmaFwdWarpRows];
-#pragma unroll
-  for (int i = 0; i < kMmaFwdWarpRows; ++i) {
-    const int ul = warp * kMmaFwdWarpRows + i;
-    rch[i] = ul < rows ? (int)rowch[u0 + ul] : 0;
+  cp_async_wait_all();
+  __syncthreads();  // every thread's copies have landed
+  // split, in consecutive 16-byte units (conflict-free)
+  for (int q = tid; q < pcs * RM; q += kMmaFwdThreads) {
+    float4* h = reinterpret_cast<float4*>(ph) + q;
+    float4 v = *h, w;
+    uint32_t hi, lo;
+    split_tf32(v.x, hi, lo); v.x = __uint_as_float(hi); w.x = __uint_as_float(lo);
+    split_tf32(v.y, hi, lo); v.y = __uint_as_float(hi); w.y = __uint_as_float(lo);
+    split_tf32(v.z, hi, lo); v.z = __uint_as_float(hi); w.z = __uint_as_float(lo);
+    split_tf32(v.w, hi, lo); v.w = __uint_as_float(hi); w.w = __uint_as_float(lo);
+    *h = v;
+    reinterpret_cast<float4*>(pl_)[q] = w;
   }
   float acc[kMmaFwdWarpRows][MT][4];
 #pragma unroll
@@ -946,43 +955,53 @@ __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
     for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][mt][q] = 0.0f;
-  const float* pk = plane + (size_t)k * pcs * RM + rq * 2 * MT;
+  const size_t koff = (size_t)k * pcs * RM + rq * 2 * MT;
+  const float* hk = ph + koff;
+  const float* lk = pl_ + koff;
   int c = 0;
   for (; c < nch; ++c) {
-    const int st = c % kMmaStages;
-    if (!mbar_wait(&bar[st], (c / kMmaStages) & 1)) fail = 1;
-    __syncthreads();  // also orders the plane gather before the first chunk
+    const int st = c % NS;
+    if (!mbar_wait(&bar[st], (c / NS) & 1)) fail = 1;
+    __syncthreads();  // also orders the split planes before the first chunk
     if (fail) break;
     const unsigned char* base = smem_raw + st * kMmaFwdStage;
     const float* cs = reinterpret_cast<const float*>(base);
     const uint16_t* ls = reinterpret_cast<const uint16_t*>(base + kCoefBytes);
+    // no branch per row, so the rows' independent mma chains interleave: a
+    // row past its own chunks multiplies zero coefficients (its padding),
+    // a row past the tile's end (the last tile) reads clamped plane cells
+    // and is never stored
 #pragma unroll
     for (int i = 0; i < kMmaFwdWarpRows; ++i) {
-      if (c >= rch[i]) continue;  // warp-uniform: the row has no more chunks
       const int ul = warp * kMmaFwdWarpRows + i;
-      const int lc0 = ls[ul * 8 + t], lc1 = ls[ul * 8 + t + 4];
+      const int lc0 = min((int)ls[ul * 8 + t], pcs - 1), lc1 = min((int)ls[ul * 8 + t + 4], pcs - 1);
       uint32_t bh[2], bl[2];
       split_tf32(cs[t * kMmaFwdSlot + ul * 8 + g], bh[0], bl[0]);
       split_tf32(cs[(t + 4) * kMmaFwdSlot + ul * 8 + g], bh[1], bl[1]);
-      float va[2 * MT], vb[2 * MT];
+      uint32_t ha[2 * MT], hb[2 * MT], la[2 * MT], lb[2 * MT];
       if (MT == 2) {
-        const float4 p = *reinterpret_cast<const float4*>(pk + (size_t)lc0 * RM);
-        const float4 q = *reinterpret_cast<const float4*>(pk + (size_t)lc1 * RM);
-        va[0] = p.x; va[1] = p.y; va[2] = p.z; va[3] = p.w;
-        vb[0] = q.x; vb[1] = q.y; vb[2] = q.z; vb[3] = q.w;
+        const uint4 p = *reinterpret_cast<const uint4*>(hk + (size_t)lc0 * RM);
+        const uint4 q = *reinterpret_cast<const uint4*>(hk + (size_t)lc1 * RM);
+        const uint4 u = *reinterpret_cast<const uint4*>(lk + (size_t)lc0 * RM);
+        const uint4 v = *reinterpret_cast<const uint4*>(lk + (size_t)lc1 * RM);
+        ha[0] = p.x; ha[1] = p.y; ha[2] = p.z; ha[3] = p.w;
+        hb[0] = q.x; hb[1] = q.y; hb[2] = q.z; hb[3] = q.w;
+        la[0] = u.x; la[1] = u.y; la[2] = u.z; la[3] = u.w;
+        lb[0] = v.x; lb[1] = v.y; lb[2] = v.z; lb[3] = v.w;
       } else {
-        const float2 p = *reinterpret_cast<const float2*>(pk + (size_t)lc0 * RM);
-        const float2 q = *reinterpret_cast<const float2*>(pk + (size_t)lc1 * RM);
-        va[0] = p.x; va[1] = p.y;
-        vb[0] = q.x; vb[1] = q.y;
+        const uint2 p = *reinterpret_cast<const uint2*>(hk + (size_t)lc0 * RM);
+        const uint2 q = *reinterpret_cast<const uint2*>(hk + (size_t)lc1 * RM);
+        const uint2 u = *reinterpret_cast<const uint2*>(lk + (size_t)lc0 * RM);
+        const uint2 v = *reinterpret_cast<const uint2*>(lk + (size_t)lc1 * RM);
+        ha[0] = p.x; ha[1] = p.y;
+        hb[0] = q.x; hb[1] = q.y;
+        la[0] = u.x; la[1] = u.y;
+        lb[0] = v.x; lb[1] = v.y;
       }
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt) {
-        uint32_t ah[4], al[4];
-        split_tf32(va[2 * mt], ah[0], al[0]);
-        split_tf32(va[2 * mt + 1], ah[1], al[1]);
-        split_tf32(vb[2 * mt], ah[2], al[2]);
-        split_tf32(vb[2 * mt + 1], ah[3], al[3]);
+        const uint32_t ah[4] = {ha[2 * mt], ha[2 * mt + 1], hb[2 * mt], hb[2 * mt + 1]};
+        const uint32_t al[4] = {la[2 * mt], la[2 * mt + 1], lb[2 * mt], lb[2 * mt + 1]};
         float d[4];
         mma3(d, ah, al, bh, bl);
 #pragma unroll
@@ -990,12 +1009,11 @@ __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
       }
     }
     __syncthreads();  // the stage is read: refill it
-    if (tid == 0 && c + kMmaStages < nch) issue(c + kMmaStages);
+    if (tid == 0 && c + NS < nch) issue(c + NS);
   }
   if (fail) {
     bool drained = true;
-    for (int q = c; q < min(nch, c + kMmaStages); ++q)
-      drained &= mbar_wait(&bar[q % kMmaStages], (q / kMmaStages) & 1);
+    for (int q = c; q < min(nch, c + NS); ++q) drained &= mbar_wait(&bar[q % NS], (q / NS) & 1);
     if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
     return;
   }
@@ -1032,26 +1050,26 @@ __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
   }
 }
 
-// Adjoint: one CTA per (tile, 4 cotangent rows), warp w the rows 16 w ..
-// 16 w + 15 of the tile.  Warp w adds the products of its rows into
-// private sums [4 k][wls][4 r] over the distinct cells of its rows
-// (warp-local numbering), so no other warp touches them and no barrier
-// separates the slots; per chunk and row one mma gives the 16 x 8 products
-// (rotation and row) x (slot) of the row's cotangents with its
-// coefficients.  The coefficients and warp-local cells stream through
-// kMmaStages bulk-copy stages.  Then every tile cell's partial is the sum
-// over the warps, in warp order, written to part[tile][k][pcs][R].  madd:
-// the modulus VJP added to the cotangents first, as k_conv_adj_colored.
+// Adjoint: one CTA per (tile, 4 cotangent rows), warp w the rows 8 w ..
+// 8 w + 7 of the tile.  Warp w adds the products of its rows into private
+// sums [4 k][wls][4 r] over the distinct cells of its rows (warp-local
+// numbering), so no other warp touches them and no barrier separates the
+// slots; per chunk and row one mma gives the 16 x 8 products (rotation and
+// row) x (slot) of the row's cotangents with its coefficients.  The
+// coefficients and warp-local cells stream through NS bulk-copy stages.
+// Then every tile cell's partial is the sum over the warps, in warp order,
+// written to part[tile][k][pcs][R].  madd: the modulus VJP added to the
+// cotangents first, as k_conv_adj_colored.
+template <int NS>
 __global__ void __launch_bounds__(kMmaAdjThreads, 2) k_conv_adj_mma(
     const uint8_t* __restrict__ m_wlc, const float* __restrict__ coef, int Sm, i64 n_rep, int o2,
-    const int32_t* __restrict__ tch, const uint8_t* __restrict__ rowch, const uint8_t* __restrict__ m_winv, int pcs,
-    int wls, const float* __restrict__ gy, int R, float* __restrict__ part, int* __restrict__ err,
-    ModulusAdd<float> madd) {
+    const int32_t* __restrict__ tch, const uint8_t* __restrict__ m_winv, int pcs, int wls,
+    const float* __restrict__ gy, int R, float* __restrict__ part, int* __restrict__ err, ModulusAdd<float> madd) {
   constexpr size_t kCoefBytes = 8 * kMmaAdjSlot * sizeof(float);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[kMmaStages];
+  __shared__ __align__(8) uint64_t bar[NS];
   __shared__ int fail;
-  float* sums = reinterpret_cast<float*>(smem_raw + kMmaStages * kMmaAdjStage);  // [warps][4][wls][4]
+  float* sums = reinterpret_cast<float*>(smem_raw + NS * kMmaAdjStage);  // [warps][4][wls][4]
   const int ngroups = (R + 3) / 4;  // rows past R (the last group of R % 4 != 0) are zero
   const i64 tile = blockIdx.x / ngroups;
   const int r0 = (int)(blockIdx.x % ngroups) * 4;
@@ -1061,14 +1079,14 @@ __global__ void __launch_bounds__(kMmaAdjThreads, 2) k_conv_adj_mma(
   const int rows = (int)min((i64)kMmaRows, n_rep - u0);
   const int nch = tch[tile];
   if (tid == 0) {
-    for (int b = 0; b < kMmaStages; ++b) mbar_init(&bar[b], 1);
+    for (int b = 0; b < NS; ++b) mbar_init(&bar[b], 1);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int c) {
-    const int st = c % kMmaStages;
+    const int st = c % NS;
     unsigned char* base = smem_raw + st * kMmaAdjStage;
     const unsigned cb = (unsigned)(rows * 8 * sizeof(float));
     const unsigned wb = (unsigned)(8 * kMmaRows);
@@ -1079,11 +1097,12 @@ __global__ void __launch_bounds__(kMmaAdjThreads, 2) k_conv_adj_mma(
     bulk_g2s(base + kCoefBytes, m_wlc + ((i64)tile * (Sm / 8) + c) * kMmaRows * 8, wb, &bar[st]);
   };
   if (tid == 0)
-    for (int c = 0; c < min(nch, kMmaStages); ++c) issue(c);
+    for (int c = 0; c < min(nch, NS); ++c) issue(c);
   float* mine = sums + (size_t)warp * 16 * wls;
   for (int i = lane; i < 16 * wls; i += 32) mine[i] = 0.0f;
   // the rows' cotangents under rotation k (gauge permutation, conjugation
-  // and the modulus VJP folded in), as A fragments split per chunk
+  // and the modulus VJP folded in) as split A fragments; rows past the
+  // tile's end are zero
   const bool odd = k & 1;
   auto cot = [&](i64 p, int rr, int o) {
     if (r0 + rr >= R) return 0.0f;
@@ -1100,61 +1119,62 @@ __global__ void __launch_bounds__(kMmaAdjThreads, 2) k_conv_adj_mma(
     }
     return (pt && rot_conj(k, gg)) ? -v : v;
   };
-  float av[kMmaWarpRows][4];
-  int rch[kMmaWarpRows];
+  uint32_t ah[kMmaWarpRows][4], al[kMmaWarpRows][4];
 #pragma unroll
   for (int i = 0; i < kMmaWarpRows; ++i) {
     const int ul = warp * kMmaWarpRows + i;
-    rch[i] = ul < rows ? (int)rowch[u0 + ul] : 0;
-    av[i][0] = av[i][1] = av[i][2] = av[i][3] = 0.0f;
+    float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     if (ul < rows) {
       const i64 p = rot_pixel(u0 + ul, k, o2);
-      av[i][0] = cot(p, 2 * rp, t);
-      av[i][1] = cot(p, 2 * rp + 1, t);
-      av[i][2] = cot(p, 2 * rp, t + 4);
-      av[i][3] = cot(p, 2 * rp + 1, t + 4);
+      a[0] = cot(p, 2 * rp, t);
+      a[1] = cot(p, 2 * rp + 1, t);
+      a[2] = cot(p, 2 * rp, t + 4);
+      a[3] = cot(p, 2 * rp + 1, t + 4);
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) split_tf32(a[q], ah[i][q], al[i][q]);
   }
   float* mk = mine + (size_t)k * wls * 4 + 2 * rp;
   int c = 0;
   for (; c < nch; ++c) {
-    const int st = c % kMmaStages;
-    if (!mbar_wait(&bar[st], (c / kMmaStages) & 1)) fail = 1;
+    const int st = c % NS;
+    if (!mbar_wait(&bar[st], (c / NS) & 1)) fail = 1;
     __syncthreads();  // also orders the zeroed sums before the first chunk
     if (fail) break;
     const unsigned char* base = smem_raw + st * kMmaAdjStage;
     const float* cs = reinterpret_cast<const float*>(base);
     const uint8_t* ws = base + kCoefBytes;
+    // per row: the products (independent of the other rows, so the chains
+    // interleave; a row past its own chunks multiplies zero coefficients),
+    // then the additions in row order: a later row may add to the same
+    // cells, and the warp's shared-memory accesses are issued in program
+    // order (no lane diverges here; the compiler keeps the order of
+    // accesses that may alias)
 #pragma unroll
     for (int i = 0; i < kMmaWarpRows; ++i) {
-      if (c >= rch[i]) continue;  // warp-uniform
       const int ul = warp * kMmaWarpRows + i;
-      uint32_t ah[4], al[4], bh[2], bl[2];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) split_tf32(av[i][q], ah[q], al[q]);
+      uint32_t bh[2], bl[2];
       split_tf32(cs[g * kMmaAdjSlot + ul * 8 + t], bh[0], bl[0]);
       split_tf32(cs[g * kMmaAdjSlot + ul * 8 + t + 4], bh[1], bl[1]);
       float d[4];
-      mma3(d, ah, al, bh, bl);
-      const uint16_t wp = *reinterpret_cast<const uint16_t*>(ws + ul * 8 + 2 * t);
-      float2* s0 = reinterpret_cast<float2*>(mk + (size_t)(wp & 0xff) * 4);
-      float2* s1 = reinterpret_cast<float2*>(mk + (size_t)(wp >> 8) * 4);
-      float2 v0 = *s0, v1 = *s1;
-      v0.x += d[0]; v0.y += d[2];
-      v1.x += d[1]; v1.y += d[3];
-      *s0 = v0;
-      *s1 = v1;
-      // the next row may add to the same cells: the warp's shared-memory
-      // accesses are issued in program order (no lane diverges here) and
-      // the compiler keeps the order (the addresses may alias)
+      mma3(d, ah[i], al[i], bh, bl);
+      if (ul < rows) {  // past the tile's end: the stage holds no data for the row
+        const uint16_t wp = *reinterpret_cast<const uint16_t*>(ws + ul * 8 + 2 * t);
+        float2* s0 = reinterpret_cast<float2*>(mk + (size_t)(wp & 0xff) * 4);
+        float2* s1 = reinterpret_cast<float2*>(mk + (size_t)(wp >> 8) * 4);
+        float2 v0 = *s0, v1 = *s1;
+        v0.x += d[0]; v0.y += d[2];
+        v1.x += d[1]; v1.y += d[3];
+        *s0 = v0;
+        *s1 = v1;
+      }
     }
     __syncthreads();  // the stage is read: refill it
-    if (tid == 0 && c + kMmaStages < nch) issue(c + kMmaStages);
+    if (tid == 0 && c + NS < nch) issue(c + NS);
   }
   if (fail) {
     bool drained = true;
-    for (int q = c; q < min(nch, c + kMmaStages); ++q)
-      drained &= mbar_wait(&bar[q % kMmaStages], (q / kMmaStages) & 1);
+    for (int q = c; q < min(nch, c + NS); ++q) drained &= mbar_wait(&bar[q % NS], (q / NS) & 1);
     if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
     return;
   }
@@ -2137,33 +2157,60 @@ void dec_apply_w(const DecOp& op, bool transpose, const Tin* x, int x_pix, int x
                              accumulate, s, rb);
 }
 
-// tensor-core launches (FP32 operators in the tensor-core layout)
-inline size_t fwd_mma_smem(const ConvOp& op, int MT) {
-  return kMmaStages * kMmaFwdStage + sizeof(float) * 4 * op.m_pc * 4 * MT;
+// stages of the tensor-core launches: as many (up to 4) as leave two CTAs per SM
+inline size_t fwd_mma_planes(const ConvOp& op, int MT) { return 2 * sizeof(float) * 4 * op.m_pc * 4 * MT; }
+inline int fwd_mma_stages(const ConvOp& op, int MT) {
+  for (int ns = 4; ns > 2; --ns)
+    if (ns * kMmaFwdStage + fwd_mma_planes(op, MT) <= 112 * 1024) return ns;
+  return 2;
 }
-inline size_t adj_mma_smem(const ConvOp& op) {
-  return kMmaStages * kMmaAdjStage + sizeof(float) * kMmaAdjWarps * 16 * op.m_wl;
+inline size_t fwd_mma_smem(const ConvOp& op, int MT) {
+  return fwd_mma_stages(op, MT) * kMmaFwdStage + fwd_mma_planes(op, MT);
+}
+inline size_t adj_mma_sums(const ConvOp& op) { return sizeof(float) * kMmaAdjWarps * 16 * op.m_wl; }
+inline int adj_mma_stages(const ConvOp& op) {
+  for (int ns = 4; ns > 2; --ns)
+    if (ns * kMmaAdjStage + adj_mma_sums(op) <= 112 * 1024) return ns;
+  return 2;
+}
+inline size_t adj_mma_smem(const ConvOp& op) { return adj_mma_stages(op) * kMmaAdjStage + adj_mma_sums(op); }
+
+template <int MT, int NS>
+void conv_forward_mma_ns(const ConvOp& op, const float* x, int R, float* out, float* mod, int mod_pix, int mod_row,
+                         int mod_off, int* err, const double* rc, cudaStream_t s) {
+  allow_dynamic_smem(k_conv_fwd_mma<MT, NS>);
+  dim3 grid((unsigned)(op.m_tiles * ((R + 4 * MT - 1) / (4 * MT))));
+  k_conv_fwd_mma<MT, NS><<<grid, kMmaFwdThreads, fwd_mma_smem(op, MT), s>>>(
+      op.m_lc.as<uint16_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_cells.as<int32_t>(), op.m_pc,
+      op.m_tch.as<int32_t>(), x, R, out, mod, mod_pix, mod_row, mod_off, err, op.rowsum.as<float>(), rc);
 }
 
 template <int MT>
 void conv_forward_mma_mt(const ConvOp& op, const float* x, int R, float* out, float* mod, int mod_pix, int mod_row,
                          int mod_off, int* err, const double* rc, cudaStream_t s) {
-  allow_dynamic_smem(k_conv_fwd_mma<MT>);
-  dim3 grid((unsigned)(op.m_tiles * ((R + 4 * MT - 1) / (4 * MT))));
-  k_conv_fwd_mma<MT><<<grid, kMmaFwdThreads, fwd_mma_smem(op, MT), s>>>(
-      op.m_lc.as<uint16_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_cells.as<int32_t>(), op.m_pc,
-      op.m_tch.as<int32_t>(), op.m_rowch.as<uint8_t>(), x, R, out, mod, mod_pix, mod_row, mod_off, err,
-      op.rowsum.as<float>(), rc);
+  const int ns = fwd_mma_stages(op, MT);
+  if (ns == 4) conv_forward_mma_ns<MT, 4>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+  else if (ns == 3) conv_forward_mma_ns<MT, 3>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+  else conv_forward_mma_ns<MT, 2>(op, x, R, out, mod, mod_pix, mod_row, mod_off, err, rc, s);
+}
+
+template <int NS>
+void conv_adjoint_mma_ns(const ConvOp& op, const float* gy, int R, const AdjScratch& scr, cudaStream_t s, int* err,
+                         const ModulusAdd<float>* madd) {
+  allow_dynamic_smem(k_conv_adj_mma<NS>);
+  dim3 grid((unsigned)(op.m_tiles * ((R + 3) / 4)));
+  k_conv_adj_mma<NS><<<grid, kMmaAdjThreads, adj_mma_smem(op), s>>>(
+      op.m_wlc.as<uint8_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_tch.as<int32_t>(),
+      op.m_winv.as<uint8_t>(), op.m_pc, op.m_wl, gy, R, static_cast<float*>(scr.part), err,
+      madd ? *madd : ModulusAdd<float>());
 }
 
 void conv_adjoint_mma(const ConvOp& op, const float* gy, int R, float* gx, bool accumulate, const AdjScratch& scr,
                       cudaStream_t s, int* err, const ModulusAdd<float>* madd) {
-  allow_dynamic_smem(k_conv_adj_mma);
-  dim3 grid((unsigned)(op.m_tiles * ((R + 3) / 4)));
-  k_conv_adj_mma<<<grid, kMmaAdjThreads, adj_mma_smem(op), s>>>(
-      op.m_wlc.as<uint8_t>(), op.m_coef.as<float>(), op.m_S, op.n_rep, op.o2, op.m_tch.as<int32_t>(),
-      op.m_rowch.as<uint8_t>(), op.m_winv.as<uint8_t>(), op.m_pc, op.m_wl, gy, R, static_cast<float*>(scr.part), err,
-      madd ? *madd : ModulusAdd<float>());
+  const int ns = adj_mma_stages(op);
+  if (ns == 4) conv_adjoint_mma_ns<4>(op, gy, R, scr, s, err, madd);
+  else if (ns == 3) conv_adjoint_mma_ns<3>(op, gy, R, scr, s, err, madd);
+  else conv_adjoint_mma_ns<2>(op, gy, R, scr, s, err, madd);
   if (R % 4 == 0) adj_combine_rb<float, 4>(op, R, gx, accumulate, scr, s);
   else if (R % 2 == 0) adj_combine_rb<float, 2>(op, R, gx, accumulate, scr, s);
   else adj_combine_rb<float, 1>(op, R, gx, accumulate, scr, s);
@@ -2269,13 +2316,13 @@ std::vector<int> conv_forward_choices(const ConvOp& op, size_t elem, int R, bool
 }
 
 size_t adjoint_part_bytes(const ConvOp& op, size_t elem, int R) {
-  if (op.mma) return elem * (size_t)op.m_tiles * 4 * op.m_pc * R;
+  if (op.mma_adj) return elem * (size_t)op.m_tiles * 4 * op.m_pc * R;
   if (!op.adj_tiles) return 0;
   return elem * (size_t)op.n_tiles * 4 * op.ncs * R;
 }
 
 bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
-  if (op.mma)
+  if (op.mma_adj)
     return scr && elem == 4 && adjoint_part_bytes(op, elem, R) <= scr->capacity && adj_mma_smem(op) <= 227 * 1024;
   if (!scr || !op.adj_tiles || op.nk != 4) return false;
   if (adjoint_part_bytes(op, elem, R) > scr->capacity) return false;
@@ -2286,7 +2333,7 @@ bool adjoint_tiles_usable(const ConvOp& op, size_t elem, int R, const AdjScratch
 }
 
 bool conv_adjoint_fuses_modulus(const ConvOp& op, size_t elem, int R, const AdjScratch* scr, int* err) {
-  return (op.colored || op.mma) && err && adjoint_tiles_usable(op, elem, R, scr);
+  return (op.colored || op.mma_adj) && err && adjoint_tiles_usable(op, elem, R, scr);
 }
 
 template <typename T>
@@ -2298,7 +2345,7 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
     const std::vector<int> ok = conv_adjoint_choices(op, sizeof(T), R, scr);
     if (std::find(ok.begin(), ok.end(), rb) == ok.end()) throw std::runtime_error("invalid adjoint tile height");
   }
-  if (op.mma) {
+  if (op.mma_adj) {
     if (!adjoint_tiles_usable(op, sizeof(T), R, scr) || !err)
       throw std::runtime_error("the tensor-core adjoint needs FP32 rows, an error flag and tile scratch");
     conv_adjoint_mma(op, reinterpret_cast<const float*>(gy), R, reinterpret_cast<float*>(gx), accumulate, *scr, s,
@@ -2330,7 +2377,7 @@ void conv_adjoint(const ConvOp& op, const T* gy, int R, T* gx, bool accumulate, 
 // valid tile heights of an adjoint launch
 std::vector<int> conv_adjoint_choices(const ConvOp& op, size_t elem, int R, const AdjScratch* scr) {
   std::vector<int> v;
-  if (op.mma) {
+  if (op.mma_adj) {
     if (adjoint_tiles_usable(op, elem, R, scr)) v.push_back(4);
     return v;
   }

@@ -42,9 +42,10 @@ struct Options {
   bool fp32 = false;  // compute precision of the fields (sums are FP64 in both)
   int device = 0;
   bool autotune = true;  // time the tile heights of the wavelet and decimation launches at prepare
-  // FP32 full-sky wavelets on the tensor cores (3xTF32 mma.sync; else the
-  // FP32 CUDA-core kernels of the coloured layout)
-  bool tensor_cores = true;
+  // FP32 full-sky wavelets on the tensor cores (3xTF32 mma.sync): 0 none
+  // (the CUDA-core kernels of the coloured layout), 1 the forward (the
+  // adjoint on the CUDA cores), 2 forward and adjoint
+  int tensor_cores = 1;
   // Two channels and the plan of their cross terms only (c1 != c2: S1 of the
   // root-normalised z, S2, S3 and S4 in both channel orders), maps
   // [B][2][N]; the fields then hold 2 B maps (map 2 b + c).

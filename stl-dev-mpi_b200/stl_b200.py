@@ -206,8 +206,10 @@ class NativeEngine:
                            orientations=int(orientations), device=self.device, dtype=dtype)
         if not autotune:  # keep the default tile heights (no timing at prepare)
             self.config["autotune"] = False
-        if not tensor_cores:  # FP32 wavelets on the CUDA cores (the coloured layout)
-            self.config["tensor_cores"] = False
+        # FP32 wavelets: True / "forward" (the default: forward on the tensor cores,
+        # adjoint on the CUDA cores), "all" (both on the tensor cores), False / "none"
+        if tensor_cores is not True and tensor_cores != "forward":
+            self.config["tensor_cores"] = tensor_cores if isinstance(tensor_cores, str) else bool(tensor_cores)
         if fields != "keep":  # "recompute": z and branches recomputed per level in the VJP; "auto"
             self.config["fields"] = fields
         if cross:

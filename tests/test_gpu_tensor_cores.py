@@ -41,16 +41,18 @@ def maps(seed, B, nside):
 
 
 def test_layout_per_level(stl):
-    """FP32 levels above nside 32 hold the tensor-core layout; the FP64 coarse
-    levels (and every level with tensor_cores off) the coloured one."""
-    e = stl.NativeEngine(128, 5, dtype="float32")
-    e.prepare()
-    layouts = [o["layout"] for o in e.info()["operators"]]
-    assert layouts[:2] == ["tensor_cores", "tensor_cores"], layouts
-    assert all(v == "coloured" for v in layouts[2:]), layouts
-    off = stl.NativeEngine(128, 5, dtype="float32", tensor_cores=False)
-    off.prepare()
-    assert all(o["layout"] == "coloured" for o in off.info()["operators"])
+    """FP32 levels above nside 32 hold the tensor-core layout (for the
+    forward, with the coloured one for the adjoint by default; for both with
+    "all"); the FP64 coarse levels and every level with tensor_cores off
+    hold the coloured one."""
+    for mode, want in ((True, "tensor_cores+coloured"), ("all", "tensor_cores"), (False, "coloured")):
+        e = stl.NativeEngine(128, 5, dtype="float32", tensor_cores=mode)
+        e.prepare()
+        layouts = [o["layout"] for o in e.info()["operators"]]
+        first = 2 if mode is not False else 0
+        assert all(v == want for v in layouts[:first]), (mode, layouts)
+        assert all(v == "coloured" for v in layouts[first:]), (mode, layouts)
+        e.close()
 
 
 @pytest.mark.parametrize("nside,J,B", [(128, 5, 4), (256, 6, 2), (128, 4, 1), (64, 4, 3)])
@@ -58,8 +60,8 @@ def test_tensor_cores_match_cuda_cores_and_fp64(stl, nside, J, B):
     x = maps(nside + B, B, nside)
     t = maps(1000 + nside, B, nside)
     out = {}
-    for name, kw in (("tc", dict(dtype="float32")), ("cc", dict(dtype="float32", tensor_cores=False)),
-                     ("f64", dict(dtype="float64"))):
+    for name, kw in (("tc", dict(dtype="float32")), ("tca", dict(dtype="float32", tensor_cores="all")),
+                     ("cc", dict(dtype="float32", tensor_cores=False)), ("f64", dict(dtype="float64"))):
         e = stl.NativeEngine(nside, J, batch=B, **kw)
         tv, _ = e.forward(t, generation=1)
         v, _ = e.forward(x, generation=2)
@@ -68,22 +70,26 @@ def test_tensor_cores_match_cuda_cores_and_fp64(stl, nside, J, B):
         out[name] = (v, g, e.plan)
         e.close()
     v64, g64, plan = out["f64"]
-    for name in ("tc", "cc"):
+    for name in ("tc", "tca", "cc"):
         v, g, _ = out[name]
         ratio = family_ratio(plan, v, v64)
         gerr = float(np.max(np.abs(g - g64)) / np.max(np.abs(g64)))
         print(f"nside {nside}: {name} vs FP64 family ratio {ratio:.3f}, gradient {gerr:.2e}")
         assert ratio <= 1.0
         assert gerr <= 1e-4
-    # the two FP32 forms agree with each other as closely as either with FP64
+    # the FP32 forms agree with each other as closely as with FP64; the
+    # default and "all" share the forward bit for bit
     assert family_ratio(plan, out["tc"][0], out["cc"][0]) <= 1.0
+    assert np.array_equal(out["tc"][0], out["tca"][0])
     assert np.max(np.abs(out["tc"][1] - out["cc"][1])) <= 1e-4 * np.max(np.abs(g64))
+    assert np.max(np.abs(out["tca"][1] - out["cc"][1])) <= 1e-4 * np.max(np.abs(g64))
 
 
-def test_tensor_cores_bit_reproducible(stl):
+@pytest.mark.parametrize("mode", [True, "all"])
+def test_tensor_cores_bit_reproducible(stl, mode):
     nside, J, B = 128, 5, 2
     x = maps(9, B, nside)
-    e = stl.NativeEngine(nside, J, batch=B, dtype="float32")
+    e = stl.NativeEngine(nside, J, batch=B, dtype="float32", tensor_cores=mode)
     v1, _ = e.forward(x, generation=1)
     cot = np.random.default_rng(10).standard_normal(v1.shape) + 1j * np.random.default_rng(11).standard_normal(v1.shape)
     g1 = e.vjp(cot, generation=1)
@@ -91,7 +97,7 @@ def test_tensor_cores_bit_reproducible(stl):
     g2 = e.vjp(cot, generation=2)
     assert np.array_equal(v1, v2)
     assert np.array_equal(g1, g2)
-    e2 = stl.NativeEngine(nside, J, batch=B, dtype="float32", autotune=False)
+    e2 = stl.NativeEngine(nside, J, batch=B, dtype="float32", autotune=False, tensor_cores=mode)
     v3, _ = e2.forward(x, generation=3)
     g3 = e2.vjp(cot, generation=3)
     assert np.array_equal(v1, v3)
