@@ -169,12 +169,15 @@ int stlp_memory(size_t* live, size_t* peak, int reset_peak);
 
 /* The integer tables of the engine's operators, for exact checks: kind 0
  * the sorted distinct input cells (full-sky NESTED ids) each output pixel
- * of level `level` reads in its wavelet, kind 1 the sorted fine cells of
- * nonzero weight each coarse pixel of level + 1 reads in the decimation.
+ * of level `level` reads in its wavelet (weight: the cell's largest
+ * |coefficient|), kind 1 the sorted fine cells of nonzero weight each
+ * coarse pixel of level + 1 reads in the decimation (weight: |w|).
  * *needed = the widest row; when out is not NULL and width >= *needed,
- * out [pixels][width] gets the rows in pixel order, padded with -1.  No
- * reference counterpart (the reference's tests read its Rust tables). */
-int stlp_operator_rows(StlpHandle* h, size_t level, int kind, int64_t* out, size_t width, size_t* needed);
+ * out [pixels][width] gets the rows in pixel order, padded with -1, and
+ * weight (or NULL) the weights, padded with 0.  No reference counterpart
+ * (the reference's tests read its Rust tables). */
+int stlp_operator_rows(StlpHandle* h, size_t level, int kind, int64_t* out, double* weight, size_t width,
+                       size_t* needed);
 
 /* Objective terms of the synthesis on the device (the loss terms stl-synth
  * adds after the statistics).  The reference has no C entry points for

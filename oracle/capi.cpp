@@ -1,6 +1,7 @@
 // C entry points of the oracle, for ctypes (oracle/oracle.py).
 // TEST INFRASTRUCTURE ONLY: the engine never links this library.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -92,26 +93,37 @@ int or_bind(const i64* grid, i64 ngrid, i64 nside, int ksz, int G, int gauge, do
 
 // The sorted distinct cells of nonzero weight each row reads, bound on the
 // whole sky (conv.rs rows_eps with every cell present): out [nrows][width]
-// padded with -1, counts [nrows]; -1 when a row has more than width cells.
-int or_row_cells(const i64* rows, i64 nrows, i64 nside, int ksz, int G, int gauge, i64* out, i64 width,
-                 i64* counts) {
+// padded with -1, wmax [nrows][width] the cell's largest bound weight over
+// the gauges and taps, counts [nrows]; -1 when a row has more than width
+// cells.
+typedef std::pair<i64, double> CellWeight;
+
+int or_row_cells(const i64* rows, i64 nrows, i64 nside, int ksz, int G, int gauge, i64* out, double* wmax,
+                 i64 width, i64* counts) {
   GUARD(-1, {
     Bound b;
     bind_rows(nullptr, 12 * nside * nside, rows, nrows, nside, ksz, G, (Gauge)gauge, 0.0, b);
     const int P = ksz * ksz;
     for (i64 k = 0; k < nrows; ++k) {
-      std::vector<i64> c;
+      std::vector<CellWeight> c;
       for (int g = 0; g < G; ++g)
         for (int p = 0; p < P; ++p)
           for (int n = 0; n < 4; ++n) {
             const size_t e = (((size_t)k * G + g) * P + p) * 4 + n;
-            if (b.w[e] != 0.0) c.push_back(b.pos[e]);
+            if (b.w[e] != 0.0) c.push_back({b.pos[e], std::fabs(b.w[e])});
           }
       std::sort(c.begin(), c.end());
-      c.erase(std::unique(c.begin(), c.end()), c.end());
-      if ((i64)c.size() > width) throw std::runtime_error("a row reads more cells than the width");
-      counts[k] = (i64)c.size();
-      for (i64 j = 0; j < width; ++j) out[k * width + j] = j < (i64)c.size() ? c[j] : -1;
+      std::vector<CellWeight> m;
+      for (const auto& e : c) {
+        if (!m.empty() && m.back().first == e.first) m.back().second = std::max(m.back().second, e.second);
+        else m.push_back(e);
+      }
+      if ((i64)m.size() > width) throw std::runtime_error("a row reads more cells than the width");
+      counts[k] = (i64)m.size();
+      for (i64 j = 0; j < width; ++j) {
+        out[k * width + j] = j < (i64)m.size() ? m[j].first : -1;
+        wmax[k * width + j] = j < (i64)m.size() ? m[j].second : 0.0;
+      }
     }
     return 0;
   })

@@ -53,7 +53,7 @@ def lib():
             "or_kernel_grid": ([C.c_int, C.c_int64, _D], None),
             "or_wavelet_weights": ([C.c_int, _D], None),
             "or_bind": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, _I64, _D, _U8], C.c_int),
-            "or_row_cells": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, _I64, C.c_int64, _I64],
+            "or_row_cells": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, _I64, _D, C.c_int64, _I64],
                              C.c_int),
             "or_conv_forward": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, C.c_int64, _D], C.c_int),
             "or_conv_adjoint": ([_I64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, C.c_int64, _D], C.c_int),
@@ -170,14 +170,17 @@ def bind(grid, nside, ksz, G, gauge="cosmo", eps=0.0):
 
 
 def row_cells(rows, nside, ksz=5, G=4, gauge="cosmo", width=128):
-    """[len(rows), width] int64: the sorted distinct cells of nonzero weight each
-    row reads in its bound stencils on the whole sky (padded with -1)."""
+    """(cells [len(rows), w] int64 padded with -1, weights [len(rows), w]): the
+    sorted distinct cells of nonzero weight each row reads in its bound
+    stencils on the whole sky and their largest bound weights."""
     rows = np.ascontiguousarray(rows, dtype=np.int64)
     out = np.empty((rows.size, width), np.int64)
+    wmax = np.empty((rows.size, width))
     counts = np.empty(rows.size, np.int64)
-    _check(lib().or_row_cells(_p(rows, _I64), rows.size, nside, ksz, G, GAUGES[gauge], _p(out, _I64), width,
-                              _p(counts, _I64)))
-    return out[:, : max(int(counts.max()) if counts.size else 0, 1)]
+    _check(lib().or_row_cells(_p(rows, _I64), rows.size, nside, ksz, G, GAUGES[gauge], _p(out, _I64), _p(wmax),
+                              width, _p(counts, _I64)))
+    w = max(int(counts.max()) if counts.size else 0, 1)
+    return out[:, :w], wmax[:, :w]
 
 
 def _weights(weights, ksz):

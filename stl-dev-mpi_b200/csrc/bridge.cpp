@@ -262,18 +262,24 @@ int stlp_memory(size_t* live, size_t* peak, int reset_peak) {
   });
 }
 
-int stlp_operator_rows(StlpHandle* h, size_t level, int kind, int64_t* out, size_t width, size_t* needed) {
+int stlp_operator_rows(StlpHandle* h, size_t level, int kind, int64_t* out, double* weight, size_t width,
+                       size_t* needed) {
   return guard<int>(-1, [&] {
     require(h != nullptr && needed != nullptr, "null argument");
     std::vector<int64_t> rows;
+    std::vector<double> wts;
     int w = 0;
-    h->engine->operator_rows((int)level, kind, rows, w);
+    h->engine->operator_rows((int)level, kind, rows, wts, w);
     *needed = (size_t)w;
     if (out && width >= (size_t)w && w > 0) {
       const size_t n = rows.size() / (size_t)w;
       for (size_t r = 0; r < n; ++r) {
         std::copy(rows.begin() + r * w, rows.begin() + (r + 1) * w, out + r * width);
         std::fill(out + r * width + w, out + (r + 1) * width, (int64_t)-1);
+        if (weight) {
+          std::copy(wts.begin() + r * w, wts.begin() + (r + 1) * w, weight + r * width);
+          std::fill(weight + r * width + w, weight + (r + 1) * width, 0.0);
+        }
       }
     }
     return 0;

@@ -1002,7 +1002,8 @@ class EngineImpl final : public Engine {
     return v;
   }
   std::vector<std::array<int, 8>> tile_heights() const override { return tiles_; }
-  void operator_rows(int level, int kind, std::vector<int64_t>& out, int& width) override {
+  void operator_rows(int level, int kind, std::vector<int64_t>& out, std::vector<double>& weight,
+                     int& width) override {
     prepare();
     if (grid_mode()) throw std::runtime_error("operator tables are exported for full-sky engines");
     if (level < 0 || level >= levels_ || kind < 0 || kind > 1 || (kind == 1 && level + 1 >= levels_))
@@ -1014,6 +1015,19 @@ class EngineImpl final : public Engine {
       if (m.bytes) STL_CUDA(cudaMemcpyAsync(h.data(), m.p, m.bytes, cudaMemcpyDeviceToHost, s));
       return h;
     };
+    auto fetch_real = [&](const DevMem& m, DType t) {
+      std::vector<double> h;
+      if (t == DType::F64) {
+        auto v = fetch(m, (double*)nullptr);
+        STL_CUDA(cudaStreamSynchronize(s));
+        h.assign(v.begin(), v.end());
+      } else {
+        auto v = fetch(m, (float*)nullptr);
+        STL_CUDA(cudaStreamSynchronize(s));
+        h.assign(v.begin(), v.end());
+      }
+      return h;
+    };
     auto rotp = [](i64 u, int k, int o2) {
       return ((4 * (u >> o2) + k) << o2) | (u & ((i64(1) << o2) - 1));
     };
@@ -1021,8 +1035,15 @@ class EngineImpl final : public Engine {
       const i64 f = c >> o2;
       return (((f & ~i64(3)) | ((f + k) & 3)) << o2) | (c & ((i64(1) << o2) - 1));
     };
-    std::vector<std::vector<int64_t>> rows;  // per stored row
+    // per stored row: (cell, weight) entries; the weight of a wavelet cell is
+    // its largest |coefficient|, of a decimation column |w|
+    std::vector<std::vector<std::pair<int64_t, double>>> rows;
     int nk = 1, o2_row = 0, o2_cell = 0;
+    auto cmax = [](const double* c) {
+      double m = 0.0;
+      for (int j = 0; j < 8; ++j) m = std::max(m, std::fabs(c[j]));
+      return m;
+    };
     if (kind == 0) {
       const ConvOp& op = conv_[level];
       nk = op.nk; o2_row = o2_cell = op.o2;
@@ -1031,56 +1052,61 @@ class EngineImpl final : public Engine {
         auto lc = fetch(op.m_lc, (uint16_t*)nullptr);
         auto cells = fetch(op.m_cells, (int32_t*)nullptr);
         auto rch = fetch(op.m_rowch, (uint8_t*)nullptr);
-        STL_CUDA(cudaStreamSynchronize(s));
+        auto coef = fetch_real(op.m_coef, DType::F32);
         for (i64 u = 0; u < op.n_rep; ++u) {
           const i64 tile = u / kMmaRows, ul = u % kMmaRows;
           for (int c = 0; c < rch[u]; ++c)
             for (int p = 0; p < 8; ++p) {
               const int pl = lc[((tile * (op.m_S / 8) + c) * kMmaRows + ul) * 8 + p];
               const int32_t cell = cells[tile * op.m_pc + pl];
-              if (cell >= 0) rows[u].push_back(cell);
+              if (cell >= 0) rows[u].push_back({cell, cmax(&coef[((i64)(8 * c + p) * op.n_rep + u) * 8])});
             }
         }
       } else {
         auto cell = fetch(op.cell, (int32_t*)nullptr);
-        STL_CUDA(cudaStreamSynchronize(s));
+        auto coef = fetch_real(op.coef, op.dtype);
         for (i64 u = 0; u < op.n_rep; ++u)
-          for (int sl = 0; sl < op.S; ++sl) rows[u].push_back(cell[(i64)sl * op.n_rep + u]);
+          for (int sl = 0; sl < op.S; ++sl)
+            rows[u].push_back({cell[(i64)sl * op.n_rep + u], cmax(&coef[((i64)sl * op.n_rep + u) * 8])});
       }
     } else {
       const DecOp& op = dec_[level];
       nk = op.nk; o2_row = op.co2; o2_cell = op.o2;
       rows.resize(op.n_rep_out);
       auto col = fetch(op.col, (int32_t*)nullptr);
-      std::vector<double> w(col.size());
-      if (op.dtype == DType::F64) {
-        auto wd = fetch(op.w, (double*)nullptr);
-        STL_CUDA(cudaStreamSynchronize(s));
-        w.assign(wd.begin(), wd.end());
-      } else {
-        auto wf = fetch(op.w, (float*)nullptr);
-        STL_CUDA(cudaStreamSynchronize(s));
-        w.assign(wf.begin(), wf.end());
-      }
+      auto w = fetch_real(op.w, op.dtype);
       for (i64 u = 0; u < op.n_rep_out; ++u)
-        for (int e = 0; e < op.W; ++e)
-          if (w[(i64)e * op.n_rep_out + u] != 0.0) rows[u].push_back(col[(i64)e * op.n_rep_out + u]);
+        for (int e = 0; e < op.W; ++e) {
+          const double v = w[(i64)e * op.n_rep_out + u];
+          if (v != 0.0) rows[u].push_back({col[(i64)e * op.n_rep_out + u], std::fabs(v)});
+        }
     }
+    // distinct cells (a padding slot repeats a real cell with zero
+    // coefficients: the largest weight is kept)
     width = 0;
     for (auto& r : rows) {
       std::sort(r.begin(), r.end());
-      r.erase(std::unique(r.begin(), r.end()), r.end());
+      std::vector<std::pair<int64_t, double>> m;
+      for (const auto& e : r) {
+        if (!m.empty() && m.back().first == e.first) m.back().second = std::max(m.back().second, e.second);
+        else m.push_back(e);
+      }
+      r.swap(m);
       width = std::max(width, (int)r.size());
     }
     const i64 npx = (i64)rows.size() * nk;
     out.assign((size_t)npx * width, -1);
+    weight.assign((size_t)npx * width, 0.0);
     for (i64 u = 0; u < (i64)rows.size(); ++u)
       for (int k = 0; k < nk; ++k) {
         const i64 p = nk == 4 ? rotp(u, k, o2_row) : u;
-        std::vector<int64_t> r;
-        for (int64_t c : rows[u]) r.push_back(nk == 4 ? rotc(c, k, o2_cell) : c);
+        std::vector<std::pair<int64_t, double>> r;
+        for (const auto& e : rows[u]) r.push_back({nk == 4 ? rotc(e.first, k, o2_cell) : e.first, e.second});
         std::sort(r.begin(), r.end());
-        std::copy(r.begin(), r.end(), out.begin() + (size_t)p * width);
+        for (size_t j = 0; j < r.size(); ++j) {
+          out[(size_t)p * width + j] = r[j].first;
+          weight[(size_t)p * width + j] = r[j].second;
+        }
       }
   }
 

@@ -102,7 +102,7 @@ struct ConvSpec {
   // FP32 full sky: 0 the coloured layout only (CUDA cores), 1 the tensor-core
   // layout for the forward and the coloured one for the adjoint, 2 the
   // tensor-core layout for both
-  int tensor_cores = 1;
+  int tensor_cores = 0;
   int ksz = 5, G = 4, gauge = 0;
   double eps = 0.0;
   const i64* d_grid = nullptr;  // sorted NESTED ids of the grid (device), nullptr: whole sky

@@ -43,9 +43,10 @@ struct Options {
   int device = 0;
   bool autotune = true;  // time the tile heights of the wavelet and decimation launches at prepare
   // FP32 full-sky wavelets on the tensor cores (3xTF32 mma.sync): 0 none
-  // (the CUDA-core kernels of the coloured layout), 1 the forward (the
-  // adjoint on the CUDA cores), 2 forward and adjoint
-  int tensor_cores = 1;
+  // (the CUDA-core kernels of the coloured layout, the default: as fast,
+  // a single layout, closer to FP64), 1 the forward (the adjoint on the
+  // CUDA cores), 2 forward and adjoint
+  int tensor_cores = 0;
   // Two channels and the plan of their cross terms only (c1 != c2: S1 of the
   // root-normalised z, S2, S3 and S4 in both channel orders), maps
   // [B][2][N]; the fields then hold 2 B maps (map 2 b + c).
@@ -175,10 +176,12 @@ class Engine {
   virtual size_t kept_field_bytes() const = 0;  // bytes of z and branches of every level (after prepare)
   // The integer tables of the operators, for exact checks: kind 0, the
   // sorted distinct input cells of every output pixel of level `level`'s
-  // wavelet; kind 1, the sorted fine cells of nonzero weight of every coarse
-  // pixel of the decimation from level `level` to `level` + 1.  Rows of the
-  // full level in pixel order, padded with -1 to the widest (width).
-  virtual void operator_rows(int level, int kind, std::vector<int64_t>& out, int& width) = 0;
+  // wavelet (weight: the cell's largest |coefficient|); kind 1, the sorted
+  // fine cells of nonzero weight of every coarse pixel of the decimation
+  // from level `level` to `level` + 1 (weight: |w|).  Rows of the full level
+  // in pixel order, padded with -1 (weight 0) to the widest (width).
+  virtual void operator_rows(int level, int kind, std::vector<int64_t>& out, std::vector<double>& weight,
+                             int& width) = 0;
   // Per level, the tile heights (rows of the field a thread takes) chosen
   // for: the wavelet of the maps, of the moduli, their adjoints, the
   // decimation of the maps (to the next level), of the moduli (from the

@@ -87,7 +87,7 @@ def lib():
             "stlp_patch_vjp": ([_VOID, _D, sz, u64, _D], C.c_int),
             "stlp_patch_forward_device": ([_VOID, u64, sz, u64, b, _D, _D], C.c_int),
             "stlp_patch_vjp_device": ([_VOID, _D, sz, u64, u64], C.c_int),
-            "stlp_operator_rows": ([_VOID, sz, C.c_int, C.POINTER(C.c_int64), sz, _SIZE], C.c_int),
+            "stlp_operator_rows": ([_VOID, sz, C.c_int, C.POINTER(C.c_int64), _D, sz, _SIZE], C.c_int),
             "stlp_memory": ([_SIZE, _SIZE, C.c_int], C.c_int),
             "stlp_terms_new": ([C.c_char_p], _VOID),
             "stlp_terms_free": ([_VOID], None),
@@ -188,7 +188,7 @@ class NativeEngine:
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
-                 prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=True, fields="keep",
+                 prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=False, fields="keep",
                  **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
@@ -206,9 +206,9 @@ class NativeEngine:
                            orientations=int(orientations), device=self.device, dtype=dtype)
         if not autotune:  # keep the default tile heights (no timing at prepare)
             self.config["autotune"] = False
-        # FP32 wavelets: True / "forward" (the default: forward on the tensor cores,
-        # adjoint on the CUDA cores), "all" (both on the tensor cores), False / "none"
-        if tensor_cores is not True and tensor_cores != "forward":
+        # FP32 wavelets: False / "none" (the default: CUDA cores), True / "forward"
+        # (forward on the tensor cores, adjoint on the CUDA cores), "all" (both)
+        if tensor_cores is not False and tensor_cores != "none":
             self.config["tensor_cores"] = tensor_cores if isinstance(tensor_cores, str) else bool(tensor_cores)
         if fields != "keep":  # "recompute": z and branches recomputed per level in the VJP; "auto"
             self.config["fields"] = fields
@@ -279,22 +279,24 @@ class NativeEngine:
             return values
 
     def operator_rows(self, level, kind="wavelet"):
-        """Integer tables of the device operators, [pixels, width] int64 padded
-        with -1, rows in pixel order: "wavelet", the sorted input cells each
-        pixel of `level` reads; "decimation", the fine cells of nonzero weight
-        of each coarse pixel of level + 1."""
+        """Integer tables of the device operators in pixel order: (cells [pixels,
+        width] int64 padded with -1, weights [pixels, width]).  "wavelet": the
+        sorted input cells each pixel of `level` reads (weight: the cell's
+        largest |coefficient|); "decimation": the fine cells of nonzero weight
+        of each coarse pixel of level + 1 (weight: |w|)."""
         k = {"wavelet": 0, "decimation": 1}[kind]
         with self._mutex:
             self._open()
             need = C.c_size_t(0)
-            if self._lib.stlp_operator_rows(self._handle, int(level), k, None, 0, C.byref(need)):
+            if self._lib.stlp_operator_rows(self._handle, int(level), k, None, None, 0, C.byref(need)):
                 raise _error()
             rows = 12 * (self.nside >> (level + k)) ** 2
             out = np.empty((rows, need.value), dtype=np.int64)
+            wts = np.empty((rows, need.value))
             if self._lib.stlp_operator_rows(self._handle, int(level), k, out.ctypes.data_as(C.POINTER(C.c_int64)),
-                                            need.value, C.byref(need)):
+                                            _ptr(wts), need.value, C.byref(need)):
                 raise _error()
-            return out
+            return out, wts
 
     def set_masks(self, masks):
         """Averages every coefficient over each of K masks from the next forward

@@ -1,7 +1,8 @@
 """The FP32 wavelets on the tensor cores (3xTF32 mma.sync over the
-tensor-core operator layout) against the FP32 CUDA-core kernels of the
-coloured layout and the FP64 path: statistics under the 1e-6 family
-criterion, gradients, bit-reproducibility, and the layout each level gets."""
+tensor-core operator layout; engine option tensor_cores "forward" or "all")
+against the FP32 CUDA-core kernels of the coloured layout (the default) and
+the FP64 path: statistics under the 1e-6 family criterion, gradients,
+bit-reproducibility, and the layout each level gets."""
 import numpy as np
 import pytest
 
@@ -44,7 +45,7 @@ def test_layout_per_level(stl):
     """FP32 levels above nside 32 hold the tensor-core layout (for the
     forward, with the coloured one for the adjoint by default; for both with
     "all"); the FP64 coarse levels and every level with tensor_cores off
-    hold the coloured one."""
+    hold the coloured one (the default)."""
     for mode, want in ((True, "tensor_cores+coloured"), ("all", "tensor_cores"), (False, "coloured")):
         e = stl.NativeEngine(128, 5, dtype="float32", tensor_cores=mode)
         e.prepare()
@@ -60,8 +61,8 @@ def test_tensor_cores_match_cuda_cores_and_fp64(stl, nside, J, B):
     x = maps(nside + B, B, nside)
     t = maps(1000 + nside, B, nside)
     out = {}
-    for name, kw in (("tc", dict(dtype="float32")), ("tca", dict(dtype="float32", tensor_cores="all")),
-                     ("cc", dict(dtype="float32", tensor_cores=False)), ("f64", dict(dtype="float64"))):
+    for name, kw in (("tc", dict(dtype="float32", tensor_cores=True)), ("tca", dict(dtype="float32", tensor_cores="all")),
+                     ("cc", dict(dtype="float32")), ("f64", dict(dtype="float64"))):
         e = stl.NativeEngine(nside, J, batch=B, **kw)
         tv, _ = e.forward(t, generation=1)
         v, _ = e.forward(x, generation=2)
