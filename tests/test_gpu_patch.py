@@ -145,3 +145,33 @@ def test_batched_discs_match_one_engine_per_disc(stl):
                 for part in (np.real, np.imag):
                     assert np.max(np.abs(part(a) - part(r)) / (1e-6 * scale + 1e-6 * np.abs(part(r)))) <= 1.0
         assert np.max(np.abs(runs["batch32"][2][k] - g[k])) <= 1e-5 * np.max(np.abs(g[k]))
+
+
+def test_config4_subset_batched_equals_one_engine_per_disc(stl):
+    """32 discs of the ragged workload of config 4 (nside 512, J 5, centres
+    uniform on the sphere, pixel counts log-uniform in [1024, 65536]): the
+    segmented engine holding all of them gives every disc's statistics and
+    gradients as an engine of its own does (FP64; the same kernels over
+    segment-bounded tables)."""
+    nside, J, n = 512, 5, 32
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    counts = np.exp(rng.uniform(np.log(1024.0), np.log(65536.0), n))
+    omega = 4.0 * np.pi / (12.0 * nside * nside)
+    radii = np.degrees(np.arccos(1.0 - counts * omega / (2.0 * np.pi)))
+    batched = stl.PatchEngine(nside, J, dtype="float64", autotune=False)
+    single = stl.PatchEngine(nside, J, dtype="float64", autotune=False, group_pixels=1)
+    ids = batched.select(v, radii)
+    assert [i.size for i in single.select(v, radii)] == [i.size for i in ids]
+    xs = [np.random.default_rng(100 + k).standard_normal(i.size) for k, i in enumerate(ids)]
+    vb, varb = batched.forward(xs, generation=1)
+    vs, vars_ = single.forward(xs, generation=1)
+    assert close_ratio(vb, vs, 1e-11, 1e-10) <= 1.0
+    assert close_ratio(varb, vars_, 1e-11, 1e-10) <= 1.0
+    cot = rng.standard_normal(vb.shape) + 1j * rng.standard_normal(vb.shape)
+    gb = batched.vjp(cot, generation=1)
+    gs = single.vjp(cot, generation=1)
+    for a, b in zip(gb, gs):
+        assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))
+    assert batched.info()["groups"] == 1 and single.info()["groups"] == n
