@@ -238,6 +238,12 @@ int or_engine_set_masks(void* hv, const double* w, i64 K) {
     return 0;
   })
 }
+int or_engine_set_mask_levels(void* hv, const double* w, i64 K) {
+  GUARD(-1, {
+    ((EngineH*)hv)->e.set_mask_levels(w, K);
+    return 0;
+  })
+}
 i64 or_engine_native_pixels(void* hv, i64* out) {
   auto& e = ((EngineH*)hv)->e;
   i64 np = (i64)e.plan.size();

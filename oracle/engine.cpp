@@ -106,6 +106,30 @@ void Engine::set_masks(const double* w0, i64 Kc) {  // mask.rs:203-228
   has_masks = true;
 }
 
+void Engine::set_mask_levels(const double* w, i64 Kc) {  // mask.rs:75-82
+  if (Kc <= 0) { has_masks = false; masks = Masks(); return; }
+  masks = Masks();
+  for (i64 k = 0; k < Kc; ++k) {
+    std::vector<std::vector<double>> per;
+    std::vector<i64> cnt;
+    for (int n = 0; n < levels; ++n) {
+      std::vector<double> level(npix(n));
+      i64 c = 0;
+      for (i64 i = 0; i < npix(n); ++i) {
+        level[i] = w[i] != 0.0 ? 1.0 : 0.0;
+        c += w[i] != 0.0;
+      }
+      w += npix(n);
+      if (c == 0) throw std::runtime_error("empty mask at some level");
+      cnt.push_back(c);
+      per.push_back(level);
+    }
+    masks.weights.push_back(per);
+    masks.counts.push_back(cnt);
+  }
+  has_masks = true;
+}
+
 std::vector<double> Engine::decimate(int d, const std::vector<double>& x, i64 rows) const {
   i64 n = down[d].n_cols, nc = down[d].n_rows;
   std::vector<double> y((size_t)rows * nc);

@@ -51,6 +51,8 @@ struct Engine {
   void init(i64 nside, int J, int L, int ksz, Gauge gauge, int B, int C, bool fewer, const std::vector<int>& dg,
             bool cross_only, size_t cache_budget);
   void set_masks(const double* w0, i64 K);
+  // masks given at every level ([K][levels][N_n] indicators, mask.rs:75-82)
+  void set_mask_levels(const double* w, i64 K);
   void load(const double* x);
   void load_levels(const double* x);
   // values [B][K][np] complex; second [B][K][np] when moments
