@@ -37,8 +37,13 @@ void stlp_string_free(char* p);
 /* New handle from a JSON config: nside (128), j (7), batch (1), kernel (5),
  * orientations (4), backend ("gpu"; "cpu" is refused: no CPU fallback),
  * device (0), dtype ("float64" | "float32": field precision; sums stay
- * FP64).  Unknown keys are ignored.  The device operators are built on
- * first use (or by stlp_prepare).  NULL on failure.  (lib.rs:280-351) */
+ * FP64), cross (false), spin (0 | 2), spin_kernel (5: 3, 5, 7 or 9),
+ * spin_pyramid ("scalar" | "transported"), spin_a (2 | 0, with cross).
+ * Spin 2: maps are (Q, U) [batch, 2, 12 nside^2] (cross: the first fields
+ * [batch, 1 or 2, npix] then the second [batch, 2, npix]); values
+ * [batch, 2 (chi_E, chi_B), K, ncoeff]; cotangents of the maps' shape.
+ * Unknown keys are ignored.  The device operators are built on first use
+ * (or by stlp_prepare).  NULL on failure.  (lib.rs:280-351) */
 StlpHandle* stlp_new(const char* config);
 
 /* Frees a handle (NULL ignored).  (lib.rs:354-359) */
@@ -218,11 +223,26 @@ int stlp_terms_marginal(StlpTerms* h, uint64_t x, uint64_t perm, uint64_t t_sort
 /* g += a b (b 0: g += a), n values (terms.rs:271-275) */
 int stlp_terms_add_product(StlpTerms* h, uint64_t g, uint64_t a, uint64_t b, size_t n);
 
-/* Entry points of subsystems outside this engine (spin-2 front end,
- * spectrum, U-Net training).  They exist so that native.py's signature
- * table binds; each returns failure with stlp_last_error() naming the
- * subsystem as not built.  (lib.rs:628-643, 1178-1492; unet.rs) */
+/* Spin 2: the (Q, U) of `level` (means of the children turned into the
+ * parents' frames) and its (chi_E, chi_B), each [batch, 2, 12 (nside /
+ * 2^level)^2], of the maps x [batch, 2, 12 nside^2]; level 0 only with the
+ * scalar pyramid; not for cross handles.  (lib.rs:625-643) */
 int stlp_spin_fields(StlpHandle* h, const double* x, size_t n, size_t level, double* qu, double* chi);
+
+/* Spin 2: the device-built operator rows of `level` for exact checks:
+ * kind 0 the stencil -(d_x - i d_y)^2 (cells and complex weights of every
+ * pixel), kind 1 the transported means (the 4 children of every coarse
+ * pixel of level + 1); cells [rows][width] (-1 past a row's end), weights
+ * [rows][width][2]; *needed = the rows' width (cells / weights may be NULL
+ * to ask for it).  No reference counterpart (the reference's operators are
+ * host structures, crates/stl-core/src/spin.rs:88-157). */
+int stlp_spin_rows(StlpHandle* h, size_t level, int kind, int64_t* cells, double* weights, size_t width,
+                   size_t* needed);
+
+/* Entry points of subsystems outside this engine (spectrum, U-Net
+ * training).  They exist so that native.py's signature table binds; each
+ * returns failure with stlp_last_error() naming the subsystem as not
+ * built.  (lib.rs:1178-1492; unet.rs) */
 void* stlp_spec_new(const char* config);
 void stlp_spec_free(void* h);
 char* stlp_spec_info(void* h);

@@ -153,8 +153,8 @@ def scalar_pyramid_valid(nside0, levels, valid0):
         fine = out[-1]
         bad = np.flatnonzero(fine == 0.0)
         rings = down_rings(nside0, d)
-        if rings >= nside:
-            reach = np.arange(12 * nside * nside) if bad.size else bad
+        if rings >= nside:  # the dilation covers the whole level (neighbours.rs:31-35)
+            reach = np.arange(12 * nside * nside)
         else:
             reach = np.unique(np.concatenate([O.kth_neighbourhood(p, nside, rings) for p in bad])) if bad.size else bad
         nxt = np.ones(12 * (nside // 2) ** 2)

@@ -22,6 +22,7 @@
 #include "json.hpp"
 #include "lbfgs.hpp"
 #include "scatcov.hpp"
+#include "spin.hpp"
 #include "../../include/stl_b200.h"
 
 using namespace stl;
@@ -75,11 +76,16 @@ long long synthesize_device(Engine& e, double* x, size_t n, const double* target
 
 struct StlpHandle {
   std::unique_ptr<Engine> engine;
+  // spin 2: (Q, U) maps through the spin front end; the engine's batch is
+  // twice the handle's (chi_E and chi_B of every map)
+  std::unique_ptr<SpinFront> spin;
   uint64_t id = 0;
   bool has_current = false;
   Identity current;
   int device = 0;
-  size_t input_len() const { return (size_t)engine->options().B * (size_t)engine->npix(0); }
+  size_t input_len() const {
+    return spin ? spin->input_len() : (size_t)engine->options().B * (size_t)engine->npix(0);
+  }
   // B K np: K masks (1 without)
   size_t values_len() const {
     return (size_t)engine->value_batch() * std::max(1, engine->nmasks()) * engine->plan().size();
@@ -130,12 +136,36 @@ StlpHandle* stlp_new(const char* config) {
     require(fields == "keep" || fields == "recompute" || fields == "auto", "fields must be auto, keep or recompute");
     o.recompute = fields == "recompute";
     o.fields_auto = fields == "auto";
-    require(v.integer("spin", 0) == 0, "spin-2 statistics are not built in this library");
+    // spin 2 (lib.rs:301-319): "spin" 0 or 2, "spin_kernel" 3, 5, 7 or 9,
+    // "spin_pyramid" scalar (default) or transported, "spin_a" 0 or 2 (cross)
+    const long long spin = v.integer("spin", 0);
+    require(spin == 0 || spin == 2, "spin must be 0 or 2, not " + std::to_string(spin));
+    const std::string pyramid = v.string("spin_pyramid", "scalar");
+    require(pyramid == "scalar" || pyramid == "transported",
+            "spin_pyramid must be transported or scalar, not " + jstr(pyramid));
+    const int spin_a = (int)v.integer("spin_a", 2);
+    require(spin_a == 0 || spin_a == 2, "spin_a must be 0 or 2");
+    const int spin_kernel = (int)v.integer("spin_kernel", 5);
     require(o.nside > 0 && (o.nside & (o.nside - 1)) == 0, "nside must be a power of two");
+    SpinConfig sc;
+    if (spin == 2) {
+      require(!o.cross || pyramid == "scalar", "spin 2: cross statistics need the scalar pyramid");
+      require(spin_kernel == 3 || spin_kernel == 5 || spin_kernel == 7 || spin_kernel == 9,
+              "spin_kernel must be 3, 5, 7 or 9");
+      sc.nside = o.nside;
+      sc.levels = o.J;
+      sc.kernel = spin_kernel;
+      sc.transported = pyramid == "transported";
+      sc.cross = o.cross;
+      sc.spin_a = spin_a;
+      sc.batch = o.B;
+      o.B = 2 * o.B;  // the engine sees chi_E and chi_B of every map as two of its maps
+    }
     auto h = std::make_unique<StlpHandle>();
     h->engine = Engine::create(o);
     h->device = o.device;
     h->id = g_next_id.fetch_add(1);
+    if (spin == 2) h->spin = SpinFront::create(sc, h->engine->stream());
     return h.release();
   });
 }
@@ -154,6 +184,7 @@ int stlp_prepare(StlpHandle* h) {
     require(h != nullptr, "null handle");
     h->activate();
     h->engine->prepare();
+    if (h->spin) h->spin->prepare();
     return 0;
   });
 }
@@ -172,6 +203,7 @@ int stlp_set_stream(StlpHandle* h, uint64_t stream) {
   return guard<int>(-1, [&] {
     require(h != nullptr, "null handle");
     h->engine->set_stream(reinterpret_cast<cudaStream_t>(stream));
+    if (h->spin) h->spin->set_stream(reinterpret_cast<cudaStream_t>(stream));
     return 0;
   });
 }
@@ -188,9 +220,16 @@ char* stlp_info(StlpHandle* h) {
        << ", \"cross\": " << (o.cross ? "true" : "false")
        << ", \"dtype\": " << jstr(o.fp32 ? "float32 fields, float64 sums/complex128" : "float64/complex128")
        << ", \"fewer\": false, \"orientations\": " << o.L << ", \"kernel\": " << o.ksz
-       << ", \"levels\": " << e.levels() << ", \"masks\": " << e.nmasks() << ", \"spin\": 0, \"device\": " << o.device
+       << ", \"levels\": " << e.levels() << ", \"masks\": " << e.nmasks() << ", \"spin\": " << (h->spin ? 2 : 0)
+       << ", \"device\": " << o.device
        << ", \"conv\": \"folded-stencil\", \"fields\": "
        << jstr(e.recomputes() ? "recompute" : "keep");
+    if (h->spin) {
+      const SpinConfig& sc = h->spin->config();
+      js << ", \"spin_kernel\": " << sc.kernel << ", \"spin_pyramid\": " << jstr(sc.transported ? "transported" : "scalar")
+         << ", \"spin_a\": " << (sc.cross ? std::to_string(sc.spin_a) : std::string("null"))
+         << ", \"spin_bytes\": " << h->spin->bytes() << ", \"spin_batch\": " << sc.batch;
+    }
     js << ", \"device_memory\": {\"operator_bytes\": " << e.operator_bytes() << ", \"field_bytes\": " << e.field_bytes()
        << ", \"live_bytes\": " << device_bytes_live() << ", \"peak_bytes\": " << device_bytes_peak()
        << ", \"kept_field_bytes\": " << e.kept_field_bytes() << "}";
@@ -292,7 +331,8 @@ int stlp_set_masks(StlpHandle* h, const double* weights, size_t k) {
     require(k == 0 || weights != nullptr, "null mask weights");
     h->has_current = false;
     h->activate();
-    h->engine->set_masks(weights, k);
+    if (h->spin && k > 0) h->engine->set_mask_levels(h->spin->mask_levels(weights, k));  // eroded, every level
+    else h->engine->set_masks(weights, k);
     return 0;
   });
 }
@@ -317,7 +357,8 @@ int stlp_forward(StlpHandle* h, const double* x, size_t n, uint64_t generation, 
       for (size_t i = 0; i < n; ++i) require(std::isfinite(x[i]), "input map contains non-finite values");
     h->activate();
     h->has_current = false;
-    h->engine->load_host(x);
+    if (h->spin) h->spin->load_host(*h->engine, x);
+    else h->engine->load_host(x);
     return forward_common(h, generation, member, objective, moments, out, var);
   });
 }
@@ -330,7 +371,8 @@ int stlp_forward_device(StlpHandle* h, uint64_t x, size_t n, int f32, uint64_t g
     require(!moments || var != nullptr, "moments need a variance buffer");
     h->activate();
     h->has_current = false;
-    h->engine->load_device(reinterpret_cast<const void*>(x), f32 != 0);
+    if (h->spin) h->spin->load_device(*h->engine, reinterpret_cast<const void*>(x), f32 != 0);
+    else h->engine->load_device(reinterpret_cast<const void*>(x), f32 != 0);
     return forward_common(h, generation, member, objective, moments, out, var);
   });
 }
@@ -347,7 +389,8 @@ int stlp_vjp(StlpHandle* h, const double* cot, size_t n, uint64_t generation, ui
     require(h != nullptr && cot != nullptr && out != nullptr, "null argument");
     check_identity(h, generation, member, objective, n);
     h->activate();
-    h->engine->reverse_host(cot, out);
+    if (h->spin) h->spin->reverse_host(*h->engine, cot, out);
+    else h->engine->reverse_host(cot, out);
     return 0;
   });
 }
@@ -358,7 +401,8 @@ int stlp_vjp_device(StlpHandle* h, const double* cot, size_t n, uint64_t generat
     require(h != nullptr && cot != nullptr && out != 0, "null argument");
     check_identity(h, generation, member, objective, n);
     h->activate();
-    h->engine->reverse_device(cot, reinterpret_cast<void*>(out), f32 != 0);
+    if (h->spin) h->spin->reverse_device(*h->engine, cot, reinterpret_cast<void*>(out), f32 != 0);
+    else h->engine->reverse_device(cot, reinterpret_cast<void*>(out), f32 != 0);
     return 0;
   });
 }
@@ -367,6 +411,7 @@ int64_t stlp_synthesize_device(StlpHandle* h, uint64_t x, size_t n, const double
                                const double* weights, const char* options, double* losses, size_t n_losses) {
   return guard<int64_t>(-1, [&]() -> int64_t {
     require(h != nullptr && x != 0 && target != nullptr, "null argument");
+    require(!h->spin, "the device synthesis takes scalar maps: spin-2 handles synthesise through stlp_lbfgs");
     require(n == h->input_len(), "map shape mismatch");
     require(n_target == h->values_len(), "target shape mismatch");
     const lbfgs::Options o = lbfgs::parse_options(options);
@@ -388,7 +433,8 @@ StlpSnapshot* stlp_checkpoint(StlpHandle* h) {
     auto s = std::make_unique<StlpSnapshot>();
     s->identity = h->current;
     s->owner = h->id;
-    h->engine->save_state(s->maps);
+    if (h->spin) h->spin->save_input(s->maps);  // the (Q, U) maps: the front end runs again at restore
+    else h->engine->save_state(s->maps);
     return s.release();
   });
 }
@@ -406,7 +452,12 @@ int stlp_restore(StlpHandle* h, const StlpSnapshot* s, uint64_t generation, uint
     h->has_current = false;
     // The forward state is recomputed from the saved maps: the sweeps are
     // deterministic, so the restored fields equal the checkpointed ones.
-    h->engine->load_state(s->maps);
+    if (h->spin) {
+      require(s->maps.size() == h->input_len(), "checkpoint of another configuration");
+      h->spin->load_host(*h->engine, s->maps.data());
+    } else {
+      h->engine->load_state(s->maps);
+    }
     std::vector<double> values(2 * h->values_len());
     h->engine->forward(false, values.data(), nullptr);
     h->current = s->identity;
@@ -426,6 +477,48 @@ int stlp_forward_levels(StlpHandle* h, const double* x, size_t n, double* out) {
     h->has_current = false;  // a validation sweep: no vjp or checkpoint follows it
     h->engine->load_levels(x);
     h->engine->forward(false, out, nullptr);
+    return 0;
+  });
+}
+
+int stlp_spin_fields(StlpHandle* h, const double* x, size_t n, size_t level, double* qu, double* chi) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && x != nullptr && qu != nullptr && chi != nullptr, "null argument");
+    require(h->spin != nullptr, "not a spin-2 handle");
+    require(!h->spin->config().cross, "spin fields of auto handles only");
+    require(n == h->input_len(), "input shape mismatch");
+    const int levels = h->spin->config().transported ? h->engine->levels() : 1;
+    require(level < (size_t)levels, "level out of range");
+    for (size_t i = 0; i < n; ++i) require(std::isfinite(x[i]), "input map contains non-finite values");
+    h->activate();
+    h->spin->fields(x, (int)level, qu, chi);
+    return 0;
+  });
+}
+
+int stlp_spin_rows(StlpHandle* h, size_t level, int kind, int64_t* cells, double* weights, size_t width,
+                   size_t* needed) {
+  return guard<int>(-1, [&] {
+    require(h != nullptr && needed != nullptr, "null argument");
+    require(h->spin != nullptr, "not a spin-2 handle");
+    require(kind == 0 || kind == 1, "kind must be 0 (stencil) or 1 (transported means)");
+    h->activate();
+    std::vector<int64_t> c;
+    std::vector<double> w;
+    int wd = 0;
+    h->spin->export_rows((int)level, kind, c, w, wd);
+    *needed = (size_t)wd;
+    if (cells && width >= (size_t)wd && wd > 0) {
+      const size_t rows = c.size() / (size_t)wd;
+      for (size_t r = 0; r < rows; ++r) {
+        std::copy(c.begin() + r * wd, c.begin() + (r + 1) * wd, cells + r * width);
+        std::fill(cells + r * width + wd, cells + (r + 1) * width, (int64_t)-1);
+        if (weights) {
+          std::copy(w.begin() + 2 * r * wd, w.begin() + 2 * (r + 1) * wd, weights + 2 * r * width);
+          std::fill(weights + 2 * (r * width + wd), weights + 2 * (r + 1) * width, 0.0);
+        }
+      }
+    }
     return 0;
   });
 }

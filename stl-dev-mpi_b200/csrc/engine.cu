@@ -520,6 +520,15 @@ class EngineImpl final : public Engine {
     }
     upload_masks(levels);
   }
+  void set_mask_levels(const std::vector<std::vector<std::vector<uint8_t>>>& levels) override {
+    if (grid_mode()) throw std::runtime_error("a patch engine averages its core: no masks");
+    for (const auto& lv : levels) {
+      if ((int)lv.size() != levels_) throw std::runtime_error("masks of every level expected");
+      for (int d = 0; d < levels_; ++d)
+        if ((i64)lv[d].size() != npix(d)) throw std::runtime_error("mask size mismatch");
+    }
+    upload_masks(levels);
+  }
   int nmasks() const override { return kmask_.empty() || grid_mode() ? 0 : K_; }
   i64 mask_count(int k, int n) const override { return count(k, n); }
 
@@ -784,6 +793,22 @@ class EngineImpl final : public Engine {
     levels_given_ = true;
   }
 
+  void load_device_levels(const double* const* x) override {
+    prepare();
+    for (int d = 0; d < levels_; ++d) {
+      double* c = xc_.as<double>() + (size_t)d * opt_.B;
+      prof_.launch(Profiler::ELEM, 3, opt_.B * npix(d) * (2.0 * 8 + esz(d)), 0.0, stream_, [&] {
+        row_means<double>(x[d], false, false, npix(d), opt_.B, mpart_.as<double>(), c, stream_);
+        typed(d, [&](auto t) {
+          using U = typename decltype(t)::type;
+          to_pixel_major<double, U>(x[d], X_[d].as<U>(), npix(d), opt_.B, stream_, c);
+        });
+      });
+    }
+    loaded_ = true;
+    levels_given_ = true;
+  }
+
   void load_device(const void* x, bool f32) override {
     prepare();
     if (f32) load_maps(static_cast<const float*>(x));
@@ -987,6 +1012,19 @@ class EngineImpl final : public Engine {
         else to_map_major<U, double>(gX_[0].as<U>(), static_cast<double*>(out), npix(0), opt_.B, stream_);
       });
     });
+    STL_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  void reverse_levels(const double* cot, double* const* out) override {
+    if (!levels_given_) throw std::runtime_error("per-level cotangents need maps given at every level");
+    reverse_impl(cot);
+    for (int d = 0; d < levels_; ++d)
+      prof_.launch(Profiler::ELEM, 1, (double)opt_.B * npix(d) * (8.0 + esz(d)), 0.0, stream_, [&] {
+        typed(d, [&](auto t) {
+          using U = typename decltype(t)::type;
+          to_map_major<U, double>(gX_[d].as<U>(), out[d], npix(d), opt_.B, stream_);
+        });
+      });
     STL_CUDA(cudaStreamSynchronize(stream_));
   }
 
@@ -1349,7 +1387,7 @@ class EngineImpl final : public Engine {
                    conv_adjoint<U>(op, gZ_.as<U>(), B, gX_[n].as<U>(), false, s, adj_ptr(), err_.as<int>(),
                                    fuse ? &madd : nullptr, tile(n, T_ADJ_Z));
                  });
-    if (n + 1 < levels_)
+    if (n + 1 < levels_ && !levels_given_)  // maps given per level: no chain through the decimation
       prof_.launch(Profiler::DEC, 1, dec_bytes(dec_[n], B, true) + (double)B * N * sz, dec_flops(dec_[n], B, true), s,
                    [&] {
                      typed(n + 1, [&](auto ti) {

@@ -127,10 +127,17 @@ class Engine {
   // [B][npix(d)]): the next forward uses them instead of the decimation
   // pyramid of level 0.
   virtual void load_levels(const double* x) = 0;
+  // Maps given at every level on the device (map-major f64 [B][N_d] each,
+  // d = 0 .. levels - 1): the decimation of the maps is skipped (the spin-2
+  // transported pyramid feeds its own fields of every level)
+  virtual void load_device_levels(const double* const* x) = 0;
   // Averages over k masks (level-0 indicators [k][npix(0)], nonzero: in the
   // mask) from the next forward on, or over every pixel (k = 0); values,
   // variances and cotangents are then [B][K][np].
   virtual void set_masks(const double* w, size_t k) = 0;
+  // masks given at every level: [k][level][pixel] indicators, level d + 1
+  // not derived from level d (the spin-2 front end erodes them itself)
+  virtual void set_mask_levels(const std::vector<std::vector<std::vector<uint8_t>>>& levels) = 0;
   virtual int nmasks() const = 0;                   // 0: no masks
   virtual i64 mask_count(int k, int n) const = 0;   // pixels mask k averages at level n
   // Forward sweep on the loaded maps: values [B][np] complex (interleaved),
@@ -140,6 +147,10 @@ class Engine {
   // complex interleaved (host).  Output to host f64 or device f64/f32.
   virtual void reverse_host(const double* cot, double* out) = 0;
   virtual void reverse_device(const double* cot, void* out, bool f32) = 0;
+  // After a forward of maps given at every level: the map cotangent of every
+  // level (its own terms, without the chain through the decimations),
+  // map-major f64 [B][N_d] into the device buffers out[d]
+  virtual void reverse_levels(const double* cot, double* const* out) = 0;
   // The synthesis objective on the device: loss = sum_o w_(o mod np)
   // |S_o(x) - T_o|^2 over the coefficients [B][K][np] of the maps x (f64
   // [B][N_0], device), its gradient into g (f64, device) and the loss into

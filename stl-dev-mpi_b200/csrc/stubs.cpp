@@ -1,6 +1,5 @@
 // Entry points of the reference's stl-bridge that belong to subsystems
-// outside this engine: the spin-2 front end (crates/stl-core/src/spin.rs),
-// the spectrum engine (crates/stl-core/src/sht.rs) and the U-Net training
+// outside this engine: the spectrum engine (crates/stl-core/src/sht.rs) and the U-Net training
 // (crates/stl-bridge/src/unet.rs).  The reference's native.py binds every
 // name of its signature table when it loads the library, so each is
 // exported here and fails with a message naming the subsystem.
@@ -25,9 +24,6 @@ void* fail_ptr(const char* what) {
 
 extern "C" {
 
-int stlp_spin_fields(StlpHandle*, const double*, size_t, size_t, double*, double*) {
-  return fail("the spin-2 front end (stlp_spin_fields)");
-}
 void* stlp_spec_new(const char*) { return fail_ptr("the spectrum engine (stlp_spec_new)"); }
 void stlp_spec_free(void*) {}
 char* stlp_spec_info(void*) { return (char*)fail_ptr("the spectrum engine (stlp_spec_info)"); }

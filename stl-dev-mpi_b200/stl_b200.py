@@ -89,6 +89,8 @@ def lib():
             "stlp_patch_vjp_device": ([_VOID, _D, sz, u64, u64], C.c_int),
             "stlp_operator_rows": ([_VOID, sz, C.c_int, C.POINTER(C.c_int64), _D, sz, _SIZE], C.c_int),
             "stlp_memory": ([_SIZE, _SIZE, C.c_int], C.c_int),
+            "stlp_spin_fields": ([_VOID, _D, sz, sz, _D, _D], C.c_int),
+            "stlp_spin_rows": ([_VOID, sz, C.c_int, C.POINTER(C.c_int64), _D, sz, _SIZE], C.c_int),
             "stlp_terms_new": ([C.c_char_p], _VOID),
             "stlp_terms_free": ([_VOID], None),
             "stlp_terms_set_stream": ([_VOID, u64], C.c_int),
@@ -189,7 +191,7 @@ class NativeEngine:
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
                  prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=False, fields="keep",
-                 **unused):
+                 spin=0, spin_kernel=5, spin_pyramid="scalar", spin_a=2, **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -199,7 +201,22 @@ class NativeEngine:
         self.npix = 12 * self.nside ** 2
         # cross: two channels and the plan of their cross terms, maps [batch, 2, npix] (native.py's cross engine)
         self.cross, self.channels = bool(cross), 2 if cross else 1
-        self._map_shape = (self.batch, 2, self.npix) if cross else (self.batch, self.npix)
+        # spin 2: (Q, U) maps, statistics of chi_E and chi_B (values [batch, 2, (K,) ncoeff]); with cross,
+        # pairs (a, b) of a (Q, U) or scalar field a (spin_a 2 or 0) and a (Q, U) field b
+        if spin not in (0, 2) or spin_kernel not in (3, 5, 7, 9):
+            raise ValueError("spin is 0 or 2 and spin_kernel 3, 5, 7 or 9")
+        if spin_pyramid not in ("scalar", "transported") or spin_a not in (0, 2):
+            raise ValueError("spin_pyramid is 'scalar' or 'transported', spin_a 0 or 2")
+        if spin and cross and spin_pyramid != "scalar":
+            raise ValueError("spin-2 cross statistics run on the scalar pyramid")
+        self.spin = int(spin)
+        self.spin_a = int(spin_a) if spin and cross else None
+        if spin and cross:
+            self._map_shape = (self.batch, (2 if spin_a == 2 else 1) + 2, self.npix)
+        elif spin or cross:
+            self._map_shape = (self.batch, 2, self.npix)
+        else:
+            self._map_shape = (self.batch, self.npix)
         self.dtype = dtype
         self.device = int(device)
         self.config = dict(nside=self.nside, j=self.j, batch=self.batch, backend="gpu", kernel=int(kernel),
@@ -214,6 +231,8 @@ class NativeEngine:
             self.config["fields"] = fields
         if cross:
             self.config["cross"] = True
+        if spin:
+            self.config.update(spin=2, spin_kernel=int(spin_kernel), spin_pyramid=spin_pyramid, spin_a=int(spin_a))
         if autotune_cache:  # a file of tile heights timed before (read, then extended)
             self.config["autotune_cache"] = str(autotune_cache)
         self._lib = lib()
@@ -341,7 +360,73 @@ class NativeEngine:
         return int(n), losses[:min(int(n), losses.size)]
 
     def _shape(self):
-        return (self.batch, self.nmasks, self.ncoeff) if self.nmasks else (self.batch, self.ncoeff)
+        head = (self.batch, 2) if self.spin else (self.batch,)
+        return head + ((self.nmasks, self.ncoeff) if self.nmasks else (self.ncoeff,))
+
+    def spin_fields(self, maps, level=0):
+        """Spin 2: ((Q, U), (chi_E, chi_B)) of `level`, each [batch, 2, npix of the
+        level] (the scalar pyramid has level 0 only; native.py:305-317)."""
+        if not self.spin:
+            raise RuntimeError("spin_fields needs NativeEngine(..., spin=2)")
+        with self._mutex:
+            self._open()
+            x = np.ascontiguousarray(maps, dtype=np.float64).reshape(self._map_shape)
+            n = 12 * (self.nside >> int(level)) ** 2
+            qu = np.empty((self.batch, 2, n))
+            chi = np.empty((self.batch, 2, n))
+            if self._lib.stlp_spin_fields(self._handle, _ptr(x), x.size, int(level), _ptr(qu), _ptr(chi)):
+                raise _error()
+            return qu, chi
+
+    def spin_rows(self, level, kind="stencil"):
+        """Spin 2: the device-built operator rows (cells [rows, width] int64 padded
+        with -1, complex weights [rows, width]): "stencil" the chi operator of
+        `level`, "means" the transported means into level + 1."""
+        k = {"stencil": 0, "means": 1}[kind]
+        with self._mutex:
+            self._open()
+            need = C.c_size_t(0)
+            if self._lib.stlp_spin_rows(self._handle, int(level), k, None, None, 0, C.byref(need)):
+                raise _error()
+            rows = 12 * (self.nside >> (level + k)) ** 2
+            cells = np.empty((rows, need.value), dtype=np.int64)
+            w = np.empty((rows, need.value), dtype=np.complex128)
+            if self._lib.stlp_spin_rows(self._handle, int(level), k, cells.ctypes.data_as(C.POINTER(C.c_int64)),
+                                        _ptr(w.view(np.float64)), need.value, C.byref(need)):
+                raise _error()
+            return cells, w
+
+    def forward_cross(self, a, b, generation=0, member=0, objective="gaussian", moments=False):
+        """Cross statistics of the pairs (a, b) (cross=True): a, b [batch, npix], or
+        with spin 2 b [batch, 2, npix] (Q, U) and a [batch, 2, npix] or [batch, npix]."""
+        if not self.cross:
+            raise RuntimeError("forward_cross needs NativeEngine(..., cross=True)")
+        if self.spin:
+            return self.forward((a, b), generation, member, objective, moments)
+        a = np.asarray(a, dtype=np.float64).reshape(self.batch, self.npix)
+        b = np.asarray(b, dtype=np.float64).reshape(self.batch, self.npix)
+        return self.forward(np.stack([a, b], 1), generation, member, objective, moments)
+
+    def vjp_cross(self, cotangents, generation=0, member=0, objective="gaussian"):
+        """(grad_a, grad_b) in the shapes of a and b, after forward_cross."""
+        g = self.vjp(cotangents, generation, member, objective)
+        return g if self.spin else (g[:, 0], g[:, 1])
+
+    def _input(self, maps):
+        """The library's input array of maps (spin-2 pairs: a then b, flat)."""
+        if self.spin and self.cross:
+            if not (isinstance(maps, (tuple, list)) and len(maps) == 2):
+                raise ValueError("spin-2 cross maps are a pair (a, b)")
+            pa = 2 if self.spin_a == 2 else 1
+            a = np.asarray(maps[0], dtype=np.float64).reshape(self.batch, pa, self.npix)
+            b = np.asarray(maps[1], dtype=np.float64).reshape(self.batch, 2, self.npix)
+            return np.concatenate([a.ravel(), b.ravel()])
+        x = np.ascontiguousarray(maps, dtype=np.float64)
+        if x.shape == self._map_shape[1:] and self.batch == 1:
+            x = x[None]
+        if x.shape != self._map_shape:
+            raise ValueError(f"expected maps {self._map_shape}, got {x.shape}")
+        return x
 
     def native_pixels(self):
         """Pixels each coefficient averages: [K, ncoeff] with masks, else [ncoeff]."""
@@ -372,11 +457,7 @@ class NativeEngine:
         with self._mutex:
             self._open()
             key = _key(generation, member, objective)
-            x = np.ascontiguousarray(maps, dtype=np.float64)
-            if x.shape == (self.npix,) and self.batch == 1 and not self.cross:
-                x = x[None]
-            if x.shape != self._map_shape:
-                raise ValueError(f"expected maps {self._map_shape}, got {x.shape}")
+            x = self._input(maps)
             # non-finite values: the library counts them while it copies the maps (ValueError)
             values = np.empty(self._shape(), dtype=np.complex128)
             var = np.empty(self._shape() if moments else (self.batch, 0))
@@ -409,10 +490,15 @@ class NativeEngine:
             key = _key(generation, member, objective)
             self._require_state(key)
             c = self._cotangent(cotangents)
-            grad = np.empty(self._map_shape)
+            grad = np.empty(int(np.prod(self._map_shape)))
             if self._lib.stlp_vjp(self._handle, _ptr(c.view(np.float64)), c.size, *key, _ptr(grad)):
                 raise _error()
-            return grad
+            if self.spin and self.cross:  # (grad_a, grad_b) in the shapes of a and b
+                pa = 2 if self.spin_a == 2 else 1
+                ga, gb = np.split(grad, [self.batch * pa * self.npix])
+                ga = ga.reshape(self.batch, 2, self.npix) if pa == 2 else ga.reshape(self.batch, self.npix)
+                return ga, gb.reshape(self.batch, 2, self.npix)
+            return grad.reshape(self._map_shape)
 
     def checkpoint(self):
         """A copy of the current forward state (the level-0 maps it ran on),
@@ -459,7 +545,9 @@ class NativeEngine:
             key = _key(generation, member, objective)
             if not x.is_cuda or x.dtype not in (torch.float32, torch.float64):
                 raise ValueError("forward_tensor needs a float32/float64 CUDA tensor")
-            x = x.detach().reshape(self.batch * self.channels, self.npix).contiguous()
+            if x.numel() != int(np.prod(self._map_shape)):
+                raise ValueError(f"expected {int(np.prod(self._map_shape))} map values, got {x.numel()}")
+            x = x.detach().reshape(-1).contiguous()
             self._bind_stream(torch)
             values = np.empty(self._shape(), dtype=np.complex128)
             var = np.empty(self._shape() if moments else (self.batch, 0))
@@ -477,7 +565,7 @@ class NativeEngine:
             self._open()
             key = _key(generation, member, objective)
             self._require_state(key)
-            if not (out.is_cuda and out.is_contiguous() and out.numel() == self.batch * self.channels * self.npix
+            if not (out.is_cuda and out.is_contiguous() and out.numel() == int(np.prod(self._map_shape))
                     and out.dtype in (torch.float32, torch.float64)):
                 raise ValueError("out must be a contiguous float32/float64 CUDA tensor [batch, npix]")
             c = self._cotangent(cotangents)

@@ -71,6 +71,11 @@ def test_info_reports_sizes_and_dtype(stl):
     ({"nside": 16, "j": 3, "batch": 0, "backend": "gpu"}, "batch"),
     ({"nside": 16, "j": 3, "dtype": "float16", "backend": "gpu"}, "dtype"),
     ({"nside": 16, "j": 3, "orientations": 2, "backend": "gpu"}, "orientations"),
+    ({"nside": 16, "j": 3, "spin": 1}, "spin must be 0 or 2"),
+    ({"nside": 16, "j": 3, "spin": 2, "spin_kernel": 4}, "spin_kernel"),
+    ({"nside": 16, "j": 3, "spin": 2, "spin_pyramid": "flat"}, "spin_pyramid"),
+    ({"nside": 16, "j": 3, "spin": 2, "cross": True, "spin_pyramid": "transported"}, "scalar pyramid"),
+    ({"nside": 16, "j": 3, "spin": 2, "cross": True, "spin_a": 1}, "spin_a"),
 ])
 def test_bad_configs_fail_with_a_message(stl, config, message):
     lib = stl.lib()
@@ -103,6 +108,20 @@ def test_python_side_checks(stl):
         e.forward(np.full(e.npix, np.nan))
     with pytest.raises(ValueError, match="backend"):
         stl.NativeEngine(16, 3, backend="cpu")
+
+
+def test_spin_handle_shapes(stl):
+    """Spin 2: (Q, U) maps, values of chi_E and chi_B; the operators are built
+    at the first use, so the handle's description needs no device."""
+    e = stl.NativeEngine(16, 3, batch=2, spin=2, spin_pyramid="transported")
+    info = e.info()
+    assert info["spin"] == 2 and info["spin_pyramid"] == "transported" and info["spin_kernel"] == 5
+    assert info["batch"] == 4 and info["spin_batch"] == 2  # the engine's maps: chi_E, chi_B of each
+    assert e._map_shape == (2, 2, 3072) and e._shape() == (2, 2, e.ncoeff)
+    c = stl.NativeEngine(16, 3, batch=2, spin=2, cross=True, spin_a=0)
+    assert c._map_shape == (2, 3, 3072) and c.info()["spin_a"] == 0
+    with pytest.raises(ValueError, match="pair"):
+        c._input(np.zeros((2, 3, 3072)))
 
 
 def test_out_of_scope_entry_points_fail_cleanly(stl):
