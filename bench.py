@@ -504,8 +504,19 @@ def main():
         eng.vjp_tensor(2.0 * (values - target), grad, generation=g)
 
     if args.profile_step:
+        # one step for a profiler's launch list: its launches are the last ones
+        # of the process; the line gives their count and the classes' calls and
+        # algorithmic bytes, to match a capture's launches to the classes
+        eng.profile(on=False, reset=True)
         step32()
         torch.cuda.synchronize()
+        info = eng.info()
+        stats = {k["name"]: {"launches": k["launches"], "calls": k["calls"], "bytes": k["bytes"]}
+                 for k in info["kernels"]}
+        print(json.dumps({"profile_step": {"nside": nside, "J": J, "batch": B,
+                                           "launches": sum(v["launches"] for v in stats.values()),
+                                           "kernels": stats, "mean_cells_per_row": info["mean_cells_per_row"],
+                                           "tile_heights": info["tile_heights"]}}))
         eng.close()
         return
     for _ in range(args.warmup):

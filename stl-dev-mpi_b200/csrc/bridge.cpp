@@ -240,6 +240,7 @@ char* stlp_info(StlpHandle* h) {
     auto ks = e.kernel_stats();
     for (size_t i = 0; i < ks.size(); ++i)
       js << (i ? ", " : "") << "{\"name\": " << jstr(ks[i].name) << ", \"launches\": " << ks[i].launches
+         << ", \"calls\": " << ks[i].calls
          << ", \"ms\": " << ks[i].ms << ", \"bytes\": " << ks[i].bytes << ", \"flops\": " << ks[i].flops << "}";
     js << "], \"mean_cells_per_row\": [";
     auto ms = e.mean_slots();

@@ -438,6 +438,7 @@ class Profiler {
   template <typename F>
   void launch(Cat c, int kernels, double bytes, double flops, cudaStream_t s, F&& f) {
     stat[c].launches += kernels;
+    stat[c].calls += 1;
     stat[c].bytes += bytes;
     stat[c].flops += flops;
     if (!on) { f(); return; }
@@ -460,7 +461,7 @@ class Profiler {
   }
   void reset() {
     collect();
-    for (auto& s : stat) { s.launches = 0; s.ms = s.bytes = s.flops = 0.0; }
+    for (auto& s : stat) { s.launches = s.calls = 0; s.ms = s.bytes = s.flops = 0.0; }
   }
 
  private:

@@ -60,6 +60,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+// one arrival (a consumer releasing a stage)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 // global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -282,7 +286,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     const T* __restrict__ rowsum, const double* __restrict__ rc, const int32_t* __restrict__ tile_slots) {
   constexpr int SC = fwd_sc<T>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
+  // bar: a stage's copies have landed; empty: every warp has read the stage
+  __shared__ __align__(8) uint64_t bar[2], empty[2];
   __shared__ int fail;
   // stage: coef [SC][kAdjTile][8] T, then indices [SC][kAdjTile] uint16
   constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
@@ -301,6 +306,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    mbar_init(&empty[0], kFwdThreads / 32);
+    mbar_init(&empty[1], kFwdThreads / 32);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -343,12 +350,20 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[rb][j] = (T)0;
   const T* sxk = sx + (size_t)k * pc * RB;
-  int c = 0;
-  for (; c < nch; ++c) {
+  __syncthreads();  // the cell gather, before any thread reads it
+  // The chunks: every warp waits for a stage's copies on its own, reads it,
+  // then releases it (one arrival per warp on `empty`); thread 0 refills a
+  // stage once every warp has released it.  No CTA-wide barrier in the loop:
+  // warps drift apart by up to a stage.
+  const int lane = tid & 31;
+  bool ok = true;
+  int issued = min(nch, 2);  // chunks issued (thread 0's count)
+  for (int c = 0; c < nch; ++c) {
     const int st = c & 1;
-    if (!mbar_wait(&bar[st], (c >> 1) & 1)) fail = 1;
-    __syncthreads();  // also orders the cell gather before the first chunk
-    if (fail) break;
+    if (!mbar_wait(&bar[st], (c >> 1) & 1)) {
+      ok = false;
+      break;
+    }
     const unsigned char* base = smem_raw + st * kStage;
     const T* cs = reinterpret_cast<const T*>(base);
     const uint16_t* ls = reinterpret_cast<const uint16_t*>(base + kStageCoef);
@@ -370,13 +385,25 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
         }
       }
     }
-    __syncthreads();  // the stage is read: refill it
-    if (tid == 0 && c + 2 < nch) issue(c + 2);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);
+    if (tid == 0 && c + 2 < nch) {
+      if (!mbar_wait(&empty[st], (c >> 1) & 1)) {
+        ok = false;
+        break;
+      }
+      issue(c + 2);
+      issued = c + 3;
+    }
   }
-  if (fail) {
-    bool drained = true;
-    for (int q = c; q < min(nch, c + 2); ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
-    if (tid == 0) atomicMax(err, drained ? kErrWait : kErrDrain);
+  if (!ok) fail = 1;
+  __syncthreads();
+  if (fail) {  // thread 0 waits (bounded) for the copies it may have in flight
+    if (tid == 0) {
+      bool drained = true;
+      for (int q = max(0, issued - 2); q < issued; ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+      atomicMax(err, drained ? kErrWait : kErrDrain);
+    }
     return;
   }
   if (row >= rows) return;

@@ -302,6 +302,7 @@ char* stlp_patch_info(StlpPatchHandle* h) {
       else
         for (size_t i = 0; i < ks.size() && i < k.size(); ++i) {
           ks[i].launches += k[i].launches;
+          ks[i].calls += k[i].calls;
           ks[i].ms += k[i].ms;
           ks[i].bytes += k[i].bytes;
           ks[i].flops += k[i].flops;
@@ -311,7 +312,7 @@ char* stlp_patch_info(StlpPatchHandle* h) {
        << "}, \"kernels\": [";
     for (size_t i = 0; i < ks.size(); ++i)
       js << (i ? ", " : "") << "{\"name\": \"" << ks[i].name << "\", \"launches\": " << ks[i].launches
-         << ", \"ms\": " << ks[i].ms << ", \"bytes\": " << ks[i].bytes << "}";
+         << ", \"calls\": " << ks[i].calls << ", \"ms\": " << ks[i].ms << ", \"bytes\": " << ks[i].bytes << "}";
     js << "]";
     js
        << ", \"backend\": \"gpu\", \"cache\": {\"capacity\": " << h->capacity << ", \"entries\": " << h->cache.size()

@@ -73,6 +73,7 @@ struct Timers {
 struct KernelStat {
   const char* name;
   long launches = 0;
+  long calls = 0;  // operations (a call may take more than one kernel launch)
   double ms = 0.0, bytes = 0.0, flops = 0.0;
 };
 

