@@ -85,6 +85,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
   return false;
 }
 
+// BYTES (4, 8 or 16) global -> shared, zero fill when !live, not waited
+template <int BYTES>
+__device__ __forceinline__ void cp_async_r(void* dst, const void* src, bool live) {
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(live ? 16 : 0)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
+                 "r"(live ? BYTES : 0)
+                 : "memory");
+}
 // 16-byte global -> shared copy of src_bytes (16, or 0: zero fill), not waited
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
@@ -160,6 +171,39 @@ __device__ __forceinline__ void loadR(const double* p, double v[RB]) {
     }
   } else {
     v[0] = __ldg(p);
+  }
+}
+
+// RB consecutive values in shared memory at an address aligned to RB values
+// (one vector access where RB values make 8 or 16 bytes), read or added to
+template <int RB, typename T>
+__device__ __forceinline__ void loadR_shared(const T* p, T v[RB]) {
+  if (sizeof(T) == 4 && RB == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  } else if (RB == 2) {
+    typedef typename V2<T>::type V;
+    const V a = *reinterpret_cast<const V*>(p);
+    v[0] = a.x; v[1] = a.y;
+  } else {
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) v[rb] = p[rb];
+  }
+}
+template <int RB, typename T>
+__device__ __forceinline__ void addR_shared(T* p, const T a[RB]) {
+  if (sizeof(T) == 4 && RB == 4) {
+    float4 v = *reinterpret_cast<float4*>(p);
+    v.x += a[0]; v.y += a[1]; v.z += a[2]; v.w += a[3];
+    *reinterpret_cast<float4*>(p) = v;
+  } else if (RB == 2) {
+    typedef typename V2<T>::type V;
+    V v = *reinterpret_cast<V*>(p);
+    v.x += a[0]; v.y += a[1];
+    *reinterpret_cast<V*>(p) = v;
+  } else {
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) p[rb] += a[rb];
   }
 }
 
@@ -336,14 +380,11 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   const int pc = fwd_plane_cells<T, RB>(nc);
   for (int i = tid; i < 4 * pc; i += kFwdThreads) {
     const int kk = i / pc, lc = i - kk * pc;
-    T v[RB];
-    if (lc < nc) loadR<RB>(x + rot_cell(tc[lc], kk, o2) * R + r0, v);  // cells >= nc: zero
-    else
-#pragma unroll
-      for (int rb = 0; rb < RB; ++rb) v[rb] = (T)0;
-#pragma unroll
-    for (int rb = 0; rb < RB; ++rb) sx[(size_t)i * RB + rb] = v[rb];
+    const bool live = lc < nc;
+    const T* src = x + (live ? rot_cell(tc[lc], kk, o2) * R + r0 : 0);
+    cp_async_r<RB * sizeof(T)>(sx + (size_t)i * RB, src, live);  // cells >= nc: zero
   }
+  cp_async_wait_all();
   T acc[RB][8];
 #pragma unroll
   for (int rb = 0; rb < RB; ++rb)
@@ -375,9 +416,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
           T w[8];
           load8_shared(cs + ((size_t)sl * kAdjTile + row) * 8, w);
           T xv[RB];
-          const T* xs = sxk + (size_t)ls[sl * kAdjTile + row] * RB;
-#pragma unroll
-          for (int rb = 0; rb < RB; ++rb) xv[rb] = xs[rb];
+          loadR_shared<RB>(sxk + (size_t)ls[sl * kAdjTile + row] * RB, xv);
 #pragma unroll
           for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
@@ -773,14 +812,14 @@ __global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
       if (valid && lc < nc) {
         T w[8];
         load8_shared(cs + ((size_t)sl * kAdjTile + row) * 8, w);
-        T* p = acc + ((size_t)lc * 4 + k) * RB;
+        T a[RB];
 #pragma unroll
         for (int rb = 0; rb < RB; ++rb) {
-          T a = (T)0;
+          a[rb] = (T)0;
 #pragma unroll
-          for (int q = 0; q < 8; ++q) a = fma(w[q], g[rb][q], a);
-          p[rb] += a;
+          for (int q = 0; q < 8; ++q) a[rb] = fma(w[q], g[rb][q], a[rb]);
         }
+        addR_shared<RB>(acc + ((size_t)lc * 4 + k) * RB, a);
       }
       __syncthreads();  // the slot's sums are in: the next slot may read them
     }
