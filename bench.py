@@ -317,6 +317,31 @@ def run_patches(args, torch, dist, world, rank, dev):
 
     ms_e2e = time_steps(torch, step_host, max(2, args.steps // 2), 1, dist)
     e2e_steps = max(2, args.steps // 2)
+    # Launch overhead of the per-level launches: an engine with CUDA events
+    # around every launch (after the timed steps) gives the device time of
+    # one step; the rest of the step's time is the device idle between
+    # launches, which one persistent kernel would at most recover.
+    split = None
+    if rank == 0:
+        pp = stl_b200.PatchEngine(nside, J, dtype="float32", device=dev.index, autotune=not args.no_autotune,
+                                  profile=True)
+        pp.select(centres, radii)
+        saved = pe
+        pe = pp
+        for _ in range(2):
+            step_dev()
+        before = {k["name"]: k["ms"] for k in pp.info()["kernels"]}
+        for _ in range(3):
+            step_dev()
+        torch.cuda.synchronize()
+        after = {k["name"]: k["ms"] for k in pp.info()["kernels"]}
+        kms = {k: (after[k] - before.get(k, 0.0)) / 3 for k in after}
+        busy = sum(kms.values())
+        split = {"kernel_ms_per_step": kms, "device_busy_ms_per_step": busy,
+                 "idle_fraction": max(0.0, 1.0 - busy / (ms / args.steps)),
+                 "split_from": "3 steps of a second engine with CUDA events around every launch"}
+        pe = saved
+        pp.close()
     if rank == 0:
         b = len(ids)
         line = {"metric": "disc-patch fwd+VJP patches/s (512 ragged discs, nside 512, J=5)",
@@ -327,7 +352,7 @@ def run_patches(args, torch, dist, world, rank, dev):
                 "config": {"workload": "512 disc patches, nside 512, J 5, L 4, FP32 fields, values N(0,1)",
                            "pixels_min": int(sizes.min()), "pixels_max": int(sizes.max()),
                            "pixels_total": int(sizes.sum()), "build_s": build_s,
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}", "launch_overhead": split},
                 "e2e": {"value": world * b * e2e_steps / (ms_e2e / 1e3), "unit": "patches/s",
                         "h2d_bytes_per_step": int(x_host.size * 8 + cot.size * 16),
                         "d2h_bytes_per_step": int(vals.size * 16 + x_host.size * 8)},
@@ -547,14 +572,22 @@ def main():
     # roofline of the dominant kernel class, timed live with CUDA events
     dom = max(stats.values(), key=lambda s: s["ms"])
     achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9 if dom["ms"] > 0 else 0.0
-    traffic = None
+    # DRAM traffic per call of the class: its measured DRAM / algorithmic ratio
+    # (single-launch capture of the level-0 call, profiles/traffic.json) times
+    # the class's algorithmic bytes per call here
+    calls = dom["calls"] / prof_steps
+    traffic, traffic_basis = None, None
     tp = ROOT / "profiles" / "traffic.json"
-    if tp.exists():
+    if tp.exists() and calls > 0:
         t = json.loads(tp.read_text()).get(dom["name"])
         if t:
-            traffic = t.get("dram_bytes_per_launch")
+            traffic = t["dram_over_algorithmic"] * dom["bytes"] / prof_steps / calls
+            traffic_basis = (f"DRAM bytes per call: {t['dram_over_algorithmic']} (DRAM / algorithmic bytes of "
+                             f"{t['call']}, profiles/{t['profile']}) x the class's algorithmic bytes per call")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom["name"],
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "traffic_basis": traffic_basis,
+                "kernel": dom["name"], "calls_per_step": calls, "algorithmic_bytes_per_call":
+                    dom["bytes"] / prof_steps / calls if calls else None,
                 "launches_per_step": dom["launches"] / prof_steps, "ms_per_step": dom["ms"] / prof_steps,
                 "peak_source": peaks["source"],
                 "fp32_tflops": dom["flops"] / (dom["ms"] / 1e3) / 1e12 if dom["ms"] > 0 else 0.0,

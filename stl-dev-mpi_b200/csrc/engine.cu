@@ -864,9 +864,11 @@ class EngineImpl final : public Engine {
     forward_sweep(moments);
     // the coefficients (and variances) of every map and mask, from the sums
     const size_t nv = (size_t)vb_ * K_ * plan_.size();
-    assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
-                    counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(),
-                    moments ? var_dev_.as<double>() : nullptr, s);
+    prof_.launch(Profiler::ELEM, 1, 16.0 * nv, 0.0, s, [&] {
+      assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
+                      counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(),
+                      moments ? var_dev_.as<double>() : nullptr, s);
+    });
     STL_CUDA(cudaMemcpyAsync(values, vals_dev_.p, 16 * nv, cudaMemcpyDeviceToHost, s));
     if (moments && var) STL_CUDA(cudaMemcpyAsync(var, var_dev_.p, 8 * nv, cudaMemcpyDeviceToHost, s));
     int err = 0;
@@ -922,8 +924,10 @@ class EngineImpl final : public Engine {
     load_maps(x);
     forward_sweep(false);
     const i64 nv = (i64)vb_ * K_ * plan_.size();
-    assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
-                    counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(), nullptr, s);
+    prof_.launch(Profiler::ELEM, 1, 16.0 * nv, 0.0, s, [&] {
+      assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
+                      counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(), nullptr, s);
+    });
     objective_terms(vals_dev_.as<double>(), target_dev_.as<double>(),
                     weights_dev_.p ? weights_dev_.as<double>() : nullptr, nv, (int)plan_.size(),
                     cot_dev_.as<double>(), loss, s);
@@ -964,7 +968,8 @@ class EngineImpl final : public Engine {
                      });
                    });
     const int R = B * (n + 1) * L;
-    branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s);
+    prof_.launch(Profiler::ELEM, 1, 16.0 * B * L, 0.0, s,
+                 [&] { branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s); });
     prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, R, true, false), conv_flops(op, R), s, [&] {
       conv_forward<U>(op, mod, R, brf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>(),
                       tile(n, T_FWD_BR));
@@ -1176,7 +1181,7 @@ class EngineImpl final : public Engine {
   double conv_flops(const ConvOp& op, int R) const { return 2.0 * 8.0 * R * (double)op.n_rows * op.mean_slots; }
   double dec_bytes(const DecOp& op, int R, bool transpose) const {
     const double s = op.dtype == DType::F64 ? 8.0 : 4.0;
-    double nnz = op.mean_w * (double)op.n_out;
+    double nnz = op.mean_w * (double)op.n_rep_out;  // the stored rows (a quarter on the full sky) are read
     return nnz * (s + 4.0) + R * (double)(op.n_in + op.n_out) * s;
     (void)transpose;
   }
@@ -1298,8 +1303,10 @@ class EngineImpl final : public Engine {
         });
       });
     if (!opt_.cross)
-      build_mean_var(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, i_mean_, i_var_,
-                     mv_.as<double>(), s);
+      prof_.launch(Profiler::ELEM, 1, 16.0 * B * K_ * 2, 0.0, s, [&] {
+        build_mean_var(cot_dev_.as<double>(), np, B, K_, counts_dev_.as<double>(), levels_, i_mean_, i_var_,
+                       mv_.as<double>(), s);
+      });
     for (int n = levels_ - 1; n >= 0; --n)
       typed(n, [&](auto t) { reverse_level<typename decltype(t)::type>(n); });
     for (int k = 0; k < launch_sets() && !opt_.cross; ++k)  // the cross plan has no mean or variance
@@ -1341,7 +1348,8 @@ class EngineImpl final : public Engine {
         conv_forward<U>(op, X_[n].as<U>(), B, zf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(),
                         xc_.as<double>() + (size_t)n * B, tile(n, T_FWD_Z));
       });
-      branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s);
+      prof_.launch(Profiler::ELEM, 1, 16.0 * B * L, 0.0, s,
+                   [&] { branch_constants(zc_.as<double>(), n, B, L, rc_.as<double>(), s); });
       prof_.launch(Profiler::CONV_FWD, 1, conv_bytes(op, Rb, true, false), conv_flops(op, Rb), s, [&] {
         conv_forward<U>(op, Mod_[n].as<U>(), Rb, brf<U>(n), nullptr, 0, 0, 0, s, err_.as<int>(), rc_.as<double>(),
                         tile(n, T_FWD_BR));
