@@ -55,10 +55,10 @@ def parse():
     p.add_argument("--no-autotune", action="store_true",
                    help="default tile heights instead of timing them at prepare (for runs under a profiler, whose "
                         "replays make the timing meaningless)")
-    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches", "synthesis", "cross"],
+    p.add_argument("--workload", default="scatcov", choices=["scatcov", "patches", "synthesis", "cross", "spin"],
                    help="scatcov: the headline metric; patches: 512 ragged disc patches (nside 512, J 5); "
                         "synthesis: 200 L-BFGS iterations at nside 1024, J 9; cross: the cross terms of two "
-                        "channels at nside 1024, J 9")
+                        "channels at nside 1024, J 9; spin: two (Q, U) maps through the spin-2 front end")
     return p.parse_args()
 
 
@@ -420,6 +420,89 @@ def run_cross(args, torch, dist, world, rank, dev):
     eng.close()
 
 
+def run_spin(args, torch, dist, world, rank, dev):
+    """Spin-2 statistics (the (Q, U) front end feeding the engine) at nside 1024,
+    J 9, L 4, FP32 fields, a batch of 2 (Q, U) maps (4 engine maps: chi_E, chi_B
+    of each), scalar pyramid, stencil kernel 5: Q + iU = (g1 + i g2) exp(0.5 g0)
+    (g ~ N(0, 1), seeds per rank), the cotangent that of sum |S - S_t|^2 with S_t
+    from other seeds.  Forward + VJP evaluations ((Q, U) maps) per second; the
+    front end's share is the step's time minus that of a scalar engine of 4 maps
+    on the same device (same statistics work)."""
+    import stl_b200
+    nside, J, B = args.nside, args.J, 2
+    npix = 12 * nside * nside
+    pyramid = "scalar"
+    eng = stl_b200.NativeEngine(nside, J, batch=B, dtype="float32", device=dev.index, spin=2, spin_pyramid=pyramid,
+                                autotune=not args.no_autotune)
+    t0 = time.perf_counter()
+    eng.prepare()
+    build_s = time.perf_counter() - t0
+
+    def maps(seed):
+        rng = np.random.default_rng(seed)
+        g = rng.standard_normal((B, 3, npix))
+        amp = np.exp(0.5 * g[:, 0])
+        return np.stack([g[:, 1] * amp, g[:, 2] * amp], 1)
+
+    x_host = maps(700 + rank)
+    x = torch.tensor(x_host, dtype=torch.float32, device=dev)
+    target, _ = eng.forward_tensor(torch.tensor(maps(900 + rank), dtype=torch.float32, device=dev), generation=1)
+    grad = torch.empty_like(x)
+    gen = iter(range(10, 10 ** 9))
+
+    def step():
+        k = next(gen)
+        values, _ = eng.forward_tensor(x, generation=k)
+        eng.vjp_tensor(2.0 * (values - target), grad, generation=k)
+
+    for _ in range(args.warmup):
+        step()
+    with Clocks(dev.index) as clk:
+        ms = time_steps(torch, step, args.steps, 0, dist)
+    clocks = clk.summary()
+
+    def step_host():
+        k = next(gen)
+        values, _ = eng.forward(x_host, generation=k)
+        eng.vjp(2.0 * (values - target), generation=k)
+
+    e2e_steps = max(2, args.steps // 2)
+    ms_e2e = time_steps(torch, step_host, e2e_steps, 1, dist)
+    info = eng.info()
+    eng.close()
+    del x, grad
+    torch.cuda.empty_cache()
+    # the same statistics of 4 scalar maps: the front end's cost is the difference
+    sc = stl_b200.NativeEngine(nside, J, batch=2 * B, dtype="float32", device=dev.index, prepare=True,
+                               autotune=not args.no_autotune)
+    xs = torch.tensor(np.abs(x_host.reshape(2 * B, npix)) + 1.0, dtype=torch.float32, device=dev)
+    ts, _ = sc.forward_tensor(xs, generation=1)
+    gs = torch.empty_like(xs)
+
+    def step_scalar():
+        k = next(gen)
+        values, _ = sc.forward_tensor(xs, generation=k)
+        sc.vjp_tensor(2.0 * (values - ts), gs, generation=k)
+
+    ms_scalar = time_steps(torch, step_scalar, args.steps, args.warmup, dist)
+    sc.close()
+    if rank == 0:
+        line = {"metric": f"spin-2 S1-S4 fwd+VJP evals/s ((Q, U) maps, nside {nside}, J={J}, FP32)",
+                "value": job_rate(world, B * args.steps, ms), "unit": "evals/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"spin 2 ({pyramid} pyramid, stencil 5), nside {nside}, J {J}, L 4, "
+                                       f"{B} (Q, U) maps (4 engine maps), FP32 fields",
+                           "ncoeff": info["plan"].__len__(), "parallelism": f"replicas x{world}",
+                           "spin_operator_bytes": info.get("spin_bytes"), "spin_build_s": build_s,
+                           "scalar_4_maps_ms_per_step": ms_scalar / args.steps,
+                           "front_end_ms_per_step": (ms - ms_scalar) / args.steps},
+                "e2e": {"value": job_rate(world, B * e2e_steps, ms_e2e), "unit": "evals/s",
+                        "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(x_host.nbytes)},
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+
+
 def run_synthesis(args, torch, dist, world, rank, dev):
     """L-BFGS synthesis at nside 1024, J 9, L 4, m = 10, FP32 engine: target the
     lognormal map of seed 7, start from N(0, 1) (seed 8) rescaled to the target's
@@ -500,8 +583,8 @@ def main():
         torch.cuda.set_device(0)
     import stl_b200
 
-    if args.workload in ("patches", "synthesis", "cross"):
-        run = {"patches": run_patches, "synthesis": run_synthesis, "cross": run_cross}[args.workload]
+    if args.workload in ("patches", "synthesis", "cross", "spin"):
+        run = {"patches": run_patches, "synthesis": run_synthesis, "cross": run_cross, "spin": run_spin}[args.workload]
         run(args, torch, dist, world, rank, torch.device("cuda", local if world > 1 else 0))
         if dist:
             dist.barrier()
