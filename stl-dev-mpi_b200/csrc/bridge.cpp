@@ -123,6 +123,7 @@ StlpHandle* stlp_new(const char* config) {
     require(dtype == "float64" || dtype == "float32", "dtype must be float64 or float32");
     o.fp32 = dtype == "float32";
     o.autotune = v.boolean("autotune", true);
+    o.graphs = v.boolean("graphs", true);  // the sweeps as CUDA graphs
     if (const Json* tcv = v.get("tensor_cores")) {  // true / false, or "forward", "all", "none"
       if (tcv->kind == Json::Bool) o.tensor_cores = tcv->b ? 1 : 0;
       else if (tcv->kind == Json::String && (tcv->str == "none" || tcv->str == "forward" || tcv->str == "all"))

@@ -489,6 +489,11 @@ template <typename U> struct Tag { typedef U type; };
 template <typename T>
 class EngineImpl final : public Engine {
  public:
+  ~EngineImpl() override {
+    gfwd_.reset();
+    grev_.reset();
+    if (capture_stream_) cudaStreamDestroy(capture_stream_);
+  }
   explicit EngineImpl(const Options& o, const Support* sup = nullptr) : Engine(o, sup) {
     int K0 = 0;
     (void)K0;
@@ -744,6 +749,7 @@ class EngineImpl final : public Engine {
     STL_CUDA(cudaStreamSynchronize(stream_));
     tune();
     ready_ = true;
+    ++graph_epoch_;
     timers.build_s += ms_since(t0) / 1000.0;
   }
 
@@ -860,15 +866,17 @@ class EngineImpl final : public Engine {
     if (!loaded_) throw std::runtime_error("forward before the maps were loaded");
     auto t0 = std::chrono::steady_clock::now();
     const int B = opt_.B;
-    cudaStream_t s = stream_;
-    forward_sweep(moments);
-    // the coefficients (and variances) of every map and mask, from the sums
     const size_t nv = (size_t)vb_ * K_ * plan_.size();
-    prof_.launch(Profiler::ELEM, 1, 16.0 * nv, 0.0, s, [&] {
-      assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
-                      counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(),
-                      moments ? var_dev_.as<double>() : nullptr, s);
+    in_graph(gfwd_, (moments ? 1 : 0) + (levels_given_ ? 2 : 0), [&] {
+      forward_sweep(moments);
+      // the coefficients (and variances) of every map and mask, from the sums
+      prof_.launch(Profiler::ELEM, 1, 16.0 * nv, 0.0, stream_, [&] {
+        assemble_values(sums_.as<double>(), total_sums_, plan_dev_.as<PlanSlots>(), (int)plan_.size(),
+                        counts_dev_.as<double>(), levels_, vb_, K_, vals_dev_.as<double>(),
+                        moments ? var_dev_.as<double>() : nullptr, stream_);
+      });
     });
+    cudaStream_t s = stream_;
     STL_CUDA(cudaMemcpyAsync(values, vals_dev_.p, 16 * nv, cudaMemcpyDeviceToHost, s));
     if (moments && var) STL_CUDA(cudaMemcpyAsync(var, var_dev_.p, 8 * nv, cudaMemcpyDeviceToHost, s));
     int err = 0;
@@ -1269,7 +1277,7 @@ class EngineImpl final : public Engine {
   void reverse_sweep() {
     auto t0 = std::chrono::steady_clock::now();
     cudaStream_t s = stream_;
-    reverse_launches();
+    in_graph(grev_, levels_given_ ? 1 : 0, [&] { reverse_launches(); });
     int err = 0;
     STL_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     STL_CUDA(cudaStreamSynchronize(s));
@@ -1412,6 +1420,7 @@ class EngineImpl final : public Engine {
   // matrices (per level the masks' matrices one after the other, then their
   // S1 scales: a segmented launch reads all of them) and the mask counts
   void size_mask_buffers() {
+    ++graph_epoch_;  // the sweeps' buffers move: capture them again
     const int L = opt_.L, B = opt_.B;
     const size_t nv = (size_t)vb_ * K_ * plan_.size();
     sums_.alloc(sizeof(double) * total_sums_ * K_);
@@ -1524,6 +1533,74 @@ class EngineImpl final : public Engine {
   std::vector<ConvOp> conv_;
   std::vector<DecOp> dec_;
   std::vector<DevMem> X_, Z_, Mod_, Br_, gMod_, gX_;
+  // Sweeps as CUDA graphs: the launches of a sweep are captured on a private
+  // stream at the first sweep of a configuration (key: the sweep's variant;
+  // epoch: bumped whenever buffers, masks or tile heights change) and the
+  // graph is launched into the engine's stream from then on.  Replays add the
+  // captured launches' accounting.  Off while profiling (CUDA events need the
+  // launches one by one) or with "graphs": false.
+  struct SweepGraph {
+    cudaGraphExec_t exec = nullptr;
+    long key = -1;
+    KernelStat delta[Profiler::NCAT];
+    void reset() {
+      if (exec) cudaGraphExecDestroy(exec);
+      exec = nullptr;
+      key = -1;
+    }
+    ~SweepGraph() { reset(); }
+  };
+  SweepGraph gfwd_, grev_;
+  long graph_epoch_ = 0;
+  cudaStream_t capture_stream_ = nullptr;
+  template <typename F>
+  void in_graph(SweepGraph& g, int variant, F&& launches) {
+    if (!opt_.graphs || prof_.on) {
+      launches();
+      return;
+    }
+    const long key = graph_epoch_ * 8 + variant;
+    if (!(g.exec && g.key == key)) {
+      g.reset();
+      if (!capture_stream_) STL_CUDA(cudaStreamCreateWithFlags(&capture_stream_, cudaStreamNonBlocking));
+      KernelStat before[Profiler::NCAT];
+      std::copy(prof_.stat, prof_.stat + Profiler::NCAT, before);
+      cudaStream_t user = stream_;
+      stream_ = capture_stream_;
+      cudaGraph_t graph = nullptr;
+      STL_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      try {
+        launches();
+      } catch (...) {
+        cudaStreamEndCapture(stream_, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        stream_ = user;
+        throw;
+      }
+      const cudaError_t ec = cudaStreamEndCapture(stream_, &graph);
+      stream_ = user;
+      STL_CUDA(ec);
+      const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      STL_CUDA(ei);
+      g.key = key;
+      for (int c = 0; c < Profiler::NCAT; ++c) {  // the capture counted the launches once: keep that
+        g.delta[c].launches = prof_.stat[c].launches - before[c].launches;
+        g.delta[c].calls = prof_.stat[c].calls - before[c].calls;
+        g.delta[c].bytes = prof_.stat[c].bytes - before[c].bytes;
+        g.delta[c].flops = prof_.stat[c].flops - before[c].flops;
+      }
+    } else {
+      for (int c = 0; c < Profiler::NCAT; ++c) {
+        prof_.stat[c].launches += g.delta[c].launches;
+        prof_.stat[c].calls += g.delta[c].calls;
+        prof_.stat[c].bytes += g.delta[c].bytes;
+        prof_.stat[c].flops += g.delta[c].flops;
+      }
+    }
+    STL_CUDA(cudaGraphLaunch(g.exec, stream_));
+  }
+
   // recompute field store: the one z and branch buffer of every level
   bool recompute_ = false;
   size_t keep_bytes_ = 0;  // z and branches of every level (the kept store)

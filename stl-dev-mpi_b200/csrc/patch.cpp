@@ -270,6 +270,7 @@ StlpPatchHandle* stlp_patch_new(const char* config) {
     h->group_pixels = (i64)v.integer("group_pixels", (long long)h->group_pixels);
     h->profile = v.boolean("profile", false);
     h->opt.autotune = v.boolean("autotune", true);
+    h->opt.graphs = v.boolean("graphs", true);
     h->opt.tune_cache = v.string("autotune_cache", "");
     require(h->group_pixels >= 1, "group_pixels must be positive");
     // validates nside, J, L, kernel as the full-sky engine does

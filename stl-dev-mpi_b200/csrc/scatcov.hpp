@@ -59,6 +59,9 @@ struct Options {
   bool recompute = false;
   bool fields_auto = false;  // recompute only when keeping them would not fit the device's free memory
   std::string tune_cache;  // file of tile heights already timed (read, then extended); empty: none
+  // the launches of a forward or reverse sweep as one CUDA graph, captured at
+  // the first sweep of a configuration and replayed (not while profiling)
+  bool graphs = true;
 };
 
 struct Timers {

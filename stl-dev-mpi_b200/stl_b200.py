@@ -191,7 +191,7 @@ class NativeEngine:
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
                  prepare=False, autotune=True, autotune_cache=None, cross=False, tensor_cores=False, fields="keep",
-                 spin=0, spin_kernel=5, spin_pyramid="scalar", spin_a=2, **unused):
+                 spin=0, spin_kernel=5, spin_pyramid="scalar", spin_a=2, graphs=True, **unused):
         if backend != "gpu":
             raise ValueError("backend must be 'gpu': the B200 engine has no CPU fallback")
         for v in (nside, j, batch, kernel, orientations):
@@ -223,6 +223,8 @@ class NativeEngine:
                            orientations=int(orientations), device=self.device, dtype=dtype)
         if not autotune:  # keep the default tile heights (no timing at prepare)
             self.config["autotune"] = False
+        if not graphs:  # launch the sweeps kernel by kernel instead of as CUDA graphs
+            self.config["graphs"] = False
         # FP32 wavelets: False / "none" (the default: CUDA cores), True / "forward"
         # (forward on the tensor cores, adjoint on the CUDA cores), "all" (both)
         if tensor_cores is not False and tensor_cores != "none":
@@ -725,7 +727,7 @@ class PatchEngine:
     radius in degrees; the coefficients average the core (else the whole disc)."""
 
     def __init__(self, nside, j, kernel=5, orientations=4, dtype="float64", device=0, cache=256, threads=0,
-                 group_pixels=None, profile=False, autotune=True):
+                 group_pixels=None, profile=False, autotune=True, graphs=True):
         cfg = dict(nside=int(nside), j=int(j), kernel=int(kernel), orientations=int(orientations), backend="gpu",
                    dtype=dtype, device=int(device), cache=int(cache), threads=int(threads))
         if group_pixels is not None:  # level-0 pixels of the discs one batched engine holds
@@ -734,6 +736,8 @@ class PatchEngine:
             cfg["profile"] = True
         if not autotune:  # keep the default tile heights
             cfg["autotune"] = False
+        if not graphs:  # the sweeps kernel by kernel instead of as CUDA graphs
+            cfg["graphs"] = False
         self._lib = lib()
         self._mutex = threading.RLock()
         self._handle = self._lib.stlp_patch_new(json.dumps(cfg).encode())
