@@ -1029,6 +1029,11 @@ class EngineImpl final : public Engine {
     STL_CUDA(cudaStreamSynchronize(stream_));
   }
 
+  size_t host_to_device(void* dst, const void* src, size_t n, bool check) override {
+    return io_.to_device(dst, src, n, stream_, check);
+  }
+  void device_to_host(void* dst, const void* src, size_t n) override { io_.to_host(dst, src, n, stream_); }
+
   void reverse_levels(const double* cot, double* const* out) override {
     if (!levels_given_) throw std::runtime_error("per-level cotangents need maps given at every level");
     reverse_impl(cot);

@@ -155,6 +155,12 @@ class Engine {
   // level (its own terms, without the chain through the decimations),
   // map-major f64 [B][N_d] into the device buffers out[d]
   virtual void reverse_levels(const double* cot, double* const* out) = 0;
+  // Large host <-> device copies on the engine's stream through its pinned
+  // staging (pageable host memory, several host threads): to the device,
+  // returning the non-finite doubles counted on the way when check; to the
+  // host, synchronising.
+  virtual size_t host_to_device(void* dst, const void* src, size_t n, bool check) = 0;
+  virtual void device_to_host(void* dst, const void* src, size_t n) = 0;
   // The synthesis objective on the device: loss = sum_o w_(o mod np)
   // |S_o(x) - T_o|^2 over the coefficients [B][K][np] of the maps x (f64
   // [B][N_0], device), its gradient into g (f64, device) and the loss into
