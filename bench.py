@@ -342,6 +342,20 @@ def run_patches(args, torch, dist, world, rank, dev):
                  "split_from": "3 steps of a second engine with CUDA events around every launch"}
         pe = saved
         pp.close()
+    # FP32 patches against an FP64 engine on the same discs and values (the
+    # 1e-6 family criterion of the headline), after the timed steps
+    accuracy = None
+    if rank == 0:
+        v32, _ = pe.forward(patches, moments=False, generation=next(gen))
+        p64 = stl_b200.PatchEngine(nside, J, dtype="float64", device=dev.index, autotune=False)
+        p64.select(centres, radii)
+        v64, _ = p64.forward(patches, moments=False, generation=1)
+        p64.close()
+        ratio, rel = family_errors(pe.plan, v32, v64)
+        accuracy = {"max_err_ratio": ratio, "max_rel_err": rel,
+                    "criterion": "|v32 - v64| <= 1e-6 (max |v64| of the coefficient's family, level and disc) "
+                                 "+ 1e-6 |v64|; max_err_ratio <= 1 passes",
+                    "reference": "the FP64 disc engine on the same discs and values"}
     if rank == 0:
         b = len(ids)
         line = {"metric": "disc-patch fwd+VJP patches/s (512 ragged discs, nside 512, J=5)",
@@ -352,7 +366,8 @@ def run_patches(args, torch, dist, world, rank, dev):
                 "config": {"workload": "512 disc patches, nside 512, J 5, L 4, FP32 fields, values N(0,1)",
                            "pixels_min": int(sizes.min()), "pixels_max": int(sizes.max()),
                            "pixels_total": int(sizes.sum()), "build_s": build_s,
-                           "parallelism": f"replicas x{world}", "launch_overhead": split},
+                           "parallelism": f"replicas x{world}", "launch_overhead": split,
+                           "accuracy": accuracy},
                 "e2e": {"value": world * b * e2e_steps / (ms_e2e / 1e3), "unit": "patches/s",
                         "h2d_bytes_per_step": int(x_host.size * 8 + cot.size * 16),
                         "d2h_bytes_per_step": int(vals.size * 16 + x_host.size * 8)},

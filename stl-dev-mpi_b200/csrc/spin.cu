@@ -393,30 +393,15 @@ __global__ void k_spin_tsort(const i64* __restrict__ tptr, i64 cols, int* __rest
 }
 
 // Field addressing: element p of component q (0: real part, 1: imaginary
-// part) of map r at base + r map + q comp + p pix.  Map-major fields
-// [R][2][n] have (map, comp, pix) = (2n, n, 1); the pixel-major copies the
-// gathers read, [n][R][2], (2, 1, 2R): a cell's values share one sector.
+// part) of map r at base + r map + q comp + p.
 struct FieldRef {
   const double* base;
-  i64 map, comp, pix;
+  i64 map, comp;
 };
 struct FieldOut {
   double* base;
-  i64 map, comp, pix;
+  i64 map, comp;
 };
-inline FieldRef map_major(const double* b, i64 n, i64 map_stride) { return FieldRef{b, map_stride, n, 1}; }
-inline FieldOut map_major_out(double* b, i64 n, i64 map_stride) { return FieldOut{b, map_stride, n, 1}; }
-inline FieldRef pixel_major(const double* b, int R) { return FieldRef{b, 2, 1, 2 * (i64)R}; }
-inline FieldOut pixel_major_out(double* b, int R) { return FieldOut{b, 2, 1, 2 * (i64)R}; }
-
-// y = x in another layout (n pixels, R maps, 2 components); thread per output value
-__global__ void k_relayout(FieldRef x, FieldOut y, int R, i64 n) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 2 * R * n) return;
-  const i64 p = i / (2 * R);
-  const int j = (int)(i - p * 2 * R), r = j >> 1, q = j & 1;
-  y.base[r * y.map + q * y.comp + p * y.pix] = x.base[r * x.map + q * x.comp + p * x.pix];
-}
 
 // y = A x (rows stored per turn), maps [r0, r0 + RB) of R; accumulate: y +=
 template <int RB>
@@ -441,7 +426,7 @@ __global__ void __launch_bounds__(kApplyThreads) k_spin_apply(const int* __restr
 #pragma unroll
       for (int j = 0; j < RB; ++j)
         if (r0 + j < R) {
-          const double* xm = x.base + (i64)(r0 + j) * x.map + c * x.pix;
+          const double* xm = x.base + (i64)(r0 + j) * x.map + c;
           const double q = xm[0], uu = xm[x.comp];
           are[j] += v.x * q - v.y * uu;
           aim[j] += v.x * uu + v.y * q;
@@ -450,7 +435,7 @@ __global__ void __launch_bounds__(kApplyThreads) k_spin_apply(const int* __restr
 #pragma unroll
     for (int j = 0; j < RB; ++j)
       if (r0 + j < R) {
-        double* ym = y.base + (i64)(r0 + j) * y.map + p * y.pix;
+        double* ym = y.base + (i64)(r0 + j) * y.map + p;
         if (accumulate) {
           ym[0] += are[j];
           ym[y.comp] += aim[j];
@@ -485,7 +470,7 @@ __global__ void __launch_bounds__(kApplyThreads) k_spin_adjoint(const i64* __res
 #pragma unroll
       for (int j = 0; j < RB; ++j)
         if (r0 + j < R) {
-          const double* gm = g.base + (i64)(r0 + j) * g.map + r * g.pix;
+          const double* gm = g.base + (i64)(r0 + j) * g.map + r;
           const double q = gm[0], uu = gm[g.comp];
           are[j] += v.x * q - v.y * uu;
           aim[j] += v.x * uu + v.y * q;
@@ -494,7 +479,7 @@ __global__ void __launch_bounds__(kApplyThreads) k_spin_adjoint(const i64* __res
 #pragma unroll
     for (int j = 0; j < RB; ++j)
       if (r0 + j < R) {
-        double* xm = x.base + (i64)(r0 + j) * x.map + c * x.pix;
+        double* xm = x.base + (i64)(r0 + j) * x.map + c;
         if (accumulate) {
           xm[0] += are[j];
           xm[x.comp] += aim[j];
@@ -517,10 +502,10 @@ __global__ void k_spin_down_adjoint(const double2* __restrict__ w, i64 rows_c, i
   const i64 uP = ((f >> 2) << o2_c) | (P & ((i64(1) << o2_c) - 1));
   const double2 v = w[(size_t)j * rows_c + uP];  // conj(v) g
   for (int r = 0; r < R; ++r) {
-    const double* gm = g.base + (i64)r * g.map + P * g.pix;
+    const double* gm = g.base + (i64)r * g.map + P;
     const double q = gm[0], uu = gm[g.comp];
     const double re = v.x * q + v.y * uu, im = v.x * uu - v.y * q;
-    double* xm = x.base + (i64)r * x.map + c * x.pix;
+    double* xm = x.base + (i64)r * x.map + c;
     if (accumulate) {
       xm[0] += re;
       xm[x.comp] += im;
@@ -766,24 +751,22 @@ class SpinFrontImpl final : public SpinFront {
     const size_t n0 = input_len();
     DevMem xin(8 * n0);
     STL_CUDA(cudaMemcpyAsync(xin.p, x, 8 * n0, cudaMemcpyHostToDevice, s_));
+    std::vector<DevMem> pol(level + 1);
     const int B = cfg_.batch;
-    std::vector<DevMem> pol(level + 1);  // pixel-major P_j
     for (int j = 0; j <= level; ++j) {
+      if (j == 0) continue;
       pol[j].alloc(8 * (size_t)B * 2 * npix(j));
-      if (j == 0)
-        relayout(map_major(xin.as<double>(), npix(0), 2 * npix(0)), pixel_major_out(pol[0].as<double>(), B), B,
-                 npix(0));
-      else
-        apply(down_[j - 1], pixel_major(pol[j - 1].as<double>(), B), pixel_major_out(pol[j].as<double>(), B), B,
-              false, s_);
+      const double* src = j == 1 ? xin.as<double>() : pol[j - 1].as<double>();
+      apply(down_[j - 1], FieldRef{src, 2 * npix(j - 1), npix(j - 1)},
+            FieldOut{pol[j].as<double>(), 2 * npix(j), npix(j)}, B, false, s_);
     }
-    const i64 nl = npix(level);
-    DevMem c(8 * (size_t)B * 2 * nl), q(8 * (size_t)B * 2 * nl);
-    apply(eth_[level], pixel_major(pol[level].as<double>(), B), map_major_out(c.as<double>(), nl, 2 * nl), B, false,
-          s_);
-    relayout(pixel_major(pol[level].as<double>(), B), map_major_out(q.as<double>(), nl, 2 * nl), B, nl);
-    STL_CUDA(cudaMemcpyAsync(qu, q.p, 8 * (size_t)B * 2 * nl, cudaMemcpyDeviceToHost, s_));
-    STL_CUDA(cudaMemcpyAsync(chi, c.p, 8 * (size_t)B * 2 * nl, cudaMemcpyDeviceToHost, s_));
+    const double* P = level == 0 ? xin.as<double>() : pol[level].as<double>();
+    DevMem c(8 * (size_t)B * 2 * npix(level));
+    apply(eth_[level], FieldRef{P, 2 * npix(level), npix(level)}, FieldOut{c.as<double>(), 2 * npix(level), npix(level)},
+          B, false, s_);
+    const size_t nl = (size_t)B * 2 * npix(level);
+    STL_CUDA(cudaMemcpyAsync(qu, P, 8 * nl, cudaMemcpyDeviceToHost, s_));
+    STL_CUDA(cudaMemcpyAsync(chi, c.p, 8 * nl, cudaMemcpyDeviceToHost, s_));
     STL_CUDA(cudaStreamSynchronize(s_));
   }
 
@@ -886,18 +869,6 @@ class SpinFrontImpl final : public SpinFront {
     if (bad) throw std::runtime_error("input map contains non-finite values");
   }
 
-  // x (R maps, 2 components, n pixels) into y in another layout
-  void relayout(FieldRef x, FieldOut y, int R, i64 n) {
-    k_relayout<<<blocks_of(2 * R * n, 256), 256, 0, s_>>>(x, y, R, n);
-    check_launch();
-  }
-  // a pixel-major copy of x in buffer b, for the gathers of the operators
-  FieldRef gathered(FieldRef x, int R, i64 n, Buffer& b) {
-    b.alloc_at_least(8 * (size_t)2 * R * n);
-    relayout(x, pixel_major_out(b.as<double>(), R), R, n);
-    return pixel_major(b.as<double>(), R);
-  }
-
   // the engine's maps from the staged input in_, then loaded
   void run_forward(Engine& e) {
     const int B = cfg_.batch;
@@ -908,11 +879,9 @@ class SpinFrontImpl final : public SpinFront {
       const double* a = in_.as<double>();
       const double* b = a + (size_t)B * pa * n;
       double* m = maps_[0].as<double>();
-      apply(eth_[0], gathered(map_major(b, n, 2 * n), B, n, pm_[0]), map_major_out(m + n, 2 * n, 4 * n), B, false,
-            s_);
+      apply(eth_[0], FieldRef{b, 2 * n, n}, FieldOut{m + n, 4 * n, 2 * n}, B, false, s_);
       if (pa == 2) {
-        apply(eth_[0], gathered(map_major(a, n, 2 * n), B, n, pm_[1]), map_major_out(m, 2 * n, 4 * n), B, false,
-              s_);
+        apply(eth_[0], FieldRef{a, 2 * n, n}, FieldOut{m, 4 * n, 2 * n}, B, false, s_);
       } else {
         k_copy_t<<<blocks_of((i64)B * n, 256), 256, 0, s_>>>(a, n, B, m);
         check_launch();
@@ -920,22 +889,22 @@ class SpinFrontImpl final : public SpinFront {
       e.load_device(m, false);
     } else if (!cfg_.transported) {  // chi of level 0 as maps [2B][n] (= [B][2][n])
       maps_[0].alloc_at_least(8 * (size_t)B * 2 * n);
-      apply(eth_[0], gathered(map_major(in_.as<double>(), n, 2 * n), B, n, pm_[0]),
-            map_major_out(maps_[0].as<double>(), n, 2 * n), B, false, s_);
+      apply(eth_[0], FieldRef{in_.as<double>(), 2 * n, n}, FieldOut{maps_[0].as<double>(), 2 * n, n}, B, false, s_);
       e.load_device(maps_[0].as<double>(), false);
-    } else {  // P_j (pixel-major) and chi_j of every level
+    } else {  // P_j and chi_j of every level
       const int L = (int)eth_.size();
       std::vector<const double*> lv(L);
       for (int j = 0; j < L; ++j) {
         const i64 nj = npix(j);
-        FieldRef P = j == 0 ? gathered(map_major(in_.as<double>(), n, 2 * n), B, n, pm_[0])
-                            : pixel_major(pm_[j].as<double>(), B);
-        if (j + 1 < L) {
-          pm_[j + 1].alloc_at_least(8 * (size_t)B * 2 * npix(j + 1));
-          apply(down_[j], P, pixel_major_out(pm_[j + 1].as<double>(), B), B, false, s_);
+        if (j > 0) {
+          pol_[j].alloc_at_least(8 * (size_t)B * 2 * nj);
+          const double* src = j == 1 ? in_.as<double>() : pol_[j - 1].as<double>();
+          apply(down_[j - 1], FieldRef{src, 2 * npix(j - 1), npix(j - 1)}, FieldOut{pol_[j].as<double>(), 2 * nj, nj},
+                B, false, s_);
         }
         maps_[j].alloc_at_least(8 * (size_t)B * 2 * nj);
-        apply(eth_[j], P, map_major_out(maps_[j].as<double>(), nj, 2 * nj), B, false, s_);
+        const double* P = j == 0 ? in_.as<double>() : pol_[j].as<double>();
+        apply(eth_[j], FieldRef{P, 2 * nj, nj}, FieldOut{maps_[j].as<double>(), 2 * nj, nj}, B, false, s_);
         lv[j] = maps_[j].as<double>();
       }
       e.load_device_levels(lv.data());
@@ -961,11 +930,10 @@ class SpinFrontImpl final : public SpinFront {
         const i64 nj = npix(j);
         if (j > 0) gpol_[j].alloc_at_least(8 * (size_t)B * 2 * nj);
         double* hj = j == 0 ? gin_.as<double>() : gpol_[j].as<double>();
-        adjoint(eth_[j], false, gathered(map_major(lv[j], nj, 2 * nj), B, nj, gpm_), map_major_out(hj, nj, 2 * nj),
-                B, false, s_);
+        adjoint(eth_[j], false, FieldRef{lv[j], 2 * nj, nj}, FieldOut{hj, 2 * nj, nj}, B, false, s_);
         if (j + 1 < L)
-          adjoint(down_[j], true, map_major(gpol_[j + 1].as<double>(), npix(j + 1), 2 * npix(j + 1)),
-                  map_major_out(hj, nj, 2 * nj), B, true, s_);
+          adjoint(down_[j], true, FieldRef{gpol_[j + 1].as<double>(), 2 * npix(j + 1), npix(j + 1)},
+                  FieldOut{hj, 2 * nj, nj}, B, true, s_);
       }
       return;
     }
@@ -974,18 +942,15 @@ class SpinFrontImpl final : public SpinFront {
     e.reverse_device(cot, gmaps_[0].as<double>(), false);
     const double* g = gmaps_[0].as<double>();
     if (!cfg_.cross) {
-      adjoint(eth_[0], false, gathered(map_major(g, n, 2 * n), B, n, gpm_), map_major_out(gin_.as<double>(), n, 2 * n),
-              B, false, s_);
+      adjoint(eth_[0], false, FieldRef{g, 2 * n, n}, FieldOut{gin_.as<double>(), 2 * n, n}, B, false, s_);
       return;
     }
     const int pa = cfg_.spin_a == 2 ? 2 : 1;
     double* ga = gin_.as<double>();
     double* gb = ga + (size_t)B * pa * n;
-    adjoint(eth_[0], false, gathered(map_major(g + n, 2 * n, 4 * n), B, n, gpm_), map_major_out(gb, n, 2 * n), B,
-            false, s_);
+    adjoint(eth_[0], false, FieldRef{g + n, 4 * n, 2 * n}, FieldOut{gb, 2 * n, n}, B, false, s_);
     if (pa == 2) {
-      adjoint(eth_[0], false, gathered(map_major(g, 2 * n, 4 * n), B, n, gpm_), map_major_out(ga, n, 2 * n), B,
-              false, s_);
+      adjoint(eth_[0], false, FieldRef{g, 4 * n, 2 * n}, FieldOut{ga, 2 * n, n}, B, false, s_);
     } else {
       k_sum_t<<<blocks_of((i64)B * n, 256), 256, 0, s_>>>(g, n, B, ga);
       check_launch();
@@ -1032,7 +997,7 @@ class SpinFrontImpl final : public SpinFront {
   std::vector<SpinOp> eth_, down_;
   DevMem err_, bad_;
   Buffer in_, gin_;
-  Buffer maps_[32], pm_[32], gmaps_[32], gpol_[32], gpm_;
+  Buffer maps_[32], pol_[32], gmaps_[32], gpol_[32];
   bool loaded_ = false, built_ = false;
 };
 
