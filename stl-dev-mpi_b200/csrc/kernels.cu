@@ -1601,7 +1601,7 @@ __host__ __device__ constexpr int p0_sums() {  // diag blocks, full blocks, (d, 
 }
 template <typename T, int ND>
 __host__ __device__ constexpr int p0_threads() {
-  return (sizeof(T) == 4 ? 1024 : 512) / ND;
+  return sizeof(T) == 4 ? (ND == 1 ? 768 : 1024 / ND) : 512 / ND;
 }
 
 // warps of a CTA: the FP64 sums of the warps fit in 200 KB
@@ -1683,16 +1683,38 @@ __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
   const i64 p0 = blk ? blk[blockIdx.x] : (i64)blockIdx.x * chunk;
   const i64 p1 = blk ? blk[blockIdx.x + 1] : min(N, p0 + chunk);
   int cnt = 0;
-  for (i64 base = p0 + (i64)warp * P; base < p1; base += (i64)nw * P) {
+  // the operands of the thread's next pixel are loaded while this pixel's
+  // products run (two pixels' loads in flight a thread)
+  const i64 step = (i64)nw * P;
+  T2 an[ND][4], zn;
+  bool live_n = false;
+  auto fetch = [&](i64 p, T2 (&a)[ND][4], T2& zz) -> bool {
+    if (!(p < p1 && (!mask || mask[p]))) return false;
+    const i64 q = (p * B + b) * (ND * 16) + l3;  // Br [N][B][ND L][L]
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) a[d][l] = __ldg(brv + q + (d * 4 + l) * 4);
+    zz = __ldg(zv + (p * B + b) * 4 + l3);
+    return true;
+  };
+  if (ND == 1) live_n = fetch(p0 + (i64)warp * P + pw, an, zn);  // ND > 1: no registers to spare
+  for (i64 base = p0 + (i64)warp * P; base < p1; base += step) {
     const i64 p = base + pw;
-    if (p < p1 && (!mask || mask[p])) {
-      const i64 q = (p * B + b) * (ND * 16) + l3;  // Br [N][B][ND L][L]
-      T2 a[ND][4];
+    T2 a[ND][4], zz;
+    bool live;
+    if (ND == 1) {
+      live = live_n;
 #pragma unroll
       for (int d = 0; d < ND; ++d)
 #pragma unroll
-        for (int l = 0; l < 4; ++l) a[d][l] = __ldg(brv + q + (d * 4 + l) * 4);
-      const T2 zz = __ldg(zv + (p * B + b) * 4 + l3);
+        for (int l = 0; l < 4; ++l) a[d][l] = an[d][l];
+      zz = zn;
+      live_n = fetch(p + step, an, zn);
+    } else {
+      live = fetch(p, a, zz);
+    }
+    if (live) {
 #pragma unroll
       for (int d = 0; d < ND; ++d) {
         T* fd = f + d * 16;
