@@ -3104,6 +3104,137 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
   }
 }
 
+// ---- the forward with the four gauges in one CTA (levels with K <= kCross4MaxK) ----
+// The operands of a (pixel, map, operand) are the 4 gauges' complex values in
+// one run (32 bytes in FP32): a CTA that takes all four gauges of a pixel range
+// loads whole sectors, where one CTA a gauge used a quarter of each (the
+// products of the nside 1024 bench: 17.5 -> 14.3 ms; the same form of the VJP
+// was slower, 22.4 -> 27.2 ms, and is not used).  Staged values
+// sv[j][g][c][i] (i < K the operands, i = K the S1 factor), FP64.
+constexpr int kCross4MaxK = 21;  // 4 (K^2 + 1) entries within kCrossMaxEnt per thread
+
+template <typename T>
+__device__ __forceinline__ void load_gauges(const typename V2<T>::type* src, double2 v[4]) {
+  if (sizeof(T) == 4) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(src)), c = __ldg(reinterpret_cast<const float4*>(src) + 1);
+    v[0] = make_double2(a.x, a.y); v[1] = make_double2(a.z, a.w);
+    v[2] = make_double2(c.x, c.y); v[3] = make_double2(c.z, c.w);
+  } else {
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const double2 a = __ldg(reinterpret_cast<const double2*>(src) + g);
+      v[g] = a;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void cross_stage4(double2* sv, double* nv, i64 p0, int np, int K, int Bm, int b,
+                                             const T* __restrict__ z, const T* __restrict__ br,
+                                             const uint8_t* __restrict__ mask) {
+  typedef typename V2<T>::type T2;
+  const T2* zv = reinterpret_cast<const T2*>(z);
+  const T2* bv = reinterpret_cast<const T2*>(br);
+  const int K1 = K - 1, KS = K + 1, L = 4, n = np * 2 * K;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {  // one (pixel, channel, operand) a thread
+    const int j = t / (2 * K), rem = t - j * 2 * K, c = rem / K, i = rem - c * K;
+    const i64 p = p0 + j, m = 2 * b + c;
+    double2 v[4];
+    load_gauges<T>(i < K1 ? bv + ((p * Bm + m) * K1 + i) * L : zv + (p * Bm + m) * L, v);
+    const bool on = !mask || mask[p];
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const double2 w = on ? v[g] : make_double2(0.0, 0.0);
+      const int at = ((j * 4 + g) * 2 + c) * KS + i;
+      sv[at] = w;
+      if (nv) nv[at] = fma(w.x, w.x, w.y * w.y);
+    }
+  }
+  for (int t = threadIdx.x; t < np * 8; t += blockDim.x) {  // rn(z) of (pixel, gauge, channel): the S1 factor
+    const int j = t >> 3, g = (t >> 1) & 3, c = t & 1;
+    const i64 p = p0 + j;
+    double2 v = make_double2(0.0, 0.0);
+    if (!mask || mask[p]) {
+      const T2 w = zv[(p * Bm + 2 * b + c) * L + g];
+      v = root_normalise(make_double2((double)w.x, (double)w.y));
+    }
+    const int at = ((j * 4 + g) * 2 + c) * KS + K;
+    sv[at] = v;
+    if (nv) nv[at] = fma(v.x, v.x, v.y * v.y);
+  }
+}
+
+// forward: grid pixel ranges x B; thread (entry e of the 4 (K^2 + 1) of the
+// four gauges, pixel lane q); partials [range][b][l3][xslots] as k_cross_fwd
+template <typename T, bool MOM, int NENT>
+__global__ void __launch_bounds__(kCrossThreads) k_cross_fwd4(i64 N, int K, int Bm, const T* __restrict__ z,
+                                                              const T* __restrict__ br,
+                                                              const uint8_t* __restrict__ mask, i64 chunk, int PC,
+                                                              double* __restrict__ partials) {
+  extern __shared__ __align__(16) double2 sv[];  // [PC][4][2][K + 1], (MOM) moduli; then the lane sums
+  const int B = Bm / 2, b = (int)(blockIdx.x % (unsigned)B);
+  const i64 range = blockIdx.x / (unsigned)B;
+  const int E = K * K + 1, E4 = 4 * E, NE = min(E4, kCrossThreads), Q = kCrossThreads / NE;
+  const int t = threadIdx.x, q = t / NE, e0 = t - q * NE;
+  const int nent = (E4 - e0 + NE - 1) / NE;
+  const bool lane = q < Q;
+  const int KS = K + 1, G = 2 * KS, PS = 4 * G;  // values per (pixel, gauge) and per pixel
+  double* nv = MOM ? reinterpret_cast<double*>(sv + (size_t)PC * PS) : nullptr;
+  double acc[NENT][3];
+  int o0[NENT], o1[NENT];  // the entry's operands within a pixel's values
+#pragma unroll
+  for (int s = 0; s < NENT; ++s) {
+    acc[s][0] = acc[s][1] = acc[s][2] = 0.0;
+    const int e = e0 + s * NE, g = e / E, el = e - g * E;
+    o0[s] = g * G + (el < K * K ? el / K : K);
+    o1[s] = g * G + KS + (el < K * K ? el - (el / K) * K : K);
+  }
+  const i64 P0 = range * chunk, P1 = min(N, P0 + chunk);
+  for (i64 pc = P0; pc < P1; pc += PC) {
+    const int np = (int)min((i64)PC, P1 - pc);
+    __syncthreads();
+    cross_stage4<T>(sv, nv, pc, np, K, Bm, b, z, br, mask);
+    __syncthreads();
+    if (!lane) continue;
+    for (int j = q; j < np; j += Q) {
+      const double2* v = sv + (size_t)j * PS;
+#pragma unroll
+      for (int s = 0; s < NENT; ++s) {
+        if (s >= nent) continue;
+        const double2 a = v[o0[s]], c = v[o1[s]];
+        acc[s][0] = fma(a.y, c.y, fma(a.x, c.x, acc[s][0]));
+        acc[s][1] = fma(-a.x, c.y, fma(a.y, c.x, acc[s][1]));
+        if (MOM) {
+          const double* n0 = nv + (size_t)j * PS;
+          acc[s][2] = fma(n0[o0[s]], n0[o1[s]], acc[s][2]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(sv);  // [Q][NE][NENT][3]
+  if (lane) {
+#pragma unroll
+    for (int s = 0; s < NENT; ++s)
+      if (s < nent)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) red[(((size_t)q * NE + e0) * NENT + s) * 3 + k] = acc[s][k];
+  }
+  __syncthreads();
+  if (q != 0) return;
+  for (int s = 0; s < nent; ++s) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int r = 0; r < Q; ++r)
+      for (int k = 0; k < 3; ++k) v[k] = __dadd_rn(v[k], red[(((size_t)r * NE + e0) * NENT + s) * 3 + k]);
+    const int e = e0 + s * NE, g = e / E, el = e - g * E;
+    double* out = partials + ((range * B + b) * 4 + g) * cross_slots(K);
+    const int at = el < K * K ? 2 * el : 2 * K * K;
+    out[at] = v[0];
+    out[at + 1] = v[1];
+    out[el < K * K ? 2 * K * K + 2 + el : 3 * K * K + 2] = v[2];
+  }
+}
+
 template <typename T, bool MOM, int NENT>
 void launch_cross_fwd(unsigned grid, size_t smem, cudaStream_t s, i64 N, int K, int Bm, const T* z, const T* br,
                       const uint8_t* mask, i64 chunk, int PC, double* partials) {
@@ -3120,9 +3251,43 @@ void launch_cross_fwd(int nent, unsigned grid, size_t smem, cudaStream_t s, i64 
   else launch_cross_fwd<T, MOM, kCrossMaxEnt>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
 }
 
+template <typename T, bool MOM, int NENT>
+void launch_cross_fwd4(unsigned grid, size_t smem, cudaStream_t s, i64 N, int K, int Bm, const T* z, const T* br,
+                       const uint8_t* mask, i64 chunk, int PC, double* partials) {
+  if (smem > 48 * 1024) allow_dynamic_smem(k_cross_fwd4<T, MOM, NENT>);
+  k_cross_fwd4<T, MOM, NENT><<<grid, kCrossThreads, smem, s>>>(N, K, Bm, z, br, mask, chunk, PC, partials);
+}
+template <typename T, bool MOM>
+void launch_cross_fwd4(int nent, unsigned grid, size_t smem, cudaStream_t s, i64 N, int K, int Bm, const T* z,
+                       const T* br, const uint8_t* mask, i64 chunk, int PC, double* partials) {
+  if (nent <= 1) launch_cross_fwd4<T, MOM, 1>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else if (nent <= 2) launch_cross_fwd4<T, MOM, 2>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else if (nent <= 4) launch_cross_fwd4<T, MOM, 4>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+  else launch_cross_fwd4<T, MOM, kCrossMaxEnt>(grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+}
+
 template <typename T>
 void cross_forward(int K, i64 N, int Bm, const T* z, const T* br, const uint8_t* mask, bool moments,
                    double* partials, int nblk, double* sums, cudaStream_t s) {
+  if (K <= kCross4MaxK) {  // the four gauges a CTA
+    const int E4 = 4 * (K * K + 1), NE = std::min(E4, kCrossThreads), Q = kCrossThreads / NE;
+    const int nent = (E4 + NE - 1) / NE;
+    const int per = 4 * 2 * (K + 1) * (moments ? 24 : 16);
+    const int PC = std::max(8, std::min(256, (48 * 1024) / per));
+    const size_t smem = std::max((size_t)PC * per, sizeof(double) * (size_t)Q * NE * kCrossMaxEnt * 3);
+    const i64 chunk = (N + nblk - 1) / nblk;
+    const unsigned grid = (unsigned)nblk * (unsigned)(Bm / 2);
+    if (moments)
+      launch_cross_fwd4<T, true>(nent, grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+    else
+      launch_cross_fwd4<T, false>(nent, grid, smem, s, N, K, Bm, z, br, mask, chunk, PC, partials);
+    STL_CUDA(cudaGetLastError());
+    const i64 rows = (i64)Bm / 2 * 4, total = rows * cross_slots(K);
+    k_reduce_partials<<<(unsigned)std::min<i64>((total + 255) / 256, 1024), 256, 0, s>>>(partials, nblk, (int)rows,
+                                                                                          cross_slots(K), sums);
+    STL_CUDA(cudaGetLastError());
+    return;
+  }
   const int E = K * K + 1, NE = std::min(E, kCrossThreads), Q = kCrossThreads / NE;
   const int nent = (E + NE - 1) / NE;
   if (nent > kCrossMaxEnt) throw std::runtime_error("too many cross terms per level");
