@@ -211,3 +211,50 @@ def test_device_tensors_and_bit_reproducible(stl):
     e.vjp_tensor(cot, g_dev)
     e.forward(x)
     assert np.array_equal(e.vjp(cot), g_dev.cpu().numpy())
+
+
+@pytest.mark.parametrize("kernel,tol", [(3, 1e-12), (7, 1e-10), (9, 1e-8)])
+def test_other_stencils_match_oracle(stl, kernel, tol):
+    """Kernels 3, 7 and 9: statistics and gradients against the oracle, the bar
+    scaled by the weights' conditioning (the operator rows' bounds above)."""
+    x = _maps(1, 13)
+    e = stl.NativeEngine(NSIDE, J, spin=2, spin_kernel=kernel, spin_pyramid="transported")
+    o = S.SpinOracle(NSIDE, J, kernel=kernel, pyramid="transported")
+    v, vo = e.forward(x)[0], o.forward(x)
+    assert np.abs(v - vo).max() <= tol * np.abs(vo).max()
+    cot = np.random.default_rng(14).normal(size=v.shape) + 0j
+    assert np.abs(e.vjp(cot) - o.vjp(cot)).max() <= 10 * tol * np.abs(o.vjp(cot)).max()
+
+
+def test_cross_pairs_with_masks_match_oracle(stl):
+    """Cross pairs (spin_a 2) with eroded masks: the scalar-pyramid erosion of
+    both channels' level-0 stencil."""
+    rng = np.random.default_rng(15)
+    n = 12 * NSIDE ** 2
+    a, b = rng.normal(size=(2, 2, n)), rng.normal(size=(2, 2, n))
+    w = np.ones((2, n))
+    w[0, :300] = 0.0
+    w[1, 1500:1900] = 0.0
+    e = stl.NativeEngine(NSIDE, J, batch=2, spin=2, cross=True)
+    o = S.SpinOracle(NSIDE, J, batch=2, cross=True)
+    e.set_masks(w)
+    o.set_masks(w)
+    assert np.array_equal(e.native_pixels(), o.native_pixels())
+    v, vo = e.forward_cross(a, b)[0], o.forward((a, b))
+    assert v.shape == vo.shape == (2, 2, 2, e.ncoeff)
+    assert np.abs(v - vo).max() <= 1e-12 * np.abs(vo).max()
+    cot = rng.normal(size=v.shape) + 0j
+    for x, y in zip(e.vjp_cross(cot), o.vjp(cot)):
+        assert np.abs(x - y).max() <= 1e-11 * np.abs(y).max()
+
+
+def test_fp32_cross_pairs_within_tolerance(stl):
+    """FP32 cross pairs (spin_a 0: a scalar T with (Q, U)) against FP64."""
+    rng = np.random.default_rng(16)
+    n = 12 * 64 ** 2
+    a, b = rng.normal(size=(2, n)), rng.normal(size=(2, 2, n))
+    v32 = stl.NativeEngine(64, 4, batch=2, spin=2, cross=True, spin_a=0, dtype="float32").forward_cross(a, b)[0]
+    v64 = stl.NativeEngine(64, 4, batch=2, spin=2, cross=True, spin_a=0).forward_cross(a, b)[0]
+    scale = np.abs(v64).max(axis=-1, keepdims=True)
+    err = np.maximum(np.abs((v32 - v64).real), np.abs((v32 - v64).imag))
+    assert (err <= 1e-6 * scale + 1e-6 * np.abs(v64)).all()
