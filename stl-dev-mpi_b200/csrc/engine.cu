@@ -114,9 +114,10 @@ class CopyPool {
   }
   // dst[0, n) = src[0, n), split over the threads; returns when done.  With
   // check (n a multiple of 8): the number of non-finite doubles copied.
-  size_t copy(void* dst, const void* src, size_t n, bool check = false) {
-    if (n < (size_t(1) << 20) || workers_.empty()) return copy_part(static_cast<char*>(dst),
-                                                                     static_cast<const char*>(src), n, check);
+  // With widen: src holds n bytes of floats, dst receives them as doubles.
+  size_t copy(void* dst, const void* src, size_t n, bool check = false, bool widen = false) {
+    if (n < (size_t(1) << 20) || workers_.empty())
+      return copy_part(static_cast<char*>(dst), static_cast<const char*>(src), n, check, widen);
     std::unique_lock<std::mutex> lk(call_mu_);  // one copy at a time
     const size_t parts = workers_.size() + 1;
     const size_t part = ((n + parts - 1) / parts + 63) & ~(size_t)63;
@@ -127,6 +128,7 @@ class CopyPool {
       n_ = n;
       part_ = part;
       check_ = check;
+      widen_ = widen;
       bad_ = 0;
       pending_ = (int)workers_.size();
       ++gen_;
@@ -137,7 +139,13 @@ class CopyPool {
     done_.wait(g, [&] { return pending_ == 0; });
     return bad_ + b0;
   }
-  static size_t copy_part(char* dst, const char* src, size_t n, bool check) {
+  static size_t copy_part(char* dst, const char* src, size_t n, bool check, bool widen = false) {
+    if (widen) {  // floats to doubles (exact)
+      const float* s = reinterpret_cast<const float*>(src);
+      double* d = reinterpret_cast<double*>(dst);
+      for (size_t i = 0, m = n / 4; i < m; ++i) d[i] = (double)s[i];
+      return 0;
+    }
     if (!check) {
       std::memcpy(dst, src, n);
       return 0;
@@ -164,7 +172,7 @@ class CopyPool {
   }
   size_t run(size_t k) {
     const size_t lo = std::min(n_, k * part_), hi = std::min(n_, lo + part_);
-    return hi > lo ? copy_part(dst_ + lo, src_ + lo, hi - lo, check_) : 0;
+    return hi > lo ? copy_part(dst_ + (widen_ ? 2 * lo : lo), src_ + lo, hi - lo, check_, widen_) : 0;
   }
   void loop(size_t k) {
     uint64_t seen = 0;
@@ -186,7 +194,7 @@ class CopyPool {
   char* dst_ = nullptr;
   const char* src_ = nullptr;
   size_t n_ = 0, part_ = 0, bad_ = 0;
-  bool check_ = false;
+  bool check_ = false, widen_ = false;
   int pending_ = 0;
   uint64_t gen_ = 0;
 };
@@ -238,6 +246,33 @@ class HostStage {
     for (size_t c = 0; c < nc; ++c) {
       const size_t off = c * kChunk, len = std::min(kChunk, n - off);
       STL_CUDA(cudaMemcpyAsync(buf_[c & 1].p, static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, s));
+      STL_CUDA(cudaEventRecord(ev_[c & 1], s));
+      if (c > 0) drain(c - 1);
+    }
+    drain(nc - 1);
+  }
+  // host doubles dst <- device floats src (n floats), widened on the host: half
+  // the bytes cross PCIe; synchronises
+  void to_host_widen(double* dst, const float* src, size_t n, cudaStream_t s) {
+    const size_t bytes = n * sizeof(float);
+    if (bytes < kDirect) {
+      std::vector<float> tmp(n);
+      STL_CUDA(cudaMemcpyAsync(tmp.data(), src, bytes, cudaMemcpyDeviceToHost, s));
+      STL_CUDA(cudaStreamSynchronize(s));
+      for (size_t i = 0; i < n; ++i) dst[i] = (double)tmp[i];
+      return;
+    }
+    ensure();
+    const size_t nc = (bytes + kChunk - 1) / kChunk;
+    auto drain = [&](size_t c) {
+      const size_t off = c * kChunk, len = std::min(kChunk, bytes - off);
+      STL_CUDA(cudaEventSynchronize(ev_[c & 1]));
+      CopyPool::get().copy(reinterpret_cast<char*>(dst) + 2 * off, buf_[c & 1].p, len, false, true);
+    };
+    for (size_t c = 0; c < nc; ++c) {
+      const size_t off = c * kChunk, len = std::min(kChunk, bytes - off);
+      STL_CUDA(cudaMemcpyAsync(buf_[c & 1].p, reinterpret_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost,
+                               s));
       STL_CUDA(cudaEventRecord(ev_[c & 1], s));
       if (c > 0) drain(c - 1);
     }
@@ -1007,6 +1042,13 @@ class EngineImpl final : public Engine {
   void reverse_host(const double* cot, double* out) override {
     reverse_impl(cot);
     i64 n = (i64)opt_.B * npix(0);
+    if (!hi(0)) {  // FP32 gradients: moved as floats and widened on the host (exact)
+      prof_.launch(Profiler::ELEM, 1, n * (4.0 + esz(0)), 0.0, stream_, [&] {
+        to_map_major<float, float>(gX_[0].as<float>(), in_f64_.as<float>(), npix(0), opt_.B, stream_);
+      });
+      io_.to_host_widen(out, in_f64_.as<float>(), (size_t)n, stream_);
+      return;
+    }
     prof_.launch(Profiler::ELEM, 1, n * (8.0 + esz(0)), 0.0, stream_, [&] {
       typed(0, [&](auto t) {
         using U = typename decltype(t)::type;
