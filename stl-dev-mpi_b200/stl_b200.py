@@ -187,6 +187,14 @@ class NativeEngine:
     "float32": convolutions, moduli and products in FP32, the pixel sums in
     FP64).  Values are complex128 ``[batch, ncoeff]`` in the order of
     ``plan``.
+
+    ``spin=2``: the maps are (Q, U) ``[batch, 2, npix]``; the statistics are
+    those of chi_E and chi_B = -(d_x - i d_y)^2 (Q + iU) (a stencil of
+    ``spin_kernel`` cells a side), values ``[batch, 2, (K,) ncoeff]``;
+    ``spin_pyramid="transported"`` builds chi at every level from the
+    children's means turned into the parents' frames.  With ``cross=True``
+    the maps are pairs (a, b) (``forward_cross``), a a (Q, U) field
+    (``spin_a=2``) or a scalar map (``spin_a=0``).
     """
 
     def __init__(self, nside, j, batch=1, backend="gpu", kernel=5, orientations=4, device=0, dtype="float64",
