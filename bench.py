@@ -693,10 +693,12 @@ def main():
                 "split_from": f"{prof_steps} steps with CUDA events around every launch, after the timed steps"}
 
     # -- end to end through the reference-facing host API ---------------------
+    g_host = np.empty_like(x_host)  # the caller's gradient buffer, reused (vjp's out=)
+
     def step_e2e():
         g = next(gen)
         values, _ = eng.forward(x_host, generation=g)
-        eng.vjp(2.0 * (values - target), generation=g)
+        eng.vjp(2.0 * (values - target), generation=g, out=g_host)
 
     ms_e2e = time_steps(torch, step_e2e, max(2, args.steps // 2), 1, dist)
     e2e_steps = max(2, args.steps // 2)
@@ -709,7 +711,8 @@ def main():
     plan = eng.plan
     e2e = {"value": world * B * e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": B * npix * 8 + B * ncoeff * 16, "d2h_bytes_per_step": B * ncoeff * 16 + B * npix * 8,
-           "api": "stlp_forward + stlp_vjp (host f64 buffers)"}
+           "api": "stlp_forward + stlp_vjp (host f64 buffers, the gradient into a reused out= array; the FP32 "
+                  "gradient crosses PCIe as floats and is widened by the host threads)"}
     eng.close()
     del x, xt, grad
     torch.cuda.empty_cache()

@@ -493,14 +493,24 @@ class NativeEngine:
             raise ValueError("non-finite coefficient cotangent")
         return c
 
-    def vjp(self, cotangents, generation=0, member=0, objective="gaussian"):
-        """Gradient ``[batch, npix]`` of ``Re sum(conj(cotangents) * values)``."""
+    def vjp(self, cotangents, generation=0, member=0, objective="gaussian", out=None):
+        """Gradient ``[batch, npix]`` of ``Re sum(conj(cotangents) * values)``.
+        ``out``: a C-contiguous float64 array of the maps' size to write it into
+        (returned in the maps' shape), instead of a new array: a caller that
+        keeps one spares the page faults of fresh memory on every call."""
         with self._mutex:
             self._open()
             key = _key(generation, member, objective)
             self._require_state(key)
             c = self._cotangent(cotangents)
-            grad = np.empty(int(np.prod(self._map_shape)))
+            size = int(np.prod(self._map_shape))
+            if out is None:
+                grad = np.empty(size)
+            else:
+                if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                        and out.size == size):
+                    raise ValueError(f"out must be a C-contiguous float64 array of {size} values")
+                grad = out.reshape(-1)
             if self._lib.stlp_vjp(self._handle, _ptr(c.view(np.float64)), c.size, *key, _ptr(grad)):
                 raise _error()
             if self.spin and self.cross:  # (grad_a, grad_b) in the shapes of a and b
