@@ -719,6 +719,7 @@ def main():
 
     # -- FP64 plain single map --------------------------------------------------
     fp64 = None
+    fp64_split = None
     accuracy = None
     if not args.skip_fp64:
         e64 = stl_b200.NativeEngine(nside, J, batch=1, dtype="float64", device=dev.index, prepare=True,
@@ -736,6 +737,13 @@ def main():
 
         ms64 = time_steps(torch, step64, args.steps, args.warmup, dist)
         fp64 = world * args.steps / (ms64 / 1e3)
+        # its class split, from 3 profiled steps after the timed ones
+        e64.profile(on=True, reset=True)
+        for _ in range(3):
+            step64()
+        torch.cuda.synchronize()
+        fp64_split = {k: v["ms"] / 3 for k, v in e64.kernel_stats().items()}
+        e64.profile(on=False, reset=False)
         # the FP32 batch against FP64 on the same maps (after the timed steps):
         # every coefficient under the 1e-6 family criterion, and the gradients
         v64 = np.empty_like(v32)
@@ -775,6 +783,7 @@ def main():
                            "l2": "inputs larger than L2 (fields and operators of tens of GB per step)",
                            "parallelism": f"replicas x{world}",
                            "fp64_plain_evals_per_s": fp64,
+                           "fp64_plain_kernels_ms_per_step": fp64_split,
                            "fp32_batched_over_fp64_plain": (value / world) / (fp64 / world) if fp64 else None,
                            "evaluation_roofline": eval_roof, "accuracy": accuracy,
                            "max_err_ratio": accuracy["max_err_ratio"] if accuracy else None},

@@ -3104,14 +3104,16 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_rev(i64 N, int K, int B
   }
 }
 
-// ---- the forward with the four gauges in one CTA (levels with K <= kCross4MaxK) ----
+// ---- the forward with the four gauges in one CTA (levels with K <= kCross4MaxK) ---
 // The operands of a (pixel, map, operand) are the 4 gauges' complex values in
 // one run (32 bytes in FP32): a CTA that takes all four gauges of a pixel range
 // loads whole sectors, where one CTA a gauge used a quarter of each (the
 // products of the nside 1024 bench: 17.5 -> 14.3 ms; the same form of the VJP
 // was slower, 22.4 -> 27.2 ms, and is not used).  Staged values
 // sv[j][g][c][i] (i < K the operands, i = K the S1 factor), FP64.
-constexpr int kCross4MaxK = 21;  // 4 (K^2 + 1) entries within kCrossMaxEnt per thread
+// levels 0-2 (K = 5, 9, 13): the deeper levels have too few pixel ranges to
+// fill the GPU with a quarter of the CTAs (measured slower at K = 17, 21)
+constexpr int kCross4MaxK = 13;
 
 template <typename T>
 __device__ __forceinline__ void load_gauges(const typename V2<T>::type* src, double2 v[4]) {
