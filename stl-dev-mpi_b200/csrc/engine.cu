@@ -771,6 +771,11 @@ class EngineImpl final : public Engine {
     mpart_.alloc(sizeof(double) * kMeansBlocks * B * L);
     in_f64_.alloc(sizeof(double) * B * npix(0));
     field_bytes_ += partials_.bytes + sums_.bytes + gZ_.bytes + gBr_.bytes + in_f64_.bytes;
+    if (!hi(0)) {  // FP32 level 0: the rounding residuals of its deviations
+      xr_.alloc(sizeof(float) * B * npix(0));
+      STL_CUDA(cudaMemsetAsync(xr_.p, 0, xr_.bytes, stream_));
+      field_bytes_ += xr_.bytes;
+    }
     // partial sums of the row-centric adjoint
     {
       size_t cap = 0;
@@ -806,7 +811,7 @@ class EngineImpl final : public Engine {
       row_means<Tin>(x, false, false, N, B, mpart_.as<double>(), xc_.as<double>(), stream_);
       typed(0, [&](auto t) {
         using U = typename decltype(t)::type;
-        to_pixel_major<Tin, U>(x, X_[0].as<U>(), N, B, stream_, xc_.as<double>());
+        to_pixel_major<Tin, U>(x, X_[0].as<U>(), N, B, stream_, xc_.as<double>(), xr_.as<U>());
       });
     });
     for (int d = 1; d < levels_; ++d)
@@ -826,7 +831,8 @@ class EngineImpl final : public Engine {
       row_means<double>(in_f64_.as<double>(), false, false, npix(d), opt_.B, mpart_.as<double>(), c, stream_);
       typed(d, [&](auto t) {
         using U = typename decltype(t)::type;
-        to_pixel_major<double, U>(in_f64_.as<double>(), X_[d].as<U>(), npix(d), opt_.B, stream_, c);
+        to_pixel_major<double, U>(in_f64_.as<double>(), X_[d].as<U>(), npix(d), opt_.B, stream_, c,
+                                  d == 0 ? xr_.as<U>() : nullptr);
       });
       STL_CUDA(cudaStreamSynchronize(stream_));  // the staging buffer is reused for the next level
       off += n;
@@ -843,7 +849,7 @@ class EngineImpl final : public Engine {
         row_means<double>(x[d], false, false, npix(d), opt_.B, mpart_.as<double>(), c, stream_);
         typed(d, [&](auto t) {
           using U = typename decltype(t)::type;
-          to_pixel_major<double, U>(x[d], X_[d].as<U>(), npix(d), opt_.B, stream_, c);
+          to_pixel_major<double, U>(x[d], X_[d].as<U>(), npix(d), opt_.B, stream_, c, d == 0 ? xr_.as<U>() : nullptr);
         });
       });
     }
@@ -857,14 +863,17 @@ class EngineImpl final : public Engine {
     else load_maps(static_cast<const double*>(x));
   }
 
-  // the level-0 deviations (exact in FP64) and their constants
+  // the level-0 deviations in FP64 (FP32 fields: with their residuals) and
+  // their constants
   void save_state(std::vector<double>& st) override {
     const size_t n = (size_t)opt_.B * npix(0);
     st.resize(n + opt_.B);
-    typed(0, [&](auto t) {
-      using U = typename decltype(t)::type;
-      convert<U, double>(X_[0].as<U>(), in_f64_.as<double>(), (i64)n, stream_);
-    });
+    if (xr_.p) join_f64(X_[0].as<float>(), xr_.as<float>(), in_f64_.as<double>(), (i64)n, stream_);
+    else
+      typed(0, [&](auto t) {
+        using U = typename decltype(t)::type;
+        convert<U, double>(X_[0].as<U>(), in_f64_.as<double>(), (i64)n, stream_);
+      });
     STL_CUDA(cudaMemcpyAsync(st.data(), in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
     STL_CUDA(cudaMemcpyAsync(st.data() + n, xc_.p, sizeof(double) * opt_.B, cudaMemcpyDeviceToHost, stream_));
     STL_CUDA(cudaStreamSynchronize(stream_));
@@ -874,10 +883,12 @@ class EngineImpl final : public Engine {
     const size_t n = (size_t)opt_.B * npix(0);
     if (st.size() != n + (size_t)opt_.B) throw std::runtime_error("checkpoint of another configuration");
     STL_CUDA(cudaMemcpyAsync(in_f64_.p, st.data(), n * 8, cudaMemcpyHostToDevice, stream_));
-    typed(0, [&](auto t) {
-      using U = typename decltype(t)::type;
-      convert<double, U>(in_f64_.as<double>(), X_[0].as<U>(), (i64)n, stream_);
-    });
+    if (xr_.p) split_f64(in_f64_.as<double>(), X_[0].as<float>(), xr_.as<float>(), (i64)n, stream_);
+    else
+      typed(0, [&](auto t) {
+        using U = typename decltype(t)::type;
+        convert<double, U>(in_f64_.as<double>(), X_[0].as<U>(), (i64)n, stream_);
+      });
     for (int d = 0; d < levels_; ++d)
       STL_CUDA(cudaMemcpyAsync(xc_.as<double>() + (size_t)d * opt_.B, st.data() + n, sizeof(double) * opt_.B,
                                cudaMemcpyHostToDevice, stream_));
@@ -888,6 +899,19 @@ class EngineImpl final : public Engine {
 
   void save_input(std::vector<double>& x) override {
     i64 n = (i64)opt_.B * npix(0);
+    if (xr_.p) {  // deviations and residuals in FP64 (pixel-major), then map-major plus the constants
+      const i64 N = npix(0);
+      const int B = opt_.B;
+      std::vector<double> d(n), c(B);
+      join_f64(X_[0].as<float>(), xr_.as<float>(), in_f64_.as<double>(), n, stream_);
+      STL_CUDA(cudaMemcpyAsync(d.data(), in_f64_.p, n * 8, cudaMemcpyDeviceToHost, stream_));
+      STL_CUDA(cudaMemcpyAsync(c.data(), xc_.p, sizeof(double) * B, cudaMemcpyDeviceToHost, stream_));
+      STL_CUDA(cudaStreamSynchronize(stream_));
+      x.resize(n);
+      for (int b = 0; b < B; ++b)
+        for (i64 p = 0; p < N; ++p) x[(size_t)b * N + p] = d[(size_t)p * B + b] + c[b];
+      return;
+    }
     typed(0, [&](auto t) {
       using U = typename decltype(t)::type;
       to_map_major<U, double>(X_[0].as<U>(), in_f64_.as<double>(), npix(0), opt_.B, stream_, xc_.as<double>());
@@ -1033,7 +1057,7 @@ class EngineImpl final : public Engine {
       prof_.launch(Profiler::PROD_FWD, 2, (double)B * L * N * sh.K * 2 * sizeof(U), (double)B * L * N * E * 10.0, s,
                    [&] {
                      products_forward<U>(sh, zf<U>(n), brf<U>(n), n == 0 ? X_[0].as<U>() : nullptr,
-                                         xc_.as<double>(), mask(k, n), partials_.as<double>(),
+                                         n == 0 ? xr_.as<U>() : nullptr, xc_.as<double>(), mask(k, n), partials_.as<double>(),
                                          sums_.as<double>() + k * total_sums_ + sum_off_[n], err_.as<int>(), s,
                                          moments);
                    });
@@ -1666,6 +1690,9 @@ class EngineImpl final : public Engine {
   HostStage io_;                     // large host <-> device copies
   bool objective_set_ = false;
   DevMem xc_, zc_, rc_, mpart_;  // field constants (see row_means in kernels.cu)
+  // FP32 level 0: the rounding residuals of the deviations X_[0], so that the
+  // map sums (the mean and variance) are those of the FP64 maps
+  DevMem xr_;
   std::vector<DevMem> ids_dev_;  // grid mode: supports per level
   // averaging masks [k][level] (grid mode: the core; none: every pixel) and
   // their pixel counts

@@ -334,11 +334,12 @@ void segment_ranges(ProductShape& sh, const std::vector<i64>& seg);
 // z [N][B][L], br [N][B][(n+1) L][L] complex, x0 [N][B] (level 0) ->
 // sums [B][L][slots] (FP64), per segment with segments
 // *err becomes nonzero when a wait on a staged copy timed out.  x0 holds
-// the level-0 maps as deviations from x0c [B].
+// the level-0 maps as deviations from x0c [B], x0r (or null) their rounding
+// residuals: the map sums take x0c + x0 + x0r in FP64.
 // mask (or null): 1 on the pixels the sums cover.  moments: also the
 // second sums the coefficient variances need (otherwise zero).
 template <typename T>
-void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
+void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const T* x0r, const double* x0c,
                       const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s, bool moments);
 // M [B][L][K][K] complex, s1c [B][L] -> gz [N][B][L], gbr [N][B][(n+1) L][L]
 // (with segments: M [nseg][B][L][K][K], s1c [nseg][B][L])
@@ -420,9 +421,14 @@ void moduli_deviations(const T* z, i64 N, int B, int L, const double* cz, T* mod
 void branch_constants(const double* zc, int n, int B, int L, double* rc, cudaStream_t s);
 template <typename Tin, typename Tout>
 void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s);
-// [B][N] map-major <-> [N][B] pixel-major (minus sub[b] / plus add[b] in FP64)
+// [B][N] map-major <-> [N][B] pixel-major (minus sub[b] / plus add[b] in
+// FP64); res (or null): the rounding residual of each output, in Tout
 template <typename Tin, typename Tout>
-void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub = nullptr);
+void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub = nullptr,
+                    Tout* res = nullptr);
+// FP64 values as FP32 pairs (hi rounded, lo the rounded rest) and back
+void split_f64(const double* x, float* hi, float* lo, i64 n, cudaStream_t s);
+void join_f64(const float* hi, const float* lo, double* x, i64 n, cudaStream_t s);
 template <typename Tin, typename Tout>
 void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* add = nullptr);
 

@@ -321,6 +321,9 @@ __host__ __device__ inline int fwd_plane_cells(int nc) {
 
 template <typename T>
 __host__ __device__ constexpr int fwd_sc() { return sizeof(T) == 4 ? 8 : 4; }
+// bulk-copy stages of the coefficient stream
+template <typename T>
+__host__ __device__ constexpr int fwd_stages() { return 2; }
 
 template <typename T, int RB>
 __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
@@ -328,15 +331,15 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     const int32_t* __restrict__ tile_cells, const int32_t* __restrict__ tile_nc, const T* __restrict__ x, int R,
     T* __restrict__ out, T* __restrict__ mod, int mod_pix, int mod_row, int mod_off, int* __restrict__ err,
     const T* __restrict__ rowsum, const double* __restrict__ rc, const int32_t* __restrict__ tile_slots) {
-  constexpr int SC = fwd_sc<T>();
+  constexpr int SC = fwd_sc<T>(), NST = fwd_stages<T>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // bar: a stage's copies have landed; empty: every warp has read the stage
-  __shared__ __align__(8) uint64_t bar[2], empty[2];
+  __shared__ __align__(8) uint64_t bar[NST], empty[NST];
   __shared__ int fail;
   // stage: coef [SC][kAdjTile][8] T, then indices [SC][kAdjTile] uint16
   constexpr size_t kStageCoef = (size_t)SC * kAdjTile * 8 * sizeof(T);
   constexpr size_t kStage = kStageCoef + (size_t)SC * kAdjTile * sizeof(uint16_t);
-  T* sx = reinterpret_cast<T*>(smem_raw + 2 * kStage);  // [4][pc][RB]: cell nc (padding) is zero
+  T* sx = reinterpret_cast<T*>(smem_raw + NST * kStage);  // [4][pc][RB]: cell nc (padding) is zero
   const int ngroups = R / RB;  // CTAs of a tile: consecutive, so its coefficients stay in L2
   const int tile = blockIdx.x / ngroups, tid = threadIdx.x;
   const int k = tid & 3, row = tid >> 2;
@@ -348,17 +351,18 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   S = tile_slots[tile];              // the tile's rows use no later slot
   const int nch = (S + SC - 1) / SC;
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_init(&empty[0], kFwdThreads / 32);
-    mbar_init(&empty[1], kFwdThreads / 32);
+#pragma unroll
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&bar[q], 1);
+      mbar_init(&empty[q], kFwdThreads / 32);
+    }
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int c) {
-    const int st = c & 1;
+    const int st = c % NST;
     unsigned char* base = smem_raw + st * kStage;
     const int s0 = c * SC, sn = min(SC, S - s0);
     const int sn4 = min(SC, S4 - s0);  // index rows are padded to 4 slots
@@ -369,10 +373,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
       bulk_g2s(base + (size_t)sl * kAdjTile * 8 * sizeof(T), coef + ((i64)(s0 + sl) * n_rep + u0) * 8, cb, &bar[st]);
     bulk_g2s(base + kStageCoef, lcell_t + ((i64)tile * S4 + s0) * kAdjTile, lb, &bar[st]);
   };
-  if (tid == 0) {
-    issue(0);
-    if (nch > 1) issue(1);
-  }
+  if (tid == 0)
+    for (int c = 0; c < min(nch, NST); ++c) issue(c);
   const int32_t* tc = tile_cells + (i64)tile * kAdjCells;
   // planes of pc >= nc + 1 cells, pc chosen so that consecutive planes start
   // 32 bytes apart modulo 128: the 4 rotations of a row, which read the same
@@ -398,10 +400,11 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   // warps drift apart by up to a stage.
   const int lane = tid & 31;
   bool ok = true;
-  int issued = min(nch, 2);  // chunks issued (thread 0's count)
+  int issued = min(nch, NST);  // chunks issued (thread 0's count)
   for (int c = 0; c < nch; ++c) {
-    const int st = c & 1;
-    if (!mbar_wait(&bar[st], (c >> 1) & 1)) {
+    const int st = c % NST;
+    const unsigned par = (unsigned)(c / NST) & 1;
+    if (!mbar_wait(&bar[st], par)) {
       ok = false;
       break;
     }
@@ -426,13 +429,13 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[st]);
-    if (tid == 0 && c + 2 < nch) {
-      if (!mbar_wait(&empty[st], (c >> 1) & 1)) {
+    if (tid == 0 && c + NST < nch) {
+      if (!mbar_wait(&empty[st], par)) {
         ok = false;
         break;
       }
-      issue(c + 2);
-      issued = c + 3;
+      issue(c + NST);
+      issued = c + NST + 1;
     }
   }
   if (!ok) fail = 1;
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
   if (fail) {  // thread 0 waits (bounded) for the copies it may have in flight
     if (tid == 0) {
       bool drained = true;
-      for (int q = max(0, issued - 2); q < issued; ++q) drained &= mbar_wait(&bar[q & 1], (q >> 1) & 1);
+      for (int q = max(0, issued - NST); q < issued; ++q) drained &= mbar_wait(&bar[q % NST], (q / NST) & 1);
       atomicMax(err, drained ? kErrWait : kErrDrain);
     }
     return;
@@ -1376,7 +1379,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
     int nd, i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0, int slots,
     const int32_t* __restrict__ roles, int W, int PC, i64 chunk, double* __restrict__ partials,
     int* __restrict__ err, const double* __restrict__ x0c, const uint8_t* __restrict__ mask,
-    const i64* __restrict__ blk) {
+    const i64* __restrict__ blk, const T* __restrict__ x0r) {
   typedef typename V2<T>::type T2;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[kProdStages];
@@ -1500,7 +1503,8 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
             f[1] += m2;
             if (MOM) f[2] = fma(m2, m2, f[2]);
             if (x0 && l3 == 0) {
-              const double xv = x0c[b] + (double)sx[(size_t)j * B + b];
+              const double xv = x0c[b] + (double)sx[(size_t)j * B + b] +
+                                (x0r ? (double)x0r[(pc + j) * B + b] : 0.0);
               const double x2 = xv * xv;
               acc[3] += xv;
               acc[4] += x2;
@@ -1654,7 +1658,7 @@ template <typename T, int ND>
 __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
     i64 N, int B, const T* __restrict__ z, const T* __restrict__ br, const T* __restrict__ x0,
     const double* __restrict__ x0c, const uint8_t* __restrict__ mask, i64 chunk, int slots,
-    double* __restrict__ partials, const i64* __restrict__ blk) {
+    double* __restrict__ partials, const i64* __restrict__ blk, const T* __restrict__ x0r) {
   typedef typename V2<T>::type T2;
   constexpr int NF = p0_sums<ND>(), OFF = ND * 16 + ND * (ND - 1) / 2 * 32, ZB = OFF;  // (d, z) blocks start
   extern __shared__ __align__(16) double p0s[];  // [warps][4B][NF], then map sums [warps][B][2]
@@ -1756,7 +1760,7 @@ __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
       f[NF - 2] += m;
       f[NF - 1] = fma(m, m, f[NF - 1]);
       if (x0 && l3 == 0) {
-        const double xv = x0c[b] + (double)x0[p * B + b];
+        const double xv = x0c[b] + (double)x0[p * B + b] + (x0r ? (double)x0r[p * B + b] : 0.0);
         xs += xv;
         xs2 += xv * xv;
       }
@@ -1794,14 +1798,14 @@ __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
 }
 
 template <typename T, int ND>
-void products0_launch(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
+void products0_launch(const ProductShape& sh, const T* z, const T* br, const T* x0, const T* x0r, const double* x0c,
                       const uint8_t* mask, double* partials, cudaStream_t s) {
   const int nw = p0_warps<T, ND>(sh.B);
   const size_t smem = (size_t)nw * (4 * sh.B * p0_sums<ND>() + sh.B * 2) * sizeof(double);
   allow_dynamic_smem(k_products0<T, ND>);
   const i64 chunk = (sh.N + sh.blocks - 1) / sh.blocks;
   k_products0<T, ND><<<sh.blocks, 32 * nw, smem, s>>>(sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, x0c, mask, chunk,
-                                                      sh.slots, partials, sh.d_blk);
+                                                      sh.slots, partials, sh.d_blk, sh.level0 ? x0r : nullptr);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -2084,15 +2088,32 @@ __global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, i6
 }
 
 // [B][N] <-> [N][B] transposes of the level-0 maps at the boundary
+// res (optional): the rounding residual of out, (x - sub) - out rounded to Tout
 template <typename Tin, typename Tout, typename I>
 __global__ void k_to_pixel_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B,
-                                 const double* __restrict__ sub) {
+                                 const double* __restrict__ sub, Tout* __restrict__ res) {
   const I i = (I)blockIdx.x * blockDim.x + threadIdx.x;  // over N * B, output order
   if ((i64)i >= N * B) return;
   const I p = i / (I)B;
   const int b = (int)(i - p * (I)B);
   const Tin v = in[(i64)b * N + p];
-  out[i] = sub ? (Tout)((double)v - sub[b]) : (Tout)v;
+  const double d = sub ? (double)v - sub[b] : (double)v;
+  const Tout o = (Tout)d;
+  out[i] = o;
+  if (res) res[i] = (Tout)(d - (double)o);
+}
+// FP64 values as FP32 pairs: hi = x rounded, lo = (x - hi) rounded
+__global__ void k_split_f64(const double* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo, i64 n) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float h = (float)x[i];
+  hi[i] = h;
+  lo[i] = (float)(x[i] - (double)h);
+}
+__global__ void k_join_f64(const float* __restrict__ hi, const float* __restrict__ lo, double* __restrict__ x, i64 n) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = (double)hi[i] + (double)lo[i];
 }
 template <typename Tin, typename Tout, typename I>
 __global__ void k_to_map_major(const Tin* __restrict__ in, Tout* __restrict__ out, i64 N, int B,
@@ -2317,7 +2338,7 @@ inline int adj_rb(const ConvOp& op, size_t elem, int R) {
 template <typename T, int RB>
 size_t fwd_tiles_smem(const ConvOp& op) {
   const size_t stage = (size_t)fwd_sc<T>() * kAdjTile * (8 * sizeof(T) + sizeof(uint16_t));
-  return 2 * stage + sizeof(T) * 4 * (size_t)(op.max_tile_cells + 1 + 32) * RB;
+  return fwd_stages<T>() * stage + sizeof(T) * 4 * (size_t)(op.max_tile_cells + 1 + 32) * RB;
 }
 
 template <typename T, int RB>
@@ -2653,15 +2674,15 @@ void products_reverse_k(const ProductShape& sh, const T* z, const T* br, const T
 }  // namespace
 
 template <typename T>
-void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const double* x0c,
+void products_forward(const ProductShape& sh, const T* z, const T* br, const T* x0, const T* x0r, const double* x0c,
                       const uint8_t* mask, double* partials, double* sums, int* err, cudaStream_t s, bool moments) {
   if (sh.level0 && !x0c) throw std::runtime_error("level-0 products need the map constants");
   const int L = sh.L, nd = sh.nd;
   if (!sh.d_roles) throw std::runtime_error("products role table not on the device");
   // levels 0 and 1 without variances: the register-resident kernel
   if (!moments && (sh.nd == 1 || sh.nd == 2) && 32 % (4 * sh.B) == 0 && (!sh.level0 || x0)) {
-    if (sh.nd == 1) products0_launch<T, 1>(sh, z, br, x0, x0c, mask, partials, s);
-    else products0_launch<T, 2>(sh, z, br, x0, x0c, mask, partials, s);
+    if (sh.nd == 1) products0_launch<T, 1>(sh, z, br, x0, x0r, x0c, mask, partials, s);
+    else products0_launch<T, 2>(sh, z, br, x0, x0r, x0c, mask, partials, s);
     reduce_partials(sh, partials, sums, s);
     return;
   }
@@ -2670,7 +2691,8 @@ void products_forward(const ProductShape& sh, const T* z, const T* br, const T* 
     allow_dynamic_smem(kern);
   dim3 grid(sh.blocks, 1, sh.item_chunks);
   kern<<<grid, 32 * sh.warps, sh.smem, s>>>(nd, sh.N, sh.B, z, br, sh.level0 ? x0 : nullptr, sh.slots, sh.d_roles,
-                                             sh.warps, sh.px_chunk, sh.chunk, partials, err, x0c, mask, sh.d_blk);
+                                             sh.warps, sh.px_chunk, sh.chunk, partials, err, x0c, mask, sh.d_blk,
+                                             sh.level0 ? x0r : nullptr);
   STL_CUDA(cudaGetLastError());
   reduce_partials(sh, partials, sums, s);
 }
@@ -3374,9 +3396,22 @@ void convert(const Tin* in, Tout* out, i64 n, cudaStream_t s) {
 }
 
 template <typename Tin, typename Tout>
-void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub) {
-  if (N * B < ((i64)1 << 31)) k_to_pixel_major<Tin, Tout, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub);
-  else k_to_pixel_major<Tin, Tout, i64><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub);
+void to_pixel_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const double* sub, Tout* res) {
+  if (N * B < ((i64)1 << 31))
+    k_to_pixel_major<Tin, Tout, uint32_t><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub, res);
+  else k_to_pixel_major<Tin, Tout, i64><<<nblocks(N * B, 256), 256, 0, s>>>(in, out, N, B, sub, res);
+  STL_CUDA(cudaGetLastError());
+}
+
+void split_f64(const double* x, float* hi, float* lo, i64 n, cudaStream_t s) {
+  if (n <= 0) return;
+  k_split_f64<<<nblocks(n, 256), 256, 0, s>>>(x, hi, lo, n);
+  STL_CUDA(cudaGetLastError());
+}
+
+void join_f64(const float* hi, const float* lo, double* x, i64 n, cudaStream_t s) {
+  if (n <= 0) return;
+  k_join_f64<<<nblocks(n, 256), 256, 0, s>>>(hi, lo, x, n);
   STL_CUDA(cudaGetLastError());
 }
 
@@ -3393,7 +3428,7 @@ void to_map_major(const Tin* in, Tout* out, i64 N, int B, cudaStream_t s, const 
   template void conv_adjoint<T>(const ConvOp&, const T*, int, T*, bool, cudaStream_t, const AdjScratch*, int*,        \
                                 const ModulusAdd<T>*, int);                                                           \
   template void modulus_vjp_add<T>(const T*, const T*, int, int, T*, i64, int, int, cudaStream_t);                \
-  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const double*,             \
+  template void products_forward<T>(const ProductShape&, const T*, const T*, const T*, const T*, const double*,  \
                                     const uint8_t*, double*, double*, int*, cudaStream_t, bool);                                                                \
   template void products_reverse<T>(const ProductShape&, const T*, const T*, const T*, const T*, const uint8_t*, \
                                     bool, T*, T*, cudaStream_t);                                                                \
@@ -3421,10 +3456,10 @@ template void convert<double, float>(const double*, float*, i64, cudaStream_t);
 template void convert<float, double>(const float*, double*, i64, cudaStream_t);
 template void convert<double, double>(const double*, double*, i64, cudaStream_t);
 template void convert<float, float>(const float*, float*, i64, cudaStream_t);
-template void to_pixel_major<double, float>(const double*, float*, i64, int, cudaStream_t, const double*);
-template void to_pixel_major<double, double>(const double*, double*, i64, int, cudaStream_t, const double*);
-template void to_pixel_major<float, float>(const float*, float*, i64, int, cudaStream_t, const double*);
-template void to_pixel_major<float, double>(const float*, double*, i64, int, cudaStream_t, const double*);
+template void to_pixel_major<double, float>(const double*, float*, i64, int, cudaStream_t, const double*, float*);
+template void to_pixel_major<double, double>(const double*, double*, i64, int, cudaStream_t, const double*, double*);
+template void to_pixel_major<float, float>(const float*, float*, i64, int, cudaStream_t, const double*, float*);
+template void to_pixel_major<float, double>(const float*, double*, i64, int, cudaStream_t, const double*, double*);
 template void to_map_major<float, double>(const float*, double*, i64, int, cudaStream_t, const double*);
 template void to_map_major<double, double>(const double*, double*, i64, int, cudaStream_t, const double*);
 template void to_map_major<float, float>(const float*, float*, i64, int, cudaStream_t, const double*);

@@ -101,6 +101,38 @@ def test_fp32_masks_within_1e6(stl):
     e.close()
 
 
+@pytest.mark.parametrize("masked", [False, True])
+@pytest.mark.parametrize("moments", [False, True])
+def test_fp32_map_sums_are_those_of_the_fp64_maps(stl, masked, moments):
+    """FP32 fields hold the maps' deviations from their means rounded to FP32;
+    the map sums add the rounding residuals back, so a mean near zero (1e-7
+    against deviations of 1, on the sky or under a latitude mask) keeps the
+    FP64 engine's value to 1e-6 of itself, and the variance to 1e-12."""
+    nside, J, B = 64, 4, 2
+    rng = np.random.default_rng(44)
+    g = rng.standard_normal((B, 12 * nside * nside))
+    cut = latitude_cut(nside, 20.0)
+    over = g[:, cut] if masked else g
+    x = g - over.mean(axis=1, keepdims=True) + 1e-7 * (1.0 + np.arange(B))[:, None]
+    e32 = stl.NativeEngine(nside, J, batch=B, dtype="float32")
+    e64 = stl.NativeEngine(nside, J, batch=B, dtype="float64")
+    if masked:
+        e32.set_masks([cut])
+        e64.set_masks([cut])
+    v32, var32 = e32.forward(x, moments=moments)
+    v64, var64 = e64.forward(x, moments=moments)
+    fam = [c["family"] for c in e32.plan]
+    im, iv = fam.index("mean"), fam.index("var")
+    m32, m64 = v32[..., im].real, v64[..., im].real
+    assert np.max(np.abs(m64)) < 1e-6
+    assert np.max(np.abs(m32 - m64) / np.abs(m64)) <= 1e-6
+    assert np.max(np.abs(v32[..., iv] - v64[..., iv]) / np.abs(v64[..., iv])) <= 1e-12
+    if moments:
+        assert np.max(np.abs(var32[..., im] - var64[..., im]) / var64[..., im]) <= 1e-9
+    e32.close()
+    e64.close()
+
+
 def test_masks_reset_and_refusals(stl):
     nside, J = 16, 3
     rng = np.random.default_rng(42)

@@ -100,6 +100,44 @@ def test_fp32_disc_within_1e6(stl):
     assert worst <= 1.0
 
 
+@pytest.mark.parametrize("moments", [False, True])
+def test_fp32_disc_means_near_zero(stl, moments):
+    """Disc values whose mean is near zero (1e-7 against values of 1): the FP32
+    engine's mean of each disc is the FP64 engine's to 1e-6 of itself (the
+    map sums take the FP32 deviations with their rounding residuals), and
+    every other coefficient within the 1e-6 family criterion."""
+    nside, J = 128, 4
+    centres = np.array([100, 30000, 70000, 150000, 190000], dtype=np.int64)
+    p32 = stl.PatchEngine(nside, J, dtype="float32")
+    p64 = stl.PatchEngine(nside, J, dtype="float64")
+    ids = p32.select(centres, 12.0)
+    p64.select(centres, 12.0)
+    rng = np.random.default_rng(9)
+    xs = []
+    for k, i in enumerate(ids):
+        v = rng.standard_normal(i.size)
+        xs.append(v - v.mean() + 1e-7 * (k + 1))
+    v32, var32 = p32.forward(xs, moments=moments)
+    v64, var64 = p64.forward(xs, moments=moments)
+    fam = np.array([c["family"] for c in p64.plan])
+    lev = np.array([c["native_dg"] for c in p64.plan])
+    im = int(np.flatnonzero(fam == "mean")[0])
+    assert np.max(np.abs(v64[:, im])) < 1e-6
+    assert np.max(np.abs(v32[:, im].real - v64[:, im].real) / np.abs(v64[:, im].real)) <= 1e-6
+    worst = 0.0
+    for f in set(fam):
+        for n in set(lev):
+            sel = (fam == f) & (lev == n)
+            if sel.any():
+                r, a = v64[:, sel], v32[:, sel]
+                scale = np.max(np.abs(r), axis=1, keepdims=True)
+                for part in (np.real, np.imag):
+                    worst = max(worst, float(np.max(np.abs(part(a) - part(r)) / (1e-6 * scale + 1e-6 * np.abs(part(r))))))
+    assert worst <= 1.0
+    if moments:
+        assert np.max(np.abs(var32[:, im] - var64[:, im]) / var64[:, im]) <= 1e-9
+
+
 def test_batched_discs_match_one_engine_per_disc(stl):
     """Discs of different sizes (one selected twice, cores on some) in one
     segmented engine, in two groups, and one engine per disc: the same
