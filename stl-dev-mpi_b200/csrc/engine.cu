@@ -33,6 +33,7 @@
 #include <string>
 
 #include "engine.cuh"
+#include "hostcopy.hpp"
 #include "scatcov.hpp"
 
 namespace stl {
@@ -141,26 +142,10 @@ class CopyPool {
   }
   static size_t copy_part(char* dst, const char* src, size_t n, bool check, bool widen = false) {
     if (widen) {  // floats to doubles (exact)
-      const float* s = reinterpret_cast<const float*>(src);
-      double* d = reinterpret_cast<double*>(dst);
-      for (size_t i = 0, m = n / 4; i < m; ++i) d[i] = (double)s[i];
+      host_widen(reinterpret_cast<double*>(dst), reinterpret_cast<const float*>(src), n / 4);
       return 0;
     }
-    if (!check) {
-      std::memcpy(dst, src, n);
-      return 0;
-    }
-    // doubles whose exponent bits are all ones are inf or nan
-    const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
-    uint64_t* d = reinterpret_cast<uint64_t*>(dst);
-    const uint64_t e = 0x7FF0000000000000ull;
-    size_t bad = 0;
-    for (size_t i = 0, m = n / 8; i < m; ++i) {
-      const uint64_t v = s[i];
-      d[i] = v;
-      bad += (v & e) == e;
-    }
-    return bad;
+    return host_copy(dst, src, n, check);
   }
 
  private:
