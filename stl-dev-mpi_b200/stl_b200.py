@@ -768,6 +768,7 @@ class PatchEngine:
         self.levels = info["levels"]
         self._native = np.array([c["native_dg"] for c in self.plan], dtype=np.int64)
         self.ids, self._selection, self._generation, self._dense = [], None, None, False
+        self._xbuf = None  # the packed patches of the current selection
 
     def _open(self):
         if not self._handle:
@@ -857,7 +858,14 @@ class PatchEngine:
         for i, (m, size) in enumerate(zip(flat, sizes)):
             if m.shape != (size,):
                 raise ValueError(f"patch {i} has shape {m.shape}; its disc holds {size} pixels")
-        return np.ascontiguousarray(np.concatenate(flat)) if flat else np.zeros(0)
+        if not flat:
+            return np.zeros(0)
+        # one buffer per selection, reused: the library has read it when the
+        # call returns, and fresh memory would cost its page faults every call
+        total = sum(sizes)
+        if self._xbuf is None or self._xbuf.size != total:
+            self._xbuf = np.empty(total, dtype=np.float64)
+        return np.concatenate(flat, out=self._xbuf)
 
     def forward(self, maps, centres=None, radius=None, core=None, moments=True, generation=0):
         """Statistics [B, ncoeff] (and variances, or [B, 0]) of the patches of
@@ -883,9 +891,12 @@ class PatchEngine:
             self._generation = int(generation)
             return values, variance
 
-    def vjp(self, cotangents, generation=0):
+    def vjp(self, cotangents, generation=0, out=None):
         """Gradients of Re sum(conj(cotangents) values) with respect to the
-        patches of the forward of this generation, shaped like its maps."""
+        patches of the forward of this generation, shaped like its maps.
+        ``out``: a C-contiguous float64 array of the selection's total pixel
+        count to write them into (the gradients returned are views of it):
+        a caller that keeps one spares the page faults of fresh memory."""
         with self._mutex:
             self._open()
             if self._generation is None or int(generation) != self._generation:
@@ -897,7 +908,14 @@ class PatchEngine:
             if not np.isfinite(c.view(np.float64)).all():
                 raise ValueError("non-finite coefficient cotangent")
             sizes = np.array([i.size for i in self.ids], dtype=np.int64)
-            grad = np.empty(int(sizes.sum()), dtype=np.float64)
+            total = int(sizes.sum())
+            if out is None:
+                grad = np.empty(total, dtype=np.float64)
+            else:
+                if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                        and out.size == total):
+                    raise ValueError(f"out must be a C-contiguous float64 array of {total} values")
+                grad = out.reshape(-1)
             if self._lib.stlp_patch_vjp(self._handle, _ptr(c.view(np.float64)), c.size, int(generation),
                                         _ptr(grad)):
                 raise _error()

@@ -185,6 +185,36 @@ def test_batched_discs_match_one_engine_per_disc(stl):
         assert np.max(np.abs(runs["batch32"][2][k] - g[k])) <= 1e-5 * np.max(np.abs(g[k]))
 
 
+def test_vjp_into_a_kept_array_and_the_reused_input_buffer(stl):
+    """vjp(out=) writes the same gradients into the caller's array (the
+    patches returned are views of it); a second forward of other values
+    through the reused packing buffer equals a fresh engine's."""
+    nside, J = 32, 3
+    centres = np.array([100, 5000], dtype=np.int64)
+    pe = stl.PatchEngine(nside, J, dtype="float64")
+    ids = pe.select(centres, 20.0)
+    rng = np.random.default_rng(2)
+    xa = [rng.standard_normal(i.size) for i in ids]
+    xb = [rng.standard_normal(i.size) for i in ids]
+    va, _ = pe.forward(xa, moments=False, generation=1)
+    cot = rng.standard_normal(va.shape) + 1j * rng.standard_normal(va.shape)
+    ga = pe.vjp(cot, generation=1)
+    out = np.empty(sum(i.size for i in ids))
+    gb = pe.vjp(cot, generation=1, out=out)
+    for a, b in zip(ga, gb):
+        np.testing.assert_array_equal(a, b)
+    assert all(np.shares_memory(b, out) for b in gb)
+    with pytest.raises(ValueError):
+        pe.vjp(cot, generation=1, out=np.empty(3))
+    vb, _ = pe.forward(xb, moments=False, generation=2)
+    fresh = stl.PatchEngine(nside, J, dtype="float64")
+    fresh.select(centres, 20.0)
+    vb2, _ = fresh.forward(xb, moments=False, generation=1)
+    np.testing.assert_array_equal(vb, vb2)
+    pe.close()
+    fresh.close()
+
+
 def test_config4_subset_batched_equals_one_engine_per_disc(stl):
     """32 discs of the ragged workload of config 4 (nside 512, J 5, centres
     uniform on the sphere, pixel counts log-uniform in [1024, 65536]): the
