@@ -415,10 +415,12 @@ def run_cross(args, torch, dist, world, rank, dev):
     stats = eng.kernel_stats()
     eng.profile(on=False, reset=False)
 
+    g_host = np.empty(x_host.size)  # the gradients' array, kept across calls (vjp out=)
+
     def step_host():
         k = next(gen)
         values, _ = eng.forward(x_host, generation=k)
-        eng.vjp(2.0 * (values - target), generation=k)
+        eng.vjp(2.0 * (values - target), generation=k, out=g_host)
 
     e2e_steps = max(2, args.steps // 2)
     ms_e2e = time_steps(torch, step_host, e2e_steps, 1, dist)
@@ -478,10 +480,12 @@ def run_spin(args, torch, dist, world, rank, dev):
         ms = time_steps(torch, step, args.steps, 0, dist)
     clocks = clk.summary()
 
+    g_host = np.empty(x_host.size)  # the gradients' array, kept across calls (vjp out=)
+
     def step_host():
         k = next(gen)
         values, _ = eng.forward(x_host, generation=k)
-        eng.vjp(2.0 * (values - target), generation=k)
+        eng.vjp(2.0 * (values - target), generation=k, out=g_host)
 
     e2e_steps = max(2, args.steps // 2)
     ms_e2e = time_steps(torch, step_host, e2e_steps, 1, dist)
