@@ -207,6 +207,52 @@ __device__ __forceinline__ void addR_shared(T* p, const T a[RB]) {
   }
 }
 
+// The per-slot products of the tiled wavelets.  FP32 pairs go through the
+// paired FMA of sm_100 (__ffma2_rn: each component rounds as fmaf), half the
+// instructions of the scalar form.
+// acc[rb][j] += w[j] xv[rb]: the same roundings as scalar fmas, pair by pair
+template <int RB>
+__device__ __forceinline__ void fma_rows(float (&acc)[RB][8], const float (&w)[8], const float (&xv)[RB]) {
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb) {
+    const float2 x2 = make_float2(xv[rb], xv[rb]);
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      const float2 r = __ffma2_rn(make_float2(w[j], w[j + 1]), x2, make_float2(acc[rb][j], acc[rb][j + 1]));
+      acc[rb][j] = r.x;
+      acc[rb][j + 1] = r.y;
+    }
+  }
+}
+template <int RB>
+__device__ __forceinline__ void fma_rows(double (&acc)[RB][8], const double (&w)[8], const double (&xv)[RB]) {
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[rb][j] = fma(w[j], xv[rb], acc[rb][j]);
+}
+// a[rb] = sum_q w[q] g[rb][q]; FP32: the even and the odd terms in two
+// chains, then added (a fixed order)
+template <int RB>
+__device__ __forceinline__ void dot8_rows(const float (&w)[8], const float (&g)[RB][8], float (&a)[RB]) {
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb) {
+    float2 p = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 8; q += 2) p = __ffma2_rn(make_float2(w[q], w[q + 1]), make_float2(g[rb][q], g[rb][q + 1]), p);
+    a[rb] = p.x + p.y;
+  }
+}
+template <int RB>
+__device__ __forceinline__ void dot8_rows(const double (&w)[8], const double (&g)[RB][8], double (&a)[RB]) {
+#pragma unroll
+  for (int rb = 0; rb < RB; ++rb) {
+    a[rb] = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[rb] = fma(w[q], g[rb][q], a[rb]);
+  }
+}
+
 // gauge map of rotation k: output gauge g of pixel (4m + k) takes the
 // stored gauge (g + 2k) mod 4, conjugated when ((2k - g + 3) >> 2) is odd
 __host__ __device__ constexpr int rot_src(int k, int g) { return (g + 2 * k) & 3; }
@@ -420,10 +466,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
           load8_shared(cs + ((size_t)sl * kAdjTile + row) * 8, w);
           T xv[RB];
           loadR_shared<RB>(sxk + (size_t)ls[sl * kAdjTile + row] * RB, xv);
-#pragma unroll
-          for (int rb = 0; rb < RB; ++rb)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[rb][j] = fma(w[j], xv[rb], acc[rb][j]);
+          fma_rows<RB>(acc, w, xv);
         }
       }
     }
@@ -816,12 +859,7 @@ __global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
         T w[8];
         load8_shared(cs + ((size_t)sl * kAdjTile + row) * 8, w);
         T a[RB];
-#pragma unroll
-        for (int rb = 0; rb < RB; ++rb) {
-          a[rb] = (T)0;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) a[rb] = fma(w[q], g[rb][q], a[rb]);
-        }
+        dot8_rows<RB>(w, g, a);
         addR_shared<RB>(acc + ((size_t)lc * 4 + k) * RB, a);
       }
       __syncthreads();  // the slot's sums are in: the next slot may read them
