@@ -300,11 +300,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ ce
       if (s + 2 < S) cn = __ldg(cell + (i64)(s + 2) * n_rep + u);
     }
 #pragma unroll
-    for (int k = 0; k < NK; ++k)
-#pragma unroll
-      for (int rb = 0; rb < RB; ++rb)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[k][rb][j] = fma(w[j], xv[k][rb], acc[k][rb][j]);
+    for (int k = 0; k < NK; ++k) fma_rows<RB>(acc[k], w, xv[k]);
 #pragma unroll
     for (int k = 0; k < NK; ++k)
 #pragma unroll
