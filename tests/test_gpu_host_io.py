@@ -1,7 +1,8 @@
 """Host buffers through the C ABI (stlp_forward / stlp_vjp): large maps and
 gradients cross through pinned chunks filled and drained by host threads.
 The results equal those of the device-tensor entry points bit for bit, for
-buffers of several chunks and for one smaller than a chunk."""
+buffers of several chunks and for one smaller than a chunk, and so does the
+gradient written into a caller's array (vjp out=)."""
 import numpy as np
 import pytest
 
@@ -27,6 +28,14 @@ def test_host_buffers_equal_device_tensors(stl, nside, batch):
     v_host, _ = e.forward(x, generation=1)
     cot = rng.standard_normal(v_host.shape) + 1j * rng.standard_normal(v_host.shape)
     g_host = e.vjp(cot, generation=1)
+    # into a caller's array, twice (the second call overwrites the first)
+    out = np.full_like(x, np.nan)
+    for _ in range(2):
+        g_out = e.vjp(cot, generation=1, out=out)
+        assert np.shares_memory(g_out, out)
+        np.testing.assert_array_equal(g_out, g_host)
+    with pytest.raises(ValueError):
+        e.vjp(cot, generation=1, out=np.empty(3))
     xt = torch.tensor(x, dtype=torch.float64, device="cuda")
     v_dev, _ = e.forward_tensor(xt, generation=2)
     g_dev = torch.empty_like(xt)
