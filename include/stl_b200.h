@@ -172,6 +172,36 @@ int stlp_patch_vjp_device(StlpPatchHandle* h, const double* cot, size_t n, uint6
  * engine's memory in stlp_info, lib.rs:365-391, as stlp_info does here). */
 int stlp_memory(size_t* live, size_t* peak, int reset_peak);
 
+/* Map files, the formats on either side of the statistics: NESTED .npy
+ * arrays ('<f8' '>f8' '<f4' '>f4' '<i8' '>i8' '<i4' '>i4', C order) and
+ * HEALPix FITS binary tables (the map in the first column, 'E' or 'D', a
+ * repeat count allowed; RING maps reordered to NESTED on reading).  A path
+ * ending in .fits or .fit is FITS, any other .npy.  The reference's
+ * synthesis tools call these in-process (crates/stl-mpi/src/io.rs:18-569:
+ * map_len, read_map, read_npy_shape, read_map_range, write_npy_shape,
+ * write_healpix_fits, SlicedMap::create / write); no C entry to mirror.
+ *   stlp_map_len: *n = the pixels of the map;
+ *   stlp_npy_shape: *ndim and shape[0 .. ndim) of a .npy array (an error
+ *     when it has more than max_dims axes);
+ *   stlp_map_read: the whole map (NESTED float64) into out[n], n its length;
+ *   stlp_map_read_range: pixels [start, end) into out[end - start] (read at
+ *     their offset; a RING map is read whole);
+ *   stlp_npy_write: little-endian float64 .npy of shape[ndim];
+ *   stlp_fits_write: a full-sky NESTED map of n pixels as a binary table of
+ *     one column named `column`, float64 ('D') when dbl, else float32 ('E');
+ *   stlp_map_create / stlp_map_write: a file written in pieces (each
+ *     process its own range): the headers and the size for n pixels (.npy
+ *     float64, or FITS as stlp_fits_write), then pixels [start, start +
+ *     count) at their offset. */
+int stlp_map_len(const char* path, size_t* n);
+int stlp_npy_shape(const char* path, size_t* shape, size_t max_dims, size_t* ndim);
+int stlp_map_read(const char* path, double* out, size_t n);
+int stlp_map_read_range(const char* path, size_t start, size_t end, double* out);
+int stlp_npy_write(const char* path, const double* values, const size_t* shape, size_t ndim);
+int stlp_fits_write(const char* path, const double* values, size_t n, const char* column, int dbl);
+int stlp_map_create(const char* path, size_t n, const char* column, int dbl);
+int stlp_map_write(const char* path, size_t start, const double* values, size_t count, int dbl);
+
 /* The integer tables of the engine's operators, for exact checks: kind 0
  * the sorted distinct input cells (full-sky NESTED ids) each output pixel
  * of level `level` reads in its wavelet (weight: the cell's largest

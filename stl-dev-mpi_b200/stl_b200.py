@@ -104,6 +104,14 @@ def lib():
             "stlp_terms_sort": ([_VOID, u64, sz, u64], C.c_int),
             "stlp_terms_marginal": ([_VOID, u64, u64, u64, sz, C.c_double, u64, _D], C.c_int),
             "stlp_terms_add_product": ([_VOID, u64, u64, u64, sz], C.c_int),
+            "stlp_map_len": ([C.c_char_p, _SIZE], C.c_int),
+            "stlp_npy_shape": ([C.c_char_p, _SIZE, sz, _SIZE], C.c_int),
+            "stlp_map_read": ([C.c_char_p, _D, sz], C.c_int),
+            "stlp_map_read_range": ([C.c_char_p, sz, sz, _D], C.c_int),
+            "stlp_npy_write": ([C.c_char_p, _D, _SIZE, sz], C.c_int),
+            "stlp_fits_write": ([C.c_char_p, _D, sz, C.c_char_p, C.c_int], C.c_int),
+            "stlp_map_create": ([C.c_char_p, sz, C.c_char_p, C.c_int], C.c_int),
+            "stlp_map_write": ([C.c_char_p, sz, _D, sz, C.c_int], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(l, name)
@@ -119,6 +127,84 @@ def device_memory(reset_peak=False):
     if lib().stlp_memory(C.byref(live), C.byref(peak), int(bool(reset_peak))):
         raise _error()
     return live.value, peak.value
+
+
+# ---- map files: NESTED .npy and HEALPix FITS (the library's reader and writer) ----
+
+def _path(path):
+    return os.fsencode(os.fspath(path))
+
+
+def map_len(path):
+    """Pixels of the map in a file (.fits / .fit: HEALPix FITS, else .npy),
+    read from its header."""
+    n = C.c_size_t(0)
+    if lib().stlp_map_len(_path(path), C.byref(n)):
+        raise _error()
+    return n.value
+
+
+def read_map(path):
+    """The whole map as a NESTED float64 vector (a RING FITS map is
+    reordered; any float or integer .npy is read as float64)."""
+    out = np.empty(map_len(path))
+    if lib().stlp_map_read(_path(path), _ptr(out), out.size):
+        raise _error()
+    return out
+
+
+def read_npy(path):
+    """A .npy array as float64, in its own shape (C order)."""
+    shape = (C.c_size_t * 32)()
+    ndim = C.c_size_t(0)
+    if lib().stlp_npy_shape(_path(path), shape, 32, C.byref(ndim)):
+        raise _error()
+    return read_map(path).reshape(tuple(shape[i] for i in range(ndim.value)))
+
+
+def read_map_range(path, start, end):
+    """Pixels [start, end) of the NESTED map, read at their offset."""
+    start, end = int(start), int(end)
+    if end < start:
+        raise ValueError("range end before its start")
+    out = np.empty(end - start)
+    if lib().stlp_map_read_range(_path(path), start, end, _ptr(out)):
+        raise _error()
+    return out
+
+
+def write_npy(path, values):
+    """values as a little-endian float64 .npy of their shape."""
+    v = np.require(values, dtype=np.float64, requirements="C")  # 0-d arrays stay 0-d
+    shape = (C.c_size_t * max(1, v.ndim))(*v.shape)
+    if lib().stlp_npy_write(_path(path), _ptr(v), shape, v.ndim):
+        raise _error()
+
+
+def write_healpix_fits(path, values, column="VALUE", double=False):
+    """A full-sky NESTED map as a HEALPix FITS binary table of one column,
+    float32 ('E') or float64 ('D', double=True)."""
+    v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    if lib().stlp_fits_write(_path(path), _ptr(v), v.size, str(column).encode(), int(bool(double))):
+        raise _error()
+
+
+class SlicedMap:
+    """A map file written in pieces, each at its own offset (every process
+    its range): create() writes the headers and sizes the file, write()
+    puts one piece.  .npy float64, or HEALPix FITS ('D' when double)."""
+
+    def __init__(self, path, double=False):
+        self.path, self.double = path, bool(double)
+
+    def create(self, n, column="VALUE"):
+        if lib().stlp_map_create(_path(self.path), int(n), str(column).encode(), int(self.double)):
+            raise _error()
+
+    def write(self, start, values):
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if lib().stlp_map_write(_path(self.path), int(start), _ptr(v), v.size, int(self.double)):
+            raise _error()
 
 
 def _error():
