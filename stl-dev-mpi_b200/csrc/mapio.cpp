@@ -350,6 +350,8 @@ size_t map_len(const std::string& path) {
   return npy_layout(path).count;
 }
 
+std::vector<size_t> npy_shape(const std::string& path) { return npy_layout(path).shape; }
+
 std::vector<double> read_npy(const std::string& path, std::vector<size_t>* shape) {
   const Npy L = npy_layout(path);
   const std::vector<unsigned char> b = read_at(path, L.offset, L.count * L.size);

@@ -22,6 +22,8 @@ size_t map_len(const std::string& path);
 std::vector<double> read_map(const std::string& path);
 // the shape of a .npy array (C order) and its values as float64
 std::vector<double> read_npy(const std::string& path, std::vector<size_t>* shape);
+// the shape alone, from the header
+std::vector<size_t> npy_shape(const std::string& path);
 // pixels [start, end) of the NESTED map (a RING FITS map is read whole)
 std::vector<double> read_map_range(const std::string& path, size_t start, size_t end);
 

@@ -47,8 +47,7 @@ int stlp_map_len(const char* path, size_t* n) {
 int stlp_npy_shape(const char* path, size_t* shape, size_t max_dims, size_t* ndim) {
   return guarded([&] {
     if (!ndim || (max_dims && !shape)) throw std::runtime_error("null argument");
-    std::vector<size_t> s;
-    stl::mapio::read_npy(path_of(path), &s);
+    const std::vector<size_t> s = stl::mapio::npy_shape(path_of(path));
     *ndim = s.size();
     if (s.size() > max_dims) throw std::runtime_error("the array has more axes than the buffer holds");
     for (size_t i = 0; i < s.size(); ++i) shape[i] = s[i];
