@@ -310,12 +310,14 @@ def run_patches(args, torch, dist, world, rank, dev):
         ms = time_steps(torch, step_dev, args.steps, 0, dist)
     clocks = clk.summary()
 
-    g_host = np.empty(x_host.size)  # the gradients' array, kept across calls (vjp out=)
+    g_host = np.empty(x_host.size)  # the gradients' and the statistics' arrays, kept across calls (out=)
+    v_host = np.empty((len(ids), pe.ncoeff), np.complex128)
+    ones = np.ones_like(v_host)
 
     def step_host():
         g = next(gen)
-        v, _ = pe.forward(patches, moments=False, generation=g)
-        pe.vjp(np.ones_like(v), generation=g, out=g_host)
+        v, _ = pe.forward(patches, moments=False, generation=g, out=v_host)
+        pe.vjp(ones, generation=g, out=g_host)
 
     ms_e2e = time_steps(torch, step_host, max(2, args.steps // 2), 1, dist)
     e2e_steps = max(2, args.steps // 2)

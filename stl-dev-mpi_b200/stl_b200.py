@@ -207,6 +207,19 @@ class SlicedMap:
             raise _error()
 
 
+def _all_finite(a, chunk=1 << 20):
+    """Every value of a finite, checked a chunk at a time (a check of the
+    whole array at once would allocate, and page-fault, a mask of its size
+    on every call)."""
+    v = np.asarray(a).reshape(-1)
+    if np.iscomplexobj(v):
+        v = v.view(np.float64) if v.flags.c_contiguous else np.ascontiguousarray(v).view(np.float64)
+    for i in range(0, v.size, chunk):
+        if not np.isfinite(v[i:i + chunk]).all():
+            return False
+    return True
+
+
 def _error():
     msg = lib().stlp_last_error().decode("utf-8", errors="replace")
     # non-finite input maps (the library counts them while it copies the maps) are value errors
@@ -575,7 +588,7 @@ class NativeEngine:
             c = c[None]
         if c.shape != self._shape():
             raise ValueError(f"expected cotangents {self._shape()}, got {c.shape}")
-        if not np.isfinite(c).all():
+        if not _all_finite(c):
             raise ValueError("non-finite coefficient cotangent")
         return c
 
@@ -953,9 +966,11 @@ class PatchEngine:
             self._xbuf = np.empty(total, dtype=np.float64)
         return np.concatenate(flat, out=self._xbuf)
 
-    def forward(self, maps, centres=None, radius=None, core=None, moments=True, generation=0):
+    def forward(self, maps, centres=None, radius=None, core=None, moments=True, generation=0, out=None):
         """Statistics [B, ncoeff] (and variances, or [B, 0]) of the patches of
-        the selected discs (selecting them first when centres are given)."""
+        the selected discs (selecting them first when centres are given).
+        ``out``: a C-contiguous complex128 array [B, ncoeff] to write the
+        statistics into (returned), instead of a new one each call."""
         with self._mutex:
             self._open()
             if centres is not None:
@@ -966,7 +981,13 @@ class PatchEngine:
                 raise RuntimeError("forward before any disc was selected")
             x = self._pack(maps)  # non-finite values are counted by the library's copy (ValueError)
             b = len(self.ids)
-            values = np.empty((b, self.ncoeff), dtype=np.complex128)
+            if out is None:
+                values = np.empty((b, self.ncoeff), dtype=np.complex128)
+            else:
+                if not (isinstance(out, np.ndarray) and out.dtype == np.complex128 and out.flags.c_contiguous
+                        and out.shape == (b, self.ncoeff)):
+                    raise ValueError(f"out must be a C-contiguous complex128 array of shape {(b, self.ncoeff)}")
+                values = out
             variance = np.empty((b, self.ncoeff if moments else 0), dtype=np.float64)
             self._generation = None
             self._dense = isinstance(maps, np.ndarray)
@@ -991,7 +1012,7 @@ class PatchEngine:
             c = np.ascontiguousarray(cotangents, dtype=np.complex128)
             if c.shape != (b, self.ncoeff):
                 raise ValueError(f"cotangents have shape {c.shape}, the statistics {(b, self.ncoeff)}")
-            if not np.isfinite(c.view(np.float64)).all():
+            if not _all_finite(c):
                 raise ValueError("non-finite coefficient cotangent")
             sizes = np.array([i.size for i in self.ids], dtype=np.int64)
             total = int(sizes.sum())

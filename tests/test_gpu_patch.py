@@ -187,8 +187,9 @@ def test_batched_discs_match_one_engine_per_disc(stl):
 
 def test_vjp_into_a_kept_array_and_the_reused_input_buffer(stl):
     """vjp(out=) writes the same gradients into the caller's array (the
-    patches returned are views of it); a second forward of other values
-    through the reused packing buffer equals a fresh engine's."""
+    patches returned are views of it), forward(out=) the same statistics;
+    a second forward of other values through the reused packing buffer
+    equals a fresh engine's."""
     nside, J = 32, 3
     centres = np.array([100, 5000], dtype=np.int64)
     pe = stl.PatchEngine(nside, J, dtype="float64")
@@ -207,6 +208,12 @@ def test_vjp_into_a_kept_array_and_the_reused_input_buffer(stl):
     with pytest.raises(ValueError):
         pe.vjp(cot, generation=1, out=np.empty(3))
     vb, _ = pe.forward(xb, moments=False, generation=2)
+    kept = np.empty_like(vb)
+    vk, _ = pe.forward(xb, moments=False, generation=3, out=kept)
+    assert vk is kept
+    np.testing.assert_array_equal(vk, vb)
+    with pytest.raises(ValueError):
+        pe.forward(xb, moments=False, generation=4, out=np.empty((1, 1), np.complex128))
     fresh = stl.PatchEngine(nside, J, dtype="float64")
     fresh.select(centres, 20.0)
     vb2, _ = fresh.forward(xb, moments=False, generation=1)
