@@ -30,6 +30,14 @@ template <typename T> struct V2;
 template <> struct V2<float> { typedef float2 type; };
 template <> struct V2<double> { typedef double2 type; };
 
+// |z| of every kernel (forward and VJP take moduli through the same
+// function).  FP32: sqrt(x^2 + y^2) with one FMA, within about an ulp of
+// hypotf and without its overflow scaling (fields and moduli are far from
+// overflow); it took the FP32 row means of |z| from 2.27 to 2.02-2.06 ms a step at
+// nside 1024, J 9, B 4.  FP64 keeps hypot: the FMA form measured no faster there.
+__device__ __forceinline__ float zabs(float x, float y) { return sqrtf(fmaf(x, x, y * y)); }
+__device__ __forceinline__ double zabs(double x, double y) { return hypot(x, y); }
+
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 
 // pixel of rotation k of stored index u (full sky: faces 4 (u >> o2) + k)
@@ -338,7 +346,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const int32_t* __restrict__ ce
       if (mod) {
         T* m = mod + p * mod_pix + (i64)r * mod_row + mod_off;
 #pragma unroll
-        for (int g = 0; g < 4; ++g) m[g] = hypot(o[2 * g], o[2 * g + 1]);
+        for (int g = 0; g < 4; ++g) m[g] = zabs(o[2 * g], o[2 * g + 1]);
       }
     }
   }
@@ -516,7 +524,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_conv_fwd_tiles(
     if (mod) {
       T* m = mod + p * mod_pix + (i64)r * mod_row + mod_off;
 #pragma unroll
-      for (int g = 0; g < 4; ++g) m[g] = hypot(o[2 * g], o[2 * g + 1]);
+      for (int g = 0; g < 4; ++g) m[g] = zabs(o[2 * g], o[2 * g + 1]);
     }
   }
 }
@@ -819,7 +827,7 @@ __global__ void __launch_bounds__(kAdjCThreads, 2) k_conv_adj_colored(
         const T* gm = madd.g + pk * madd.g_pix + (i64)(r0 + rb) * madd.g_row;
 #pragma unroll
         for (int l = 0; l < 4; ++l) {
-          const T mag = hypot(zz[2 * l], zz[2 * l + 1]);
+          const T mag = zabs(zz[2 * l], zz[2 * l + 1]);
           const T dd = mag == (T)0 ? (T)1 : mag;
           const T gv = gm[l];
           t[2 * l] += gv * zz[2 * l] / dd;
@@ -1148,7 +1156,7 @@ __global__ void __launch_bounds__(kMmaFwdThreads, 2) k_conv_fwd_mma(
         }
         if (cj) im = -im;
         *reinterpret_cast<float2*>(out + (p * R + r) * 8 + 2 * go) = make_float2(re, im);
-        if (mod) mod[p * mod_pix + (i64)r * mod_row + mod_off + go] = hypotf(re, im);
+        if (mod) mod[p * mod_pix + (i64)r * mod_row + mod_off + go] = zabs(re, im);
       }
   }
 }
@@ -1215,7 +1223,7 @@ __global__ void __launch_bounds__(kMmaAdjThreads, 2) k_conv_adj_mma(
     float v = gy[e + 2 * gg + pt];
     if (madd.z) {
       const float zr = madd.z[e + 2 * gg], zi = madd.z[e + 2 * gg + 1];
-      const float mag = hypotf(zr, zi);
+      const float mag = zabs(zr, zi);
       const float dd = mag == 0.0f ? 1.0f : mag;
       const float gv = madd.g[p * madd.g_pix + (i64)(r0 + rr) * madd.g_row + gg];
       v += gv * (pt ? zi : zr) / dd;
@@ -1363,7 +1371,7 @@ __global__ void k_modvjp(const T* __restrict__ z, const T* __restrict__ g, int g
   const i64 p = i / (B * L);
   const int b = (int)((i / L) % B), l = (int)(i % L);
   const T zr = z[2 * i], zm = z[2 * i + 1];
-  const T mag = hypot(zr, zm);
+  const T mag = zabs(zr, zm);
   const T gv = g[p * g_pix + (i64)b * g_row + l];
   const T dd = mag == (T)0 ? (T)1 : mag;
   gz[2 * i] += gv * zr / dd;
@@ -1531,7 +1539,7 @@ __global__ void __launch_bounds__(kProdMaxWarps * 32, 1) k_products(
           const int j = 8 * it + q8;
           if (j < np && (!mask || mask[pc + j])) {
             const T2 zz = sz[((size_t)j * B + b) * L + l3];
-            const T m = hypot(zz.x, zz.y);
+            const T m = zabs(zz.x, zz.y);
             const T m2 = m * m;
             f[0] += m;
             f[1] += m2;
@@ -1790,7 +1798,7 @@ __global__ void __launch_bounds__(p0_threads<T, ND>(), 1) k_products0(
           fz[2 * l] = fma(a[d][l].x, zz.x, fma(a[d][l].y, zz.y, fz[2 * l]));
           fz[2 * l + 1] = fma(a[d][l].y, zz.x, fma(-a[d][l].x, zz.y, fz[2 * l + 1]));
         }
-      const T m = hypot(zz.x, zz.y);
+      const T m = zabs(zz.x, zz.y);
       f[NF - 2] += m;
       f[NF - 1] = fma(m, m, f[NF - 1]);
       if (x0 && l3 == 0) {
@@ -1951,7 +1959,7 @@ __global__ void __launch_bounds__(kRevThreads) k_products_rev(i64 N, int B, int 
         T2 o;
         T2* dst;
         if (i == K1) {
-          const T mag = hypot(v[q][K1].x, v[q][K1].y);
+          const T mag = zabs(v[q][K1].x, v[q][K1].y);
           const T c = c1 / (mag == (T)0 ? (T)1 : mag);
           o.x = ar[q] + c * v[q][K1].x;
           o.y = ai[q] + c * v[q][K1].y;
@@ -2008,7 +2016,7 @@ __global__ void k_mean_var_grad(const T* __restrict__ x0, const double* __restri
 template <typename T>
 __device__ __forceinline__ T cabs2(const T* f, i64 j) {
   const typename V2<T>::type v = reinterpret_cast<const typename V2<T>::type*>(f)[j];
-  return hypot(v.x, v.y);
+  return zabs(v.x, v.y);
 }
 
 template <typename T, bool CPLX>
@@ -2102,7 +2110,7 @@ __global__ void k_mod_dev(const T* __restrict__ z, i64 N, int B, int L, const do
   // constant is subtracted in FP64 before the one rounding to T
   T o[4];
 #pragma unroll
-  for (int l = 0; l < 4; ++l) o[l] = (T)((double)hypot(v[l].x, v[l].y) - cz[b * 4 + l]);
+  for (int l = 0; l < 4; ++l) o[l] = (T)((double)zabs(v[l].x, v[l].y) - cz[b * 4 + l]);
   store4(mod + p * mod_pix + (i64)b * mod_row + mod_off, o);
 }
 
